@@ -1,0 +1,464 @@
+"""Throughput of the batched soft-body step on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (default): the uneven population -- 512 voxel robots with side
+uniform in 3..8 cells (64 to 729 masses, up to 7,448 springs each), cell
+materials iid {air .3, bone .175, tissue .175, muscle_a .175, muscle_b .175},
+seeded synthetic robots -- stepped with the reference's step semantics at
+dt = 1e-4 for 1 s of simulated time (10,000 steps, the reference's float
+clock).  One bench step = one such evaluation of the whole population.
+
+Metric: spring-updates/s = (non-air springs of all robots) x (steps) /
+seconds.  `value` is device-timed (CUDA events on the context's stream) with
+the population resident in HBM; `e2e` is wall-timed through the C ABI with
+host buffers: upload of the population from pinned memory (mb_set_elements),
+mb_simulate, and the read-back of positions, velocities, stresses and centres
+of mass.  With N GPUs (torchrun) every rank simulates its own population of
+the same shape (weak scaling) and timings are the max over ranks.
+
+--impl reference: the reference's step on this box.  Its `value` is the CPU
+restatement of the reference step (oracle, OpenMP over all host cores) on a
+bounded sample of the same workload; the line also carries the reference's
+own CUDA simulator (built from its sources into oracle/_ref) timed on the
+GPU on the same population, padded to equal mass counts as it requires.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # name: (population, duration s, dt, track stresses)
+    "uneven": ("uneven", 1.0, 1e-4, False),
+    "small": ("small", 1.0, 1e-4, False),
+    "streamed": ("streamed", 0.1, 1e-4, True),
+}
+
+# Algorithmic bytes per spring-update.
+#   HBM (a streaming step that keeps nothing on chip, the reference design):
+#   9 B topology (2 x u16 pair, u8 material, f32 mean length) + 8 B stress
+#   read+write when tracking + per-mass state (pos and vel, 3 floats each,
+#   read and write: 48 B) x masses/springs.
+#   Shared memory (this kernel, per spring-update): 24 B endpoint positions +
+#   12 B correction store + 2 x (4 B incidence entry + 12 B correction) gather
+#   + 8 B material factors; per mass 12 B position store.
+HBM_TOPO_B, HBM_STRESS_B, HBM_MASS_B = 9.0, 8.0, 48.0
+SMEM_SPRING_B, SMEM_MASS_B = 76.0, 12.0
+SMEM_BYTES_PER_CLK_SM = 128.0
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        try:
+            for line in open(self.path):
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        except Exception:
+            pass
+        finally:
+            try:
+                os.unlink(self.path)
+            except Exception:
+                pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+class Pinned:
+    """Keeps pinned host copies of a batch's arrays alive."""
+
+    def __init__(self, batch):
+        import torch
+        self._t = []
+        self.arrays = {}
+        for name in ("mass_offsets", "pos", "vel", "mass_material", "spring_offsets", "pairs",
+                     "spring_material", "lbar"):
+            a = getattr(batch, name)
+            t = torch.empty(a.nbytes, dtype=torch.uint8, pin_memory=True)
+            v = t.numpy().view(a.dtype).reshape(a.shape)
+            v[...] = a
+            self._t.append(t)
+            self.arrays[name] = v
+
+    def batch(self, like):
+        from mercury_b200.element import Batch
+        return Batch(**self.arrays)
+
+    def empty(self, shape, dtype):
+        import torch
+        n = int(np.prod(shape)) * np.dtype(dtype).itemsize
+        t = torch.empty(n, dtype=torch.uint8, pin_memory=True)
+        self._t.append(t)
+        return t.numpy().view(dtype).reshape(shape)
+
+
+def cpu_baseline(batch, dt, track, seconds_target=15.0):
+    """Oracle (C restatement, OpenMP over robots) on a bounded sample: all
+    robots, a number of steps sized to ~seconds_target of work."""
+    import mercury_b200 as mb
+    from oracle import core
+    threads = os.cpu_count() or 1
+    table = mb.material_table()
+    active = batch.active_springs()
+    # calibrate on 20 steps
+    p, v = batch.pos.copy(), batch.vel.copy()
+    s = np.zeros(batch.n_springs, np.float32)
+    t0 = time.perf_counter()
+    core.xpbd_run(batch, p, v, s, table, dt, 0.0, 20, track, threads)
+    rate = active * 20 / max(time.perf_counter() - t0, 1e-9)
+    steps = int(max(20, min(5000, seconds_target * rate / active)))
+    p, v = batch.pos.copy(), batch.vel.copy()
+    s = np.zeros(batch.n_springs, np.float32)
+    t0 = time.perf_counter()
+    core.xpbd_run(batch, p, v, s, table, dt, 0.0, steps, track, threads)
+    el = time.perf_counter() - t0
+    return {"value": active * steps / el, "unit": "spring-updates/s", "cores": threads, "kind": "port",
+            "sample": f"all {batch.n_robots} robots, first {steps} steps of the workload ({el:.1f} s)"}
+
+
+def run_ours(args, rank, local_rank, world):
+    import torch
+
+    import mercury_b200 as mb
+    from mercury_b200 import dist, robots
+
+    pop, duration, dt, track = WORKLOADS[args.workload]
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    batch = robots.population_batch(pop, seed_base=dist.seed_base(1000 * {"small": 0, "uneven": 1, "streamed": 4}[pop], rank))
+    active = batch.active_springs()
+    sim = mb.Simulator(local_rank)
+    sim.setTimeStep(dt)
+    sim.set_batch(batch)
+    steps_per_eval = None
+
+    stream = torch.cuda.ExternalStream(sim.stream, device=dev)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+
+    def one_eval():
+        sim.set_state(batch.pos, batch.vel)
+        sim.Reset()
+        return sim.Simulate(duration, trackStresses=track)
+
+    for _ in range(args.warmup):
+        steps_per_eval = one_eval()
+    sim.synchronize()
+    cfg = sim.launch_config()
+    launches_per_eval = -(-steps_per_eval // cfg["chunk"])
+
+    dist.barrier()
+    times = []
+    with ClockSampler(local_rank) as clk:
+        for _ in range(args.steps):
+            flush.zero_()  # L2 flush between timed iterations (256 MB > 126 MB L2)
+            sim.set_state(batch.pos, batch.vel)
+            sim.Reset()
+            torch.cuda.synchronize(dev)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            sim.Simulate(duration, trackStresses=track)
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1) / 1e3)
+        torch.cuda.synchronize(dev)
+    dist.barrier()
+    t_local = float(np.sum(times))
+    t_max = dist.max_over_ranks(t_local, dev)
+    updates_local = float(active) * steps_per_eval * args.steps
+    updates_all = dist.sum_over_ranks(updates_local, dev)
+    value = updates_all / t_max
+    ms_per_step = 1e3 * t_max / args.steps
+
+    # roofline of the step kernel (per launch)
+    t_launch = t_local / (args.steps * launches_per_eval)
+    upd_launch = float(active) * steps_per_eval / launches_per_eval
+    hbm_b = HBM_TOPO_B + (HBM_STRESS_B if track else 0.0) + HBM_MASS_B * batch.n_masses / active
+    smem_b = SMEM_SPRING_B + SMEM_MASS_B * batch.n_masses / active
+    hbm_peak, hbm_src = peaks()
+    clocks = clk.summary()
+    sm_clk = clocks.get("sm_mhz") or 1965.0
+    smem_peak = SMEM_BYTES_PER_CLK_SM * torch.cuda.get_device_properties(dev).multi_processor_count * sm_clk * 1e6 / 1e9
+    hbm_ach = hbm_b * upd_launch / t_launch / 1e9
+    smem_ach = smem_b * upd_launch / t_launch / 1e9
+
+    # plain configuration: one robot per CTA, one step per launch, no graph
+    plain = None
+    if not args.no_plain:
+        psim = mb.Simulator(local_rank)
+        psim.setTimeStep(dt)
+        psim.set_launch_config(bins=batch.n_robots, chunk=1, use_graph=0)
+        psim.set_batch(batch)
+        pstream = torch.cuda.ExternalStream(psim.stream, device=dev)
+        psim.run_steps(50, track)
+        psim.synchronize()
+        n_plain = 1000
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(pstream)
+        psim.run_steps(n_plain, track)
+        e1.record(pstream)
+        e1.synchronize()
+        tp = dist.max_over_ranks(e0.elapsed_time(e1) / 1e3, dev)
+        plain = dist.sum_over_ranks(float(active) * n_plain, dev) / tp
+        del psim
+
+    # end to end through the C ABI with host buffers (pinned)
+    pinned = Pinned(batch)
+    hb = pinned.batch(batch)
+    out_pos = pinned.empty((batch.n_masses, 4), np.float32)
+    out_vel = pinned.empty((batch.n_masses, 4), np.float32)
+    out_st = pinned.empty((batch.n_springs,), np.float32)
+    esim = mb.Simulator(local_rank)
+    esim.setTimeStep(dt)
+    esim.set_batch(hb)
+    esim.Simulate(duration, track)  # warm: graph built for this clock
+    esim.synchronize()
+    e_steps = max(1, min(args.steps, 5))
+    dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e_steps):
+        esim.set_batch(hb)
+        esim.Reset()
+        esim.Simulate(duration, trackStresses=track)
+        esim.collect_arrays((out_pos, out_vel, out_st))
+        esim.CentreOfMass()
+    e2e_t = dist.max_over_ranks(time.perf_counter() - t0, dev)
+    e2e = dist.sum_over_ranks(float(active) * steps_per_eval * e_steps, dev) / e2e_t
+    h2d = sum(a.nbytes for a in pinned.arrays.values())
+    d2h = out_pos.nbytes + out_vel.nbytes + out_st.nbytes + 12 * batch.n_robots
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(batch, dt, track)
+
+    line = {
+        "metric": "spring-updates/s",
+        "value": value,
+        "unit": "spring-updates/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_per_step,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "vs_plain": (value / plain) if plain else None,
+        "plain": {"value": plain, "unit": "spring-updates/s",
+                  "config": "one robot per CTA, one step per launch, no graph, 1,000 steps"} if plain else None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": {
+            "workload": f"{args.workload}: {batch.n_robots} voxel robots per GPU, "
+                        f"{batch.n_masses} masses, {batch.n_springs} springs ({active} non-air), "
+                        f"reference XPBD step, dt={dt}, {duration} s = {steps_per_eval} steps per bench step",
+            "robots_per_gpu": batch.n_robots,
+            "steps_per_bench_step": steps_per_eval,
+            "active_springs_per_gpu": active,
+            "launch": cfg,
+            "l2": "flushed between timed iterations (256 MB write)",
+            "parallelism": f"population sharded over {world} GPU(s), no collective in the step",
+        },
+        "roofline": {"bound": "hbm", "achieved": hbm_ach, "peak": hbm_peak, "unit": "GB/s",
+                     "frac": hbm_ach / hbm_peak, "traffic": None,
+                     "bytes_per_update": hbm_b, "peak_source": hbm_src,
+                     "note": "HBM bytes a streaming step must move per spring-update; this kernel keeps "
+                             "robots on chip for a whole launch, see roofline_smem"},
+        "roofline_smem": {"bound": "smem", "achieved": smem_ach, "peak": smem_peak, "unit": "GB/s",
+                          "frac": smem_ach / smem_peak, "bytes_per_update": smem_b,
+                          "peak_source": f"nominal 128 B/clk/SM x SMs x median SM clock {sm_clk} MHz"},
+        "kernel_ms_per_launch": 1e3 * t_launch,
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e, "unit": "spring-updates/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h), "steps": e_steps},
+        "gpu_launches": int(launches_per_eval * args.steps),
+        "clocks": clocks,
+    }
+    return line
+
+
+def run_reference(args, rank, local_rank, world):
+    """Reference arm: rank 0 only."""
+    import mercury_b200 as mb  # noqa: F401
+    from mercury_b200 import robots
+    if rank != 0:
+        return None
+    pop, duration, dt, track = WORKLOADS[args.workload]
+    batch = robots.population_batch(pop, seed_base=1000 * {"small": 0, "uneven": 1, "streamed": 4}[pop])
+    active = batch.active_springs()
+    from oracle import core
+    import mercury_b200 as mbm
+    table = mbm.material_table()
+    threads = os.cpu_count() or 1
+    steps_total = core.step_count(duration, dt)
+    # bounded sample per bench step: all robots, `sample` steps
+    p, v = batch.pos.copy(), batch.vel.copy()
+    s = np.zeros(batch.n_springs, np.float32)
+    t0 = time.perf_counter()
+    core.xpbd_run(batch, p, v, s, table, dt, 0.0, 10, track, threads)
+    rate = active * 10 / max(time.perf_counter() - t0, 1e-9)
+    sample = int(max(10, min(steps_total, 4.0 * rate / active)))
+    for _ in range(args.warmup):
+        p, v = batch.pos.copy(), batch.vel.copy()
+        core.xpbd_run(batch, p, v, s, table, dt, 0.0, min(sample, 10), track, threads)
+    tt = 0.0
+    for _ in range(args.steps):
+        p, v = batch.pos.copy(), batch.vel.copy()
+        s[:] = 0
+        t0 = time.perf_counter()
+        core.xpbd_run(batch, p, v, s, table, dt, 0.0, sample, track, threads)
+        tt += time.perf_counter() - t0
+    value = active * sample * args.steps / tt
+    ref_cuda = None
+    if not args.no_ref_cuda:
+        try:
+            ref_cuda = reference_cuda(batch, dt, duration, track)
+        except Exception as e:  # the reference's GPU path is optional evidence
+            ref_cuda = {"unavailable": str(e)[:200]}
+    return {
+        "impl": "reference",
+        "metric": "spring-updates/s",
+        "value": value,
+        "unit": "spring-updates/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1e3 * tt / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": f"{args.workload}: {batch.n_robots} voxel robots, {active} non-air springs, "
+                               f"reference XPBD step, dt={dt}; each bench step = all robots x {sample} of the "
+                               f"{steps_total} steps",
+                   "parallelism": "CPU, OpenMP over robots"},
+        "cpu_baseline": {"value": value, "unit": "spring-updates/s", "cores": threads, "kind": "port",
+                         "sample": f"all {batch.n_robots} robots x {sample} steps per bench step"},
+        "e2e": {"value": value, "unit": "spring-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "reference_cuda": ref_cuda,
+    }
+
+
+def reference_cuda(batch, dt, duration, track):
+    """The reference's own CUDA simulator (oracle/_ref, built from its
+    sources) on the same population: SetElements + Simulate + Collect, wall
+    time around Simulate as optimize/benchmark.cpp:96-109 measures it."""
+    import ctypes
+    path = os.path.join(ROOT, "oracle", "_ref", "libmercury_ref.so")
+    if not os.path.exists(path):
+        return {"unavailable": "oracle/_ref/libmercury_ref.so not built"}
+    L = ctypes.CDLL(path)
+    L.ref_decode_id.argtypes = [ctypes.c_uint32]
+    L.ref_decode_id(1)
+    L.ref_simulate.argtypes = [ctypes.c_int] + [ctypes.c_void_p] * 8 + [ctypes.c_float, ctypes.c_float, ctypes.c_int] + [ctypes.c_void_p] * 4
+    L.ref_simulate.restype = ctypes.c_int
+    mo = batch.mass_offsets.astype(np.int32)
+    so = batch.spring_offsets.astype(np.int32)
+    pos3 = np.ascontiguousarray(batch.pos[:, :3])
+    vel3 = np.ascontiguousarray(batch.vel[:, :3])
+    po, vo = np.zeros_like(pos3), np.zeros_like(vel3)
+    st = np.zeros(batch.n_springs, np.float32)
+    tt = np.zeros(1, np.float32)
+    P = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+    args = (batch.n_robots, P(mo), P(pos3), P(vel3), P(batch.mass_material), P(so),
+            P(np.ascontiguousarray(batch.pairs)), P(batch.lbar), P(batch.spring_material))
+    short = min(duration, 0.01)
+    L.ref_simulate(*args, dt, short, int(track), P(po), P(vo), P(st), P(tt))  # warm-up
+    t0 = time.perf_counter()
+    steps = L.ref_simulate(*args, dt, duration, int(track), P(po), P(vo), P(st), P(tt))
+    wall = time.perf_counter() - t0
+    active = batch.active_springs()
+    return {"value": active * steps / wall, "unit": "spring-updates/s", "steps": steps, "wall_s": wall,
+            "value_all_springs": batch.n_springs * steps / wall,
+            "note": "wall time of SetElements+Simulate+Collect (host packing, H2D, 4 launches and 4 syncs "
+                    "per step, D2H); masses padded per robot to the largest count"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="uneven", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-ref-cuda", action="store_true")
+    args = ap.parse_args()
+
+    from mercury_b200 import dist
+    rank, local_rank, world = dist.env_rank()
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        line = run_reference(args, rank, local_rank, world)
+        print(json.dumps(line), flush=True)
+        return
+    dist.init("nccl" if world > 1 else "gloo")
+    try:
+        line = run_ours(args, rank, local_rank, world)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+    finally:
+        dist.finalize()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,115 @@
+"""ctypes binding of the C ABI declared in include/mercury_b200.h.
+
+The shared library is built in-tree (mercury_b200/libmercury_b200.so) by
+__graft_entry__.build().  There is no fallback: importing this module raises
+if the library is missing, and every call that fails raises MercuryError.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libmercury_b200.so")
+
+MB_OK = 0
+STATUS_NAMES = {
+    0: "MB_OK",
+    1: "MB_ERR_ARGUMENT",
+    2: "MB_ERR_CUDA",
+    3: "MB_ERR_CAPACITY",
+    4: "MB_ERR_STATE",
+    5: "MB_ERR_NONFINITE",
+}
+COMPOSITE_COUNT = 254
+MODE_REF_XPBD = 0
+
+
+class MercuryError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+class BatchDesc(ctypes.Structure):
+    _fields_ = [
+        ("n_robots", ctypes.c_uint32),
+        ("mass_offsets", ctypes.c_void_p),
+        ("pos", ctypes.c_void_p),
+        ("vel", ctypes.c_void_p),
+        ("mass_material", ctypes.c_void_p),
+        ("spring_offsets", ctypes.c_void_p),
+        ("pairs", ctypes.c_void_p),
+        ("spring_material", ctypes.c_void_p),
+        ("lbar", ctypes.c_void_p),
+    ]
+
+
+class LaunchConfig(ctypes.Structure):
+    _fields_ = [
+        ("threads", ctypes.c_uint32),
+        ("springs_per_thread", ctypes.c_uint32),
+        ("masses_per_thread", ctypes.c_uint32),
+        ("bins", ctypes.c_uint32),
+        ("chunk", ctypes.c_uint32),
+        ("use_graph", ctypes.c_uint32),
+    ]
+
+
+def _load() -> ctypes.CDLL:
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"{LIB_PATH} is missing: build it with `python -c 'import __graft_entry__ as g; g.build()'`"
+        )
+    lib = ctypes.CDLL(LIB_PATH)
+    P, U32, I32, F32 = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int, ctypes.c_float
+    sigs = {
+        "mb_context_create": (I32, [I32, ctypes.POINTER(P)]),
+        "mb_context_destroy": (None, [P]),
+        "mb_last_error": (ctypes.c_char_p, [P]),
+        "mb_set_materials": (I32, [P, P]),
+        "mb_set_time_step": (I32, [P, F32]),
+        "mb_get_time_step": (F32, [P]),
+        "mb_set_total_time": (I32, [P, F32]),
+        "mb_get_total_time": (F32, [P]),
+        "mb_set_mode": (I32, [P, I32]),
+        "mb_set_elements": (I32, [P, ctypes.POINTER(BatchDesc)]),
+        "mb_set_state": (I32, [P, P, P]),
+        "mb_simulate": (I32, [P, F32, I32, ctypes.POINTER(U32)]),
+        "mb_run_steps": (I32, [P, U32, I32]),
+        "mb_collect": (I32, [P, P, P, P]),
+        "mb_centre_of_mass": (I32, [P, P]),
+        "mb_robot_flags": (I32, [P, P]),
+        "mb_synchronize": (I32, [P]),
+        "mb_get_stream": (P, [P]),
+        "mb_device_state": (I32, [P, ctypes.POINTER(P), ctypes.POINTER(P), ctypes.POINTER(P)]),
+        "mb_get_launch_config": (I32, [P, ctypes.POINTER(LaunchConfig)]),
+        "mb_set_launch_config": (I32, [P, ctypes.POINTER(LaunchConfig)]),
+        "mb_voxel_build": (I32, [I32, I32, I32, F32, P, ctypes.POINTER(I32), ctypes.POINTER(I32), P, P, P, P, P]),
+        "mb_version": (ctypes.c_char_p, []),
+    }
+    for name, (res, args) in sigs.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+LIB = _load()
+
+
+def ptr(a: np.ndarray | None) -> int | None:
+    """Address of a C-contiguous numpy array (None passes NULL)."""
+    if a is None:
+        return None
+    if not a.flags["C_CONTIGUOUS"]:
+        raise ValueError("array must be C-contiguous")
+    return a.ctypes.data
+
+
+def check(status: int, ctx=None) -> None:
+    if status != MB_OK:
+        msg = LIB.mb_last_error(ctx).decode() if ctx else ""
+        raise MercuryError(status, msg)

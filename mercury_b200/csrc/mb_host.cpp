@@ -1,0 +1,758 @@
+// Host side of the C ABI (include/mercury_b200.h): context, upload and
+// packing of a population into bins, launch configuration, chunked step
+// launches replayed from CUDA graphs, collection.
+//
+// Packing.  The reference gives every robot one CTA and pads every robot to
+// the largest mass and spring count (Simulator.cu:231-239, 489-494).  Here
+// robots keep their own sizes and are grouped into bins, each simulated by
+// one CTA; bins are filled largest-robot-first onto the least loaded bin
+// (LPT), and the bin count is a multiple of the SM count so that every SM
+// gets the same work.  Inside a bin:
+//   - masses keep robot order (robot r's masses, then robot r+1's ...);
+//   - non-air springs are sorted by (b - a, a) so that a warp's springs read
+//     consecutive positions (for a lattice: one direction, consecutive a);
+//   - every mass gets a row of incident springs sorted by (other end,
+//     spring index, a end before b end) -- the fixed summation order -- and
+//     rows are stored 32 masses per slice, column-major (SELL-32), so that a
+//     warp's k-th entries are consecutive words.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/mercury_b200.h"
+#include "mb_internal.h"
+
+namespace mb {
+
+// Composite id of two base materials (material.h:192-213).
+int composite_id(int m1, int m2) {
+    if (m1 == 0 || m2 == 0) return 0;
+    int i = std::min(m1, m2) - 1, j = std::max(m1, m2) - 1;
+    if (i == j) return i + 1;
+    // pairs (i < j) of 22 materials numbered from 23 in row-major order
+    return 23 + i * 21 - i * (i - 1) / 2 + (j - i - 1);
+}
+
+// Composite id of a material encoding (material.h:275-322): the lowest set
+// bit, and the next one if any; air (bit 0) as the lowest bit gives air.
+int decode_id(uint32_t e) {
+    int idx[2] = {0, 0}, count = 0;
+    for (int i = 0; i < 32; ++i)
+        if (e & (1u << i)) {
+            idx[count++] = i;
+            if (i == 0 || count == 2) break;
+        }
+    if (idx[0] == 0) return 0;
+    if (idx[1] == 0) return idx[0];
+    return composite_id(idx[0], idx[1]);
+}
+
+namespace {
+
+template <typename T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    cudaError_t alloc(size_t count) {
+        if (count <= n && p) return cudaSuccess;
+        release();
+        size_t c = std::max<size_t>(count, 1);
+        cudaError_t e = cudaMalloc(&p, c * sizeof(T));
+        if (e == cudaSuccess) n = c;
+        return e;
+    }
+};
+
+struct GraphKey {
+    uint32_t steps;
+    uint32_t t0_bits;
+    uint32_t track;
+    bool operator<(const GraphKey& o) const {
+        if (steps != o.steps) return steps < o.steps;
+        if (t0_bits != o.t0_bits) return t0_bits < o.t0_bits;
+        return track < o.track;
+    }
+};
+
+}  // namespace
+}  // namespace mb
+
+struct mb_context {
+    int device = 0;
+    int num_sms = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+
+    float dt = 0.0001f;  // Simulator.h:55
+    float total_time = 0.0f;
+    mb_mode mode = MB_MODE_REF_XPBD;
+    float table[4 * MB_COMPOSITE_COUNT] = {};
+    bool have_table = false;
+
+    // population
+    bool loaded = false;
+    uint32_t n_robots = 0;
+    uint64_t n_mass = 0, n_spring = 0;
+    std::vector<int64_t> mass_off, spring_off;
+
+    // packing result
+    mb::KernelShape shape{512, 8, 2};
+    uint32_t n_bins = 0;
+    uint32_t chunk = 1000;
+    bool use_graph = true;
+    uint32_t smem_bytes = 0;
+    mb_launch_config override_cfg{};
+
+    // device buffers
+    mb::DevBuf<float4> pos, vel;
+    mb::DevBuf<float> stress;
+    mb::DevBuf<uint8_t> mass_mat;
+    mb::DevBuf<int64_t> d_mass_off;
+    mb::DevBuf<float4> d_table;
+    mb::DevBuf<mb::BinDesc> bins;
+    mb::DevBuf<uint32_t> mass_gidx, spring_gidx, spring_pair, slice_off, slice_width, inc;
+    mb::DevBuf<float> spring_lbar;
+    mb::DevBuf<uint8_t> mat_ids;
+    mb::DevBuf<uint32_t> bin_flags, robot_bin, robot_flags;
+    mb::DevBuf<float> com;
+
+    std::map<mb::GraphKey, cudaGraphExec_t> graphs;
+
+    void clear_graphs() {
+        for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
+        graphs.clear();
+    }
+    ~mb_context() {
+        clear_graphs();
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+namespace {
+
+mb_status fail(mb_context* c, mb_status s, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    if (c) c->err = buf;
+    return s;
+}
+
+mb_status cuda_fail(mb_context* c, cudaError_t e, const char* what) {
+    return fail(c, MB_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define MB_CUDA(ctx, call)                                  \
+    do {                                                    \
+        cudaError_t _e = (call);                            \
+        if (_e != cudaSuccess) return cuda_fail(ctx, _e, #call); \
+    } while (0)
+
+// Per-robot topology after removing air springs, in packed order.
+struct RobotPack {
+    std::vector<uint32_t> springs;  // original local spring index, packed order
+};
+
+// Shapes the automatic choice considers, most springs per CTA first.
+const mb::KernelShape kAuto[] = {
+    {512, 16, 4}, {1024, 8, 2}, {512, 8, 2}, {256, 16, 4}, {256, 8, 2}, {1024, 4, 1},
+    {512, 4, 1}, {256, 4, 1},
+};
+
+struct BinPlan {
+    std::vector<std::vector<uint32_t>> robots;  // per bin, robot ids ascending
+};
+
+// LPT assignment of robots to `nb` bins by non-air spring count (+ masses).
+bool plan_bins(const std::vector<uint64_t>& cost, const std::vector<uint32_t>& nm,
+               const std::vector<uint32_t>& ns, const std::vector<uint64_t>& ninc,
+               uint32_t nb, const mb::KernelShape& sh, uint32_t smem_cap, BinPlan& plan,
+               uint32_t& smem_needed) {
+    const uint32_t n = (uint32_t)cost.size();
+    std::vector<uint32_t> order(n);
+    for (uint32_t i = 0; i < n; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](uint32_t a, uint32_t b) { return cost[a] > cost[b]; });
+    std::vector<uint64_t> load(nb, 0), bm(nb, 0), bs(nb, 0), bi(nb, 0);
+    plan.robots.assign(nb, {});
+    const uint64_t cap_s = (uint64_t)sh.threads * sh.spt;
+    const uint64_t cap_m = std::min<uint64_t>((uint64_t)sh.threads * sh.mpt, 4096);
+    for (uint32_t r : order) {
+        // least loaded bin that still has room
+        int best = -1;
+        for (uint32_t b = 0; b < nb; ++b) {
+            if (bm[b] + nm[r] > cap_m || bs[b] + ns[r] > cap_s) continue;
+            // incidence estimate: padded rows, bounded by smem
+            const uint64_t smem =
+                mb::bin_smem_bytes((uint32_t)(bm[b] + nm[r]), (uint32_t)(bs[b] + ns[r]),
+                                   (uint32_t)(bi[b] + ninc[r]));
+            if (smem > smem_cap) continue;
+            if (best < 0 || load[b] < load[best]) best = (int)b;
+        }
+        if (best < 0) return false;
+        load[best] += cost[r];
+        bm[best] += nm[r];
+        bs[best] += ns[r];
+        bi[best] += ninc[r];
+        plan.robots[best].push_back(r);
+    }
+    smem_needed = 0;
+    for (uint32_t b = 0; b < nb; ++b) {
+        std::sort(plan.robots[b].begin(), plan.robots[b].end());
+        smem_needed = std::max(smem_needed, mb::bin_smem_bytes((uint32_t)bm[b], (uint32_t)bs[b],
+                                                               (uint32_t)bi[b]));
+    }
+    return true;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* mb_version(void) { return "mercury_b200 0.1"; }
+
+mb_status mb_context_create(int device, mb_context** out) {
+    if (!out) return MB_ERR_ARGUMENT;
+    *out = nullptr;
+    std::unique_ptr<mb_context> c(new mb_context());
+    c->device = device;
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return MB_ERR_CUDA;
+    e = cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
+    if (e != cudaSuccess) return MB_ERR_CUDA;
+    e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return MB_ERR_CUDA;
+    *out = c.release();
+    return MB_OK;
+}
+
+void mb_context_destroy(mb_context* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    delete ctx;
+}
+
+const char* mb_last_error(const mb_context* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+mb_status mb_set_materials(mb_context* ctx, const float* table) {
+    if (!ctx || !table) return fail(ctx, MB_ERR_ARGUMENT, "null argument");
+    for (int i = 0; i < 4 * MB_COMPOSITE_COUNT; ++i)
+        if (!std::isfinite(table[i])) return fail(ctx, MB_ERR_ARGUMENT, "non-finite material entry %d", i);
+    std::memcpy(ctx->table, table, sizeof(ctx->table));
+    ctx->have_table = true;
+    cudaSetDevice(ctx->device);
+    MB_CUDA(ctx, ctx->d_table.alloc(MB_COMPOSITE_COUNT));
+    MB_CUDA(ctx, cudaMemcpyAsync(ctx->d_table.p, ctx->table, sizeof(ctx->table),
+                                 cudaMemcpyHostToDevice, ctx->stream));
+    MB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    ctx->clear_graphs();
+    return MB_OK;
+}
+
+mb_status mb_set_time_step(mb_context* ctx, float dt) {
+    if (!ctx) return MB_ERR_ARGUMENT;
+    if (!(dt > 0.0f) || !std::isfinite(dt)) return fail(ctx, MB_ERR_ARGUMENT, "time step must be > 0");
+    if (dt != ctx->dt) ctx->clear_graphs();
+    ctx->dt = dt;
+    return MB_OK;
+}
+float mb_get_time_step(const mb_context* ctx) { return ctx ? ctx->dt : 0.0f; }
+mb_status mb_set_total_time(mb_context* ctx, float t) {
+    if (!ctx) return MB_ERR_ARGUMENT;
+    ctx->total_time = t;
+    return MB_OK;
+}
+float mb_get_total_time(const mb_context* ctx) { return ctx ? ctx->total_time : 0.0f; }
+
+mb_status mb_set_mode(mb_context* ctx, mb_mode mode) {
+    if (!ctx) return MB_ERR_ARGUMENT;
+    if (mode != MB_MODE_REF_XPBD) return fail(ctx, MB_ERR_ARGUMENT, "unknown mode %d", (int)mode);
+    ctx->mode = mode;
+    return MB_OK;
+}
+
+void* mb_get_stream(const mb_context* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+mb_status mb_get_launch_config(const mb_context* ctx, mb_launch_config* cfg) {
+    if (!ctx || !cfg) return MB_ERR_ARGUMENT;
+    cfg->threads = ctx->shape.threads;
+    cfg->springs_per_thread = ctx->shape.spt;
+    cfg->masses_per_thread = ctx->shape.mpt;
+    cfg->bins = ctx->n_bins;
+    cfg->chunk = ctx->chunk;
+    cfg->use_graph = ctx->use_graph ? 1 : 0;
+    return MB_OK;
+}
+
+mb_status mb_set_launch_config(mb_context* ctx, const mb_launch_config* cfg) {
+    if (!ctx || !cfg) return MB_ERR_ARGUMENT;
+    if (cfg->threads) {
+        mb::KernelShape s{cfg->threads, cfg->springs_per_thread, cfg->masses_per_thread};
+        if (!mb::shape_supported(s))
+            return fail(ctx, MB_ERR_ARGUMENT, "kernel shape %u/%u/%u not compiled", s.threads,
+                        s.spt, s.mpt);
+    }
+    ctx->override_cfg = *cfg;
+    if (cfg->chunk) ctx->chunk = cfg->chunk;
+    ctx->use_graph = cfg->use_graph != 0;
+    ctx->clear_graphs();
+    return MB_OK;
+}
+
+mb_status mb_set_elements(mb_context* ctx, const mb_batch_desc* b) {
+    if (!ctx || !b) return fail(ctx, MB_ERR_ARGUMENT, "null argument");
+    if (!ctx->have_table) return fail(ctx, MB_ERR_STATE, "material table not set");
+    const uint32_t R = b->n_robots;
+    if (R == 0) return fail(ctx, MB_ERR_ARGUMENT, "empty population");
+    if (!b->mass_offsets || !b->spring_offsets || !b->pos || !b->vel || !b->mass_material)
+        return fail(ctx, MB_ERR_ARGUMENT, "null array");
+    if (b->mass_offsets[0] != 0 || b->spring_offsets[0] != 0)
+        return fail(ctx, MB_ERR_ARGUMENT, "offsets must start at 0");
+    const uint64_t M = (uint64_t)b->mass_offsets[R], S = (uint64_t)b->spring_offsets[R];
+    if (S && (!b->pairs || !b->spring_material || !b->lbar))
+        return fail(ctx, MB_ERR_ARGUMENT, "null spring array");
+    if (M >= (1ull << 31) || S >= (1ull << 31)) return fail(ctx, MB_ERR_CAPACITY, "population too large");
+
+    // validate and prepare per-robot packing
+    std::vector<uint32_t> nm(R), ns(R);
+    std::vector<uint64_t> cost(R), ninc(R);
+    std::vector<RobotPack> packs(R);
+    for (uint32_t r = 0; r < R; ++r) {
+        const int64_t m0 = b->mass_offsets[r], m1 = b->mass_offsets[r + 1];
+        const int64_t s0 = b->spring_offsets[r], s1 = b->spring_offsets[r + 1];
+        if (m1 < m0 || s1 < s0) return fail(ctx, MB_ERR_ARGUMENT, "offsets decrease at robot %u", r);
+        const int64_t cm = m1 - m0;
+        if (cm > 4096) return fail(ctx, MB_ERR_CAPACITY, "robot %u has %lld masses (max 4096)", r, (long long)cm);
+        std::vector<uint32_t> deg((size_t)cm, 0);
+        auto& sp = packs[r].springs;
+        for (int64_t s = s0; s < s1; ++s) {
+            const uint16_t a = b->pairs[2 * s], c = b->pairs[2 * s + 1];
+            if (a >= cm || c >= cm)
+                return fail(ctx, MB_ERR_ARGUMENT, "spring %lld of robot %u joins mass %u/%u of %lld",
+                            (long long)(s - s0), r, a, c, (long long)cm);
+            if (b->spring_material[s] >= MB_COMPOSITE_COUNT)
+                return fail(ctx, MB_ERR_ARGUMENT, "spring material %u out of range", b->spring_material[s]);
+            if (!std::isfinite(b->lbar[s])) return fail(ctx, MB_ERR_ARGUMENT, "non-finite mean length");
+            if (b->spring_material[s] == 0) continue;  // air springs never act (sim_kernel.cu:211)
+            sp.push_back((uint32_t)(s - s0));
+            deg[a]++;
+            deg[c]++;
+        }
+        for (int64_t i = m0; i < m1; ++i)
+            if (b->mass_material[i] > 22) return fail(ctx, MB_ERR_ARGUMENT, "mass material out of range");
+        std::stable_sort(sp.begin(), sp.end(), [&](uint32_t x, uint32_t y) {
+            const int64_t gx = s0 + x, gy = s0 + y;
+            const int dx = (int)b->pairs[2 * gx + 1] - (int)b->pairs[2 * gx];
+            const int dy = (int)b->pairs[2 * gy + 1] - (int)b->pairs[2 * gy];
+            if (dx != dy) return dx < dy;
+            return b->pairs[2 * gx] < b->pairs[2 * gy];
+        });
+        nm[r] = (uint32_t)cm;
+        ns[r] = (uint32_t)sp.size();
+        cost[r] = (uint64_t)ns[r] * 4 + nm[r];
+        // incidence estimate for smem: rows padded to the slice maximum
+        uint64_t est = 0;
+        for (int64_t i = 0; i < cm; i += 32) {
+            uint32_t w = 0;
+            for (int64_t k = i; k < std::min<int64_t>(i + 32, cm); ++k) w = std::max(w, deg[k]);
+            est += 32ull * w;
+        }
+        ninc[r] = est + 64;  // slack for slices straddling robots
+    }
+
+    // choose shape and bin count
+    cudaSetDevice(ctx->device);
+    const uint32_t smem_cap = mb::max_step_smem(ctx->device);
+    const uint32_t sms = (uint32_t)std::max(ctx->num_sms, 1);
+    uint64_t tot_s = 0, tot_m = 0;
+    uint32_t max_s = 0, max_m = 0;
+    for (uint32_t r = 0; r < R; ++r) {
+        tot_s += ns[r];
+        tot_m += nm[r];
+        max_s = std::max(max_s, ns[r]);
+        max_m = std::max(max_m, nm[r]);
+    }
+    std::vector<mb::KernelShape> shapes;
+    if (ctx->override_cfg.threads)
+        shapes.push_back({ctx->override_cfg.threads, ctx->override_cfg.springs_per_thread,
+                          ctx->override_cfg.masses_per_thread});
+    else
+        for (const auto& s : kAuto) shapes.push_back(s);
+    // Plan bins, build them, and re-plan with more bins while a built bin
+    // overflows shared memory (rows of slices that straddle two robots are
+    // padded to the wider robot, so the estimate is not exact).
+    struct Built {
+        std::vector<mb::BinDesc> bins;
+        std::vector<uint32_t> mass_gidx, spring_gidx, pair, slice_off, slice_width, inc, robot_bin;
+        std::vector<float> lbar;
+        std::vector<uint8_t> mat_ids;
+        uint32_t max_smem = 0;
+    } out;
+    auto build = [&](const BinPlan& plan, uint32_t nb) {
+        out = Built();
+        out.bins.resize(nb);
+        out.robot_bin.resize(R);
+        out.mass_gidx.reserve(M);
+        out.spring_gidx.reserve(S);
+        for (uint32_t bi = 0; bi < nb; ++bi) {
+            mb::BinDesc& d = out.bins[bi];
+            std::memset(&d, 0, sizeof(d));
+            d.mass_begin = (uint32_t)out.mass_gidx.size();
+            d.spring_begin = (uint32_t)out.spring_gidx.size();
+            d.inc_begin = (uint32_t)out.inc.size();
+            d.slice_begin = (uint32_t)out.slice_off.size();
+            d.mat_begin = (uint32_t)out.mat_ids.size();
+            // material slots of the bin, ascending composite id
+            std::vector<int> slot(MB_COMPOSITE_COUNT, -1);
+            std::vector<uint8_t> used;
+            for (uint32_t r : plan.robots[bi])
+                for (uint32_t ls : packs[r].springs) {
+                    const uint8_t m = b->spring_material[b->spring_offsets[r] + ls];
+                    if (slot[m] < 0) {
+                        slot[m] = 0;
+                        used.push_back(m);
+                    }
+                }
+            std::sort(used.begin(), used.end());
+            for (size_t i = 0; i < used.size(); ++i) slot[used[i]] = (int)i;
+            for (uint8_t m : used) out.mat_ids.push_back(m);
+            d.n_mat = (uint32_t)used.size();
+            struct Ent {
+                uint32_t other, orig, sign, packed;
+            };
+            std::vector<std::vector<Ent>> rows;
+            uint32_t mbase = 0, sbase = 0;
+            for (uint32_t r : plan.robots[bi]) {
+                out.robot_bin[r] = bi;
+                const int64_t m0 = b->mass_offsets[r], s0 = b->spring_offsets[r];
+                for (uint32_t i = 0; i < nm[r]; ++i) out.mass_gidx.push_back((uint32_t)(m0 + i));
+                rows.resize(mbase + nm[r]);
+                for (uint32_t k = 0; k < packs[r].springs.size(); ++k) {
+                    const uint32_t ls = packs[r].springs[k];
+                    const int64_t g = s0 + ls;
+                    const uint32_t a = b->pairs[2 * g], c = b->pairs[2 * g + 1];
+                    const uint32_t pa = mbase + a, pc = mbase + c;
+                    out.spring_gidx.push_back((uint32_t)g);
+                    out.pair.push_back(pa | (pc << 12) | ((uint32_t)slot[b->spring_material[g]] << 24));
+                    out.lbar.push_back(b->lbar[g]);
+                    const uint32_t packed = sbase + k;
+                    rows[pa].push_back({c, ls, 0u, packed});
+                    rows[pc].push_back({a, ls, 1u, packed});
+                }
+                mbase += nm[r];
+                sbase += (uint32_t)packs[r].springs.size();
+            }
+            d.n_mass = mbase;
+            d.n_spring = sbase;
+            // rows in summation order, stored SELL-32; padding points at the
+            // zero correction slot after the last spring
+            const uint32_t pad = sbase << 1;
+            for (uint32_t i0 = 0; i0 < mbase; i0 += mb::kSliceWidth) {
+                const uint32_t i1 = std::min<uint32_t>(i0 + mb::kSliceWidth, mbase);
+                uint32_t w = 0;
+                for (uint32_t i = i0; i < i1; ++i) {
+                    auto& row = rows[i];
+                    std::sort(row.begin(), row.end(), [](const Ent& x, const Ent& y) {
+                        if (x.other != y.other) return x.other < y.other;
+                        if (x.orig != y.orig) return x.orig < y.orig;
+                        return x.sign < y.sign;
+                    });
+                    w = std::max<uint32_t>(w, (uint32_t)row.size());
+                }
+                out.slice_off.push_back((uint32_t)out.inc.size() - d.inc_begin);
+                out.slice_width.push_back(w);
+                const size_t base = out.inc.size();
+                out.inc.resize(base + (size_t)w * mb::kSliceWidth, pad);
+                for (uint32_t i = i0; i < i1; ++i)
+                    for (uint32_t k = 0; k < rows[i].size(); ++k)
+                        out.inc[base + (size_t)k * mb::kSliceWidth + (i - i0)] =
+                            (rows[i][k].packed << 1) | rows[i][k].sign;
+            }
+            d.n_inc = (uint32_t)out.inc.size() - d.inc_begin;
+            out.max_smem = std::max(out.max_smem, mb::bin_smem_bytes(d.n_mass, d.n_spring, d.n_inc));
+        }
+    };
+
+    BinPlan plan;
+    bool ok = false;
+    uint32_t smem_needed = 0;
+    for (const auto& sh : shapes) {
+        const uint64_t cap_s = (uint64_t)sh.threads * sh.spt;
+        const uint64_t cap_m = std::min<uint64_t>((uint64_t)sh.threads * sh.mpt, 4096);
+        if (max_s > cap_s || max_m > cap_m) continue;
+        uint32_t nb = ctx->override_cfg.bins;
+        const bool fixed = nb != 0;
+        if (!nb) {
+            const uint64_t need = std::max<uint64_t>((tot_s + cap_s - 1) / cap_s, (tot_m + cap_m - 1) / cap_m);
+            nb = (uint32_t)std::max<uint64_t>(need, 1);
+            if (R >= sms) nb = std::max<uint32_t>(nb, sms);  // one bin per SM at least
+            nb = std::min<uint32_t>(nb, R);
+        }
+        for (uint32_t tries = 0; tries < 16; ++tries) {
+            if (plan_bins(cost, nm, ns, ninc, nb, sh, smem_cap, plan, smem_needed)) {
+                build(plan, nb);
+                if (out.max_smem <= smem_cap) {
+                    ok = true;
+                    break;
+                }
+            }
+            if (fixed || nb >= R) break;
+            nb = std::min<uint32_t>(R, nb + sms);
+        }
+        if (ok) {
+            ctx->shape = sh;
+            ctx->n_bins = nb;
+            break;
+        }
+    }
+    if (!ok)
+        return fail(ctx, MB_ERR_CAPACITY,
+                    "population does not fit any compiled kernel shape (largest robot: %u springs, %u masses)",
+                    max_s, max_m);
+    const uint32_t nb = ctx->n_bins;
+    const uint32_t max_smem = out.max_smem;
+    auto& bins = out.bins;
+    auto& h_mass_gidx = out.mass_gidx;
+    auto& h_spring_gidx = out.spring_gidx;
+    auto& h_pair = out.pair;
+    auto& h_lbar = out.lbar;
+    auto& h_slice_off = out.slice_off;
+    auto& h_slice_width = out.slice_width;
+    auto& h_inc = out.inc;
+    auto& h_mat_ids = out.mat_ids;
+    auto& h_robot_bin = out.robot_bin;
+
+    // upload
+    ctx->clear_graphs();
+    ctx->loaded = false;
+    ctx->n_robots = R;
+    ctx->n_mass = M;
+    ctx->n_spring = S;
+    ctx->mass_off.assign(b->mass_offsets, b->mass_offsets + R + 1);
+    ctx->spring_off.assign(b->spring_offsets, b->spring_offsets + R + 1);
+    ctx->smem_bytes = max_smem;
+    cudaStream_t st = ctx->stream;
+    auto up = [&](auto& buf, const auto* src, size_t n) -> cudaError_t {
+        cudaError_t e = buf.alloc(n);
+        if (e != cudaSuccess || n == 0) return e;
+        return cudaMemcpyAsync(buf.p, src, n * sizeof(*src), cudaMemcpyHostToDevice, st);
+    };
+    MB_CUDA(ctx, up(ctx->pos, reinterpret_cast<const float4*>(b->pos), M));
+    MB_CUDA(ctx, up(ctx->vel, reinterpret_cast<const float4*>(b->vel), M));
+    MB_CUDA(ctx, up(ctx->mass_mat, b->mass_material, M));
+    MB_CUDA(ctx, up(ctx->d_mass_off, b->mass_offsets, R + 1));
+    MB_CUDA(ctx, ctx->stress.alloc(S));
+    if (S) MB_CUDA(ctx, cudaMemsetAsync(ctx->stress.p, 0, S * sizeof(float), st));
+    MB_CUDA(ctx, up(ctx->bins, bins.data(), bins.size()));
+    MB_CUDA(ctx, up(ctx->mass_gidx, h_mass_gidx.data(), h_mass_gidx.size()));
+    MB_CUDA(ctx, up(ctx->spring_gidx, h_spring_gidx.data(), h_spring_gidx.size()));
+    MB_CUDA(ctx, up(ctx->spring_pair, h_pair.data(), h_pair.size()));
+    MB_CUDA(ctx, up(ctx->spring_lbar, h_lbar.data(), h_lbar.size()));
+    MB_CUDA(ctx, up(ctx->slice_off, h_slice_off.data(), h_slice_off.size()));
+    MB_CUDA(ctx, up(ctx->slice_width, h_slice_width.data(), h_slice_width.size()));
+    MB_CUDA(ctx, up(ctx->inc, h_inc.data(), h_inc.size()));
+    MB_CUDA(ctx, up(ctx->mat_ids, h_mat_ids.data(), h_mat_ids.size()));
+    MB_CUDA(ctx, up(ctx->robot_bin, h_robot_bin.data(), h_robot_bin.size()));
+    MB_CUDA(ctx, ctx->bin_flags.alloc(nb));
+    MB_CUDA(ctx, cudaMemsetAsync(ctx->bin_flags.p, 0, nb * sizeof(uint32_t), st));
+    MB_CUDA(ctx, ctx->robot_flags.alloc(R));
+    MB_CUDA(ctx, ctx->com.alloc(3 * (size_t)R));
+    // the host vectors above die with this call: wait for the copies
+    MB_CUDA(ctx, cudaStreamSynchronize(st));
+    ctx->loaded = true;
+    return MB_OK;
+}
+
+mb_status mb_set_state(mb_context* ctx, const float* pos, const float* vel) {
+    if (!ctx || !pos || !vel) return fail(ctx, MB_ERR_ARGUMENT, "null argument");
+    if (!ctx->loaded) return fail(ctx, MB_ERR_STATE, "no population uploaded");
+    cudaSetDevice(ctx->device);
+    const size_t bytes = ctx->n_mass * sizeof(float4);
+    MB_CUDA(ctx, cudaMemcpyAsync(ctx->pos.p, pos, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    MB_CUDA(ctx, cudaMemcpyAsync(ctx->vel.p, vel, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    MB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return MB_OK;
+}
+
+namespace {
+
+mb::StepParams make_params(mb_context* c, float t0, uint32_t steps, bool track) {
+    mb::StepParams p{};
+    p.bins = c->bins.p;
+    p.n_bins = c->n_bins;
+    p.pos = c->pos.p;
+    p.vel = c->vel.p;
+    p.stress = c->stress.p;
+    p.mass_gidx = c->mass_gidx.p;
+    p.spring_gidx = c->spring_gidx.p;
+    p.spring_pair = c->spring_pair.p;
+    p.spring_lbar = c->spring_lbar.p;
+    p.slice_off = c->slice_off.p;
+    p.slice_width = c->slice_width.p;
+    p.inc = c->inc.p;
+    p.mat_ids = c->mat_ids.p;
+    p.table = c->d_table.p;
+    p.bin_flags = c->bin_flags.p;
+    p.dt = c->dt;
+    p.t0 = t0;
+    p.steps = steps;
+    p.track = track ? 1u : 0u;
+    p.smem_bytes = c->smem_bytes;
+    return p;
+}
+
+// Float clock after `n` steps from t (Simulator.cu:447).
+float advance(float t, float dt, uint32_t n) {
+    volatile float v = t;
+    for (uint32_t i = 0; i < n; ++i) v = v + dt;
+    return v;
+}
+
+// Issues the chunk launches for `steps` steps from clock t0 on the stream.
+cudaError_t issue_chunks(mb_context* c, float t0, uint32_t steps, bool track) {
+    float t = t0;
+    uint32_t done = 0;
+    while (done < steps) {
+        const uint32_t n = std::min(c->chunk, steps - done);
+        mb::StepParams p = make_params(c, t, n, track);
+        cudaError_t e = mb::launch_step(p, c->shape, c->stream);
+        if (e != cudaSuccess) return e;
+        t = advance(t, c->dt, n);
+        done += n;
+    }
+    return cudaSuccess;
+}
+
+mb_status run(mb_context* c, uint32_t steps, bool track) {
+    if (!c->loaded) return fail(c, MB_ERR_STATE, "no population uploaded");
+    if (steps == 0) return MB_OK;
+    cudaSetDevice(c->device);
+    const float t0 = c->total_time;
+    if (c->use_graph) {
+        uint32_t bits;
+        std::memcpy(&bits, &t0, 4);
+        const mb::GraphKey key{steps, bits, track ? 1u : 0u};
+        auto it = c->graphs.find(key);
+        if (it == c->graphs.end()) {
+            if (c->graphs.size() >= 16) c->clear_graphs();
+            // kernel attributes cannot change inside a capture
+            MB_CUDA(c, mb::prepare_step(c->shape, track, c->smem_bytes));
+            cudaGraph_t g;
+            MB_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+            cudaError_t e = issue_chunks(c, t0, steps, track);
+            cudaError_t e2 = cudaStreamEndCapture(c->stream, &g);
+            if (e != cudaSuccess) {
+                if (e2 == cudaSuccess) cudaGraphDestroy(g);
+                return cuda_fail(c, e, "capture of step launches");
+            }
+            if (e2 != cudaSuccess) return cuda_fail(c, e2, "cudaStreamEndCapture");
+            cudaGraphExec_t ex;
+            cudaError_t e3 = cudaGraphInstantiate(&ex, g, 0);
+            cudaGraphDestroy(g);
+            if (e3 != cudaSuccess) return cuda_fail(c, e3, "cudaGraphInstantiate");
+            it = c->graphs.emplace(key, ex).first;
+        }
+        MB_CUDA(c, cudaGraphLaunch(it->second, c->stream));
+    } else {
+        MB_CUDA(c, mb::prepare_step(c->shape, track, c->smem_bytes));
+        cudaError_t e = issue_chunks(c, t0, steps, track);
+        if (e != cudaSuccess) return cuda_fail(c, e, "step launch");
+    }
+    c->total_time = advance(t0, c->dt, steps);
+    return MB_OK;
+}
+
+}  // namespace
+
+mb_status mb_run_steps(mb_context* ctx, uint32_t steps, int track_stresses) {
+    if (!ctx) return MB_ERR_ARGUMENT;
+    return run(ctx, steps, track_stresses != 0);
+}
+
+mb_status mb_simulate(mb_context* ctx, float duration, int track_stresses, uint32_t* steps_taken) {
+    if (!ctx) return MB_ERR_ARGUMENT;
+    if (!std::isfinite(duration)) return fail(ctx, MB_ERR_ARGUMENT, "non-finite duration");
+    // step count of the reference loop (Simulator.cu:428-449)
+    uint32_t n = 0;
+    volatile float rem = duration;
+    while (rem > 0.0f) {
+        rem = rem - ctx->dt;
+        ++n;
+        if (n == 0xFFFFFFFFu) return fail(ctx, MB_ERR_ARGUMENT, "too many steps");
+    }
+    if (steps_taken) *steps_taken = n;
+    return run(ctx, n, track_stresses != 0);
+}
+
+mb_status mb_collect(mb_context* ctx, float* pos, float* vel, float* stress) {
+    if (!ctx) return MB_ERR_ARGUMENT;
+    if (!ctx->loaded) return fail(ctx, MB_ERR_STATE, "no population uploaded");
+    cudaSetDevice(ctx->device);
+    const size_t mb4 = ctx->n_mass * sizeof(float4);
+    if (pos) MB_CUDA(ctx, cudaMemcpyAsync(pos, ctx->pos.p, mb4, cudaMemcpyDeviceToHost, ctx->stream));
+    if (vel) MB_CUDA(ctx, cudaMemcpyAsync(vel, ctx->vel.p, mb4, cudaMemcpyDeviceToHost, ctx->stream));
+    if (stress && ctx->n_spring)
+        MB_CUDA(ctx, cudaMemcpyAsync(stress, ctx->stress.p, ctx->n_spring * sizeof(float),
+                                     cudaMemcpyDeviceToHost, ctx->stream));
+    MB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return MB_OK;
+}
+
+mb_status mb_centre_of_mass(mb_context* ctx, float* com) {
+    if (!ctx || !com) return fail(ctx, MB_ERR_ARGUMENT, "null argument");
+    if (!ctx->loaded) return fail(ctx, MB_ERR_STATE, "no population uploaded");
+    cudaSetDevice(ctx->device);
+    MB_CUDA(ctx, mb::launch_com(ctx->pos.p, ctx->mass_mat.p, ctx->d_mass_off.p, ctx->n_robots,
+                                ctx->com.p, ctx->stream));
+    MB_CUDA(ctx, cudaMemcpyAsync(com, ctx->com.p, 3 * sizeof(float) * ctx->n_robots,
+                                 cudaMemcpyDeviceToHost, ctx->stream));
+    MB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return MB_OK;
+}
+
+mb_status mb_robot_flags(mb_context* ctx, uint32_t* flags) {
+    if (!ctx || !flags) return fail(ctx, MB_ERR_ARGUMENT, "null argument");
+    if (!ctx->loaded) return fail(ctx, MB_ERR_STATE, "no population uploaded");
+    cudaSetDevice(ctx->device);
+    MB_CUDA(ctx, mb::launch_flags(ctx->pos.p, ctx->d_mass_off.p, ctx->n_robots,
+                                  ctx->robot_flags.p, ctx->stream));
+    MB_CUDA(ctx, cudaMemcpyAsync(flags, ctx->robot_flags.p, sizeof(uint32_t) * ctx->n_robots,
+                                 cudaMemcpyDeviceToHost, ctx->stream));
+    MB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return MB_OK;
+}
+
+mb_status mb_synchronize(mb_context* ctx) {
+    if (!ctx) return MB_ERR_ARGUMENT;
+    cudaSetDevice(ctx->device);
+    MB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return MB_OK;
+}
+
+mb_status mb_device_state(mb_context* ctx, void** pos, void** vel, void** stress) {
+    if (!ctx) return MB_ERR_ARGUMENT;
+    if (!ctx->loaded) return fail(ctx, MB_ERR_STATE, "no population uploaded");
+    if (pos) *pos = ctx->pos.p;
+    if (vel) *vel = ctx->vel.p;
+    if (stress) *stress = ctx->stress.p;
+    return MB_OK;
+}
+
+}  // extern "C"

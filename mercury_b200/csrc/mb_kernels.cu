@@ -1,0 +1,340 @@
+// Step kernels of the batched soft-body simulator (sm_100a).
+//
+// The reference step (common/simulator/sim_kernel.cu:141-269) launches four
+// kernels per step and re-stages every robot through shared memory each
+// time, accumulating the spring corrections with shared-memory float
+// atomics.  Here one CTA simulates one "bin" (a group of whole robots) for a
+// whole chunk of steps without leaving the SM:
+//
+//   registers : each thread's springs (packed pair + material slot, mean
+//               length, optional 1/length and stress) and masses (x, v);
+//   shared    : predicted positions x~ (SoA), per-spring corrections dp
+//               (SoA), the bin's incidence lists (SELL-32), and the per-step
+//               actuation factors and 1/K of the bin's materials.
+//
+// Per step: (1) warp 0 evaluates the actuation factor dL0*sin(omega*t+phi)
+// of each material of the bin; every thread predicts x~ = x + v*dt for its
+// masses; barrier.  (2) every thread solves its springs (XPBD distance
+// constraint, sim_kernel.cu:209-243) and stores dp per spring; barrier.
+// (3) every thread gathers, for each of its masses, the corrections of the
+// incident springs in a fixed order from its SELL row (no atomics), then
+// integrates x and v (sim_kernel.cu:246-252, 261-268).
+//
+// All arithmetic uses explicit round-to-nearest intrinsics so that the
+// result is bit-identical to the CPU restatement in the oracle.
+#include "mb_internal.h"
+#include "mb_sin.cuh"
+
+namespace mb {
+
+namespace {
+
+constexpr float kEps = 1e-12f;  // sim_kernel.cu:6
+
+__host__ __device__ inline uint32_t round4(uint32_t x) { return (x + 3u) & ~3u; }
+
+// Packed spring word: a (12 bits) | b << 12 (12 bits) | slot << 24 (8 bits).
+__device__ __forceinline__ uint32_t pk_a(uint32_t w) { return w & 0xFFFu; }
+__device__ __forceinline__ uint32_t pk_b(uint32_t w) { return (w >> 12) & 0xFFFu; }
+__device__ __forceinline__ uint32_t pk_slot(uint32_t w) { return w >> 24; }
+
+template <int T, int SPT, int MPT, bool TRACK>
+__global__ void __launch_bounds__(T, 1) step_kernel(const StepParams p) {
+    extern __shared__ float4 smem4[];
+    float* const sm = reinterpret_cast<float*>(smem4);
+    const int tid = threadIdx.x;
+    const float dt = p.dt;
+    const double ddt = (double)dt;
+
+    for (uint32_t b = blockIdx.x; b < p.n_bins; b += gridDim.x) {
+        const BinDesc bd = p.bins[b];
+        const uint32_t m4 = round4(bd.n_mass), s4 = round4(bd.n_spring + 1);
+        float* sx = sm;
+        float* sy = sx + m4;
+        float* sz = sy + m4;
+        float* sdx = sz + m4;
+        float* sdy = sdx + s4;
+        float* sdz = sdy + s4;
+        uint32_t* sinc = reinterpret_cast<uint32_t*>(sdz + s4);
+        float* srate = reinterpret_cast<float*>(sinc + bd.n_inc);  // dL0*sin(...)
+        float* sinvk = srate + kMaxMaterialSlots;                   // 1/K
+
+        for (uint32_t i = tid; i < bd.n_inc; i += T) sinc[i] = __ldg(&p.inc[bd.inc_begin + i]);
+        if (tid == 0) {
+            sdx[bd.n_spring] = 0.0f;
+            sdy[bd.n_spring] = 0.0f;
+            sdz[bd.n_spring] = 0.0f;
+        }
+        for (uint32_t i = tid; i < bd.n_mat; i += T) {
+            const float4 mt = __ldg(&p.table[p.mat_ids[bd.mat_begin + i]]);
+            // alpha = 1/k/dt/dt, K = 2 + alpha (sim_kernel.cu:220, 225)
+            const float alpha = __fdiv_rn(__fdiv_rn(__fdiv_rn(1.0f, mt.x), dt), dt);
+            sinvk[i] = __frcp_rn(__fadd_rn(2.0f, alpha));
+        }
+
+        // Springs of this thread: packed word, mean length, 1/length, stress.
+        uint32_t sw[SPT];
+        float lb[SPT], il[SPT], st[SPT];
+#pragma unroll
+        for (int j = 0; j < SPT; ++j) {
+            const uint32_t s = tid + j * T;
+            sw[j] = 0;
+            lb[j] = 0.0f;
+            il[j] = 0.0f;
+            st[j] = 0.0f;
+            if (s < bd.n_spring) {
+                const uint32_t g = bd.spring_begin + s;
+                sw[j] = __ldg(&p.spring_pair[g]);
+                lb[j] = __ldg(&p.spring_lbar[g]);
+                if (TRACK) {
+                    il[j] = __frcp_rn(lb[j]);
+                    st[j] = p.stress[__ldg(&p.spring_gidx[g])];
+                }
+            }
+        }
+        // Masses of this thread: x, v (float4 keeps w), SELL row.
+        float4 x[MPT], v[MPT];
+        uint32_t roff[MPT], rwid[MPT];
+#pragma unroll
+        for (int j = 0; j < MPT; ++j) {
+            const uint32_t m = tid + j * T;
+            x[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+            v[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+            roff[j] = 0;
+            rwid[j] = 0;
+            if (m < bd.n_mass) {
+                const uint32_t g = __ldg(&p.mass_gidx[bd.mass_begin + m]);
+                x[j] = p.pos[g];
+                v[j] = p.vel[g];
+                const uint32_t sl = bd.slice_begin + m / kSliceWidth;
+                roff[j] = __ldg(&p.slice_off[sl]) + (m % kSliceWidth);
+                rwid[j] = __ldg(&p.slice_width[sl]);
+            }
+        }
+        __syncthreads();
+
+        float t = p.t0;
+        for (uint32_t step = 0; step < p.steps; ++step) {
+            // (1) actuation factors of the bin's materials (sim_kernel.cu:222)
+            if (tid < 32) {
+                for (uint32_t i = tid; i < bd.n_mat; i += 32) {
+                    const float4 mt = __ldg(&p.table[p.mat_ids[bd.mat_begin + i]]);
+                    const float arg = __fmaf_rn(mt.z, t, mt.w);
+                    const float sn = __double2float_rn(sin_cw((double)arg));
+                    srate[i] = __fmul_rn(mt.y, sn);
+                }
+            }
+            // (1) predict x~ = x + v*dt (sim_kernel.cu:147-152)
+            float3 xt[MPT];
+#pragma unroll
+            for (int j = 0; j < MPT; ++j) {
+                const uint32_t m = tid + j * T;
+                xt[j].x = __fadd_rn(x[j].x, __fmul_rn(v[j].x, dt));
+                xt[j].y = __fadd_rn(x[j].y, __fmul_rn(v[j].y, dt));
+                xt[j].z = __fadd_rn(x[j].z, __fmul_rn(v[j].z, dt));
+                if (m < bd.n_mass) {
+                    sx[m] = xt[j].x;
+                    sy[m] = xt[j].y;
+                    sz[m] = xt[j].z;
+                }
+            }
+            __syncthreads();
+            // (2) distance constraints (sim_kernel.cu:209-243)
+#pragma unroll
+            for (int j = 0; j < SPT; ++j) {
+                const uint32_t s = tid + j * T;
+                if (s < bd.n_spring) {
+                    const uint32_t a = pk_a(sw[j]), bb = pk_b(sw[j]), sl = pk_slot(sw[j]);
+                    const float L = __fmaf_rn(lb[j], srate[sl], lb[j]);
+                    const float dx = __fsub_rn(sx[a], sx[bb]);
+                    const float dy = __fsub_rn(sy[a], sy[bb]);
+                    const float dz = __fsub_rn(sz[a], sz[bb]);
+                    const float d2 = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, __fmul_rn(dz, dz)));
+                    const float d = __fsqrt_rn(d2);
+                    const float r = __frcp_rn(__fadd_rn(d, kEps));
+                    const float C = __fsub_rn(d, L);
+                    const float lam = __fmul_rn(-C, sinvk[sl]);
+                    const float coef = __fmul_rn(lam, r);
+                    sdx[s] = __fmul_rn(coef, dx);
+                    sdy[s] = __fmul_rn(coef, dy);
+                    sdz[s] = __fmul_rn(coef, dz);
+                    if (TRACK) st[j] = __fadd_rn(st[j], __fmul_rn(lam, il[j]));
+                }
+            }
+            __syncthreads();
+            // (3) gather in SELL order and integrate (sim_kernel.cu:246-268)
+#pragma unroll
+            for (int j = 0; j < MPT; ++j) {
+                const uint32_t m = tid + j * T;
+                if (m < bd.n_mass) {
+                    float ax = 0.0f, ay = 0.0f, az = 0.0f;
+                    const uint32_t base = roff[j], w = rwid[j];
+                    for (uint32_t k = 0; k < w; ++k) {
+                        const uint32_t e = sinc[base + k * kSliceWidth];
+                        const uint32_t s = e >> 1;
+                        float cx = sdx[s], cy = sdy[s], cz = sdz[s];
+                        if (e & 1u) {
+                            cx = -cx;
+                            cy = -cy;
+                            cz = -cz;
+                        }
+                        ax = __fadd_rn(ax, cx);
+                        ay = __fadd_rn(ay, cy);
+                        az = __fadd_rn(az, cz);
+                    }
+                    const float nx = __fadd_rn(xt[j].x, ax);
+                    const float ny = __fadd_rn(xt[j].y, ay);
+                    const float nz = __fadd_rn(xt[j].z, az);
+                    // v = 0.99*(x~ - x)/dt in double (sim_kernel.cu:265-267)
+                    v[j].x = __double2float_rn(__ddiv_rn(__dmul_rn(0.99, (double)__fsub_rn(nx, x[j].x)), ddt));
+                    v[j].y = __double2float_rn(__ddiv_rn(__dmul_rn(0.99, (double)__fsub_rn(ny, x[j].y)), ddt));
+                    v[j].z = __double2float_rn(__ddiv_rn(__dmul_rn(0.99, (double)__fsub_rn(nz, x[j].z)), ddt));
+                    x[j].x = nx;
+                    x[j].y = ny;
+                    x[j].z = nz;
+                }
+            }
+            t = __fadd_rn(t, dt);
+        }
+
+        // Write back in the upload layout; flag non-finite positions.
+        bool bad = false;
+#pragma unroll
+        for (int j = 0; j < MPT; ++j) {
+            const uint32_t m = tid + j * T;
+            if (m < bd.n_mass) {
+                const uint32_t g = __ldg(&p.mass_gidx[bd.mass_begin + m]);
+                p.pos[g] = x[j];
+                p.vel[g] = v[j];
+                bad |= !(isfinite(x[j].x) && isfinite(x[j].y) && isfinite(x[j].z));
+            }
+        }
+        if (TRACK) {
+#pragma unroll
+            for (int j = 0; j < SPT; ++j) {
+                const uint32_t s = tid + j * T;
+                if (s < bd.n_spring) p.stress[__ldg(&p.spring_gidx[bd.spring_begin + s])] = st[j];
+            }
+        }
+        if (__syncthreads_or(bad) && tid == 0) atomicOr(&p.bin_flags[b], 1u);
+    }
+}
+
+// Centre of mass of non-air masses, one warp per robot: lane l sums masses
+// l, l+32, ... in double, then an xor butterfly; mean rounded to float.
+__global__ void com_kernel(const float4* __restrict__ pos, const uint8_t* __restrict__ mat,
+                           const int64_t* __restrict__ off, uint32_t n_robots,
+                           float* __restrict__ com) {
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) / 32;
+    const uint32_t lane = threadIdx.x % 32;
+    if (warp >= n_robots) return;
+    const int64_t b = off[warp], n = off[warp + 1] - b;
+    double sx = 0.0, sy = 0.0, sz = 0.0;
+    long long cnt = 0;
+    for (int64_t i = lane; i < n; i += 32) {
+        if (!mat[b + i]) continue;
+        const float4 q = pos[b + i];
+        sx = __dadd_rn(sx, (double)q.x);
+        sy = __dadd_rn(sy, (double)q.y);
+        sz = __dadd_rn(sz, (double)q.z);
+        ++cnt;
+    }
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) {
+        sx = __dadd_rn(sx, __shfl_xor_sync(0xffffffffu, sx, o));
+        sy = __dadd_rn(sy, __shfl_xor_sync(0xffffffffu, sy, o));
+        sz = __dadd_rn(sz, __shfl_xor_sync(0xffffffffu, sz, o));
+        cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+    }
+    if (lane == 0) {
+        const double dc = (double)cnt;
+        com[3 * warp + 0] = cnt ? __double2float_rn(__ddiv_rn(sx, dc)) : 0.0f;
+        com[3 * warp + 1] = cnt ? __double2float_rn(__ddiv_rn(sy, dc)) : 0.0f;
+        com[3 * warp + 2] = cnt ? __double2float_rn(__ddiv_rn(sz, dc)) : 0.0f;
+    }
+}
+
+// Per-robot status: bit 0 set when any position of the robot is NaN/Inf.
+// One warp per robot.
+__global__ void flags_kernel(const float4* __restrict__ pos, const int64_t* __restrict__ off,
+                             uint32_t n_robots, uint32_t* __restrict__ out) {
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) / 32;
+    const uint32_t lane = threadIdx.x % 32;
+    if (warp >= n_robots) return;
+    bool bad = false;
+    for (int64_t i = off[warp] + lane; i < off[warp + 1]; i += 32) {
+        const float4 q = pos[i];
+        bad |= !(isfinite(q.x) && isfinite(q.y) && isfinite(q.z));
+    }
+    bad = __any_sync(0xffffffffu, bad);
+    if (lane == 0) out[warp] = bad ? 1u : 0u;
+}
+
+using StepFn = void (*)(const StepParams);
+
+struct ShapeEntry {
+    uint32_t threads, spt, mpt;
+    StepFn fn[2];  // [track]
+};
+
+#define MB_SHAPE(T, S, M) {T, S, M, {step_kernel<T, S, M, false>, step_kernel<T, S, M, true>}}
+const ShapeEntry kShapes[] = {
+    MB_SHAPE(256, 4, 1),  MB_SHAPE(256, 8, 2),  MB_SHAPE(256, 16, 4),
+    MB_SHAPE(512, 4, 1),  MB_SHAPE(512, 8, 2),  MB_SHAPE(512, 16, 4),
+    MB_SHAPE(1024, 4, 1), MB_SHAPE(1024, 8, 2),
+};
+#undef MB_SHAPE
+
+const ShapeEntry* find_shape(const KernelShape& s) {
+    for (const auto& e : kShapes)
+        if (e.threads == s.threads && e.spt == s.spt && e.mpt == s.mpt) return &e;
+    return nullptr;
+}
+
+}  // namespace
+
+uint32_t bin_smem_bytes(uint32_t n_mass, uint32_t n_spring, uint32_t n_inc) {
+    return 4u * (3u * round4(n_mass) + 3u * round4(n_spring + 1) + n_inc + 2u * kMaxMaterialSlots);
+}
+
+uint32_t max_step_smem(int device) {
+    int v = 0;
+    cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+    return (uint32_t)v;
+}
+
+bool shape_supported(const KernelShape& shape) { return find_shape(shape) != nullptr; }
+
+cudaError_t prepare_step(const KernelShape& shape, bool track, uint32_t smem_bytes) {
+    const ShapeEntry* e = find_shape(shape);
+    if (!e) return cudaErrorInvalidValue;
+    return cudaFuncSetAttribute(e->fn[track ? 1 : 0], cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)smem_bytes);
+}
+
+cudaError_t launch_step(const StepParams& p, const KernelShape& shape, cudaStream_t s) {
+    const ShapeEntry* e = find_shape(shape);
+    if (!e) return cudaErrorInvalidValue;
+    if (p.n_bins == 0) return cudaSuccess;
+    e->fn[p.track ? 1 : 0]<<<p.n_bins, shape.threads, p.smem_bytes, s>>>(p);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_com(const float4* pos, const uint8_t* mass_mat, const int64_t* mass_off,
+                       uint32_t n_robots, float* com, cudaStream_t s) {
+    if (n_robots == 0) return cudaSuccess;
+    const uint32_t threads = 256, warps = threads / 32;
+    com_kernel<<<(n_robots + warps - 1) / warps, threads, 0, s>>>(pos, mass_mat, mass_off,
+                                                                   n_robots, com);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_flags(const float4* pos, const int64_t* mass_off, uint32_t n_robots,
+                         uint32_t* out, cudaStream_t s) {
+    if (n_robots == 0) return cudaSuccess;
+    const uint32_t threads = 256, warps = threads / 32;
+    flags_kernel<<<(n_robots + warps - 1) / warps, threads, 0, s>>>(pos, mass_off, n_robots, out);
+    return cudaGetLastError();
+}
+
+}  // namespace mb

@@ -1,0 +1,98 @@
+"""Seeded synthetic robot populations.
+
+Voxel robots are built by the library's lattice builder (mb_voxel_build, the
+topology of the reference's VoxelRobot::Build, VoxelRobot.cpp:310-331).  A
+robot of `side` cells per axis has (side+1)^3 grid points; grid point p
+carries the material of the cell whose lowest corner is p, so points on the
+upper faces carry air (as VoxelRobot::Initialize does, VoxelRobot.cpp:375-378).
+
+Populations (cell size 0.1 m, one seed per robot = 1000*population + robot,
+numpy PCG64):
+  small      32 robots of 4x4x4 cells, cells iid {air .3, bone .175,
+             tissue .175, muscle_a .175, muscle_b .175}
+  uneven     512 robots, side uniform in 3..8, same materials
+  streamed   64 robots of 10x10x10 cells, all occupied, iid over
+             {bone, tissue, muscle_a, muscle_b}
+For the reference step, muscle_a is adductor_muscle0 (phase 0) and muscle_b
+abductor_muscle0 (phase pi), material.h:112, 122.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from .element import Element, pack
+from .materials import ABDUCTOR_MUSCLE0, ADDUCTOR_MUSCLE0, AIR, BONE, TISSUE
+
+CELL = 0.1
+FIVE = np.array([AIR, BONE, TISSUE, ADDUCTOR_MUSCLE0, ABDUCTOR_MUSCLE0], np.uint8)
+FIVE_P = np.array([0.3, 0.175, 0.175, 0.175, 0.175])
+FOUR = np.array([BONE, TISSUE, ADDUCTOR_MUSCLE0, ABDUCTOR_MUSCLE0], np.uint8)
+
+
+def voxel_robot(cells: np.ndarray, h: float = CELL) -> Element:
+    """Robot from a (nz, ny, nx)... cell grid given as a cubic array of base
+    material ids indexed [x, y, z]; one extra air layer closes the upper
+    faces."""
+    cells = np.asarray(cells, np.uint8)
+    sx, sy, sz = cells.shape
+    nx, ny, nz = sx + 1, sy + 1, sz + 1
+    grid = np.zeros((nx, ny, nz), np.uint8)
+    grid[:sx, :sy, :sz] = cells
+    return lattice_robot(grid, h)
+
+
+def lattice_robot(grid: np.ndarray, h: float = CELL) -> Element:
+    """Robot from a grid of points indexed [x, y, z] (mb_voxel_build)."""
+    grid = np.asarray(grid, np.uint8)
+    nx, ny, nz = grid.shape
+    mats = np.ascontiguousarray(grid.transpose(2, 1, 0).reshape(-1))  # x fastest
+    n = nx * ny * nz
+    pos = np.zeros(3 * n, np.float32)
+    mm = np.zeros(n, np.uint8)
+    pairs = np.zeros(2 * 13 * n, np.uint16)
+    lbar = np.zeros(13 * n, np.float32)
+    sm = np.zeros(13 * n, np.uint8)
+    nm, ns = ctypes.c_int(), ctypes.c_int()
+    st = _lib.LIB.mb_voxel_build(nx, ny, nz, h, _lib.ptr(mats), ctypes.byref(nm), ctypes.byref(ns),
+                                 _lib.ptr(pos), _lib.ptr(mm), _lib.ptr(pairs), _lib.ptr(lbar),
+                                 _lib.ptr(sm))
+    _lib.check(st)
+    s = ns.value
+    return Element(pos.reshape(n, 3), mm, pairs[: 2 * s].reshape(s, 2), lbar[:s], sm[:s])
+
+
+def random_cells(side: int, rng: np.random.Generator, choices=FIVE, p=FIVE_P) -> np.ndarray:
+    return choices[rng.choice(len(choices), size=(side, side, side), p=p)]
+
+
+def population(name: str, n_robots: int | None = None, seed_base: int | None = None) -> list[Element]:
+    """One of the named synthetic populations (see module docstring)."""
+    spec = {
+        "small": (0, 32),
+        "uneven": (1, 512),
+        "streamed": (4, 64),
+    }
+    if name not in spec:
+        raise ValueError(f"unknown population {name!r}")
+    base, default_n = spec[name]
+    n = default_n if n_robots is None else n_robots
+    seed0 = 1000 * base if seed_base is None else seed_base
+    out = []
+    for r in range(n):
+        rng = np.random.default_rng(seed0 + r)
+        if name == "small":
+            cells = random_cells(4, rng)
+        elif name == "uneven":
+            side = int(rng.integers(3, 9))
+            cells = random_cells(side, rng)
+        else:
+            cells = FOUR[rng.integers(0, 4, size=(10, 10, 10))]
+        out.append(voxel_robot(cells))
+    return out
+
+
+def population_batch(name: str, n_robots: int | None = None, seed_base: int | None = None):
+    return pack(population(name, n_robots, seed_base))

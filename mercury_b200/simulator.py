@@ -1,0 +1,205 @@
+"""Python mirror of the reference's class Simulator
+(common/simulator/Simulator.h:19-149) over the C ABI.
+
+Method names, arguments and defaults follow the reference so that its
+callers read the same:
+
+    sim = Simulator()
+    sim.Initialize(SimulatorConfig(time_step=1e-3))
+    trackers = sim.SetElements(elements)
+    sim.Simulate(1.0, trackStresses=False)
+    results = sim.Collect(trackers)
+
+Differences, by design: robots may have different mass counts (the
+reference requires equal counts, Simulator.cu:231); errors raise
+MercuryError instead of exiting the process (Simulator.cu:10-18); Collect
+also returns spring stresses (the reference copies them but drops them,
+Simulator.cu:540); CentreOfMass() reduces on the device.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from .element import Batch, Element, pack, unpack
+from .materials import material_table
+
+ENVIRONMENT_LAND, ENVIRONMENT_WATER = 0, 1
+
+
+@dataclass
+class SimulatorConfig:
+    """Config::Simulator (common/util/config.h:16-21)."""
+    visual: bool = False
+    replaced_springs_per_element: int = 128
+    time_step: float = 0.005
+    env_type: int = ENVIRONMENT_WATER
+
+
+@dataclass
+class ElementTracker:
+    """Simulator.h:11-17: which masses and springs of the batch are robot ID."""
+    ID: int
+    mass_begin: int
+    mass_end: int
+    spring_begin: int
+    spring_end: int
+
+
+class Simulator:
+    def __init__(self, device: int = 0):
+        ctx = ctypes.c_void_p()
+        _lib.check(_lib.LIB.mb_context_create(device, ctypes.byref(ctx)))
+        self._ctx = ctx
+        self._batch: Batch | None = None
+        self._elements: list[Element] = []
+        self.config = SimulatorConfig()
+        self._table = material_table()
+        _lib.check(_lib.LIB.mb_set_materials(self._ctx, _lib.ptr(self._table)), self._ctx)
+        # the reference's m_deltaT before Initialize (Simulator.h:55)
+        self.setTimeStep(0.0001)
+
+    def __del__(self):
+        ctx = getattr(self, "_ctx", None)
+        if ctx:
+            _lib.LIB.mb_context_destroy(ctx)
+            self._ctx = None
+
+    # -- Simulator.h:27-48 ------------------------------------------------
+    def Initialize(self, config: SimulatorConfig | None = None) -> None:
+        self.config = config or SimulatorConfig()
+        self.setTimeStep(self.config.time_step)
+        self.Reset()
+
+    def SetElement(self, element: Element) -> ElementTracker:
+        return self.SetElements([element])[0]
+
+    def SetElements(self, elements: list[Element]) -> list[ElementTracker]:
+        batch = pack(elements)
+        self.set_batch(batch)
+        self._elements = list(elements)
+        return [ElementTracker(r, int(batch.mass_offsets[r]), int(batch.mass_offsets[r + 1]),
+                               int(batch.spring_offsets[r]), int(batch.spring_offsets[r + 1]))
+                for r in range(batch.n_robots)]
+
+    def Simulate(self, sim_duration: float, trackStresses: bool = False, trace: bool = False,
+                 tracefile: str = "trace.csv") -> int:
+        """Runs sim_duration seconds; returns the number of steps taken."""
+        if trace:
+            raise NotImplementedError("tracing is not supported; Collect between Simulate calls")
+        n = ctypes.c_uint32()
+        _lib.check(_lib.LIB.mb_simulate(self._ctx, float(sim_duration), int(bool(trackStresses)),
+                                        ctypes.byref(n)), self._ctx)
+        return n.value
+
+    def Devo(self) -> None:
+        raise NotImplementedError("Devo is not part of this build")
+
+    def Collect(self, trackers):
+        single = isinstance(trackers, ElementTracker)
+        trackers = [trackers] if single else list(trackers)
+        pos, vel, stress = self.collect_arrays()
+        full = unpack(self._batch, pos, vel, stress, self._elements)
+        out = [full[t.ID] for t in trackers]
+        return out[0] if single else out
+
+    def CollectElement(self, tracker: ElementTracker) -> Element:
+        return self.Collect(tracker)
+
+    def getDeltaT(self) -> float:
+        return float(_lib.LIB.mb_get_time_step(self._ctx))
+
+    def setTimeStep(self, dt: float) -> None:
+        _lib.check(_lib.LIB.mb_set_time_step(self._ctx, float(dt)), self._ctx)
+
+    def getTotalTime(self) -> float:
+        return float(_lib.LIB.mb_get_total_time(self._ctx))
+
+    def Reset(self) -> None:
+        _lib.check(_lib.LIB.mb_set_total_time(self._ctx, 0.0), self._ctx)
+
+    # -- array-level interface ---------------------------------------------
+    def set_batch(self, batch: Batch) -> None:
+        self._batch = batch
+        d = _lib.BatchDesc(
+            batch.n_robots, _lib.ptr(batch.mass_offsets), _lib.ptr(batch.pos), _lib.ptr(batch.vel),
+            _lib.ptr(batch.mass_material), _lib.ptr(batch.spring_offsets), _lib.ptr(batch.pairs),
+            _lib.ptr(batch.spring_material), _lib.ptr(batch.lbar))
+        _lib.check(_lib.LIB.mb_set_elements(self._ctx, ctypes.byref(d)), self._ctx)
+
+    def set_state(self, pos: np.ndarray, vel: np.ndarray) -> None:
+        pos = np.ascontiguousarray(pos, np.float32)
+        vel = np.ascontiguousarray(vel, np.float32)
+        _lib.check(_lib.LIB.mb_set_state(self._ctx, _lib.ptr(pos), _lib.ptr(vel)), self._ctx)
+
+    def run_steps(self, steps: int, track_stresses: bool = False) -> None:
+        _lib.check(_lib.LIB.mb_run_steps(self._ctx, int(steps), int(bool(track_stresses))), self._ctx)
+
+    def collect_arrays(self, out=None):
+        b = self._batch
+        if b is None:
+            raise _lib.MercuryError(4, "no population uploaded")
+        if out is None:
+            pos = np.empty((b.n_masses, 4), np.float32)
+            vel = np.empty((b.n_masses, 4), np.float32)
+            stress = np.empty(b.n_springs, np.float32)
+        else:
+            pos, vel, stress = out
+        _lib.check(_lib.LIB.mb_collect(self._ctx, _lib.ptr(pos), _lib.ptr(vel), _lib.ptr(stress)),
+                   self._ctx)
+        return pos, vel, stress
+
+    def CentreOfMass(self) -> np.ndarray:
+        """(R, 3) centre of mass of the non-air masses of every robot."""
+        com = np.empty((self._batch.n_robots, 3), np.float32)
+        _lib.check(_lib.LIB.mb_centre_of_mass(self._ctx, _lib.ptr(com)), self._ctx)
+        return com
+
+    def robot_flags(self) -> np.ndarray:
+        f = np.empty(self._batch.n_robots, np.uint32)
+        _lib.check(_lib.LIB.mb_robot_flags(self._ctx, _lib.ptr(f)), self._ctx)
+        return f
+
+    def synchronize(self) -> None:
+        _lib.check(_lib.LIB.mb_synchronize(self._ctx), self._ctx)
+
+    @property
+    def stream(self) -> int:
+        return int(_lib.LIB.mb_get_stream(self._ctx) or 0)
+
+    def device_state(self):
+        p, v, s = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
+        _lib.check(_lib.LIB.mb_device_state(self._ctx, ctypes.byref(p), ctypes.byref(v),
+                                            ctypes.byref(s)), self._ctx)
+        return p.value, v.value, s.value
+
+    def launch_config(self) -> dict:
+        c = _lib.LaunchConfig()
+        _lib.check(_lib.LIB.mb_get_launch_config(self._ctx, ctypes.byref(c)), self._ctx)
+        return {f: getattr(c, f) for f, _ in c._fields_}
+
+    def set_launch_config(self, threads=0, springs_per_thread=0, masses_per_thread=0, bins=0,
+                          chunk=0, use_graph=1) -> None:
+        c = _lib.LaunchConfig(threads, springs_per_thread, masses_per_thread, bins, chunk, use_graph)
+        _lib.check(_lib.LIB.mb_set_launch_config(self._ctx, ctypes.byref(c)), self._ctx)
+
+
+def fitness(com: np.ndarray, base_com: np.ndarray, length: np.ndarray) -> np.ndarray:
+    """SoftBody::updateFitness (SoftBody.cpp:124-137): max((x - x0)/length, 0)."""
+    return np.maximum((com[:, 0] - base_com[:, 0]) / length, 0.0).astype(np.float32)
+
+
+def body_length(batch: Batch) -> np.ndarray:
+    """SoftBody::updateLength (SoftBody.cpp:98-110): max(|x_max - x_min|, 1)
+    over non-air masses, with both extremes starting at 0."""
+    out = np.ones(batch.n_robots, np.float32)
+    for r in range(batch.n_robots):
+        ms, _ = batch.robot_slices(r)
+        x = batch.pos[ms, 0][batch.mass_material[ms] != 0]
+        lo = min(0.0, float(x.min())) if x.size else 0.0
+        hi = max(0.0, float(x.max())) if x.size else 0.0
+        out[r] = max(abs(np.float32(hi) - np.float32(lo)), 1.0)
+    return out

@@ -1,0 +1,115 @@
+"""Python wrapper of the CPU oracle liboracle.so (mercury_oracle.c).
+
+Test infrastructure: the checker for the CUDA kernels, never the product.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "liboracle.so")
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} missing; run `make -C oracle oracle`")
+        L = ctypes.CDLL(LIB_PATH)
+        P, U32, I32, F32, F64 = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int, ctypes.c_float, ctypes.c_double
+        L.or_material_table.argtypes = [P]
+        L.or_material_table.restype = None
+        L.or_decode_id.argtypes = [U32]
+        L.or_decode_id.restype = I32
+        L.or_composite_id.argtypes = [I32, I32]
+        L.or_composite_id.restype = I32
+        L.or_step_count.argtypes = [F32, F32]
+        L.or_step_count.restype = U32
+        L.or_advance_clock.argtypes = [F32, F32, U32]
+        L.or_advance_clock.restype = F32
+        L.or_sin.argtypes = [F64]
+        L.or_sin.restype = F64
+        L.or_xpbd_run.argtypes = [I32, P, P, P, P, P, P, P, P, P, F32, F32, U32, I32, I32]
+        L.or_xpbd_run.restype = I32
+        L.or_xpbd_run_f64.argtypes = [I32, P, P, P, P, P, P, P, P, P, F64, F64, U32, I32]
+        L.or_xpbd_run_f64.restype = I32
+        L.or_com_device.argtypes = [I32, P, P, P, P]
+        L.or_com_device.restype = None
+        L.or_com_reference.argtypes = [I32, P, P, P, P]
+        L.or_com_reference.restype = None
+        L.or_max_threads.argtypes = []
+        L.or_max_threads.restype = I32
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data
+
+
+def material_table() -> np.ndarray:
+    t = np.zeros((254, 4), np.float32)
+    lib().or_material_table(_p(t))
+    return t
+
+
+def decode_id(enc: int) -> int:
+    return lib().or_decode_id(enc)
+
+
+def step_count(duration: float, dt: float) -> int:
+    return lib().or_step_count(duration, dt)
+
+
+def advance_clock(t0: float, dt: float, steps: int) -> float:
+    return lib().or_advance_clock(t0, dt, steps)
+
+
+def sin(x: float) -> float:
+    return lib().or_sin(x)
+
+
+def max_threads() -> int:
+    return lib().or_max_threads()
+
+
+def xpbd_run(batch, pos, vel, stress, table, dt, t0, steps, track, threads=0):
+    """Runs the FP32 restatement in place on pos/vel ((M,4) float32) and
+    stress ((S,) float32)."""
+    assert pos.dtype == np.float32 and pos.flags.c_contiguous
+    assert vel.dtype == np.float32 and vel.flags.c_contiguous
+    table = np.ascontiguousarray(table, np.float32)
+    rc = lib().or_xpbd_run(batch.n_robots, _p(batch.mass_offsets), _p(pos), _p(vel),
+                           _p(batch.spring_offsets), _p(batch.pairs), _p(batch.spring_material),
+                           _p(batch.lbar), _p(stress), _p(table), dt, t0, steps,
+                           int(bool(track)), threads)
+    assert rc == 0
+
+
+def xpbd_run_f64(batch, pos, vel, stress, table, dt, t0, steps, track):
+    assert pos.dtype == np.float64 and vel.dtype == np.float64
+    lbar = np.ascontiguousarray(batch.lbar, np.float64)
+    table = np.ascontiguousarray(table, np.float32)
+    rc = lib().or_xpbd_run_f64(batch.n_robots, _p(batch.mass_offsets), _p(pos), _p(vel),
+                               _p(batch.spring_offsets), _p(batch.pairs), _p(batch.spring_material),
+                               _p(lbar), _p(stress), _p(table), dt, t0, steps, int(bool(track)))
+    assert rc == 0
+
+
+def com_device(batch, pos) -> np.ndarray:
+    com = np.zeros((batch.n_robots, 3), np.float32)
+    lib().or_com_device(batch.n_robots, _p(batch.mass_offsets), _p(np.ascontiguousarray(pos, np.float32)),
+                        _p(batch.mass_material), _p(com))
+    return com
+
+
+def com_reference(batch, pos) -> np.ndarray:
+    com = np.zeros((batch.n_robots, 3), np.float32)
+    lib().or_com_reference(batch.n_robots, _p(batch.mass_offsets), _p(np.ascontiguousarray(pos, np.float32)),
+                           _p(batch.mass_material), _p(com))
+    return com

@@ -1,0 +1,439 @@
+/*
+ * CPU ORACLE -- test infrastructure, never shipped.
+ *
+ * A restatement of the reference's (DawsonCohen/Mercury) batched soft-body
+ * step, used by tests/, __graft_entry__.smoke() and the CPU-baseline leg of
+ * bench.py as the checker.  The product (mercury_b200/) never links it.
+ *
+ * Pinned by: the reference's own code run through oracle/ref_harness.cpp
+ * (material table, composite decode, lattice topology on the CPU; the CUDA
+ * step on the GPU), see tests/golden/.
+ *
+ * What follows the reference, and where:
+ *   material table .......... common/simulator/material.h:9-10, 111-133,
+ *                             192-227 (avg), 253-273 (id_lookup)
+ *   composite decode ........ material.h:275-322
+ *   step count / clock ...... common/simulator/Simulator.cu:428-449
+ *   XPBD step ............... common/simulator/sim_kernel.cu:141-153 (predict),
+ *                             166-253 (distance constraint), 255-269 (update)
+ *   centre of mass .......... common/evolvables/SoftBody.cpp:112-121
+ *
+ * The reference accumulates the per-mass corrections with shared-memory
+ * atomics, so its own summation order is unspecified and run-to-run
+ * non-deterministic.  This restatement fixes one order: for every mass, the
+ * corrections of its incident non-air springs are summed by the spring's
+ * other end (ascending), then spring index, the "a" end (+dp) of a spring
+ * before its "b" end (-dp).  The CUDA kernels use the same order, so kernel
+ * and oracle agree to the bit.
+ *
+ * Arithmetic choices (all IEEE-754 round-to-nearest, no contraction; build
+ * with -ffp-contract=off):
+ *   - sin of the actuation phase: the float phase fmaf(omega, t, phi) (nvcc
+ *     contracts the reference's omega*t+phi into one fma) is widened to
+ *     double, and sin is evaluated by Cody-Waite reduction by pi/2 and Taylor
+ *     polynomials (or_sin), then rounded to float.  The reference calls sinf
+ *     (or __sinf under -use_fast_math).
+ *   - |x| is sqrtf(fmaf(dx,dx, fmaf(dy,dy, dz*dz))); the reference calls
+ *     norm3df.
+ *   - the three divisions by (d + EPS) become one correctly rounded
+ *     reciprocal and multiplications; -C/K becomes -C * (1/K); lambda/Lbar
+ *     becomes lambda * (1/Lbar).
+ *   - the velocity update keeps the reference's double-precision expression
+ *     0.99*(x~ - x)/dt (sim_kernel.cu:265-267: 0.99 is a double literal).
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define OR_COMPOSITE_COUNT 254
+#define OR_BASE_COUNT 23
+#define OR_EPS 1e-12f
+
+/* ------------------------------------------------------------------ */
+/* Materials (material.h:111-133).  Each base material: k, dL0, omega, phi
+ * as the reference's constexpr initialisers evaluate them (double
+ * expressions narrowed to float). */
+static void base_material(int id, float* k, float* dl0, float* om, float* ph) {
+    const double PI = 3.14159265358979323846;
+    const double OMEGA = (double)(float)1.0f * (2.0f * PI); /* (float)1.0f*(2.0f*M_PI) */
+    const float AMP = .14f;
+    if (id == 0) { *k = 0; *dl0 = 0; *om = 0; *ph = 0; return; }
+    if (id >= 1 && id <= 20) {
+        int j = (id - 1) % 10; /* 0..9 */
+        int abductor = id >= 11;
+        *k = 50.0f; *dl0 = AMP;
+        if (j <= 7) {
+            /* phi = n*M_PI/8 with n = j (adductor) or 8 + j (abductor);
+             * 5*M_PI/4 etc. in the reference are the same doubles. */
+            *om = (float)OMEGA;
+            *ph = (float)((double)((abductor ? 8 : 0) + j) * PI / 8.0);
+        } else if (j == 8) {
+            *om = (float)(OMEGA * 2);
+            *ph = (float)(abductor ? PI : 0.0);
+        } else {
+            *om = (float)(OMEGA / 2);
+            *ph = (float)(abductor ? PI : 0.0);
+        }
+        return;
+    }
+    if (id == 21) { *k = 40.0f; *dl0 = 0.0f; *om = (float)OMEGA; *ph = 0.0f; return; }
+    /* id == 22 */
+    *k = 100.0f; *dl0 = 0.0f; *om = (float)OMEGA; *ph = 0.0f;
+}
+
+/* Composite id of a pair of base materials (material.h:192-213): ids 1..22
+ * for a base material with itself, then pairs (i<j) numbered from 23 in
+ * row-major order. */
+int or_composite_id(int m1, int m2) {
+    if (m1 == 0 || m2 == 0) return 0;
+    int i = m1 < m2 ? m1 - 1 : m2 - 1, j = m1 < m2 ? m2 - 1 : m1 - 1;
+    if (i == j) return i + 1;
+    int count = 23;
+    for (int a = 0; a < 22; ++a)
+        for (int b = a + 1; b < 22; ++b) {
+            if (a == i && b == j) return count;
+            ++count;
+        }
+    return -1;
+}
+
+/* id_lookup table (material.h:253-273): base materials at their ids, pair
+ * composites at or_composite_id with every field the double-precision mean
+ * of the two (material.h:215-227). */
+void or_material_table(float* out) {
+    memset(out, 0, sizeof(float) * 4 * OR_COMPOSITE_COUNT);
+    for (int i = 0; i < OR_BASE_COUNT; ++i)
+        base_material(i, &out[4 * i], &out[4 * i + 1], &out[4 * i + 2], &out[4 * i + 3]);
+    for (int i = 1; i < OR_BASE_COUNT; ++i)
+        for (int j = i + 1; j < OR_BASE_COUNT; ++j) {
+            float a[4], b[4];
+            base_material(i, &a[0], &a[1], &a[2], &a[3]);
+            base_material(j, &b[0], &b[1], &b[2], &b[3]);
+            int id = or_composite_id(i, j);
+            for (int c = 0; c < 4; ++c) out[4 * id + c] = (float)(((double)a[c] + (double)b[c]) / 2.0);
+        }
+}
+
+/* materials::decode(encoding).id (material.h:275-322): the lowest set bit
+ * selects the first material; bit 0 (air) anywhere below the second set bit
+ * gives air; otherwise the two lowest set bits form the composite. */
+int or_decode_id(uint32_t enc) {
+    int idx[2] = {0, 0}, count = 0;
+    for (int i = 0; i < 32; ++i)
+        if (enc & (1u << i)) {
+            idx[count++] = i;
+            if (i == 0 || count == 2) break;
+        }
+    if (idx[0] == 0) return 0;
+    if (idx[1] == 0) return idx[0];
+    return or_composite_id(idx[0], idx[1]);
+}
+
+/* ------------------------------------------------------------------ */
+/* Clock (Simulator.cu:428-449): steps taken by Simulate(duration) and the
+ * float clock after them. */
+uint32_t or_step_count(float duration, float dt) {
+    volatile float rem = duration;
+    uint32_t n = 0;
+    while (rem > 0.0f) { rem = rem - dt; ++n; }
+    return n;
+}
+
+float or_advance_clock(float t0, float dt, uint32_t steps) {
+    volatile float t = t0;
+    for (uint32_t i = 0; i < steps; ++i) t = t + dt;
+    return t;
+}
+
+/* ------------------------------------------------------------------ */
+/* sin(x) for |x| < 2^20: Cody & Waite (1980) reduction by pi/2 with a
+ * three-part constant, then the Taylor series of sin / cos on |r| <= pi/4
+ * evaluated by Horner's rule with fused multiply-adds.  The coefficients are
+ * (-1)^k/(2k+1)! and (-1)^k/(2k)!, rounded to double. */
+/* Values printed by oracle/sin_constants.py. */
+static const double OR_2_OVER_PI = 0.6366197723675814;
+static const double OR_PIO2_1 = 1.5707963267341256;  /* 33 bits of pi/2 */
+static const double OR_PIO2_2 = 6.077100506303966e-11;  /* next 33 bits   */
+static const double OR_PIO2_3 = 2.0222662487959506e-21;  /* remainder      */
+static const double OR_SIN_C[10] = {
+    1.0, -0.16666666666666666, 0.008333333333333333, -0.0001984126984126984, 2.7557319223985893e-06, -2.505210838544172e-08, 1.6059043836821613e-10, -7.647163731819816e-13, 2.8114572543455206e-15, -8.22063524662433e-18};
+static const double OR_COS_C[11] = {
+    1.0, -0.5, 0.041666666666666664, -0.001388888888888889, 2.48015873015873e-05, -2.755731922398589e-07, 2.08767569878681e-09, -1.1470745597729725e-11, 4.779477332387385e-14, -1.5619206968586225e-16, 4.110317623312165e-19};
+
+double or_sin(double x) {
+    double k = nearbyint(x * OR_2_OVER_PI);
+    double r = fma(-k, OR_PIO2_1, x);
+    r = fma(-k, OR_PIO2_2, r);
+    r = fma(-k, OR_PIO2_3, r);
+    long q = (long)k & 3;
+    double r2 = r * r, p;
+    if (q == 0 || q == 2) {
+        p = OR_SIN_C[9];
+        for (int i = 8; i >= 0; --i) p = fma(p, r2, OR_SIN_C[i]);
+        p = p * r;
+    } else {
+        p = OR_COS_C[10];
+        for (int i = 9; i >= 0; --i) p = fma(p, r2, OR_COS_C[i]);
+    }
+    return (q >= 2) ? -p : p;
+}
+
+/* ------------------------------------------------------------------ */
+/* Incidence entry h = 2*spring + (1 if this mass is the b end).  Returns 1
+ * if entry x sorts after entry y: key (other end, spring, end). */
+static int inc_after(int x, int y, const uint16_t* pairs) {
+    int sx = x >> 1, sy = y >> 1;
+    int ox = (x & 1) ? pairs[2 * sx] : pairs[2 * sx + 1];
+    int oy = (y & 1) ? pairs[2 * sy] : pairs[2 * sy + 1];
+    if (ox != oy) return ox > oy;
+    if (sx != sy) return sx > sy;
+    return (x & 1) > (y & 1);
+}
+
+/* ------------------------------------------------------------------ */
+/* One robot, FP32 reference semantics, `steps` steps from clock t0.
+ * pos/vel: float4 per mass (x, y, z, w); w of pos is the mass and is
+ * carried unchanged, w of vel is untouched.  stress: one float per spring,
+ * accumulated when track != 0.  Springs with material 0 (air) are skipped
+ * (sim_kernel.cu:211). */
+static void xpbd_robot_f32(int nm, float* pos, float* vel, int ns,
+                           const uint16_t* pairs, const uint8_t* mat,
+                           const float* lbar, float* stress,
+                           const float* table, float dt, float t0,
+                           uint32_t steps, int track) {
+    /* Incidence lists in ascending spring order: +dp at a, then -dp at b. */
+    int* deg = (int*)calloc((size_t)nm + 1, sizeof(int));
+    for (int s = 0; s < ns; ++s) {
+        if (!mat[s]) continue;
+        deg[pairs[2 * s] + 1]++;
+        deg[pairs[2 * s + 1] + 1]++;
+    }
+    for (int i = 0; i < nm; ++i) deg[i + 1] += deg[i];
+    int* inc = (int*)malloc(sizeof(int) * (size_t)(deg[nm] + 1));
+    int* fill = (int*)malloc(sizeof(int) * (size_t)(nm + 1));
+    memcpy(fill, deg, sizeof(int) * (size_t)nm);
+    for (int s = 0; s < ns; ++s) {
+        if (!mat[s]) continue;
+        inc[fill[pairs[2 * s]]++] = 2 * s;          /* even: +dp */
+        inc[fill[pairs[2 * s + 1]]++] = 2 * s + 1;  /* odd:  -dp */
+    }
+    /* Summation order of a mass: by the spring's other end, then spring
+     * index, then the a end before the b end (insertion sort per row). */
+    for (int i = 0; i < nm; ++i)
+        for (int e = deg[i] + 1; e < deg[i + 1]; ++e) {
+            int h = inc[e], k = e - 1;
+            while (k >= deg[i] && inc_after(inc[k], h, pairs)) { inc[k + 1] = inc[k]; --k; }
+            inc[k + 1] = h;
+        }
+    float* xt = (float*)malloc(sizeof(float) * 3 * (size_t)(nm + 1));
+    float* dp = (float*)malloc(sizeof(float) * 3 * (size_t)(ns + 1));
+    float rc[OR_COMPOSITE_COUNT], invK[OR_COMPOSITE_COUNT];
+    for (int m = 0; m < OR_COMPOSITE_COUNT; ++m) {
+        float k = table[4 * m];
+        float alpha = ((1.0f / k) / dt) / dt;
+        float K = 2.0f + alpha;
+        invK[m] = 1.0f / K;
+    }
+    volatile float t = t0;
+    for (uint32_t step = 0; step < steps; ++step) {
+        float tn = t;
+        for (int m = 0; m < OR_COMPOSITE_COUNT; ++m) {
+            float arg = fmaf(table[4 * m + 2], tn, table[4 * m + 3]);
+            float sn = (float)or_sin((double)arg);
+            rc[m] = table[4 * m + 1] * sn;
+        }
+        /* predict (sim_kernel.cu:147-152) */
+        for (int i = 0; i < nm; ++i)
+            for (int c = 0; c < 3; ++c) {
+                float dv = vel[4 * i + c] * dt;
+                xt[3 * i + c] = pos[4 * i + c] + dv;
+            }
+        /* distance constraints (sim_kernel.cu:209-243) */
+        for (int s = 0; s < ns; ++s) {
+            int m = mat[s];
+            if (!m) continue;
+            int a = pairs[2 * s], b = pairs[2 * s + 1];
+            float L = fmaf(lbar[s], rc[m], lbar[s]);
+            float dx = xt[3 * a] - xt[3 * b];
+            float dy = xt[3 * a + 1] - xt[3 * b + 1];
+            float dz = xt[3 * a + 2] - xt[3 * b + 2];
+            float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            float d = sqrtf(d2);
+            float r = 1.0f / (d + OR_EPS);
+            float C = d - L;
+            float lam = (-C) * invK[m];
+            float coef = lam * r;
+            dp[3 * s] = coef * dx;
+            dp[3 * s + 1] = coef * dy;
+            dp[3 * s + 2] = coef * dz;
+            if (track) {
+                float il = 1.0f / lbar[s];
+                stress[s] = stress[s] + lam * il;
+            }
+        }
+        /* gather + update (sim_kernel.cu:246-252, 261-268) */
+        for (int i = 0; i < nm; ++i) {
+            float acc[3] = {0.0f, 0.0f, 0.0f};
+            for (int e = deg[i]; e < deg[i + 1]; ++e) {
+                int h = inc[e], s = h >> 1;
+                for (int c = 0; c < 3; ++c)
+                    acc[c] = (h & 1) ? acc[c] - dp[3 * s + c] : acc[c] + dp[3 * s + c];
+            }
+            for (int c = 0; c < 3; ++c) {
+                float xn = xt[3 * i + c] + acc[c];
+                float diff = xn - pos[4 * i + c];
+                vel[4 * i + c] = (float)((0.99 * (double)diff) / (double)dt);
+                pos[4 * i + c] = xn;
+            }
+        }
+        t = t + dt;
+    }
+    free(deg); free(inc); free(fill); free(xt); free(dp);
+}
+
+/* Batch driver.  mass_off / spring_off: n_robots+1 offsets into the flat
+ * arrays; pairs are robot-local mass indices.  Robots are independent and
+ * are spread over `threads` OpenMP threads (0 = library default). */
+int or_xpbd_run(int n_robots, const int64_t* mass_off, float* pos, float* vel,
+                const int64_t* spring_off, const uint16_t* pairs,
+                const uint8_t* mat, const float* lbar, float* stress,
+                const float* table, float dt, float t0, uint32_t steps,
+                int track, int threads) {
+#ifdef _OPENMP
+    if (threads > 0) omp_set_num_threads(threads);
+#pragma omp parallel for schedule(dynamic, 1)
+#endif
+    for (int r = 0; r < n_robots; ++r) {
+        int64_t m0 = mass_off[r], s0 = spring_off[r];
+        xpbd_robot_f32((int)(mass_off[r + 1] - m0), pos + 4 * m0, vel + 4 * m0,
+                       (int)(spring_off[r + 1] - s0), pairs + 2 * s0, mat + s0,
+                       lbar + s0, stress ? stress + s0 : NULL, table, dt, t0,
+                       steps, track && stress);
+    }
+    return 0;
+}
+
+int or_max_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+/* ------------------------------------------------------------------ */
+/* FP64 transcription of the same step (libm sin and sqrt, true divisions),
+ * used to measure FP32 drift.  State in double, same layout as above. */
+static void xpbd_robot_f64(int nm, double* pos, double* vel, int ns,
+                           const uint16_t* pairs, const uint8_t* mat,
+                           const double* lbar, double* stress,
+                           const float* table, double dt, double t0,
+                           uint32_t steps, int track) {
+    double* xt = (double*)malloc(sizeof(double) * 3 * (size_t)(nm + 1));
+    double* acc = (double*)malloc(sizeof(double) * 3 * (size_t)(nm + 1));
+    for (uint32_t step = 0; step < steps; ++step) {
+        double tn = t0 + dt * (double)step;
+        for (int i = 0; i < nm; ++i)
+            for (int c = 0; c < 3; ++c) {
+                xt[3 * i + c] = pos[4 * i + c] + vel[4 * i + c] * dt;
+                acc[3 * i + c] = 0.0;
+            }
+        for (int s = 0; s < ns; ++s) {
+            int m = mat[s];
+            if (!m) continue;
+            int a = pairs[2 * s], b = pairs[2 * s + 1];
+            double k = table[4 * m], dl0 = table[4 * m + 1], om = table[4 * m + 2], ph = table[4 * m + 3];
+            double L = lbar[s] * (1.0 + dl0 * sin(om * tn + ph));
+            double dx = xt[3 * a] - xt[3 * b], dy = xt[3 * a + 1] - xt[3 * b + 1], dz = xt[3 * a + 2] - xt[3 * b + 2];
+            double d = sqrt(dx * dx + dy * dy + dz * dz);
+            double K = 2.0 + 1.0 / (k * dt * dt);
+            double lam = -(d - L) / K;
+            double inv = 1.0 / (d + 1e-12);
+            acc[3 * a] += lam * dx * inv; acc[3 * a + 1] += lam * dy * inv; acc[3 * a + 2] += lam * dz * inv;
+            acc[3 * b] -= lam * dx * inv; acc[3 * b + 1] -= lam * dy * inv; acc[3 * b + 2] -= lam * dz * inv;
+            if (track) stress[s] += lam / lbar[s];
+        }
+        for (int i = 0; i < nm; ++i)
+            for (int c = 0; c < 3; ++c) {
+                double xn = xt[3 * i + c] + acc[3 * i + c];
+                vel[4 * i + c] = 0.99 * (xn - pos[4 * i + c]) / dt;
+                pos[4 * i + c] = xn;
+            }
+    }
+    free(xt); free(acc);
+}
+
+int or_xpbd_run_f64(int n_robots, const int64_t* mass_off, double* pos, double* vel,
+                    const int64_t* spring_off, const uint16_t* pairs,
+                    const uint8_t* mat, const double* lbar, double* stress,
+                    const float* table, double dt, double t0, uint32_t steps,
+                    int track) {
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 1)
+#endif
+    for (int r = 0; r < n_robots; ++r) {
+        int64_t m0 = mass_off[r], s0 = spring_off[r];
+        xpbd_robot_f64((int)(mass_off[r + 1] - m0), pos + 4 * m0, vel + 4 * m0,
+                       (int)(spring_off[r + 1] - s0), pairs + 2 * s0, mat + s0,
+                       lbar + s0, stress ? stress + s0 : NULL, table, dt, t0,
+                       steps, track && stress);
+    }
+    return 0;
+}
+
+/* ------------------------------------------------------------------ */
+/* Centre of mass of the non-air masses of each robot.
+ *
+ * or_com_device: the fixed reduction order of the CUDA kernels -- 32 lanes,
+ * lane l sums masses l, l+32, ... in double, then an xor butterfly over
+ * offsets 16, 8, 4, 2, 1; mean = sum / count, rounded to float.
+ *
+ * or_com_reference: SoftBody::updateCOM (SoftBody.cpp:112-121), a float
+ * running mean mean += (p - mean) / (i + 1). */
+void or_com_device(int n_robots, const int64_t* mass_off, const float* pos,
+                   const uint8_t* mass_mat, float* com) {
+    for (int r = 0; r < n_robots; ++r) {
+        for (int c = 0; c < 3; ++c) {
+            double lane[32];
+            long cnt[32];
+            for (int l = 0; l < 32; ++l) { lane[l] = 0.0; cnt[l] = 0; }
+            int64_t n = mass_off[r + 1] - mass_off[r];
+            for (int64_t i = 0; i < n; ++i) {
+                int64_t g = mass_off[r] + i;
+                if (!mass_mat[g]) continue;
+                lane[i & 31] += (double)pos[4 * g + c];
+                cnt[i & 31] += 1;
+            }
+            for (int off = 16; off >= 1; off >>= 1) {
+                double nl[32];
+                long nc[32];
+                for (int l = 0; l < 32; ++l) { nl[l] = lane[l] + lane[l ^ off]; nc[l] = cnt[l] + cnt[l ^ off]; }
+                for (int l = 0; l < 32; ++l) { lane[l] = nl[l]; cnt[l] = nc[l]; }
+            }
+            com[3 * r + c] = cnt[0] ? (float)(lane[0] / (double)cnt[0]) : 0.0f;
+        }
+    }
+}
+
+void or_com_reference(int n_robots, const int64_t* mass_off, const float* pos,
+                      const uint8_t* mass_mat, float* com) {
+    for (int r = 0; r < n_robots; ++r) {
+        float mean[3] = {0.0f, 0.0f, 0.0f};
+        volatile float i = 0.0f;
+        for (int64_t g = mass_off[r]; g < mass_off[r + 1]; ++g) {
+            if (!mass_mat[g]) continue;
+            float den = i + 1.0f;
+            for (int c = 0; c < 3; ++c) {
+                float d = (pos[4 * g + c] - mean[c]) * 1.0f;
+                mean[c] = mean[c] + d / den;
+            }
+            i = i + 1.0f;
+        }
+        for (int c = 0; c < 3; ++c) com[3 * r + c] = mean[c];
+    }
+}
