@@ -30,6 +30,14 @@
 extern "C" {
 #endif
 
+/* Only the entry points below are exported; the library is built with
+ * hidden default visibility. */
+#if defined(__GNUC__)
+#define MB_API __attribute__((visibility("default")))
+#else
+#define MB_API
+#endif
+
 #define MB_COMPOSITE_COUNT 254 /* material.h:106 COMPOSITE_COUNT = 22*23/2 + 1 */
 
 typedef struct mb_context mb_context;
@@ -74,81 +82,81 @@ typedef struct mb_launch_config {
 
 /* Creates a context on CUDA device `device` with its own stream.
  * Replaces Simulator::Simulator / Initialize (Simulator.cu:103-109). */
-mb_status mb_context_create(int device, mb_context** out);
+MB_API mb_status mb_context_create(int device, mb_context** out);
 
 /* Frees every device and host buffer of the context.
  * Replaces Simulator::~Simulator / freeMemory (Simulator.cu:45-101). */
-void mb_context_destroy(mb_context* ctx);
+MB_API void mb_context_destroy(mb_context* ctx);
 
 /* Message of the last failed call on this context (never NULL). */
-const char* mb_last_error(const mb_context* ctx);
+MB_API const char* mb_last_error(const mb_context* ctx);
 
 /* Composite material table, MB_COMPOSITE_COUNT float4 {k, dL0, omega, phi}
  * indexed by composite id.  Replaces setCompositeMats_id
  * (softbodysystem.h:65, sim_kernel.cu:58-60). */
-mb_status mb_set_materials(mb_context* ctx, const float* table);
+MB_API mb_status mb_set_materials(mb_context* ctx, const float* table);
 
 /* Time step and accumulated clock.  Replace Simulator::setTimeStep,
  * getDeltaT, getTotalTime and Reset (Simulator.h:42-48). */
-mb_status mb_set_time_step(mb_context* ctx, float dt);
-float mb_get_time_step(const mb_context* ctx);
-mb_status mb_set_total_time(mb_context* ctx, float t);
-float mb_get_total_time(const mb_context* ctx);
+MB_API mb_status mb_set_time_step(mb_context* ctx, float dt);
+MB_API float mb_get_time_step(const mb_context* ctx);
+MB_API mb_status mb_set_total_time(mb_context* ctx, float t);
+MB_API float mb_get_total_time(const mb_context* ctx);
 
 /* Step semantics.  Replaces the fixed kernel set of integrateBodies
  * (sim_kernel.cu:271-325). */
-mb_status mb_set_mode(mb_context* ctx, mb_mode mode);
+MB_API mb_status mb_set_mode(mb_context* ctx, mb_mode mode);
 
 /* Uploads a population: packs it into bins, builds the per-mass incidence
  * lists, copies everything to the device and zeroes the spring stresses.
  * Robots may differ in mass and spring count.  Replaces
  * Simulator::SetElements / AllocateElement (Simulator.cu:206-367, 460-529)
  * and the kernel-side part of setSimOpts (sim_kernel.cu:62-64). */
-mb_status mb_set_elements(mb_context* ctx, const mb_batch_desc* batch);
+MB_API mb_status mb_set_elements(mb_context* ctx, const mb_batch_desc* batch);
 
 /* Replaces the uploaded positions and velocities (same robots, same
  * layout) without repacking the topology.  Stresses are kept. */
-mb_status mb_set_state(mb_context* ctx, const float* pos, const float* vel);
+MB_API mb_status mb_set_state(mb_context* ctx, const float* pos, const float* vel);
 
 /* Runs the step loop for `duration` seconds of simulated time: the number of
  * steps and the clock follow the reference's float accumulation
  * (Simulator.cu:428-449).  Replaces Simulator::Simulate (Simulator.cu:369-458)
  * and integrateBodies (sim_kernel.cu:271-325).  Asynchronous on the
  * context's stream; *steps_taken may be NULL. */
-mb_status mb_simulate(mb_context* ctx, float duration, int track_stresses,
+MB_API mb_status mb_simulate(mb_context* ctx, float duration, int track_stresses,
                       uint32_t* steps_taken);
 
 /* Runs exactly `steps` steps from the current clock. */
-mb_status mb_run_steps(mb_context* ctx, uint32_t steps, int track_stresses);
+MB_API mb_status mb_run_steps(mb_context* ctx, uint32_t steps, int track_stresses);
 
 /* Copies the state back to host arrays in the upload layout (pos, vel: 4
  * floats per mass; stress: 1 per spring; any may be NULL).  Synchronous.
  * Replaces Simulator::Collect (Simulator.cu:537-580). */
-mb_status mb_collect(mb_context* ctx, float* pos, float* vel, float* stress);
+MB_API mb_status mb_collect(mb_context* ctx, float* pos, float* vel, float* stress);
 
 /* Centre of mass of the non-air masses of every robot (3 floats per robot),
  * reduced on the device.  Synchronous.  Replaces the host-side
  * SoftBody::updateCOM after Collect (SoftBody.cpp:112-121). */
-mb_status mb_centre_of_mass(mb_context* ctx, float* com);
+MB_API mb_status mb_centre_of_mass(mb_context* ctx, float* com);
 
 /* Per-robot status after the last run: bit 0 = a position became NaN/Inf.
  * Synchronous.  The reference asserts on NaN in Collect (Simulator.cu:550). */
-mb_status mb_robot_flags(mb_context* ctx, uint32_t* flags);
+MB_API mb_status mb_robot_flags(mb_context* ctx, uint32_t* flags);
 
 /* Waits for all work on the context's stream. */
-mb_status mb_synchronize(mb_context* ctx);
+MB_API mb_status mb_synchronize(mb_context* ctx);
 
 /* The stream the context launches on (a cudaStream_t). */
-void* mb_get_stream(const mb_context* ctx);
+MB_API void* mb_get_stream(const mb_context* ctx);
 
 /* Device addresses of the state arrays in the upload layout, for callers
  * that keep inputs resident on the device. */
-mb_status mb_device_state(mb_context* ctx, void** pos, void** vel, void** stress);
+MB_API mb_status mb_device_state(mb_context* ctx, void** pos, void** vel, void** stress);
 
 /* Launch configuration: read, override (0 fields keep the automatic
  * choice), and the automatic choice for the uploaded batch. */
-mb_status mb_get_launch_config(const mb_context* ctx, mb_launch_config* cfg);
-mb_status mb_set_launch_config(mb_context* ctx, const mb_launch_config* cfg);
+MB_API mb_status mb_get_launch_config(const mb_context* ctx, mb_launch_config* cfg);
+MB_API mb_status mb_set_launch_config(mb_context* ctx, const mb_launch_config* cfg);
 
 /* Builds a voxel-lattice robot (one mass per grid point, 13 forward lattice
  * springs per point, largest 6-connected component kept, shifted so that
@@ -156,13 +164,13 @@ mb_status mb_set_launch_config(mb_context* ctx, const mb_launch_config* cfg);
  * material mats[i].  Output buffers hold nx*ny*nz masses (pos: 3 floats) and
  * 13*nx*ny*nz springs.  Replaces VoxelRobot::Build (VoxelRobot.cpp:310-331).
  * Host only. */
-mb_status mb_voxel_build(int nx, int ny, int nz, float h, const uint8_t* mats,
+MB_API mb_status mb_voxel_build(int nx, int ny, int nz, float h, const uint8_t* mats,
                          int* n_masses, int* n_springs, float* pos,
                          uint8_t* mass_material, uint16_t* pairs, float* lbar,
                          uint8_t* spring_material);
 
 /* Library version string. */
-const char* mb_version(void);
+MB_API const char* mb_version(void);
 
 #ifdef __cplusplus
 }

@@ -16,7 +16,7 @@ DEPS = SRC + [os.path.join(HERE, "csrc", f) for f in ("mb_internal.h", "mb_sin.c
 OUT = os.path.join(HERE, "libmercury_b200.so")
 NVCC = os.environ.get("NVCC", "nvcc")
 FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-gencode", "arch=compute_100a,code=sm_100a",
-         "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall", "-shared"]
+         "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall", "-Xcompiler", "-fvisibility=hidden", "-shared"]
 
 
 def up_to_date() -> bool:

@@ -19,6 +19,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -26,6 +27,10 @@
 #include <vector>
 
 #include <cuda_runtime.h>
+#include <execinfo.h>
+#include <signal.h>
+#include <sys/syscall.h>
+#include <unistd.h>
 
 #include "../../include/mercury_b200.h"
 #include "mb_internal.h"
@@ -153,6 +158,46 @@ mb_status fail(mb_context* c, mb_status s, const char* fmt, ...) {
     if (c) c->err = buf;
     return s;
 }
+
+// Stage log on stderr when MB_TRACE is set (diagnostics of host crashes).
+bool trace_on() {
+    static const bool on = std::getenv("MB_TRACE") != nullptr;
+    return on;
+}
+#define MB_TRACE(...)                                   \
+    do {                                                \
+        if (trace_on()) {                               \
+            std::fprintf(stderr, "[mb] " __VA_ARGS__);  \
+            std::fputc('\n', stderr);                   \
+            std::fflush(stderr);                        \
+        }                                               \
+    } while (0)
+
+// Under MB_TRACE: on SIGSEGV print the faulting address, thread and native
+// backtrace to stderr, then re-raise with the default action.
+void segv_report(int sig, siginfo_t* si, void*) {
+    char buf[160];
+    int n = std::snprintf(buf, sizeof(buf), "[mb] signal %d at address %p in thread %ld\n", sig,
+                          si ? si->si_addr : nullptr, (long)syscall(SYS_gettid));
+    if (n > 0) (void)!write(2, buf, (size_t)n);
+    void* frames[64];
+    int k = backtrace(frames, 64);
+    backtrace_symbols_fd(frames, k, 2);
+    signal(sig, SIG_DFL);
+    raise(sig);
+}
+
+struct SegvReporter {
+    SegvReporter() {
+        if (!std::getenv("MB_TRACE")) return;
+        struct sigaction sa;
+        std::memset(&sa, 0, sizeof(sa));
+        sa.sa_sigaction = segv_report;
+        sa.sa_flags = SA_SIGINFO;
+        sigaction(SIGSEGV, &sa, nullptr);
+    }
+};
+const SegvReporter kSegvReporter;
 
 mb_status cuda_fail(mb_context* c, cudaError_t e, const char* what) {
     return fail(c, MB_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
@@ -591,7 +636,10 @@ mb_status mb_set_state(mb_context* ctx, const float* pos, const float* vel) {
     return MB_OK;
 }
 
-namespace {
+}  // extern "C"
+
+// Internal helpers: C++ linkage, internal to this file.
+namespace mb_detail {
 
 mb::StepParams make_params(mb_context* c, float t0, uint32_t steps, bool track) {
     mb::StepParams p{};
@@ -632,11 +680,20 @@ cudaError_t issue_chunks(mb_context* c, float t0, uint32_t steps, bool track) {
     while (done < steps) {
         const uint32_t n = std::min(c->chunk, steps - done);
         mb::StepParams p = make_params(c, t, n, track);
+        MB_TRACE("launch bins=%u threads=%u spt=%u mpt=%u smem=%u steps=%u", p.n_bins, c->shape.threads,
+                 c->shape.spt, c->shape.mpt, p.smem_bytes, n);
         cudaError_t e = mb::launch_step(p, c->shape, c->stream);
+        MB_TRACE("launch returned %d", (int)e);
+        if (trace_on() && std::getenv("MB_SYNC")) {
+            cudaError_t es = cudaStreamSynchronize(c->stream);
+            MB_TRACE("sync after launch: %d %s", (int)es, cudaGetErrorString(es));
+        }
         if (e != cudaSuccess) return e;
         t = advance(t, c->dt, n);
         done += n;
+        MB_TRACE("chunk done");
     }
+    MB_TRACE("chunks issued");
     return cudaSuccess;
 }
 
@@ -653,11 +710,14 @@ mb_status run(mb_context* c, uint32_t steps, bool track) {
         if (it == c->graphs.end()) {
             if (c->graphs.size() >= 16) c->clear_graphs();
             // kernel attributes cannot change inside a capture
+            MB_TRACE("prepare");
             MB_CUDA(c, mb::prepare_step(c->shape, track, c->smem_bytes));
             cudaGraph_t g;
+            MB_TRACE("begin capture");
             MB_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
             cudaError_t e = issue_chunks(c, t0, steps, track);
             cudaError_t e2 = cudaStreamEndCapture(c->stream, &g);
+            MB_TRACE("end capture %d %d", (int)e, (int)e2);
             if (e != cudaSuccess) {
                 if (e2 == cudaSuccess) cudaGraphDestroy(g);
                 return cuda_fail(c, e, "capture of step launches");
@@ -665,25 +725,31 @@ mb_status run(mb_context* c, uint32_t steps, bool track) {
             if (e2 != cudaSuccess) return cuda_fail(c, e2, "cudaStreamEndCapture");
             cudaGraphExec_t ex;
             cudaError_t e3 = cudaGraphInstantiate(&ex, g, 0);
+            MB_TRACE("instantiate %d", (int)e3);
             cudaGraphDestroy(g);
             if (e3 != cudaSuccess) return cuda_fail(c, e3, "cudaGraphInstantiate");
             it = c->graphs.emplace(key, ex).first;
         }
         MB_CUDA(c, cudaGraphLaunch(it->second, c->stream));
+        MB_TRACE("graph launched");
     } else {
+        MB_TRACE("prepare (no graph)");
         MB_CUDA(c, mb::prepare_step(c->shape, track, c->smem_bytes));
         cudaError_t e = issue_chunks(c, t0, steps, track);
         if (e != cudaSuccess) return cuda_fail(c, e, "step launch");
     }
     c->total_time = advance(t0, c->dt, steps);
+    MB_TRACE("run returns");
     return MB_OK;
 }
 
-}  // namespace
+}  // namespace mb_detail
+
+extern "C" {
 
 mb_status mb_run_steps(mb_context* ctx, uint32_t steps, int track_stresses) {
     if (!ctx) return MB_ERR_ARGUMENT;
-    return run(ctx, steps, track_stresses != 0);
+    return mb_detail::run(ctx, steps, track_stresses != 0);
 }
 
 mb_status mb_simulate(mb_context* ctx, float duration, int track_stresses, uint32_t* steps_taken) {
@@ -698,7 +764,7 @@ mb_status mb_simulate(mb_context* ctx, float duration, int track_stresses, uint3
         if (n == 0xFFFFFFFFu) return fail(ctx, MB_ERR_ARGUMENT, "too many steps");
     }
     if (steps_taken) *steps_taken = n;
-    return run(ctx, n, track_stresses != 0);
+    return mb_detail::run(ctx, n, track_stresses != 0);
 }
 
 mb_status mb_collect(mb_context* ctx, float* pos, float* vel, float* stress) {
@@ -719,6 +785,7 @@ mb_status mb_centre_of_mass(mb_context* ctx, float* com) {
     if (!ctx || !com) return fail(ctx, MB_ERR_ARGUMENT, "null argument");
     if (!ctx->loaded) return fail(ctx, MB_ERR_STATE, "no population uploaded");
     cudaSetDevice(ctx->device);
+    MB_TRACE("com launch robots=%u", ctx->n_robots);
     MB_CUDA(ctx, mb::launch_com(ctx->pos.p, ctx->mass_mat.p, ctx->d_mass_off.p, ctx->n_robots,
                                 ctx->com.p, ctx->stream));
     MB_CUDA(ctx, cudaMemcpyAsync(com, ctx->com.p, 3 * sizeof(float) * ctx->n_robots,
