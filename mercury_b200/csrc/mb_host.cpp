@@ -544,10 +544,22 @@ mb_status mb_set_elements(mb_context* ctx, const mb_batch_desc* b) {
         if (max_s > cap_s || max_m > cap_m) continue;
         uint32_t nb = ctx->override_cfg.bins;
         const bool fixed = nb != 0;
+        // One wave = SMs x resident CTAs per SM (registers usually limit it;
+        // shared memory is estimated at the even share of the population).
+        uint32_t wave = sms;
         if (!nb) {
             const uint64_t need = std::max<uint64_t>((tot_s + cap_s - 1) / cap_s, (tot_m + cap_m - 1) / cap_m);
             nb = (uint32_t)std::max<uint64_t>(need, 1);
-            if (R >= sms) nb = std::max<uint32_t>(nb, sms);  // one bin per SM at least
+            if (R >= sms) {
+                const uint32_t est_smem = std::min<uint32_t>(
+                    smem_cap, mb::bin_smem_bytes((uint32_t)std::min<uint64_t>(cap_m, tot_m / sms + 1),
+                                                 (uint32_t)std::min<uint64_t>(cap_s, tot_s / sms + 1),
+                                                 (uint32_t)std::min<uint64_t>(3 * cap_s, 3 * (tot_s / sms + 1))));
+                const int per_sm = std::max(1, mb::ctas_per_sm(sh, false, est_smem));
+                wave = sms * (uint32_t)per_sm;
+                nb = std::max<uint32_t>(nb, wave);
+                nb = (nb + wave - 1) / wave * wave;  // whole waves
+            }
             nb = std::min<uint32_t>(nb, R);
         }
         for (uint32_t tries = 0; tries < 16; ++tries) {
@@ -559,7 +571,7 @@ mb_status mb_set_elements(mb_context* ctx, const mb_batch_desc* b) {
                 }
             }
             if (fixed || nb >= R) break;
-            nb = std::min<uint32_t>(R, nb + sms);
+            nb = std::min<uint32_t>(R, nb + wave);
         }
         if (ok) {
             ctx->shape = sh;

@@ -66,6 +66,10 @@ cudaError_t prepare_step(const KernelShape& shape, bool track, uint32_t smem_byt
 // Launches the step kernel for `p.steps` steps.  Returns a CUDA error.
 cudaError_t launch_step(const StepParams& p, const KernelShape& shape, cudaStream_t s);
 
+// Resident CTAs per SM of a kernel variant with `smem_bytes` of dynamic
+// shared memory (0 if the shape is not compiled or does not fit).
+int ctas_per_sm(const KernelShape& shape, bool track, uint32_t smem_bytes);
+
 // Shared memory a bin needs, in bytes.
 uint32_t bin_smem_bytes(uint32_t n_mass, uint32_t n_spring, uint32_t n_inc);
 

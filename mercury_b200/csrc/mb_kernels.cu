@@ -312,6 +312,18 @@ cudaError_t prepare_step(const KernelShape& shape, bool track, uint32_t smem_byt
                                 (int)smem_bytes);
 }
 
+int ctas_per_sm(const KernelShape& shape, bool track, uint32_t smem_bytes) {
+    const ShapeEntry* e = find_shape(shape);
+    if (!e) return 0;
+    StepFn fn = e->fn[track ? 1 : 0];
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes) != cudaSuccess)
+        return 0;
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, (int)shape.threads, smem_bytes) != cudaSuccess)
+        return 0;
+    return n;
+}
+
 cudaError_t launch_step(const StepParams& p, const KernelShape& shape, cudaStream_t s) {
     const ShapeEntry* e = find_shape(shape);
     if (!e) return cudaErrorInvalidValue;
