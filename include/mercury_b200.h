@@ -169,6 +169,45 @@ MB_API mb_status mb_voxel_build(int nx, int ny, int nz, float h, const uint8_t* 
                          uint8_t* mass_material, uint16_t* pairs, float* lbar,
                          uint8_t* spring_material);
 
+/* ----------------------------------------------------------------------
+ * Entry point that allocates nothing.  It has no counterpart in the
+ * reference; it exists for callers that cannot call cudaMalloc -- an engine
+ * that owns every device allocation through its own pool, or a plugin host
+ * with a fixed memory budget.
+ *
+ * Runs `steps` steps of the reference step on ONE robot whose arrays are
+ * already on the current device (device pointers; layouts as in
+ * mb_batch_desc: pos/vel 4 floats per mass, pairs 2 per spring, stress 1
+ * per spring, table MB_COMPOSITE_COUNT float4), starting from clock t0, on
+ * `stream` (a cudaStream_t; NULL = the legacy default stream).  pos, vel and
+ * stress (when track_stresses != 0) are updated in place; *t_end (may be
+ * NULL) receives the float clock after the last step.  Results are bit for
+ * bit those of mb_set_elements + mb_run_steps on the same robot.
+ *
+ * Limits: n_masses <= MB_NOALLOC_MAX_MASSES, n_springs <=
+ * MB_NOALLOC_MAX_SPRINGS, and at most MB_NOALLOC_MAX_INCIDENCE incidence
+ * entries (32 x the longest per-mass row of each group of 32 masses);
+ * larger robots return MB_ERR_CAPACITY.  The packed topology is built on the
+ * device in one scratch array of about 300 KB that is part of the library
+ * image: every GPU that loads the library holds it until the process exits.
+ * The call calls no cudaMalloc, cudaFree or other allocating routine.
+ *
+ * The first call on a device looks up the scratch array's device address;
+ * make that first call before any stream capture.  Every call shares the
+ * scratch array and keeps the last call's contents, so calls that overlap on
+ * the GPU (different streams or host threads) race: serialise them.  The
+ * call synchronises `stream` to read its status. */
+#define MB_NOALLOC_MAX_MASSES 2048
+#define MB_NOALLOC_MAX_SPRINGS 8192
+#define MB_NOALLOC_MAX_INCIDENCE 26624
+MB_API mb_status mb_simulate_robot_noalloc(void* stream, const float* table,
+                                           uint32_t n_masses, float* pos, float* vel,
+                                           uint32_t n_springs, const uint16_t* pairs,
+                                           const uint8_t* spring_material,
+                                           const float* lbar, float* stress, float dt,
+                                           float t0, uint32_t steps, int track_stresses,
+                                           float* t_end);
+
 /* Library version string. */
 MB_API const char* mb_version(void);
 
