@@ -129,3 +129,34 @@ def test_com_device_order_close_to_reference_running_mean():
     a = core.com_device(b, b.pos)
     r = core.com_reference(b, b.pos)
     assert np.allclose(a, r, atol=1e-6)
+
+
+def _golden_cases(golden_dir):
+    g = np.load(os.path.join(golden_dir, "ref_sim.npz"))
+    for i in range(int(g["n_cases"])):
+        yield {k: g[f"c{i}_{k}"] for k in ("flavour", "dt", "duration", "steps", "total_time", "pos", "vel", "stress")}
+
+
+def test_oracle_matches_reference_cuda_fixture(golden_dir):
+    """The oracle against the reference's own CUDA step (both builds), run on
+    a B200 by tests/golden/make_fixtures.py: same step count and clock, and
+    positions within 2e-4 x body length."""
+    import mercury_b200 as mb
+    from mercury_b200 import robots
+    b = robots.population_batch("small", 8)
+    length = mb.body_length(b)
+    table = mb.material_table()
+    for c in _golden_cases(golden_dir):
+        dt, dur = float(c["dt"]), float(c["duration"])
+        n = core.step_count(dur, dt)
+        assert n == int(c["steps"])
+        assert core.advance_clock(0.0, dt, n) == float(c["total_time"])
+        p, v = b.pos.copy(), b.vel.copy()
+        s = np.zeros(b.n_springs, np.float32)
+        core.xpbd_run(b, p, v, s, table, dt, 0.0, n, True)
+        for r in range(b.n_robots):
+            ms, ss = b.robot_slices(r)
+            dx = np.abs(p[ms, :3] - c["pos"][ms]).max() / length[r]
+            assert dx < 2e-4, (c["flavour"], dt, r, dx)
+        rel = np.abs(s - c["stress"]).max() / max(np.abs(c["stress"]).max(), 1e-12)
+        assert rel < 1e-2, (c["flavour"], dt, rel)
