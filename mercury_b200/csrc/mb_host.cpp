@@ -129,9 +129,13 @@ struct mb_context {
     mb::DevBuf<int64_t> d_mass_off;
     mb::DevBuf<float4> d_table;
     mb::DevBuf<mb::BinDesc> bins;
-    mb::DevBuf<uint32_t> mass_gidx, spring_gidx, spring_pair, slice_off, slice_width, inc;
+    mb::DevBuf<uint32_t> mass_gidx, spring_gidx, spring_pair, slice_off, slice_width;
+    mb::DevBuf<uint16_t> inc;
     mb::DevBuf<float> spring_lbar;
-    mb::DevBuf<uint8_t> mat_ids;
+    mb::DevBuf<uint8_t> mat_ids;           // composite ids used by the population
+    mb::DevBuf<uint32_t> n_mat;            // their count (device scalar)
+    mb::DevBuf<float> rates, invk;         // actuation table of one launch; 1/K per material
+    uint32_t n_mat_host = 0;
     mb::DevBuf<uint32_t> bin_flags, robot_bin, robot_flags;
     mb::DevBuf<float> com;
 
@@ -214,10 +218,11 @@ struct RobotPack {
     std::vector<uint32_t> springs;  // original local spring index, packed order
 };
 
-// Shapes the automatic choice considers, most springs per CTA first.
+// Shapes the automatic choice considers, in order of preference: 32 warps
+// per SM with about 8-10 springs per thread first.
 const mb::KernelShape kAuto[] = {
-    {512, 16, 4}, {1024, 8, 2}, {512, 8, 2}, {256, 16, 4}, {256, 8, 2}, {1024, 4, 1},
-    {512, 4, 1}, {256, 4, 1},
+    {1024, 10, 2}, {1024, 12, 2}, {1024, 8, 2}, {512, 16, 4}, {512, 12, 2}, {512, 8, 2},
+    {1024, 6, 2},  {1024, 4, 1},  {512, 4, 1},  {256, 16, 4}, {256, 8, 2},
 };
 
 struct BinPlan {
@@ -236,7 +241,7 @@ bool plan_bins(const std::vector<uint64_t>& cost, const std::vector<uint32_t>& n
                      [&](uint32_t a, uint32_t b) { return cost[a] > cost[b]; });
     std::vector<uint64_t> load(nb, 0), bm(nb, 0), bs(nb, 0), bi(nb, 0);
     plan.robots.assign(nb, {});
-    const uint64_t cap_s = (uint64_t)sh.threads * sh.spt;
+    const uint64_t cap_s = std::min<uint64_t>((uint64_t)sh.threads * sh.spt, mb::kMaxBinSprings);
     const uint64_t cap_m = std::min<uint64_t>((uint64_t)sh.threads * sh.mpt, 4096);
     for (uint32_t r : order) {
         // least loaded bin that still has room
@@ -355,7 +360,13 @@ mb_status mb_set_launch_config(mb_context* ctx, const mb_launch_config* cfg) {
                         s.spt, s.mpt);
     }
     ctx->override_cfg = *cfg;
-    if (cfg->chunk) ctx->chunk = cfg->chunk;
+    if (cfg->chunk) {
+        ctx->chunk = cfg->chunk;
+        if (ctx->loaded) {
+            cudaSetDevice(ctx->device);
+            MB_CUDA(ctx, ctx->rates.alloc((size_t)std::max<uint32_t>(ctx->n_mat_host, 1) * ctx->chunk));
+        }
+    }
     ctx->use_graph = cfg->use_graph != 0;
     ctx->clear_graphs();
     return MB_OK;
@@ -445,7 +456,8 @@ mb_status mb_set_elements(mb_context* ctx, const mb_batch_desc* b) {
     // padded to the wider robot, so the estimate is not exact).
     struct Built {
         std::vector<mb::BinDesc> bins;
-        std::vector<uint32_t> mass_gidx, spring_gidx, pair, slice_off, slice_width, inc, robot_bin;
+        std::vector<uint32_t> mass_gidx, spring_gidx, pair, slice_off, slice_width, robot_bin;
+        std::vector<uint16_t> inc;
         std::vector<float> lbar;
         std::vector<uint8_t> mat_ids;
         uint32_t max_smem = 0;
@@ -456,6 +468,15 @@ mb_status mb_set_elements(mb_context* ctx, const mb_batch_desc* b) {
         out.robot_bin.resize(R);
         out.mass_gidx.reserve(M);
         out.spring_gidx.reserve(S);
+        // material slots: the composite ids used by the whole population
+        std::vector<int> slot_of(MB_COMPOSITE_COUNT, -1);
+        for (uint32_t r = 0; r < R; ++r)
+            for (uint32_t ls : packs[r].springs) slot_of[b->spring_material[b->spring_offsets[r] + ls]] = 0;
+        for (int m = 0; m < MB_COMPOSITE_COUNT; ++m)
+            if (slot_of[m] == 0) {
+                slot_of[m] = (int)out.mat_ids.size();
+                out.mat_ids.push_back((uint8_t)m);
+            }
         for (uint32_t bi = 0; bi < nb; ++bi) {
             mb::BinDesc& d = out.bins[bi];
             std::memset(&d, 0, sizeof(d));
@@ -463,22 +484,7 @@ mb_status mb_set_elements(mb_context* ctx, const mb_batch_desc* b) {
             d.spring_begin = (uint32_t)out.spring_gidx.size();
             d.inc_begin = (uint32_t)out.inc.size();
             d.slice_begin = (uint32_t)out.slice_off.size();
-            d.mat_begin = (uint32_t)out.mat_ids.size();
-            // material slots of the bin, ascending composite id
-            std::vector<int> slot(MB_COMPOSITE_COUNT, -1);
-            std::vector<uint8_t> used;
-            for (uint32_t r : plan.robots[bi])
-                for (uint32_t ls : packs[r].springs) {
-                    const uint8_t m = b->spring_material[b->spring_offsets[r] + ls];
-                    if (slot[m] < 0) {
-                        slot[m] = 0;
-                        used.push_back(m);
-                    }
-                }
-            std::sort(used.begin(), used.end());
-            for (size_t i = 0; i < used.size(); ++i) slot[used[i]] = (int)i;
-            for (uint8_t m : used) out.mat_ids.push_back(m);
-            d.n_mat = (uint32_t)used.size();
+            (void)slot_of;
             struct Ent {
                 uint32_t other, orig, sign, packed;
             };
@@ -495,7 +501,7 @@ mb_status mb_set_elements(mb_context* ctx, const mb_batch_desc* b) {
                     const uint32_t a = b->pairs[2 * g], c = b->pairs[2 * g + 1];
                     const uint32_t pa = mbase + a, pc = mbase + c;
                     out.spring_gidx.push_back((uint32_t)g);
-                    out.pair.push_back(pa | (pc << 12) | ((uint32_t)slot[b->spring_material[g]] << 24));
+                    out.pair.push_back(pa | (pc << 12) | ((uint32_t)slot_of[b->spring_material[g]] << 24));
                     out.lbar.push_back(b->lbar[g]);
                     const uint32_t packed = sbase + k;
                     rows[pa].push_back({c, ls, 0u, packed});
@@ -506,12 +512,17 @@ mb_status mb_set_elements(mb_context* ctx, const mb_batch_desc* b) {
             }
             d.n_mass = mbase;
             d.n_spring = sbase;
-            // rows in summation order, stored SELL-32; padding points at the
-            // zero correction slot after the last spring
-            const uint32_t pad = sbase << 1;
+            // Rows in summation order, stored SELL-32.  Columns are aligned
+            // by the offset of the other end (other - i) when every row of the
+            // slice has distinct offsets: then the k-th entries of a warp's 32
+            // masses are springs of one direction with consecutive packed
+            // indices (conflict-free gather).  Otherwise, or when alignment
+            // would widen the slice by more than 4 columns, columns are ranks.
             for (uint32_t i0 = 0; i0 < mbase; i0 += mb::kSliceWidth) {
                 const uint32_t i1 = std::min<uint32_t>(i0 + mb::kSliceWidth, mbase);
-                uint32_t w = 0;
+                uint32_t w_rank = 0;
+                bool distinct = true;
+                std::vector<int> offs;
                 for (uint32_t i = i0; i < i1; ++i) {
                     auto& row = rows[i];
                     std::sort(row.begin(), row.end(), [](const Ent& x, const Ent& y) {
@@ -519,16 +530,30 @@ mb_status mb_set_elements(mb_context* ctx, const mb_batch_desc* b) {
                         if (x.orig != y.orig) return x.orig < y.orig;
                         return x.sign < y.sign;
                     });
-                    w = std::max<uint32_t>(w, (uint32_t)row.size());
+                    w_rank = std::max<uint32_t>(w_rank, (uint32_t)row.size());
+                    for (size_t q = 0; q < row.size(); ++q) {
+                        if (q && row[q].other == row[q - 1].other) distinct = false;
+                        offs.push_back((int)row[q].other - (int)i);
+                    }
                 }
+                std::sort(offs.begin(), offs.end());
+                offs.erase(std::unique(offs.begin(), offs.end()), offs.end());
+                const bool aligned = distinct && offs.size() <= w_rank + 4;
+                const uint32_t w = aligned ? (uint32_t)offs.size() : w_rank;
                 out.slice_off.push_back((uint32_t)out.inc.size() - d.inc_begin);
                 out.slice_width.push_back(w);
                 const size_t base = out.inc.size();
-                out.inc.resize(base + (size_t)w * mb::kSliceWidth, pad);
+                out.inc.resize(base + (size_t)w * mb::kSliceWidth, mb::kPadEntry);
                 for (uint32_t i = i0; i < i1; ++i)
-                    for (uint32_t k = 0; k < rows[i].size(); ++k)
-                        out.inc[base + (size_t)k * mb::kSliceWidth + (i - i0)] =
-                            (rows[i][k].packed << 1) | rows[i][k].sign;
+                    for (uint32_t q = 0; q < rows[i].size(); ++q) {
+                        const Ent& e = rows[i][q];
+                        const uint32_t col =
+                            aligned ? (uint32_t)(std::lower_bound(offs.begin(), offs.end(),
+                                                                  (int)e.other - (int)i) - offs.begin())
+                                    : q;
+                        out.inc[base + (size_t)col * mb::kSliceWidth + (i - i0)] =
+                            (uint16_t)((e.packed << 1) | e.sign);
+                    }
             }
             d.n_inc = (uint32_t)out.inc.size() - d.inc_begin;
             out.max_smem = std::max(out.max_smem, mb::bin_smem_bytes(d.n_mass, d.n_spring, d.n_inc));
@@ -539,7 +564,7 @@ mb_status mb_set_elements(mb_context* ctx, const mb_batch_desc* b) {
     bool ok = false;
     uint32_t smem_needed = 0;
     for (const auto& sh : shapes) {
-        const uint64_t cap_s = (uint64_t)sh.threads * sh.spt;
+        const uint64_t cap_s = std::min<uint64_t>((uint64_t)sh.threads * sh.spt, mb::kMaxBinSprings);
         const uint64_t cap_m = std::min<uint64_t>((uint64_t)sh.threads * sh.mpt, 4096);
         if (max_s > cap_s || max_m > cap_m) continue;
         uint32_t nb = ctx->override_cfg.bins;
@@ -626,6 +651,10 @@ mb_status mb_set_elements(mb_context* ctx, const mb_batch_desc* b) {
     MB_CUDA(ctx, up(ctx->slice_width, h_slice_width.data(), h_slice_width.size()));
     MB_CUDA(ctx, up(ctx->inc, h_inc.data(), h_inc.size()));
     MB_CUDA(ctx, up(ctx->mat_ids, h_mat_ids.data(), h_mat_ids.size()));
+    ctx->n_mat_host = (uint32_t)h_mat_ids.size();
+    MB_CUDA(ctx, up(ctx->n_mat, &ctx->n_mat_host, 1));
+    MB_CUDA(ctx, ctx->invk.alloc(std::max<uint32_t>(ctx->n_mat_host, 1)));
+    MB_CUDA(ctx, ctx->rates.alloc((size_t)std::max<uint32_t>(ctx->n_mat_host, 1) * ctx->chunk));
     MB_CUDA(ctx, up(ctx->robot_bin, h_robot_bin.data(), h_robot_bin.size()));
     MB_CUDA(ctx, ctx->bin_flags.alloc(nb));
     MB_CUDA(ctx, cudaMemsetAsync(ctx->bin_flags.p, 0, nb * sizeof(uint32_t), st));
@@ -667,8 +696,9 @@ mb::StepParams make_params(mb_context* c, float t0, uint32_t steps, bool track) 
     p.slice_off = c->slice_off.p;
     p.slice_width = c->slice_width.p;
     p.inc = c->inc.p;
-    p.mat_ids = c->mat_ids.p;
-    p.table = c->d_table.p;
+    p.n_mat = c->n_mat.p;
+    p.rates = c->rates.p;
+    p.invk = c->invk.p;
     p.bin_flags = c->bin_flags.p;
     p.dt = c->dt;
     p.t0 = t0;
@@ -691,6 +721,9 @@ cudaError_t issue_chunks(mb_context* c, float t0, uint32_t steps, bool track) {
     uint32_t done = 0;
     while (done < steps) {
         const uint32_t n = std::min(c->chunk, steps - done);
+        cudaError_t ea = mb::launch_actuation(c->d_table.p, c->mat_ids.p, c->n_mat.p, t, c->dt, n,
+                                              c->rates.p, c->invk.p, c->stream);
+        if (ea != cudaSuccess) return ea;
         mb::StepParams p = make_params(c, t, n, track);
         MB_TRACE("launch bins=%u threads=%u spt=%u mpt=%u smem=%u steps=%u", p.n_bins, c->shape.threads,
                  c->shape.spt, c->shape.mpt, p.smem_bytes, n);

@@ -7,9 +7,11 @@
 
 namespace mb {
 
-// Sentinel in the incidence lists: a padding entry that points at the zero
-// correction slot kept after the last spring of a bin.
+// Incidence entries are uint16: packed spring index << 1 | (1 at the b end);
+// kPadEntry pads rows to the slice width and is skipped by the gather.
 constexpr uint32_t kMaxMaterialSlots = 256;
+constexpr uint16_t kPadEntry = 0xFFFFu;
+constexpr uint32_t kMaxBinSprings = 32767;  // 15-bit spring index in an entry
 constexpr uint32_t kSliceWidth = 32;  // masses per SELL slice (one warp)
 
 // One bin: a group of whole robots that one CTA simulates together.  Masses
@@ -23,9 +25,7 @@ struct BinDesc {
     uint32_t inc_begin;    // first incidence entry (SELL-32 layout)
     uint32_t n_inc;        // incidence entries incl. padding
     uint32_t slice_begin;  // first slice descriptor
-    uint32_t mat_begin;    // first material slot
-    uint32_t n_mat;        // material slots used by the bin
-    uint32_t pad[3];
+    uint32_t pad[5];
 };
 
 // Everything one step launch needs.  Pointers are device addresses.
@@ -42,9 +42,10 @@ struct StepParams {
     const uint8_t* spring_slot;   // packed spring material slot (bin-local)
     const uint32_t* slice_off;    // per slice: first entry relative to bin inc_begin
     const uint32_t* slice_width;  // per slice: entries per mass (row length)
-    const uint32_t* inc;          // incidence entries: spring << 1 | (b end)
-    const uint8_t* mat_ids;       // per material slot: composite id
-    const float4* table;          // composite table {k, dL0, omega, phi}
+    const uint16_t* inc;          // incidence entries: spring << 1 | (b end), or kPadEntry
+    const uint32_t* n_mat;        // material slots used by the population (device scalar)
+    const float* rates;           // [steps][n_mat]: dL0 * sin(omega t_n + phi) of this launch
+    const float* invk;            // [n_mat]: 1 / (2 + 1/(k dt^2))
     uint32_t* bin_flags;          // per bin: bit 0 = non-finite position
     float dt;
     float t0;
@@ -62,6 +63,13 @@ struct KernelShape {
 // Sets the dynamic shared memory limit of a kernel variant; call before
 // launching (and outside stream capture).
 cudaError_t prepare_step(const KernelShape& shape, bool track, uint32_t smem_bytes);
+
+// Actuation factors of one launch: rates[n][i] = dL0 * sin(omega t_n + phi)
+// for steps n < steps of the float clock t_0 = t0, t_{n+1} = t_n + dt, and
+// the materials mat_ids[i], i < *n_mat; invk[i] = 1/(2 + 1/k/dt/dt).
+cudaError_t launch_actuation(const float4* table, const uint8_t* mat_ids, const uint32_t* n_mat,
+                             float t0, float dt, uint32_t steps, float* rates, float* invk,
+                             cudaStream_t s);
 
 // Launches the step kernel for `p.steps` steps.  Returns a CUDA error.
 cudaError_t launch_step(const StepParams& p, const KernelShape& shape, cudaStream_t s);

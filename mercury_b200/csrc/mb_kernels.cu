@@ -31,181 +31,147 @@ namespace {
 
 constexpr float kEps = 1e-12f;  // sim_kernel.cu:6
 
-__host__ __device__ inline uint32_t round4(uint32_t x) { return (x + 3u) & ~3u; }
-
 // Packed spring word: a (12 bits) | b << 12 (12 bits) | slot << 24 (8 bits).
 __device__ __forceinline__ uint32_t pk_a(uint32_t w) { return w & 0xFFFu; }
 __device__ __forceinline__ uint32_t pk_b(uint32_t w) { return (w >> 12) & 0xFFFu; }
 __device__ __forceinline__ uint32_t pk_slot(uint32_t w) { return w >> 24; }
 
 template <int T, int SPT, int MPT, bool TRACK>
-__global__ void __launch_bounds__(T, 1) step_kernel(const StepParams p) {
+__global__ void __launch_bounds__(T, 1024 / T) step_kernel(const StepParams p) {
     extern __shared__ float4 smem4[];
-    float* const sm = reinterpret_cast<float*>(smem4);
     const int tid = threadIdx.x;
     const float dt = p.dt;
     const double ddt = (double)dt;
 
     for (uint32_t b = blockIdx.x; b < p.n_bins; b += gridDim.x) {
         const BinDesc bd = p.bins[b];
-        const uint32_t m4 = round4(bd.n_mass), s4 = round4(bd.n_spring + 1);
-        float* sx = sm;
-        float* sy = sx + m4;
-        float* sz = sy + m4;
-        float* sdx = sz + m4;
-        float* sdy = sdx + s4;
-        float* sdz = sdy + s4;
-        uint32_t* sinc = reinterpret_cast<uint32_t*>(sdz + s4);
-        float* srate = reinterpret_cast<float*>(sinc + bd.n_inc);  // dL0*sin(...)
-        float* sinvk = srate + kMaxMaterialSlots;                   // 1/K
+        float4* sxt = smem4;                    // predicted positions x~, one float4 per mass
+        float4* sdp = sxt + bd.n_mass;          // corrections dp, one float4 per spring
+        float2* smat = reinterpret_cast<float2*>(sdp + bd.n_spring);  // {dL0 sin(..), 1/K} per slot
+        uint16_t* sinc = reinterpret_cast<uint16_t*>(smat + kMaxMaterialSlots);
 
+        const uint32_t n_mat = *p.n_mat;
         for (uint32_t i = tid; i < bd.n_inc; i += T) sinc[i] = __ldg(&p.inc[bd.inc_begin + i]);
-        if (tid == 0) {
-            sdx[bd.n_spring] = 0.0f;
-            sdy[bd.n_spring] = 0.0f;
-            sdz[bd.n_spring] = 0.0f;
-        }
-        for (uint32_t i = tid; i < bd.n_mat; i += T) {
-            const float4 mt = __ldg(&p.table[p.mat_ids[bd.mat_begin + i]]);
-            // alpha = 1/k/dt/dt, K = 2 + alpha (sim_kernel.cu:220, 225)
-            const float alpha = __fdiv_rn(__fdiv_rn(__fdiv_rn(1.0f, mt.x), dt), dt);
-            sinvk[i] = __frcp_rn(__fadd_rn(2.0f, alpha));
+        float next_rate = 0.0f;  // actuation factor of material tid for the coming step
+        if (tid < n_mat) {
+            smat[tid].y = __ldg(&p.invk[tid]);
+            next_rate = __ldg(&p.rates[tid]);
         }
 
-        // Springs of this thread: packed word, mean length, 1/length, stress.
+        // Springs of this thread: packed word and mean length (+ stress).
         uint32_t sw[SPT];
-        float lb[SPT], il[SPT], st[SPT];
+        float lb[SPT], st[SPT];
 #pragma unroll
         for (int j = 0; j < SPT; ++j) {
             const uint32_t s = tid + j * T;
             sw[j] = 0;
             lb[j] = 0.0f;
-            il[j] = 0.0f;
             st[j] = 0.0f;
             if (s < bd.n_spring) {
                 const uint32_t g = bd.spring_begin + s;
                 sw[j] = __ldg(&p.spring_pair[g]);
                 lb[j] = __ldg(&p.spring_lbar[g]);
-                if (TRACK) {
-                    il[j] = __frcp_rn(lb[j]);
-                    st[j] = p.stress[__ldg(&p.spring_gidx[g])];
-                }
+                if (TRACK) st[j] = p.stress[__ldg(&p.spring_gidx[g])];
             }
         }
-        // Masses of this thread: x, v (float4 keeps w), SELL row.
-        float4 x[MPT], v[MPT];
-        uint32_t roff[MPT], rwid[MPT];
+        // Masses of this thread: x, v and the SELL row (offset | width << 20).
+        float3 x[MPT], v[MPT];
+        uint32_t row[MPT];
 #pragma unroll
         for (int j = 0; j < MPT; ++j) {
             const uint32_t m = tid + j * T;
-            x[j] = make_float4(0.f, 0.f, 0.f, 0.f);
-            v[j] = make_float4(0.f, 0.f, 0.f, 0.f);
-            roff[j] = 0;
-            rwid[j] = 0;
+            x[j] = make_float3(0.f, 0.f, 0.f);
+            v[j] = make_float3(0.f, 0.f, 0.f);
+            row[j] = 0;
             if (m < bd.n_mass) {
                 const uint32_t g = __ldg(&p.mass_gidx[bd.mass_begin + m]);
-                x[j] = p.pos[g];
-                v[j] = p.vel[g];
+                const float4 P = p.pos[g], V = p.vel[g];
+                x[j] = make_float3(P.x, P.y, P.z);
+                v[j] = make_float3(V.x, V.y, V.z);
                 const uint32_t sl = bd.slice_begin + m / kSliceWidth;
-                roff[j] = __ldg(&p.slice_off[sl]) + (m % kSliceWidth);
-                rwid[j] = __ldg(&p.slice_width[sl]);
+                row[j] = (__ldg(&p.slice_off[sl]) + (m % kSliceWidth)) | (__ldg(&p.slice_width[sl]) << 20);
             }
         }
         __syncthreads();
 
-        float t = p.t0;
         for (uint32_t step = 0; step < p.steps; ++step) {
-            // (1) actuation factors of the bin's materials (sim_kernel.cu:222)
-            if (tid < 32) {
-                for (uint32_t i = tid; i < bd.n_mat; i += 32) {
-                    const float4 mt = __ldg(&p.table[p.mat_ids[bd.mat_begin + i]]);
-                    const float arg = __fmaf_rn(mt.z, t, mt.w);
-                    const float sn = __double2float_rn(sin_cw((double)arg));
-                    srate[i] = __fmul_rn(mt.y, sn);
-                }
+            // (1) actuation factors of this step (sim_kernel.cu:222), loaded one
+            // step ahead from the launch's table
+            if (tid < n_mat) {
+                smat[tid].x = next_rate;
+                if (step + 1 < p.steps) next_rate = __ldg(&p.rates[(step + 1) * n_mat + tid]);
             }
             // (1) predict x~ = x + v*dt (sim_kernel.cu:147-152)
-            float3 xt[MPT];
 #pragma unroll
             for (int j = 0; j < MPT; ++j) {
                 const uint32_t m = tid + j * T;
-                xt[j].x = __fadd_rn(x[j].x, __fmul_rn(v[j].x, dt));
-                xt[j].y = __fadd_rn(x[j].y, __fmul_rn(v[j].y, dt));
-                xt[j].z = __fadd_rn(x[j].z, __fmul_rn(v[j].z, dt));
-                if (m < bd.n_mass) {
-                    sx[m] = xt[j].x;
-                    sy[m] = xt[j].y;
-                    sz[m] = xt[j].z;
-                }
+                if (m >= bd.n_mass) break;
+                sxt[m] = make_float4(__fadd_rn(x[j].x, __fmul_rn(v[j].x, dt)),
+                                     __fadd_rn(x[j].y, __fmul_rn(v[j].y, dt)),
+                                     __fadd_rn(x[j].z, __fmul_rn(v[j].z, dt)), 0.0f);
             }
             __syncthreads();
             // (2) distance constraints (sim_kernel.cu:209-243)
 #pragma unroll
             for (int j = 0; j < SPT; ++j) {
                 const uint32_t s = tid + j * T;
-                if (s < bd.n_spring) {
-                    const uint32_t a = pk_a(sw[j]), bb = pk_b(sw[j]), sl = pk_slot(sw[j]);
-                    const float L = __fmaf_rn(lb[j], srate[sl], lb[j]);
-                    const float dx = __fsub_rn(sx[a], sx[bb]);
-                    const float dy = __fsub_rn(sy[a], sy[bb]);
-                    const float dz = __fsub_rn(sz[a], sz[bb]);
-                    const float d2 = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, __fmul_rn(dz, dz)));
-                    const float d = __fsqrt_rn(d2);
-                    const float r = __frcp_rn(__fadd_rn(d, kEps));
-                    const float C = __fsub_rn(d, L);
-                    const float lam = __fmul_rn(-C, sinvk[sl]);
-                    const float coef = __fmul_rn(lam, r);
-                    sdx[s] = __fmul_rn(coef, dx);
-                    sdy[s] = __fmul_rn(coef, dy);
-                    sdz[s] = __fmul_rn(coef, dz);
-                    if (TRACK) st[j] = __fadd_rn(st[j], __fmul_rn(lam, il[j]));
-                }
+                if (s >= bd.n_spring) break;
+                const float4 pa = sxt[pk_a(sw[j])], pb = sxt[pk_b(sw[j])];
+                const float2 mt = smat[pk_slot(sw[j])];
+                const float L = __fmaf_rn(lb[j], mt.x, lb[j]);
+                const float dx = __fsub_rn(pa.x, pb.x);
+                const float dy = __fsub_rn(pa.y, pb.y);
+                const float dz = __fsub_rn(pa.z, pb.z);
+                const float d = __fsqrt_rn(__fmaf_rn(dx, dx, __fmaf_rn(dy, dy, __fmul_rn(dz, dz))));
+                const float r = __frcp_rn(__fadd_rn(d, kEps));
+                const float lam = __fmul_rn(-__fsub_rn(d, L), mt.y);
+                const float coef = __fmul_rn(lam, r);
+                sdp[s] = make_float4(__fmul_rn(coef, dx), __fmul_rn(coef, dy), __fmul_rn(coef, dz), 0.0f);
+                if (TRACK) st[j] = __fadd_rn(st[j], __fmul_rn(lam, __frcp_rn(lb[j])));
             }
             __syncthreads();
-            // (3) gather in SELL order and integrate (sim_kernel.cu:246-268)
+            // (3) gather in summation order and integrate (sim_kernel.cu:246-268).
+            // acc + (+-c) is computed as fma(c, +-1, acc): c*(+-1) is exact, so
+            // the single rounding equals that of the addition.
 #pragma unroll
             for (int j = 0; j < MPT; ++j) {
                 const uint32_t m = tid + j * T;
-                if (m < bd.n_mass) {
-                    float ax = 0.0f, ay = 0.0f, az = 0.0f;
-                    const uint32_t base = roff[j], w = rwid[j];
-                    for (uint32_t k = 0; k < w; ++k) {
-                        const uint32_t e = sinc[base + k * kSliceWidth];
-                        const uint32_t s = e >> 1;
-                        float cx = sdx[s], cy = sdy[s], cz = sdz[s];
-                        if (e & 1u) {
-                            cx = -cx;
-                            cy = -cy;
-                            cz = -cz;
-                        }
-                        ax = __fadd_rn(ax, cx);
-                        ay = __fadd_rn(ay, cy);
-                        az = __fadd_rn(az, cz);
+                if (m >= bd.n_mass) break;
+                float ax = 0.0f, ay = 0.0f, az = 0.0f;
+                const uint16_t* rp = sinc + (row[j] & 0xFFFFFu);
+                const uint32_t w = row[j] >> 20;
+                for (uint32_t k = 0; k < w; ++k) {
+                    const uint32_t e = rp[k * kSliceWidth];
+                    if (e != kPadEntry) {
+                        const float4 c = sdp[e >> 1];
+                        const float sg = __uint_as_float(0x3f800000u | ((e & 1u) << 31));
+                        ax = __fmaf_rn(c.x, sg, ax);
+                        ay = __fmaf_rn(c.y, sg, ay);
+                        az = __fmaf_rn(c.z, sg, az);
                     }
-                    const float nx = __fadd_rn(xt[j].x, ax);
-                    const float ny = __fadd_rn(xt[j].y, ay);
-                    const float nz = __fadd_rn(xt[j].z, az);
-                    // v = 0.99*(x~ - x)/dt in double (sim_kernel.cu:265-267)
-                    v[j].x = __double2float_rn(__ddiv_rn(__dmul_rn(0.99, (double)__fsub_rn(nx, x[j].x)), ddt));
-                    v[j].y = __double2float_rn(__ddiv_rn(__dmul_rn(0.99, (double)__fsub_rn(ny, x[j].y)), ddt));
-                    v[j].z = __double2float_rn(__ddiv_rn(__dmul_rn(0.99, (double)__fsub_rn(nz, x[j].z)), ddt));
-                    x[j].x = nx;
-                    x[j].y = ny;
-                    x[j].z = nz;
                 }
+                const float4 xt = sxt[m];
+                const float nx = __fadd_rn(xt.x, ax);
+                const float ny = __fadd_rn(xt.y, ay);
+                const float nz = __fadd_rn(xt.z, az);
+                // v = 0.99*(x~ - x)/dt in double (sim_kernel.cu:265-267)
+                v[j].x = __double2float_rn(__ddiv_rn(__dmul_rn(0.99, (double)__fsub_rn(nx, x[j].x)), ddt));
+                v[j].y = __double2float_rn(__ddiv_rn(__dmul_rn(0.99, (double)__fsub_rn(ny, x[j].y)), ddt));
+                v[j].z = __double2float_rn(__ddiv_rn(__dmul_rn(0.99, (double)__fsub_rn(nz, x[j].z)), ddt));
+                x[j] = make_float3(nx, ny, nz);
             }
-            t = __fadd_rn(t, dt);
         }
 
-        // Write back in the upload layout; flag non-finite positions.
+        // Write back in the upload layout (w components unchanged); flag
+        // non-finite positions.
         bool bad = false;
 #pragma unroll
         for (int j = 0; j < MPT; ++j) {
             const uint32_t m = tid + j * T;
             if (m < bd.n_mass) {
                 const uint32_t g = __ldg(&p.mass_gidx[bd.mass_begin + m]);
-                p.pos[g] = x[j];
-                p.vel[g] = v[j];
+                p.pos[g] = make_float4(x[j].x, x[j].y, x[j].z, p.pos[g].w);
+                p.vel[g] = make_float4(v[j].x, v[j].y, v[j].z, p.vel[g].w);
                 bad |= !(isfinite(x[j].x) && isfinite(x[j].y) && isfinite(x[j].z));
             }
         }
@@ -217,6 +183,46 @@ __global__ void __launch_bounds__(T, 1) step_kernel(const StepParams p) {
             }
         }
         if (__syncthreads_or(bad) && tid == 0) atomicOr(&p.bin_flags[b], 1u);
+    }
+}
+
+// Actuation factors of one launch.  Block b covers steps [256 b, 256 b + 256):
+// thread 0 accumulates the float clock from t0 (the clock is a sequential
+// float sum, Simulator.cu:447, so it is not reassociated), then every thread
+// evaluates its step for every material.
+__global__ void __launch_bounds__(256) actuation_kernel(const float4* __restrict__ table,
+                                                        const uint8_t* __restrict__ mat_ids,
+                                                        const uint32_t* __restrict__ n_mat_ptr,
+                                                        float t0, float dt, uint32_t steps,
+                                                        float* __restrict__ rates,
+                                                        float* __restrict__ invk) {
+    __shared__ float s_t[256];
+    const uint32_t n_mat = *n_mat_ptr;
+    const uint32_t base = blockIdx.x * 256u;
+    if (threadIdx.x == 0) {
+        float t = t0;
+        for (uint32_t i = 0; i < base; ++i) t = __fadd_rn(t, dt);
+        for (uint32_t i = 0; i < 256u; ++i) {
+            s_t[i] = t;
+            t = __fadd_rn(t, dt);
+        }
+    }
+    if (blockIdx.x == 0) {
+        for (uint32_t i = threadIdx.x; i < n_mat; i += 256u) {
+            const float4 mt = table[mat_ids[i]];
+            // alpha = 1/k/dt/dt, K = 2 + alpha (sim_kernel.cu:220, 225)
+            const float alpha = __fdiv_rn(__fdiv_rn(__fdiv_rn(1.0f, mt.x), dt), dt);
+            invk[i] = __frcp_rn(__fadd_rn(2.0f, alpha));
+        }
+    }
+    __syncthreads();
+    const uint32_t n = base + threadIdx.x;
+    if (n >= steps) return;
+    const float t = s_t[threadIdx.x];
+    for (uint32_t i = 0; i < n_mat; ++i) {
+        const float4 mt = table[mat_ids[i]];
+        const float arg = __fmaf_rn(mt.z, t, mt.w);
+        rates[(size_t)n * n_mat + i] = __fmul_rn(mt.y, __double2float_rn(sin_cw((double)arg)));
     }
 }
 
@@ -279,9 +285,9 @@ struct ShapeEntry {
 
 #define MB_SHAPE(T, S, M) {T, S, M, {step_kernel<T, S, M, false>, step_kernel<T, S, M, true>}}
 const ShapeEntry kShapes[] = {
-    MB_SHAPE(256, 4, 1),  MB_SHAPE(256, 8, 2),  MB_SHAPE(256, 16, 4),
-    MB_SHAPE(512, 4, 1),  MB_SHAPE(512, 8, 2),  MB_SHAPE(512, 16, 4),
-    MB_SHAPE(1024, 4, 1), MB_SHAPE(1024, 8, 2),
+    MB_SHAPE(256, 8, 2),   MB_SHAPE(256, 16, 4),  MB_SHAPE(512, 4, 1),  MB_SHAPE(512, 8, 2),
+    MB_SHAPE(512, 12, 2),  MB_SHAPE(512, 16, 4),  MB_SHAPE(1024, 4, 1), MB_SHAPE(1024, 6, 2),
+    MB_SHAPE(1024, 8, 2),  MB_SHAPE(1024, 10, 2), MB_SHAPE(1024, 12, 2),
 };
 #undef MB_SHAPE
 
@@ -294,7 +300,7 @@ const ShapeEntry* find_shape(const KernelShape& s) {
 }  // namespace
 
 uint32_t bin_smem_bytes(uint32_t n_mass, uint32_t n_spring, uint32_t n_inc) {
-    return 4u * (3u * round4(n_mass) + 3u * round4(n_spring + 1) + n_inc + 2u * kMaxMaterialSlots);
+    return 16u * n_mass + 16u * n_spring + 8u * kMaxMaterialSlots + 2u * n_inc;
 }
 
 uint32_t max_step_smem(int device) {
@@ -329,6 +335,14 @@ cudaError_t launch_step(const StepParams& p, const KernelShape& shape, cudaStrea
     if (!e) return cudaErrorInvalidValue;
     if (p.n_bins == 0) return cudaSuccess;
     e->fn[p.track ? 1 : 0]<<<p.n_bins, shape.threads, p.smem_bytes, s>>>(p);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_actuation(const float4* table, const uint8_t* mat_ids, const uint32_t* n_mat,
+                             float t0, float dt, uint32_t steps, float* rates, float* invk,
+                             cudaStream_t s) {
+    if (steps == 0) return cudaSuccess;
+    actuation_kernel<<<(steps + 255) / 256, 256, 0, s>>>(table, mat_ids, n_mat, t0, dt, steps, rates, invk);
     return cudaGetLastError();
 }
 

@@ -32,6 +32,7 @@ constexpr uint32_t kNaMaxSprings = MB_NOALLOC_MAX_SPRINGS;
 constexpr uint32_t kNaMaxIncidence = MB_NOALLOC_MAX_INCIDENCE;
 constexpr uint32_t kNaSlices = kNaMaxMasses / kSliceWidth;
 constexpr uint32_t kBuildThreads = 1024;
+constexpr uint32_t kNaChunk = 128;  // steps per launch: bounds the actuation table
 
 // Status bits written by the build kernel.
 constexpr uint32_t kNaBadTopology = 1u;  // index or material out of range
@@ -49,10 +50,13 @@ constexpr size_t kOffLbar = align256(kOffSpringPair + 4 * kNaMaxSprings);
 constexpr size_t kOffSliceOff = align256(kOffLbar + 4 * kNaMaxSprings);
 constexpr size_t kOffSliceWidth = align256(kOffSliceOff + 4 * kNaSlices);
 constexpr size_t kOffMatIds = align256(kOffSliceWidth + 4 * kNaSlices);
-constexpr size_t kOffRowStart = align256(kOffMatIds + kMaxMaterialSlots);
+constexpr size_t kOffNMat = align256(kOffMatIds + kMaxMaterialSlots);
+constexpr size_t kOffInvK = align256(kOffNMat + sizeof(uint32_t));
+constexpr size_t kOffRates = align256(kOffInvK + 4 * kMaxMaterialSlots);
+constexpr size_t kOffRowStart = align256(kOffRates + 4 * kMaxMaterialSlots * kNaChunk);
 constexpr size_t kOffRows = align256(kOffRowStart + 4 * (kNaMaxMasses + 1));
 constexpr size_t kOffInc = align256(kOffRows + 4 * 2 * kNaMaxSprings);
-constexpr size_t kScratchBytes = align256(kOffInc + 4 * kNaMaxIncidence);
+constexpr size_t kScratchBytes = align256(kOffInc + 2 * kNaMaxIncidence);
 
 // The scratch array itself.  In host code `g_noalloc_scratch` names a host
 // shadow, not device memory; its device address comes from
@@ -110,7 +114,8 @@ __global__ void __launch_bounds__(kBuildThreads) noalloc_build(const BuildArgs a
     uint8_t* mat_ids = reinterpret_cast<uint8_t*>(sc + kOffMatIds);
     uint32_t* row_start = reinterpret_cast<uint32_t*>(sc + kOffRowStart);
     uint32_t* rows = reinterpret_cast<uint32_t*>(sc + kOffRows);
-    uint32_t* inc = reinterpret_cast<uint32_t*>(sc + kOffInc);
+    uint16_t* inc = reinterpret_cast<uint16_t*>(sc + kOffInc);
+    uint32_t* n_mat = reinterpret_cast<uint32_t*>(sc + kOffNMat);
 
     // clear what must start at zero (the scratch keeps the previous call)
     for (uint32_t i = tid; i < kNaMaxMasses; i += kBuildThreads) s_deg[i] = 0;
@@ -148,6 +153,7 @@ __global__ void __launch_bounds__(kBuildThreads) noalloc_build(const BuildArgs a
                 s_slot[m] = n++;
             }
         s_nmat = n;
+        *n_mat = n;
     }
     __syncthreads();
 
@@ -225,13 +231,12 @@ __global__ void __launch_bounds__(kBuildThreads) noalloc_build(const BuildArgs a
     __syncthreads();
     const bool ok = s_status == 0;
     if (ok) {
-        const uint32_t pad = n_act << 1;  // the zero correction slot
-        for (uint32_t x = tid; x < s_ninc; x += kBuildThreads) inc[x] = pad;
+        for (uint32_t x = tid; x < s_ninc; x += kBuildThreads) inc[x] = kPadEntry;
         __syncthreads();
         for (uint32_t i = tid; i < a.n_mass; i += kBuildThreads) {
             const uint32_t o = slice_off[i / kSliceWidth] + (i % kSliceWidth);
             for (uint32_t x = row_start[i]; x < row_start[i + 1]; ++x)
-                inc[o + (x - row_start[i]) * kSliceWidth] = rows[x];
+                inc[o + (x - row_start[i]) * kSliceWidth] = (uint16_t)rows[x];
             mass_gidx[i] = i;
         }
     }
@@ -242,7 +247,6 @@ __global__ void __launch_bounds__(kBuildThreads) noalloc_build(const BuildArgs a
             d.n_mass = a.n_mass;
             d.n_spring = n_act;
             d.n_inc = s_ninc;
-            d.n_mat = s_nmat;
         }
         *bin = d;
         *status = s_status;
@@ -292,7 +296,7 @@ extern "C" mb_status mb_simulate_robot_noalloc(void* stream, const float* table,
     if (cudaGetLastError() != cudaSuccess) return MB_ERR_CUDA;
 
     // the step kernel of the batched path, on one bin that lives in the scratch
-    const KernelShape shape{512, 16, 4};  // holds kNaMaxSprings springs, kNaMaxMasses masses
+    const KernelShape shape{1024, 8, 2};  // holds kNaMaxSprings springs, kNaMaxMasses masses
     StepParams p{};
     p.bins = reinterpret_cast<const BinDesc*>(sc + kOffBin);
     p.n_bins = 1;
@@ -305,9 +309,10 @@ extern "C" mb_status mb_simulate_robot_noalloc(void* stream, const float* table,
     p.spring_lbar = reinterpret_cast<const float*>(sc + kOffLbar);
     p.slice_off = reinterpret_cast<const uint32_t*>(sc + kOffSliceOff);
     p.slice_width = reinterpret_cast<const uint32_t*>(sc + kOffSliceWidth);
-    p.inc = reinterpret_cast<const uint32_t*>(sc + kOffInc);
-    p.mat_ids = reinterpret_cast<const uint8_t*>(sc + kOffMatIds);
-    p.table = reinterpret_cast<const float4*>(table);
+    p.inc = reinterpret_cast<const uint16_t*>(sc + kOffInc);
+    p.n_mat = reinterpret_cast<const uint32_t*>(sc + kOffNMat);
+    p.rates = reinterpret_cast<const float*>(sc + kOffRates);
+    p.invk = reinterpret_cast<const float*>(sc + kOffInvK);
     p.bin_flags = reinterpret_cast<uint32_t*>(sc + kOffFlag);
     p.dt = dt;
     p.track = track_stresses ? 1u : 0u;
@@ -317,7 +322,12 @@ extern "C" mb_status mb_simulate_robot_noalloc(void* stream, const float* table,
     float t = t0;
     uint32_t done = 0;
     while (done < steps) {
-        const uint32_t n = steps - done < 1000u ? steps - done : 1000u;
+        const uint32_t n = steps - done < kNaChunk ? steps - done : kNaChunk;
+        if (launch_actuation(reinterpret_cast<const float4*>(table),
+                             reinterpret_cast<const uint8_t*>(sc + kOffMatIds), p.n_mat, t, dt, n,
+                             reinterpret_cast<float*>(sc + kOffRates),
+                             reinterpret_cast<float*>(sc + kOffInvK), st) != cudaSuccess)
+            return MB_ERR_CUDA;
         p.t0 = t;
         p.steps = n;
         if (launch_step(p, shape, st) != cudaSuccess) return MB_ERR_CUDA;

@@ -64,8 +64,9 @@ class Simulator:
 
     def __del__(self):
         ctx = getattr(self, "_ctx", None)
-        if ctx:
-            _lib.LIB.mb_context_destroy(ctx)
+        lib = getattr(_lib, "LIB", None)  # None during interpreter shutdown
+        if ctx and lib is not None:
+            lib.mb_context_destroy(ctx)
             self._ctx = None
 
     # -- Simulator.h:27-48 ------------------------------------------------
