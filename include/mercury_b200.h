@@ -52,8 +52,29 @@ typedef enum mb_status {
 } mb_status;
 
 typedef enum mb_mode {
-    MB_MODE_REF_XPBD = 0 /* the reference step: sim_kernel.cu:141-269 */
+    MB_MODE_REF_XPBD = 0,    /* the reference step: sim_kernel.cu:141-269 */
+    MB_MODE_FORCE_LAND = 1,  /* Hooke springs, gravity, ground with friction */
+    MB_MODE_FORCE_WATER = 2  /* Hooke springs, quadratic drag, no net gravity */
 } mb_mode;
+
+/* Environment of the force modes (the fields of the reference's
+ * Environment, environment.h:6-32, with both friction coefficients and a
+ * drag coefficient that acts):
+ *   g                gravity along -z (land), m/s^2
+ *   floor_stiffness  penalty stiffness of the ground plane z = 0, N/m
+ *   friction_static, friction_kinetic   Coulomb coefficients (land)
+ *   drag             0.5 * rho * Cd * A of the quadratic drag per mass (water)
+ *   damping          velocity factor per step
+ * Force modes integrate x' = x + v dt + (F/m) dt^2, v' = damping (x' - x)/dt
+ * with m the w component of the position. */
+typedef struct mb_environment {
+    float g;
+    float floor_stiffness;
+    float friction_static;
+    float friction_kinetic;
+    float drag;
+    float damping;
+} mb_environment;
 
 /* One population on the host.  Offsets have n_robots + 1 entries and index
  * the flat arrays; pairs are local to their robot. */
@@ -106,6 +127,14 @@ MB_API float mb_get_total_time(const mb_context* ctx);
 /* Step semantics.  Replaces the fixed kernel set of integrateBodies
  * (sim_kernel.cu:271-325). */
 MB_API mb_status mb_set_mode(mb_context* ctx, mb_mode mode);
+MB_API mb_status mb_get_mode(const mb_context* ctx, mb_mode* mode);
+
+/* Environment of the force modes; the default is land with g = 9.81,
+ * floor_stiffness = 1e6 (environment.h:15-22), friction 1.0 / 0.8, drag 0.05,
+ * damping 0.999.  Replaces Simulator::_initialize's environment choice
+ * (Simulator.cu:191-196). */
+MB_API mb_status mb_set_environment(mb_context* ctx, const mb_environment* env);
+MB_API mb_status mb_get_environment(const mb_context* ctx, mb_environment* env);
 
 /* Uploads a population: packs it into bins, builds the per-mass incidence
  * lists, copies everything to the device and zeroes the spring stresses.

@@ -24,7 +24,7 @@ STATUS_NAMES = {
     5: "MB_ERR_NONFINITE",
 }
 COMPOSITE_COUNT = 254
-MODE_REF_XPBD = 0
+MODE_REF_XPBD, MODE_FORCE_LAND, MODE_FORCE_WATER = 0, 1, 2
 
 
 class MercuryError(RuntimeError):
@@ -45,6 +45,11 @@ class BatchDesc(ctypes.Structure):
         ("spring_material", ctypes.c_void_p),
         ("lbar", ctypes.c_void_p),
     ]
+
+
+class Environment(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_float) for n in ("g", "floor_stiffness", "friction_static",
+                                              "friction_kinetic", "drag", "damping")]
 
 
 class LaunchConfig(ctypes.Structure):
@@ -75,6 +80,9 @@ def _load() -> ctypes.CDLL:
         "mb_set_total_time": (I32, [P, F32]),
         "mb_get_total_time": (F32, [P]),
         "mb_set_mode": (I32, [P, I32]),
+        "mb_get_mode": (I32, [P, ctypes.POINTER(ctypes.c_int)]),
+        "mb_set_environment": (I32, [P, ctypes.POINTER(Environment)]),
+        "mb_get_environment": (I32, [P, ctypes.POINTER(Environment)]),
         "mb_set_elements": (I32, [P, ctypes.POINTER(BatchDesc)]),
         "mb_set_state": (I32, [P, P, P]),
         "mb_simulate": (I32, [P, F32, I32, ctypes.POINTER(U32)]),

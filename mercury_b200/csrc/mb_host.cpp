@@ -105,6 +105,7 @@ struct mb_context {
     float dt = 0.0001f;  // Simulator.h:55
     float total_time = 0.0f;
     mb_mode mode = MB_MODE_REF_XPBD;
+    mb_environment env{9.81f, 1.0e6f, 1.0f, 0.8f, 0.05f, 0.999f};
     float table[4 * MB_COMPOSITE_COUNT] = {};
     bool have_table = false;
 
@@ -333,8 +334,33 @@ float mb_get_total_time(const mb_context* ctx) { return ctx ? ctx->total_time : 
 
 mb_status mb_set_mode(mb_context* ctx, mb_mode mode) {
     if (!ctx) return MB_ERR_ARGUMENT;
-    if (mode != MB_MODE_REF_XPBD) return fail(ctx, MB_ERR_ARGUMENT, "unknown mode %d", (int)mode);
+    if (mode != MB_MODE_REF_XPBD && mode != MB_MODE_FORCE_LAND && mode != MB_MODE_FORCE_WATER)
+        return fail(ctx, MB_ERR_ARGUMENT, "unknown mode %d", (int)mode);
+    if (mode != ctx->mode) ctx->clear_graphs();
     ctx->mode = mode;
+    return MB_OK;
+}
+
+mb_status mb_get_mode(const mb_context* ctx, mb_mode* mode) {
+    if (!ctx || !mode) return MB_ERR_ARGUMENT;
+    *mode = ctx->mode;
+    return MB_OK;
+}
+
+mb_status mb_set_environment(mb_context* ctx, const mb_environment* env) {
+    if (!ctx || !env) return fail(ctx, MB_ERR_ARGUMENT, "null argument");
+    const float v[6] = {env->g, env->floor_stiffness, env->friction_static, env->friction_kinetic,
+                        env->drag, env->damping};
+    for (float f : v)
+        if (!std::isfinite(f) || f < 0.0f) return fail(ctx, MB_ERR_ARGUMENT, "environment values must be finite and >= 0");
+    ctx->env = *env;
+    ctx->clear_graphs();
+    return MB_OK;
+}
+
+mb_status mb_get_environment(const mb_context* ctx, mb_environment* env) {
+    if (!ctx || !env) return MB_ERR_ARGUMENT;
+    *env = ctx->env;
     return MB_OK;
 }
 
@@ -580,7 +606,7 @@ mb_status mb_set_elements(mb_context* ctx, const mb_batch_desc* b) {
                     smem_cap, mb::bin_smem_bytes((uint32_t)std::min<uint64_t>(cap_m, tot_m / sms + 1),
                                                  (uint32_t)std::min<uint64_t>(cap_s, tot_s / sms + 1),
                                                  (uint32_t)std::min<uint64_t>(3 * cap_s, 3 * (tot_s / sms + 1))));
-                const int per_sm = std::max(1, mb::ctas_per_sm(sh, false, est_smem));
+                const int per_sm = std::max(1, mb::ctas_per_sm(sh, (uint32_t)ctx->mode, false, est_smem));
                 wave = sms * (uint32_t)per_sm;
                 nb = std::max<uint32_t>(nb, wave);
                 nb = (nb + wave - 1) / wave * wave;  // whole waves
@@ -705,6 +731,13 @@ mb::StepParams make_params(mb_context* c, float t0, uint32_t steps, bool track) 
     p.steps = steps;
     p.track = track ? 1u : 0u;
     p.smem_bytes = c->smem_bytes;
+    p.mode = (uint32_t)c->mode;
+    p.g = c->env.g;
+    p.floor_stiffness = c->env.floor_stiffness;
+    p.mu_s = c->env.friction_static;
+    p.mu_k = c->env.friction_kinetic;
+    p.drag = c->env.drag;
+    p.damping = c->env.damping;
     return p;
 }
 
@@ -722,7 +755,7 @@ cudaError_t issue_chunks(mb_context* c, float t0, uint32_t steps, bool track) {
     while (done < steps) {
         const uint32_t n = std::min(c->chunk, steps - done);
         cudaError_t ea = mb::launch_actuation(c->d_table.p, c->mat_ids.p, c->n_mat.p, t, c->dt, n,
-                                              c->rates.p, c->invk.p, c->stream);
+                                              (uint32_t)c->mode, c->rates.p, c->invk.p, c->stream);
         if (ea != cudaSuccess) return ea;
         mb::StepParams p = make_params(c, t, n, track);
         MB_TRACE("launch bins=%u threads=%u spt=%u mpt=%u smem=%u steps=%u", p.n_bins, c->shape.threads,
@@ -756,7 +789,7 @@ mb_status run(mb_context* c, uint32_t steps, bool track) {
             if (c->graphs.size() >= 16) c->clear_graphs();
             // kernel attributes cannot change inside a capture
             MB_TRACE("prepare");
-            MB_CUDA(c, mb::prepare_step(c->shape, track, c->smem_bytes));
+            MB_CUDA(c, mb::prepare_step(c->shape, (uint32_t)c->mode, track, c->smem_bytes));
             cudaGraph_t g;
             MB_TRACE("begin capture");
             MB_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
@@ -779,7 +812,7 @@ mb_status run(mb_context* c, uint32_t steps, bool track) {
         MB_TRACE("graph launched");
     } else {
         MB_TRACE("prepare (no graph)");
-        MB_CUDA(c, mb::prepare_step(c->shape, track, c->smem_bytes));
+        MB_CUDA(c, mb::prepare_step(c->shape, (uint32_t)c->mode, track, c->smem_bytes));
         cudaError_t e = issue_chunks(c, t0, steps, track);
         if (e != cudaSuccess) return cuda_fail(c, e, "step launch");
     }

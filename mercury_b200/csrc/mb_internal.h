@@ -52,7 +52,16 @@ struct StepParams {
     uint32_t steps;
     uint32_t track;
     uint32_t smem_bytes;
+    uint32_t mode;                // 0 reference XPBD, 1 force + land, 2 force + water
+    // environment of the force modes
+    float g;                      // gravity along -z (land)
+    float floor_stiffness;        // penalty stiffness of the ground z = 0 (land)
+    float mu_s, mu_k;             // static / kinetic friction coefficients (land)
+    float drag;                   // 0.5 rho Cd A of the quadratic drag per mass (water)
+    float damping;                // velocity factor per step
 };
+
+enum StepMode : uint32_t { kModeXpbd = 0, kModeForceLand = 1, kModeForceWater = 2 };
 
 struct KernelShape {
     uint32_t threads;
@@ -60,23 +69,26 @@ struct KernelShape {
     uint32_t mpt;  // masses per thread
 };
 
+// Mode-dependent launch helpers take the mode of the step as well.
+
 // Sets the dynamic shared memory limit of a kernel variant; call before
 // launching (and outside stream capture).
-cudaError_t prepare_step(const KernelShape& shape, bool track, uint32_t smem_bytes);
+cudaError_t prepare_step(const KernelShape& shape, uint32_t mode, bool track, uint32_t smem_bytes);
 
 // Actuation factors of one launch: rates[n][i] = dL0 * sin(omega t_n + phi)
 // for steps n < steps of the float clock t_0 = t0, t_{n+1} = t_n + dt, and
-// the materials mat_ids[i], i < *n_mat; invk[i] = 1/(2 + 1/k/dt/dt).
+// the materials mat_ids[i], i < *n_mat; coef[i] = 1/(2 + 1/k/dt/dt) for the
+// reference step, k for the force modes.
 cudaError_t launch_actuation(const float4* table, const uint8_t* mat_ids, const uint32_t* n_mat,
-                             float t0, float dt, uint32_t steps, float* rates, float* invk,
-                             cudaStream_t s);
+                             float t0, float dt, uint32_t steps, uint32_t mode, float* rates,
+                             float* coef, cudaStream_t s);
 
 // Launches the step kernel for `p.steps` steps.  Returns a CUDA error.
 cudaError_t launch_step(const StepParams& p, const KernelShape& shape, cudaStream_t s);
 
 // Resident CTAs per SM of a kernel variant with `smem_bytes` of dynamic
 // shared memory (0 if the shape is not compiled or does not fit).
-int ctas_per_sm(const KernelShape& shape, bool track, uint32_t smem_bytes);
+int ctas_per_sm(const KernelShape& shape, uint32_t mode, bool track, uint32_t smem_bytes);
 
 // Shared memory a bin needs, in bytes.
 uint32_t bin_smem_bytes(uint32_t n_mass, uint32_t n_spring, uint32_t n_inc);

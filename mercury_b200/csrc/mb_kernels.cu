@@ -36,8 +36,56 @@ __device__ __forceinline__ uint32_t pk_a(uint32_t w) { return w & 0xFFFu; }
 __device__ __forceinline__ uint32_t pk_b(uint32_t w) { return (w >> 12) & 0xFFFu; }
 __device__ __forceinline__ uint32_t pk_slot(uint32_t w) { return w >> 24; }
 
-template <int T, int SPT, int MPT, bool TRACK>
+// Force modes, per mass, after the spring forces (fx, fy, fz) are gathered:
+// environment forces, then x' = x + v dt + (F/m) dt^2, v' = damping (x' - x)/dt.
+//   land : gravity -m g along z; below z = 0 a penalty normal force
+//          fn = k_floor (-z) and Coulomb friction on the horizontal velocity
+//          h = v + (F_h/m) dt the step would reach: static (the friction force
+//          cancels the horizontal motion, F_h = -m v_h/dt) when |h| <= mu_s fn
+//          dt/m, else kinetic, mu_k fn against h.
+//   water: gravity balanced by buoyancy; quadratic drag -drag |v| v.
+template <int MODE>
+__device__ __forceinline__ void force_integrate(const StepParams& p, float3& x, float3& v, float m,
+                                                float fx, float fy, float fz) {
+    const float dt = p.dt;
+    if (MODE == kModeForceLand) {
+        fz = __fsub_rn(fz, __fmul_rn(m, p.g));
+        if (x.z < 0.0f) {
+            const float fn = __fmul_rn(p.floor_stiffness, -x.z);
+            fz = __fadd_rn(fz, fn);
+            const float hx = __fadd_rn(v.x, __fmul_rn(__fdiv_rn(fx, m), dt));
+            const float hy = __fadd_rn(v.y, __fmul_rn(__fdiv_rn(fy, m), dt));
+            const float hs = __fsqrt_rn(__fmaf_rn(hx, hx, __fmul_rn(hy, hy)));
+            const float budget = __fmul_rn(__fdiv_rn(fn, m), dt);
+            if (hs <= __fmul_rn(p.mu_s, budget)) {
+                fx = __fdiv_rn(__fmul_rn(-m, v.x), dt);
+                fy = __fdiv_rn(__fmul_rn(-m, v.y), dt);
+            } else {
+                const float s = __fdiv_rn(__fmul_rn(p.mu_k, fn), hs);
+                fx = __fsub_rn(fx, __fmul_rn(s, hx));
+                fy = __fsub_rn(fy, __fmul_rn(s, hy));
+            }
+        }
+    } else {
+        const float sp = __fsqrt_rn(__fmaf_rn(v.x, v.x, __fmaf_rn(v.y, v.y, __fmul_rn(v.z, v.z))));
+        const float c = __fmul_rn(p.drag, sp);
+        fx = __fsub_rn(fx, __fmul_rn(c, v.x));
+        fy = __fsub_rn(fy, __fmul_rn(c, v.y));
+        fz = __fsub_rn(fz, __fmul_rn(c, v.z));
+    }
+    const float dt2 = __fmul_rn(dt, dt);
+    const float nx = __fadd_rn(__fadd_rn(x.x, __fmul_rn(v.x, dt)), __fmul_rn(__fdiv_rn(fx, m), dt2));
+    const float ny = __fadd_rn(__fadd_rn(x.y, __fmul_rn(v.y, dt)), __fmul_rn(__fdiv_rn(fy, m), dt2));
+    const float nz = __fadd_rn(__fadd_rn(x.z, __fmul_rn(v.z, dt)), __fmul_rn(__fdiv_rn(fz, m), dt2));
+    v.x = __fmul_rn(p.damping, __fdiv_rn(__fsub_rn(nx, x.x), dt));
+    v.y = __fmul_rn(p.damping, __fdiv_rn(__fsub_rn(ny, x.y), dt));
+    v.z = __fmul_rn(p.damping, __fdiv_rn(__fsub_rn(nz, x.z), dt));
+    x = make_float3(nx, ny, nz);
+}
+
+template <int T, int SPT, int MPT, int MODE, bool TRACK>
 __global__ void __launch_bounds__(T, 1024 / T) step_kernel(const StepParams p) {
+    constexpr bool XPBD = MODE == kModeXpbd;
     extern __shared__ float4 smem4[];
     const int tid = threadIdx.x;
     const float dt = p.dt;
@@ -54,7 +102,7 @@ __global__ void __launch_bounds__(T, 1024 / T) step_kernel(const StepParams p) {
         for (uint32_t i = tid; i < bd.n_inc; i += T) sinc[i] = __ldg(&p.inc[bd.inc_begin + i]);
         float next_rate = 0.0f;  // actuation factor of material tid for the coming step
         if (tid < n_mat) {
-            smat[tid].y = __ldg(&p.invk[tid]);
+            smat[tid].y = __ldg(&p.invk[tid]);  // 1/K (reference step) or k (force modes)
             next_rate = __ldg(&p.rates[tid]);
         }
 
@@ -74,8 +122,9 @@ __global__ void __launch_bounds__(T, 1024 / T) step_kernel(const StepParams p) {
                 if (TRACK) st[j] = p.stress[__ldg(&p.spring_gidx[g])];
             }
         }
-        // Masses of this thread: x, v and the SELL row (offset | width << 20).
+        // Masses of this thread: x, v, mass and the SELL row (offset | width << 20).
         float3 x[MPT], v[MPT];
+        float mass[MPT];
         uint32_t row[MPT];
 #pragma unroll
         for (int j = 0; j < MPT; ++j) {
@@ -83,10 +132,12 @@ __global__ void __launch_bounds__(T, 1024 / T) step_kernel(const StepParams p) {
             x[j] = make_float3(0.f, 0.f, 0.f);
             v[j] = make_float3(0.f, 0.f, 0.f);
             row[j] = 0;
+            mass[j] = 1.0f;
             if (m < bd.n_mass) {
                 const uint32_t g = __ldg(&p.mass_gidx[bd.mass_begin + m]);
                 const float4 P = p.pos[g], V = p.vel[g];
                 x[j] = make_float3(P.x, P.y, P.z);
+                mass[j] = P.w;
                 v[j] = make_float3(V.x, V.y, V.z);
                 const uint32_t sl = bd.slice_begin + m / kSliceWidth;
                 row[j] = (__ldg(&p.slice_off[sl]) + (m % kSliceWidth)) | (__ldg(&p.slice_width[sl]) << 20);
@@ -101,14 +152,18 @@ __global__ void __launch_bounds__(T, 1024 / T) step_kernel(const StepParams p) {
                 smat[tid].x = next_rate;
                 if (step + 1 < p.steps) next_rate = __ldg(&p.rates[(step + 1) * n_mat + tid]);
             }
-            // (1) predict x~ = x + v*dt (sim_kernel.cu:147-152)
+            // (1) reference step: predict x~ = x + v*dt (sim_kernel.cu:147-152);
+            //     force modes: publish the current positions
 #pragma unroll
             for (int j = 0; j < MPT; ++j) {
                 const uint32_t m = tid + j * T;
                 if (m >= bd.n_mass) break;
-                sxt[m] = make_float4(__fadd_rn(x[j].x, __fmul_rn(v[j].x, dt)),
-                                     __fadd_rn(x[j].y, __fmul_rn(v[j].y, dt)),
-                                     __fadd_rn(x[j].z, __fmul_rn(v[j].z, dt)), 0.0f);
+                if (XPBD)
+                    sxt[m] = make_float4(__fadd_rn(x[j].x, __fmul_rn(v[j].x, dt)),
+                                         __fadd_rn(x[j].y, __fmul_rn(v[j].y, dt)),
+                                         __fadd_rn(x[j].z, __fmul_rn(v[j].z, dt)), 0.0f);
+                else
+                    sxt[m] = make_float4(x[j].x, x[j].y, x[j].z, 0.0f);
             }
             __syncthreads();
             // (2) distance constraints (sim_kernel.cu:209-243)
@@ -124,10 +179,13 @@ __global__ void __launch_bounds__(T, 1024 / T) step_kernel(const StepParams p) {
                 const float dz = __fsub_rn(pa.z, pb.z);
                 const float d = __fsqrt_rn(__fmaf_rn(dx, dx, __fmaf_rn(dy, dy, __fmul_rn(dz, dz))));
                 const float r = __frcp_rn(__fadd_rn(d, kEps));
+                // reference step: lambda = -C/K, dp = lambda n (sim_kernel.cu:230-232);
+                // force modes: Hooke force on the a end, -k (d - L) n
                 const float lam = __fmul_rn(-__fsub_rn(d, L), mt.y);
                 const float coef = __fmul_rn(lam, r);
                 sdp[s] = make_float4(__fmul_rn(coef, dx), __fmul_rn(coef, dy), __fmul_rn(coef, dz), 0.0f);
-                if (TRACK) st[j] = __fadd_rn(st[j], __fmul_rn(lam, __frcp_rn(lb[j])));
+                // stress: lambda/Lbar (reference, sim_kernel.cu:234); k (d - L)/Lbar (force)
+                if (TRACK) st[j] = __fadd_rn(st[j], __fmul_rn(XPBD ? lam : -lam, __frcp_rn(lb[j])));
             }
             __syncthreads();
             // (3) gather in summation order and integrate (sim_kernel.cu:246-268).
@@ -150,15 +208,19 @@ __global__ void __launch_bounds__(T, 1024 / T) step_kernel(const StepParams p) {
                         az = __fmaf_rn(c.z, sg, az);
                     }
                 }
-                const float4 xt = sxt[m];
-                const float nx = __fadd_rn(xt.x, ax);
-                const float ny = __fadd_rn(xt.y, ay);
-                const float nz = __fadd_rn(xt.z, az);
-                // v = 0.99*(x~ - x)/dt in double (sim_kernel.cu:265-267)
-                v[j].x = __double2float_rn(__ddiv_rn(__dmul_rn(0.99, (double)__fsub_rn(nx, x[j].x)), ddt));
-                v[j].y = __double2float_rn(__ddiv_rn(__dmul_rn(0.99, (double)__fsub_rn(ny, x[j].y)), ddt));
-                v[j].z = __double2float_rn(__ddiv_rn(__dmul_rn(0.99, (double)__fsub_rn(nz, x[j].z)), ddt));
-                x[j] = make_float3(nx, ny, nz);
+                if (XPBD) {
+                    const float4 xt = sxt[m];
+                    const float nx = __fadd_rn(xt.x, ax);
+                    const float ny = __fadd_rn(xt.y, ay);
+                    const float nz = __fadd_rn(xt.z, az);
+                    // v = 0.99*(x~ - x)/dt in double (sim_kernel.cu:265-267)
+                    v[j].x = __double2float_rn(__ddiv_rn(__dmul_rn(0.99, (double)__fsub_rn(nx, x[j].x)), ddt));
+                    v[j].y = __double2float_rn(__ddiv_rn(__dmul_rn(0.99, (double)__fsub_rn(ny, x[j].y)), ddt));
+                    v[j].z = __double2float_rn(__ddiv_rn(__dmul_rn(0.99, (double)__fsub_rn(nz, x[j].z)), ddt));
+                    x[j] = make_float3(nx, ny, nz);
+                } else {
+                    force_integrate<MODE>(p, x[j], v[j], mass[j], ax, ay, az);
+                }
             }
         }
 
@@ -194,7 +256,7 @@ __global__ void __launch_bounds__(256) actuation_kernel(const float4* __restrict
                                                         const uint8_t* __restrict__ mat_ids,
                                                         const uint32_t* __restrict__ n_mat_ptr,
                                                         float t0, float dt, uint32_t steps,
-                                                        float* __restrict__ rates,
+                                                        uint32_t mode, float* __restrict__ rates,
                                                         float* __restrict__ invk) {
     __shared__ float s_t[256];
     const uint32_t n_mat = *n_mat_ptr;
@@ -210,9 +272,13 @@ __global__ void __launch_bounds__(256) actuation_kernel(const float4* __restrict
     if (blockIdx.x == 0) {
         for (uint32_t i = threadIdx.x; i < n_mat; i += 256u) {
             const float4 mt = table[mat_ids[i]];
-            // alpha = 1/k/dt/dt, K = 2 + alpha (sim_kernel.cu:220, 225)
-            const float alpha = __fdiv_rn(__fdiv_rn(__fdiv_rn(1.0f, mt.x), dt), dt);
-            invk[i] = __frcp_rn(__fadd_rn(2.0f, alpha));
+            if (mode == kModeXpbd) {
+                // alpha = 1/k/dt/dt, K = 2 + alpha (sim_kernel.cu:220, 225)
+                const float alpha = __fdiv_rn(__fdiv_rn(__fdiv_rn(1.0f, mt.x), dt), dt);
+                invk[i] = __frcp_rn(__fadd_rn(2.0f, alpha));
+            } else {
+                invk[i] = mt.x;
+            }
         }
     }
     __syncthreads();
@@ -280,14 +346,23 @@ using StepFn = void (*)(const StepParams);
 
 struct ShapeEntry {
     uint32_t threads, spt, mpt;
-    StepFn fn[2];  // [track]
+    StepFn fn[3][2];  // [mode][track]
 };
 
-#define MB_SHAPE(T, S, M) {T, S, M, {step_kernel<T, S, M, false>, step_kernel<T, S, M, true>}}
+#define MB_SHAPE(T, S, M)                                                                     \
+    {                                                                                         \
+        T, S, M, {                                                                            \
+            {step_kernel<T, S, M, kModeXpbd, false>, step_kernel<T, S, M, kModeXpbd, true>},  \
+                {step_kernel<T, S, M, kModeForceLand, false>,                                 \
+                 step_kernel<T, S, M, kModeForceLand, true>},                                 \
+                {step_kernel<T, S, M, kModeForceWater, false>,                                \
+                 step_kernel<T, S, M, kModeForceWater, true>},                                \
+        }                                                                                     \
+    }
 const ShapeEntry kShapes[] = {
-    MB_SHAPE(256, 8, 2),   MB_SHAPE(256, 16, 4),  MB_SHAPE(512, 4, 1),  MB_SHAPE(512, 8, 2),
-    MB_SHAPE(512, 12, 2),  MB_SHAPE(512, 16, 4),  MB_SHAPE(1024, 4, 1), MB_SHAPE(1024, 6, 2),
-    MB_SHAPE(1024, 8, 2),  MB_SHAPE(1024, 10, 2), MB_SHAPE(1024, 12, 2),
+    MB_SHAPE(256, 8, 2),  MB_SHAPE(512, 4, 1),   MB_SHAPE(512, 8, 2),   MB_SHAPE(512, 16, 4),
+    MB_SHAPE(1024, 4, 1), MB_SHAPE(1024, 6, 2),  MB_SHAPE(1024, 8, 2),  MB_SHAPE(1024, 10, 2),
+    MB_SHAPE(1024, 12, 2),
 };
 #undef MB_SHAPE
 
@@ -311,17 +386,17 @@ uint32_t max_step_smem(int device) {
 
 bool shape_supported(const KernelShape& shape) { return find_shape(shape) != nullptr; }
 
-cudaError_t prepare_step(const KernelShape& shape, bool track, uint32_t smem_bytes) {
+cudaError_t prepare_step(const KernelShape& shape, uint32_t mode, bool track, uint32_t smem_bytes) {
     const ShapeEntry* e = find_shape(shape);
-    if (!e) return cudaErrorInvalidValue;
-    return cudaFuncSetAttribute(e->fn[track ? 1 : 0], cudaFuncAttributeMaxDynamicSharedMemorySize,
+    if (!e || mode > kModeForceWater) return cudaErrorInvalidValue;
+    return cudaFuncSetAttribute(e->fn[mode][track ? 1 : 0], cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)smem_bytes);
 }
 
-int ctas_per_sm(const KernelShape& shape, bool track, uint32_t smem_bytes) {
+int ctas_per_sm(const KernelShape& shape, uint32_t mode, bool track, uint32_t smem_bytes) {
     const ShapeEntry* e = find_shape(shape);
-    if (!e) return 0;
-    StepFn fn = e->fn[track ? 1 : 0];
+    if (!e || mode > kModeForceWater) return 0;
+    StepFn fn = e->fn[mode][track ? 1 : 0];
     if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes) != cudaSuccess)
         return 0;
     int n = 0;
@@ -334,15 +409,17 @@ cudaError_t launch_step(const StepParams& p, const KernelShape& shape, cudaStrea
     const ShapeEntry* e = find_shape(shape);
     if (!e) return cudaErrorInvalidValue;
     if (p.n_bins == 0) return cudaSuccess;
-    e->fn[p.track ? 1 : 0]<<<p.n_bins, shape.threads, p.smem_bytes, s>>>(p);
+    if (p.mode > kModeForceWater) return cudaErrorInvalidValue;
+    e->fn[p.mode][p.track ? 1 : 0]<<<p.n_bins, shape.threads, p.smem_bytes, s>>>(p);
     return cudaGetLastError();
 }
 
 cudaError_t launch_actuation(const float4* table, const uint8_t* mat_ids, const uint32_t* n_mat,
-                             float t0, float dt, uint32_t steps, float* rates, float* invk,
-                             cudaStream_t s) {
+                             float t0, float dt, uint32_t steps, uint32_t mode, float* rates,
+                             float* coef, cudaStream_t s) {
     if (steps == 0) return cudaSuccess;
-    actuation_kernel<<<(steps + 255) / 256, 256, 0, s>>>(table, mat_ids, n_mat, t0, dt, steps, rates, invk);
+    actuation_kernel<<<(steps + 255) / 256, 256, 0, s>>>(table, mat_ids, n_mat, t0, dt, steps, mode,
+                                                         rates, coef);
     return cudaGetLastError();
 }
 

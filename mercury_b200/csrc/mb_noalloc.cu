@@ -318,14 +318,15 @@ extern "C" mb_status mb_simulate_robot_noalloc(void* stream, const float* table,
     p.track = track_stresses ? 1u : 0u;
     p.smem_bytes = bin_smem_bytes(n_masses, n_springs, kNaMaxIncidence);
     if (p.smem_bytes > max_step_smem(device)) return MB_ERR_CAPACITY;
-    if (prepare_step(shape, p.track != 0, p.smem_bytes) != cudaSuccess) return MB_ERR_CUDA;
+    p.mode = kModeXpbd;
+    if (prepare_step(shape, kModeXpbd, p.track != 0, p.smem_bytes) != cudaSuccess) return MB_ERR_CUDA;
     float t = t0;
     uint32_t done = 0;
     while (done < steps) {
         const uint32_t n = steps - done < kNaChunk ? steps - done : kNaChunk;
         if (launch_actuation(reinterpret_cast<const float4*>(table),
                              reinterpret_cast<const uint8_t*>(sc + kOffMatIds), p.n_mat, t, dt, n,
-                             reinterpret_cast<float*>(sc + kOffRates),
+                             kModeXpbd, reinterpret_cast<float*>(sc + kOffRates),
                              reinterpret_cast<float*>(sc + kOffInvK), st) != cudaSuccess)
             return MB_ERR_CUDA;
         p.t0 = t;

@@ -67,3 +67,32 @@ def material_table() -> np.ndarray:
             b = np.array(_base(j), np.float64).astype(np.float32).astype(np.float64)
             t[composite_id(i, j)] = ((a + b) / 2.0).astype(np.float32)
     return t
+
+
+# Materials of the force-based benchmark configurations: stiffness bone
+# 1e5, tissue 1e4, muscles 1e4 N/m; muscle rest length L0 (1 + 0.14 sin(2 pi
+# 2 Hz t + phi)) with phi = 0 (muscle_a) and pi (muscle_b).  Composite
+# springs average their two materials as the reference does
+# (material.h:215-227); base materials the configurations do not use keep
+# the reference's values.
+FORCE_BASE = {
+    BONE: (1.0e5, 0.0, 2.0 * math.pi * 2.0, 0.0),
+    TISSUE: (1.0e4, 0.0, 2.0 * math.pi * 2.0, 0.0),
+    ADDUCTOR_MUSCLE0: (1.0e4, 0.14, 2.0 * math.pi * 2.0, 0.0),
+    ABDUCTOR_MUSCLE0: (1.0e4, 0.14, 2.0 * math.pi * 2.0, math.pi),
+}
+
+
+def force_table() -> np.ndarray:
+    """(254, 4) float32 table of the force-based configurations."""
+    def base(i):
+        return FORCE_BASE.get(i, _base(i))
+    t = np.zeros((COMPOSITE_COUNT, 4), np.float32)
+    for i in range(23):
+        t[i] = np.array(base(i), np.float64).astype(np.float32)
+    for i in range(1, 23):
+        a = np.array(base(i), np.float64).astype(np.float32).astype(np.float64)
+        for j in range(i + 1, 23):
+            b = np.array(base(j), np.float64).astype(np.float32).astype(np.float64)
+            t[composite_id(i, j)] = ((a + b) / 2.0).astype(np.float32)
+    return t

@@ -14,7 +14,9 @@ numpy PCG64):
   streamed   64 robots of 10x10x10 cells, all occupied, iid over
              {bone, tissue, muscle_a, muscle_b}
 For the reference step, muscle_a is adductor_muscle0 (phase 0) and muscle_b
-abductor_muscle0 (phase pi), material.h:112, 122.
+abductor_muscle0 (phase pi), material.h:112, 122.  The force-based
+configurations give every mass 0.1 kg (population(..., mass=0.1)) and use
+materials.force_table().
 """
 from __future__ import annotations
 
@@ -32,19 +34,18 @@ FIVE_P = np.array([0.3, 0.175, 0.175, 0.175, 0.175])
 FOUR = np.array([BONE, TISSUE, ADDUCTOR_MUSCLE0, ABDUCTOR_MUSCLE0], np.uint8)
 
 
-def voxel_robot(cells: np.ndarray, h: float = CELL) -> Element:
-    """Robot from a (nz, ny, nx)... cell grid given as a cubic array of base
-    material ids indexed [x, y, z]; one extra air layer closes the upper
-    faces."""
+def voxel_robot(cells: np.ndarray, h: float = CELL, mass: float = 1.0) -> Element:
+    """Robot from a grid of cells (base material ids indexed [x, y, z]); an
+    extra air layer of grid points closes the upper faces."""
     cells = np.asarray(cells, np.uint8)
     sx, sy, sz = cells.shape
     nx, ny, nz = sx + 1, sy + 1, sz + 1
     grid = np.zeros((nx, ny, nz), np.uint8)
     grid[:sx, :sy, :sz] = cells
-    return lattice_robot(grid, h)
+    return lattice_robot(grid, h, mass)
 
 
-def lattice_robot(grid: np.ndarray, h: float = CELL) -> Element:
+def lattice_robot(grid: np.ndarray, h: float = CELL, mass: float = 1.0) -> Element:
     """Robot from a grid of points indexed [x, y, z] (mb_voxel_build)."""
     grid = np.asarray(grid, np.uint8)
     nx, ny, nz = grid.shape
@@ -61,14 +62,16 @@ def lattice_robot(grid: np.ndarray, h: float = CELL) -> Element:
                                  _lib.ptr(sm))
     _lib.check(st)
     s = ns.value
-    return Element(pos.reshape(n, 3), mm, pairs[: 2 * s].reshape(s, 2), lbar[:s], sm[:s])
+    return Element(pos.reshape(n, 3), mm, pairs[: 2 * s].reshape(s, 2), lbar[:s], sm[:s],
+                   mass=np.full(n, mass, np.float32))
 
 
 def random_cells(side: int, rng: np.random.Generator, choices=FIVE, p=FIVE_P) -> np.ndarray:
     return choices[rng.choice(len(choices), size=(side, side, side), p=p)]
 
 
-def population(name: str, n_robots: int | None = None, seed_base: int | None = None) -> list[Element]:
+def population(name: str, n_robots: int | None = None, seed_base: int | None = None,
+               mass: float = 1.0) -> list[Element]:
     """One of the named synthetic populations (see module docstring)."""
     spec = {
         "small": (0, 32),
@@ -90,9 +93,10 @@ def population(name: str, n_robots: int | None = None, seed_base: int | None = N
             cells = random_cells(side, rng)
         else:
             cells = FOUR[rng.integers(0, 4, size=(10, 10, 10))]
-        out.append(voxel_robot(cells))
+        out.append(voxel_robot(cells, mass=mass))
     return out
 
 
-def population_batch(name: str, n_robots: int | None = None, seed_base: int | None = None):
-    return pack(population(name, n_robots, seed_base))
+def population_batch(name: str, n_robots: int | None = None, seed_base: int | None = None,
+                     mass: float = 1.0):
+    return pack(population(name, n_robots, seed_base, mass))

@@ -29,6 +29,17 @@ from .materials import material_table
 
 ENVIRONMENT_LAND, ENVIRONMENT_WATER = 0, 1
 
+MODE_REF_XPBD, MODE_FORCE_LAND, MODE_FORCE_WATER = 0, 1, 2
+
+# Environments of the force-based benchmark configurations (land: g, the
+# reference's floor stiffness 1e6 (environment.h:15-22), mu_s 1.0, mu_k 0.8;
+# water: buoyancy cancels gravity, 0.5 rho Cd A = 0.5 * 1000 * 1 * 1e-4);
+# velocity damping 0.999 per step.
+LAND = dict(g=9.81, floor_stiffness=1.0e6, friction_static=1.0, friction_kinetic=0.8, drag=0.0,
+            damping=0.999)
+WATER = dict(g=0.0, floor_stiffness=0.0, friction_static=0.0, friction_kinetic=0.0,
+             drag=0.5 * 1000.0 * 1.0 * 1e-4, damping=0.999)
+
 
 @dataclass
 class SimulatorConfig:
@@ -123,6 +134,26 @@ class Simulator:
         _lib.check(_lib.LIB.mb_set_total_time(self._ctx, 0.0), self._ctx)
 
     # -- array-level interface ---------------------------------------------
+    def set_mode(self, mode: int) -> None:
+        """MODE_REF_XPBD (the reference step), MODE_FORCE_LAND or MODE_FORCE_WATER."""
+        _lib.check(_lib.LIB.mb_set_mode(self._ctx, int(mode)), self._ctx)
+
+    def set_environment(self, **kw) -> None:
+        env = _lib.Environment()
+        _lib.check(_lib.LIB.mb_get_environment(self._ctx, ctypes.byref(env)), self._ctx)
+        for k, v in kw.items():
+            setattr(env, k, float(v))
+        _lib.check(_lib.LIB.mb_set_environment(self._ctx, ctypes.byref(env)), self._ctx)
+
+    def environment(self) -> dict:
+        env = _lib.Environment()
+        _lib.check(_lib.LIB.mb_get_environment(self._ctx, ctypes.byref(env)), self._ctx)
+        return {f: getattr(env, f) for f, _ in env._fields_}
+
+    def set_materials(self, table: np.ndarray) -> None:
+        self._table = np.ascontiguousarray(table, np.float32)
+        _lib.check(_lib.LIB.mb_set_materials(self._ctx, _lib.ptr(self._table)), self._ctx)
+
     def set_batch(self, batch: Batch) -> None:
         self._batch = batch
         d = _lib.BatchDesc(

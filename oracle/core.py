@@ -42,6 +42,10 @@ def lib() -> ctypes.CDLL:
         L.or_com_device.restype = None
         L.or_com_reference.argtypes = [I32, P, P, P, P]
         L.or_com_reference.restype = None
+        L.or_force_run.argtypes = [I32, I32, P, P, P, P, P, P, P, P, P, P, F32, F32, U32, I32, I32]
+        L.or_force_run.restype = I32
+        L.or_force_run_f64.argtypes = [I32, I32, P, P, P, P, P, P, P, P, P, F64, F64, U32]
+        L.or_force_run_f64.restype = I32
         L.or_max_threads.argtypes = []
         L.or_max_threads.restype = I32
         _lib = L
@@ -113,3 +117,26 @@ def com_reference(batch, pos) -> np.ndarray:
     lib().or_com_reference(batch.n_robots, _p(batch.mass_offsets), _p(np.ascontiguousarray(pos, np.float32)),
                            _p(batch.mass_material), _p(com))
     return com
+
+
+def force_run(mode, batch, pos, vel, stress, table, env, dt, t0, steps, track, threads=0):
+    """Force modes (1 land, 2 water), FP32, in place.  env = (g, floor
+    stiffness, mu_s, mu_k, drag, damping)."""
+    assert pos.dtype == np.float32 and vel.dtype == np.float32
+    table = np.ascontiguousarray(table, np.float32)
+    envf = np.ascontiguousarray(env, np.float32)
+    rc = lib().or_force_run(mode, batch.n_robots, _p(batch.mass_offsets), _p(pos), _p(vel),
+                            _p(batch.spring_offsets), _p(batch.pairs), _p(batch.spring_material),
+                            _p(batch.lbar), _p(stress), _p(table), _p(envf), dt, t0, steps,
+                            int(bool(track)), threads)
+    assert rc == 0
+
+
+def force_run_f64(mode, batch, pos, vel, table, env, dt, t0, steps):
+    assert pos.dtype == np.float64 and vel.dtype == np.float64
+    lbar = np.ascontiguousarray(batch.lbar, np.float64)
+    rc = lib().or_force_run_f64(mode, batch.n_robots, _p(batch.mass_offsets), _p(pos), _p(vel),
+                                _p(batch.spring_offsets), _p(batch.pairs), _p(batch.spring_material),
+                                _p(lbar), _p(np.ascontiguousarray(table, np.float32)),
+                                _p(np.ascontiguousarray(env, np.float64)), dt, t0, steps)
+    assert rc == 0

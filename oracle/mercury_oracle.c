@@ -386,6 +386,206 @@ int or_xpbd_run_f64(int n_robots, const int64_t* mass_off, double* pos, double* 
     return 0;
 }
 
+
+/* ------------------------------------------------------------------ */
+/* Force modes (no reference code: restated from the paper's Algorithm 1,
+ * mercury_fall_2023.pdf section II.B, and the benchmark configurations):
+ * Hooke springs F_a = -k (d - L) n, n = (x_a - x_b)/d, L = Lbar (1 + dL0
+ * sin(omega t + phi)); per mass, mode 1 (land): gravity -m g along z, a
+ * penalty ground below z = 0 with normal force fn = k_floor (-z) and
+ * Coulomb friction on the horizontal velocity h = v + (F_h/m) dt the step
+ * would reach -- static (F_h = -m v_h / dt) when |h| <= mu_s fn dt / m,
+ * else kinetic mu_k fn against h; mode 2 (water): drag -c |v| v.  Then
+ * x' = x + v dt + (F/m) dt^2, v' = damping (x' - x)/dt.  Stress accumulates
+ * k (d - L)/Lbar.  The same fixed gather order as the reference step.
+ * env = {g, floor_stiffness, mu_s, mu_k, drag, damping}; m = pos.w. */
+static void force_robot_f32(int mode, int nm, float* pos, float* vel, int ns,
+                            const uint16_t* pairs, const uint8_t* mat,
+                            const float* lbar, float* stress,
+                            const float* table, const float* env, float dt, float t0,
+                            uint32_t steps, int track) {
+    int* deg = (int*)calloc((size_t)nm + 1, sizeof(int));
+    for (int s = 0; s < ns; ++s) {
+        if (!mat[s]) continue;
+        deg[pairs[2 * s] + 1]++;
+        deg[pairs[2 * s + 1] + 1]++;
+    }
+    for (int i = 0; i < nm; ++i) deg[i + 1] += deg[i];
+    int* inc = (int*)malloc(sizeof(int) * (size_t)(deg[nm] + 1));
+    int* fill = (int*)malloc(sizeof(int) * (size_t)(nm + 1));
+    memcpy(fill, deg, sizeof(int) * (size_t)nm);
+    for (int s = 0; s < ns; ++s) {
+        if (!mat[s]) continue;
+        inc[fill[pairs[2 * s]]++] = 2 * s;
+        inc[fill[pairs[2 * s + 1]]++] = 2 * s + 1;
+    }
+    for (int i = 0; i < nm; ++i)
+        for (int e = deg[i] + 1; e < deg[i + 1]; ++e) {
+            int h = inc[e], k = e - 1;
+            while (k >= deg[i] && inc_after(inc[k], h, pairs)) { inc[k + 1] = inc[k]; --k; }
+            inc[k + 1] = h;
+        }
+    float* f = (float*)malloc(sizeof(float) * 3 * (size_t)(ns + 1));
+    float rc[OR_COMPOSITE_COUNT];
+    const float g = env[0], kfl = env[1], mus = env[2], muk = env[3], cdrag = env[4], damp = env[5];
+    volatile float t = t0;
+    for (uint32_t step = 0; step < steps; ++step) {
+        float tn = t;
+        for (int m = 0; m < OR_COMPOSITE_COUNT; ++m) {
+            float arg = fmaf(table[4 * m + 2], tn, table[4 * m + 3]);
+            rc[m] = table[4 * m + 1] * (float)or_sin((double)arg);
+        }
+        for (int s = 0; s < ns; ++s) {
+            int m = mat[s];
+            if (!m) continue;
+            int a = pairs[2 * s], b = pairs[2 * s + 1];
+            float L = fmaf(lbar[s], rc[m], lbar[s]);
+            float dx = pos[4 * a] - pos[4 * b];
+            float dy = pos[4 * a + 1] - pos[4 * b + 1];
+            float dz = pos[4 * a + 2] - pos[4 * b + 2];
+            float d = sqrtf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
+            float r = 1.0f / (d + OR_EPS);
+            float lam = (-(d - L)) * table[4 * m];
+            float coef = lam * r;
+            f[3 * s] = coef * dx;
+            f[3 * s + 1] = coef * dy;
+            f[3 * s + 2] = coef * dz;
+            if (track) stress[s] = stress[s] + (-lam) * (1.0f / lbar[s]);
+        }
+        for (int i = 0; i < nm; ++i) {
+            float F[3] = {0.0f, 0.0f, 0.0f};
+            for (int e = deg[i]; e < deg[i + 1]; ++e) {
+                int h = inc[e], s = h >> 1;
+                for (int c = 0; c < 3; ++c) F[c] = (h & 1) ? F[c] - f[3 * s + c] : F[c] + f[3 * s + c];
+            }
+            float* x = pos + 4 * i;
+            float* v = vel + 4 * i;
+            float mass = x[3];
+            if (mode == 1) {
+                F[2] = F[2] - mass * g;
+                if (x[2] < 0.0f) {
+                    float fn = kfl * (-x[2]);
+                    F[2] = F[2] + fn;
+                    float hx = v[0] + (F[0] / mass) * dt;
+                    float hy = v[1] + (F[1] / mass) * dt;
+                    float hs = sqrtf(fmaf(hx, hx, hy * hy));
+                    float budget = (fn / mass) * dt;
+                    if (hs <= mus * budget) {
+                        F[0] = ((-mass) * v[0]) / dt;
+                        F[1] = ((-mass) * v[1]) / dt;
+                    } else {
+                        float sc = (muk * fn) / hs;
+                        F[0] = F[0] - sc * hx;
+                        F[1] = F[1] - sc * hy;
+                    }
+                }
+            } else {
+                float sp = sqrtf(fmaf(v[0], v[0], fmaf(v[1], v[1], v[2] * v[2])));
+                float c = cdrag * sp;
+                for (int q = 0; q < 3; ++q) F[q] = F[q] - c * v[q];
+            }
+            float dt2 = dt * dt;
+            for (int q = 0; q < 3; ++q) {
+                float xn = (x[q] + v[q] * dt) + (F[q] / mass) * dt2;
+                v[q] = damp * ((xn - x[q]) / dt);
+                x[q] = xn;
+            }
+        }
+        t = t + dt;
+    }
+    free(deg); free(inc); free(fill); free(f);
+}
+
+int or_force_run(int mode, int n_robots, const int64_t* mass_off, float* pos, float* vel,
+                 const int64_t* spring_off, const uint16_t* pairs, const uint8_t* mat,
+                 const float* lbar, float* stress, const float* table, const float* env,
+                 float dt, float t0, uint32_t steps, int track, int threads) {
+    if (mode != 1 && mode != 2) return -1;
+#ifdef _OPENMP
+    if (threads > 0) omp_set_num_threads(threads);
+#pragma omp parallel for schedule(dynamic, 1)
+#endif
+    for (int r = 0; r < n_robots; ++r) {
+        int64_t m0 = mass_off[r], s0 = spring_off[r];
+        force_robot_f32(mode, (int)(mass_off[r + 1] - m0), pos + 4 * m0, vel + 4 * m0,
+                        (int)(spring_off[r + 1] - s0), pairs + 2 * s0, mat + s0, lbar + s0,
+                        stress ? stress + s0 : NULL, table, env, dt, t0, steps, track && stress);
+    }
+    return 0;
+}
+
+/* FP64 transcription of the force modes (libm sin/sqrt), for drift. */
+static void force_robot_f64(int mode, int nm, double* pos, double* vel, int ns,
+                            const uint16_t* pairs, const uint8_t* mat, const double* lbar,
+                            const float* table, const double* env, double dt, double t0,
+                            uint32_t steps) {
+    double* F = (double*)malloc(sizeof(double) * 3 * (size_t)(nm + 1));
+    const double g = env[0], kfl = env[1], mus = env[2], muk = env[3], cdrag = env[4], damp = env[5];
+    for (uint32_t step = 0; step < steps; ++step) {
+        double tn = t0 + dt * (double)step;
+        memset(F, 0, sizeof(double) * 3 * (size_t)nm);
+        for (int s = 0; s < ns; ++s) {
+            int m = mat[s];
+            if (!m) continue;
+            int a = pairs[2 * s], b = pairs[2 * s + 1];
+            double L = lbar[s] * (1.0 + (double)table[4 * m + 1] * sin((double)table[4 * m + 2] * tn + (double)table[4 * m + 3]));
+            double dx = pos[4 * a] - pos[4 * b], dy = pos[4 * a + 1] - pos[4 * b + 1], dz = pos[4 * a + 2] - pos[4 * b + 2];
+            double d = sqrt(dx * dx + dy * dy + dz * dz);
+            double c = -(double)table[4 * m] * (d - L) / (d + 1e-12);
+            F[3 * a] += c * dx; F[3 * a + 1] += c * dy; F[3 * a + 2] += c * dz;
+            F[3 * b] -= c * dx; F[3 * b + 1] -= c * dy; F[3 * b + 2] -= c * dz;
+        }
+        for (int i = 0; i < nm; ++i) {
+            double* x = pos + 4 * i;
+            double* v = vel + 4 * i;
+            double* Fi = F + 3 * i;
+            double mass = x[3];
+            if (mode == 1) {
+                Fi[2] -= mass * g;
+                if (x[2] < 0.0) {
+                    double fn = kfl * (-x[2]);
+                    Fi[2] += fn;
+                    double hx = v[0] + Fi[0] / mass * dt, hy = v[1] + Fi[1] / mass * dt;
+                    double hs = sqrt(hx * hx + hy * hy);
+                    if (hs <= mus * fn / mass * dt) {
+                        Fi[0] = -mass * v[0] / dt;
+                        Fi[1] = -mass * v[1] / dt;
+                    } else {
+                        Fi[0] -= muk * fn * hx / hs;
+                        Fi[1] -= muk * fn * hy / hs;
+                    }
+                }
+            } else {
+                double sp = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+                for (int q = 0; q < 3; ++q) Fi[q] -= cdrag * sp * v[q];
+            }
+            for (int q = 0; q < 3; ++q) {
+                double xn = x[q] + v[q] * dt + Fi[q] / mass * dt * dt;
+                v[q] = damp * (xn - x[q]) / dt;
+                x[q] = xn;
+            }
+        }
+    }
+    free(F);
+}
+
+int or_force_run_f64(int mode, int n_robots, const int64_t* mass_off, double* pos, double* vel,
+                     const int64_t* spring_off, const uint16_t* pairs, const uint8_t* mat,
+                     const double* lbar, const float* table, const double* env, double dt,
+                     double t0, uint32_t steps) {
+    if (mode != 1 && mode != 2) return -1;
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 1)
+#endif
+    for (int r = 0; r < n_robots; ++r) {
+        int64_t m0 = mass_off[r], s0 = spring_off[r];
+        force_robot_f64(mode, (int)(mass_off[r + 1] - m0), pos + 4 * m0, vel + 4 * m0,
+                        (int)(spring_off[r + 1] - s0), pairs + 2 * s0, mat + s0, lbar + s0,
+                        table, env, dt, t0, steps);
+    }
+    return 0;
+}
+
 /* ------------------------------------------------------------------ */
 /* Centre of mass of the non-air masses of each robot.
  *
