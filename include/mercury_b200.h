@@ -91,7 +91,10 @@ typedef struct mb_batch_desc {
 } mb_batch_desc;
 
 /* Launch configuration of the step kernel.  threads: CTA size; bins: number
- * of robot groups, each simulated by one CTA; chunk: steps per launch. */
+ * of robot groups, each simulated by one CTA; chunk: steps per launch;
+ * streamed: 1 = keep only positions in shared memory and stream springs,
+ * rows and per-spring scratch through global memory (one robot per CTA; used
+ * automatically when a robot does not fit a resident bin). */
 typedef struct mb_launch_config {
     uint32_t threads;
     uint32_t springs_per_thread;
@@ -99,6 +102,7 @@ typedef struct mb_launch_config {
     uint32_t bins;
     uint32_t chunk;
     uint32_t use_graph;
+    uint32_t streamed;
 } mb_launch_config;
 
 /* Creates a context on CUDA device `device` with its own stream.

@@ -60,6 +60,7 @@ class LaunchConfig(ctypes.Structure):
         ("bins", ctypes.c_uint32),
         ("chunk", ctypes.c_uint32),
         ("use_graph", ctypes.c_uint32),
+        ("streamed", ctypes.c_uint32),
     ]
 
 

@@ -132,6 +132,12 @@ struct mb_context {
     mb::DevBuf<mb::BinDesc> bins;
     mb::DevBuf<uint32_t> mass_gidx, spring_gidx, spring_pair, slice_off, slice_width;
     mb::DevBuf<uint16_t> inc;
+    // streamed path: one robot per CTA, rows with u32 entries, per-spring scratch
+    bool streamed = false;
+    uint32_t stream_mpt = 2;
+    mb::DevBuf<uint32_t> inc32;
+    mb::DevBuf<float4> dp_scratch;
+    mb::DevBuf<float> st_scratch;
     mb::DevBuf<float> spring_lbar;
     mb::DevBuf<uint8_t> mat_ids;           // composite ids used by the population
     mb::DevBuf<uint32_t> n_mat;            // their count (device scalar)
@@ -374,12 +380,13 @@ mb_status mb_get_launch_config(const mb_context* ctx, mb_launch_config* cfg) {
     cfg->bins = ctx->n_bins;
     cfg->chunk = ctx->chunk;
     cfg->use_graph = ctx->use_graph ? 1 : 0;
+    cfg->streamed = ctx->streamed ? 1 : 0;
     return MB_OK;
 }
 
 mb_status mb_set_launch_config(mb_context* ctx, const mb_launch_config* cfg) {
     if (!ctx || !cfg) return MB_ERR_ARGUMENT;
-    if (cfg->threads) {
+    if (cfg->threads && !cfg->streamed) {
         mb::KernelShape s{cfg->threads, cfg->springs_per_thread, cfg->masses_per_thread};
         if (!mb::shape_supported(s))
             return fail(ctx, MB_ERR_ARGUMENT, "kernel shape %u/%u/%u not compiled", s.threads,
@@ -484,11 +491,12 @@ mb_status mb_set_elements(mb_context* ctx, const mb_batch_desc* b) {
         std::vector<mb::BinDesc> bins;
         std::vector<uint32_t> mass_gidx, spring_gidx, pair, slice_off, slice_width, robot_bin;
         std::vector<uint16_t> inc;
+        std::vector<uint32_t> inc32;
         std::vector<float> lbar;
         std::vector<uint8_t> mat_ids;
         uint32_t max_smem = 0;
     } out;
-    auto build = [&](const BinPlan& plan, uint32_t nb) {
+    auto build = [&](const BinPlan& plan, uint32_t nb, bool streamed) {
         out = Built();
         out.bins.resize(nb);
         out.robot_bin.resize(R);
@@ -508,7 +516,7 @@ mb_status mb_set_elements(mb_context* ctx, const mb_batch_desc* b) {
             std::memset(&d, 0, sizeof(d));
             d.mass_begin = (uint32_t)out.mass_gidx.size();
             d.spring_begin = (uint32_t)out.spring_gidx.size();
-            d.inc_begin = (uint32_t)out.inc.size();
+            d.inc_begin = (uint32_t)(streamed ? out.inc32.size() : out.inc.size());
             d.slice_begin = (uint32_t)out.slice_off.size();
             (void)slot_of;
             struct Ent {
@@ -566,10 +574,13 @@ mb_status mb_set_elements(mb_context* ctx, const mb_batch_desc* b) {
                 offs.erase(std::unique(offs.begin(), offs.end()), offs.end());
                 const bool aligned = distinct && offs.size() <= w_rank + 4;
                 const uint32_t w = aligned ? (uint32_t)offs.size() : w_rank;
-                out.slice_off.push_back((uint32_t)out.inc.size() - d.inc_begin);
+                const size_t base = streamed ? out.inc32.size() : out.inc.size();
+                out.slice_off.push_back((uint32_t)base - d.inc_begin);
                 out.slice_width.push_back(w);
-                const size_t base = out.inc.size();
-                out.inc.resize(base + (size_t)w * mb::kSliceWidth, mb::kPadEntry);
+                if (streamed)
+                    out.inc32.resize(base + (size_t)w * mb::kSliceWidth, mb::kPadEntry32);
+                else
+                    out.inc.resize(base + (size_t)w * mb::kSliceWidth, mb::kPadEntry);
                 for (uint32_t i = i0; i < i1; ++i)
                     for (uint32_t q = 0; q < rows[i].size(); ++q) {
                         const Ent& e = rows[i][q];
@@ -577,12 +588,16 @@ mb_status mb_set_elements(mb_context* ctx, const mb_batch_desc* b) {
                             aligned ? (uint32_t)(std::lower_bound(offs.begin(), offs.end(),
                                                                   (int)e.other - (int)i) - offs.begin())
                                     : q;
-                        out.inc[base + (size_t)col * mb::kSliceWidth + (i - i0)] =
-                            (uint16_t)((e.packed << 1) | e.sign);
+                        const size_t at = base + (size_t)col * mb::kSliceWidth + (i - i0);
+                        if (streamed)
+                            out.inc32[at] = (e.packed << 1) | e.sign;
+                        else
+                            out.inc[at] = (uint16_t)((e.packed << 1) | e.sign);
                     }
             }
-            d.n_inc = (uint32_t)out.inc.size() - d.inc_begin;
-            out.max_smem = std::max(out.max_smem, mb::bin_smem_bytes(d.n_mass, d.n_spring, d.n_inc));
+            d.n_inc = (uint32_t)(streamed ? out.inc32.size() : out.inc.size()) - d.inc_begin;
+            out.max_smem = std::max(out.max_smem, streamed ? mb::stream_smem_bytes(d.n_mass)
+                                                           : mb::bin_smem_bytes(d.n_mass, d.n_spring, d.n_inc));
         }
     };
 
@@ -615,7 +630,7 @@ mb_status mb_set_elements(mb_context* ctx, const mb_batch_desc* b) {
         }
         for (uint32_t tries = 0; tries < 16; ++tries) {
             if (plan_bins(cost, nm, ns, ninc, nb, sh, smem_cap, plan, smem_needed)) {
-                build(plan, nb);
+                build(plan, nb, false);
                 if (out.max_smem <= smem_cap) {
                     ok = true;
                     break;
@@ -628,6 +643,24 @@ mb_status mb_set_elements(mb_context* ctx, const mb_batch_desc* b) {
             ctx->shape = sh;
             ctx->n_bins = nb;
             break;
+        }
+    }
+    // Streamed path: when forced, or when no resident shape holds the
+    // largest robot.  One robot per bin.
+    bool streamed = false;
+    uint32_t stream_mpt = 2;
+    if (ctx->override_cfg.streamed || !ok) {
+        stream_mpt = max_m <= 2048 ? 2u : 4u;
+        if (max_m <= 4096 && mb::stream_supported(1024, stream_mpt)) {
+            plan.robots.assign(R, {});
+            for (uint32_t r = 0; r < R; ++r) plan.robots[r].push_back(r);
+            build(plan, R, true);
+            if (out.max_smem <= smem_cap) {
+                ok = true;
+                streamed = true;
+                ctx->shape = mb::KernelShape{1024, 0, stream_mpt};
+                ctx->n_bins = R;
+            }
         }
     }
     if (!ok)
@@ -644,6 +677,7 @@ mb_status mb_set_elements(mb_context* ctx, const mb_batch_desc* b) {
     auto& h_slice_off = out.slice_off;
     auto& h_slice_width = out.slice_width;
     auto& h_inc = out.inc;
+    auto& h_inc32 = out.inc32;
     auto& h_mat_ids = out.mat_ids;
     auto& h_robot_bin = out.robot_bin;
 
@@ -676,6 +710,13 @@ mb_status mb_set_elements(mb_context* ctx, const mb_batch_desc* b) {
     MB_CUDA(ctx, up(ctx->slice_off, h_slice_off.data(), h_slice_off.size()));
     MB_CUDA(ctx, up(ctx->slice_width, h_slice_width.data(), h_slice_width.size()));
     MB_CUDA(ctx, up(ctx->inc, h_inc.data(), h_inc.size()));
+    ctx->streamed = streamed;
+    ctx->stream_mpt = stream_mpt;
+    if (streamed) {
+        MB_CUDA(ctx, up(ctx->inc32, h_inc32.data(), h_inc32.size()));
+        MB_CUDA(ctx, ctx->dp_scratch.alloc(std::max<size_t>(h_pair.size(), 1)));
+        MB_CUDA(ctx, ctx->st_scratch.alloc(std::max<size_t>(h_pair.size(), 1)));
+    }
     MB_CUDA(ctx, up(ctx->mat_ids, h_mat_ids.data(), h_mat_ids.size()));
     ctx->n_mat_host = (uint32_t)h_mat_ids.size();
     MB_CUDA(ctx, up(ctx->n_mat, &ctx->n_mat_host, 1));
@@ -732,6 +773,9 @@ mb::StepParams make_params(mb_context* c, float t0, uint32_t steps, bool track) 
     p.track = track ? 1u : 0u;
     p.smem_bytes = c->smem_bytes;
     p.mode = (uint32_t)c->mode;
+    p.inc32 = c->inc32.p;
+    p.dp = c->dp_scratch.p;
+    p.st = c->st_scratch.p;
     p.g = c->env.g;
     p.floor_stiffness = c->env.floor_stiffness;
     p.mu_s = c->env.friction_static;
@@ -760,7 +804,8 @@ cudaError_t issue_chunks(mb_context* c, float t0, uint32_t steps, bool track) {
         mb::StepParams p = make_params(c, t, n, track);
         MB_TRACE("launch bins=%u threads=%u spt=%u mpt=%u smem=%u steps=%u", p.n_bins, c->shape.threads,
                  c->shape.spt, c->shape.mpt, p.smem_bytes, n);
-        cudaError_t e = mb::launch_step(p, c->shape, c->stream);
+        cudaError_t e = c->streamed ? mb::launch_stream(p, 1024, c->stream_mpt, c->stream)
+                                    : mb::launch_step(p, c->shape, c->stream);
         MB_TRACE("launch returned %d", (int)e);
         if (trace_on() && std::getenv("MB_SYNC")) {
             cudaError_t es = cudaStreamSynchronize(c->stream);
@@ -789,7 +834,8 @@ mb_status run(mb_context* c, uint32_t steps, bool track) {
             if (c->graphs.size() >= 16) c->clear_graphs();
             // kernel attributes cannot change inside a capture
             MB_TRACE("prepare");
-            MB_CUDA(c, mb::prepare_step(c->shape, (uint32_t)c->mode, track, c->smem_bytes));
+            MB_CUDA(c, c->streamed ? mb::prepare_stream(1024, c->stream_mpt, (uint32_t)c->mode, track, c->smem_bytes)
+                                    : mb::prepare_step(c->shape, (uint32_t)c->mode, track, c->smem_bytes));
             cudaGraph_t g;
             MB_TRACE("begin capture");
             MB_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
@@ -812,7 +858,8 @@ mb_status run(mb_context* c, uint32_t steps, bool track) {
         MB_TRACE("graph launched");
     } else {
         MB_TRACE("prepare (no graph)");
-        MB_CUDA(c, mb::prepare_step(c->shape, (uint32_t)c->mode, track, c->smem_bytes));
+        MB_CUDA(c, c->streamed ? mb::prepare_stream(1024, c->stream_mpt, (uint32_t)c->mode, track, c->smem_bytes)
+                                    : mb::prepare_step(c->shape, (uint32_t)c->mode, track, c->smem_bytes));
         cudaError_t e = issue_chunks(c, t0, steps, track);
         if (e != cudaSuccess) return cuda_fail(c, e, "step launch");
     }

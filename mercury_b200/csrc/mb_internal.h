@@ -11,6 +11,7 @@ namespace mb {
 // kPadEntry pads rows to the slice width and is skipped by the gather.
 constexpr uint32_t kMaxMaterialSlots = 256;
 constexpr uint16_t kPadEntry = 0xFFFFu;
+constexpr uint32_t kPadEntry32 = 0xFFFFFFFFu;
 constexpr uint32_t kMaxBinSprings = 32767;  // 15-bit spring index in an entry
 constexpr uint32_t kSliceWidth = 32;  // masses per SELL slice (one warp)
 
@@ -53,6 +54,11 @@ struct StepParams {
     uint32_t track;
     uint32_t smem_bytes;
     uint32_t mode;                // 0 reference XPBD, 1 force + land, 2 force + water
+    // streamed kernel only: rows with 32-bit entries (spring << 1 | b end, or
+    // kPadEntry32) and per-spring scratch in packed order
+    const uint32_t* inc32;
+    float4* dp;                   // corrections / forces of the current step
+    float* st;                    // stresses during a launch
     // environment of the force modes
     float g;                      // gravity along -z (land)
     float floor_stiffness;        // penalty stiffness of the ground z = 0 (land)
@@ -89,6 +95,15 @@ cudaError_t launch_step(const StepParams& p, const KernelShape& shape, cudaStrea
 // Resident CTAs per SM of a kernel variant with `smem_bytes` of dynamic
 // shared memory (0 if the shape is not compiled or does not fit).
 int ctas_per_sm(const KernelShape& shape, uint32_t mode, bool track, uint32_t smem_bytes);
+
+// Streamed variant for bins whose springs do not fit in shared memory:
+// only predicted positions live in shared memory; springs, rows and the
+// per-spring scratch stream through global memory (L2).
+cudaError_t prepare_stream(uint32_t threads, uint32_t mpt, uint32_t mode, bool track,
+                           uint32_t smem_bytes);
+cudaError_t launch_stream(const StepParams& p, uint32_t threads, uint32_t mpt, cudaStream_t s);
+uint32_t stream_smem_bytes(uint32_t n_mass);
+bool stream_supported(uint32_t threads, uint32_t mpt);
 
 // Shared memory a bin needs, in bytes.
 uint32_t bin_smem_bytes(uint32_t n_mass, uint32_t n_spring, uint32_t n_inc);

@@ -248,6 +248,147 @@ __global__ void __launch_bounds__(T, 1024 / T) step_kernel(const StepParams p) {
     }
 }
 
+
+// Streamed step: one CTA per bin (typically one large robot).  Shared memory
+// holds the predicted positions and the material factors; every step reads
+// the bin's springs and rows from global memory and exchanges the per-spring
+// corrections through a global scratch array (L2-resident), with the same
+// arithmetic and summation order as step_kernel.
+template <int T, int MPT, int MODE, bool TRACK>
+__global__ void __launch_bounds__(T, 1024 / T) stream_kernel(const StepParams p) {
+    constexpr bool XPBD = MODE == kModeXpbd;
+    extern __shared__ float4 smem4[];
+    const int tid = threadIdx.x;
+    const float dt = p.dt;
+    const double ddt = (double)dt;
+
+    for (uint32_t b = blockIdx.x; b < p.n_bins; b += gridDim.x) {
+        const BinDesc bd = p.bins[b];
+        float4* sxt = smem4;
+        float2* smat = reinterpret_cast<float2*>(sxt + bd.n_mass);
+        float4* dp = p.dp + bd.spring_begin;
+        float* stp = p.st + bd.spring_begin;
+        const uint32_t* pair = p.spring_pair + bd.spring_begin;
+        const float* lbar = p.spring_lbar + bd.spring_begin;
+        const uint32_t* inc = p.inc32 + bd.inc_begin;
+        const uint32_t n_mat = *p.n_mat;
+        float next_rate = 0.0f;
+        if (tid < n_mat) {
+            smat[tid].y = __ldg(&p.invk[tid]);
+            next_rate = __ldg(&p.rates[tid]);
+        }
+        if (TRACK)
+            for (uint32_t s = tid; s < bd.n_spring; s += T)
+                stp[s] = p.stress[__ldg(&p.spring_gidx[bd.spring_begin + s])];
+
+        float3 x[MPT], v[MPT];
+        float mass[MPT];
+        uint32_t roff[MPT], rwid[MPT];
+#pragma unroll
+        for (int j = 0; j < MPT; ++j) {
+            const uint32_t m = tid + j * T;
+            x[j] = make_float3(0.f, 0.f, 0.f);
+            v[j] = make_float3(0.f, 0.f, 0.f);
+            mass[j] = 1.0f;
+            roff[j] = 0;
+            rwid[j] = 0;
+            if (m < bd.n_mass) {
+                const uint32_t g = __ldg(&p.mass_gidx[bd.mass_begin + m]);
+                const float4 P = p.pos[g], V = p.vel[g];
+                x[j] = make_float3(P.x, P.y, P.z);
+                v[j] = make_float3(V.x, V.y, V.z);
+                mass[j] = P.w;
+                const uint32_t sl = bd.slice_begin + m / kSliceWidth;
+                roff[j] = __ldg(&p.slice_off[sl]) + (m % kSliceWidth);
+                rwid[j] = __ldg(&p.slice_width[sl]);
+            }
+        }
+        __syncthreads();
+
+        for (uint32_t step = 0; step < p.steps; ++step) {
+            if (tid < n_mat) {
+                smat[tid].x = next_rate;
+                if (step + 1 < p.steps) next_rate = __ldg(&p.rates[(step + 1) * n_mat + tid]);
+            }
+#pragma unroll
+            for (int j = 0; j < MPT; ++j) {
+                const uint32_t m = tid + j * T;
+                if (m >= bd.n_mass) break;
+                if (XPBD)
+                    sxt[m] = make_float4(__fadd_rn(x[j].x, __fmul_rn(v[j].x, dt)),
+                                         __fadd_rn(x[j].y, __fmul_rn(v[j].y, dt)),
+                                         __fadd_rn(x[j].z, __fmul_rn(v[j].z, dt)), 0.0f);
+                else
+                    sxt[m] = make_float4(x[j].x, x[j].y, x[j].z, 0.0f);
+            }
+            __syncthreads();
+            for (uint32_t s = tid; s < bd.n_spring; s += T) {
+                const uint32_t w = __ldg(&pair[s]);
+                const float lb = __ldg(&lbar[s]);
+                const float4 pa = sxt[pk_a(w)], pb = sxt[pk_b(w)];
+                const float2 mt = smat[pk_slot(w)];
+                const float L = __fmaf_rn(lb, mt.x, lb);
+                const float dx = __fsub_rn(pa.x, pb.x);
+                const float dy = __fsub_rn(pa.y, pb.y);
+                const float dz = __fsub_rn(pa.z, pb.z);
+                const float d = __fsqrt_rn(__fmaf_rn(dx, dx, __fmaf_rn(dy, dy, __fmul_rn(dz, dz))));
+                const float r = __frcp_rn(__fadd_rn(d, kEps));
+                const float lam = __fmul_rn(-__fsub_rn(d, L), mt.y);
+                const float coef = __fmul_rn(lam, r);
+                __stcg(&dp[s], make_float4(__fmul_rn(coef, dx), __fmul_rn(coef, dy), __fmul_rn(coef, dz), 0.0f));
+                if (TRACK) stp[s] = __fadd_rn(stp[s], __fmul_rn(XPBD ? lam : -lam, __frcp_rn(lb)));
+            }
+            __syncthreads();
+#pragma unroll
+            for (int j = 0; j < MPT; ++j) {
+                const uint32_t m = tid + j * T;
+                if (m >= bd.n_mass) break;
+                float ax = 0.0f, ay = 0.0f, az = 0.0f;
+                for (uint32_t k = 0; k < rwid[j]; ++k) {
+                    const uint32_t e = __ldg(&inc[roff[j] + k * kSliceWidth]);
+                    if (e != kPadEntry32) {
+                        const float4 c = __ldcg(&dp[e >> 1]);
+                        const float sg = __uint_as_float(0x3f800000u | ((e & 1u) << 31));
+                        ax = __fmaf_rn(c.x, sg, ax);
+                        ay = __fmaf_rn(c.y, sg, ay);
+                        az = __fmaf_rn(c.z, sg, az);
+                    }
+                }
+                if (XPBD) {
+                    const float4 xt = sxt[m];
+                    const float nx = __fadd_rn(xt.x, ax);
+                    const float ny = __fadd_rn(xt.y, ay);
+                    const float nz = __fadd_rn(xt.z, az);
+                    v[j].x = __double2float_rn(__ddiv_rn(__dmul_rn(0.99, (double)__fsub_rn(nx, x[j].x)), ddt));
+                    v[j].y = __double2float_rn(__ddiv_rn(__dmul_rn(0.99, (double)__fsub_rn(ny, x[j].y)), ddt));
+                    v[j].z = __double2float_rn(__ddiv_rn(__dmul_rn(0.99, (double)__fsub_rn(nz, x[j].z)), ddt));
+                    x[j] = make_float3(nx, ny, nz);
+                } else {
+                    force_integrate<MODE>(p, x[j], v[j], mass[j], ax, ay, az);
+                }
+            }
+        }
+
+        bool bad = false;
+#pragma unroll
+        for (int j = 0; j < MPT; ++j) {
+            const uint32_t m = tid + j * T;
+            if (m < bd.n_mass) {
+                const uint32_t g = __ldg(&p.mass_gidx[bd.mass_begin + m]);
+                p.pos[g] = make_float4(x[j].x, x[j].y, x[j].z, p.pos[g].w);
+                p.vel[g] = make_float4(v[j].x, v[j].y, v[j].z, p.vel[g].w);
+                bad |= !(isfinite(x[j].x) && isfinite(x[j].y) && isfinite(x[j].z));
+            }
+        }
+        if (TRACK) {
+            __syncthreads();
+            for (uint32_t s = tid; s < bd.n_spring; s += T)
+                p.stress[__ldg(&p.spring_gidx[bd.spring_begin + s])] = stp[s];
+        }
+        if (__syncthreads_or(bad) && tid == 0) atomicOr(&p.bin_flags[b], 1u);
+    }
+}
+
 // Actuation factors of one launch.  Block b covers steps [256 b, 256 b + 256):
 // thread 0 accumulates the float clock from t0 (the clock is a sequential
 // float sum, Simulator.cu:447, so it is not reassociated), then every thread
@@ -366,6 +507,31 @@ const ShapeEntry kShapes[] = {
 };
 #undef MB_SHAPE
 
+
+struct StreamEntry {
+    uint32_t threads, mpt;
+    StepFn fn[3][2];
+};
+#define MB_STREAM(T, M)                                                                          \
+    {                                                                                            \
+        T, M, {                                                                                  \
+            {stream_kernel<T, M, kModeXpbd, false>, stream_kernel<T, M, kModeXpbd, true>},       \
+                {stream_kernel<T, M, kModeForceLand, false>,                                     \
+                 stream_kernel<T, M, kModeForceLand, true>},                                     \
+                {stream_kernel<T, M, kModeForceWater, false>,                                    \
+                 stream_kernel<T, M, kModeForceWater, true>},                                    \
+        }                                                                                        \
+    }
+// up to threads * MPT masses per bin (2,048 or 4,096 with 1,024 threads)
+const StreamEntry kStream[] = {MB_STREAM(1024, 2), MB_STREAM(1024, 4)};
+#undef MB_STREAM
+
+const StreamEntry* find_stream(uint32_t threads, uint32_t mpt) {
+    for (const auto& e : kStream)
+        if (e.threads == threads && e.mpt == mpt) return &e;
+    return nullptr;
+}
+
 const ShapeEntry* find_shape(const KernelShape& s) {
     for (const auto& e : kShapes)
         if (e.threads == s.threads && e.spt == s.spt && e.mpt == s.mpt) return &e;
@@ -403,6 +569,26 @@ int ctas_per_sm(const KernelShape& shape, uint32_t mode, bool track, uint32_t sm
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, (int)shape.threads, smem_bytes) != cudaSuccess)
         return 0;
     return n;
+}
+
+uint32_t stream_smem_bytes(uint32_t n_mass) { return 16u * n_mass + 8u * kMaxMaterialSlots; }
+
+bool stream_supported(uint32_t threads, uint32_t mpt) { return find_stream(threads, mpt) != nullptr; }
+
+cudaError_t prepare_stream(uint32_t threads, uint32_t mpt, uint32_t mode, bool track,
+                           uint32_t smem_bytes) {
+    const StreamEntry* e = find_stream(threads, mpt);
+    if (!e || mode > kModeForceWater) return cudaErrorInvalidValue;
+    return cudaFuncSetAttribute(e->fn[mode][track ? 1 : 0],
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
+}
+
+cudaError_t launch_stream(const StepParams& p, uint32_t threads, uint32_t mpt, cudaStream_t s) {
+    const StreamEntry* e = find_stream(threads, mpt);
+    if (!e || p.mode > kModeForceWater) return cudaErrorInvalidValue;
+    if (p.n_bins == 0) return cudaSuccess;
+    e->fn[p.mode][p.track ? 1 : 0]<<<p.n_bins, threads, p.smem_bytes, s>>>(p);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_step(const StepParams& p, const KernelShape& shape, cudaStream_t s) {

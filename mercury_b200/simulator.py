@@ -214,8 +214,9 @@ class Simulator:
         return {f: getattr(c, f) for f, _ in c._fields_}
 
     def set_launch_config(self, threads=0, springs_per_thread=0, masses_per_thread=0, bins=0,
-                          chunk=0, use_graph=1) -> None:
-        c = _lib.LaunchConfig(threads, springs_per_thread, masses_per_thread, bins, chunk, use_graph)
+                          chunk=0, use_graph=1, streamed=0) -> None:
+        c = _lib.LaunchConfig(threads, springs_per_thread, masses_per_thread, bins, chunk, use_graph,
+                              streamed)
         _lib.check(_lib.LIB.mb_set_launch_config(self._ctx, ctypes.byref(c)), self._ctx)
 
 

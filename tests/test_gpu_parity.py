@@ -203,3 +203,46 @@ def test_robot_too_large_rejected():
     with pytest.raises(mb.MercuryError) as err:
         mb.Simulator(0).set_batch(mb.pack([e]))
     assert err.value.status == 3
+
+
+# ---------------------------------------------------------------------------
+# Streamed variant: springs, rows and per-spring scratch in global memory.
+
+@pytest.mark.parametrize("track", [False, True])
+def test_streamed_forced_bit_exact(track):
+    b = robots.population_batch("uneven", 20, seed_base=321)
+    _, pos, vel, stress = run_gpu(b, 1e-3, 200, track, cfg=dict(streamed=1, chunk=64))
+    p, v, s = run_oracle(b, 1e-3, 200, track)
+    assert bits_equal(pos, p) and bits_equal(vel, v)
+    if track:
+        assert bits_equal(stress, s)
+
+
+def test_large_robots_use_the_streamed_path():
+    """10x10x10-cell robots (1,331 masses, 14,230 springs) do not fit a
+    resident bin: the library streams them, with the same results."""
+    b = robots.population_batch("streamed", 6)
+    sim, pos, vel, stress = run_gpu(b, 1e-4, 150, True)
+    assert sim.launch_config()["streamed"] == 1
+    p, v, s = run_oracle(b, 1e-4, 150, True)
+    assert bits_equal(pos, p) and bits_equal(vel, v) and bits_equal(stress, s)
+
+
+@pytest.mark.parametrize("mode", [1, 2])
+def test_streamed_force_modes_bit_exact(mode):
+    from mercury_b200 import simulator as S
+    env = S.LAND if mode == 1 else S.WATER
+    b = robots.population_batch("streamed", 3, mass=0.1)
+    sim = mb.Simulator(0)
+    sim.set_materials(mb.materials.force_table())
+    sim.set_mode(mode)
+    sim.set_environment(**env)
+    sim.setTimeStep(1e-4)
+    sim.set_batch(b)
+    sim.run_steps(300, True)
+    pos, vel, stress = sim.collect_arrays()
+    p, v = b.pos.copy(), b.vel.copy()
+    s = np.zeros(b.n_springs, np.float32)
+    keys = ("g", "floor_stiffness", "friction_static", "friction_kinetic", "drag", "damping")
+    core.force_run(mode, b, p, v, s, mb.materials.force_table(), [env[k] for k in keys], 1e-4, 0.0, 300, True)
+    assert bits_equal(pos, p) and bits_equal(vel, v) and bits_equal(stress, s)
