@@ -188,6 +188,10 @@ def run_ours(args, rank, local_rank, world):
     sim = mb.Simulator(local_rank)
     sim.setTimeStep(dt)
     sim.set_batch(batch)
+    tuned = None
+    if not args.no_autotune:
+        from mercury_b200 import autotune
+        tuned = autotune.tune(sim, batch, track=track, steps=300, use_cache=False)
     steps_per_eval = None
 
     stream = torch.cuda.ExternalStream(sim.stream, device=dev)
@@ -288,6 +292,8 @@ def run_ours(args, rank, local_rank, world):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(batch, dt, track)
 
+    extra = {} if args.no_extra else secondary(args, batch, local_rank, dev, hbm_peak)
+
     line = {
         "metric": "spring-updates/s",
         "value": value,
@@ -327,10 +333,69 @@ def run_ours(args, rank, local_rank, world):
         "cpu_baseline": cpu,
         "e2e": {"value": e2e, "unit": "spring-updates/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "steps": e_steps},
-        "gpu_launches": int(launches_per_eval * args.steps),
+        "gpu_launches": int(2 * launches_per_eval * args.steps),
+        "gpu_launches_note": "per chunk of steps: one actuation-table launch and one step launch",
         "clocks": clocks,
+        "autotune": ({"candidates": len(tuned["candidates"]), "chosen": tuned["config"]} if tuned else None),
+        **extra,
     }
     return line
+
+
+def _device_rate(sim, active, steps, track, dev):
+    import torch
+    st = torch.cuda.ExternalStream(sim.stream, device=dev)
+    sim.run_steps(min(200, steps), track)
+    sim.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    sim.run_steps(steps, track)
+    e1.record(st)
+    e1.synchronize()
+    return active * steps / (e0.elapsed_time(e1) / 1e3)
+
+
+def secondary(args, batch, local_rank, dev, hbm_peak):
+    """Beside the headline: the force modes (the benchmark configurations'
+    physics) on the same robots with 0.1 kg masses, and the streamed
+    workload (64 robots of 10x10x10 cells, 1,331 masses and 14,230 springs
+    each, stresses tracked) with its HBM-figure roofline."""
+    import mercury_b200 as mb
+    from mercury_b200 import robots
+    from mercury_b200 import simulator as S
+    out = {}
+    fb = mb.Batch(**{k: getattr(batch, k) for k in ("mass_offsets", "pos", "vel", "mass_material",
+                                                    "spring_offsets", "pairs", "spring_material", "lbar")})
+    fb.pos = batch.pos.copy()
+    fb.pos[:, 3] = 0.1
+    for name, mode, env in (("force_land", S.MODE_FORCE_LAND, S.LAND),
+                            ("force_water", S.MODE_FORCE_WATER, S.WATER)):
+        fs = mb.Simulator(local_rank)
+        fs.set_materials(mb.materials.force_table())
+        fs.set_mode(mode)
+        fs.set_environment(**env)
+        fs.setTimeStep(1e-4)
+        fs.set_batch(fb)
+        rate = _device_rate(fs, fb.active_springs(), 5000, False, dev)
+        p, _, _ = fs.collect_arrays()
+        out[name] = {"value": rate, "unit": "spring-updates/s", "steps": 5000,
+                     "finite": bool(np.isfinite(p).all()), "config": fs.launch_config()}
+        del fs
+    sb = robots.population_batch("streamed", 64, seed_base=4000)
+    ss = mb.Simulator(local_rank)
+    ss.setTimeStep(1e-4)
+    ss.set_batch(sb)
+    act = sb.active_springs()
+    rate = _device_rate(ss, act, 1000, True, dev)
+    hbm_b = HBM_TOPO_B + HBM_STRESS_B + HBM_MASS_B * sb.n_masses / act
+    out["streamed"] = {"value": rate, "unit": "spring-updates/s", "steps": 1000,
+                       "workload": f"64 robots of 10x10x10 cells, {sb.n_masses} masses, {act} springs, "
+                                   f"stresses tracked, reference step, dt=1e-4",
+                       "config": ss.launch_config(),
+                       "roofline": {"bound": "hbm", "achieved": rate * hbm_b / 1e9, "peak": hbm_peak,
+                                    "unit": "GB/s", "frac": rate * hbm_b / 1e9 / hbm_peak,
+                                    "bytes_per_update": hbm_b}}
+    return out
 
 
 def run_reference(args, rank, local_rank, world):
@@ -441,6 +506,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-ref-cuda", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--no-extra", action="store_true", help="skip the force-mode and streamed lines")
     args = ap.parse_args()
 
     from mercury_b200 import dist

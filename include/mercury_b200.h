@@ -191,6 +191,13 @@ MB_API mb_status mb_device_state(mb_context* ctx, void** pos, void** vel, void**
 MB_API mb_status mb_get_launch_config(const mb_context* ctx, mb_launch_config* cfg);
 MB_API mb_status mb_set_launch_config(mb_context* ctx, const mb_launch_config* cfg);
 
+/* Compiled kernel shapes, for autotuners: writes up to `capacity` entries
+ * (threads, springs_per_thread, masses_per_thread; streamed = 1 for the
+ * streamed kernel, whose springs_per_thread is 0) and returns the count.  No
+ * reference counterpart (the reference launches fixed shapes,
+ * sim_kernel.cu:277-304). */
+MB_API uint32_t mb_kernel_shapes(mb_launch_config* out, uint32_t capacity);
+
 /* Builds a voxel-lattice robot (one mass per grid point, 13 forward lattice
  * springs per point, largest 6-connected component kept, shifted so that
  * max x = 0 and min y = 0).  Grid point i = x + y*nx + z*nx*ny carries base

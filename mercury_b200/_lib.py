@@ -96,6 +96,7 @@ def _load() -> ctypes.CDLL:
         "mb_device_state": (I32, [P, ctypes.POINTER(P), ctypes.POINTER(P), ctypes.POINTER(P)]),
         "mb_get_launch_config": (I32, [P, ctypes.POINTER(LaunchConfig)]),
         "mb_set_launch_config": (I32, [P, ctypes.POINTER(LaunchConfig)]),
+        "mb_kernel_shapes": (U32, [ctypes.POINTER(LaunchConfig), U32]),
         "mb_voxel_build": (I32, [I32, I32, I32, F32, P, ctypes.POINTER(I32), ctypes.POINTER(I32), P, P, P, P, P]),
         "mb_version": (ctypes.c_char_p, []),
     }

@@ -1,6 +1,8 @@
 """Builds libmercury_b200.so in-tree for sm_100a with nvcc.
 
-    python -m mercury_b200.build [--force]
+    python mercury_b200/build.py [--force] [-v]
+
+(Run as a file: importing the package loads the library this builds.)
 """
 from __future__ import annotations
 

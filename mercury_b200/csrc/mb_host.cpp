@@ -384,6 +384,23 @@ mb_status mb_get_launch_config(const mb_context* ctx, mb_launch_config* cfg) {
     return MB_OK;
 }
 
+uint32_t mb_kernel_shapes(mb_launch_config* out, uint32_t capacity) {
+    mb::KernelShape tmp[64];
+    const uint32_t nr = mb::list_shapes(tmp, 64, false);
+    const uint32_t ns = mb::list_shapes(tmp + std::min<uint32_t>(nr, 64), 64 - std::min<uint32_t>(nr, 64), true);
+    const uint32_t n = std::min<uint32_t>(nr + ns, 64);
+    for (uint32_t i = 0; i < n && out && i < capacity; ++i) {
+        mb_launch_config c{};
+        c.threads = tmp[i].threads;
+        c.springs_per_thread = tmp[i].spt;
+        c.masses_per_thread = tmp[i].mpt;
+        c.streamed = i >= nr ? 1u : 0u;
+        c.use_graph = 1;
+        out[i] = c;
+    }
+    return n;
+}
+
 mb_status mb_set_launch_config(mb_context* ctx, const mb_launch_config* cfg) {
     if (!ctx || !cfg) return MB_ERR_ARGUMENT;
     if (cfg->threads && !cfg->streamed) {

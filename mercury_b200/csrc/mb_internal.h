@@ -105,6 +105,10 @@ cudaError_t launch_stream(const StepParams& p, uint32_t threads, uint32_t mpt, c
 uint32_t stream_smem_bytes(uint32_t n_mass);
 bool stream_supported(uint32_t threads, uint32_t mpt);
 
+// Compiled shapes of the resident (streamed = false) or streamed kernel;
+// writes up to cap entries, returns the count.
+uint32_t list_shapes(KernelShape* out, uint32_t cap, bool streamed);
+
 // Shared memory a bin needs, in bytes.
 uint32_t bin_smem_bytes(uint32_t n_mass, uint32_t n_spring, uint32_t n_inc);
 

@@ -571,6 +571,22 @@ int ctas_per_sm(const KernelShape& shape, uint32_t mode, bool track, uint32_t sm
     return n;
 }
 
+uint32_t list_shapes(KernelShape* out, uint32_t cap, bool streamed) {
+    uint32_t n = 0;
+    if (streamed) {
+        for (const auto& e : kStream) {
+            if (n < cap) out[n] = KernelShape{e.threads, 0, e.mpt};
+            ++n;
+        }
+    } else {
+        for (const auto& e : kShapes) {
+            if (n < cap) out[n] = KernelShape{e.threads, e.spt, e.mpt};
+            ++n;
+        }
+    }
+    return n;
+}
+
 uint32_t stream_smem_bytes(uint32_t n_mass) { return 16u * n_mass + 8u * kMaxMaterialSlots; }
 
 bool stream_supported(uint32_t threads, uint32_t mpt) { return find_stream(threads, mpt) != nullptr; }
