@@ -1,0 +1,73 @@
+"""The C++ drop-in Simulator (mercury_b200/compat): the reference's callers
+compile against it unchanged, and a C++ program that uses it the way the
+reference's TestSimulator does gets deterministic fitness and states equal
+to the oracle's bit for bit."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+BIN = os.path.join(ROOT, "tests", "cpp", "_bin", "test_dropin")
+
+
+@pytest.mark.skipif(not os.path.isdir("/root/reference"), reason="needs the reference sources")
+def test_reference_callers_compile_against_dropin():
+    r = subprocess.run(["make", "-C", os.path.join(ROOT, "tests", "cpp"), "check-callers"],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-2000:]
+
+
+def _read(path):
+    buf = open(path, "rb").read()
+    off = 0
+
+    def take(dtype, n):
+        nonlocal off
+        a = np.frombuffer(buf, dtype, n, off)
+        off += a.nbytes
+        return a.copy()
+
+    R = int(take(np.uint32, 1)[0])
+    robots = []
+    for _ in range(R):
+        nm, ns = (int(x) for x in take(np.uint32, 2))
+        masses = [(take(np.float32, 4), int(take(np.uint8, 1)[0])) for _ in range(nm)]
+        springs = [(take(np.uint16, 2), int(take(np.uint8, 1)[0]), float(take(np.float32, 1)[0])) for _ in range(ns)]
+        out = take(np.float32, 6 * nm).reshape(nm, 6)
+        st = take(np.float32, ns)
+        robots.append((masses, springs, out, st))
+    tt = float(take(np.float32, 1)[0])
+    return robots, tt
+
+
+@pytest.mark.gpu
+def test_dropin_matches_oracle(tmp_path):
+    if not os.path.exists(BIN):
+        pytest.skip("tests/cpp/_bin/test_dropin not built")
+    import mercury_b200 as mb
+    from oracle import core
+    out = str(tmp_path / "dropin.bin")
+    r = subprocess.run([BIN, out], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    robots, tt = _read(out)
+    els = []
+    for masses, springs, _, _ in robots:
+        pos = np.array([m[0][:3] for m in masses], np.float32)
+        els.append(mb.Element(pos, np.array([m[1] for m in masses], np.uint8),
+                              np.array([s[0] for s in springs], np.uint16),
+                              np.array([s[2] for s in springs], np.float32),
+                              np.array([s[1] for s in springs], np.uint8),
+                              mass=np.array([m[0][3] for m in masses], np.float32)))
+    b = mb.pack(els)
+    n = core.step_count(0.25, 1e-3)
+    p, v = b.pos.copy(), b.vel.copy()
+    s = np.zeros(b.n_springs, np.float32)
+    core.xpbd_run(b, p, v, s, core.material_table(), 1e-3, 0.0, n, True)
+    assert tt == core.advance_clock(0.0, 1e-3, n)
+    for k, (_, _, o, st) in enumerate(robots):
+        ms, ss = b.robot_slices(k)
+        assert np.array_equal(o[:, :3].view(np.uint32), p[ms, :3].view(np.uint32))
+        assert np.array_equal(o[:, 3:].view(np.uint32), v[ms, :3].view(np.uint32))
+        assert np.array_equal(st.view(np.uint32), s[ss].view(np.uint32))
