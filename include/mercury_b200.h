@@ -191,6 +191,21 @@ MB_API mb_status mb_device_state(mb_context* ctx, void** pos, void** vel, void**
 MB_API mb_status mb_get_launch_config(const mb_context* ctx, mb_launch_config* cfg);
 MB_API mb_status mb_set_launch_config(mb_context* ctx, const mb_launch_config* cfg);
 
+/* Launch plan of a population, computed on the host without a device:
+ * the shape, bin count and path the automatic choice (or `cfg`, may be
+ * NULL) would use on a GPU with `num_sms` SMs and `smem_bytes` of dynamic
+ * shared memory per CTA (0 = B200: 148, 232,448), and statistics of the
+ * packed layout.  No reference counterpart. */
+typedef struct mb_plan_stats {
+    uint32_t threads, springs_per_thread, masses_per_thread, bins, streamed;
+    uint32_t max_smem_bytes;
+    uint64_t masses, active_springs, incidence_entries, incidence_padding;
+    uint32_t aligned_slices, rank_slices, material_slots;
+    uint32_t max_bin_springs, min_bin_springs;
+} mb_plan_stats;
+MB_API mb_status mb_plan_population(const mb_batch_desc* batch, const mb_launch_config* cfg,
+                                    uint32_t num_sms, uint32_t smem_bytes, mb_plan_stats* stats);
+
 /* Compiled kernel shapes, for autotuners: writes up to `capacity` entries
  * (threads, springs_per_thread, masses_per_thread; streamed = 1 for the
  * streamed kernel, whose springs_per_thread is 0) and returns the count.  No

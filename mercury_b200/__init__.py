@@ -8,6 +8,6 @@ model, material tables and seeded robot populations.
 from ._lib import LIB, MercuryError  # noqa: F401  (fails loudly if the library is missing)
 from .element import Batch, Element, pack, unpack  # noqa: F401
 from .materials import COMPOSITE_COUNT, material_table  # noqa: F401
-from .simulator import ElementTracker, Simulator, SimulatorConfig, body_length, fitness  # noqa: F401
+from .simulator import ElementTracker, Simulator, SimulatorConfig, body_length, fitness, plan  # noqa: F401
 
 __version__ = LIB.mb_version().decode()

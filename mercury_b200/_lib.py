@@ -52,6 +52,15 @@ class Environment(ctypes.Structure):
                                               "friction_kinetic", "drag", "damping")]
 
 
+class PlanStats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint32) for n in ("threads", "springs_per_thread", "masses_per_thread",
+                                               "bins", "streamed", "max_smem_bytes")] + \
+               [(n, ctypes.c_uint64) for n in ("masses", "active_springs", "incidence_entries",
+                                               "incidence_padding")] + \
+               [(n, ctypes.c_uint32) for n in ("aligned_slices", "rank_slices", "material_slots",
+                                               "max_bin_springs", "min_bin_springs")]
+
+
 class LaunchConfig(ctypes.Structure):
     _fields_ = [
         ("threads", ctypes.c_uint32),
@@ -97,6 +106,8 @@ def _load() -> ctypes.CDLL:
         "mb_get_launch_config": (I32, [P, ctypes.POINTER(LaunchConfig)]),
         "mb_set_launch_config": (I32, [P, ctypes.POINTER(LaunchConfig)]),
         "mb_kernel_shapes": (U32, [ctypes.POINTER(LaunchConfig), U32]),
+        "mb_plan_population": (I32, [ctypes.POINTER(BatchDesc), ctypes.POINTER(LaunchConfig), U32, U32,
+                                     ctypes.POINTER(PlanStats)]),
         "mb_voxel_build": (I32, [I32, I32, I32, F32, P, ctypes.POINTER(I32), ctypes.POINTER(I32), P, P, P, P, P]),
         "mb_version": (ctypes.c_char_p, []),
     }

@@ -12,14 +12,14 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
-SRC = [os.path.join(HERE, "csrc", f) for f in ("mb_kernels.cu", "mb_host.cpp", "mb_voxel.cpp",
-                                               "mb_noalloc.cu")]
-DEPS = SRC + [os.path.join(HERE, "csrc", f) for f in ("mb_internal.h", "mb_sin.cuh")] + [
+SRC = [os.path.join(HERE, "csrc", f) for f in ("mb_kernels.cu", "mb_host.cpp", "mb_pack.cpp",
+                                               "mb_voxel.cpp", "mb_noalloc.cu")]
+DEPS = SRC + [os.path.join(HERE, "csrc", f) for f in ("mb_internal.h", "mb_sin.cuh", "mb_pack.h")] + [
     os.path.join(ROOT, "include", "mercury_b200.h")]
 OUT = os.path.join(HERE, "libmercury_b200.so")
 NVCC = os.environ.get("NVCC", "nvcc")
 FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-gencode", "arch=compute_100a,code=sm_100a",
-         "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall", "-Xcompiler", "-fvisibility=hidden", "-shared"]
+         "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall", "-Xcompiler", "-fvisibility=hidden", "-shared", "-lpthread"]
 
 
 def up_to_date() -> bool:

@@ -34,6 +34,7 @@
 
 #include "../../include/mercury_b200.h"
 #include "mb_internal.h"
+#include "mb_pack.h"
 
 namespace mb {
 
@@ -220,64 +221,6 @@ mb_status cuda_fail(mb_context* c, cudaError_t e, const char* what) {
         if (_e != cudaSuccess) return cuda_fail(ctx, _e, #call); \
     } while (0)
 
-// Per-robot topology after removing air springs, in packed order.
-struct RobotPack {
-    std::vector<uint32_t> springs;  // original local spring index, packed order
-};
-
-// Shapes the automatic choice considers, in order of preference: 32 warps
-// per SM with about 8-10 springs per thread first.
-const mb::KernelShape kAuto[] = {
-    {1024, 10, 2}, {1024, 12, 2}, {1024, 8, 2}, {512, 16, 4}, {512, 12, 2}, {512, 8, 2},
-    {1024, 6, 2},  {1024, 4, 1},  {512, 4, 1},  {256, 16, 4}, {256, 8, 2},
-};
-
-struct BinPlan {
-    std::vector<std::vector<uint32_t>> robots;  // per bin, robot ids ascending
-};
-
-// LPT assignment of robots to `nb` bins by non-air spring count (+ masses).
-bool plan_bins(const std::vector<uint64_t>& cost, const std::vector<uint32_t>& nm,
-               const std::vector<uint32_t>& ns, const std::vector<uint64_t>& ninc,
-               uint32_t nb, const mb::KernelShape& sh, uint32_t smem_cap, BinPlan& plan,
-               uint32_t& smem_needed) {
-    const uint32_t n = (uint32_t)cost.size();
-    std::vector<uint32_t> order(n);
-    for (uint32_t i = 0; i < n; ++i) order[i] = i;
-    std::stable_sort(order.begin(), order.end(),
-                     [&](uint32_t a, uint32_t b) { return cost[a] > cost[b]; });
-    std::vector<uint64_t> load(nb, 0), bm(nb, 0), bs(nb, 0), bi(nb, 0);
-    plan.robots.assign(nb, {});
-    const uint64_t cap_s = std::min<uint64_t>((uint64_t)sh.threads * sh.spt, mb::kMaxBinSprings);
-    const uint64_t cap_m = std::min<uint64_t>((uint64_t)sh.threads * sh.mpt, 4096);
-    for (uint32_t r : order) {
-        // least loaded bin that still has room
-        int best = -1;
-        for (uint32_t b = 0; b < nb; ++b) {
-            if (bm[b] + nm[r] > cap_m || bs[b] + ns[r] > cap_s) continue;
-            // incidence estimate: padded rows, bounded by smem
-            const uint64_t smem =
-                mb::bin_smem_bytes((uint32_t)(bm[b] + nm[r]), (uint32_t)(bs[b] + ns[r]),
-                                   (uint32_t)(bi[b] + ninc[r]));
-            if (smem > smem_cap) continue;
-            if (best < 0 || load[b] < load[best]) best = (int)b;
-        }
-        if (best < 0) return false;
-        load[best] += cost[r];
-        bm[best] += nm[r];
-        bs[best] += ns[r];
-        bi[best] += ninc[r];
-        plan.robots[best].push_back(r);
-    }
-    smem_needed = 0;
-    for (uint32_t b = 0; b < nb; ++b) {
-        std::sort(plan.robots[b].begin(), plan.robots[b].end());
-        smem_needed = std::max(smem_needed, mb::bin_smem_bytes((uint32_t)bm[b], (uint32_t)bs[b],
-                                                               (uint32_t)bi[b]));
-    }
-    return true;
-}
-
 }  // namespace
 
 extern "C" {
@@ -384,6 +327,44 @@ mb_status mb_get_launch_config(const mb_context* ctx, mb_launch_config* cfg) {
     return MB_OK;
 }
 
+mb_status mb_plan_population(const mb_batch_desc* batch, const mb_launch_config* cfg, uint32_t num_sms,
+                             uint32_t smem_bytes, mb_plan_stats* stats) {
+    if (!batch || !stats || batch->n_robots == 0 || !batch->mass_offsets || !batch->spring_offsets ||
+        !batch->mass_material || (batch->spring_offsets[batch->n_robots] &&
+                                  (!batch->pairs || !batch->spring_material || !batch->lbar)))
+        return MB_ERR_ARGUMENT;
+    mb::PackOptions po;
+    po.sms = num_sms ? num_sms : 148;
+    po.smem_cap = smem_bytes ? smem_bytes : 232448;
+    if (cfg) po.override = *cfg;
+    mb::Packed out;
+    std::string err;
+    const mb_status st = mb::pack_population(batch, po, out, err);
+    if (st != MB_OK) return st;
+    std::memset(stats, 0, sizeof(*stats));
+    stats->threads = out.shape.threads;
+    stats->springs_per_thread = out.shape.spt;
+    stats->masses_per_thread = out.shape.mpt;
+    stats->bins = out.n_bins;
+    stats->streamed = out.streamed ? 1u : 0u;
+    stats->max_smem_bytes = out.max_smem;
+    stats->masses = out.masses;
+    stats->active_springs = out.active_springs;
+    stats->incidence_entries = out.inc_entries;
+    stats->incidence_padding = out.inc_padding;
+    stats->aligned_slices = out.aligned_slices;
+    stats->rank_slices = out.rank_slices;
+    stats->material_slots = (uint32_t)out.mat_ids.size();
+    uint32_t mx = 0, mn = 0xFFFFFFFFu;
+    for (const auto& d : out.bins) {
+        mx = std::max(mx, d.n_spring);
+        mn = std::min(mn, d.n_spring);
+    }
+    stats->max_bin_springs = mx;
+    stats->min_bin_springs = out.bins.empty() ? 0 : mn;
+    return MB_OK;
+}
+
 uint32_t mb_kernel_shapes(mb_launch_config* out, uint32_t capacity) {
     mb::KernelShape tmp[64];
     const uint32_t nr = mb::list_shapes(tmp, 64, false);
@@ -436,254 +417,23 @@ mb_status mb_set_elements(mb_context* ctx, const mb_batch_desc* b) {
         return fail(ctx, MB_ERR_ARGUMENT, "null spring array");
     if (M >= (1ull << 31) || S >= (1ull << 31)) return fail(ctx, MB_ERR_CAPACITY, "population too large");
 
-    // validate and prepare per-robot packing
-    std::vector<uint32_t> nm(R), ns(R);
-    std::vector<uint64_t> cost(R), ninc(R);
-    std::vector<RobotPack> packs(R);
-    for (uint32_t r = 0; r < R; ++r) {
-        const int64_t m0 = b->mass_offsets[r], m1 = b->mass_offsets[r + 1];
-        const int64_t s0 = b->spring_offsets[r], s1 = b->spring_offsets[r + 1];
-        if (m1 < m0 || s1 < s0) return fail(ctx, MB_ERR_ARGUMENT, "offsets decrease at robot %u", r);
-        const int64_t cm = m1 - m0;
-        if (cm > 4096) return fail(ctx, MB_ERR_CAPACITY, "robot %u has %lld masses (max 4096)", r, (long long)cm);
-        std::vector<uint32_t> deg((size_t)cm, 0);
-        auto& sp = packs[r].springs;
-        for (int64_t s = s0; s < s1; ++s) {
-            const uint16_t a = b->pairs[2 * s], c = b->pairs[2 * s + 1];
-            if (a >= cm || c >= cm)
-                return fail(ctx, MB_ERR_ARGUMENT, "spring %lld of robot %u joins mass %u/%u of %lld",
-                            (long long)(s - s0), r, a, c, (long long)cm);
-            if (b->spring_material[s] >= MB_COMPOSITE_COUNT)
-                return fail(ctx, MB_ERR_ARGUMENT, "spring material %u out of range", b->spring_material[s]);
-            if (!std::isfinite(b->lbar[s])) return fail(ctx, MB_ERR_ARGUMENT, "non-finite mean length");
-            if (b->spring_material[s] == 0) continue;  // air springs never act (sim_kernel.cu:211)
-            sp.push_back((uint32_t)(s - s0));
-            deg[a]++;
-            deg[c]++;
-        }
-        for (int64_t i = m0; i < m1; ++i)
-            if (b->mass_material[i] > 22) return fail(ctx, MB_ERR_ARGUMENT, "mass material out of range");
-        std::stable_sort(sp.begin(), sp.end(), [&](uint32_t x, uint32_t y) {
-            const int64_t gx = s0 + x, gy = s0 + y;
-            const int dx = (int)b->pairs[2 * gx + 1] - (int)b->pairs[2 * gx];
-            const int dy = (int)b->pairs[2 * gy + 1] - (int)b->pairs[2 * gy];
-            if (dx != dy) return dx < dy;
-            return b->pairs[2 * gx] < b->pairs[2 * gy];
-        });
-        nm[r] = (uint32_t)cm;
-        ns[r] = (uint32_t)sp.size();
-        cost[r] = (uint64_t)ns[r] * 4 + nm[r];
-        // incidence estimate for smem: rows padded to the slice maximum
-        uint64_t est = 0;
-        for (int64_t i = 0; i < cm; i += 32) {
-            uint32_t w = 0;
-            for (int64_t k = i; k < std::min<int64_t>(i + 32, cm); ++k) w = std::max(w, deg[k]);
-            est += 32ull * w;
-        }
-        ninc[r] = est + 64;  // slack for slices straddling robots
-    }
-
-    // choose shape and bin count
     cudaSetDevice(ctx->device);
-    const uint32_t smem_cap = mb::max_step_smem(ctx->device);
-    const uint32_t sms = (uint32_t)std::max(ctx->num_sms, 1);
-    uint64_t tot_s = 0, tot_m = 0;
-    uint32_t max_s = 0, max_m = 0;
-    for (uint32_t r = 0; r < R; ++r) {
-        tot_s += ns[r];
-        tot_m += nm[r];
-        max_s = std::max(max_s, ns[r]);
-        max_m = std::max(max_m, nm[r]);
-    }
-    std::vector<mb::KernelShape> shapes;
-    if (ctx->override_cfg.threads)
-        shapes.push_back({ctx->override_cfg.threads, ctx->override_cfg.springs_per_thread,
-                          ctx->override_cfg.masses_per_thread});
-    else
-        for (const auto& s : kAuto) shapes.push_back(s);
-    // Plan bins, build them, and re-plan with more bins while a built bin
-    // overflows shared memory (rows of slices that straddle two robots are
-    // padded to the wider robot, so the estimate is not exact).
-    struct Built {
-        std::vector<mb::BinDesc> bins;
-        std::vector<uint32_t> mass_gidx, spring_gidx, pair, slice_off, slice_width, robot_bin;
-        std::vector<uint16_t> inc;
-        std::vector<uint32_t> inc32;
-        std::vector<float> lbar;
-        std::vector<uint8_t> mat_ids;
-        uint32_t max_smem = 0;
-    } out;
-    auto build = [&](const BinPlan& plan, uint32_t nb, bool streamed) {
-        out = Built();
-        out.bins.resize(nb);
-        out.robot_bin.resize(R);
-        out.mass_gidx.reserve(M);
-        out.spring_gidx.reserve(S);
-        // material slots: the composite ids used by the whole population
-        std::vector<int> slot_of(MB_COMPOSITE_COUNT, -1);
-        for (uint32_t r = 0; r < R; ++r)
-            for (uint32_t ls : packs[r].springs) slot_of[b->spring_material[b->spring_offsets[r] + ls]] = 0;
-        for (int m = 0; m < MB_COMPOSITE_COUNT; ++m)
-            if (slot_of[m] == 0) {
-                slot_of[m] = (int)out.mat_ids.size();
-                out.mat_ids.push_back((uint8_t)m);
-            }
-        for (uint32_t bi = 0; bi < nb; ++bi) {
-            mb::BinDesc& d = out.bins[bi];
-            std::memset(&d, 0, sizeof(d));
-            d.mass_begin = (uint32_t)out.mass_gidx.size();
-            d.spring_begin = (uint32_t)out.spring_gidx.size();
-            d.inc_begin = (uint32_t)(streamed ? out.inc32.size() : out.inc.size());
-            d.slice_begin = (uint32_t)out.slice_off.size();
-            (void)slot_of;
-            struct Ent {
-                uint32_t other, orig, sign, packed;
-            };
-            std::vector<std::vector<Ent>> rows;
-            uint32_t mbase = 0, sbase = 0;
-            for (uint32_t r : plan.robots[bi]) {
-                out.robot_bin[r] = bi;
-                const int64_t m0 = b->mass_offsets[r], s0 = b->spring_offsets[r];
-                for (uint32_t i = 0; i < nm[r]; ++i) out.mass_gidx.push_back((uint32_t)(m0 + i));
-                rows.resize(mbase + nm[r]);
-                for (uint32_t k = 0; k < packs[r].springs.size(); ++k) {
-                    const uint32_t ls = packs[r].springs[k];
-                    const int64_t g = s0 + ls;
-                    const uint32_t a = b->pairs[2 * g], c = b->pairs[2 * g + 1];
-                    const uint32_t pa = mbase + a, pc = mbase + c;
-                    out.spring_gidx.push_back((uint32_t)g);
-                    out.pair.push_back(pa | (pc << 12) | ((uint32_t)slot_of[b->spring_material[g]] << 24));
-                    out.lbar.push_back(b->lbar[g]);
-                    const uint32_t packed = sbase + k;
-                    rows[pa].push_back({c, ls, 0u, packed});
-                    rows[pc].push_back({a, ls, 1u, packed});
-                }
-                mbase += nm[r];
-                sbase += (uint32_t)packs[r].springs.size();
-            }
-            d.n_mass = mbase;
-            d.n_spring = sbase;
-            // Rows in summation order, stored SELL-32.  Columns are aligned
-            // by the offset of the other end (other - i) when every row of the
-            // slice has distinct offsets: then the k-th entries of a warp's 32
-            // masses are springs of one direction with consecutive packed
-            // indices (conflict-free gather).  Otherwise, or when alignment
-            // would widen the slice by more than 4 columns, columns are ranks.
-            for (uint32_t i0 = 0; i0 < mbase; i0 += mb::kSliceWidth) {
-                const uint32_t i1 = std::min<uint32_t>(i0 + mb::kSliceWidth, mbase);
-                uint32_t w_rank = 0;
-                bool distinct = true;
-                std::vector<int> offs;
-                for (uint32_t i = i0; i < i1; ++i) {
-                    auto& row = rows[i];
-                    std::sort(row.begin(), row.end(), [](const Ent& x, const Ent& y) {
-                        if (x.other != y.other) return x.other < y.other;
-                        if (x.orig != y.orig) return x.orig < y.orig;
-                        return x.sign < y.sign;
-                    });
-                    w_rank = std::max<uint32_t>(w_rank, (uint32_t)row.size());
-                    for (size_t q = 0; q < row.size(); ++q) {
-                        if (q && row[q].other == row[q - 1].other) distinct = false;
-                        offs.push_back((int)row[q].other - (int)i);
-                    }
-                }
-                std::sort(offs.begin(), offs.end());
-                offs.erase(std::unique(offs.begin(), offs.end()), offs.end());
-                const bool aligned = distinct && offs.size() <= w_rank + 4;
-                const uint32_t w = aligned ? (uint32_t)offs.size() : w_rank;
-                const size_t base = streamed ? out.inc32.size() : out.inc.size();
-                out.slice_off.push_back((uint32_t)base - d.inc_begin);
-                out.slice_width.push_back(w);
-                if (streamed)
-                    out.inc32.resize(base + (size_t)w * mb::kSliceWidth, mb::kPadEntry32);
-                else
-                    out.inc.resize(base + (size_t)w * mb::kSliceWidth, mb::kPadEntry);
-                for (uint32_t i = i0; i < i1; ++i)
-                    for (uint32_t q = 0; q < rows[i].size(); ++q) {
-                        const Ent& e = rows[i][q];
-                        const uint32_t col =
-                            aligned ? (uint32_t)(std::lower_bound(offs.begin(), offs.end(),
-                                                                  (int)e.other - (int)i) - offs.begin())
-                                    : q;
-                        const size_t at = base + (size_t)col * mb::kSliceWidth + (i - i0);
-                        if (streamed)
-                            out.inc32[at] = (e.packed << 1) | e.sign;
-                        else
-                            out.inc[at] = (uint16_t)((e.packed << 1) | e.sign);
-                    }
-            }
-            d.n_inc = (uint32_t)(streamed ? out.inc32.size() : out.inc.size()) - d.inc_begin;
-            out.max_smem = std::max(out.max_smem, streamed ? mb::stream_smem_bytes(d.n_mass)
-                                                           : mb::bin_smem_bytes(d.n_mass, d.n_spring, d.n_inc));
-        }
+    mb::PackOptions po;
+    po.sms = (uint32_t)std::max(ctx->num_sms, 1);
+    po.smem_cap = mb::max_step_smem(ctx->device);
+    po.mode = (uint32_t)ctx->mode;
+    po.override = ctx->override_cfg;
+    po.ctas_per_sm = [ctx](const mb::KernelShape& sh, uint32_t smem) {
+        return mb::ctas_per_sm(sh, (uint32_t)ctx->mode, false, smem);
     };
-
-    BinPlan plan;
-    bool ok = false;
-    uint32_t smem_needed = 0;
-    for (const auto& sh : shapes) {
-        const uint64_t cap_s = std::min<uint64_t>((uint64_t)sh.threads * sh.spt, mb::kMaxBinSprings);
-        const uint64_t cap_m = std::min<uint64_t>((uint64_t)sh.threads * sh.mpt, 4096);
-        if (max_s > cap_s || max_m > cap_m) continue;
-        uint32_t nb = ctx->override_cfg.bins;
-        const bool fixed = nb != 0;
-        // One wave = SMs x resident CTAs per SM (registers usually limit it;
-        // shared memory is estimated at the even share of the population).
-        uint32_t wave = sms;
-        if (!nb) {
-            const uint64_t need = std::max<uint64_t>((tot_s + cap_s - 1) / cap_s, (tot_m + cap_m - 1) / cap_m);
-            nb = (uint32_t)std::max<uint64_t>(need, 1);
-            if (R >= sms) {
-                const uint32_t est_smem = std::min<uint32_t>(
-                    smem_cap, mb::bin_smem_bytes((uint32_t)std::min<uint64_t>(cap_m, tot_m / sms + 1),
-                                                 (uint32_t)std::min<uint64_t>(cap_s, tot_s / sms + 1),
-                                                 (uint32_t)std::min<uint64_t>(3 * cap_s, 3 * (tot_s / sms + 1))));
-                const int per_sm = std::max(1, mb::ctas_per_sm(sh, (uint32_t)ctx->mode, false, est_smem));
-                wave = sms * (uint32_t)per_sm;
-                nb = std::max<uint32_t>(nb, wave);
-                nb = (nb + wave - 1) / wave * wave;  // whole waves
-            }
-            nb = std::min<uint32_t>(nb, R);
-        }
-        for (uint32_t tries = 0; tries < 16; ++tries) {
-            if (plan_bins(cost, nm, ns, ninc, nb, sh, smem_cap, plan, smem_needed)) {
-                build(plan, nb, false);
-                if (out.max_smem <= smem_cap) {
-                    ok = true;
-                    break;
-                }
-            }
-            if (fixed || nb >= R) break;
-            nb = std::min<uint32_t>(R, nb + wave);
-        }
-        if (ok) {
-            ctx->shape = sh;
-            ctx->n_bins = nb;
-            break;
-        }
-    }
-    // Streamed path: when forced, or when no resident shape holds the
-    // largest robot.  One robot per bin.
-    bool streamed = false;
-    uint32_t stream_mpt = 2;
-    if (ctx->override_cfg.streamed || !ok) {
-        stream_mpt = max_m <= 2048 ? 2u : 4u;
-        if (max_m <= 4096 && mb::stream_supported(1024, stream_mpt)) {
-            plan.robots.assign(R, {});
-            for (uint32_t r = 0; r < R; ++r) plan.robots[r].push_back(r);
-            build(plan, R, true);
-            if (out.max_smem <= smem_cap) {
-                ok = true;
-                streamed = true;
-                ctx->shape = mb::KernelShape{1024, 0, stream_mpt};
-                ctx->n_bins = R;
-            }
-        }
-    }
-    if (!ok)
-        return fail(ctx, MB_ERR_CAPACITY,
-                    "population does not fit any compiled kernel shape (largest robot: %u springs, %u masses)",
-                    max_s, max_m);
+    mb::Packed out;
+    std::string err;
+    const mb_status pst = mb::pack_population(b, po, out, err);
+    if (pst != MB_OK) return fail(ctx, pst, "%s", err.c_str());
+    ctx->shape = out.shape;
+    ctx->n_bins = out.n_bins;
+    const bool streamed = out.streamed;
+    const uint32_t stream_mpt = out.shape.mpt;
     const uint32_t nb = ctx->n_bins;
     const uint32_t max_smem = out.max_smem;
     auto& bins = out.bins;

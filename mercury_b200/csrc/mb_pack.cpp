@@ -1,0 +1,460 @@
+// Packing of a population into bins (host only; see mb_pack.h).
+//
+// The reference gives every robot one CTA and pads every robot to the
+// largest mass and spring count (Simulator.cu:231-239, 489-494).  Here
+// robots keep their own sizes and are grouped into bins, each simulated by
+// one CTA; bins are filled largest-robot-first onto the least loaded bin
+// (LPT), and the bin count is a whole number of waves (SMs x resident CTAs
+// per SM) so that every SM gets the same work.  Inside a bin:
+//   - masses keep robot order (robot r's masses, then robot r+1's ...);
+//   - non-air springs are sorted by (b - a, a) so that a warp's springs read
+//     consecutive positions (for a lattice: one direction, consecutive a);
+//   - every mass gets a row of incident springs sorted by (other end,
+//     spring index, a end before b end) -- the fixed summation order -- and
+//     rows are stored 32 masses per slice, column-major (SELL-32), with
+//     columns aligned by the offset of the other end where possible.
+// Robots are preprocessed and bins built in parallel over host threads; the
+// result does not depend on the number of threads.
+#include "mb_pack.h"
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <thread>
+
+namespace mb {
+namespace {
+
+struct RobotPack {
+    std::vector<uint32_t> springs;  // robot-local indices of non-air springs, packed order
+    uint32_t n_mass = 0;
+    uint64_t cost = 0;
+    uint64_t inc_estimate = 0;
+    std::string error;
+    mb_status status = MB_OK;
+};
+
+// Shapes the automatic choice considers, in order of preference: 32 warps
+// per SM with about 8-10 springs per thread first.
+const KernelShape kAuto[] = {
+    {1024, 10, 2}, {1024, 12, 2}, {1024, 8, 2}, {512, 16, 4}, {512, 8, 2},
+    {1024, 6, 2},  {1024, 4, 1},  {512, 4, 1},  {256, 8, 2},
+};
+
+template <typename F>
+void parallel_for(uint32_t n, unsigned threads, F&& f) {
+    if (threads <= 1 || n <= 1) {
+        for (uint32_t i = 0; i < n; ++i) f(i);
+        return;
+    }
+    std::atomic<uint32_t> next{0};
+    std::vector<std::thread> pool;
+    const unsigned t = std::min<unsigned>(threads, n);
+    for (unsigned k = 0; k < t; ++k)
+        pool.emplace_back([&] {
+            for (uint32_t i = next++; i < n; i = next++) f(i);
+        });
+    for (auto& th : pool) th.join();
+}
+
+void preprocess(const mb_batch_desc* b, uint32_t r, RobotPack& p) {
+    const int64_t m0 = b->mass_offsets[r], m1 = b->mass_offsets[r + 1];
+    const int64_t s0 = b->spring_offsets[r], s1 = b->spring_offsets[r + 1];
+    char buf[256];
+    if (m1 < m0 || s1 < s0) {
+        std::snprintf(buf, sizeof(buf), "offsets decrease at robot %u", r);
+        p.error = buf;
+        p.status = MB_ERR_ARGUMENT;
+        return;
+    }
+    const int64_t cm = m1 - m0;
+    if (cm > 4096) {
+        std::snprintf(buf, sizeof(buf), "robot %u has %lld masses (max 4096)", r, (long long)cm);
+        p.error = buf;
+        p.status = MB_ERR_CAPACITY;
+        return;
+    }
+    for (int64_t i = m0; i < m1; ++i)
+        if (b->mass_material[i] > 22) {
+            std::snprintf(buf, sizeof(buf), "mass material %u of robot %u out of range", b->mass_material[i], r);
+            p.error = buf;
+            p.status = MB_ERR_ARGUMENT;
+            return;
+        }
+    std::vector<uint32_t> deg((size_t)cm, 0);
+    auto& sp = p.springs;
+    sp.reserve((size_t)(s1 - s0));
+    for (int64_t s = s0; s < s1; ++s) {
+        const uint16_t a = b->pairs[2 * s], c = b->pairs[2 * s + 1];
+        if (a >= cm || c >= cm) {
+            std::snprintf(buf, sizeof(buf), "spring %lld of robot %u joins mass %u/%u of %lld",
+                          (long long)(s - s0), r, a, c, (long long)cm);
+            p.error = buf;
+            p.status = MB_ERR_ARGUMENT;
+            return;
+        }
+        if (b->spring_material[s] >= MB_COMPOSITE_COUNT) {
+            std::snprintf(buf, sizeof(buf), "spring material %u out of range", b->spring_material[s]);
+            p.error = buf;
+            p.status = MB_ERR_ARGUMENT;
+            return;
+        }
+        if (!std::isfinite(b->lbar[s])) {
+            p.error = "non-finite mean length";
+            p.status = MB_ERR_ARGUMENT;
+            return;
+        }
+        if (b->spring_material[s] == 0) continue;  // air springs never act (sim_kernel.cu:211)
+        sp.push_back((uint32_t)(s - s0));
+        deg[a]++;
+        deg[c]++;
+    }
+    std::stable_sort(sp.begin(), sp.end(), [&](uint32_t x, uint32_t y) {
+        const int64_t gx = s0 + x, gy = s0 + y;
+        const int dx = (int)b->pairs[2 * gx + 1] - (int)b->pairs[2 * gx];
+        const int dy = (int)b->pairs[2 * gy + 1] - (int)b->pairs[2 * gy];
+        if (dx != dy) return dx < dy;
+        return b->pairs[2 * gx] < b->pairs[2 * gy];
+    });
+    p.n_mass = (uint32_t)cm;
+    p.cost = (uint64_t)sp.size() * 4 + (uint64_t)cm;
+    uint64_t est = 0;  // incidence entries with rows padded to the slice maximum
+    for (int64_t i = 0; i < cm; i += 32) {
+        uint32_t w = 0;
+        for (int64_t k = i; k < std::min<int64_t>(i + 32, cm); ++k) w = std::max(w, deg[k]);
+        est += 32ull * w;
+    }
+    p.inc_estimate = est + 64;  // slack for slices straddling robots
+}
+
+// LPT assignment of robots to `nb` bins by cost, within the shape's and the
+// shared memory's capacity.
+bool plan_bins(const std::vector<RobotPack>& packs, uint32_t nb, const KernelShape& sh,
+               uint32_t smem_cap, std::vector<std::vector<uint32_t>>& plan) {
+    const uint32_t n = (uint32_t)packs.size();
+    std::vector<uint32_t> order(n);
+    for (uint32_t i = 0; i < n; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](uint32_t a, uint32_t b) { return packs[a].cost > packs[b].cost; });
+    std::vector<uint64_t> load(nb, 0), bm(nb, 0), bs(nb, 0), bi(nb, 0);
+    plan.assign(nb, {});
+    const uint64_t cap_s = std::min<uint64_t>((uint64_t)sh.threads * sh.spt, kMaxBinSprings);
+    const uint64_t cap_m = std::min<uint64_t>((uint64_t)sh.threads * sh.mpt, 4096);
+    for (uint32_t r : order) {
+        const auto& p = packs[r];
+        int best = -1;
+        for (uint32_t b = 0; b < nb; ++b) {
+            if (bm[b] + p.n_mass > cap_m || bs[b] + p.springs.size() > cap_s) continue;
+            if (bin_smem_bytes((uint32_t)(bm[b] + p.n_mass), (uint32_t)(bs[b] + p.springs.size()),
+                               (uint32_t)(bi[b] + p.inc_estimate)) > smem_cap)
+                continue;
+            if (best < 0 || load[b] < load[best]) best = (int)b;
+        }
+        if (best < 0) return false;
+        load[best] += p.cost;
+        bm[best] += p.n_mass;
+        bs[best] += p.springs.size();
+        bi[best] += p.inc_estimate;
+        plan[best].push_back(r);
+    }
+    for (auto& v : plan) std::sort(v.begin(), v.end());
+    return true;
+}
+
+struct BinLocal {
+    std::vector<uint32_t> mass_gidx, spring_gidx, pair, slice_off, slice_width, inc32;
+    std::vector<uint16_t> inc;
+    std::vector<float> lbar;
+    uint32_t n_mass = 0, n_spring = 0, n_inc = 0, smem = 0, aligned = 0, ranked = 0;
+    uint64_t padding = 0;
+};
+
+struct Ent {
+    uint32_t other, orig, sign, packed;
+};
+
+inline bool ent_less(const Ent& x, const Ent& y) {
+    if (x.other != y.other) return x.other < y.other;
+    if (x.orig != y.orig) return x.orig < y.orig;
+    return x.sign < y.sign;
+}
+
+void build_bin(const mb_batch_desc* b, const std::vector<RobotPack>& packs,
+               const std::vector<uint32_t>& robots, const std::vector<int>& slot_of, bool streamed,
+               BinLocal& L) {
+    uint32_t nm = 0, ns = 0;
+    for (uint32_t r : robots) {
+        nm += packs[r].n_mass;
+        ns += (uint32_t)packs[r].springs.size();
+    }
+    L.mass_gidx.reserve(nm);
+    L.spring_gidx.reserve(ns);
+    L.pair.reserve(ns);
+    L.lbar.reserve(ns);
+    std::vector<uint32_t> row_start(nm + 1, 0);
+    uint32_t mbase = 0;
+    for (uint32_t r : robots) {
+        const int64_t m0 = b->mass_offsets[r], s0 = b->spring_offsets[r];
+        for (uint32_t i = 0; i < packs[r].n_mass; ++i) L.mass_gidx.push_back((uint32_t)(m0 + i));
+        for (uint32_t ls : packs[r].springs) {
+            const int64_t g = s0 + ls;
+            const uint32_t pa = mbase + b->pairs[2 * g], pc = mbase + b->pairs[2 * g + 1];
+            L.spring_gidx.push_back((uint32_t)g);
+            L.pair.push_back(pa | (pc << 12) | ((uint32_t)slot_of[b->spring_material[g]] << 24));
+            L.lbar.push_back(b->lbar[g]);
+            row_start[pa + 1]++;
+            row_start[pc + 1]++;
+        }
+        mbase += packs[r].n_mass;
+    }
+    for (uint32_t i = 0; i < nm; ++i) row_start[i + 1] += row_start[i];
+    std::vector<Ent> ents(row_start[nm]);
+    std::vector<uint32_t> fill(row_start.begin(), row_start.end() - 1);
+    {
+        uint32_t base = 0, sb = 0;
+        for (uint32_t r : robots) {
+            const int64_t s0 = b->spring_offsets[r];
+            const auto& sp = packs[r].springs;
+            for (uint32_t k = 0; k < sp.size(); ++k) {
+                const int64_t g = s0 + sp[k];
+                const uint32_t a = b->pairs[2 * g], c = b->pairs[2 * g + 1];
+                ents[fill[base + a]++] = {c, sp[k], 0u, sb + k};
+                ents[fill[base + c]++] = {a, sp[k], 1u, sb + k};
+            }
+            base += packs[r].n_mass;
+            sb += (uint32_t)sp.size();
+        }
+    }
+    for (uint32_t i = 0; i < nm; ++i) {  // summation order within each row
+        Ent* first = ents.data() + row_start[i];
+        Ent* last = ents.data() + row_start[i + 1];
+        if (last - first > 24) {
+            std::sort(first, last, ent_less);
+        } else {
+            for (Ent* x = first + 1; x < last; ++x) {
+                const Ent e = *x;
+                Ent* y = x;
+                while (y > first && ent_less(e, *(y - 1))) {
+                    *y = *(y - 1);
+                    --y;
+                }
+                *y = e;
+            }
+        }
+    }
+    L.n_mass = nm;
+    L.n_spring = ns;
+    // SELL-32: columns aligned by the offset of the other end (other - i)
+    // when every row of the slice has distinct offsets -- then the k-th
+    // entries of a warp's 32 masses are springs of one direction with
+    // consecutive packed indices (conflict-free gather) -- otherwise, or
+    // when alignment would widen the slice by more than 4 columns, ranks.
+    std::vector<int> offs;
+    for (uint32_t i0 = 0; i0 < nm; i0 += kSliceWidth) {
+        const uint32_t i1 = std::min<uint32_t>(i0 + kSliceWidth, nm);
+        uint32_t w_rank = 0;
+        bool distinct = true;
+        offs.clear();
+        for (uint32_t i = i0; i < i1; ++i) {
+            const uint32_t r0 = row_start[i], r1 = row_start[i + 1];
+            w_rank = std::max(w_rank, r1 - r0);
+            for (uint32_t q = r0; q < r1; ++q) {
+                if (q > r0 && ents[q].other == ents[q - 1].other) distinct = false;
+                offs.push_back((int)ents[q].other - (int)i);
+            }
+        }
+        std::sort(offs.begin(), offs.end());
+        offs.erase(std::unique(offs.begin(), offs.end()), offs.end());
+        const bool aligned = distinct && offs.size() <= w_rank + 4;
+        const uint32_t w = aligned ? (uint32_t)offs.size() : w_rank;
+        aligned ? ++L.aligned : ++L.ranked;
+        const size_t base = streamed ? L.inc32.size() : L.inc.size();
+        L.slice_off.push_back((uint32_t)base);
+        L.slice_width.push_back(w);
+        if (streamed)
+            L.inc32.resize(base + (size_t)w * kSliceWidth, kPadEntry32);
+        else
+            L.inc.resize(base + (size_t)w * kSliceWidth, kPadEntry);
+        for (uint32_t i = i0; i < i1; ++i)
+            for (uint32_t q = row_start[i]; q < row_start[i + 1]; ++q) {
+                const Ent& e = ents[q];
+                const uint32_t col =
+                    aligned ? (uint32_t)(std::lower_bound(offs.begin(), offs.end(), (int)e.other - (int)i) -
+                                         offs.begin())
+                            : q - row_start[i];
+                const size_t at = base + (size_t)col * kSliceWidth + (i - i0);
+                if (streamed)
+                    L.inc32[at] = (e.packed << 1) | e.sign;
+                else
+                    L.inc[at] = (uint16_t)((e.packed << 1) | e.sign);
+            }
+    }
+    L.n_inc = (uint32_t)(streamed ? L.inc32.size() : L.inc.size());
+    L.padding = L.n_inc - 2ull * ns;
+    L.smem = streamed ? stream_smem_bytes(nm) : bin_smem_bytes(nm, ns, L.n_inc);
+}
+
+void build_all(const mb_batch_desc* b, const std::vector<RobotPack>& packs,
+               const std::vector<std::vector<uint32_t>>& plan, const std::vector<int>& slot_of,
+               bool streamed, unsigned threads, Packed& out) {
+    const uint32_t nb = (uint32_t)plan.size(), R = (uint32_t)packs.size();
+    std::vector<BinLocal> locals(nb);
+    parallel_for(nb, threads, [&](uint32_t i) { build_bin(b, packs, plan[i], slot_of, streamed, locals[i]); });
+    out.bins.assign(nb, BinDesc{});
+    out.robot_bin.assign(R, 0);
+    out.mass_gidx.clear();
+    out.spring_gidx.clear();
+    out.pair.clear();
+    out.lbar.clear();
+    out.slice_off.clear();
+    out.slice_width.clear();
+    out.inc.clear();
+    out.inc32.clear();
+    out.max_smem = 0;
+    out.inc_entries = out.inc_padding = 0;
+    out.aligned_slices = out.rank_slices = 0;
+    for (uint32_t i = 0; i < nb; ++i) {
+        const BinLocal& L = locals[i];
+        BinDesc& d = out.bins[i];
+        std::memset(&d, 0, sizeof(d));
+        d.mass_begin = (uint32_t)out.mass_gidx.size();
+        d.n_mass = L.n_mass;
+        d.spring_begin = (uint32_t)out.spring_gidx.size();
+        d.n_spring = L.n_spring;
+        d.inc_begin = (uint32_t)(streamed ? out.inc32.size() : out.inc.size());
+        d.n_inc = L.n_inc;
+        d.slice_begin = (uint32_t)out.slice_off.size();
+        for (uint32_t r : plan[i]) out.robot_bin[r] = i;
+        out.mass_gidx.insert(out.mass_gidx.end(), L.mass_gidx.begin(), L.mass_gidx.end());
+        out.spring_gidx.insert(out.spring_gidx.end(), L.spring_gidx.begin(), L.spring_gidx.end());
+        out.pair.insert(out.pair.end(), L.pair.begin(), L.pair.end());
+        out.lbar.insert(out.lbar.end(), L.lbar.begin(), L.lbar.end());
+        out.slice_off.insert(out.slice_off.end(), L.slice_off.begin(), L.slice_off.end());
+        out.slice_width.insert(out.slice_width.end(), L.slice_width.begin(), L.slice_width.end());
+        if (streamed)
+            out.inc32.insert(out.inc32.end(), L.inc32.begin(), L.inc32.end());
+        else
+            out.inc.insert(out.inc.end(), L.inc.begin(), L.inc.end());
+        out.max_smem = std::max(out.max_smem, L.smem);
+        out.inc_entries += L.n_inc;
+        out.inc_padding += L.padding;
+        out.aligned_slices += L.aligned;
+        out.rank_slices += L.ranked;
+    }
+}
+
+}  // namespace
+
+mb_status pack_population(const mb_batch_desc* b, const PackOptions& o, Packed& out, std::string& err) {
+    const uint32_t R = b->n_robots;
+    const unsigned threads = o.threads ? o.threads : std::max(1u, std::thread::hardware_concurrency());
+    std::vector<RobotPack> packs(R);
+    parallel_for(R, threads, [&](uint32_t r) { preprocess(b, r, packs[r]); });
+    for (uint32_t r = 0; r < R; ++r)
+        if (packs[r].status != MB_OK) {
+            err = packs[r].error;
+            return packs[r].status;
+        }
+    uint64_t tot_s = 0, tot_m = 0;
+    uint32_t max_s = 0, max_m = 0;
+    for (const auto& p : packs) {
+        tot_s += p.springs.size();
+        tot_m += p.n_mass;
+        max_s = std::max<uint32_t>(max_s, (uint32_t)p.springs.size());
+        max_m = std::max(max_m, p.n_mass);
+    }
+    out.masses = tot_m;
+    out.active_springs = tot_s;
+
+    // material slots: the composite ids used by the whole population
+    std::vector<int> slot_of(MB_COMPOSITE_COUNT, -1);
+    for (uint32_t r = 0; r < R; ++r)
+        for (uint32_t ls : packs[r].springs) slot_of[b->spring_material[b->spring_offsets[r] + ls]] = 0;
+    out.mat_ids.clear();
+    for (int m = 0; m < MB_COMPOSITE_COUNT; ++m)
+        if (slot_of[m] == 0) {
+            slot_of[m] = (int)out.mat_ids.size();
+            out.mat_ids.push_back((uint8_t)m);
+        }
+
+    std::vector<KernelShape> shapes;
+    if (o.override.threads && !o.override.streamed)
+        shapes.push_back({o.override.threads, o.override.springs_per_thread, o.override.masses_per_thread});
+    else if (!o.override.streamed)
+        for (const auto& s : kAuto) shapes.push_back(s);
+    const uint32_t sms = std::max<uint32_t>(o.sms, 1);
+    std::vector<std::vector<uint32_t>> plan;
+    bool ok = false;
+    for (const auto& sh : shapes) {
+        if (!shape_supported(sh)) continue;
+        const uint64_t cap_s = std::min<uint64_t>((uint64_t)sh.threads * sh.spt, kMaxBinSprings);
+        const uint64_t cap_m = std::min<uint64_t>((uint64_t)sh.threads * sh.mpt, 4096);
+        if (max_s > cap_s || max_m > cap_m) continue;
+        uint32_t nb = o.override.bins;
+        const bool fixed = nb != 0;
+        uint32_t wave = sms;
+        if (!nb) {
+            const uint64_t need = std::max<uint64_t>((tot_s + cap_s - 1) / cap_s, (tot_m + cap_m - 1) / cap_m);
+            nb = (uint32_t)std::max<uint64_t>(need, 1);
+            if (R >= sms) {
+                // One wave = SMs x resident CTAs per SM; shared memory is
+                // estimated at the even share of the population.
+                const uint32_t est_smem = std::min<uint32_t>(
+                    o.smem_cap, bin_smem_bytes((uint32_t)std::min<uint64_t>(cap_m, tot_m / sms + 1),
+                                               (uint32_t)std::min<uint64_t>(cap_s, tot_s / sms + 1),
+                                               (uint32_t)std::min<uint64_t>(3 * cap_s, 3 * (tot_s / sms + 1))));
+                const int per_sm = o.ctas_per_sm ? std::max(1, o.ctas_per_sm(sh, est_smem)) : 1;
+                wave = sms * (uint32_t)per_sm;
+                nb = std::max<uint32_t>(nb, wave);
+                nb = (nb + wave - 1) / wave * wave;  // whole waves
+            }
+            nb = std::min<uint32_t>(nb, R);
+        }
+        for (uint32_t tries = 0; tries < 16; ++tries) {
+            if (plan_bins(packs, nb, sh, o.smem_cap, plan)) {
+                build_all(b, packs, plan, slot_of, false, threads, out);
+                if (out.max_smem <= o.smem_cap) {
+                    ok = true;
+                    break;
+                }
+            }
+            if (fixed || nb >= R) break;
+            nb = std::min<uint32_t>(R, nb + wave);
+        }
+        if (ok) {
+            out.shape = sh;
+            out.n_bins = nb;
+            out.streamed = false;
+            break;
+        }
+    }
+    // Streamed: when forced, or when no resident shape holds the largest
+    // robot.  One robot per bin.
+    if (o.override.streamed || !ok) {
+        const uint32_t mpt = max_m <= 2048 ? 2u : 4u;
+        if (max_m <= 4096 && stream_supported(1024, mpt)) {
+            plan.assign(R, {});
+            for (uint32_t r = 0; r < R; ++r) plan[r].push_back(r);
+            build_all(b, packs, plan, slot_of, true, threads, out);
+            if (out.max_smem <= o.smem_cap) {
+                ok = true;
+                out.streamed = true;
+                out.shape = KernelShape{1024, 0, mpt};
+                out.n_bins = R;
+            }
+        }
+    }
+    if (!ok) {
+        char buf[256];
+        std::snprintf(buf, sizeof(buf),
+                      "population does not fit any compiled kernel shape (largest robot: %u springs, %u masses)",
+                      max_s, max_m);
+        err = buf;
+        return MB_ERR_CAPACITY;
+    }
+    return MB_OK;
+}
+
+}  // namespace mb

@@ -1,0 +1,46 @@
+// Host-side packing of a population into bins (no CUDA calls).
+#pragma once
+
+#include <cstdint>
+#include <functional>
+#include <string>
+#include <vector>
+
+#include "../../include/mercury_b200.h"
+#include "mb_internal.h"
+
+namespace mb {
+
+struct PackOptions {
+    uint32_t sms = 148;            // SMs of the device
+    uint32_t smem_cap = 232448;    // dynamic shared memory per CTA, bytes
+    uint32_t mode = 0;             // step mode (for occupancy queries)
+    mb_launch_config override{};   // zero fields = automatic choice
+    // resident CTAs per SM of a shape with a given dynamic shared memory;
+    // empty = 1
+    std::function<int(const KernelShape&, uint32_t)> ctas_per_sm;
+    unsigned threads = 0;          // host threads (0 = hardware concurrency)
+};
+
+struct Packed {
+    KernelShape shape{0, 0, 0};
+    uint32_t n_bins = 0;
+    bool streamed = false;
+    uint32_t max_smem = 0;
+    std::vector<BinDesc> bins;
+    std::vector<uint32_t> mass_gidx, spring_gidx, pair, slice_off, slice_width, robot_bin;
+    std::vector<uint16_t> inc;    // resident rows
+    std::vector<uint32_t> inc32;  // streamed rows
+    std::vector<float> lbar;
+    std::vector<uint8_t> mat_ids;
+    // statistics
+    uint64_t masses = 0, active_springs = 0, inc_entries = 0, inc_padding = 0;
+    uint32_t aligned_slices = 0, rank_slices = 0;
+};
+
+// Validates `b`, chooses the launch shape and bin count (or applies the
+// override), and builds the packed arrays.  On failure returns the status
+// and a message in `err`.
+mb_status pack_population(const mb_batch_desc* b, const PackOptions& o, Packed& out, std::string& err);
+
+}  // namespace mb

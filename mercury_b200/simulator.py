@@ -236,3 +236,19 @@ def body_length(batch: Batch) -> np.ndarray:
         hi = max(0.0, float(x.max())) if x.size else 0.0
         out[r] = max(abs(np.float32(hi) - np.float32(lo)), 1.0)
     return out
+
+
+def plan(batch: Batch, num_sms: int = 148, smem_bytes: int = 0, **cfg) -> dict:
+    """Launch plan of a population computed on the host, without a GPU
+    (mb_plan_population): shape, bins, path and packed-layout statistics."""
+    d = _lib.BatchDesc(
+        batch.n_robots, _lib.ptr(batch.mass_offsets), _lib.ptr(batch.pos), _lib.ptr(batch.vel),
+        _lib.ptr(batch.mass_material), _lib.ptr(batch.spring_offsets), _lib.ptr(batch.pairs),
+        _lib.ptr(batch.spring_material), _lib.ptr(batch.lbar))
+    c = _lib.LaunchConfig(cfg.get("threads", 0), cfg.get("springs_per_thread", 0),
+                          cfg.get("masses_per_thread", 0), cfg.get("bins", 0), cfg.get("chunk", 0),
+                          cfg.get("use_graph", 1), cfg.get("streamed", 0))
+    st = _lib.PlanStats()
+    _lib.check(_lib.LIB.mb_plan_population(ctypes.byref(d), ctypes.byref(c), num_sms, smem_bytes,
+                                           ctypes.byref(st)))
+    return {f: getattr(st, f) for f, _ in st._fields_}
