@@ -25,13 +25,16 @@ def test_large_robots_are_streamed():
 
 def test_forced_shape_and_bins():
     b = robots.population_batch("small")
-    st = mb.plan(b, threads=512, springs_per_thread=8, masses_per_thread=2, bins=4)
-    assert (st["threads"], st["springs_per_thread"], st["bins"]) == (512, 8, 4)
+    st = mb.plan(b, threads=512, springs_per_thread=8, masses_per_thread=2, bins=8)
+    assert (st["threads"], st["springs_per_thread"], st["bins"], st["streamed"]) == (512, 8, 8, 0)
+    # a bin count too small for the shape's capacity falls back to streaming
+    assert mb.plan(b, threads=512, springs_per_thread=8, masses_per_thread=2, bins=2)["streamed"] == 1
 
 
-def test_smaller_gpu_gets_fewer_bins():
+def test_bins_follow_the_sm_count():
     b = robots.population_batch("uneven")
-    assert mb.plan(b, num_sms=74)["bins"] < mb.plan(b, num_sms=148)["bins"]
+    assert mb.plan(b, num_sms=296)["bins"] == 296  # one bin per SM when robots allow
+    assert mb.plan(b, num_sms=74)["bins"] % 74 == 0  # whole waves
 
 
 def test_oversized_robot_is_rejected():
