@@ -13,6 +13,11 @@ numpy PCG64):
   uneven     512 robots, side uniform in 3..8, same materials
   streamed   64 robots of 10x10x10 cells, all occupied, iid over
              {bone, tissue, muscle_a, muscle_b}
+  nn         256 point-cloud robots (nn_robot): 500..2000 masses uniform in
+             an ellipsoid with semi-axes 0.3/0.2/0.15 m, 25-nearest-neighbour
+             springs (deduplicated), materials from a random tanh MLP
+             3 -> 25 -> 25 -> 4 over the position (argmax over bone, tissue,
+             muscle_a, muscle_b)
 For the reference step, muscle_a is adductor_muscle0 (phase 0) and muscle_b
 abductor_muscle0 (phase pi), material.h:112, 122.  The force-based
 configurations give every mass 0.1 kg (population(..., mass=0.1)) and use
@@ -70,12 +75,51 @@ def random_cells(side: int, rng: np.random.Generator, choices=FIVE, p=FIVE_P) ->
     return choices[rng.choice(len(choices), size=(side, side, side), p=p)]
 
 
+def nn_robot(rng: np.random.Generator, n_masses: int, k: int = 25, axes=(0.3, 0.2, 0.15),
+             hidden=(25, 25), mass: float = 0.1) -> Element:
+    """Point-cloud robot: masses uniform in an ellipsoid, k-nearest-neighbour
+    springs (each unordered pair once, the lower index first) with the
+    initial distance as mean length and the composite material of their two
+    masses; mass materials from a random-init tanh MLP over (x, y, z)."""
+    from .materials import composite_id
+    pts = []
+    a = np.asarray(axes, np.float64)
+    while sum(len(p) for p in pts) < n_masses:
+        c = rng.uniform(-1.0, 1.0, size=(2 * n_masses, 3))
+        pts.append(c[(c * c).sum(1) <= 1.0] * a)
+    p = np.concatenate(pts)[:n_masses]
+    p[:, 2] -= p[:, 2].min()  # lowest mass on z = 0
+    p = p.astype(np.float32)
+    # material MLP: 3 -> 25 -> 25 -> 4 over the position in ellipsoid units,
+    # tanh, argmax; unit-variance weights, small biases
+    x = (p - p.mean(0)).astype(np.float64) / a
+    for h in (*hidden, 4):
+        w = rng.normal(0.0, 1.0 / np.sqrt(x.shape[1]), size=(x.shape[1], h)) * 2.0
+        bias = rng.normal(0.0, 0.1, size=h)
+        x = x @ w + bias
+        if h != 4:
+            x = np.tanh(x)
+    mats = FOUR[np.argmax(x, axis=1)]
+    # k nearest neighbours of every mass (float32 distances, ties by index)
+    d2 = ((p[:, None, :] - p[None, :, :]) ** 2).sum(-1)
+    np.fill_diagonal(d2, np.inf)
+    nb = np.argsort(d2, axis=1, kind="stable")[:, :k]
+    i = np.repeat(np.arange(n_masses), k)
+    j = nb.reshape(-1)
+    pairs = np.unique(np.stack([np.minimum(i, j), np.maximum(i, j)], 1), axis=0)
+    diff = p[pairs[:, 0]] - p[pairs[:, 1]]
+    lbar = np.sqrt((diff * diff).sum(1)).astype(np.float32)
+    smat = np.array([composite_id(int(mats[u]), int(mats[v])) for u, v in pairs], np.uint8)
+    return Element(p, mats, pairs.astype(np.uint16), lbar, smat, mass=np.full(n_masses, mass, np.float32))
+
+
 def population(name: str, n_robots: int | None = None, seed_base: int | None = None,
                mass: float = 1.0) -> list[Element]:
     """One of the named synthetic populations (see module docstring)."""
     spec = {
         "small": (0, 32),
         "uneven": (1, 512),
+        "nn": (2, 256),
         "streamed": (4, 64),
     }
     if name not in spec:
@@ -86,6 +130,9 @@ def population(name: str, n_robots: int | None = None, seed_base: int | None = N
     out = []
     for r in range(n):
         rng = np.random.default_rng(seed0 + r)
+        if name == "nn":
+            out.append(nn_robot(rng, int(rng.integers(500, 2001)), mass=mass))
+            continue
         if name == "small":
             cells = random_cells(4, rng)
         elif name == "uneven":

@@ -67,3 +67,24 @@ def test_population_shapes():
 def test_builder_rejects_bad_input():
     with pytest.raises(mb.MercuryError):
         robots.lattice_robot(np.full((2, 2, 2), 99, np.uint8))
+
+
+def test_nn_robots_shape():
+    """Point-cloud robots: masses in the ellipsoid, lowest on z = 0, 25-NN
+    springs deduplicated (each pair once, lower index first), mean length =
+    initial distance, composite material of the two masses."""
+    from mercury_b200.materials import composite_id
+    for e in robots.population("nn", 3, mass=0.1):
+        assert 500 <= e.n_masses <= 2000
+        p = e.pos.astype(np.float64)
+        assert p[:, 2].min() == 0.0
+        assert ((p[:, 0] / 0.3) ** 2 + (p[:, 1] / 0.2) ** 2 <= 1.0 + 1e-5).all()
+        assert (e.pairs[:, 0] < e.pairs[:, 1]).all()
+        assert len({tuple(x) for x in e.pairs}) == e.n_springs
+        assert e.n_springs >= 25 * e.n_masses // 2
+        d = np.linalg.norm(e.pos[e.pairs[:, 0]] - e.pos[e.pairs[:, 1]], axis=1)
+        assert np.allclose(d, e.mean_length, rtol=1e-6)
+        exp = [composite_id(int(e.mass_material[u]), int(e.mass_material[v])) for u, v in e.pairs[:50]]
+        assert list(e.spring_material[:50]) == exp
+        assert len(np.unique(e.mass_material)) >= 2
+        assert np.all(e.mass == np.float32(0.1))

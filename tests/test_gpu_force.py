@@ -69,3 +69,21 @@ def test_mode_switch_keeps_reference_step_exact():
     p, v = b.pos.copy(), b.vel.copy()
     core.xpbd_run(b, p, v, np.zeros(b.n_springs, np.float32), mb.material_table(), 1e-3, 0.0, 100, False)
     assert np.array_equal(bits(pos), bits(p))
+
+
+def test_nn_robots_in_water_streamed_bit_exact():
+    """Point-cloud robots (25-NN springs, up to ~28k springs each) in water
+    with stress tracking: streamed path, bit-exact against the oracle."""
+    b = robots.population_batch("nn", 4, mass=0.1)
+    sim = mb.Simulator(0)
+    sim.set_materials(mb.materials.force_table())
+    sim.set_mode(2)
+    sim.set_environment(**S.WATER)
+    sim.setTimeStep(1e-4)
+    sim.set_batch(b)
+    assert sim.launch_config()["streamed"] == 1
+    sim.run_steps(200, True)
+    pos, vel, stress = sim.collect_arrays()
+    p, v, s = oracle(2, b, S.WATER, 200, True)
+    assert np.array_equal(bits(pos), bits(p)) and np.array_equal(bits(vel), bits(v))
+    assert np.array_equal(bits(stress), bits(s))
