@@ -191,7 +191,7 @@ def run_ours(args, rank, local_rank, world):
     tuned = None
     if not args.no_autotune:
         from mercury_b200 import autotune
-        tuned = autotune.tune(sim, batch, track=track, steps=300, use_cache=False)
+        tuned = autotune.tune(sim, batch, track=track, steps=300, use_cache=args.autotune_cache)
     steps_per_eval = None
 
     stream = torch.cuda.ExternalStream(sim.stream, device=dev)
@@ -395,7 +395,52 @@ def secondary(args, batch, local_rank, dev, hbm_peak):
                        "roofline": {"bound": "hbm", "achieved": rate * hbm_b / 1e9, "peak": hbm_peak,
                                     "unit": "GB/s", "frac": rate * hbm_b / 1e9 / hbm_peak,
                                     "bytes_per_update": hbm_b}}
+    del ss
+    out["devo"] = devo_bench(local_rank)
     return out
+
+
+DEVO_ROBOTS, DEVO_K = 512, 128
+
+
+def devo_population():
+    """DevoBenchmark's population (optimize/benchmark.cpp:171-217): copies of
+    the reference's default VoxelRobot (VoxelRobot::Initialize,
+    VoxelRobot.cpp:352-381: 12^3 points, bone inside, air on the upper
+    faces; 1,728 masses, 18,788 springs)."""
+    import mercury_b200 as mb
+    from mercury_b200 import robots
+    grid = np.full((12, 12, 12), 22, np.uint8)
+    grid[11, :, :] = grid[:, 11, :] = grid[:, :, 11] = 0
+    e = robots.lattice_robot(grid, 1.0)
+    return mb.pack([e] * DEVO_ROBOTS)
+
+
+def devo_bench(local_rank, calls=3):
+    """Springs replaced per second by Devo() with the reference's default
+    replaced_springs_per_element (128, config.h:18) on 512 default robots,
+    after 100 stress-tracked steps; wall time of the synchronous call
+    (selection kernel, read-back, host re-pack, upload)."""
+    import mercury_b200 as mb
+    b = devo_population()
+    sim = mb.Simulator(local_rank)
+    sim.setTimeStep(1e-4)
+    sim.set_batch(b)
+    sim.run_steps(100, True)
+    sim.synchronize()
+    walls, phases = [], []
+    for i in range(calls):
+        t0 = time.perf_counter()
+        n = sim.devo(DEVO_K, i)
+        walls.append(time.perf_counter() - t0)
+        phases.append(sim.devo_profile())
+    w = float(np.median(walls))
+    ph = phases[int(np.argsort(walls)[len(walls) // 2])]
+    return {"metric": "springs replaced/s", "value": n / w, "unit": "springs/s", "replaced_per_call": n,
+            "ms_per_call": 1e3 * w, "phases_ms": ph,
+            "workload": f"{DEVO_ROBOTS} default voxel robots (1,728 masses, 18,788 springs), "
+                        f"{DEVO_K} springs per robot, after 100 tracked steps",
+            "path": "streamed" if sim.launch_config()["streamed"] else "resident"}
 
 
 def run_reference(args, rank, local_rank, world):
@@ -430,12 +475,16 @@ def run_reference(args, rank, local_rank, world):
         core.xpbd_run(batch, p, v, s, table, dt, 0.0, sample, track, threads)
         tt += time.perf_counter() - t0
     value = active * sample * args.steps / tt
-    ref_cuda = None
+    ref_cuda = ref_devo = None
     if not args.no_ref_cuda:
         try:
             ref_cuda = reference_cuda(batch, dt, duration, track)
         except Exception as e:  # the reference's GPU path is optional evidence
             ref_cuda = {"unavailable": str(e)[:200]}
+        try:
+            ref_devo = reference_devo()
+        except Exception as e:
+            ref_devo = {"unavailable": str(e)[:200]}
     return {
         "impl": "reference",
         "metric": "spring-updates/s",
@@ -458,6 +507,7 @@ def run_reference(args, rank, local_rank, world):
                          "sample": f"all {batch.n_robots} robots x {sample} steps per bench step"},
         "e2e": {"value": value, "unit": "spring-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "reference_cuda": ref_cuda,
+        "reference_cuda_devo": ref_devo,
     }
 
 
@@ -496,6 +546,40 @@ def reference_cuda(batch, dt, duration, track):
                     "per step, D2H); masses padded per robot to the largest count"}
 
 
+def _ref_lib():
+    import ctypes
+    path = os.path.join(ROOT, "oracle", "_ref", "libmercury_ref.so")
+    if not os.path.exists(path):
+        return None
+    return ctypes.CDLL(path)
+
+
+def reference_devo(calls=3):
+    """The reference's Simulator::Devo (oracle/_ref) on the population of
+    devo_bench, timed per call on the host clock as DevoBenchmark does."""
+    import ctypes
+    L = _ref_lib()
+    if L is None:
+        return {"unavailable": "oracle/_ref/libmercury_ref.so not built"}
+    b = devo_population()
+    L.ref_devo_time.argtypes = ([ctypes.c_int] + [ctypes.c_void_p] * 8 +
+                                [ctypes.c_uint, ctypes.c_float, ctypes.c_float, ctypes.c_int, ctypes.c_void_p])
+    L.ref_devo_time.restype = ctypes.c_int
+    P = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+    mo, so = b.mass_offsets.astype(np.int32), b.spring_offsets.astype(np.int32)
+    pos3, vel3 = np.ascontiguousarray(b.pos[:, :3]), np.ascontiguousarray(b.vel[:, :3])
+    secs = np.zeros(calls, np.float64)
+    L.ref_devo_time(b.n_robots, P(mo), P(pos3), P(vel3), P(b.mass_material), P(so),
+                    P(np.ascontiguousarray(b.pairs)), P(b.lbar), P(b.spring_material),
+                    DEVO_K, 1e-4, 0.01, calls, P(secs))
+    w = float(np.median(secs))
+    n = DEVO_ROBOTS * DEVO_K
+    return {"metric": "springs replaced/s", "value": n / w, "unit": "springs/s", "ms_per_call": 1e3 * w,
+            "calls_ms": [1e3 * x for x in secs],
+            "note": "Simulator::Devo after Simulate(0.01 s, track): CUB segmented sort (with its own "
+                    "cudaMalloc/cudaFree), cuRAND pairs, replaceSprings; host clock per call"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -507,7 +591,9 @@ def main():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-ref-cuda", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
-    ap.add_argument("--no-extra", action="store_true", help="skip the force-mode and streamed lines")
+    ap.add_argument("--no-extra", action="store_true", help="skip the force-mode, streamed and devo lines")
+    ap.add_argument("--autotune-cache", action="store_true",
+                    help="reuse (and store) the autotuner's choice in its cache file instead of re-tuning")
     args = ap.parse_args()
 
     from mercury_b200 import dist

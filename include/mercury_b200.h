@@ -186,6 +186,38 @@ MB_API void* mb_get_stream(const mb_context* ctx);
  * that keep inputs resident on the device. */
 MB_API mb_status mb_device_state(mb_context* ctx, void** pos, void** vel, void** stress);
 
+/* Development (Simulator::Devo, Simulator.cu:640-668, with the kernels of
+ * devo_kernel.cu:56-184 and the stress sort of Simulator.cu:597-631).  For
+ * every robot with at least two masses, the springs of stress ranks [0, k)
+ * -- stress accumulated by runs with stress tracking, descending, ties by
+ * ascending spring index -- get a random pair of distinct masses, the
+ * composite material of the two masses and the mean length
+ * |x_a - x_b| / (1 + dL0 sin(omega t + phi)) at the current clock.  With
+ * MB_DEVO_REFERENCE_RANKS, robot r replaces ranks [r k, r k + k) instead, the
+ * window the reference's indexing selects (devo_kernel.cu:112-116), clipped
+ * to the robot's own springs.  The pairs come from a counter-based
+ * generator over (seed, robot, rank), not cuRAND: same seed, same result on
+ * any device.  Stresses are kept (as in the reference); positions and
+ * velocities are untouched.  The population is re-packed for the step
+ * kernels (the launch override stays if the population still fits it).
+ * Synchronous.  k <= MB_DEVO_MAX_REPLACED; *n_replaced (may be NULL) gets
+ * the number of springs replaced. */
+#define MB_DEVO_MAX_REPLACED 1024
+#define MB_DEVO_REFERENCE_RANKS 1u
+MB_API mb_status mb_devo(mb_context* ctx, uint32_t replaced_per_robot, uint64_t seed, uint32_t flags,
+                         uint32_t* n_replaced);
+
+/* Host wall time of the phases of the last mb_devo, in ms: ms[0] selection
+ * kernel and read-back of the new springs, ms[1] re-packing on the host,
+ * ms[2] upload of the packed arrays.  No reference counterpart. */
+MB_API mb_status mb_devo_profile(const mb_context* ctx, double* ms);
+
+/* Topology in the upload layout (2 pair entries, 1 material, 1 mean length
+ * per spring; any pointer may be NULL), as changed by mb_devo.  The
+ * reference copies pairs, materials and mean lengths back in Collect
+ * (Simulator.cu:542-561). */
+MB_API mb_status mb_collect_springs(mb_context* ctx, uint16_t* pairs, uint8_t* material, float* lbar);
+
 /* Launch configuration: read, override (0 fields keep the automatic
  * choice), and the automatic choice for the uploaded batch. */
 MB_API mb_status mb_get_launch_config(const mb_context* ctx, mb_launch_config* cfg);

@@ -25,6 +25,8 @@ STATUS_NAMES = {
 }
 COMPOSITE_COUNT = 254
 MODE_REF_XPBD, MODE_FORCE_LAND, MODE_FORCE_WATER = 0, 1, 2
+DEVO_MAX_REPLACED = 1024
+DEVO_REFERENCE_RANKS = 1
 
 
 class MercuryError(RuntimeError):
@@ -109,6 +111,9 @@ def _load() -> ctypes.CDLL:
         "mb_plan_population": (I32, [ctypes.POINTER(BatchDesc), ctypes.POINTER(LaunchConfig), U32, U32,
                                      ctypes.POINTER(PlanStats)]),
         "mb_voxel_build": (I32, [I32, I32, I32, F32, P, ctypes.POINTER(I32), ctypes.POINTER(I32), P, P, P, P, P]),
+        "mb_devo": (I32, [P, U32, ctypes.c_uint64, U32, ctypes.POINTER(U32)]),
+        "mb_collect_springs": (I32, [P, P, P, P]),
+        "mb_devo_profile": (I32, [P, P]),
         "mb_version": (ctypes.c_char_p, []),
     }
     for name, (res, args) in sigs.items():

@@ -155,11 +155,23 @@ void Simulator::Simulate(float sim_duration, bool trackStresses, bool trace, std
 }
 
 void Simulator::Devo() {
-    std::fprintf(stderr, "mercury_b200: Devo is not available; springs are unchanged\n");
+    // Simulator.cu:640-668: the seed counts Devo calls from 0 (per simulator
+    // here; the reference's counter is a function-local static).
+    check(ctx_, mb_devo(ctx_, m_config.replaced_springs_per_element, (uint64_t)devoSeed_, 0, nullptr),
+          "mb_devo");
+    ++devoSeed_;
 }
 
 void Simulator::download() {
     check(ctx_, mb_collect(ctx_, pos_.data(), vel_.data(), stress_.data()), "mb_collect");
+    // pairs, materials and mean lengths as Devo left them (Simulator.cu:542-561)
+    check(ctx_, mb_collect_springs(ctx_, pairs_.data(), springMat_.data(), lbar_.data()), "mb_collect_springs");
+    for (size_t s = 0; s < springBuf_.size(); ++s) {
+        springBuf_[s].m0 = pairs_[2 * s];
+        springBuf_[s].m1 = pairs_[2 * s + 1];
+        springBuf_[s].mean_length = lbar_[s];
+        springBuf_[s].material = materials::id_lookup(springMat_[s]);
+    }
     std::vector<uint32_t> flags(elements_.size(), 0);
     check(ctx_, mb_robot_flags(ctx_, flags.data()), "mb_robot_flags");
     for (size_t r = 0; r < flags.size(); ++r)

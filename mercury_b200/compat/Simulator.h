@@ -77,6 +77,7 @@ private:
     std::vector<float> pos_, vel_, stress_, lbar_;
     std::vector<uint8_t> massMat_, springMat_;
     std::vector<uint16_t> pairs_;
+    uint64_t devoSeed_ = 0;
 };
 
 #endif

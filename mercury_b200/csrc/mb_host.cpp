@@ -16,6 +16,7 @@
 //     rows are stored 32 masses per slice, column-major (SELL-32), so that a
 //     warp's k-th entries are consecutive words.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -33,6 +34,7 @@
 #include <unistd.h>
 
 #include "../../include/mercury_b200.h"
+#include "mb_devo.h"
 #include "mb_internal.h"
 #include "mb_pack.h"
 
@@ -147,6 +149,16 @@ struct mb_context {
     mb::DevBuf<uint32_t> bin_flags, robot_bin, robot_flags;
     mb::DevBuf<float> com;
 
+    // topology in upload order, kept on the host for re-packing after
+    // development (mb_devo) and for mb_collect_springs
+    std::vector<uint16_t> h_pairs;
+    std::vector<uint8_t> h_spring_mat, h_mass_mat;
+    std::vector<float> h_lbar;
+    mb::DevBuf<int64_t> d_spring_off;
+    mb::DevBuf<mb::DevoRecord> devo_out;
+    std::vector<mb::DevoRecord> h_devo;
+    double devo_ms[3] = {0.0, 0.0, 0.0};  // last mb_devo: select+read-back, re-pack, upload
+
     std::map<mb::GraphKey, cudaGraphExec_t> graphs;
 
     void clear_graphs() {
@@ -222,6 +234,79 @@ mb_status cuda_fail(mb_context* c, cudaError_t e, const char* what) {
     } while (0)
 
 }  // namespace
+
+namespace mb_detail {
+
+// Packs a population (caller's arrays or the context's host copy) with the
+// context's device limits and launch override.  With `fallback_auto`, a
+// population that no longer fits the override (after development) is
+// re-planned automatically.
+mb_status pack(mb_context* ctx, const mb_batch_desc* b, bool fallback_auto, mb::Packed& out) {
+    mb::PackOptions po;
+    po.sms = (uint32_t)std::max(ctx->num_sms, 1);
+    po.smem_cap = mb::max_step_smem(ctx->device);
+    po.mode = (uint32_t)ctx->mode;
+    po.override = ctx->override_cfg;
+    po.ctas_per_sm = [ctx](const mb::KernelShape& sh, uint32_t smem) {
+        return mb::ctas_per_sm(sh, (uint32_t)ctx->mode, false, smem);
+    };
+    std::string err;
+    mb_status pst = mb::pack_population(b, po, out, err);
+    const mb_launch_config none{};
+    if (pst == MB_ERR_CAPACITY && fallback_auto && std::memcmp(&po.override, &none, sizeof(none)) != 0) {
+        MB_TRACE("override no longer fits (%s); automatic plan", err.c_str());
+        po.override = none;
+        po.override.chunk = ctx->override_cfg.chunk;
+        po.override.use_graph = ctx->override_cfg.use_graph;
+        pst = mb::pack_population(b, po, out, err);
+    }
+    if (pst != MB_OK) return fail(ctx, pst, "%s", err.c_str());
+    return MB_OK;
+}
+
+// Uploads the packed arrays of `out` and the per-launch buffers sized by
+// them; positions, velocities and stresses are not touched.
+mb_status upload_packed(mb_context* ctx, const mb::Packed& out) {
+    ctx->clear_graphs();
+    ctx->shape = out.shape;
+    ctx->n_bins = out.n_bins;
+    ctx->smem_bytes = out.max_smem;
+    ctx->streamed = out.streamed;
+    ctx->stream_mpt = out.shape.mpt;
+    const uint32_t nb = out.n_bins;
+    cudaStream_t st = ctx->stream;
+    auto up = [&](auto& buf, const auto* src, size_t n) -> cudaError_t {
+        cudaError_t e = buf.alloc(n);
+        if (e != cudaSuccess || n == 0) return e;
+        return cudaMemcpyAsync(buf.p, src, n * sizeof(*src), cudaMemcpyHostToDevice, st);
+    };
+    MB_CUDA(ctx, up(ctx->bins, out.bins.data(), out.bins.size()));
+    MB_CUDA(ctx, up(ctx->mass_gidx, out.mass_gidx.data(), out.mass_gidx.size()));
+    MB_CUDA(ctx, up(ctx->spring_gidx, out.spring_gidx.data(), out.spring_gidx.size()));
+    MB_CUDA(ctx, up(ctx->spring_pair, out.pair.data(), out.pair.size()));
+    MB_CUDA(ctx, up(ctx->spring_lbar, out.lbar.data(), out.lbar.size()));
+    MB_CUDA(ctx, up(ctx->slice_off, out.slice_off.data(), out.slice_off.size()));
+    MB_CUDA(ctx, up(ctx->slice_width, out.slice_width.data(), out.slice_width.size()));
+    MB_CUDA(ctx, up(ctx->inc, out.inc.data(), out.inc.size()));
+    if (out.streamed) {
+        MB_CUDA(ctx, up(ctx->inc32, out.inc32.data(), out.inc32.size()));
+        MB_CUDA(ctx, ctx->dp_scratch.alloc(std::max<size_t>(out.pair.size(), 1)));
+        MB_CUDA(ctx, ctx->st_scratch.alloc(std::max<size_t>(out.pair.size(), 1)));
+    }
+    MB_CUDA(ctx, up(ctx->mat_ids, out.mat_ids.data(), out.mat_ids.size()));
+    ctx->n_mat_host = (uint32_t)out.mat_ids.size();
+    MB_CUDA(ctx, up(ctx->n_mat, &ctx->n_mat_host, 1));
+    MB_CUDA(ctx, ctx->invk.alloc(std::max<uint32_t>(ctx->n_mat_host, 1)));
+    MB_CUDA(ctx, ctx->rates.alloc((size_t)std::max<uint32_t>(ctx->n_mat_host, 1) * ctx->chunk));
+    MB_CUDA(ctx, up(ctx->robot_bin, out.robot_bin.data(), out.robot_bin.size()));
+    MB_CUDA(ctx, ctx->bin_flags.alloc(nb));
+    MB_CUDA(ctx, cudaMemsetAsync(ctx->bin_flags.p, 0, nb * sizeof(uint32_t), st));
+    // the host vectors of `out` may die after this call: wait for the copies
+    MB_CUDA(ctx, cudaStreamSynchronize(st));
+    return MB_OK;
+}
+
+}  // namespace mb_detail
 
 extern "C" {
 
@@ -418,37 +503,12 @@ mb_status mb_set_elements(mb_context* ctx, const mb_batch_desc* b) {
     if (M >= (1ull << 31) || S >= (1ull << 31)) return fail(ctx, MB_ERR_CAPACITY, "population too large");
 
     cudaSetDevice(ctx->device);
-    mb::PackOptions po;
-    po.sms = (uint32_t)std::max(ctx->num_sms, 1);
-    po.smem_cap = mb::max_step_smem(ctx->device);
-    po.mode = (uint32_t)ctx->mode;
-    po.override = ctx->override_cfg;
-    po.ctas_per_sm = [ctx](const mb::KernelShape& sh, uint32_t smem) {
-        return mb::ctas_per_sm(sh, (uint32_t)ctx->mode, false, smem);
-    };
     mb::Packed out;
-    std::string err;
-    const mb_status pst = mb::pack_population(b, po, out, err);
-    if (pst != MB_OK) return fail(ctx, pst, "%s", err.c_str());
-    ctx->shape = out.shape;
-    ctx->n_bins = out.n_bins;
-    const bool streamed = out.streamed;
-    const uint32_t stream_mpt = out.shape.mpt;
-    const uint32_t nb = ctx->n_bins;
-    const uint32_t max_smem = out.max_smem;
-    auto& bins = out.bins;
-    auto& h_mass_gidx = out.mass_gidx;
-    auto& h_spring_gidx = out.spring_gidx;
-    auto& h_pair = out.pair;
-    auto& h_lbar = out.lbar;
-    auto& h_slice_off = out.slice_off;
-    auto& h_slice_width = out.slice_width;
-    auto& h_inc = out.inc;
-    auto& h_inc32 = out.inc32;
-    auto& h_mat_ids = out.mat_ids;
-    auto& h_robot_bin = out.robot_bin;
+    const mb_status pst = mb_detail::pack(ctx, b, false, out);
+    if (pst != MB_OK) return pst;
 
-    // upload
+    // the population is accepted: keep its topology on the host (for
+    // re-packing after development) and upload state and packed arrays
     ctx->clear_graphs();
     ctx->loaded = false;
     ctx->n_robots = R;
@@ -456,7 +516,10 @@ mb_status mb_set_elements(mb_context* ctx, const mb_batch_desc* b) {
     ctx->n_spring = S;
     ctx->mass_off.assign(b->mass_offsets, b->mass_offsets + R + 1);
     ctx->spring_off.assign(b->spring_offsets, b->spring_offsets + R + 1);
-    ctx->smem_bytes = max_smem;
+    ctx->h_mass_mat.assign(b->mass_material, b->mass_material + M);
+    ctx->h_pairs.assign(b->pairs, b->pairs + 2 * S);
+    ctx->h_spring_mat.assign(b->spring_material, b->spring_material + S);
+    ctx->h_lbar.assign(b->lbar, b->lbar + S);
     cudaStream_t st = ctx->stream;
     auto up = [&](auto& buf, const auto* src, size_t n) -> cudaError_t {
         cudaError_t e = buf.alloc(n);
@@ -467,35 +530,13 @@ mb_status mb_set_elements(mb_context* ctx, const mb_batch_desc* b) {
     MB_CUDA(ctx, up(ctx->vel, reinterpret_cast<const float4*>(b->vel), M));
     MB_CUDA(ctx, up(ctx->mass_mat, b->mass_material, M));
     MB_CUDA(ctx, up(ctx->d_mass_off, b->mass_offsets, R + 1));
+    MB_CUDA(ctx, up(ctx->d_spring_off, b->spring_offsets, R + 1));
     MB_CUDA(ctx, ctx->stress.alloc(S));
     if (S) MB_CUDA(ctx, cudaMemsetAsync(ctx->stress.p, 0, S * sizeof(float), st));
-    MB_CUDA(ctx, up(ctx->bins, bins.data(), bins.size()));
-    MB_CUDA(ctx, up(ctx->mass_gidx, h_mass_gidx.data(), h_mass_gidx.size()));
-    MB_CUDA(ctx, up(ctx->spring_gidx, h_spring_gidx.data(), h_spring_gidx.size()));
-    MB_CUDA(ctx, up(ctx->spring_pair, h_pair.data(), h_pair.size()));
-    MB_CUDA(ctx, up(ctx->spring_lbar, h_lbar.data(), h_lbar.size()));
-    MB_CUDA(ctx, up(ctx->slice_off, h_slice_off.data(), h_slice_off.size()));
-    MB_CUDA(ctx, up(ctx->slice_width, h_slice_width.data(), h_slice_width.size()));
-    MB_CUDA(ctx, up(ctx->inc, h_inc.data(), h_inc.size()));
-    ctx->streamed = streamed;
-    ctx->stream_mpt = stream_mpt;
-    if (streamed) {
-        MB_CUDA(ctx, up(ctx->inc32, h_inc32.data(), h_inc32.size()));
-        MB_CUDA(ctx, ctx->dp_scratch.alloc(std::max<size_t>(h_pair.size(), 1)));
-        MB_CUDA(ctx, ctx->st_scratch.alloc(std::max<size_t>(h_pair.size(), 1)));
-    }
-    MB_CUDA(ctx, up(ctx->mat_ids, h_mat_ids.data(), h_mat_ids.size()));
-    ctx->n_mat_host = (uint32_t)h_mat_ids.size();
-    MB_CUDA(ctx, up(ctx->n_mat, &ctx->n_mat_host, 1));
-    MB_CUDA(ctx, ctx->invk.alloc(std::max<uint32_t>(ctx->n_mat_host, 1)));
-    MB_CUDA(ctx, ctx->rates.alloc((size_t)std::max<uint32_t>(ctx->n_mat_host, 1) * ctx->chunk));
-    MB_CUDA(ctx, up(ctx->robot_bin, h_robot_bin.data(), h_robot_bin.size()));
-    MB_CUDA(ctx, ctx->bin_flags.alloc(nb));
-    MB_CUDA(ctx, cudaMemsetAsync(ctx->bin_flags.p, 0, nb * sizeof(uint32_t), st));
     MB_CUDA(ctx, ctx->robot_flags.alloc(R));
     MB_CUDA(ctx, ctx->com.alloc(3 * (size_t)R));
-    // the host vectors above die with this call: wait for the copies
-    MB_CUDA(ctx, cudaStreamSynchronize(st));
+    const mb_status ust = mb_detail::upload_packed(ctx, out);
+    if (ust != MB_OK) return ust;
     ctx->loaded = true;
     return MB_OK;
 }
@@ -711,6 +752,79 @@ mb_status mb_device_state(mb_context* ctx, void** pos, void** vel, void** stress
     if (pos) *pos = ctx->pos.p;
     if (vel) *vel = ctx->vel.p;
     if (stress) *stress = ctx->stress.p;
+    return MB_OK;
+}
+
+static_assert(MB_DEVO_MAX_REPLACED == mb::kDevoMaxReplaced, "devo limit");
+static_assert(MB_DEVO_REFERENCE_RANKS == mb::kDevoReferenceRanks, "devo flag");
+static_assert(sizeof(mb::DevoRecord) == 16, "devo record");
+
+mb_status mb_devo(mb_context* ctx, uint32_t replaced_per_robot, uint64_t seed, uint32_t flags,
+                  uint32_t* n_replaced) {
+    if (!ctx) return MB_ERR_ARGUMENT;
+    if (n_replaced) *n_replaced = 0;
+    if (!ctx->loaded) return fail(ctx, MB_ERR_STATE, "no population uploaded");
+    if (replaced_per_robot > MB_DEVO_MAX_REPLACED)
+        return fail(ctx, MB_ERR_ARGUMENT, "at most %u springs per robot and call", MB_DEVO_MAX_REPLACED);
+    if (flags & ~(uint32_t)MB_DEVO_REFERENCE_RANKS) return fail(ctx, MB_ERR_ARGUMENT, "unknown devo flags");
+    if (replaced_per_robot == 0 || ctx->n_spring == 0) return MB_OK;
+    cudaSetDevice(ctx->device);
+    using clock = std::chrono::steady_clock;
+    const auto t0 = clock::now();
+    const size_t nrec = (size_t)ctx->n_robots * replaced_per_robot;
+    MB_CUDA(ctx, ctx->devo_out.alloc(nrec));
+    mb::DevoParams p{ctx->stress.p, ctx->d_mass_off.p, ctx->d_spring_off.p, ctx->pos.p, ctx->mass_mat.p,
+                     ctx->d_table.p, ctx->total_time, replaced_per_robot, seed, flags, ctx->devo_out.p};
+    MB_TRACE("devo launch robots=%u k=%u", ctx->n_robots, replaced_per_robot);
+    MB_CUDA(ctx, mb::launch_devo(p, ctx->n_robots, ctx->stream));
+    ctx->h_devo.resize(nrec);
+    MB_CUDA(ctx, cudaMemcpyAsync(ctx->h_devo.data(), ctx->devo_out.p, nrec * sizeof(mb::DevoRecord),
+                                 cudaMemcpyDeviceToHost, ctx->stream));
+    MB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    uint32_t count = 0;
+    for (const mb::DevoRecord& rec : ctx->h_devo) {
+        if (rec.spring == 0xFFFFFFFFu) continue;
+        if (rec.spring >= ctx->n_spring || rec.material >= MB_COMPOSITE_COUNT)
+            return fail(ctx, MB_ERR_STATE, "development record out of range");
+        ctx->h_pairs[2 * (size_t)rec.spring] = (uint16_t)(rec.pair & 0xFFFFu);
+        ctx->h_pairs[2 * (size_t)rec.spring + 1] = (uint16_t)(rec.pair >> 16);
+        ctx->h_spring_mat[rec.spring] = (uint8_t)rec.material;
+        ctx->h_lbar[rec.spring] = rec.lbar;
+        ++count;
+    }
+    const auto t1 = clock::now();
+    const mb_batch_desc d{ctx->n_robots,         ctx->mass_off.data(),   nullptr,
+                          nullptr,               ctx->h_mass_mat.data(), ctx->spring_off.data(),
+                          ctx->h_pairs.data(),   ctx->h_spring_mat.data(), ctx->h_lbar.data()};
+    mb::Packed out;
+    mb_status st = mb_detail::pack(ctx, &d, true, out);
+    const auto t2 = clock::now();
+    if (st == MB_OK) st = mb_detail::upload_packed(ctx, out);
+    if (st != MB_OK) {
+        ctx->loaded = false;  // topology and packed arrays disagree now
+        return st;
+    }
+    const auto t3 = clock::now();
+    ctx->devo_ms[0] = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    ctx->devo_ms[1] = std::chrono::duration<double, std::milli>(t2 - t1).count();
+    ctx->devo_ms[2] = std::chrono::duration<double, std::milli>(t3 - t2).count();
+    if (n_replaced) *n_replaced = count;
+    return MB_OK;
+}
+
+mb_status mb_devo_profile(const mb_context* ctx, double* ms) {
+    if (!ctx || !ms) return MB_ERR_ARGUMENT;
+    for (int i = 0; i < 3; ++i) ms[i] = ctx->devo_ms[i];
+    return MB_OK;
+}
+
+mb_status mb_collect_springs(mb_context* ctx, uint16_t* pairs, uint8_t* material, float* lbar) {
+    if (!ctx) return MB_ERR_ARGUMENT;
+    if (!ctx->loaded) return fail(ctx, MB_ERR_STATE, "no population uploaded");
+    if (pairs && !ctx->h_pairs.empty()) std::memcpy(pairs, ctx->h_pairs.data(), ctx->h_pairs.size() * sizeof(uint16_t));
+    if (material && !ctx->h_spring_mat.empty())
+        std::memcpy(material, ctx->h_spring_mat.data(), ctx->h_spring_mat.size());
+    if (lbar && !ctx->h_lbar.empty()) std::memcpy(lbar, ctx->h_lbar.data(), ctx->h_lbar.size() * sizeof(float));
     return MB_OK;
 }
 

@@ -126,6 +126,10 @@ def unpack(batch: Batch, pos: np.ndarray, vel: np.ndarray, stress: np.ndarray | 
         x = e.copy()
         x.pos = pos[ms, :3].copy()
         x.vel = vel[ms, :3].copy()
+        # topology from the batch: development may have rewired springs
+        x.pairs = batch.pairs[ss].copy()
+        x.spring_material = batch.spring_material[ss].copy()
+        x.mean_length = batch.lbar[ss].copy()
         if stress is not None:
             x.stress = stress[ss].copy()
         out.append(x)

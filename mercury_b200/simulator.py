@@ -19,6 +19,7 @@ Simulator.cu:540); CentreOfMass() reduces on the device.
 from __future__ import annotations
 
 import ctypes
+import dataclasses
 from dataclasses import dataclass
 
 import numpy as np
@@ -69,6 +70,7 @@ class Simulator:
         self._elements: list[Element] = []
         self.config = SimulatorConfig()
         self._table = material_table()
+        self._devo_seed = 0
         _lib.check(_lib.LIB.mb_set_materials(self._ctx, _lib.ptr(self._table)), self._ctx)
         # the reference's m_deltaT before Initialize (Simulator.h:55)
         self.setTimeStep(0.0001)
@@ -108,7 +110,12 @@ class Simulator:
         return n.value
 
     def Devo(self) -> None:
-        raise NotImplementedError("Devo is not part of this build")
+        """Simulator::Devo (Simulator.cu:640-668): rewires every robot's
+        config.replaced_springs_per_element highest-stress springs (see
+        devo()).  The seed counts calls on this simulator from 0, as the
+        reference's static counter does."""
+        self.devo(self.config.replaced_springs_per_element, self._devo_seed)
+        self._devo_seed += 1
 
     def Collect(self, trackers):
         single = isinstance(trackers, ElementTracker)
@@ -161,6 +168,37 @@ class Simulator:
             _lib.ptr(batch.mass_material), _lib.ptr(batch.spring_offsets), _lib.ptr(batch.pairs),
             _lib.ptr(batch.spring_material), _lib.ptr(batch.lbar))
         _lib.check(_lib.LIB.mb_set_elements(self._ctx, ctypes.byref(d)), self._ctx)
+
+    def devo(self, replaced_per_robot: int, seed: int, reference_ranks: bool = False) -> int:
+        """Development (mb_devo): the springs of stress ranks [0, k) of every
+        robot (ranks [r k, r k + k) with reference_ranks) get random mass
+        pairs, the composite material of the pair and the mean length at the
+        current clock.  Updates the batch's topology; returns the number of
+        springs replaced."""
+        n = ctypes.c_uint32()
+        flags = _lib.DEVO_REFERENCE_RANKS if reference_ranks else 0
+        _lib.check(_lib.LIB.mb_devo(self._ctx, int(replaced_per_robot), int(seed), flags,
+                                    ctypes.byref(n)), self._ctx)
+        pairs, mat, lbar = self.collect_springs()
+        self._batch = dataclasses.replace(self._batch, pairs=pairs, spring_material=mat, lbar=lbar)
+        return n.value
+
+    def devo_profile(self) -> dict:
+        """Host wall time (ms) of the phases of the last devo()."""
+        ms = np.zeros(3, np.float64)
+        _lib.check(_lib.LIB.mb_devo_profile(self._ctx, _lib.ptr(ms)), self._ctx)
+        return {"select_ms": float(ms[0]), "pack_ms": float(ms[1]), "upload_ms": float(ms[2])}
+
+    def collect_springs(self):
+        """(pairs (S, 2) uint16, material (S,) uint8, mean length (S,) float32)
+        of the population on the device (mb_collect_springs)."""
+        S = self._batch.n_springs
+        pairs = np.empty((S, 2), np.uint16)
+        mat = np.empty(S, np.uint8)
+        lbar = np.empty(S, np.float32)
+        _lib.check(_lib.LIB.mb_collect_springs(self._ctx, _lib.ptr(pairs), _lib.ptr(mat), _lib.ptr(lbar)),
+                   self._ctx)
+        return pairs, mat, lbar
 
     def set_state(self, pos: np.ndarray, vel: np.ndarray) -> None:
         pos = np.ascontiguousarray(pos, np.float32)

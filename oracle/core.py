@@ -46,6 +46,13 @@ def lib() -> ctypes.CDLL:
         L.or_force_run.restype = I32
         L.or_force_run_f64.argtypes = [I32, I32, P, P, P, P, P, P, P, P, P, F64, F64, U32]
         L.or_force_run_f64.restype = I32
+        U64 = ctypes.c_uint64
+        L.or_devo.argtypes = [I32, P, P, P, P, P, P, P, P, P, F32, U32, U64, U32, P]
+        L.or_devo.restype = ctypes.c_long
+        L.or_devo_pair.argtypes = [U64, U32, U32, U32, P, P]
+        L.or_devo_pair.restype = None
+        L.or_stress_key.argtypes = [F32]
+        L.or_stress_key.restype = U32
         L.or_max_threads.argtypes = []
         L.or_max_threads.restype = I32
         _lib = L
@@ -140,3 +147,31 @@ def force_run_f64(mode, batch, pos, vel, table, env, dt, t0, steps):
                                 _p(lbar), _p(np.ascontiguousarray(table, np.float32)),
                                 _p(np.ascontiguousarray(env, np.float64)), dt, t0, steps)
     assert rc == 0
+
+
+DEVO_REFERENCE_RANKS = 1
+
+
+def devo(batch, pos, stress, table, t, k, seed, flags=0):
+    """Development step on a copy of the batch's topology.  Returns
+    (pairs, spring_material, lbar, records) with records an (n, 4) uint32
+    array: global spring, a | b << 16, material, mean-length bits."""
+    pairs = np.ascontiguousarray(batch.pairs, np.uint16).copy()
+    mat = np.ascontiguousarray(batch.spring_material, np.uint8).copy()
+    lbar = np.ascontiguousarray(batch.lbar, np.float32).copy()
+    out = np.zeros((max(batch.n_robots * k, 1), 4), np.uint32)
+    n = lib().or_devo(batch.n_robots, _p(batch.mass_offsets), _p(np.ascontiguousarray(pos, np.float32)),
+                      _p(batch.mass_material), _p(batch.spring_offsets), _p(pairs), _p(mat), _p(lbar),
+                      _p(np.ascontiguousarray(stress, np.float32)), _p(np.ascontiguousarray(table, np.float32)),
+                      t, k, seed, flags, _p(out))
+    return pairs, mat, lbar, out[:n]
+
+
+def devo_pair(seed: int, robot: int, j: int, m: int):
+    a, b = ctypes.c_uint32(), ctypes.c_uint32()
+    lib().or_devo_pair(seed, robot, j, m, ctypes.byref(a), ctypes.byref(b))
+    return a.value, b.value
+
+
+def stress_key(s: float) -> int:
+    return lib().or_stress_key(s)

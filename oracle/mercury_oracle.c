@@ -17,6 +17,8 @@
  *   XPBD step ............... common/simulator/sim_kernel.cu:141-153 (predict),
  *                             166-253 (distance constraint), 255-269 (update)
  *   centre of mass .......... common/evolvables/SoftBody.cpp:112-121
+ *   development (Devo) ...... common/simulator/Simulator.cu:597-668,
+ *                             devo_kernel.cu:56-168 (see or_devo)
  *
  * The reference accumulates the per-mass corrections with shared-memory
  * atomics, so its own summation order is unspecified and run-to-run
@@ -636,4 +638,133 @@ void or_com_reference(int n_robots, const int64_t* mass_off, const float* pos,
         }
         for (int c = 0; c < 3; ++c) com[3 * r + c] = mean[c];
     }
+}
+
+/* ------------------------------------------------------------------ */
+/* Development: replace each robot's highest-stress springs with springs
+ * between random mass pairs (Simulator::Devo, Simulator.cu:640-668;
+ * replaceSprings, devo_kernel.cu:81-168).
+ *
+ * Per robot r with n springs and m masses:
+ *   1. rank the springs by accumulated stress, descending (the reference's
+ *      CUB segmented radix sort, Simulator.cu:597-631), ties by ascending
+ *      spring index (the radix sort is stable).  Order of the floats: -0 and
+ *      +0 are equal; a NaN with the sign bit clear ranks above +inf, one with
+ *      it set below -inf.
+ *   2. replace the springs of ranks [lo, hi): lo = 0 and hi = min(k, n); or,
+ *      with the "reference ranks" flag, lo = min(r k, n), hi = min(r k + k, n)
+ *      -- the window the reference's indexing actually selects
+ *      (devo_kernel.cu:112-116 offsets the global replacement index into
+ *      robot r's sorted segment); ranks past the robot's own springs are
+ *      dropped instead of spilling into the next robot's.  Robots with fewer
+ *      than two masses are left alone.
+ *   3. the spring of rank lo + j gets the pair (a, b) drawn by or_devo_pair
+ *      for (seed, r, j), the composite material of the two masses
+ *      (devo_kernel.cu:131-148), and the mean length
+ *      |x_a - x_b| / (1 + dL0 sin(omega t + phi)) of that material at clock t
+ *      (devo_kernel.cu:150-157), with the arithmetic of the step (fmaf phase,
+ *      or_sin, sqrtf of the fmaf dot product, correctly rounded division).
+ *      Stresses are left as they are (the reference does not reset them).
+ *
+ * Random pairs: the reference draws them with cuRAND (XORWOW) in a kernel
+ * whose loop stride makes blocks overwrite one another (devo_kernel.cu:56-73),
+ * so its pairs are not reproducible.  This build uses a counter-based
+ * generator instead: SplitMix64's output function (Steele, Lea and Flood,
+ * "Fast splittable pseudorandom number generators", OOPSLA 2014) over
+ * (seed, robot, j, draw), mapped to [0, m) by Lemire's multiply-shift.  a is
+ * draw 0; b is draw 1, redrawn (draws 2..63) while it equals a, then a+1 mod
+ * m.
+ *
+ * out (optional, 4 words per replaced spring, robot-major, rank order):
+ * global spring index, a | b << 16, material, mean-length bits.  Returns the
+ * number of springs replaced. */
+#define OR_DEVO_REFERENCE_RANKS 1u
+
+static uint64_t or_mix64(uint64_t z) {
+    z ^= z >> 30;
+    z *= 0xbf58476d1ce4e5b9ULL;
+    z ^= z >> 27;
+    z *= 0x94d049bb133111ebULL;
+    return z ^ (z >> 31);
+}
+
+static uint32_t or_devo_draw(uint64_t key, uint32_t j, uint32_t n, uint32_t m) {
+    uint64_t u = or_mix64(key + 0xD1B54A32D192ED03ULL * ((((uint64_t)j << 8) | n) + 1));
+    return (uint32_t)(((u >> 32) * (uint64_t)m) >> 32);
+}
+
+void or_devo_pair(uint64_t seed, uint32_t robot, uint32_t j, uint32_t m, uint32_t* a, uint32_t* b) {
+    uint64_t key = or_mix64(seed + 0x9E3779B97F4A7C15ULL * ((uint64_t)robot + 1));
+    uint32_t x = or_devo_draw(key, j, 0, m), y = or_devo_draw(key, j, 1, m);
+    for (uint32_t n = 2; y == x && n < 64; ++n) y = or_devo_draw(key, j, n, m);
+    if (y == x) y = (x + 1) % m;
+    *a = x;
+    *b = y;
+}
+
+/* Key whose ascending order is descending stress. */
+uint32_t or_stress_key(float s) {
+    uint32_t u;
+    memcpy(&u, &s, 4);
+    if (u == 0x80000000u) u = 0;
+    uint32_t ord = (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+    return ~ord;
+}
+
+static int or_cmp_u64(const void* x, const void* y) {
+    uint64_t a = *(const uint64_t*)x, b = *(const uint64_t*)y;
+    return a < b ? -1 : (a > b);
+}
+
+long or_devo(int n_robots, const int64_t* mass_off, const float* pos, const uint8_t* mass_mat,
+             const int64_t* spring_off, uint16_t* pairs, uint8_t* mat, float* lbar,
+             const float* stress, const float* table, float t, uint32_t k, uint64_t seed,
+             uint32_t flags, uint32_t* out) {
+    long total = 0;
+    for (int r = 0; r < n_robots; ++r) {
+        const int64_t m0 = mass_off[r], s0 = spring_off[r];
+        const uint32_t m = (uint32_t)(mass_off[r + 1] - m0), n = (uint32_t)(spring_off[r + 1] - s0);
+        if (m < 2 || n == 0 || k == 0) continue;
+        uint64_t lo = 0, hi = k < n ? k : n;
+        if (flags & OR_DEVO_REFERENCE_RANKS) {
+            lo = (uint64_t)r * k;
+            hi = lo + k;
+            if (lo > n) lo = n;
+            if (hi > n) hi = n;
+        }
+        if (hi <= lo) continue;
+        uint64_t* keys = (uint64_t*)malloc(sizeof(uint64_t) * n);
+        for (uint32_t i = 0; i < n; ++i) keys[i] = ((uint64_t)or_stress_key(stress[s0 + i]) << 32) | i;
+        qsort(keys, n, sizeof(uint64_t), or_cmp_u64);
+        for (uint64_t q = lo; q < hi; ++q) {
+            const uint32_t j = (uint32_t)(q - lo);
+            const int64_t s = s0 + (int64_t)(uint32_t)keys[q];
+            uint32_t a, b;
+            or_devo_pair(seed, (uint32_t)r, j, m, &a, &b);
+            const int id = or_composite_id(mass_mat[m0 + a], mass_mat[m0 + b]);
+            const float* pa = pos + 4 * (m0 + a);
+            const float* pb = pos + 4 * (m0 + b);
+            float dx = pa[0] - pb[0], dy = pa[1] - pb[1], dz = pa[2] - pb[2];
+            float d = sqrtf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
+            float arg = fmaf(table[4 * id + 2], t, table[4 * id + 3]);
+            float sn = (float)or_sin((double)arg);
+            float rc = table[4 * id + 1] * sn;
+            float den = 1.0f + rc;
+            float L = d / den;
+            pairs[2 * s] = (uint16_t)a;
+            pairs[2 * s + 1] = (uint16_t)b;
+            mat[s] = (uint8_t)id;
+            lbar[s] = L;
+            if (out) {
+                uint32_t* o = out + 4 * total;
+                o[0] = (uint32_t)s;
+                o[1] = a | (b << 16);
+                o[2] = (uint32_t)id;
+                memcpy(&o[3], &L, 4);
+            }
+            ++total;
+        }
+        free(keys);
+    }
+    return total;
 }

@@ -11,6 +11,9 @@
 //                      (common/simulator/Simulator.cu:206-458, 537-580) on a
 //                      batch of robots given as flat arrays and returns the
 //                      collected state and spring stresses.  Needs a GPU.
+//   ref_devo_time    - times the reference's Simulator::Devo
+//                      (Simulator.cu:597-668) after a stress-tracked run.
+//                      Needs a GPU.
 //
 // Material arguments are reference material ids: for masses and voxels a base
 // id (0..22, materials::matLookup), for springs a composite id (0..253,
@@ -18,6 +21,7 @@
 #include "Simulator.h"
 #include "VoxelRobot.h"
 
+#include <chrono>
 #include <cstdint>
 #include <cstring>
 #include <vector>
@@ -37,6 +41,41 @@ struct HarnessVoxelRobot : public VoxelRobot {
     using VoxelRobot::VoxelRobot;
     float length() const { return mLength; }
 };
+
+// Elements of a batch given as flat arrays; masses are padded per robot to
+// the largest mass count with isolated air masses (the reference requires an
+// equal mass count per element, Simulator.cu:231).
+std::vector<Element> make_elements(int n_robots, const int* mass_off, const float* pos, const float* vel,
+                                   const uint8_t* mass_mat, const int* spring_off, const uint16_t* pairs,
+                                   const float* lbar, const uint8_t* spring_mat) {
+    int max_m = 0;
+    for (int r = 0; r < n_robots; ++r)
+        max_m = std::max(max_m, mass_off[r + 1] - mass_off[r]);
+    std::vector<Element> elements(n_robots);
+    for (int r = 0; r < n_robots; ++r) {
+        Element& e = elements[r];
+        for (int i = mass_off[r]; i < mass_off[r + 1]; ++i) {
+            Mass m(i - mass_off[r], pos[3 * i], pos[3 * i + 1], pos[3 * i + 2],
+                   1.0f, materials::matLookup(mass_mat[i]));
+            m.vel = Eigen::Vector3f(vel[3 * i], vel[3 * i + 1], vel[3 * i + 2]);
+            e.masses.push_back(m);
+        }
+        for (int i = mass_off[r + 1] - mass_off[r]; i < max_m; ++i)
+            e.masses.push_back(Mass(i, 0.0f, 0.0f, 0.0f, 1.0f, materials::air));
+        for (int s = spring_off[r]; s < spring_off[r + 1]; ++s) {
+            Spring sp{pairs[2 * s], pairs[2 * s + 1], lbar[s], lbar[s],
+                      materials::id_lookup(spring_mat[s])};
+            e.springs.push_back(sp);
+        }
+    }
+    return elements;
+}
+
+HarnessSimulator* harness_sim() {
+    static HarnessSimulator* sim = nullptr;
+    if (!sim) sim = new HarnessSimulator();
+    return sim;
+}
 
 }  // namespace
 
@@ -96,28 +135,9 @@ int ref_simulate(int n_robots,
                  float dt, float duration, int track_stresses,
                  float* pos_out, float* vel_out, float* stress_out,
                  float* total_time_out) {
-    int max_m = 0;
-    for (int r = 0; r < n_robots; ++r)
-        max_m = std::max(max_m, mass_off[r + 1] - mass_off[r]);
-    std::vector<Element> elements(n_robots);
-    for (int r = 0; r < n_robots; ++r) {
-        Element& e = elements[r];
-        for (int i = mass_off[r]; i < mass_off[r + 1]; ++i) {
-            Mass m(i - mass_off[r], pos[3 * i], pos[3 * i + 1], pos[3 * i + 2],
-                   1.0f, materials::matLookup(mass_mat[i]));
-            m.vel = Eigen::Vector3f(vel[3 * i], vel[3 * i + 1], vel[3 * i + 2]);
-            e.masses.push_back(m);
-        }
-        for (int i = mass_off[r + 1] - mass_off[r]; i < max_m; ++i)
-            e.masses.push_back(Mass(i, 0.0f, 0.0f, 0.0f, 1.0f, materials::air));
-        for (int s = spring_off[r]; s < spring_off[r + 1]; ++s) {
-            Spring sp{pairs[2 * s], pairs[2 * s + 1], lbar[s], lbar[s],
-                      materials::id_lookup(spring_mat[s])};
-            e.springs.push_back(sp);
-        }
-    }
-    static HarnessSimulator* sim = nullptr;
-    if (!sim) sim = new HarnessSimulator();
+    std::vector<Element> elements =
+        make_elements(n_robots, mass_off, pos, vel, mass_mat, spring_off, pairs, lbar, spring_mat);
+    HarnessSimulator* sim = harness_sim();
     sim->setTimeStep(dt);
     std::vector<ElementTracker> trackers = sim->SetElements(elements);
     sim->Reset();
@@ -142,6 +162,39 @@ int ref_simulate(int n_robots,
                 stress_out[s] = st[(size_t)r * spe + (s - spring_off[r])];
     }
     return steps;
+}
+
+// Times Simulator::Devo (Simulator.cu:640-668) the way the reference's
+// DevoBenchmark calls it (optimize/benchmark.cpp:171-217), after a
+// stress-tracked Simulate(duration) so that the sort has stresses to rank:
+// Initialize with replaced_springs_per_element = `replaced`, SetElements,
+// Simulate, then `calls` Devo() calls, each timed on the host clock (Devo
+// synchronises the device itself).  Robots should be identical, as in the
+// benchmark: the reference indexes springs as if every robot had the
+// largest spring count.  Returns 0.
+int ref_devo_time(int n_robots,
+                  const int* mass_off, const float* pos, const float* vel,
+                  const uint8_t* mass_mat,
+                  const int* spring_off, const uint16_t* pairs,
+                  const float* lbar, const uint8_t* spring_mat,
+                  unsigned replaced, float dt, float duration, int calls, double* seconds) {
+    std::vector<Element> elements =
+        make_elements(n_robots, mass_off, pos, vel, mass_mat, spring_off, pairs, lbar, spring_mat);
+    HarnessSimulator* sim = harness_sim();
+    Config::Simulator config;
+    config.replaced_springs_per_element = replaced;
+    config.time_step = dt;
+    sim->Initialize(config);
+    sim->SetElements(elements);
+    sim->Reset();
+    sim->Simulate(duration, true);
+    for (int i = 0; i < calls; ++i) {
+        auto t0 = std::chrono::steady_clock::now();
+        sim->Devo();
+        auto t1 = std::chrono::steady_clock::now();
+        seconds[i] = std::chrono::duration<double>(t1 - t0).count();
+    }
+    return 0;
 }
 
 // Composite material table exactly as Simulator::SetElements uploads it

@@ -2,8 +2,9 @@
 // reference's TestSimulator uses its own (common/tests/test_simulator.cpp:
 // 19-63): reference VoxelRobots, Initialize with dt = 1e-3, SetElements,
 // Simulate, Collect, SoftBody::Update (fitness), run twice -> identical
-// fitness.  Writes the robots and the collected state to a binary file for
-// the GPU pytest to compare with the oracle.
+// fitness.  Then one Devo() (Simulator.cu:640-668) and a second Collect.
+// Writes the robots, the collected state and the rewired springs to a binary
+// file for the GPU pytest to compare with the oracle.
 #include <cstdio>
 #include <cstring>
 #include <random>
@@ -72,6 +73,10 @@ int main(int argc, char** argv) {
     sim.Reset();
     sim.Simulate(0.25f, true);
     std::vector<Element> results = sim.Collect(trackers);
+    std::vector<std::vector<float>> stresses;
+    for (const auto& t : trackers) stresses.push_back(sim.Stresses(t));
+    sim.Devo();
+    std::vector<Element> devo = sim.Collect(trackers);
     FILE* f = std::fopen(out_path, "wb");
     if (!f) return 2;
     uint32_t R = (uint32_t)robots.size();
@@ -100,8 +105,15 @@ int main(int argc, char** argv) {
             float v[6] = {m.pos.x(), m.pos.y(), m.pos.z(), m.vel.x(), m.vel.y(), m.vel.z()};
             std::fwrite(v, 4, 6, f);
         }
-        std::vector<float> st = sim.Stresses(trackers[r]);
-        std::fwrite(st.data(), 4, st.size(), f);
+        std::fwrite(stresses[r].data(), 4, stresses[r].size(), f);
+        for (const Spring& s : devo[r].springs) {
+            uint16_t p[2] = {s.m0, s.m1};
+            uint8_t id = s.material.id;
+            float l = s.mean_length;
+            std::fwrite(p, 2, 2, f);
+            std::fwrite(&id, 1, 1, f);
+            std::fwrite(&l, 4, 1, f);
+        }
     }
     float tt = sim.getTotalTime();
     std::fwrite(&tt, 4, 1, f);

@@ -37,7 +37,8 @@ def _read(path):
         springs = [(take(np.uint16, 2), int(take(np.uint8, 1)[0]), float(take(np.float32, 1)[0])) for _ in range(ns)]
         out = take(np.float32, 6 * nm).reshape(nm, 6)
         st = take(np.float32, ns)
-        robots.append((masses, springs, out, st))
+        devo = [(take(np.uint16, 2), int(take(np.uint8, 1)[0]), take(np.float32, 1)[0]) for _ in range(ns)]
+        robots.append((masses, springs, out, st, devo))
     tt = float(take(np.float32, 1)[0])
     return robots, tt
 
@@ -53,7 +54,7 @@ def test_dropin_matches_oracle(tmp_path):
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
     robots, tt = _read(out)
     els = []
-    for masses, springs, _, _ in robots:
+    for masses, springs, _, _, _ in robots:
         pos = np.array([m[0][:3] for m in masses], np.float32)
         els.append(mb.Element(pos, np.array([m[1] for m in masses], np.uint8),
                               np.array([s[0] for s in springs], np.uint16),
@@ -66,8 +67,17 @@ def test_dropin_matches_oracle(tmp_path):
     s = np.zeros(b.n_springs, np.float32)
     core.xpbd_run(b, p, v, s, core.material_table(), 1e-3, 0.0, n, True)
     assert tt == core.advance_clock(0.0, 1e-3, n)
-    for k, (_, _, o, st) in enumerate(robots):
+    for k, (_, _, o, st, _) in enumerate(robots):
         ms, ss = b.robot_slices(k)
         assert np.array_equal(o[:, :3].view(np.uint32), p[ms, :3].view(np.uint32))
         assert np.array_equal(o[:, 3:].view(np.uint32), v[ms, :3].view(np.uint32))
         assert np.array_equal(st.view(np.uint32), s[ss].view(np.uint32))
+    # Devo(): replaced_springs_per_element = 128 (config.h:18), seed 0
+    pairs, mat, lbar, recs = core.devo(b, p, s, core.material_table(), tt, 128, 0)
+    assert len(recs) > 0
+    for k, (_, _, _, _, devo) in enumerate(robots):
+        ss = b.robot_slices(k)[1]
+        assert np.array_equal(np.array([d[0] for d in devo], np.uint16).reshape(-1, 2), pairs[ss])
+        assert np.array_equal(np.array([d[1] for d in devo], np.uint8), mat[ss])
+        assert np.array_equal(np.array([d[2] for d in devo], np.float32).view(np.uint32),
+                              lbar[ss].view(np.uint32))
