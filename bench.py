@@ -336,7 +336,8 @@ def run_ours(args, rank, local_rank, world):
         "gpu_launches": int(2 * launches_per_eval * args.steps),
         "gpu_launches_note": "per chunk of steps: one actuation-table launch and one step launch",
         "clocks": clocks,
-        "autotune": ({"candidates": len(tuned["candidates"]), "chosen": tuned["config"]} if tuned else None),
+        "autotune": ({"candidates": len(tuned.get("candidates", [])), "cached": "candidates" not in tuned,
+                      "chosen": tuned["config"]} if tuned else None),
         **extra,
     }
     return line
@@ -436,8 +437,10 @@ def devo_bench(local_rank, calls=3):
         phases.append(sim.devo_profile())
     w = float(np.median(walls))
     ph = phases[int(np.argsort(walls)[len(walls) // 2])]
+    sim.run_steps(1000, True)  # the rewired population keeps stepping
+    finite = not sim.robot_flags().any()
     return {"metric": "springs replaced/s", "value": n / w, "unit": "springs/s", "replaced_per_call": n,
-            "ms_per_call": 1e3 * w, "phases_ms": ph,
+            "ms_per_call": 1e3 * w, "phases": ph, "finite_after": finite,
             "workload": f"{DEVO_ROBOTS} default voxel robots (1,728 masses, 18,788 springs), "
                         f"{DEVO_K} springs per robot, after 100 tracked steps",
             "path": "streamed" if sim.launch_config()["streamed"] else "resident"}

@@ -198,8 +198,11 @@ MB_API mb_status mb_device_state(mb_context* ctx, void** pos, void** vel, void**
  * to the robot's own springs.  The pairs come from a counter-based
  * generator over (seed, robot, rank), not cuRAND: same seed, same result on
  * any device.  Stresses are kept (as in the reference); positions and
- * velocities are untouched.  The population is re-packed for the step
- * kernels (the launch override stays if the population still fits it).
+ * velocities are untouched.  The packed layout is updated on the device:
+ * springs keep their slots and the rows of every bin are rebuilt; only when
+ * that does not fit (rows beyond their spare capacity, no free slot for a
+ * spring that stops being air) is the population re-packed on the host
+ * (the launch override stays if the population still fits it).
  * Synchronous.  k <= MB_DEVO_MAX_REPLACED; *n_replaced (may be NULL) gets
  * the number of springs replaced. */
 #define MB_DEVO_MAX_REPLACED 1024
@@ -207,9 +210,11 @@ MB_API mb_status mb_device_state(mb_context* ctx, void** pos, void** vel, void**
 MB_API mb_status mb_devo(mb_context* ctx, uint32_t replaced_per_robot, uint64_t seed, uint32_t flags,
                          uint32_t* n_replaced);
 
-/* Host wall time of the phases of the last mb_devo, in ms: ms[0] selection
- * kernel and read-back of the new springs, ms[1] re-packing on the host,
- * ms[2] upload of the packed arrays.  No reference counterpart. */
+/* Phases of the last mb_devo: ms[0] host wall time (ms) of the device part
+ * -- selection, rewiring of the packed springs, rebuild of the rows, read-back
+ * of the new springs; ms[1] wall time of a host re-pack and upload (0 when
+ * the device re-pack sufficed); ms[2] the number of mb_devo calls on this
+ * context that needed the host re-pack.  No reference counterpart. */
 MB_API mb_status mb_devo_profile(const mb_context* ctx, double* ms);
 
 /* Topology in the upload layout (2 pair entries, 1 material, 1 mean length

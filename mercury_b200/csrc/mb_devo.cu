@@ -169,3 +169,313 @@ cudaError_t launch_devo(const DevoParams& p, uint32_t n_robots, cudaStream_t s) 
 }
 
 }  // namespace mb
+
+// ---------------------------------------------------------------------------
+// Re-packing on the device (see mb_devo.h).
+
+namespace mb {
+namespace {
+
+constexpr uint32_t kRebuildThreads = 512;
+constexpr uint32_t kRebuildMaxMass = 4096;
+constexpr uint32_t kRebuildMaxSlices = kRebuildMaxMass / kSliceWidth;
+constexpr uint32_t kRowLocal = 48;  // rows up to this length are sorted in registers/local memory
+
+__global__ void pslot_kernel(const uint32_t* __restrict__ gidx, uint32_t n_packed, uint32_t n_springs,
+                             uint32_t* __restrict__ pslot) {
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n_packed; q += gridDim.x * blockDim.x) {
+        const uint32_t g = gidx[q];
+        if (g < n_springs) pslot[g] = q;
+    }
+}
+
+__global__ void apply_kernel(const DevoApplyParams p, int pass) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.n_rec) return;
+    const DevoRecord rec = p.rec[i];
+    if (rec.spring == 0xFFFFFFFFu) return;
+    const uint32_t g = rec.spring, r = i / p.k;
+    const uint32_t old_mat = p.spring_mat[g], new_mat = rec.material;
+    const bool take = old_mat == 0 && new_mat != 0;  // an air spring stops being air
+    if ((pass == 1) != take) return;
+    const uint32_t a = rec.pair & 0xFFFFu, b = rec.pair >> 16;
+    p.pairs[2 * (size_t)g] = (uint16_t)a;
+    p.pairs[2 * (size_t)g + 1] = (uint16_t)b;
+    p.spring_mat[g] = (uint8_t)new_mat;
+    p.lbar[g] = rec.lbar;
+    const uint32_t bin = p.robot_bin[r];
+    const uint32_t first = p.bins[bin].spring_begin;
+    uint32_t slot = p.pslot[g];
+    if (new_mat == 0) {  // becomes (or stays) air: its slot turns inert
+        if (slot != kNoSlot) {
+            p.spring_gidx[slot] = p.inert;
+            p.pslot[g] = kNoSlot;
+            const uint32_t c = atomicAdd(&p.free_count[bin], 1u);
+            p.free_slots[first + c] = slot;
+        }
+        return;
+    }
+    if (take) {
+        const uint32_t t = atomicAdd(&p.free_taken[bin], 1u), c = p.free_count[bin];
+        if (t >= c) {
+            atomicAdd(&p.status[0], 1u);
+            return;
+        }
+        slot = p.free_slots[first + c - 1 - t];
+        p.spring_gidx[slot] = g;
+        p.pslot[g] = slot;
+    }
+    const uint32_t ms = p.slot_of[new_mat];
+    if (ms == kNoMatSlot || slot == kNoSlot) {
+        atomicAdd(&p.status[0], 1u);
+        return;
+    }
+    const uint32_t base = p.robot_mass_base[r];
+    p.spring_pair[slot] = (base + a) | ((base + b) << 12) | (ms << 24);
+    p.spring_lbar[slot] = rec.lbar;
+}
+
+__global__ void relayout_kernel(const BinDesc* __restrict__ old_bins, const uint32_t* __restrict__ new_begin,
+                                const uint8_t* __restrict__ src, uint8_t* __restrict__ dst, uint32_t eb) {
+    const BinDesc bd = old_bins[blockIdx.x];
+    const size_t from = (size_t)bd.inc_begin * eb, to = (size_t)new_begin[blockIdx.x] * eb;
+    for (size_t i = threadIdx.x; i < (size_t)bd.n_inc * eb; i += blockDim.x) dst[to + i] = src[from + i];
+}
+
+__device__ __forceinline__ uint32_t row_other(unsigned long long e) { return (uint32_t)(e >> 52); }
+
+// Exclusive scan of v[0..n) in place (n <= kRebuildMaxMass); returns the total.
+__device__ uint32_t block_scan(uint32_t* v, uint32_t n, uint32_t* warp_tot) {
+    constexpr uint32_t kPer = kRebuildMaxMass / kRebuildThreads;  // 8 entries per thread
+    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    uint32_t loc[kPer], sum = 0;
+#pragma unroll
+    for (uint32_t j = 0; j < kPer; ++j) {
+        const uint32_t i = tid * kPer + j;
+        loc[j] = i < n ? v[i] : 0u;
+        sum += loc[j];
+    }
+    uint32_t incl = sum;
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t x = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= (uint32_t)o) incl += x;
+    }
+    if (lane == 31) warp_tot[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        const uint32_t nw = kRebuildThreads / 32;
+        uint32_t t = lane < nw ? warp_tot[lane] : 0u, ti = t;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t x = __shfl_up_sync(0xffffffffu, ti, o);
+            if (lane >= (uint32_t)o) ti += x;
+        }
+        if (lane < nw) warp_tot[lane] = ti - t;  // exclusive
+        if (lane == nw - 1) warp_tot[nw] = ti;   // total
+    }
+    __syncthreads();
+    uint32_t run = warp_tot[warp] + incl - sum;
+#pragma unroll
+    for (uint32_t j = 0; j < kPer; ++j) {
+        const uint32_t i = tid * kPer + j;
+        if (i < n) v[i] = run;
+        run += loc[j];
+    }
+    const uint32_t total = warp_tot[kRebuildThreads / 32];
+    __syncthreads();
+    return total;
+}
+
+__global__ void __launch_bounds__(kRebuildThreads) rebuild_kernel(const RebuildParams p) {
+    __shared__ uint32_t start[kRebuildMaxMass + 1];
+    __shared__ uint32_t cur[kRebuildMaxMass];
+    __shared__ uint32_t swidth[kRebuildMaxSlices], soff[kRebuildMaxSlices];
+    __shared__ uint32_t warp_tot[kRebuildThreads / 32 + 1];
+    __shared__ uint32_t s_total;
+    const uint32_t b = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const BinDesc bd = p.bins[b];
+    const uint32_t nm = bd.n_mass, ns = bd.n_spring, cap = bd.pad[0];
+    if (tid == 0) {  // the free list after this call's takes
+        const uint32_t c = p.free_count[b], t = p.free_taken[b];
+        p.free_count[b] = c - min(t, c);
+        p.free_taken[b] = 0;
+    }
+    if (nm > kRebuildMaxMass || ns >= (1u << 20)) {
+        if (tid == 0) atomicAdd(&p.status[0], 1u);
+        return;
+    }
+    // 1. degrees
+    for (uint32_t i = tid; i < nm; i += kRebuildThreads) start[i] = 0;
+    __syncthreads();
+    for (uint32_t j = tid; j < ns; j += kRebuildThreads) {
+        const uint32_t q = bd.spring_begin + j;
+        if (p.spring_gidx[q] == p.inert) continue;
+        const uint32_t w = p.spring_pair[q];
+        atomicAdd(&start[w & 0xFFFu], 1u);
+        atomicAdd(&start[(w >> 12) & 0xFFFu], 1u);
+    }
+    __syncthreads();
+    // 2. row starts
+    const uint32_t n_ent = block_scan(start, nm, warp_tot);
+    if (tid == 0) start[nm] = n_ent;
+    for (uint32_t i = tid; i < nm; i += kRebuildThreads) cur[i] = start[i];
+    __syncthreads();
+    // 3. entries: other end << 52 | spring << 21 | (b end) << 20 | packed slot
+    unsigned long long* rows = p.rows + 2ull * bd.spring_begin;
+    for (uint32_t j = tid; j < ns; j += kRebuildThreads) {
+        const uint32_t q = bd.spring_begin + j, g = p.spring_gidx[q];
+        if (g == p.inert) continue;
+        const uint32_t w = p.spring_pair[q], a = w & 0xFFFu, c = (w >> 12) & 0xFFFu;
+        const unsigned long long sg = (unsigned long long)g << 21;
+        rows[atomicAdd(&cur[a], 1u)] = ((unsigned long long)c << 52) | sg | j;
+        rows[atomicAdd(&cur[c], 1u)] = ((unsigned long long)a << 52) | sg | (1ull << 20) | j;
+    }
+    __syncthreads();
+    // 4. summation order within each row
+    for (uint32_t i = tid; i < nm; i += kRebuildThreads) {
+        unsigned long long* r = rows + start[i];
+        const uint32_t len = start[i + 1] - start[i];
+        if (len <= kRowLocal) {
+            unsigned long long loc[kRowLocal];
+            for (uint32_t x = 0; x < len; ++x) {
+                const unsigned long long e = r[x];
+                uint32_t y = x;
+                while (y > 0 && loc[y - 1] > e) {
+                    loc[y] = loc[y - 1];
+                    --y;
+                }
+                loc[y] = e;
+            }
+            for (uint32_t x = 0; x < len; ++x) r[x] = loc[x];
+        } else {
+            for (uint32_t x = 1; x < len; ++x) {
+                const unsigned long long e = r[x];
+                uint32_t y = x;
+                while (y > 0 && r[y - 1] > e) {
+                    r[y] = r[y - 1];
+                    --y;
+                }
+                r[y] = e;
+            }
+        }
+    }
+    __syncthreads();
+    // 5. slice widths: aligned by neighbour offset when every row of the
+    //    slice has distinct other ends and the union of offsets is at most 4
+    //    columns wider than the longest row (the host packer's rule)
+    const uint32_t n_sl = (nm + kSliceWidth - 1) / kSliceWidth;
+    for (uint32_t sl = warp; sl < n_sl; sl += kRebuildThreads / 32) {
+        const uint32_t i = sl * kSliceWidth + lane;
+        const uint32_t r0 = i < nm ? start[i] : 0u, r1 = i < nm ? start[i + 1] : 0u;
+        uint32_t w_rank = r1 - r0;
+        for (int o = 16; o; o >>= 1) w_rank = max(w_rank, __shfl_xor_sync(0xffffffffu, w_rank, o));
+        bool mine = true;
+        for (uint32_t q = r0 + 1; q < r1; ++q) mine &= row_other(rows[q]) != row_other(rows[q - 1]);
+        bool aligned = __all_sync(0xffffffffu, mine);
+        uint32_t u = 0;
+        if (aligned) {
+            uint32_t h = r0;
+            while (true) {
+                const uint32_t head = h < r1 ? row_other(rows[h]) + kRebuildMaxMass - i : 0xFFFFFFFFu;
+                const uint32_t m = __reduce_min_sync(0xffffffffu, head);
+                if (m == 0xFFFFFFFFu) break;
+                if (head == m) ++h;
+                if (++u > w_rank + 4) break;
+            }
+            aligned = u <= w_rank + 4;
+        }
+        if (lane == 0) swidth[sl] = aligned ? (u | 0x80000000u) : w_rank;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        uint32_t off = 0;
+        for (uint32_t sl = 0; sl < n_sl; ++sl) {
+            soff[sl] = off;
+            off += kSliceWidth * (swidth[sl] & 0x7FFFFFFFu);
+        }
+        s_total = off;
+    }
+    __syncthreads();
+    const uint32_t n_inc = s_total;
+    if (n_inc > cap) {
+        if (tid == 0) atomicAdd(&p.status[0], 1u);
+        return;
+    }
+    // 6. write the slices
+    for (uint32_t sl = tid; sl < n_sl; sl += kRebuildThreads) {
+        p.slice_off[bd.slice_begin + sl] = soff[sl];
+        p.slice_width[bd.slice_begin + sl] = swidth[sl] & 0x7FFFFFFFu;
+    }
+    for (uint32_t e = tid; e < n_inc; e += kRebuildThreads) {
+        if (p.streamed)
+            p.inc32[bd.inc_begin + e] = kPadEntry32;
+        else
+            p.inc[bd.inc_begin + e] = kPadEntry;
+    }
+    __syncthreads();
+    for (uint32_t sl = warp; sl < n_sl; sl += kRebuildThreads / 32) {
+        const uint32_t i = sl * kSliceWidth + lane;
+        const uint32_t r0 = i < nm ? start[i] : 0u, r1 = i < nm ? start[i + 1] : 0u;
+        const bool aligned = (swidth[sl] & 0x80000000u) != 0;
+        const uint32_t base = bd.inc_begin + soff[sl] + lane;
+        auto put = [&](uint32_t col, unsigned long long e) {
+            const uint32_t v = ((uint32_t)(e & 0xFFFFFu) << 1) | (uint32_t)((e >> 20) & 1u);
+            if (p.streamed)
+                p.inc32[base + col * kSliceWidth] = v;
+            else
+                p.inc[base + col * kSliceWidth] = (uint16_t)v;
+        };
+        if (aligned) {
+            uint32_t h = r0, col = 0;
+            while (true) {
+                const unsigned long long e = h < r1 ? rows[h] : 0ull;
+                const uint32_t head = h < r1 ? row_other(e) + kRebuildMaxMass - i : 0xFFFFFFFFu;
+                const uint32_t m = __reduce_min_sync(0xffffffffu, head);
+                if (m == 0xFFFFFFFFu) break;
+                if (head == m) {
+                    put(col, e);
+                    ++h;
+                }
+                ++col;
+            }
+        } else {
+            for (uint32_t q = r0; q < r1; ++q) put(q - r0, rows[q]);
+        }
+    }
+    if (tid == 0) {
+        p.bins[b].n_inc = n_inc;
+        if (!p.streamed)
+            atomicMax(&p.status[1], bin_smem_bytes_dev(nm, ns, n_inc));
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_build_pslot(const uint32_t* spring_gidx, uint32_t n_packed, uint32_t n_springs,
+                               uint32_t* pslot, cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(pslot, 0xFF, (size_t)n_springs * sizeof(uint32_t), s);
+    if (e != cudaSuccess || n_packed == 0) return e;
+    pslot_kernel<<<(n_packed + 255) / 256, 256, 0, s>>>(spring_gidx, n_packed, n_springs, pslot);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_devo_apply(const DevoApplyParams& p, int pass, cudaStream_t s) {
+    if (p.n_rec == 0) return cudaSuccess;
+    apply_kernel<<<(p.n_rec + 255) / 256, 256, 0, s>>>(p, pass);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_relayout(const BinDesc* old_bins, const uint32_t* new_begin, uint32_t n_bins,
+                            const void* src, void* dst, uint32_t entry_bytes, cudaStream_t s) {
+    if (n_bins == 0) return cudaSuccess;
+    relayout_kernel<<<n_bins, 256, 0, s>>>(old_bins, new_begin, static_cast<const uint8_t*>(src),
+                                           static_cast<uint8_t*>(dst), entry_bytes);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_rebuild(const RebuildParams& p, cudaStream_t s) {
+    if (p.n_bins == 0) return cudaSuccess;
+    rebuild_kernel<<<p.n_bins, kRebuildThreads, 0, s>>>(p);
+    return cudaGetLastError();
+}
+
+}  // namespace mb

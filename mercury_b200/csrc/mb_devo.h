@@ -3,6 +3,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "mb_internal.h"
+
 namespace mb {
 
 constexpr uint32_t kDevoMaxReplaced = 1024;   // springs replaced per robot and call
@@ -32,5 +34,72 @@ struct DevoParams {
 };
 
 cudaError_t launch_devo(const DevoParams& p, uint32_t n_robots, cudaStream_t s);
+
+// ---------------------------------------------------------------------------
+// Re-packing on the device after development.  Springs keep their packed
+// slot; a spring that becomes air turns its slot inert (spring_gidx = the
+// population's spring count, a dummy stress element; no row references it)
+// and frees it for a spring of its bin that stops being air.  The rows of
+// every bin are then rebuilt: CSR by counting, each row sorted by (other
+// end, spring index, a end before b end), SELL-32 slices aligned by
+// neighbour offset when the host packer would align them.  Anything that
+// does not fit (no free slot, no material slot, rows beyond the bin's
+// capacity) is counted in status[0] and the host re-packs instead.
+
+constexpr uint32_t kNoSlot = 0xFFFFFFFFu;
+constexpr uint32_t kNoMatSlot = 0xFFu;
+
+struct DevoApplyParams {
+    const DevoRecord* rec;
+    uint32_t n_rec;
+    uint32_t k;                    // records per robot
+    uint16_t* pairs;               // canonical topology, upload order
+    uint8_t* spring_mat;
+    float* lbar;
+    uint32_t* pslot;               // canonical spring -> packed slot, or kNoSlot
+    const uint32_t* robot_bin;
+    const uint32_t* robot_mass_base;
+    const uint8_t* slot_of;        // composite id -> material slot, or kNoMatSlot
+    const BinDesc* bins;
+    uint32_t* spring_pair;         // packed
+    float* spring_lbar;
+    uint32_t* spring_gidx;
+    uint32_t inert;                // spring_gidx of an inert slot
+    uint32_t* free_count;          // per bin
+    uint32_t* free_taken;          // per bin
+    uint32_t* free_slots;          // per packed slot region of each bin
+    uint32_t* status;              // [0] problems, [1] max shared memory of a bin
+};
+
+struct RebuildParams {
+    BinDesc* bins;
+    uint32_t n_bins;
+    const uint32_t* spring_pair;
+    const uint32_t* spring_gidx;
+    uint32_t inert;
+    uint32_t* slice_off;
+    uint32_t* slice_width;
+    uint16_t* inc;                 // resident rows
+    uint32_t* inc32;               // streamed rows
+    uint32_t streamed;
+    unsigned long long* rows;      // scratch: 2 per packed slot
+    uint32_t* free_count;
+    uint32_t* free_taken;
+    uint32_t* status;
+};
+
+// Canonical spring -> packed slot map from spring_gidx (n_packed slots).
+cudaError_t launch_build_pslot(const uint32_t* spring_gidx, uint32_t n_packed, uint32_t n_springs,
+                               uint32_t* pslot, cudaStream_t s);
+// Applies development records: pass 0 everything except air -> non-air,
+// pass 1 air -> non-air (takes freed slots).
+cudaError_t launch_devo_apply(const DevoApplyParams& p, int pass, cudaStream_t s);
+// Moves each bin's rows to a region of `cap` entries (bins[b].pad[0] =
+// capacity); new_begin[b] is the new first entry.
+cudaError_t launch_relayout(const BinDesc* old_bins, const uint32_t* new_begin, uint32_t n_bins,
+                            const void* src, void* dst, uint32_t entry_bytes, cudaStream_t s);
+// Rebuilds every bin's rows; status[1] gets the largest shared memory a
+// resident bin needs.
+cudaError_t launch_rebuild(const RebuildParams& p, cudaStream_t s);
 
 }  // namespace mb

@@ -25,6 +25,7 @@
 #include <map>
 #include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -158,6 +159,21 @@ struct mb_context {
     mb::DevBuf<mb::DevoRecord> devo_out;
     std::vector<mb::DevoRecord> h_devo;
     double devo_ms[3] = {0.0, 0.0, 0.0};  // last mb_devo: select+read-back, re-pack, upload
+    uint32_t devo_host_repacks = 0;       // mb_devo calls that fell back to the host packer
+
+    // re-packing on the device after development, set up by the first
+    // mb_devo after an upload: canonical topology on the device, packed slot
+    // of every spring, free inert slots per bin, rows with spare capacity
+    bool devo_ready = false;
+    uint32_t n_packed = 0;                // packed spring slots
+    std::vector<mb::BinDesc> h_bins;
+    std::vector<uint32_t> h_robot_mass_base;
+    std::vector<uint8_t> h_mat_ids;
+    mb::DevBuf<uint16_t> d_pairs;
+    mb::DevBuf<uint8_t> d_spring_mat, slot_of;
+    mb::DevBuf<float> d_lbar;
+    mb::DevBuf<uint32_t> pslot, robot_mass_base, free_count, free_taken, free_slots, devo_status, new_begin;
+    mb::DevBuf<unsigned long long> rows_scratch;
 
     std::map<mb::GraphKey, cudaGraphExec_t> graphs;
 
@@ -299,11 +315,112 @@ mb_status upload_packed(mb_context* ctx, const mb::Packed& out) {
     MB_CUDA(ctx, ctx->invk.alloc(std::max<uint32_t>(ctx->n_mat_host, 1)));
     MB_CUDA(ctx, ctx->rates.alloc((size_t)std::max<uint32_t>(ctx->n_mat_host, 1) * ctx->chunk));
     MB_CUDA(ctx, up(ctx->robot_bin, out.robot_bin.data(), out.robot_bin.size()));
+    ctx->h_bins = out.bins;
+    ctx->h_robot_mass_base = out.robot_mass_base;
+    ctx->h_mat_ids = out.mat_ids;
+    ctx->n_packed = (uint32_t)out.pair.size();
+    ctx->devo_ready = false;
     MB_CUDA(ctx, ctx->bin_flags.alloc(nb));
     MB_CUDA(ctx, cudaMemsetAsync(ctx->bin_flags.p, 0, nb * sizeof(uint32_t), st));
     // the host vectors of `out` may die after this call: wait for the copies
     MB_CUDA(ctx, cudaStreamSynchronize(st));
     return MB_OK;
+}
+
+
+// One-time state of device re-packing (first mb_devo after an upload).
+mb_status devo_setup(mb_context* c) {
+    cudaStream_t st = c->stream;
+    const uint64_t S = c->n_spring;
+    const uint32_t nb = c->n_bins, R = c->n_robots;
+    auto up = [&](auto& buf, const auto* src, size_t n) -> cudaError_t {
+        cudaError_t e = buf.alloc(n);
+        if (e != cudaSuccess || n == 0) return e;
+        return cudaMemcpyAsync(buf.p, src, n * sizeof(*src), cudaMemcpyHostToDevice, st);
+    };
+    MB_CUDA(c, up(c->d_pairs, c->h_pairs.data(), 2 * S));
+    MB_CUDA(c, up(c->d_spring_mat, c->h_spring_mat.data(), S));
+    MB_CUDA(c, up(c->d_lbar, c->h_lbar.data(), S));
+    MB_CUDA(c, c->pslot.alloc(S));
+    MB_CUDA(c, mb::launch_build_pslot(c->spring_gidx.p, c->n_packed, (uint32_t)S, c->pslot.p, st));
+    MB_CUDA(c, up(c->robot_mass_base, c->h_robot_mass_base.data(), R));
+    // Material slots for every composite development can create: pairs of
+    // the base materials the masses carry.  Extra slots only widen the
+    // per-launch actuation table.
+    bool base[23] = {};
+    for (uint8_t m : c->h_mass_mat) base[m] = true;
+    std::vector<uint8_t> slot(256, mb::kNoMatSlot);
+    for (size_t i = 0; i < c->h_mat_ids.size(); ++i) slot[c->h_mat_ids[i]] = (uint8_t)i;
+    for (int i = 1; i < 23; ++i)
+        for (int j = i; j < 23; ++j) {
+            if (!base[i] || !base[j]) continue;
+            const int id = mb::composite_id(i, j);
+            if (slot[id] != mb::kNoMatSlot) continue;
+            slot[id] = (uint8_t)c->h_mat_ids.size();
+            c->h_mat_ids.push_back((uint8_t)id);
+        }
+    c->n_mat_host = (uint32_t)c->h_mat_ids.size();
+    MB_CUDA(c, up(c->mat_ids, c->h_mat_ids.data(), c->h_mat_ids.size()));
+    MB_CUDA(c, up(c->n_mat, &c->n_mat_host, 1));
+    MB_CUDA(c, c->invk.alloc(c->n_mat_host));
+    MB_CUDA(c, c->rates.alloc((size_t)c->n_mat_host * c->chunk));
+    MB_CUDA(c, up(c->slot_of, slot.data(), 256));
+    MB_CUDA(c, c->free_count.alloc(nb));
+    MB_CUDA(c, c->free_taken.alloc(nb));
+    MB_CUDA(c, cudaMemsetAsync(c->free_count.p, 0, nb * sizeof(uint32_t), st));
+    MB_CUDA(c, cudaMemsetAsync(c->free_taken.p, 0, nb * sizeof(uint32_t), st));
+    MB_CUDA(c, c->free_slots.alloc(c->n_packed));
+    MB_CUDA(c, c->rows_scratch.alloc(2 * (size_t)c->n_packed));
+    MB_CUDA(c, c->devo_status.alloc(2));
+    // rows get spare capacity: half their size plus 8 slice columns
+    std::vector<uint32_t> begin(nb);
+    std::vector<mb::BinDesc> nbins = c->h_bins;
+    uint64_t total = 0;
+    for (uint32_t b = 0; b < nb; ++b) {
+        const uint32_t n = c->h_bins[b].n_inc;
+        const uint32_t cap = (n + n / 2 + 8 * mb::kSliceWidth + 31) / 32 * 32;
+        begin[b] = (uint32_t)total;
+        nbins[b].inc_begin = (uint32_t)total;
+        nbins[b].pad[0] = cap;
+        total += cap;
+    }
+    if (total >= (1ull << 32)) return fail(c, MB_ERR_CAPACITY, "rows too large for development");
+    MB_CUDA(c, up(c->new_begin, begin.data(), nb));
+    const uint32_t eb = c->streamed ? 4u : 2u;
+    if (c->streamed) {
+        mb::DevBuf<uint32_t> fresh;
+        MB_CUDA(c, fresh.alloc(total));
+        MB_CUDA(c, mb::launch_relayout(c->bins.p, c->new_begin.p, nb, c->inc32.p, fresh.p, eb, st));
+        MB_CUDA(c, cudaStreamSynchronize(st));
+        std::swap(c->inc32.p, fresh.p);
+        std::swap(c->inc32.n, fresh.n);
+    } else {
+        mb::DevBuf<uint16_t> fresh;
+        MB_CUDA(c, fresh.alloc(total));
+        MB_CUDA(c, mb::launch_relayout(c->bins.p, c->new_begin.p, nb, c->inc.p, fresh.p, eb, st));
+        MB_CUDA(c, cudaStreamSynchronize(st));
+        std::swap(c->inc.p, fresh.p);
+        std::swap(c->inc.n, fresh.n);
+    }
+    c->h_bins = nbins;
+    MB_CUDA(c, up(c->bins, c->h_bins.data(), nb));
+    MB_CUDA(c, cudaStreamSynchronize(st));
+    c->clear_graphs();
+    c->devo_ready = true;
+    return MB_OK;
+}
+
+// Host re-packing of the context's topology copy (fallback of development).
+mb_status host_repack(mb_context* c) {
+    const mb_batch_desc d{c->n_robots,       c->mass_off.data(),   nullptr,
+                          nullptr,           c->h_mass_mat.data(), c->spring_off.data(),
+                          c->h_pairs.data(), c->h_spring_mat.data(), c->h_lbar.data()};
+    mb::Packed out;
+    mb_status st = pack(c, &d, true, out);
+    if (st == MB_OK) st = upload_packed(c, out);
+    if (st != MB_OK) c->loaded = false;  // topology and packed arrays disagree now
+    ++c->devo_host_repacks;
+    return st;
 }
 
 }  // namespace mb_detail
@@ -503,8 +620,21 @@ mb_status mb_set_elements(mb_context* ctx, const mb_batch_desc* b) {
     if (M >= (1ull << 31) || S >= (1ull << 31)) return fail(ctx, MB_ERR_CAPACITY, "population too large");
 
     cudaSetDevice(ctx->device);
+    // the host copy of the topology is taken while the population is packed
+    std::vector<uint8_t> h_mass_mat, h_spring_mat;
+    std::vector<uint16_t> h_pairs;
+    std::vector<float> h_lbar;
+    std::thread copier([&] {
+        h_mass_mat.assign(b->mass_material, b->mass_material + M);
+        if (S) {
+            h_pairs.assign(b->pairs, b->pairs + 2 * S);
+            h_spring_mat.assign(b->spring_material, b->spring_material + S);
+            h_lbar.assign(b->lbar, b->lbar + S);
+        }
+    });
     mb::Packed out;
     const mb_status pst = mb_detail::pack(ctx, b, false, out);
+    copier.join();
     if (pst != MB_OK) return pst;
 
     // the population is accepted: keep its topology on the host (for
@@ -516,10 +646,10 @@ mb_status mb_set_elements(mb_context* ctx, const mb_batch_desc* b) {
     ctx->n_spring = S;
     ctx->mass_off.assign(b->mass_offsets, b->mass_offsets + R + 1);
     ctx->spring_off.assign(b->spring_offsets, b->spring_offsets + R + 1);
-    ctx->h_mass_mat.assign(b->mass_material, b->mass_material + M);
-    ctx->h_pairs.assign(b->pairs, b->pairs + 2 * S);
-    ctx->h_spring_mat.assign(b->spring_material, b->spring_material + S);
-    ctx->h_lbar.assign(b->lbar, b->lbar + S);
+    ctx->h_mass_mat = std::move(h_mass_mat);
+    ctx->h_pairs = std::move(h_pairs);
+    ctx->h_spring_mat = std::move(h_spring_mat);
+    ctx->h_lbar = std::move(h_lbar);
     cudaStream_t st = ctx->stream;
     auto up = [&](auto& buf, const auto* src, size_t n) -> cudaError_t {
         cudaError_t e = buf.alloc(n);
@@ -531,8 +661,9 @@ mb_status mb_set_elements(mb_context* ctx, const mb_batch_desc* b) {
     MB_CUDA(ctx, up(ctx->mass_mat, b->mass_material, M));
     MB_CUDA(ctx, up(ctx->d_mass_off, b->mass_offsets, R + 1));
     MB_CUDA(ctx, up(ctx->d_spring_off, b->spring_offsets, R + 1));
-    MB_CUDA(ctx, ctx->stress.alloc(S));
-    if (S) MB_CUDA(ctx, cudaMemsetAsync(ctx->stress.p, 0, S * sizeof(float), st));
+    // one element more: the stress of inert packed slots (development)
+    MB_CUDA(ctx, ctx->stress.alloc(S + 1));
+    MB_CUDA(ctx, cudaMemsetAsync(ctx->stress.p, 0, (S + 1) * sizeof(float), st));
     MB_CUDA(ctx, ctx->robot_flags.alloc(R));
     MB_CUDA(ctx, ctx->com.alloc(3 * (size_t)R));
     const mb_status ust = mb_detail::upload_packed(ctx, out);
@@ -771,16 +902,43 @@ mb_status mb_devo(mb_context* ctx, uint32_t replaced_per_robot, uint64_t seed, u
     cudaSetDevice(ctx->device);
     using clock = std::chrono::steady_clock;
     const auto t0 = clock::now();
+    cudaStream_t st = ctx->stream;
+    const char* force_host = std::getenv("MB_DEVO_HOST_REPACK");
+    const bool on_device = !(force_host && force_host[0] == '1');
+    if (on_device && !ctx->devo_ready) {
+        const mb_status s = mb_detail::devo_setup(ctx);
+        if (s != MB_OK) return s;
+    }
     const size_t nrec = (size_t)ctx->n_robots * replaced_per_robot;
     MB_CUDA(ctx, ctx->devo_out.alloc(nrec));
     mb::DevoParams p{ctx->stress.p, ctx->d_mass_off.p, ctx->d_spring_off.p, ctx->pos.p, ctx->mass_mat.p,
                      ctx->d_table.p, ctx->total_time, replaced_per_robot, seed, flags, ctx->devo_out.p};
-    MB_TRACE("devo launch robots=%u k=%u", ctx->n_robots, replaced_per_robot);
-    MB_CUDA(ctx, mb::launch_devo(p, ctx->n_robots, ctx->stream));
+    MB_TRACE("devo launch robots=%u k=%u device=%d", ctx->n_robots, replaced_per_robot, (int)on_device);
+    MB_CUDA(ctx, mb::launch_devo(p, ctx->n_robots, st));
+    uint32_t status[2] = {0, 0};
+    if (on_device) {
+        MB_CUDA(ctx, cudaMemsetAsync(ctx->devo_status.p, 0, 2 * sizeof(uint32_t), st));
+        mb::DevoApplyParams ap{ctx->devo_out.p,      (uint32_t)nrec,        replaced_per_robot,
+                               ctx->d_pairs.p,       ctx->d_spring_mat.p,   ctx->d_lbar.p,
+                               ctx->pslot.p,         ctx->robot_bin.p,      ctx->robot_mass_base.p,
+                               ctx->slot_of.p,       ctx->bins.p,           ctx->spring_pair.p,
+                               ctx->spring_lbar.p,   ctx->spring_gidx.p,    (uint32_t)ctx->n_spring,
+                               ctx->free_count.p,    ctx->free_taken.p,     ctx->free_slots.p,
+                               ctx->devo_status.p};
+        MB_CUDA(ctx, mb::launch_devo_apply(ap, 0, st));
+        MB_CUDA(ctx, mb::launch_devo_apply(ap, 1, st));
+        mb::RebuildParams rp{ctx->bins.p,        ctx->n_bins,          ctx->spring_pair.p,
+                             ctx->spring_gidx.p, (uint32_t)ctx->n_spring, ctx->slice_off.p,
+                             ctx->slice_width.p, ctx->inc.p,           ctx->inc32.p,
+                             ctx->streamed ? 1u : 0u, ctx->rows_scratch.p, ctx->free_count.p,
+                             ctx->free_taken.p,  ctx->devo_status.p};
+        MB_CUDA(ctx, mb::launch_rebuild(rp, st));
+        MB_CUDA(ctx, cudaMemcpyAsync(status, ctx->devo_status.p, sizeof(status), cudaMemcpyDeviceToHost, st));
+    }
     ctx->h_devo.resize(nrec);
     MB_CUDA(ctx, cudaMemcpyAsync(ctx->h_devo.data(), ctx->devo_out.p, nrec * sizeof(mb::DevoRecord),
-                                 cudaMemcpyDeviceToHost, ctx->stream));
-    MB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+                                 cudaMemcpyDeviceToHost, st));
+    MB_CUDA(ctx, cudaStreamSynchronize(st));
     uint32_t count = 0;
     for (const mb::DevoRecord& rec : ctx->h_devo) {
         if (rec.spring == 0xFFFFFFFFu) continue;
@@ -793,21 +951,24 @@ mb_status mb_devo(mb_context* ctx, uint32_t replaced_per_robot, uint64_t seed, u
         ++count;
     }
     const auto t1 = clock::now();
-    const mb_batch_desc d{ctx->n_robots,         ctx->mass_off.data(),   nullptr,
-                          nullptr,               ctx->h_mass_mat.data(), ctx->spring_off.data(),
-                          ctx->h_pairs.data(),   ctx->h_spring_mat.data(), ctx->h_lbar.data()};
-    mb::Packed out;
-    mb_status st = mb_detail::pack(ctx, &d, true, out);
-    const auto t2 = clock::now();
-    if (st == MB_OK) st = mb_detail::upload_packed(ctx, out);
-    if (st != MB_OK) {
-        ctx->loaded = false;  // topology and packed arrays disagree now
-        return st;
+    bool repack = !on_device || status[0] != 0;
+    if (!repack && !ctx->streamed && status[1] > ctx->smem_bytes) {
+        if (status[1] > mb::max_step_smem(ctx->device)) {
+            repack = true;
+        } else {
+            ctx->smem_bytes = status[1];
+            ctx->clear_graphs();  // the graphs hold the old shared memory size
+        }
     }
-    const auto t3 = clock::now();
+    if (repack) {
+        MB_TRACE("devo: host re-pack (problems %u)", status[0]);
+        const mb_status s = mb_detail::host_repack(ctx);
+        if (s != MB_OK) return s;
+    }
+    const auto t2 = clock::now();
     ctx->devo_ms[0] = std::chrono::duration<double, std::milli>(t1 - t0).count();
-    ctx->devo_ms[1] = std::chrono::duration<double, std::milli>(t2 - t1).count();
-    ctx->devo_ms[2] = std::chrono::duration<double, std::milli>(t3 - t2).count();
+    ctx->devo_ms[1] = repack ? std::chrono::duration<double, std::milli>(t2 - t1).count() : 0.0;
+    ctx->devo_ms[2] = (double)ctx->devo_host_repacks;
     if (n_replaced) *n_replaced = count;
     return MB_OK;
 }

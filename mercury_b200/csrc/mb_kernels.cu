@@ -541,7 +541,7 @@ const ShapeEntry* find_shape(const KernelShape& s) {
 }  // namespace
 
 uint32_t bin_smem_bytes(uint32_t n_mass, uint32_t n_spring, uint32_t n_inc) {
-    return 16u * n_mass + 16u * n_spring + 8u * kMaxMaterialSlots + 2u * n_inc;
+    return bin_smem_bytes_dev(n_mass, n_spring, n_inc);
 }
 
 uint32_t max_step_smem(int device) {

@@ -304,6 +304,7 @@ void build_all(const mb_batch_desc* b, const std::vector<RobotPack>& packs,
     parallel_for(nb, threads, [&](uint32_t i) { build_bin(b, packs, plan[i], slot_of, streamed, locals[i]); });
     out.bins.assign(nb, BinDesc{});
     out.robot_bin.assign(R, 0);
+    out.robot_mass_base.assign(R, 0);
     out.mass_gidx.clear();
     out.spring_gidx.clear();
     out.pair.clear();
@@ -326,7 +327,12 @@ void build_all(const mb_batch_desc* b, const std::vector<RobotPack>& packs,
         d.inc_begin = (uint32_t)(streamed ? out.inc32.size() : out.inc.size());
         d.n_inc = L.n_inc;
         d.slice_begin = (uint32_t)out.slice_off.size();
-        for (uint32_t r : plan[i]) out.robot_bin[r] = i;
+        uint32_t base = 0;
+        for (uint32_t r : plan[i]) {
+            out.robot_bin[r] = i;
+            out.robot_mass_base[r] = base;
+            base += packs[r].n_mass;
+        }
         out.mass_gidx.insert(out.mass_gidx.end(), L.mass_gidx.begin(), L.mass_gidx.end());
         out.spring_gidx.insert(out.spring_gidx.end(), L.spring_gidx.begin(), L.spring_gidx.end());
         out.pair.insert(out.pair.end(), L.pair.begin(), L.pair.end());

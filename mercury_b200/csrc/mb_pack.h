@@ -29,6 +29,7 @@ struct Packed {
     uint32_t max_smem = 0;
     std::vector<BinDesc> bins;
     std::vector<uint32_t> mass_gidx, spring_gidx, pair, slice_off, slice_width, robot_bin;
+    std::vector<uint32_t> robot_mass_base;  // bin-local index of each robot's first mass
     std::vector<uint16_t> inc;    // resident rows
     std::vector<uint32_t> inc32;  // streamed rows
     std::vector<float> lbar;

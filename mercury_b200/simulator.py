@@ -71,6 +71,7 @@ class Simulator:
         self.config = SimulatorConfig()
         self._table = material_table()
         self._devo_seed = 0
+        self._topology_stale = False
         _lib.check(_lib.LIB.mb_set_materials(self._ctx, _lib.ptr(self._table)), self._ctx)
         # the reference's m_deltaT before Initialize (Simulator.h:55)
         self.setTimeStep(0.0001)
@@ -121,6 +122,7 @@ class Simulator:
         single = isinstance(trackers, ElementTracker)
         trackers = [trackers] if single else list(trackers)
         pos, vel, stress = self.collect_arrays()
+        self._refresh_topology()
         full = unpack(self._batch, pos, vel, stress, self._elements)
         out = [full[t.ID] for t in trackers]
         return out[0] if single else out
@@ -163,6 +165,7 @@ class Simulator:
 
     def set_batch(self, batch: Batch) -> None:
         self._batch = batch
+        self._topology_stale = False
         d = _lib.BatchDesc(
             batch.n_robots, _lib.ptr(batch.mass_offsets), _lib.ptr(batch.pos), _lib.ptr(batch.vel),
             _lib.ptr(batch.mass_material), _lib.ptr(batch.spring_offsets), _lib.ptr(batch.pairs),
@@ -179,15 +182,27 @@ class Simulator:
         flags = _lib.DEVO_REFERENCE_RANKS if reference_ranks else 0
         _lib.check(_lib.LIB.mb_devo(self._ctx, int(replaced_per_robot), int(seed), flags,
                                     ctypes.byref(n)), self._ctx)
-        pairs, mat, lbar = self.collect_springs()
-        self._batch = dataclasses.replace(self._batch, pairs=pairs, spring_material=mat, lbar=lbar)
+        self._topology_stale = True  # read back on demand (Collect, batch)
         return n.value
 
+    def _refresh_topology(self) -> None:
+        if self._topology_stale:
+            pairs, mat, lbar = self.collect_springs()
+            self._batch = dataclasses.replace(self._batch, pairs=pairs, spring_material=mat, lbar=lbar)
+            self._topology_stale = False
+
+    @property
+    def batch(self) -> Batch:
+        """The uploaded population, with the topology as development left it."""
+        self._refresh_topology()
+        return self._batch
+
     def devo_profile(self) -> dict:
-        """Host wall time (ms) of the phases of the last devo()."""
+        """Phases of the last devo(): wall ms of the device part and of a
+        host re-pack (0 if none), and the number of host re-packs so far."""
         ms = np.zeros(3, np.float64)
         _lib.check(_lib.LIB.mb_devo_profile(self._ctx, _lib.ptr(ms)), self._ctx)
-        return {"select_ms": float(ms[0]), "pack_ms": float(ms[1]), "upload_ms": float(ms[2])}
+        return {"device_ms": float(ms[0]), "host_repack_ms": float(ms[1]), "host_repacks": int(ms[2])}
 
     def collect_springs(self):
         """(pairs (S, 2) uint16, material (S,) uint8, mean length (S,) float32)

@@ -73,6 +73,47 @@ def test_devo_cycles_bit_exact(flags):
     sim.run_steps(150, True)
     orc.steps(150)
     check_same(sim, orc)
+    if not flags:  # moderate k: the device re-pack suffices every time
+        assert sim.devo_profile()["host_repacks"] == 0
+
+
+def test_devo_host_repack_path_bit_exact(monkeypatch):
+    """The host re-pack (the device path's fallback) gives the same bits."""
+    monkeypatch.setenv("MB_DEVO_HOST_REPACK", "1")
+    b = robots.population_batch("uneven", 16, seed_base=321)
+    sim = mb.Simulator(0)
+    sim.setTimeStep(1e-3)
+    sim.set_batch(b)
+    orc = OracleRun(b, mb.material_table(), np.float32(1e-3))
+    for cycle in range(2):
+        sim.run_steps(80, True)
+        orc.steps(80)
+        assert sim.devo(24, seed=cycle) == orc.devo(24, cycle)
+        check_same(sim, orc)
+    assert sim.devo_profile()["host_repacks"] == 2
+    sim.run_steps(80, True)
+    orc.steps(80)
+    check_same(sim, orc)
+
+
+def test_devo_rewiring_every_spring_bit_exact():
+    """k larger than every robot: all springs get new pairs, rows change
+    completely (the device path may fall back to the host re-pack)."""
+    els = [e for e in robots.population("uneven", 96) if e.n_springs <= 1024][:12]
+    assert len(els) == 12
+    b = mb.pack(els)
+    sim = mb.Simulator(0)
+    sim.setTimeStep(1e-3)
+    sim.set_batch(b)
+    orc = OracleRun(b, mb.material_table(), np.float32(1e-3))
+    for cycle in range(3):
+        sim.run_steps(60, True)
+        orc.steps(60)
+        assert sim.devo(1024, seed=7 + cycle) == orc.devo(1024, 7 + cycle) == b.n_springs
+        check_same(sim, orc)
+    sim.run_steps(60, True)
+    orc.steps(60)
+    check_same(sim, orc)
 
 
 def test_devo_through_simulator_api():
