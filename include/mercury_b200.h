@@ -217,6 +217,25 @@ MB_API mb_status mb_devo(mb_context* ctx, uint32_t replaced_per_robot, uint64_t 
  * context that needed the host re-pack.  No reference counterpart. */
 MB_API mb_status mb_devo_profile(const mb_context* ctx, double* ms);
 
+/* Population of voxel robots built on the device from cell grids -- the
+ * equivalent of VoxelRobot::Build (VoxelRobot.cpp:310-331, as mb_voxel_build
+ * restates it) for every robot followed by mb_set_elements, without the host
+ * build and packing.  cells: n_robots grids of sx*sy*sz base material ids
+ * (0 = air .. 22), x fastest, robot after robot (host memory); robot r is the
+ * lattice of (sx+1)(sy+1)(sz+1) points whose point (x, y, z) carries cell
+ * (x, y, z) and whose upper faces are air; spacing h, every mass `mass`,
+ * zero velocity.  Grids of one shape share one packing, planned on the
+ * first call and reused while n_robots, the shape, h, mass, the mode and
+ * the launch override stay the same; each call then costs one copy of the
+ * cells and three kernels.  At most 4,096 points per robot.  Synchronous.
+ * The topology read-back functions and mb_devo work on the result as on an
+ * uploaded batch. */
+MB_API mb_status mb_set_voxel_population(mb_context* ctx, uint32_t n_robots, int sx, int sy, int sz,
+                                         const uint8_t* cells, float h, float mass);
+
+/* Mass materials in the upload layout (after the strip of a device build). */
+MB_API mb_status mb_collect_mass_materials(mb_context* ctx, uint8_t* material);
+
 /* Topology in the upload layout (2 pair entries, 1 material, 1 mean length
  * per spring; any pointer may be NULL), as changed by mb_devo.  The
  * reference copies pairs, materials and mean lengths back in Collect

@@ -114,6 +114,8 @@ def _load() -> ctypes.CDLL:
         "mb_devo": (I32, [P, U32, ctypes.c_uint64, U32, ctypes.POINTER(U32)]),
         "mb_collect_springs": (I32, [P, P, P, P]),
         "mb_devo_profile": (I32, [P, P]),
+        "mb_set_voxel_population": (I32, [P, U32, I32, I32, I32, P, F32, F32]),
+        "mb_collect_mass_materials": (I32, [P, P]),
         "mb_version": (ctypes.c_char_p, []),
     }
     for name, (res, args) in sigs.items():

@@ -13,8 +13,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 SRC = [os.path.join(HERE, "csrc", f) for f in ("mb_kernels.cu", "mb_host.cpp", "mb_pack.cpp",
-                                               "mb_voxel.cpp", "mb_noalloc.cu", "mb_devo.cu")]
-DEPS = SRC + [os.path.join(HERE, "csrc", f) for f in ("mb_internal.h", "mb_sin.cuh", "mb_pack.h", "mb_devo.h")] + [
+                                               "mb_voxel.cpp", "mb_noalloc.cu", "mb_devo.cu", "mb_voxel_dev.cu")]
+DEPS = SRC + [os.path.join(HERE, "csrc", f) for f in ("mb_internal.h", "mb_sin.cuh", "mb_pack.h", "mb_devo.h", "mb_voxel.h", "mb_voxel_dev.h")] + [
     os.path.join(ROOT, "include", "mercury_b200.h")]
 OUT = os.path.join(HERE, "libmercury_b200.so")
 NVCC = os.environ.get("NVCC", "nvcc")

@@ -38,6 +38,8 @@
 #include "mb_devo.h"
 #include "mb_internal.h"
 #include "mb_pack.h"
+#include "mb_voxel.h"
+#include "mb_voxel_dev.h"
 
 namespace mb {
 
@@ -174,6 +176,23 @@ struct mb_context {
     mb::DevBuf<float> d_lbar;
     mb::DevBuf<uint32_t> pslot, robot_mass_base, free_count, free_taken, free_slots, devo_status, new_begin;
     mb::DevBuf<unsigned long long> rows_scratch;
+
+    // voxel populations built on the device (mb_set_voxel_population): the
+    // template packing of one grid, reused while the key matches
+    struct Voxel {
+        bool valid = false;      // template packing uploaded
+        uint32_t n_robots = 0;
+        int sx = 0, sy = 0, sz = 0;
+        uint32_t h_bits = 0, mass_bits = 0, mode = 0;
+        uint32_t n_points = 0, n_springs = 0;  // per robot
+        mb::DevBuf<float> pos;
+        mb::DevBuf<uint16_t> src;
+        mb::DevBuf<uint8_t> dir, cells;
+        mb::DevBuf<uint32_t> n_spring, word, gidx;
+        mb::DevBuf<float> lbar;
+    } vox;
+    bool vox_live = false;             // the population on the device came from the voxel builder
+    bool host_topology_stale = false;  // h_mass_mat / h_spring_mat / h_bins behind the device
 
     std::map<mb::GraphKey, cudaGraphExec_t> graphs;
 
@@ -419,8 +438,153 @@ mb_status host_repack(mb_context* c) {
     mb_status st = pack(c, &d, true, out);
     if (st == MB_OK) st = upload_packed(c, out);
     if (st != MB_OK) c->loaded = false;  // topology and packed arrays disagree now
+    c->vox.valid = false;
+    c->vox_live = false;
     ++c->devo_host_repacks;
     return st;
+}
+
+// Brings the host copies of materials and bins up to date after a device
+// build.
+mb_status ensure_host_topology(mb_context* c) {
+    if (!c->host_topology_stale) return MB_OK;
+    cudaStream_t st = c->stream;
+    c->h_mass_mat.resize(c->n_mass);
+    c->h_spring_mat.resize(c->n_spring);
+    MB_CUDA(c, cudaMemcpyAsync(c->h_mass_mat.data(), c->mass_mat.p, c->n_mass, cudaMemcpyDeviceToHost, st));
+    MB_CUDA(c, cudaMemcpyAsync(c->h_spring_mat.data(), c->d_spring_mat.p, c->n_spring, cudaMemcpyDeviceToHost, st));
+    MB_CUDA(c, cudaMemcpyAsync(c->h_bins.data(), c->bins.p, c->h_bins.size() * sizeof(mb::BinDesc),
+                               cudaMemcpyDeviceToHost, st));
+    MB_CUDA(c, cudaStreamSynchronize(st));
+    c->host_topology_stale = false;
+    return MB_OK;
+}
+
+// Template packing of a voxel population: every robot is the full lattice
+// of the grid with every spring active; rows get the template's size as
+// capacity (a robot's rows never need more than with every spring active).
+mb_status voxel_setup(mb_context* c, uint32_t R, int sx, int sy, int sz, float h, float mass) {
+    mb::VoxelTemplate T;
+    mb::voxel_template(sx + 1, sy + 1, sz + 1, h, T);
+    const uint32_t P = (uint32_t)((sx + 1) * (sy + 1) * (sz + 1)), Sr = (uint32_t)T.lbar.size();
+    const uint64_t M = (uint64_t)R * P, S = (uint64_t)R * Sr;
+    if (M >= (1ull << 31) || S >= (1ull << 31)) return fail(c, MB_ERR_CAPACITY, "population too large");
+    std::vector<int64_t> mo(R + 1), so(R + 1);
+    for (uint32_t r = 0; r <= R; ++r) {
+        mo[r] = (int64_t)r * P;
+        so[r] = (int64_t)r * Sr;
+    }
+    std::vector<uint16_t> pairs(2 * S);
+    std::vector<float> lbar(S);
+    for (uint32_t r = 0; r < R; ++r) {
+        std::memcpy(pairs.data() + 2 * (size_t)r * Sr, T.pairs.data(), 2 * Sr * sizeof(uint16_t));
+        std::memcpy(lbar.data() + (size_t)r * Sr, T.lbar.data(), Sr * sizeof(float));
+    }
+    std::vector<uint8_t> mm(M, 1), sm(S, 1);
+    const mb_batch_desc d{R, mo.data(), nullptr, nullptr, mm.data(), so.data(), pairs.data(), sm.data(), lbar.data()};
+    mb::Packed out;
+    mb_status st = pack(c, &d, false, out);
+    if (st != MB_OK) return st;
+    // rows with their template size as capacity, plus spare slice columns
+    {
+        const bool streamed = out.streamed;
+        std::vector<uint16_t> inc;
+        std::vector<uint32_t> inc32;
+        uint64_t total = 0;
+        for (auto& bd : out.bins) {
+            const uint32_t cap = (bd.n_inc + 8 * mb::kSliceWidth + 31) / 32 * 32;
+            if (streamed)
+                inc32.insert(inc32.end(), out.inc32.begin() + bd.inc_begin,
+                             out.inc32.begin() + bd.inc_begin + bd.n_inc);
+            else
+                inc.insert(inc.end(), out.inc.begin() + bd.inc_begin, out.inc.begin() + bd.inc_begin + bd.n_inc);
+            bd.inc_begin = (uint32_t)total;
+            bd.pad[0] = cap;
+            total += cap;
+            if (streamed)
+                inc32.resize(total, mb::kPadEntry32);
+            else
+                inc.resize(total, mb::kPadEntry);
+        }
+        if (total >= (1ull << 32)) return fail(c, MB_ERR_CAPACITY, "rows too large");
+        out.inc.swap(inc);
+        out.inc32.swap(inc32);
+    }
+    c->clear_graphs();
+    c->loaded = false;
+    c->n_robots = R;
+    c->n_mass = M;
+    c->n_spring = S;
+    c->mass_off = mo;
+    c->spring_off = so;
+    c->h_pairs.swap(pairs);
+    c->h_lbar.swap(lbar);
+    c->h_mass_mat.assign(M, 0);
+    c->h_spring_mat.assign(S, 0);
+    st = upload_packed(c, out);
+    if (st != MB_OK) return st;
+    cudaStream_t cs = c->stream;
+    auto up = [&](auto& buf, const auto* src, size_t n) -> cudaError_t {
+        cudaError_t e = buf.alloc(n);
+        if (e != cudaSuccess || n == 0) return e;
+        return cudaMemcpyAsync(buf.p, src, n * sizeof(*src), cudaMemcpyHostToDevice, cs);
+    };
+    // every non-air composite gets a material slot
+    std::vector<uint8_t> ids, slot(256, mb::kNoMatSlot);
+    for (int id = 1; id < MB_COMPOSITE_COUNT; ++id) {
+        slot[id] = (uint8_t)ids.size();
+        ids.push_back((uint8_t)id);
+    }
+    c->h_mat_ids = ids;
+    c->n_mat_host = (uint32_t)ids.size();
+    MB_CUDA(c, up(c->mat_ids, ids.data(), ids.size()));
+    MB_CUDA(c, up(c->n_mat, &c->n_mat_host, 1));
+    MB_CUDA(c, c->invk.alloc(c->n_mat_host));
+    MB_CUDA(c, c->rates.alloc((size_t)c->n_mat_host * c->chunk));
+    MB_CUDA(c, up(c->slot_of, slot.data(), 256));
+    // template arrays
+    std::vector<uint32_t> word(out.pair.size()), nsp(out.bins.size());
+    for (size_t i = 0; i < word.size(); ++i) word[i] = out.pair[i] & 0xFFFFFFu;
+    for (size_t b = 0; b < out.bins.size(); ++b) nsp[b] = out.bins[b].n_spring;
+    auto& v = c->vox;
+    MB_CUDA(c, up(v.word, word.data(), word.size()));
+    MB_CUDA(c, up(v.lbar, out.lbar.data(), out.lbar.size()));
+    MB_CUDA(c, up(v.gidx, out.spring_gidx.data(), out.spring_gidx.size()));
+    MB_CUDA(c, up(v.n_spring, nsp.data(), nsp.size()));
+    MB_CUDA(c, up(v.pos, T.pos.data(), T.pos.size()));
+    std::vector<uint16_t> src(Sr);
+    for (uint32_t s = 0; s < Sr; ++s) src[s] = T.pairs[2 * s];
+    MB_CUDA(c, up(v.src, src.data(), Sr));
+    MB_CUDA(c, up(v.dir, T.dir.data(), Sr));
+    // population arrays
+    MB_CUDA(c, up(c->d_mass_off, mo.data(), R + 1));
+    MB_CUDA(c, up(c->d_spring_off, so.data(), R + 1));
+    MB_CUDA(c, c->pos.alloc(M));
+    MB_CUDA(c, c->vel.alloc(M));
+    MB_CUDA(c, c->mass_mat.alloc(M));
+    MB_CUDA(c, c->d_spring_mat.alloc(S));
+    MB_CUDA(c, c->stress.alloc(S + 1));
+    MB_CUDA(c, cudaMemsetAsync(c->stress.p, 0, (S + 1) * sizeof(float), cs));
+    MB_CUDA(c, c->robot_flags.alloc(R));
+    MB_CUDA(c, c->com.alloc(3 * (size_t)R));
+    const uint32_t nb = c->n_bins;
+    MB_CUDA(c, c->free_count.alloc(nb));
+    MB_CUDA(c, c->free_taken.alloc(nb));
+    MB_CUDA(c, c->rows_scratch.alloc(2 * (size_t)c->n_packed));
+    MB_CUDA(c, c->devo_status.alloc(2));
+    MB_CUDA(c, v.cells.alloc((size_t)R * sx * sy * sz));
+    MB_CUDA(c, cudaStreamSynchronize(cs));
+    v.valid = true;
+    v.n_robots = R;
+    v.sx = sx;
+    v.sy = sy;
+    v.sz = sz;
+    std::memcpy(&v.h_bits, &h, 4);
+    std::memcpy(&v.mass_bits, &mass, 4);
+    v.mode = (uint32_t)c->mode;
+    v.n_points = P;
+    v.n_springs = Sr;
+    return MB_OK;
 }
 
 }  // namespace mb_detail
@@ -602,6 +766,7 @@ mb_status mb_set_launch_config(mb_context* ctx, const mb_launch_config* cfg) {
     }
     ctx->use_graph = cfg->use_graph != 0;
     ctx->clear_graphs();
+    ctx->vox.valid = false;  // the next voxel upload re-plans its template
     return MB_OK;
 }
 
@@ -641,6 +806,9 @@ mb_status mb_set_elements(mb_context* ctx, const mb_batch_desc* b) {
     // re-packing after development) and upload state and packed arrays
     ctx->clear_graphs();
     ctx->loaded = false;
+    ctx->vox.valid = false;
+    ctx->vox_live = false;
+    ctx->host_topology_stale = false;
     ctx->n_robots = R;
     ctx->n_mass = M;
     ctx->n_spring = S;
@@ -903,6 +1071,12 @@ mb_status mb_devo(mb_context* ctx, uint32_t replaced_per_robot, uint64_t seed, u
     using clock = std::chrono::steady_clock;
     const auto t0 = clock::now();
     cudaStream_t st = ctx->stream;
+    {
+        mb_status s = mb_detail::ensure_host_topology(ctx);
+        // a population from the voxel builder becomes a regular packing first
+        if (s == MB_OK && ctx->vox_live) s = mb_detail::host_repack(ctx);
+        if (s != MB_OK) return s;
+    }
     const char* force_host = std::getenv("MB_DEVO_HOST_REPACK");
     const bool on_device = !(force_host && force_host[0] == '1');
     if (on_device && !ctx->devo_ready) {
@@ -979,9 +1153,87 @@ mb_status mb_devo_profile(const mb_context* ctx, double* ms) {
     return MB_OK;
 }
 
+mb_status mb_set_voxel_population(mb_context* ctx, uint32_t n_robots, int sx, int sy, int sz,
+                                  const uint8_t* cells, float h, float mass) {
+    if (!ctx || !cells) return fail(ctx, MB_ERR_ARGUMENT, "null argument");
+    if (!ctx->have_table) return fail(ctx, MB_ERR_STATE, "material table not set");
+    if (n_robots == 0 || sx <= 0 || sy <= 0 || sz <= 0) return fail(ctx, MB_ERR_ARGUMENT, "empty population");
+    if ((int64_t)(sx + 1) * (sy + 1) * (sz + 1) > (int64_t)mb::kVoxelMaxPoints)
+        return fail(ctx, MB_ERR_CAPACITY, "at most %u grid points per robot", mb::kVoxelMaxPoints);
+    if (!std::isfinite(h) || !(h > 0.0f) || !std::isfinite(mass))
+        return fail(ctx, MB_ERR_ARGUMENT, "cell size and mass must be finite, cell size positive");
+    cudaSetDevice(ctx->device);
+    auto& v = ctx->vox;
+    uint32_t hb, mbits;
+    std::memcpy(&hb, &h, 4);
+    std::memcpy(&mbits, &mass, 4);
+    if (!v.valid || v.n_robots != n_robots || v.sx != sx || v.sy != sy || v.sz != sz || v.h_bits != hb ||
+        v.mass_bits != mbits || v.mode != (uint32_t)ctx->mode) {
+        const mb_status s = mb_detail::voxel_setup(ctx, n_robots, sx, sy, sz, h, mass);
+        if (s != MB_OK) {
+            ctx->loaded = false;
+            v.valid = false;
+            return s;
+        }
+    }
+    cudaStream_t st = ctx->stream;
+    const size_t nc = (size_t)n_robots * sx * sy * sz;
+    MB_CUDA(ctx, cudaMemcpyAsync(v.cells.p, cells, nc, cudaMemcpyHostToDevice, st));
+    MB_CUDA(ctx, cudaMemsetAsync(ctx->devo_status.p, 0, 2 * sizeof(uint32_t), st));
+    MB_CUDA(ctx, cudaMemsetAsync(ctx->free_count.p, 0, ctx->n_bins * sizeof(uint32_t), st));
+    MB_CUDA(ctx, cudaMemsetAsync(ctx->free_taken.p, 0, ctx->n_bins * sizeof(uint32_t), st));
+    const mb::VoxelBuildParams bp{n_robots, sx, sy, sz, v.cells.p, v.pos.p, v.src.p, v.dir.p, v.n_springs, mass,
+                                  ctx->pos.p, ctx->vel.p, ctx->mass_mat.p, ctx->d_spring_mat.p, ctx->stress.p,
+                                  ctx->devo_status.p};
+    MB_CUDA(ctx, mb::launch_voxel_build(bp, st));
+    const mb::CompactParams cp{ctx->bins.p, ctx->n_bins, v.n_spring.p, v.word.p, v.lbar.p, v.gidx.p,
+                               ctx->d_spring_mat.p, ctx->slot_of.p, ctx->spring_pair.p, ctx->spring_lbar.p,
+                               ctx->spring_gidx.p, ctx->devo_status.p};
+    MB_CUDA(ctx, mb::launch_compact(cp, st));
+    const mb::RebuildParams rp{ctx->bins.p,        ctx->n_bins,          ctx->spring_pair.p,
+                               ctx->spring_gidx.p, (uint32_t)ctx->n_spring, ctx->slice_off.p,
+                               ctx->slice_width.p, ctx->inc.p,           ctx->inc32.p,
+                               ctx->streamed ? 1u : 0u, ctx->rows_scratch.p, ctx->free_count.p,
+                               ctx->free_taken.p,  ctx->devo_status.p};
+    MB_CUDA(ctx, mb::launch_rebuild(rp, st));
+    uint32_t status[2] = {0, 0};
+    MB_CUDA(ctx, cudaMemcpyAsync(status, ctx->devo_status.p, sizeof(status), cudaMemcpyDeviceToHost, st));
+    MB_CUDA(ctx, cudaStreamSynchronize(st));
+    ctx->host_topology_stale = true;
+    ctx->vox_live = true;
+    ctx->devo_ready = false;
+    if (status[0]) {
+        ctx->loaded = false;
+        return fail(ctx, MB_ERR_ARGUMENT, "cell materials must be base material ids 0..22");
+    }
+    if (!ctx->streamed && status[1] > ctx->smem_bytes) {
+        if (status[1] > mb::max_step_smem(ctx->device)) {
+            ctx->loaded = false;
+            return fail(ctx, MB_ERR_CAPACITY, "rows exceed shared memory");
+        }
+        ctx->smem_bytes = status[1];
+        ctx->clear_graphs();
+    }
+    ctx->loaded = true;
+    return MB_OK;
+}
+
+mb_status mb_collect_mass_materials(mb_context* ctx, uint8_t* material) {
+    if (!ctx || !material) return fail(ctx, MB_ERR_ARGUMENT, "null argument");
+    if (!ctx->loaded) return fail(ctx, MB_ERR_STATE, "no population uploaded");
+    const mb_status s = mb_detail::ensure_host_topology(ctx);
+    if (s != MB_OK) return s;
+    if (!ctx->h_mass_mat.empty()) std::memcpy(material, ctx->h_mass_mat.data(), ctx->h_mass_mat.size());
+    return MB_OK;
+}
+
 mb_status mb_collect_springs(mb_context* ctx, uint16_t* pairs, uint8_t* material, float* lbar) {
     if (!ctx) return MB_ERR_ARGUMENT;
     if (!ctx->loaded) return fail(ctx, MB_ERR_STATE, "no population uploaded");
+    {
+        const mb_status s = mb_detail::ensure_host_topology(ctx);
+        if (s != MB_OK) return s;
+    }
     if (pairs && !ctx->h_pairs.empty()) std::memcpy(pairs, ctx->h_pairs.data(), ctx->h_pairs.size() * sizeof(uint16_t));
     if (material && !ctx->h_spring_mat.empty())
         std::memcpy(material, ctx->h_spring_mat.data(), ctx->h_spring_mat.size());

@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "../../include/mercury_b200.h"
+#include "mb_voxel.h"
 
 namespace mb {
 
@@ -127,6 +128,77 @@ void strip(const Lattice& L, std::vector<uint8_t>& mat) {
 }
 
 }  // namespace
+
+void voxel_template(int nx, int ny, int nz, float h, VoxelTemplate& t) {
+    const Lattice L{nx, ny, nz};
+    const int n = nx * ny * nz;
+    t.nx = nx;
+    t.ny = ny;
+    t.nz = nz;
+    // masses at h * index
+    std::vector<float> px(n), py(n), pz(n);
+    for (int v = 0; v < n; ++v) {
+        const Idx i = L.at(v);
+        px[v] = h * (float)i.x;
+        py[v] = h * (float)i.y;
+        pz[v] = h * (float)i.z;
+    }
+    // depth-first walk from point 0 (VoxelRobot.cpp:60-193), iterative; it
+    // visits every grid point whatever the materials, so the springs, their
+    // order and mean lengths depend on the grid size only
+    t.pairs.clear();
+    t.lbar.clear();
+    t.dir.clear();
+    std::vector<uint8_t> visited(n, 0);
+    struct Frame {
+        int v, k;
+    };
+    std::vector<Frame> stack;
+    visited[0] = 1;
+    stack.push_back({0, 0});
+    while (!stack.empty()) {
+        Frame& f = stack.back();
+        if (f.k == 13) {
+            stack.pop_back();
+            continue;
+        }
+        const int k = f.k++;
+        const int src = f.v;
+        const Idx it = add(L.at(src), kDirs[k]);
+        if (!L.valid(it)) continue;
+        const int v = L.id(it);
+        // mean length |base_src - base_v| as Eigen's norm(): d0^2 + (d1^2 + d2^2)
+        const float d0 = px[src] - px[v], d1 = py[src] - py[v], d2 = pz[src] - pz[v];
+        const float q12 = d1 * d1 + d2 * d2;
+        const float len = std::sqrt(d0 * d0 + q12);
+        t.pairs.push_back((uint16_t)src);
+        t.pairs.push_back((uint16_t)v);
+        t.lbar.push_back(len);
+        t.dir.push_back((uint8_t)k);
+        if (visited[v]) continue;
+        visited[v] = 1;
+        stack.push_back({v, 0});
+    }
+    // ShiftX then ShiftY (VoxelRobot.cpp:30-56): translate by -max x, then by
+    // -min y, over all masses.
+    float max_x = px[0];
+    for (int v = 1; v < n; ++v)
+        if (px[v] > max_x) max_x = px[v];
+    const float tx = -max_x;
+    for (int v = 0; v < n; ++v) px[v] = px[v] + tx;
+    float min_y = py[0];
+    for (int v = 1; v < n; ++v)
+        if (py[v] < min_y) min_y = py[v];
+    const float ty = -min_y;
+    for (int v = 0; v < n; ++v) py[v] = py[v] + ty;
+    t.pos.resize(3 * (size_t)n);
+    for (int v = 0; v < n; ++v) {
+        t.pos[3 * v] = px[v];
+        t.pos[3 * v + 1] = py[v];
+        t.pos[3 * v + 2] = pz[v];
+    }
+}
+
 }  // namespace mb
 
 extern "C" mb_status mb_voxel_build(int nx, int ny, int nz, float h, const uint8_t* mats,
@@ -144,68 +216,19 @@ extern "C" mb_status mb_voxel_build(int nx, int ny, int nz, float h, const uint8
     const Lattice L{nx, ny, nz};
     std::vector<uint8_t> mat(mats, mats + n);
     strip(L, mat);
-
-    // masses at h * index
-    std::vector<float> px(n), py(n), pz(n);
-    for (int v = 0; v < (int)n; ++v) {
-        const Idx i = L.at(v);
-        px[v] = h * (float)i.x;
-        py[v] = h * (float)i.y;
-        pz[v] = h * (float)i.z;
+    VoxelTemplate t;
+    voxel_template(nx, ny, nz, h, t);
+    const int ns = (int)t.lbar.size();
+    for (int s = 0; s < ns; ++s) {
+        pairs[2 * s] = t.pairs[2 * s];
+        pairs[2 * s + 1] = t.pairs[2 * s + 1];
+        lbar[s] = t.lbar[s];
+        spring_material[s] = (uint8_t)edge_material(L, mat, L.at(t.pairs[2 * s]), kDirs[t.dir[s]]);
     }
-
-    // depth-first walk from point 0 (VoxelRobot.cpp:60-193), iterative
-    std::vector<uint8_t> visited(n, 0);
-    struct Frame {
-        int v, k;
-    };
-    std::vector<Frame> stack;
-    int ns = 0;
-    visited[0] = 1;
-    stack.push_back({0, 0});
-    while (!stack.empty()) {
-        Frame& f = stack.back();
-        if (f.k == 13) {
-            stack.pop_back();
-            continue;
-        }
-        const int k = f.k++;
-        const int src = f.v;
-        const Idx isrc = L.at(src);
-        const Idx it = add(isrc, kDirs[k]);
-        if (!L.valid(it)) continue;
-        const int v = L.id(it);
-        // mean length |base_src - base_v| as Eigen's norm(): d0^2 + (d1^2 + d2^2)
-        const float d0 = px[src] - px[v], d1 = py[src] - py[v], d2 = pz[src] - pz[v];
-        const float q12 = d1 * d1 + d2 * d2;
-        const float len = std::sqrt(d0 * d0 + q12);
-        pairs[2 * ns] = (uint16_t)src;
-        pairs[2 * ns + 1] = (uint16_t)v;
-        lbar[ns] = len;
-        spring_material[ns] = (uint8_t)edge_material(L, mat, isrc, kDirs[k]);
-        ++ns;
-        if (visited[v]) continue;
-        visited[v] = 1;
-        stack.push_back({v, 0});
-    }
-
-    // ShiftX then ShiftY (VoxelRobot.cpp:30-56): translate by -max x, then by
-    // -min y, over all masses.
-    float max_x = px[0];
-    for (long long v = 1; v < n; ++v)
-        if (px[v] > max_x) max_x = px[v];
-    const float tx = -max_x;
-    for (long long v = 0; v < n; ++v) px[v] = px[v] + tx;
-    float min_y = py[0];
-    for (long long v = 1; v < n; ++v)
-        if (py[v] < min_y) min_y = py[v];
-    const float ty = -min_y;
-    for (long long v = 0; v < n; ++v) py[v] = py[v] + ty;
-
     for (long long v = 0; v < n; ++v) {
-        pos[3 * v] = px[v];
-        pos[3 * v + 1] = py[v];
-        pos[3 * v + 2] = pz[v];
+        pos[3 * v] = t.pos[3 * v];
+        pos[3 * v + 1] = t.pos[3 * v + 1];
+        pos[3 * v + 2] = t.pos[3 * v + 2];
         mass_material[v] = mat[v];
     }
     *n_masses = (int)n;

@@ -126,7 +126,9 @@ def unpack(batch: Batch, pos: np.ndarray, vel: np.ndarray, stress: np.ndarray | 
         x = e.copy()
         x.pos = pos[ms, :3].copy()
         x.vel = vel[ms, :3].copy()
-        # topology from the batch: development may have rewired springs
+        # topology from the batch: development may have rewired springs, a
+        # device build decides the materials
+        x.mass_material = batch.mass_material[ms].copy()
         x.pairs = batch.pairs[ss].copy()
         x.spring_material = batch.spring_material[ss].copy()
         x.mean_length = batch.lbar[ss].copy()

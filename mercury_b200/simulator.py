@@ -165,6 +165,7 @@ class Simulator:
 
     def set_batch(self, batch: Batch) -> None:
         self._batch = batch
+        self._vox_batch_n = None
         self._topology_stale = False
         d = _lib.BatchDesc(
             batch.n_robots, _lib.ptr(batch.mass_offsets), _lib.ptr(batch.pos), _lib.ptr(batch.vel),
@@ -188,8 +189,42 @@ class Simulator:
     def _refresh_topology(self) -> None:
         if self._topology_stale:
             pairs, mat, lbar = self.collect_springs()
-            self._batch = dataclasses.replace(self._batch, pairs=pairs, spring_material=mat, lbar=lbar)
+            mm = np.empty(self._batch.n_masses, np.uint8)
+            _lib.check(_lib.LIB.mb_collect_mass_materials(self._ctx, _lib.ptr(mm)), self._ctx)
+            self._batch = dataclasses.replace(self._batch, pairs=pairs, spring_material=mat, lbar=lbar,
+                                              mass_material=mm)
             self._topology_stale = False
+
+    def set_voxel_population(self, cells: np.ndarray, h: float = 0.1, mass: float = 1.0) -> None:
+        """Uploads voxel robots built on the device (mb_set_voxel_population)
+        from `cells`, an (R, sx, sy, sz) array of base material ids indexed
+        [robot, x, y, z]; the same robots as pack([robots.voxel_robot(c, h,
+        mass) for c in cells]) followed by set_batch."""
+        cells = np.asarray(cells, np.uint8)
+        if cells.ndim != 4:
+            raise ValueError("cells must be (robots, sx, sy, sz)")
+        R, sx, sy, sz = cells.shape
+        flat = np.ascontiguousarray(cells.transpose(0, 3, 2, 1))  # x fastest
+        _lib.check(_lib.LIB.mb_set_voxel_population(self._ctx, R, sx, sy, sz, _lib.ptr(flat), float(h),
+                                                    float(mass)), self._ctx)
+        key = (sx, sy, sz, float(h), float(mass))
+        if getattr(self, "_vox_tmpl_key", None) != key:
+            from .robots import lattice_robot
+            self._vox_tmpl = lattice_robot(np.ones((sx + 1, sy + 1, sz + 1), np.uint8), h, mass)
+            self._vox_tmpl_key = key
+        t = self._vox_tmpl
+        if self._batch is None or getattr(self, "_vox_batch_n", None) != (R, key):
+            P, S = t.n_masses, t.n_springs
+            pos = np.zeros((R * P, 4), np.float32)
+            pos[:, :3] = np.tile(t.pos, (R, 1))
+            pos[:, 3] = mass
+            self._batch = Batch(np.arange(R + 1, dtype=np.int64) * P, pos, np.zeros((R * P, 4), np.float32),
+                                np.zeros(R * P, np.uint8), np.arange(R + 1, dtype=np.int64) * S,
+                                np.tile(t.pairs, (R, 1)), np.zeros(R * S, np.uint8),
+                                np.tile(t.mean_length, R))
+            self._vox_batch_n = (R, key)
+        self._elements = [t] * R
+        self._topology_stale = True
 
     @property
     def batch(self) -> Batch:
