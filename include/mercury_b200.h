@@ -319,6 +319,38 @@ MB_API mb_status mb_simulate_robot_noalloc(void* stream, const float* table,
                                            float t0, uint32_t steps, int track_stresses,
                                            float* t_end);
 
+/* ----------------------------------------------------------------------
+ * Fitness surrogate (no reference counterpart): a 3-D convolutional network
+ * over 6x6x6 voxel genomes of 5 classes (0 air, 1 bone, 2 tissue, 3 muscle
+ * a, 4 muscle b; any other value reads as no class) that predicts the
+ * simulated fitness.  Three 3x3x3 convolutions of 32 channels with ReLU, a
+ * 6,912 -> 128 -> 128 MLP with ReLU, a linear output; BF16 tensor-core
+ * GEMMs with FP32 accumulation, FP32 master weights, Adam.  Genome and
+ * target pointers are host memory; every call is synchronous. */
+typedef struct mb_surrogate mb_surrogate;
+MB_API mb_status mb_surrogate_create(int device, uint32_t max_batch, uint64_t seed, mb_surrogate** out);
+MB_API void mb_surrogate_destroy(mb_surrogate* s);
+MB_API const char* mb_surrogate_last_error(const mb_surrogate* s);
+/* Parameters as one FP32 array: W1 [32][27*8] (k = offset*8 + channel,
+ * offset = (dx+1) + 3(dy+1) + 9(dz+1)), b1 [32], W2 [32][27*32], b2, W3
+ * [32][27*32], b3, W4 [128][6912] (input index voxel*32 + channel, voxel =
+ * x + 6y + 36z), b4 [128], W5 [128][128], b5, W6 [128], b6 [1]; each tensor
+ * starts at offsets[i] (13 entries, the last the total count). */
+MB_API uint32_t mb_surrogate_param_count(void);
+MB_API void mb_surrogate_layout(uint32_t* offsets);
+MB_API mb_status mb_surrogate_get_params(mb_surrogate* s, float* params);
+/* Sets the weights and resets the optimiser state. */
+MB_API mb_status mb_surrogate_set_params(mb_surrogate* s, const float* params);
+/* Predictions for n genomes (216 bytes each, voxel x + 6y + 36z). */
+MB_API mb_status mb_surrogate_predict(mb_surrogate* s, const uint8_t* genomes, uint32_t n, float* out);
+/* Mean-squared-error loss and its gradient (layout of the parameters) for
+ * one batch of n <= max_batch genomes, without an update. */
+MB_API mb_status mb_surrogate_gradients(mb_surrogate* s, const uint8_t* genomes, const float* targets, uint32_t n,
+                                        float* grads, float* loss);
+/* One Adam step (beta 0.9 / 0.999, eps 1e-8) at learning rate lr. */
+MB_API mb_status mb_surrogate_train_step(mb_surrogate* s, const uint8_t* genomes, const float* targets, uint32_t n,
+                                         float lr, float* loss);
+
 /* Library version string. */
 MB_API const char* mb_version(void);
 

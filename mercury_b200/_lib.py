@@ -116,6 +116,16 @@ def _load() -> ctypes.CDLL:
         "mb_devo_profile": (I32, [P, P]),
         "mb_set_voxel_population": (I32, [P, U32, I32, I32, I32, P, F32, F32]),
         "mb_collect_mass_materials": (I32, [P, P]),
+        "mb_surrogate_create": (I32, [I32, U32, ctypes.c_uint64, ctypes.POINTER(P)]),
+        "mb_surrogate_destroy": (None, [P]),
+        "mb_surrogate_last_error": (ctypes.c_char_p, [P]),
+        "mb_surrogate_param_count": (U32, []),
+        "mb_surrogate_layout": (None, [P]),
+        "mb_surrogate_get_params": (I32, [P, P]),
+        "mb_surrogate_set_params": (I32, [P, P]),
+        "mb_surrogate_predict": (I32, [P, P, U32, P]),
+        "mb_surrogate_gradients": (I32, [P, P, P, U32, P, P]),
+        "mb_surrogate_train_step": (I32, [P, P, P, U32, F32, P]),
         "mb_version": (ctypes.c_char_p, []),
     }
     for name, (res, args) in sigs.items():

@@ -13,13 +13,14 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 SRC = [os.path.join(HERE, "csrc", f) for f in ("mb_kernels.cu", "mb_host.cpp", "mb_pack.cpp",
-                                               "mb_voxel.cpp", "mb_noalloc.cu", "mb_devo.cu", "mb_voxel_dev.cu")]
-DEPS = SRC + [os.path.join(HERE, "csrc", f) for f in ("mb_internal.h", "mb_sin.cuh", "mb_pack.h", "mb_devo.h", "mb_voxel.h", "mb_voxel_dev.h")] + [
+                                               "mb_voxel.cpp", "mb_noalloc.cu", "mb_devo.cu", "mb_voxel_dev.cu", "mb_surrogate.cu")]
+DEPS = SRC + [os.path.join(HERE, "csrc", f) for f in ("mb_internal.h", "mb_sin.cuh", "mb_pack.h", "mb_devo.h", "mb_voxel.h", "mb_voxel_dev.h", "mb_sg_kernels.cuh")] + [
     os.path.join(ROOT, "include", "mercury_b200.h")]
 OUT = os.path.join(HERE, "libmercury_b200.so")
 NVCC = os.environ.get("NVCC", "nvcc")
-FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-gencode", "arch=compute_100a,code=sm_100a",
-         "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall", "-Xcompiler", "-fvisibility=hidden", "-shared", "-lpthread"]
+COMMON = ["-std=c++17", "-O3", "-lineinfo", "-gencode", "arch=compute_100a,code=sm_100a",
+          "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall", "-Xcompiler", "-fvisibility=hidden"]
+OBJ_DIR = os.path.join(HERE, "_build")
 
 
 def up_to_date() -> bool:
@@ -29,16 +30,27 @@ def up_to_date() -> bool:
     return all(os.path.getmtime(d) <= t for d in DEPS)
 
 
+def _run(cmd):
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"nvcc failed:\n{' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+    return r.stderr
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
+    """Compiles every source to an object in parallel (mercury_b200/_build),
+    then links libmercury_b200.so."""
     if force or not up_to_date():
-        cmd = [NVCC, *FLAGS, "-o", OUT, *SRC]
+        from concurrent.futures import ThreadPoolExecutor
+        os.makedirs(OBJ_DIR, exist_ok=True)
+        objs = [os.path.join(OBJ_DIR, os.path.basename(src) + ".o") for src in SRC]
+        extra = ["-Xptxas=-v"] if verbose else []
+        with ThreadPoolExecutor(max_workers=len(SRC)) as ex:
+            logs = list(ex.map(lambda so: _run([NVCC, *COMMON, *extra, "-c", "-o", so[1], so[0]]),
+                               zip(SRC, objs)))
+        _run([NVCC, *COMMON, "-shared", "-o", OUT, *objs, "-lpthread"])
         if verbose:
-            cmd.insert(1, "-Xptxas=-v")
-        r = subprocess.run(cmd, capture_output=True, text=True)
-        if r.returncode != 0:
-            raise RuntimeError(f"nvcc failed:\n{' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
-        if verbose:
-            print(r.stderr)
+            print("\n".join(logs))
     return OUT
 
 

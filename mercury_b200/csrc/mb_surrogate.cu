@@ -1,0 +1,682 @@
+// Fitness surrogate for the evolutionary loop: a small 3-D convolutional
+// network over voxel genomes, trained on (genome, simulated fitness) pairs
+// and used to screen candidates before they are simulated.  There is no
+// counterpart in the reference; its C ABI is in include/mercury_b200.h.
+//
+// Network (channels-last, one genome = 6x6x6 voxels of 5 classes):
+//   x0   one-hot classes, 8 channels (classes 0..4, channels 5..7 zero)
+//   a1 = relu(conv3x3x3(x0; W1 [32][27*8]) + b1)      same padding
+//   a2 = relu(conv3x3x3(a1; W2 [32][27*32]) + b2)
+//   a3 = relu(conv3x3x3(a2; W3 [32][27*32]) + b3)
+//   h1 = relu(W4 [128][6912] flatten(a3) + b4)        flatten index v*32 + c
+//   h2 = relu(W5 [128][128] h1 + b5)
+//   y  = W6 [128] . h2 + b6
+// Loss: mean squared error against the targets.  Optimiser: Adam on FP32
+// master weights; the GEMMs read BF16 copies of weights and activations and
+// accumulate in FP32 (mb_sg_kernels.cuh).  Every reduction runs in a fixed
+// order, so predictions and gradients are reproducible to the bit.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/mercury_b200.h"
+#include "mb_sg_kernels.cuh"
+
+namespace mb {
+namespace sg {
+namespace {
+
+using bf16 = __nv_bfloat16;
+
+// ---------------------------------------------------------------------------
+// GEMM
+
+__device__ __forceinline__ void ldsm_x4(uint32_t* r, const void* p) {
+    const uint32_t a = (uint32_t)__cvta_generic_to_shared(p);
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(a));
+}
+__device__ __forceinline__ void ldsm_x4_t(uint32_t* r, const void* p) {
+    const uint32_t a = (uint32_t)__cvta_generic_to_shared(p);
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(a));
+}
+__device__ __forceinline__ void mma_bf16(float* c, const uint32_t* a, const uint32_t* b) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+constexpr int kLdK = kTileK + 8;   // row of a K-major tile (elements): 80 bytes
+constexpr int kLdMN = kTileM + 8;  // row of an MN-major tile: 144 bytes
+constexpr int kStage = kTileM * kLdK;  // >= kTileK * kLdMN
+
+__device__ __forceinline__ float epilogue(const GemmArgs& g, int row, int col, float v) {
+    if (g.bias) v += g.bias[col];
+    if (g.relu) v = fmaxf(v, 0.0f);
+    if (g.mask && !(__bfloat162float(g.mask[(size_t)row * g.ldc + col]) > 0.0f)) v = 0.0f;
+    return v;
+}
+
+__device__ __forceinline__ void store(const GemmArgs& g, int row, int col, float v) {
+    const size_t i = (size_t)row * g.ldc + col;
+    if (g.c32) g.c32[i] = v;
+    if (g.c16) g.c16[i] = __float2bfloat16_rn(v);
+}
+
+template <int AV, int BV>
+__device__ __forceinline__ void load_stage(const GemmArgs& g, bf16* as, bf16* bs, int m0, int n0, int k0,
+                                           int k_end) {
+    const int tid = threadIdx.x;
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {
+        const int i = tid + t * kGemmThreads;
+        if (AV == kDenseMN) {
+            const int kr = i >> 3, ch = i & 7, gk = k0 + kr, gm = m0 + ch * 8;
+            const bool ok = gk < k_end && gm < g.M;
+            cp_async16(as + kr * kLdMN + ch * 8, ok ? g.A + (size_t)gk * g.lda + gm : g.A, ok);
+        } else {
+            const int row = i >> 2, ch = i & 3, gm = m0 + row, gk = k0 + ch * 8;
+            const bf16* src = nullptr;
+            if (gm < g.M && gk < k_end)
+                src = AV == kIm2col ? im2col_chunk(g.A, g.lda, gm, gk, g.flip_a) : g.A + (size_t)gm * g.lda + gk;
+            cp_async16(as + row * kLdK + ch * 8, src ? src : g.A, src != nullptr);
+        }
+        if (BV == kDenseK) {
+            const int row = i >> 2, ch = i & 3, gn = n0 + row, gk = k0 + ch * 8;
+            const bool ok = gn < g.N && gk < k_end;
+            cp_async16(bs + row * kLdK + ch * 8, ok ? g.B + (size_t)gn * g.ldb + gk : g.B, ok);
+        } else {
+            const int kr = i >> 3, ch = i & 7, gk = k0 + kr, gn = n0 + ch * 8;
+            const bf16* src = nullptr;
+            if (gk < k_end && gn < g.N)
+                src = BV == kIm2col ? im2col_chunk(g.B, g.ldb, gk, gn, g.flip_b) : g.B + (size_t)gk * g.ldb + gn;
+            cp_async16(bs + kr * kLdMN + ch * 8, src ? src : g.B, src != nullptr);
+        }
+    }
+}
+
+template <int AV, int BV>
+__global__ void __launch_bounds__(kGemmThreads) gemm_kernel(const GemmArgs g) {
+    __shared__ __align__(16) bf16 As[2][kStage];
+    __shared__ __align__(16) bf16 Bs[2][kStage];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int m0 = blockIdx.y * kTileM, n0 = blockIdx.x * kTileN;
+    const int k_begin = blockIdx.z * g.k_chunk;
+    const int k_end = min(g.K, k_begin + g.k_chunk);
+    const int nk = k_end > k_begin ? (k_end - k_begin + kTileK - 1) / kTileK : 0;
+    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+    float acc[2][4][4];
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.0f;
+
+    if (nk > 0) {
+        load_stage<AV, BV>(g, As[0], Bs[0], m0, n0, k_begin, k_end);
+        cp_async_commit();
+    }
+    for (int t = 0; t < nk; ++t) {
+        cp_async_wait_all();
+        __syncthreads();
+        if (t + 1 < nk) {
+            load_stage<AV, BV>(g, As[(t + 1) & 1], Bs[(t + 1) & 1], m0, n0, k_begin + (t + 1) * kTileK, k_end);
+            cp_async_commit();
+        }
+        const bf16* as = As[t & 1];
+        const bf16* bs = Bs[t & 1];
+#pragma unroll
+        for (int kk = 0; kk < kTileK; kk += 16) {
+            uint32_t a[2][4], b[4][2];
+#pragma unroll
+            for (int i = 0; i < 2; ++i) {
+                const int mb = wm + 16 * i;
+                if (AV == kDenseMN)
+                    ldsm_x4_t(a[i], as + (kk + (lane & 7) + ((lane >> 4) << 3)) * kLdMN + mb + ((lane >> 3) & 1) * 8);
+                else
+                    ldsm_x4(a[i], as + (mb + (lane & 15)) * kLdK + kk + (lane >> 4) * 8);
+            }
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                const int nb = wn + 16 * j;
+                uint32_t r[4];
+                if (BV == kDenseK)
+                    ldsm_x4(r, bs + (nb + (lane & 7) + ((lane >> 4) << 3)) * kLdK + kk + ((lane >> 3) & 1) * 8);
+                else
+                    ldsm_x4_t(r, bs + (kk + (lane & 7) + (((lane >> 3) & 1) << 3)) * kLdMN + nb + ((lane >> 4) << 3));
+                b[2 * j][0] = r[0];
+                b[2 * j][1] = r[1];
+                b[2 * j + 1][0] = r[2];
+                b[2 * j + 1][1] = r[3];
+            }
+#pragma unroll
+            for (int i = 0; i < 2; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) mma_bf16(acc[i][j], a[i], b[j]);
+        }
+    }
+    // epilogue
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int row = m0 + wm + 16 * i + (lane >> 2) + (q >= 2 ? 8 : 0);
+                const int col = n0 + wn + 8 * j + 2 * (lane & 3) + (q & 1);
+                if (row >= g.M || col >= g.N) continue;
+                if (gridDim.z > 1)
+                    g.partial[((size_t)blockIdx.z * g.M + row) * g.N + col] = acc[i][j][q];
+                else
+                    store(g, row, col, epilogue(g, row, col, acc[i][j][q]));
+            }
+}
+
+// Split-K: partial sums added in split order, then the epilogue.
+__global__ void splitk_reduce_kernel(const GemmArgs g, int splits) {
+    const size_t n = (size_t)g.M * g.N;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        float s = 0.0f;
+        for (int z = 0; z < splits; ++z) s += g.partial[(size_t)z * n + i];
+        const int row = (int)(i / g.N), col = (int)(i % g.N);
+        store(g, row, col, epilogue(g, row, col, s));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Small kernels
+
+// One-hot classes, 8 channels per voxel.
+__global__ void onehot_kernel(const uint8_t* __restrict__ cls, uint32_t n_vox, bf16* __restrict__ x) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_vox; i += gridDim.x * blockDim.x) {
+        const uint32_t c = cls[i];
+#pragma unroll
+        for (uint32_t k = 0; k < 8; ++k) x[(size_t)i * 8 + k] = __float2bfloat16_rn(c == k && c < 5 ? 1.0f : 0.0f);
+    }
+}
+
+// y[b] = b6 + sum_j h2[b, j] w6[j]: lane l adds j = l, l+32, l+64, l+96 in
+// order, then an xor butterfly.
+__global__ void head_kernel(const bf16* __restrict__ h2, const bf16* __restrict__ w6, const float* __restrict__ b6,
+                            uint32_t n, float* __restrict__ y) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t b = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+    if (b >= n) return;
+    float s = 0.0f;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const uint32_t j = lane + 32 * i;
+        s = fmaf(__bfloat162float(h2[(size_t)b * 128 + j]), __bfloat162float(w6[j]), s);
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) y[b] = s + b6[0];
+}
+
+// Loss and the gradients of the head: dy = 2 (y - t) / n; dW6[j] = sum_b dy
+// h2[b, j] (thread j, samples in order); db6 = sum_b dy; dz2 = dy w6 where
+// h2 > 0.  One block of 128 threads.
+__global__ void head_backward_kernel(const float* __restrict__ y, const float* __restrict__ t,
+                                     const bf16* __restrict__ h2, const bf16* __restrict__ w6, uint32_t n,
+                                     float* __restrict__ dw6, float* __restrict__ db6, bf16* __restrict__ dz2,
+                                     float* __restrict__ loss) {
+    const uint32_t j = threadIdx.x;
+    const float inv = 1.0f / (float)n;
+    float g = 0.0f;
+    for (uint32_t b = 0; b < n; ++b) {
+        const float dy = 2.0f * (y[b] - t[b]) * inv;
+        const float hv = __bfloat162float(h2[(size_t)b * 128 + j]);
+        g = fmaf(dy, hv, g);
+        dz2[(size_t)b * 128 + j] = __float2bfloat16_rn(hv > 0.0f ? dy * __bfloat162float(w6[j]) : 0.0f);
+    }
+    dw6[j] = g;
+    if (j == 0) {
+        float s = 0.0f, l = 0.0f;
+        for (uint32_t b = 0; b < n; ++b) {
+            const float e = y[b] - t[b];
+            s += 2.0f * e * inv;
+            l = fmaf(e, e, l);
+        }
+        db6[0] = s;
+        loss[0] = l * inv;
+    }
+}
+
+// Column sums of a bf16 [rows][cols] matrix, one block per column, fixed
+// order: thread t adds rows t, t+256, ...; then a tree over the block.
+__global__ void colsum_kernel(const bf16* __restrict__ a, uint32_t rows, uint32_t cols, float* __restrict__ out) {
+    __shared__ float red[256];
+    const uint32_t c = blockIdx.x, t = threadIdx.x;
+    float s = 0.0f;
+    for (uint32_t r = t; r < rows; r += 256) s += __bfloat162float(a[(size_t)r * cols + c]);
+    red[t] = s;
+    __syncthreads();
+    for (uint32_t o = 128; o; o >>= 1) {
+        if (t < o) red[t] += red[t + o];
+        __syncthreads();
+    }
+    if (t == 0) out[c] = red[0];
+}
+
+// wt[(o*32 + co) * cin + ci] = w[co * 27*cin + o*cin + ci]: the weights of
+// the input-gradient convolution as a K x N (MN-major) operand.
+__global__ void conv_weight_t_kernel(const bf16* __restrict__ w, uint32_t cin, bf16* __restrict__ wt) {
+    const uint32_t n = 27 * 32 * cin;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t ci = i % cin, k = i / cin, o = k / 32, co = k % 32;
+        wt[i] = w[(size_t)co * 27 * cin + o * cin + ci];
+    }
+}
+
+// Adam on the FP32 master weights, then their BF16 copies.
+__global__ void adam_kernel(float* __restrict__ w, float* __restrict__ m, float* __restrict__ v,
+                            const float* __restrict__ g, bf16* __restrict__ wb, uint32_t n, float lr, float b1,
+                            float b2, float eps, float c1, float c2) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float gi = g[i];
+        const float mi = b1 * m[i] + (1.0f - b1) * gi;
+        const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        const float wi = w[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+        w[i] = wi;
+        wb[i] = __float2bfloat16_rn(wi);
+    }
+}
+
+__global__ void to_bf16_kernel(const float* __restrict__ w, bf16* __restrict__ wb, uint32_t n) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        wb[i] = __float2bfloat16_rn(w[i]);
+}
+
+template <int AV, int BV>
+cudaError_t gemm(GemmArgs g, int splits, cudaStream_t s) {
+    if (g.M <= 0 || g.N <= 0) return cudaSuccess;
+    splits = std::max(1, std::min<int>(splits, (int)(g.partial_cap / ((size_t)g.M * g.N))));
+    g.k_chunk = ((g.K + splits - 1) / splits + kTileK - 1) / kTileK * kTileK;
+    splits = std::max(1, (g.K + g.k_chunk - 1) / g.k_chunk);
+    const dim3 grid((g.N + kTileN - 1) / kTileN, (g.M + kTileM - 1) / kTileM, splits);
+    gemm_kernel<AV, BV><<<grid, kGemmThreads, 0, s>>>(g);
+    if (splits > 1) {
+        const size_t n = (size_t)g.M * g.N;
+        splitk_reduce_kernel<<<(unsigned)std::min<size_t>((n + 255) / 256, 4096), 256, 0, s>>>(g, splits);
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace
+}  // namespace sg
+}  // namespace mb
+
+// ---------------------------------------------------------------------------
+// Host driver
+
+namespace {
+
+using bf16 = __nv_bfloat16;
+using namespace mb::sg;
+
+// Flat parameter layout: tensors in order, each padded to 8 elements.
+enum Tensor { kW1, kB1, kW2, kB2, kW3, kB3, kW4, kB4, kW5, kB5, kW6, kB6, kTensors };
+constexpr uint32_t kSize[kTensors] = {32 * 27 * 8, 32, 32 * 27 * 32, 32, 32 * 27 * 32, 32,
+                                      128 * 6912, 128, 128 * 128, 128, 128, 1};
+constexpr uint32_t kFanIn[kTensors] = {27 * 5, 0, 27 * 32, 0, 27 * 32, 0, 6912, 0, 128, 0, 128, 0};
+
+struct Layout {
+    uint32_t off[kTensors + 1];
+    Layout() {
+        uint32_t o = 0;
+        for (int i = 0; i < kTensors; ++i) {
+            off[i] = o;
+            o += (kSize[i] + 7) / 8 * 8;
+        }
+        off[kTensors] = o;
+    }
+};
+const Layout kLayout;
+
+template <typename T>
+struct Buf {
+    T* p = nullptr;
+    ~Buf() {
+        if (p) cudaFree(p);
+    }
+    cudaError_t alloc(size_t n) {
+        if (p) cudaFree(p);
+        p = nullptr;
+        return cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T));
+    }
+};
+
+uint64_t mix64(uint64_t z) {
+    z ^= z >> 30;
+    z *= 0xbf58476d1ce4e5b9ULL;
+    z ^= z >> 27;
+    z *= 0x94d049bb133111ebULL;
+    return z ^ (z >> 31);
+}
+
+}  // namespace
+
+struct mb_surrogate {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    uint32_t max_batch = 0;
+    std::string err;
+    uint64_t step = 0;
+    Buf<float> w, m, v, g, loss, y, t, partial;
+    Buf<bf16> wb, wt2, wt3, x0, a1, a2, a3, h1, h2, dz2h, dz1h, dz3, dz2c, dz1c;
+    Buf<uint8_t> cls;
+    ~mb_surrogate() {
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+namespace {
+
+mb_status sfail(mb_surrogate* s, mb_status st, const char* msg) {
+    if (s) s->err = msg;
+    return st;
+}
+
+#define SG_CUDA(s, call)                                                                  \
+    do {                                                                                  \
+        cudaError_t _e = (call);                                                          \
+        if (_e != cudaSuccess) {                                                          \
+            if (s) s->err = std::string(#call) + ": " + cudaGetErrorString(_e);           \
+            return MB_ERR_CUDA;                                                           \
+        }                                                                                 \
+    } while (0)
+
+const float* P(const mb_surrogate* s, Tensor i) { return s->w.p + kLayout.off[i]; }
+const bf16* PB(const mb_surrogate* s, Tensor i) { return s->wb.p + kLayout.off[i]; }
+float* G(mb_surrogate* s, Tensor i) { return s->g.p + kLayout.off[i]; }
+
+constexpr size_t kPartialFloats = 64 * 32 * 27 * 32;
+
+GemmArgs args(mb_surrogate* s, const bf16* A, int lda, const bf16* B, int ldb, int M, int N, int K) {
+    GemmArgs a{};
+    a.partial = s->partial.p;
+    a.partial_cap = kPartialFloats;
+    a.A = A;
+    a.B = B;
+    a.M = M;
+    a.N = N;
+    a.K = K;
+    a.lda = lda;
+    a.ldb = ldb;
+    a.ldc = N;
+    return a;
+}
+
+// Forward of n samples already one-hot in s->x0; leaves a1..a3, h1, h2, y.
+cudaError_t forward(mb_surrogate* s, uint32_t n) {
+    cudaStream_t st = s->stream;
+    const int R = (int)n * kVox;
+    cudaError_t e;
+    {
+        GemmArgs a = args(s, s->x0.p, 8, PB(s, kW1), 27 * 8, R, 32, 27 * 8);
+        a.bias = P(s, kB1);
+        a.relu = 1;
+        a.c16 = s->a1.p;
+        if ((e = gemm<kIm2col, kDenseK>(a, 1, st)) != cudaSuccess) return e;
+    }
+    {
+        GemmArgs a = args(s, s->a1.p, 32, PB(s, kW2), 27 * 32, R, 32, 27 * 32);
+        a.bias = P(s, kB2);
+        a.relu = 1;
+        a.c16 = s->a2.p;
+        if ((e = gemm<kIm2col, kDenseK>(a, 1, st)) != cudaSuccess) return e;
+    }
+    {
+        GemmArgs a = args(s, s->a2.p, 32, PB(s, kW3), 27 * 32, R, 32, 27 * 32);
+        a.bias = P(s, kB3);
+        a.relu = 1;
+        a.c16 = s->a3.p;
+        if ((e = gemm<kIm2col, kDenseK>(a, 1, st)) != cudaSuccess) return e;
+    }
+    {
+        GemmArgs a = args(s, s->a3.p, 6912, PB(s, kW4), 6912, (int)n, 128, 6912);
+        a.bias = P(s, kB4);
+        a.relu = 1;
+        a.c16 = s->h1.p;
+        if ((e = gemm<kDenseK, kDenseK>(a, 1, st)) != cudaSuccess) return e;
+    }
+    {
+        GemmArgs a = args(s, s->h1.p, 128, PB(s, kW5), 128, (int)n, 128, 128);
+        a.bias = P(s, kB5);
+        a.relu = 1;
+        a.c16 = s->h2.p;
+        if ((e = gemm<kDenseK, kDenseK>(a, 1, st)) != cudaSuccess) return e;
+    }
+    head_kernel<<<(n + 7) / 8, 256, 0, st>>>(s->h2.p, PB(s, kW6), P(s, kB6), n, s->y.p);
+    return cudaGetLastError();
+}
+
+int splits_for(int K) { return std::max(1, std::min(64, K / 1024)); }
+
+// Backward of the last forward against targets s->t; gradients into s->g.
+cudaError_t backward(mb_surrogate* s, uint32_t n) {
+    cudaStream_t st = s->stream;
+    const int R = (int)n * kVox;
+    cudaError_t e;
+    head_backward_kernel<<<1, 128, 0, st>>>(s->y.p, s->t.p, s->h2.p, PB(s, kW6), n, G(s, kW6), G(s, kB6),
+                                            s->dz2h.p, s->loss.p);
+    // fc2: dW5 = dz2^T h1, db5, dz1 = (dz2 W5) where h1 > 0
+    {
+        GemmArgs a = args(s, s->dz2h.p, 128, s->h1.p, 128, 128, 128, (int)n);
+        a.c32 = G(s, kW5);
+        if ((e = gemm<kDenseMN, kDenseMN>(a, splits_for((int)n), st)) != cudaSuccess) return e;
+    }
+    colsum_kernel<<<128, 256, 0, st>>>(s->dz2h.p, n, 128, G(s, kB5));
+    {
+        GemmArgs a = args(s, s->dz2h.p, 128, PB(s, kW5), 128, (int)n, 128, 128);
+        a.mask = s->h1.p;
+        a.c16 = s->dz1h.p;
+        if ((e = gemm<kDenseK, kDenseMN>(a, 1, st)) != cudaSuccess) return e;
+    }
+    // fc1: dW4 = dz1^T flatten(a3), db4, dz3 = (dz1 W4) where a3 > 0
+    {
+        GemmArgs a = args(s, s->dz1h.p, 128, s->a3.p, 6912, 128, 6912, (int)n);
+        a.c32 = G(s, kW4);
+        if ((e = gemm<kDenseMN, kDenseMN>(a, splits_for((int)n), st)) != cudaSuccess) return e;
+    }
+    colsum_kernel<<<128, 256, 0, st>>>(s->dz1h.p, n, 128, G(s, kB4));
+    {
+        GemmArgs a = args(s, s->dz1h.p, 128, PB(s, kW4), 6912, (int)n, 6912, 128);
+        a.mask = s->a3.p;
+        a.c16 = s->dz3.p;
+        if ((e = gemm<kDenseK, kDenseMN>(a, 1, st)) != cudaSuccess) return e;
+    }
+    // conv3: dW3 = dz3^T im2col(a2), db3, dz2 = conv^T(dz3; W3) where a2 > 0
+    {
+        GemmArgs a = args(s, s->dz3.p, 32, s->a2.p, 32, 32, 27 * 32, R);
+        a.c32 = G(s, kW3);
+        if ((e = gemm<kDenseMN, kIm2col>(a, splits_for(R), st)) != cudaSuccess) return e;
+    }
+    colsum_kernel<<<32, 256, 0, st>>>(s->dz3.p, (uint32_t)R, 32, G(s, kB3));
+    conv_weight_t_kernel<<<108, 256, 0, st>>>(PB(s, kW3), 32, s->wt3.p);
+    {
+        GemmArgs a = args(s, s->dz3.p, 32, s->wt3.p, 32, R, 32, 27 * 32);
+        a.flip_a = 1;
+        a.mask = s->a2.p;
+        a.c16 = s->dz2c.p;
+        if ((e = gemm<kIm2col, kDenseMN>(a, 1, st)) != cudaSuccess) return e;
+    }
+    // conv2
+    {
+        GemmArgs a = args(s, s->dz2c.p, 32, s->a1.p, 32, 32, 27 * 32, R);
+        a.c32 = G(s, kW2);
+        if ((e = gemm<kDenseMN, kIm2col>(a, splits_for(R), st)) != cudaSuccess) return e;
+    }
+    colsum_kernel<<<32, 256, 0, st>>>(s->dz2c.p, (uint32_t)R, 32, G(s, kB2));
+    conv_weight_t_kernel<<<108, 256, 0, st>>>(PB(s, kW2), 32, s->wt2.p);
+    {
+        GemmArgs a = args(s, s->dz2c.p, 32, s->wt2.p, 32, R, 32, 27 * 32);
+        a.flip_a = 1;
+        a.mask = s->a1.p;
+        a.c16 = s->dz1c.p;
+        if ((e = gemm<kIm2col, kDenseMN>(a, 1, st)) != cudaSuccess) return e;
+    }
+    // conv1: dW1 = dz1^T im2col(x0), db1
+    {
+        GemmArgs a = args(s, s->dz1c.p, 32, s->x0.p, 8, 32, 27 * 8, R);
+        a.c32 = G(s, kW1);
+        if ((e = gemm<kDenseMN, kIm2col>(a, splits_for(R), st)) != cudaSuccess) return e;
+    }
+    colsum_kernel<<<32, 256, 0, st>>>(s->dz1c.p, (uint32_t)R, 32, G(s, kB1));
+    return cudaGetLastError();
+}
+
+mb_status upload_batch(mb_surrogate* s, const uint8_t* genomes, const float* targets, uint32_t n) {
+    cudaStream_t st = s->stream;
+    SG_CUDA(s, cudaMemcpyAsync(s->cls.p, genomes, (size_t)n * kVox, cudaMemcpyHostToDevice, st));
+    if (targets) SG_CUDA(s, cudaMemcpyAsync(s->t.p, targets, n * sizeof(float), cudaMemcpyHostToDevice, st));
+    onehot_kernel<<<std::min<uint32_t>((n * kVox + 255) / 256, 4096), 256, 0, st>>>(s->cls.p, n * kVox, s->x0.p);
+    SG_CUDA(s, cudaGetLastError());
+    return MB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+uint32_t mb_surrogate_param_count(void) { return kLayout.off[kTensors]; }
+
+void mb_surrogate_layout(uint32_t* offsets) {
+    if (!offsets) return;
+    for (int i = 0; i <= kTensors; ++i) offsets[i] = kLayout.off[i];
+}
+
+mb_status mb_surrogate_create(int device, uint32_t max_batch, uint64_t seed, mb_surrogate** out) {
+    if (!out || max_batch == 0 || max_batch > 65536) return MB_ERR_ARGUMENT;
+    *out = nullptr;
+    std::unique_ptr<mb_surrogate> s(new mb_surrogate());
+    s->device = device;
+    s->max_batch = max_batch;
+    if (cudaSetDevice(device) != cudaSuccess) return MB_ERR_CUDA;
+    if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) return MB_ERR_CUDA;
+    const size_t np = kLayout.off[kTensors], R = (size_t)max_batch * kVox;
+    auto ok = [](cudaError_t e) { return e == cudaSuccess; };
+    if (!(ok(s->w.alloc(np)) && ok(s->m.alloc(np)) && ok(s->v.alloc(np)) && ok(s->g.alloc(np)) &&
+          ok(s->wb.alloc(np)) && ok(s->loss.alloc(1)) && ok(s->y.alloc(max_batch)) && ok(s->t.alloc(max_batch)) &&
+          ok(s->partial.alloc(kPartialFloats)) && ok(s->wt2.alloc(27 * 32 * 32)) &&
+          ok(s->wt3.alloc(27 * 32 * 32)) && ok(s->x0.alloc(R * 8)) && ok(s->a1.alloc(R * 32)) &&
+          ok(s->a2.alloc(R * 32)) && ok(s->a3.alloc(R * 32)) && ok(s->h1.alloc((size_t)max_batch * 128)) &&
+          ok(s->h2.alloc((size_t)max_batch * 128)) && ok(s->dz2h.alloc((size_t)max_batch * 128)) &&
+          ok(s->dz1h.alloc((size_t)max_batch * 128)) && ok(s->dz3.alloc(R * 32)) && ok(s->dz2c.alloc(R * 32)) &&
+          ok(s->dz1c.alloc(R * 32)) && ok(s->cls.alloc(R))))
+        return MB_ERR_CUDA;
+    // He-normal weights (fan-in of the real inputs), zero biases, zero
+    // weights on the padding channels of W1; Box-Muller over SplitMix64.
+    std::vector<float> w(np, 0.0f);
+    uint64_t state = seed;
+    auto uniform = [&]() { return ((mix64(state += 0x9E3779B97F4A7C15ULL) >> 11) + 0.5) * (1.0 / 9007199254740992.0); };
+    for (int t = 0; t < kTensors; ++t) {
+        if (!kFanIn[t]) continue;
+        const double sd = std::sqrt((t == kW6 ? 1.0 : 2.0) / kFanIn[t]);
+        for (uint32_t i = 0; i < kSize[t]; ++i) {
+            if (t == kW1 && i % 8 >= 5) continue;
+            const double u1 = uniform(), u2 = uniform();
+            w[kLayout.off[t] + i] = (float)(sd * std::sqrt(-2.0 * std::log(u1)) * std::cos(6.283185307179586 * u2));
+        }
+    }
+    const mb_status st = mb_surrogate_set_params(s.get(), w.data());
+    if (st != MB_OK) return st;
+    *out = s.release();
+    return MB_OK;
+}
+
+void mb_surrogate_destroy(mb_surrogate* s) {
+    if (!s) return;
+    cudaSetDevice(s->device);
+    cudaStreamSynchronize(s->stream);
+    delete s;
+}
+
+const char* mb_surrogate_last_error(const mb_surrogate* s) { return s ? s->err.c_str() : "null surrogate"; }
+
+mb_status mb_surrogate_set_params(mb_surrogate* s, const float* params) {
+    if (!s || !params) return sfail(s, MB_ERR_ARGUMENT, "null argument");
+    cudaSetDevice(s->device);
+    const size_t np = kLayout.off[kTensors];
+    cudaStream_t st = s->stream;
+    SG_CUDA(s, cudaMemcpyAsync(s->w.p, params, np * sizeof(float), cudaMemcpyHostToDevice, st));
+    SG_CUDA(s, cudaMemsetAsync(s->m.p, 0, np * sizeof(float), st));
+    SG_CUDA(s, cudaMemsetAsync(s->v.p, 0, np * sizeof(float), st));
+    to_bf16_kernel<<<1024, 256, 0, st>>>(s->w.p, s->wb.p, (uint32_t)np);
+    SG_CUDA(s, cudaGetLastError());
+    SG_CUDA(s, cudaStreamSynchronize(st));
+    s->step = 0;
+    return MB_OK;
+}
+
+mb_status mb_surrogate_get_params(mb_surrogate* s, float* params) {
+    if (!s || !params) return sfail(s, MB_ERR_ARGUMENT, "null argument");
+    cudaSetDevice(s->device);
+    SG_CUDA(s, cudaMemcpyAsync(params, s->w.p, kLayout.off[kTensors] * sizeof(float), cudaMemcpyDeviceToHost,
+                               s->stream));
+    SG_CUDA(s, cudaStreamSynchronize(s->stream));
+    return MB_OK;
+}
+
+mb_status mb_surrogate_predict(mb_surrogate* s, const uint8_t* genomes, uint32_t n, float* out) {
+    if (!s || !genomes || !out) return sfail(s, MB_ERR_ARGUMENT, "null argument");
+    cudaSetDevice(s->device);
+    for (uint32_t b0 = 0; b0 < n; b0 += s->max_batch) {
+        const uint32_t nb = std::min(s->max_batch, n - b0);
+        const mb_status st = upload_batch(s, genomes + (size_t)b0 * kVox, nullptr, nb);
+        if (st != MB_OK) return st;
+        SG_CUDA(s, forward(s, nb));
+        SG_CUDA(s, cudaMemcpyAsync(out + b0, s->y.p, nb * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
+    }
+    SG_CUDA(s, cudaStreamSynchronize(s->stream));
+    return MB_OK;
+}
+
+mb_status mb_surrogate_gradients(mb_surrogate* s, const uint8_t* genomes, const float* targets, uint32_t n,
+                                 float* grads, float* loss) {
+    if (!s || !genomes || !targets) return sfail(s, MB_ERR_ARGUMENT, "null argument");
+    if (n == 0 || n > s->max_batch) return sfail(s, MB_ERR_ARGUMENT, "batch must be 1..max_batch");
+    cudaSetDevice(s->device);
+    mb_status st = upload_batch(s, genomes, targets, n);
+    if (st != MB_OK) return st;
+    SG_CUDA(s, cudaMemsetAsync(s->g.p, 0, kLayout.off[kTensors] * sizeof(float), s->stream));
+    SG_CUDA(s, forward(s, n));
+    SG_CUDA(s, backward(s, n));
+    if (grads)
+        SG_CUDA(s, cudaMemcpyAsync(grads, s->g.p, kLayout.off[kTensors] * sizeof(float), cudaMemcpyDeviceToHost,
+                                   s->stream));
+    if (loss) SG_CUDA(s, cudaMemcpyAsync(loss, s->loss.p, sizeof(float), cudaMemcpyDeviceToHost, s->stream));
+    SG_CUDA(s, cudaStreamSynchronize(s->stream));
+    return MB_OK;
+}
+
+mb_status mb_surrogate_train_step(mb_surrogate* s, const uint8_t* genomes, const float* targets, uint32_t n,
+                                  float lr, float* loss) {
+    const mb_status st = mb_surrogate_gradients(s, genomes, targets, n, nullptr, loss);
+    if (st != MB_OK) return st;
+    const float b1 = 0.9f, b2 = 0.999f;
+    ++s->step;
+    const float c1 = 1.0f - std::pow(b1, (float)s->step), c2 = 1.0f - std::pow(b2, (float)s->step);
+    adam_kernel<<<1024, 256, 0, s->stream>>>(s->w.p, s->m.p, s->v.p, s->g.p, s->wb.p, kLayout.off[kTensors], lr, b1,
+                                             b2, 1e-8f, c1, c2);
+    SG_CUDA(s, cudaGetLastError());
+    SG_CUDA(s, cudaStreamSynchronize(s->stream));
+    return MB_OK;
+}
+
+}  // extern "C"
