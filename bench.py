@@ -398,10 +398,47 @@ def secondary(args, batch, local_rank, dev, hbm_peak):
                                     "bytes_per_update": hbm_b}}
     del ss
     out["devo"] = devo_bench(local_rank)
+    out["surrogate"] = surrogate_bench(local_rank)
     return out
 
 
 DEVO_ROBOTS, DEVO_K = 512, 128
+SG_CHILDREN, SG_WARMUP_BATCHES = 4096, 13
+
+
+def surrogate_bench(local_rank, generations: int = 5, plain_generations: int = 3, seed: int = 0):
+    """Surrogate-screened evolution (4096 children of 6x6x6 voxel genomes
+    per generation; the surrogate's top 25% plus a 5% random audit are
+    simulated for 1 s on land) against plain evolution (all 4096
+    simulated), after a warm-up of 13 x 4096 = 53,248 simulated random
+    genomes.  Generations/s from host wall time per generation (children,
+    screening, device builds, simulation, online training); the screen's
+    quality from every child of the screened generations also simulated,
+    outside the timed region."""
+    import copy
+    from mercury_b200 import evolve
+    from mercury_b200.surrogate import Surrogate
+    ev = evolve.Evaluator(local_rank)
+    sg = Surrogate(local_rank, max_batch=1024, seed=seed)
+    scr = evolve.ScreenedEvolution(ev, sg, seed=seed + 1, children=SG_CHILDREN)
+    warm = scr.warmup(SG_WARMUP_BATCHES * SG_CHILDREN, batch=SG_CHILDREN)
+    plain = evolve.PlainEvolution(ev, seed=seed + 2, children=SG_CHILDREN, pool=copy.deepcopy(scr.pool))
+    gens = [scr.generation(truth=True) for _ in range(generations)]
+    pgens = [plain.generation() for _ in range(plain_generations)]
+    t_s = float(np.mean([g["wall_s"] for g in gens]))
+    t_p = float(np.mean([g["wall_s"] for g in pgens]))
+    q = {k: float(np.mean([g[k] for g in gens])) for k in ("spearman", "top10_recall", "top10_recall_top10",
+                                                          "random_screen_recall")}
+    return {"metric": "generations/s", "screened": 1.0 / t_s, "plain": 1.0 / t_p, "speedup": t_p / t_s,
+            "unit": "generations/s", **q,
+            "per_generation": [{k: round(v, 4) for k, v in g.items()} for g in gens],
+            "plain_per_generation": [{k: round(v, 4) for k, v in g.items()} for g in pgens],
+            "best_fitness": {"screened": gens[-1]["best"], "plain": pgens[-1]["best"]},
+            "warmup": warm, "simulated_per_generation": {"screened": gens[0]["simulated"],
+                                                         "plain": pgens[0]["simulated"]},
+            "workload": f"{SG_CHILDREN} children of 6x6x6 voxel genomes per generation, 1 s on land "
+                        f"(dt 1e-4, 10,000 steps), screen 25% + 5% audit; warm-up "
+                        f"{SG_WARMUP_BATCHES * SG_CHILDREN} random genomes"}
 
 
 def devo_population():

@@ -347,7 +347,9 @@ MB_API mb_status mb_surrogate_predict(mb_surrogate* s, const uint8_t* genomes, u
  * one batch of n <= max_batch genomes, without an update. */
 MB_API mb_status mb_surrogate_gradients(mb_surrogate* s, const uint8_t* genomes, const float* targets, uint32_t n,
                                         float* grads, float* loss);
-/* One Adam step (beta 0.9 / 0.999, eps 1e-8) at learning rate lr. */
+/* One Adam step (beta 0.9 / 0.999, eps 1e-8) at learning rate lr, with
+ * decoupled weight decay (AdamW) when set. */
+MB_API mb_status mb_surrogate_set_weight_decay(mb_surrogate* s, float weight_decay);
 MB_API mb_status mb_surrogate_train_step(mb_surrogate* s, const uint8_t* genomes, const float* targets, uint32_t n,
                                          float lr, float* loss);
 

@@ -126,6 +126,7 @@ def _load() -> ctypes.CDLL:
         "mb_surrogate_predict": (I32, [P, P, U32, P]),
         "mb_surrogate_gradients": (I32, [P, P, P, U32, P, P]),
         "mb_surrogate_train_step": (I32, [P, P, P, U32, F32, P]),
+        "mb_surrogate_set_weight_decay": (I32, [P, F32]),
         "mb_version": (ctypes.c_char_p, []),
     }
     for name, (res, args) in sigs.items():

@@ -284,14 +284,14 @@ __global__ void conv_weight_t_kernel(const bf16* __restrict__ w, uint32_t cin, b
 // Adam on the FP32 master weights, then their BF16 copies.
 __global__ void adam_kernel(float* __restrict__ w, float* __restrict__ m, float* __restrict__ v,
                             const float* __restrict__ g, bf16* __restrict__ wb, uint32_t n, float lr, float b1,
-                            float b2, float eps, float c1, float c2) {
+                            float b2, float eps, float c1, float c2, float wd) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const float gi = g[i];
         const float mi = b1 * m[i] + (1.0f - b1) * gi;
         const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
         m[i] = mi;
         v[i] = vi;
-        const float wi = w[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+        const float wi = w[i] - lr * ((mi / c1) / (sqrtf(vi / c2) + eps) + wd * w[i]);
         w[i] = wi;
         wb[i] = __float2bfloat16_rn(wi);
     }
@@ -377,6 +377,7 @@ struct mb_surrogate {
     uint32_t max_batch = 0;
     std::string err;
     uint64_t step = 0;
+    float weight_decay = 0.0f;
     Buf<float> w, m, v, g, loss, y, t, partial;
     Buf<bf16> wb, wt2, wt3, x0, a1, a2, a3, h1, h2, dz2h, dz1h, dz3, dz2c, dz1c;
     Buf<uint8_t> cls;
@@ -624,6 +625,12 @@ mb_status mb_surrogate_set_params(mb_surrogate* s, const float* params) {
     return MB_OK;
 }
 
+mb_status mb_surrogate_set_weight_decay(mb_surrogate* s, float weight_decay) {
+    if (!s || !(weight_decay >= 0.0f)) return sfail(s, MB_ERR_ARGUMENT, "weight decay must be >= 0");
+    s->weight_decay = weight_decay;
+    return MB_OK;
+}
+
 mb_status mb_surrogate_get_params(mb_surrogate* s, float* params) {
     if (!s || !params) return sfail(s, MB_ERR_ARGUMENT, "null argument");
     cudaSetDevice(s->device);
@@ -673,7 +680,7 @@ mb_status mb_surrogate_train_step(mb_surrogate* s, const uint8_t* genomes, const
     ++s->step;
     const float c1 = 1.0f - std::pow(b1, (float)s->step), c2 = 1.0f - std::pow(b2, (float)s->step);
     adam_kernel<<<1024, 256, 0, s->stream>>>(s->w.p, s->m.p, s->v.p, s->g.p, s->wb.p, kLayout.off[kTensors], lr, b1,
-                                             b2, 1e-8f, c1, c2);
+                                             b2, 1e-8f, c1, c2, s->weight_decay);
     SG_CUDA(s, cudaGetLastError());
     SG_CUDA(s, cudaStreamSynchronize(s->stream));
     return MB_OK;

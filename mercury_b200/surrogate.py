@@ -82,6 +82,10 @@ class Surrogate:
                                                     _lib.ptr(loss)))
         return float(loss[0]), grads
 
+    def set_weight_decay(self, wd: float) -> None:
+        """Decoupled weight decay of the Adam steps (AdamW)."""
+        self._check(_lib.LIB.mb_surrogate_set_weight_decay(self._s, float(wd)))
+
     def train_step(self, genomes: np.ndarray, targets: np.ndarray, lr: float = 1e-3) -> float:
         g = self._g(genomes)
         t = np.ascontiguousarray(targets, np.float32)
