@@ -406,7 +406,7 @@ DEVO_ROBOTS, DEVO_K = 512, 128
 SG_CHILDREN, SG_WARMUP_BATCHES = 4096, 13
 
 
-def surrogate_bench(local_rank, generations: int = 5, plain_generations: int = 3, seed: int = 0):
+def surrogate_bench(local_rank, generations: int = 8, plain_generations: int = 3, seed: int = 0):
     """Surrogate-screened evolution (4096 children of 6x6x6 voxel genomes
     per generation; the surrogate's top 25% plus a 5% random audit are
     simulated for 1 s on land) against plain evolution (all 4096

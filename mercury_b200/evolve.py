@@ -18,7 +18,10 @@ evaluated, and the pool keeps the best simulated genomes.
 Screened: the surrogate predicts all children (the mean over the 8
 horizontal orientations of each), its top `screen` fraction plus a random
 `audit` fraction of the rest are simulated, and the surrogate trains on the
-new (genome, fitness) pairs; the others are discarded unsimulated.  Training
+new (genome, fitness) pairs; the others are discarded unsimulated.  A
+child differs from its (simulated) parents in a few voxels, so each
+prediction is corrected by the surrogate's error on the parents, weighted
+by the share of voxels from each (lineage correction).  Training
 draws every sample in a random orientation: after a warm-up of random
 genomes, 60 epochs with a cosine learning rate; per generation, a few
 steps whose batches are half from the newest generation.
@@ -102,16 +105,20 @@ class Evaluator:
 
 
 def make_children(rng: np.random.Generator, parents: np.ndarray, fitness: np.ndarray, n: int,
-                  p_cross: float = 0.7, p_mut: float = 0.6) -> np.ndarray:
+                  p_cross: float = 0.7, p_mut: float = 0.6, lineage: bool = False):
     """Children of rank-selected parents: axis-aligned cut crossover, then
-    redraws of about 1 + Poisson(2) voxels."""
+    redraws of about 1 + Poisson(2) voxels.  With `lineage`, also returns
+    each child's parents (indices into `parents`) and the share of its
+    voxels taken from the second one."""
     order = np.argsort(-fitness, kind="stable")
     P = len(parents)
     w = 1.0 / (1.0 + np.arange(P))  # rank weights
     w /= w.sum()
-    a = parents[order[rng.choice(P, size=n, p=w)]]
-    b = parents[order[rng.choice(P, size=n, p=w)]]
+    ia = order[rng.choice(P, size=n, p=w)]
+    ib = order[rng.choice(P, size=n, p=w)]
+    a, b = parents[ia], parents[ib]
     kids = a.copy()
+    share_b = np.zeros(n)
     cross = rng.random(n) < p_cross
     if cross.any():
         coord = np.stack(np.meshgrid(np.arange(6), np.arange(6), np.arange(6), indexing="ij"), -1)
@@ -121,6 +128,7 @@ def make_children(rng: np.random.Generator, parents: np.ndarray, fitness: np.nda
         side = coord[:, axis].T  # (n, 216): each child's coordinate along its cut axis
         take_b = (side >= cut[:, None]) & cross[:, None]
         kids[take_b] = b[take_b]
+        share_b = take_b.mean(1)
     mut = rng.random(n) < p_mut
     m = int(mut.sum())
     if m:
@@ -131,6 +139,8 @@ def make_children(rng: np.random.Generator, parents: np.ndarray, fitness: np.nda
         rows = kids[mut]
         rows[mask] = rng.choice(5, size=int(mask.sum()), p=P_CLASS)
         kids[mut] = rows
+    if lineage:
+        return kids, ia, ib, share_b
     return kids
 
 
@@ -175,11 +185,12 @@ class ScreenedEvolution:
 
     def __init__(self, evaluator: Evaluator, surrogate: Surrogate, seed: int = 0, children: int = 4096,
                  screen: float = 0.25, audit: float = 0.05, batch: int = 256, lr: float = 1e-3,
-                 steps_per_generation: int = 60, finetune_lr: float = 3e-4):
+                 steps_per_generation: int = 60, finetune_lr: float = 3e-4, lineage_correction: bool = True):
         self.ev, self.sg = evaluator, surrogate
         self.rng = np.random.default_rng(seed)
         self.children, self.screen, self.audit = children, screen, audit
         self.batch, self.lr, self.steps, self.finetune_lr = batch, lr, steps_per_generation, finetune_lr
+        self.lineage_correction = lineage_correction
         self.data = Dataset()
         self.pool = Pool()
         self.mu, self.sd = 0.0, 1.0
@@ -232,8 +243,14 @@ class ScreenedEvolution:
 
     def generation(self, truth: bool = False) -> dict:
         t0 = time.perf_counter()
-        kids = make_children(self.rng, self.pool.genomes, self.pool.fitness, self.children)
+        kids, ia, ib, sb = make_children(self.rng, self.pool.genomes, self.pool.fitness, self.children,
+                                         lineage=True)
         pred = self.predict(kids)
+        if self.lineage_correction:
+            # a child is a near copy of simulated parents: carry over the
+            # surrogate's error on them
+            res = self.pool.fitness - self.predict(self.pool.genomes) * self.sd - self.mu
+            pred = pred * self.sd + self.mu + (1.0 - sb) * res[ia] + sb * res[ib]
         sel = self.select(pred)
         f = self.ev(kids[sel])
         self.data.add(kids[sel], f)
