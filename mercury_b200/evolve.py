@@ -245,6 +245,7 @@ class ScreenedEvolution:
         t0 = time.perf_counter()
         kids, ia, ib, sb = make_children(self.rng, self.pool.genomes, self.pool.fitness, self.children,
                                          lineage=True)
+        t1 = time.perf_counter()
         pred = self.predict(kids)
         if self.lineage_correction:
             # a child is a near copy of simulated parents: carry over the
@@ -252,12 +253,15 @@ class ScreenedEvolution:
             res = self.pool.fitness - self.predict(self.pool.genomes) * self.sd - self.mu
             pred = pred * self.sd + self.mu + (1.0 - sb) * res[ia] + sb * res[ib]
         sel = self.select(pred)
+        t2 = time.perf_counter()
         f = self.ev(kids[sel])
+        t3 = time.perf_counter()
         self.data.add(kids[sel], f)
         self.pool.add(kids[sel], f)
         self.train(self.steps, self.finetune_lr, recent=(kids[sel], f))
-        wall = time.perf_counter() - t0
-        out = {"wall_s": wall, "simulated": len(sel), "best": float(self.pool.fitness[0])}
+        t4 = time.perf_counter()
+        out = {"wall_s": t4 - t0, "children_s": t1 - t0, "screen_s": t2 - t1, "simulate_s": t3 - t2,
+               "train_s": t4 - t3, "simulated": len(sel), "best": float(self.pool.fitness[0])}
         if truth:  # ground truth for every child, outside the timed region
             ft = self.ev(kids)
             out.update(quality(pred, ft, sel, self.screen))
@@ -274,9 +278,12 @@ class PlainEvolution:
     def generation(self) -> dict:
         t0 = time.perf_counter()
         kids = make_children(self.rng, self.pool.genomes, self.pool.fitness, self.children)
+        t1 = time.perf_counter()
         f = self.ev(kids)
+        t2 = time.perf_counter()
         self.pool.add(kids, f)
-        return {"wall_s": time.perf_counter() - t0, "simulated": len(kids), "best": float(self.pool.fitness[0])}
+        return {"wall_s": time.perf_counter() - t0, "children_s": t1 - t0, "simulate_s": t2 - t1,
+                "simulated": len(kids), "best": float(self.pool.fitness[0])}
 
 
 def quality(pred: np.ndarray, truth: np.ndarray, selected: np.ndarray, screen: float) -> dict:
