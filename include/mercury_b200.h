@@ -350,6 +350,10 @@ MB_API mb_status mb_surrogate_gradients(mb_surrogate* s, const uint8_t* genomes,
 /* One Adam step (beta 0.9 / 0.999, eps 1e-8) at learning rate lr, with
  * decoupled weight decay (AdamW) when set. */
 MB_API mb_status mb_surrogate_set_weight_decay(mb_surrogate* s, float weight_decay);
+/* Forward products on tcgen05 (5th-generation tensor cores, TMEM
+ * accumulators; the default) or, with on = 0, on the mma.sync kernel that
+ * also does the backward products. */
+MB_API mb_status mb_surrogate_use_tcgen05(mb_surrogate* s, int on);
 MB_API mb_status mb_surrogate_train_step(mb_surrogate* s, const uint8_t* genomes, const float* targets, uint32_t n,
                                          float lr, float* loss);
 

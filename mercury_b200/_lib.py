@@ -127,6 +127,7 @@ def _load() -> ctypes.CDLL:
         "mb_surrogate_gradients": (I32, [P, P, P, U32, P, P]),
         "mb_surrogate_train_step": (I32, [P, P, P, U32, F32, P]),
         "mb_surrogate_set_weight_decay": (I32, [P, F32]),
+        "mb_surrogate_use_tcgen05": (I32, [P, I32]),
         "mb_version": (ctypes.c_char_p, []),
     }
     for name, (res, args) in sigs.items():

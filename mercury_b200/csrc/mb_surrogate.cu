@@ -185,6 +185,183 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_kernel(const GemmArgs g) {
             }
 }
 
+// ---------------------------------------------------------------------------
+// tcgen05 GEMM (5th-generation tensor cores, accumulator in tensor memory)
+// for the forward products: C[M,N] = A[M,K] B[N,K]^T with A dense K-major or
+// an im2col view, B dense K-major (weights).  One warpgroup per 128 x BN
+// tile.  Operands are staged by cp.async into the K-major, no-swizzle
+// canonical layout of the UMMA shared-memory descriptor: 8-row x 16-byte
+// core matrices, core matrix (row group g, 8-element k chunk c) at byte
+// (c * ROWS/8 + g) * 128, so for one K=16 MMA the two k chunks are LBO =
+// ROWS/8 * 128 bytes apart and row groups SBO = 128 bytes apart.  After a
+// proxy fence and a barrier, one thread issues the 4 MMAs of a 64-deep
+// k tile and commits them to the stage's mbarrier; the next tile loads while
+// they run.  The epilogue reads the accumulator with tcgen05.ld (warp w owns
+// rows 32w..32w+31).  Every wait is bounded: on timeout the kernel records
+// an error and leaves the tile.
+constexpr int kTcM = 128, kTcK = 64, kTcThreads = 128, kTcStages = 3;
+
+template <int BN>
+__host__ __device__ constexpr uint32_t tc_stage_bytes() { return (uint32_t)(kTcM + BN) * kTcK * 2; }
+template <int BN>
+__host__ __device__ constexpr uint32_t tc_smem_bytes() { return kTcStages * tc_stage_bytes<BN>(); }
+template <int BN>
+__host__ __device__ constexpr uint32_t tc_tmem_cols() { return BN < 32 ? 32u : (uint32_t)BN; }  // a power of 2, >= 32
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ uint64_t umma_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);  // version 1, no swizzle
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+    for (uint32_t it = 0; it < (1u << 22); ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+template <int AV, int BN>
+__device__ __forceinline__ void tc_load(const GemmArgs& g, uint8_t* as, uint8_t* bs, int m0, int k0) {
+    const int tid = threadIdx.x;
+#pragma unroll
+    for (int t = 0; t < kTcM * (kTcK / 8) / kTcThreads; ++t) {
+        const int i = tid + t * kTcThreads, row = i % kTcM, c = i / kTcM;
+        const int gm = m0 + row, gk = k0 + c * 8;
+        const bf16* src = nullptr;
+        if (gm < g.M && gk < g.K)
+            src = AV == kIm2col ? im2col_chunk(g.A, g.lda, gm, gk, g.flip_a) : g.A + (size_t)gm * g.lda + gk;
+        cp_async16(as + (c * (kTcM / 8) + row / 8) * 128 + (row % 8) * 16, src ? src : g.A, src != nullptr);
+    }
+#pragma unroll
+    for (int t = 0; t < (BN * (kTcK / 8) + kTcThreads - 1) / kTcThreads; ++t) {
+        const int i = tid + t * kTcThreads;
+        if (i >= BN * (kTcK / 8)) break;
+        const int row = i % BN, c = i / BN;
+        const int gk = k0 + c * 8;
+        const bool ok = row < g.N && gk < g.K;
+        cp_async16(bs + (c * (BN / 8) + row / 8) * 128 + (row % 8) * 16,
+                   ok ? g.B + (size_t)row * g.ldb + gk : g.B, ok);
+    }
+}
+
+template <int AV, int BN>
+__global__ void __launch_bounds__(kTcThreads) gemm_tc_kernel(const GemmArgs g, uint32_t* err) {
+    extern __shared__ __align__(1024) uint8_t tc_smem[];
+    __shared__ __align__(8) uint64_t bars[kTcStages];
+    __shared__ uint32_t tmem_slot;
+    constexpr int kA = kTcM * kTcK * 2;
+    constexpr uint32_t kStageBytes = tc_stage_bytes<BN>(), kCols = tc_tmem_cols<BN>();
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int m0 = blockIdx.x * kTcM;
+    const int nk = (g.K + kTcK - 1) / kTcK;
+    if (tid == 0)
+        for (int i = 0; i < kTcStages; ++i) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&bars[i])));
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&tmem_slot)),
+                     "r"(kCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+    const uint32_t tmem = tmem_slot;
+    // instruction descriptor: D f32, A and B bf16, both K-major, N, M = 128
+    const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(kTcM >> 4) << 24);
+    auto stage = [&](int kt) { return tc_smem + (kt % kTcStages) * kStageBytes; };
+    // the j-th commit on a stage completes phase j; tile kt is commit kt / kTcStages of stage kt % kTcStages
+    auto wait_tile = [&](int kt) {
+        return mbar_wait(smem_u32(&bars[kt % kTcStages]), (uint32_t)(kt / kTcStages) & 1u);
+    };
+    // prologue: tiles 0 .. kTcStages-2 in flight
+    for (int kt = 0; kt < kTcStages - 1; ++kt) {
+        if (kt < nk) tc_load<AV, BN>(g, stage(kt), stage(kt) + kA, m0, kt * kTcK);
+        cp_async_commit();
+    }
+    bool ok = true;
+    int issued = 0;  // k tiles whose MMAs were committed
+    for (int kt = 0; kt < nk; ++kt) {
+        cp_async_wait_group<kTcStages - 2>();  // this thread's copies of tile kt landed
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+            const uint32_t a0 = smem_u32(stage(kt)), b0 = a0 + kA;
+#pragma unroll
+            for (int s = 0; s < kTcK / 16; ++s) {
+                const uint64_t da = umma_desc(a0 + 2 * s * (kTcM / 8) * 128, (kTcM / 8) * 128, 128);
+                const uint64_t db = umma_desc(b0 + 2 * s * (BN / 8) * 128, (BN / 8) * 128, 128);
+                const uint32_t acc = (kt > 0 || s > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
+                    "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                smem_u32(&bars[kt % kTcStages])));
+        }
+        issued = kt + 1;
+        // refill the stage of tile kt - 1 with tile kt + kTcStages - 1 once
+        // its MMAs are done reading it
+        const int nt = kt + kTcStages - 1;
+        if (nt < nk) {
+            const bool w = kt >= 1 ? wait_tile(kt - 1) : true;
+            if (!__syncthreads_and(w)) {
+                ok = false;
+                break;
+            }
+            tc_load<AV, BN>(g, stage(nt), stage(nt) + kA, m0, nt * kTcK);
+        }
+        cp_async_commit();
+    }
+    cp_async_wait_group<0>();
+    // the last committed tile (MMAs complete in issue order); on failure too,
+    // before the tensor memory is released
+    if (issued > 0) {
+        const bool w = wait_tile(issued - 1);
+        ok = ok && w;
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+    if (!__syncthreads_and(ok)) {
+        if (tid == 0) atomicAdd(err, 1u);
+    } else {
+        const int row = m0 + warp * 32 + lane;
+#pragma unroll
+        for (int c0 = 0; c0 < BN; c0 += 8) {
+            uint32_t r[8];
+            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
+                         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                           "=r"(r[7])
+                         : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+            if (row < g.M) {
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    const int col = c0 + j;
+                    if (col < g.N) store(g, row, col, epilogue(g, row, col, __uint_as_float(r[j])));
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(kCols));
+    }
+}
+
 // Split-K: partial sums added in split order, then the epilogue.
 __global__ void splitk_reduce_kernel(const GemmArgs g, int splits) {
     const size_t n = (size_t)g.M * g.N;
@@ -317,6 +494,20 @@ cudaError_t gemm(GemmArgs g, int splits, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+template <int AV, int BN>
+cudaError_t gemm_tc(const GemmArgs& g, uint32_t* err, cudaStream_t s) {
+    static bool prepared = false;
+    if (!prepared) {
+        cudaError_t e = cudaFuncSetAttribute(gemm_tc_kernel<AV, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)tc_smem_bytes<BN>());
+        if (e != cudaSuccess) return e;
+        prepared = true;
+    }
+    if (g.M <= 0 || g.N <= 0) return cudaSuccess;
+    gemm_tc_kernel<AV, BN><<<(g.M + kTcM - 1) / kTcM, kTcThreads, tc_smem_bytes<BN>(), s>>>(g, err);
+    return cudaGetLastError();
+}
+
 }  // namespace
 }  // namespace sg
 }  // namespace mb
@@ -378,6 +569,8 @@ struct mb_surrogate {
     std::string err;
     uint64_t step = 0;
     float weight_decay = 0.0f;
+    bool tcgen05 = true;   // forward GEMMs on the 5th-generation tensor cores
+    Buf<uint32_t> tc_err;
     Buf<float> w, m, v, g, loss, y, t, partial;
     Buf<bf16> wb, wt2, wt3, x0, a1, a2, a3, h1, h2, dz2h, dz1h, dz3, dz2c, dz1c;
     Buf<uint8_t> cls;
@@ -424,47 +617,44 @@ GemmArgs args(mb_surrogate* s, const bf16* A, int lda, const bf16* B, int ldb, i
 }
 
 // Forward of n samples already one-hot in s->x0; leaves a1..a3, h1, h2, y.
+// The products run on tcgen05 (or, when switched off, on mma.sync).
 cudaError_t forward(mb_surrogate* s, uint32_t n) {
     cudaStream_t st = s->stream;
     const int R = (int)n * kVox;
     cudaError_t e;
-    {
-        GemmArgs a = args(s, s->x0.p, 8, PB(s, kW1), 27 * 8, R, 32, 27 * 8);
-        a.bias = P(s, kB1);
+    auto conv = [&](const bf16* x, int cin, Tensor w, Tensor b, bf16* out) {
+        GemmArgs a = args(s, x, cin, PB(s, w), 27 * cin, R, 32, 27 * cin);
+        a.bias = P(s, b);
         a.relu = 1;
-        a.c16 = s->a1.p;
-        if ((e = gemm<kIm2col, kDenseK>(a, 1, st)) != cudaSuccess) return e;
-    }
-    {
-        GemmArgs a = args(s, s->a1.p, 32, PB(s, kW2), 27 * 32, R, 32, 27 * 32);
-        a.bias = P(s, kB2);
+        a.c16 = out;
+        return s->tcgen05 ? gemm_tc<kIm2col, 32>(a, s->tc_err.p, st) : gemm<kIm2col, kDenseK>(a, 1, st);
+    };
+    auto fc = [&](const bf16* x, int k, Tensor w, Tensor b, bf16* out) {
+        GemmArgs a = args(s, x, k, PB(s, w), k, (int)n, 128, k);
+        a.bias = P(s, b);
         a.relu = 1;
-        a.c16 = s->a2.p;
-        if ((e = gemm<kIm2col, kDenseK>(a, 1, st)) != cudaSuccess) return e;
-    }
-    {
-        GemmArgs a = args(s, s->a2.p, 32, PB(s, kW3), 27 * 32, R, 32, 27 * 32);
-        a.bias = P(s, kB3);
-        a.relu = 1;
-        a.c16 = s->a3.p;
-        if ((e = gemm<kIm2col, kDenseK>(a, 1, st)) != cudaSuccess) return e;
-    }
-    {
-        GemmArgs a = args(s, s->a3.p, 6912, PB(s, kW4), 6912, (int)n, 128, 6912);
-        a.bias = P(s, kB4);
-        a.relu = 1;
-        a.c16 = s->h1.p;
-        if ((e = gemm<kDenseK, kDenseK>(a, 1, st)) != cudaSuccess) return e;
-    }
-    {
-        GemmArgs a = args(s, s->h1.p, 128, PB(s, kW5), 128, (int)n, 128, 128);
-        a.bias = P(s, kB5);
-        a.relu = 1;
-        a.c16 = s->h2.p;
-        if ((e = gemm<kDenseK, kDenseK>(a, 1, st)) != cudaSuccess) return e;
-    }
+        a.c16 = out;
+        return s->tcgen05 ? gemm_tc<kDenseK, 128>(a, s->tc_err.p, st) : gemm<kDenseK, kDenseK>(a, 1, st);
+    };
+    if ((e = conv(s->x0.p, 8, kW1, kB1, s->a1.p)) != cudaSuccess) return e;
+    if ((e = conv(s->a1.p, 32, kW2, kB2, s->a2.p)) != cudaSuccess) return e;
+    if ((e = conv(s->a2.p, 32, kW3, kB3, s->a3.p)) != cudaSuccess) return e;
+    if ((e = fc(s->a3.p, 6912, kW4, kB4, s->h1.p)) != cudaSuccess) return e;
+    if ((e = fc(s->h1.p, 128, kW5, kB5, s->h2.p)) != cudaSuccess) return e;
     head_kernel<<<(n + 7) / 8, 256, 0, st>>>(s->h2.p, PB(s, kW6), P(s, kB6), n, s->y.p);
     return cudaGetLastError();
+}
+
+// Reads and clears the tensor-core GEMM error count (after a synchronise).
+mb_status check_tc(mb_surrogate* s) {
+    uint32_t err = 0;
+    SG_CUDA(s, cudaMemcpyAsync(&err, s->tc_err.p, sizeof(err), cudaMemcpyDeviceToHost, s->stream));
+    SG_CUDA(s, cudaStreamSynchronize(s->stream));
+    if (err) {
+        SG_CUDA(s, cudaMemsetAsync(s->tc_err.p, 0, sizeof(uint32_t), s->stream));
+        return sfail(s, MB_ERR_CUDA, "tensor-core GEMM wait timed out");
+    }
+    return MB_OK;
 }
 
 int splits_for(int K) { return std::max(1, std::min(64, K / 1024)); }
@@ -579,8 +769,9 @@ mb_status mb_surrogate_create(int device, uint32_t max_batch, uint64_t seed, mb_
           ok(s->a2.alloc(R * 32)) && ok(s->a3.alloc(R * 32)) && ok(s->h1.alloc((size_t)max_batch * 128)) &&
           ok(s->h2.alloc((size_t)max_batch * 128)) && ok(s->dz2h.alloc((size_t)max_batch * 128)) &&
           ok(s->dz1h.alloc((size_t)max_batch * 128)) && ok(s->dz3.alloc(R * 32)) && ok(s->dz2c.alloc(R * 32)) &&
-          ok(s->dz1c.alloc(R * 32)) && ok(s->cls.alloc(R))))
+          ok(s->dz1c.alloc(R * 32)) && ok(s->cls.alloc(R)) && ok(s->tc_err.alloc(1))))
         return MB_ERR_CUDA;
+    if (cudaMemset(s->tc_err.p, 0, sizeof(uint32_t)) != cudaSuccess) return MB_ERR_CUDA;
     // He-normal weights (fan-in of the real inputs), zero biases, zero
     // weights on the padding channels of W1; Box-Muller over SplitMix64.
     std::vector<float> w(np, 0.0f);
@@ -625,6 +816,12 @@ mb_status mb_surrogate_set_params(mb_surrogate* s, const float* params) {
     return MB_OK;
 }
 
+mb_status mb_surrogate_use_tcgen05(mb_surrogate* s, int on) {
+    if (!s) return MB_ERR_ARGUMENT;
+    s->tcgen05 = on != 0;
+    return MB_OK;
+}
+
 mb_status mb_surrogate_set_weight_decay(mb_surrogate* s, float weight_decay) {
     if (!s || !(weight_decay >= 0.0f)) return sfail(s, MB_ERR_ARGUMENT, "weight decay must be >= 0");
     s->weight_decay = weight_decay;
@@ -651,7 +848,7 @@ mb_status mb_surrogate_predict(mb_surrogate* s, const uint8_t* genomes, uint32_t
         SG_CUDA(s, cudaMemcpyAsync(out + b0, s->y.p, nb * sizeof(float), cudaMemcpyDeviceToHost, s->stream));
     }
     SG_CUDA(s, cudaStreamSynchronize(s->stream));
-    return MB_OK;
+    return check_tc(s);
 }
 
 mb_status mb_surrogate_gradients(mb_surrogate* s, const uint8_t* genomes, const float* targets, uint32_t n,
@@ -669,7 +866,7 @@ mb_status mb_surrogate_gradients(mb_surrogate* s, const uint8_t* genomes, const 
                                    s->stream));
     if (loss) SG_CUDA(s, cudaMemcpyAsync(loss, s->loss.p, sizeof(float), cudaMemcpyDeviceToHost, s->stream));
     SG_CUDA(s, cudaStreamSynchronize(s->stream));
-    return MB_OK;
+    return check_tc(s);
 }
 
 mb_status mb_surrogate_train_step(mb_surrogate* s, const uint8_t* genomes, const float* targets, uint32_t n,

@@ -82,6 +82,10 @@ class Surrogate:
                                                     _lib.ptr(loss)))
         return float(loss[0]), grads
 
+    def use_tcgen05(self, on: bool = True) -> None:
+        """Forward products on tcgen05 (default) or on the mma.sync kernel."""
+        self._check(_lib.LIB.mb_surrogate_use_tcgen05(self._s, int(bool(on))))
+
     def set_weight_decay(self, wd: float) -> None:
         """Decoupled weight decay of the Adam steps (AdamW)."""
         self._check(_lib.LIB.mb_surrogate_set_weight_decay(self._s, float(wd)))

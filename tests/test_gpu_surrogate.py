@@ -28,6 +28,26 @@ def test_predictions_match_oracle():
     assert np.abs(y - yo).max() <= 2e-2 * np.abs(yo).max()
 
 
+@pytest.mark.parametrize("n", [1, 100, 700])
+def test_tcgen05_forward_matches_mma_sync(n):
+    """The forward on tcgen05 (TMEM accumulators) against the mma.sync
+    kernel and the oracle, with partial tiles (M not a multiple of 128)."""
+    rng = np.random.default_rng(10 + n)
+    flat = so.init_params(8)
+    s = Surrogate(0, max_batch=256)
+    s.set_params(flat)
+    genomes = rng.integers(0, 5, (n, 216)).astype(np.uint8)
+    s.use_tcgen05(True)
+    y_tc = s.predict(genomes)
+    s.use_tcgen05(False)
+    y_ms = s.predict(genomes)
+    yo, _ = so.Net(flat).forward(genomes)
+    scale = np.abs(yo).max()
+    assert np.abs(y_tc - y_ms).max() <= 2e-2 * scale
+    assert np.abs(y_tc - yo).max() <= 2e-2 * scale
+    assert rel(y_tc, yo) < 1e-2
+
+
 def test_gradients_match_oracle():
     rng = np.random.default_rng(1)
     flat = so.init_params(6)
