@@ -12,7 +12,8 @@ import os
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libmercury_b200.so")
+# MB_LIBRARY selects another build of the library (A/B timing of variants)
+LIB_PATH = os.environ.get("MB_LIBRARY") or os.path.join(_HERE, "libmercury_b200.so")
 
 MB_OK = 0
 STATUS_NAMES = {
