@@ -398,8 +398,54 @@ def secondary(args, batch, local_rank, dev, hbm_peak):
                                     "bytes_per_update": hbm_b}}
     del ss
     out["devo"] = devo_bench(local_rank)
+    out["build"] = build_bench(local_rank)
     out["surrogate"] = surrogate_bench(local_rank)
     return out
+
+
+def build_bench(local_rank):
+    """Robot construction (optimize/benchmark.cpp "build" mode), robots/s:
+    4096 random 6x6x6 voxel genomes built and packed on the device
+    (mb_set_voxel_population) against the host builder plus host packing on
+    512 of them; the k = 25 nearest-neighbour springs of 256 point-cloud
+    robots (the third configuration) on the device (mb_knn_springs) against
+    the host builder on 16 of them."""
+    import mercury_b200 as mb
+    from mercury_b200 import evolve, robots
+    from mercury_b200.surrogate import to_cells
+    rng = np.random.default_rng(5)
+    cells = to_cells(evolve.random_genomes(rng, 4096))
+    sim = mb.Simulator(local_rank)
+    sim.set_voxel_population(cells, 0.1, 0.1)  # plans the packing once
+    t0 = time.perf_counter()
+    for _ in range(3):
+        sim.set_voxel_population(cells, 0.1, 0.1)
+    dev_vox = 3 * 4096 / (time.perf_counter() - t0)
+    t0 = time.perf_counter()
+    b = mb.pack([robots.voxel_robot(c, 0.1, 0.1) for c in cells[:512]])
+    hs = mb.Simulator(local_rank)
+    hs.set_batch(b)
+    host_vox = 512 / (time.perf_counter() - t0)
+    pts, mats = [], []
+    for r in range(256):
+        g = np.random.default_rng(2000 + r)
+        p, m = robots.nn_points(g, int(g.integers(500, 2001)))
+        pts.append(p)
+        mats.append(m)
+    robots.knn_springs(pts[:8], mats[:8])
+    t0 = time.perf_counter()
+    robots.knn_springs(pts, mats)
+    dev_knn = 256 / (time.perf_counter() - t0)
+    t0 = time.perf_counter()
+    for r in range(16):
+        g = np.random.default_rng(2000 + r)
+        robots.nn_robot(g, int(g.integers(500, 2001)))
+    host_knn = 16 / (time.perf_counter() - t0)
+    return {"unit": "robots/s",
+            "voxel_6x6x6": {"device": dev_vox, "host": host_vox, "speedup": dev_vox / host_vox,
+                            "note": "device: build + pack + upload of 4096; host: build + pack + upload of 512"},
+            "knn_points_500_2000": {"device": dev_knn, "host": host_knn, "speedup": dev_knn / host_knn,
+                                    "note": "springs only (point sampling and materials on the host in both)"}}
 
 
 DEVO_ROBOTS, DEVO_K = 512, 128

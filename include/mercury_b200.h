@@ -233,6 +233,21 @@ MB_API mb_status mb_devo_profile(const mb_context* ctx, double* ms);
 MB_API mb_status mb_set_voxel_population(mb_context* ctx, uint32_t n_robots, int sx, int sy, int sz,
                                          const uint8_t* cells, float h, float mass);
 
+/* k-nearest-neighbour springs of point-cloud robots, built on `device`
+ * (the springs of the reference's NNRobot, common/evolvables/knn.cu:62-145
+ * and knn_kernel.cu:34-60): every mass is joined to its k nearest masses of
+ * the same robot -- squared distances the float32 sum (dx*dx + dy*dy) +
+ * dz*dz, ties by lower index -- and each unordered pair appears once, the
+ * lower index first, pairs in lexicographic order, with the float32
+ * distance as mean length and the composite material of the two masses.
+ * pos: 3 floats per mass (host); at most 4,096 masses per robot, k <= 32.
+ * spring_offsets (n_robots + 1) is always written; with pairs == NULL the
+ * call only counts.  Synchronous; allocates its own device scratch.  No
+ * context needed. */
+MB_API mb_status mb_knn_springs(int device, uint32_t n_robots, const int64_t* mass_offsets, const float* pos,
+                                const uint8_t* mass_material, uint32_t k, int64_t* spring_offsets,
+                                uint16_t* pairs, uint8_t* spring_material, float* lbar, uint64_t capacity);
+
 /* Mass materials in the upload layout (after the strip of a device build). */
 MB_API mb_status mb_collect_mass_materials(mb_context* ctx, uint8_t* material);
 

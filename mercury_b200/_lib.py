@@ -117,6 +117,7 @@ def _load() -> ctypes.CDLL:
         "mb_devo_profile": (I32, [P, P]),
         "mb_set_voxel_population": (I32, [P, U32, I32, I32, I32, P, F32, F32]),
         "mb_collect_mass_materials": (I32, [P, P]),
+        "mb_knn_springs": (I32, [I32, U32, P, P, P, U32, P, P, P, P, ctypes.c_uint64]),
         "mb_surrogate_create": (I32, [I32, U32, ctypes.c_uint64, ctypes.POINTER(P)]),
         "mb_surrogate_destroy": (None, [P]),
         "mb_surrogate_last_error": (ctypes.c_char_p, [P]),

@@ -75,13 +75,11 @@ def random_cells(side: int, rng: np.random.Generator, choices=FIVE, p=FIVE_P) ->
     return choices[rng.choice(len(choices), size=(side, side, side), p=p)]
 
 
-def nn_robot(rng: np.random.Generator, n_masses: int, k: int = 25, axes=(0.3, 0.2, 0.15),
-             hidden=(25, 25), mass: float = 0.1) -> Element:
-    """Point-cloud robot: masses uniform in an ellipsoid, k-nearest-neighbour
-    springs (each unordered pair once, the lower index first) with the
-    initial distance as mean length and the composite material of their two
-    masses; mass materials from a random-init tanh MLP over (x, y, z)."""
-    from .materials import composite_id
+def nn_points(rng: np.random.Generator, n_masses: int, axes=(0.3, 0.2, 0.15), hidden=(25, 25)):
+    """Masses of a point-cloud robot: uniform in an ellipsoid, lowest on
+    z = 0 (float32 positions); materials from a random-init tanh MLP over
+    (x, y, z) in ellipsoid units, argmax over bone, tissue, muscle_a,
+    muscle_b (unit-variance weights, small biases)."""
     pts = []
     a = np.asarray(axes, np.float64)
     while sum(len(p) for p in pts) < n_masses:
@@ -90,8 +88,6 @@ def nn_robot(rng: np.random.Generator, n_masses: int, k: int = 25, axes=(0.3, 0.
     p = np.concatenate(pts)[:n_masses]
     p[:, 2] -= p[:, 2].min()  # lowest mass on z = 0
     p = p.astype(np.float32)
-    # material MLP: 3 -> 25 -> 25 -> 4 over the position in ellipsoid units,
-    # tanh, argmax; unit-variance weights, small biases
     x = (p - p.mean(0)).astype(np.float64) / a
     for h in (*hidden, 4):
         w = rng.normal(0.0, 1.0 / np.sqrt(x.shape[1]), size=(x.shape[1], h)) * 2.0
@@ -99,7 +95,17 @@ def nn_robot(rng: np.random.Generator, n_masses: int, k: int = 25, axes=(0.3, 0.
         x = x @ w + bias
         if h != 4:
             x = np.tanh(x)
-    mats = FOUR[np.argmax(x, axis=1)]
+    return p, FOUR[np.argmax(x, axis=1)]
+
+
+def nn_robot(rng: np.random.Generator, n_masses: int, k: int = 25, axes=(0.3, 0.2, 0.15),
+             hidden=(25, 25), mass: float = 0.1) -> Element:
+    """Point-cloud robot (nn_points) with k-nearest-neighbour springs, built
+    on the host: each unordered pair once, the lower index first, in
+    lexicographic order, the initial distance as mean length and the
+    composite material of the two masses."""
+    from .materials import composite_id
+    p, mats = nn_points(rng, n_masses, axes, hidden)
     # k nearest neighbours of every mass (float32 distances, ties by index)
     d2 = ((p[:, None, :] - p[None, :, :]) ** 2).sum(-1)
     np.fill_diagonal(d2, np.inf)
@@ -111,6 +117,41 @@ def nn_robot(rng: np.random.Generator, n_masses: int, k: int = 25, axes=(0.3, 0.
     lbar = np.sqrt((diff * diff).sum(1)).astype(np.float32)
     smat = np.array([composite_id(int(mats[u]), int(mats[v])) for u, v in pairs], np.uint8)
     return Element(p, mats, pairs.astype(np.uint16), lbar, smat, mass=np.full(n_masses, mass, np.float32))
+
+
+def knn_springs(points: list, materials: list, k: int = 25, device: int = 0):
+    """The springs nn_robot builds, for many robots at once on the GPU
+    (mb_knn_springs).  Returns (spring_offsets, pairs, spring_material,
+    lbar) over the robots in order."""
+    R = len(points)
+    mo = np.zeros(R + 1, np.int64)
+    mo[1:] = np.cumsum([len(p) for p in points])
+    pos = np.ascontiguousarray(np.concatenate(points), np.float32)
+    mm = np.ascontiguousarray(np.concatenate(materials), np.uint8)
+    so = np.zeros(R + 1, np.int64)
+    _lib.check(_lib.LIB.mb_knn_springs(device, R, _lib.ptr(mo), _lib.ptr(pos), _lib.ptr(mm), k, _lib.ptr(so),
+                                       None, None, None, 0))
+    S = int(so[-1])
+    pairs = np.empty((S, 2), np.uint16)
+    smat = np.empty(S, np.uint8)
+    lbar = np.empty(S, np.float32)
+    _lib.check(_lib.LIB.mb_knn_springs(device, R, _lib.ptr(mo), _lib.ptr(pos), _lib.ptr(mm), k, _lib.ptr(so),
+                                       _lib.ptr(pairs), _lib.ptr(smat), _lib.ptr(lbar), S))
+    return so, pairs, smat, lbar
+
+
+def nn_population_device(n_robots: int = 256, seed_base: int = 2000, mass: float = 0.1, k: int = 25,
+                         device: int = 0) -> list[Element]:
+    """population("nn", ...) with the springs built on the GPU."""
+    pts, mats = [], []
+    for r in range(n_robots):
+        rng = np.random.default_rng(seed_base + r)
+        p, m = nn_points(rng, int(rng.integers(500, 2001)))
+        pts.append(p)
+        mats.append(m)
+    so, pairs, smat, lbar = knn_springs(pts, mats, k, device)
+    return [Element(pts[r], mats[r], pairs[so[r]:so[r + 1]], lbar[so[r]:so[r + 1]], smat[so[r]:so[r + 1]],
+                    mass=np.full(len(pts[r]), mass, np.float32)) for r in range(n_robots)]
 
 
 def population(name: str, n_robots: int | None = None, seed_base: int | None = None,
