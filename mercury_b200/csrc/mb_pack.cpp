@@ -18,6 +18,7 @@
 #include "mb_pack.h"
 
 #include <algorithm>
+#include <climits>
 #include <atomic>
 #include <cmath>
 #include <cstdio>
@@ -111,13 +112,15 @@ void preprocess(const mb_batch_desc* b, uint32_t r, RobotPack& p) {
         deg[a]++;
         deg[c]++;
     }
-    std::stable_sort(sp.begin(), sp.end(), [&](uint32_t x, uint32_t y) {
-        const int64_t gx = s0 + x, gy = s0 + y;
-        const int dx = (int)b->pairs[2 * gx + 1] - (int)b->pairs[2 * gx];
-        const int dy = (int)b->pairs[2 * gy + 1] - (int)b->pairs[2 * gy];
-        if (dx != dy) return dx < dy;
-        return b->pairs[2 * gx] < b->pairs[2 * gy];
-    });
+    // order (b - a, a), ties by spring index: one unique 64-bit key each
+    std::vector<uint64_t> keys(sp.size());
+    for (size_t q = 0; q < sp.size(); ++q) {
+        const int64_t g = s0 + sp[q];
+        const int dx = (int)b->pairs[2 * g + 1] - (int)b->pairs[2 * g];
+        keys[q] = ((uint64_t)(dx + 4096) << 48) | ((uint64_t)b->pairs[2 * g] << 32) | sp[q];  // |dx| < 4096
+    }
+    std::sort(keys.begin(), keys.end());
+    for (size_t q = 0; q < sp.size(); ++q) sp[q] = (uint32_t)keys[q];
     p.n_mass = (uint32_t)cm;
     p.cost = (uint64_t)sp.size() * 4 + (uint64_t)cm;
     uint64_t est = 0;  // incidence entries with rows padded to the slice maximum
@@ -251,24 +254,42 @@ void build_bin(const mb_batch_desc* b, const std::vector<RobotPack>& packs,
     // entries of a warp's 32 masses are springs of one direction with
     // consecutive packed indices (conflict-free gather) -- otherwise, or
     // when alignment would widen the slice by more than 4 columns, ranks.
-    std::vector<int> offs;
+    // the union of a slice's offsets as a bitset over [lo, hi]: an entry's
+    // aligned column is the rank of its offset (prefix popcounts per word)
+    std::vector<uint64_t> bits;
+    std::vector<uint32_t> before;
     for (uint32_t i0 = 0; i0 < nm; i0 += kSliceWidth) {
         const uint32_t i1 = std::min<uint32_t>(i0 + kSliceWidth, nm);
         uint32_t w_rank = 0;
         bool distinct = true;
-        offs.clear();
+        int lo = INT32_MAX, hi = INT32_MIN;
         for (uint32_t i = i0; i < i1; ++i) {
             const uint32_t r0 = row_start[i], r1 = row_start[i + 1];
             w_rank = std::max(w_rank, r1 - r0);
             for (uint32_t q = r0; q < r1; ++q) {
                 if (q > r0 && ents[q].other == ents[q - 1].other) distinct = false;
-                offs.push_back((int)ents[q].other - (int)i);
+                const int o = (int)ents[q].other - (int)i;
+                lo = std::min(lo, o);
+                hi = std::max(hi, o);
             }
         }
-        std::sort(offs.begin(), offs.end());
-        offs.erase(std::unique(offs.begin(), offs.end()), offs.end());
-        const bool aligned = distinct && offs.size() <= w_rank + 4;
-        const uint32_t w = aligned ? (uint32_t)offs.size() : w_rank;
+        uint32_t n_union = 0;
+        if (distinct && lo <= hi) {
+            const size_t words = (size_t)(hi - lo) / 64 + 1;
+            bits.assign(words, 0);
+            for (uint32_t i = i0; i < i1; ++i)
+                for (uint32_t q = row_start[i]; q < row_start[i + 1]; ++q) {
+                    const int o = (int)ents[q].other - (int)i - lo;
+                    bits[o >> 6] |= 1ull << (o & 63);
+                }
+            before.assign(words, 0);
+            for (size_t wd = 0; wd < words; ++wd) {
+                before[wd] = n_union;
+                n_union += (uint32_t)__builtin_popcountll(bits[wd]);
+            }
+        }
+        const bool aligned = distinct && n_union <= w_rank + 4;
+        const uint32_t w = aligned ? n_union : w_rank;
         aligned ? ++L.aligned : ++L.ranked;
         const size_t base = streamed ? L.inc32.size() : L.inc.size();
         L.slice_off.push_back((uint32_t)base);
@@ -280,10 +301,12 @@ void build_bin(const mb_batch_desc* b, const std::vector<RobotPack>& packs,
         for (uint32_t i = i0; i < i1; ++i)
             for (uint32_t q = row_start[i]; q < row_start[i + 1]; ++q) {
                 const Ent& e = ents[q];
-                const uint32_t col =
-                    aligned ? (uint32_t)(std::lower_bound(offs.begin(), offs.end(), (int)e.other - (int)i) -
-                                         offs.begin())
-                            : q - row_start[i];
+                uint32_t col = q - row_start[i];
+                if (aligned) {
+                    const int o = (int)e.other - (int)i - lo;
+                    const uint64_t below = bits[o >> 6] & ((1ull << (o & 63)) - 1ull);
+                    col = before[o >> 6] + (uint32_t)__builtin_popcountll(below);
+                }
                 const size_t at = base + (size_t)col * kSliceWidth + (i - i0);
                 if (streamed)
                     L.inc32[at] = (e.packed << 1) | e.sign;
@@ -305,50 +328,63 @@ void build_all(const mb_batch_desc* b, const std::vector<RobotPack>& packs,
     out.bins.assign(nb, BinDesc{});
     out.robot_bin.assign(R, 0);
     out.robot_mass_base.assign(R, 0);
-    out.mass_gidx.clear();
-    out.spring_gidx.clear();
-    out.pair.clear();
-    out.lbar.clear();
-    out.slice_off.clear();
-    out.slice_width.clear();
-    out.inc.clear();
-    out.inc32.clear();
     out.max_smem = 0;
     out.inc_entries = out.inc_padding = 0;
     out.aligned_slices = out.rank_slices = 0;
+    // bin offsets, then every bin copied in parallel into sized arrays
+    uint64_t nm = 0, ns = 0, nsl = 0, ninc = 0;
     for (uint32_t i = 0; i < nb; ++i) {
         const BinLocal& L = locals[i];
         BinDesc& d = out.bins[i];
         std::memset(&d, 0, sizeof(d));
-        d.mass_begin = (uint32_t)out.mass_gidx.size();
+        d.mass_begin = (uint32_t)nm;
         d.n_mass = L.n_mass;
-        d.spring_begin = (uint32_t)out.spring_gidx.size();
+        d.spring_begin = (uint32_t)ns;
         d.n_spring = L.n_spring;
-        d.inc_begin = (uint32_t)(streamed ? out.inc32.size() : out.inc.size());
+        d.inc_begin = (uint32_t)ninc;
         d.n_inc = L.n_inc;
-        d.slice_begin = (uint32_t)out.slice_off.size();
+        d.slice_begin = (uint32_t)nsl;
+        nm += L.mass_gidx.size();
+        ns += L.spring_gidx.size();
+        nsl += L.slice_off.size();
+        ninc += streamed ? L.inc32.size() : L.inc.size();
         uint32_t base = 0;
         for (uint32_t r : plan[i]) {
             out.robot_bin[r] = i;
             out.robot_mass_base[r] = base;
             base += packs[r].n_mass;
         }
-        out.mass_gidx.insert(out.mass_gidx.end(), L.mass_gidx.begin(), L.mass_gidx.end());
-        out.spring_gidx.insert(out.spring_gidx.end(), L.spring_gidx.begin(), L.spring_gidx.end());
-        out.pair.insert(out.pair.end(), L.pair.begin(), L.pair.end());
-        out.lbar.insert(out.lbar.end(), L.lbar.begin(), L.lbar.end());
-        out.slice_off.insert(out.slice_off.end(), L.slice_off.begin(), L.slice_off.end());
-        out.slice_width.insert(out.slice_width.end(), L.slice_width.begin(), L.slice_width.end());
-        if (streamed)
-            out.inc32.insert(out.inc32.end(), L.inc32.begin(), L.inc32.end());
-        else
-            out.inc.insert(out.inc.end(), L.inc.begin(), L.inc.end());
         out.max_smem = std::max(out.max_smem, L.smem);
         out.inc_entries += L.n_inc;
         out.inc_padding += L.padding;
         out.aligned_slices += L.aligned;
         out.rank_slices += L.ranked;
     }
+    out.mass_gidx.resize(nm);
+    out.spring_gidx.resize(ns);
+    out.pair.resize(ns);
+    out.lbar.resize(ns);
+    out.slice_off.resize(nsl);
+    out.slice_width.resize(nsl);
+    out.inc.assign(streamed ? 0 : ninc, 0);
+    out.inc32.assign(streamed ? ninc : 0, 0);
+    parallel_for(nb, threads, [&](uint32_t i) {
+        const BinLocal& L = locals[i];
+        const BinDesc& d = out.bins[i];
+        auto put = [](auto& dst, size_t at, const auto& src) {
+            if (!src.empty()) std::memcpy(dst.data() + at, src.data(), src.size() * sizeof(src[0]));
+        };
+        put(out.mass_gidx, d.mass_begin, L.mass_gidx);
+        put(out.spring_gidx, d.spring_begin, L.spring_gidx);
+        put(out.pair, d.spring_begin, L.pair);
+        put(out.lbar, d.spring_begin, L.lbar);
+        put(out.slice_off, d.slice_begin, L.slice_off);
+        put(out.slice_width, d.slice_begin, L.slice_width);
+        if (streamed)
+            put(out.inc32, d.inc_begin, L.inc32);
+        else
+            put(out.inc, d.inc_begin, L.inc);
+    });
 }
 
 }  // namespace
