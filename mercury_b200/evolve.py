@@ -183,10 +183,14 @@ class ScreenedEvolution:
     orientation (the fitness does not change); predictions average the 8
     orientations."""
 
-    def __init__(self, evaluator: Evaluator, surrogate: Surrogate, seed: int = 0, children: int = 4096,
+    def __init__(self, evaluator: Evaluator, surrogate, seed: int = 0, children: int = 4096,
                  screen: float = 0.25, audit: float = 0.05, batch: int = 256, lr: float = 1e-3,
                  steps_per_generation: int = 60, finetune_lr: float = 3e-4, lineage_correction: bool = True):
-        self.ev, self.sg = evaluator, surrogate
+        """`surrogate`: one Surrogate or a list of them (an ensemble: each
+        member trains on its own minibatches, predictions are averaged)."""
+        self.ev = evaluator
+        self.members = list(surrogate) if isinstance(surrogate, (list, tuple)) else [surrogate]
+        self.sg = self.members[0]
         self.rng = np.random.default_rng(seed)
         self.children, self.screen, self.audit = children, screen, audit
         self.batch, self.lr, self.steps, self.finetune_lr = batch, lr, steps_per_generation, finetune_lr
@@ -198,7 +202,8 @@ class ScreenedEvolution:
 
     def predict(self, genomes: np.ndarray) -> np.ndarray:
         g = np.asarray(genomes, np.uint8)
-        return np.mean([self.sg.predict(np.ascontiguousarray(g[:, p])) for p in ORIENTATIONS], axis=0)
+        views = [np.ascontiguousarray(g[:, p]) for p in ORIENTATIONS]
+        return np.mean([sg.predict(v) for sg in self.members for v in views], axis=0)
 
     def _norm(self):
         _, f = self.data.arrays()
@@ -208,15 +213,16 @@ class ScreenedEvolution:
         g, f = self.data.arrays()
         loss = 0.0
         for i in range(steps):
-            idx = self.rng.integers(0, len(f), self.batch)
-            gb, fb = g[idx], f[idx]
-            if recent is not None:  # half of every batch from the newest generation
-                r = self.rng.integers(0, len(recent[1]), self.batch // 2)
-                gb = np.concatenate([gb[: self.batch - len(r)], recent[0][r]])
-                fb = np.concatenate([fb[: self.batch - len(r)], recent[1][r]])
-            gb = np.take_along_axis(gb, ORIENTATIONS[self.rng.integers(0, 8, len(gb))], axis=1)
             step_lr = lr * 0.5 * (1.0 + np.cos(np.pi * i / steps)) if cosine else lr
-            loss = self.sg.train_step(gb, (fb - self.mu) / self.sd, step_lr)
+            for sg in self.members:
+                idx = self.rng.integers(0, len(f), self.batch)
+                gb, fb = g[idx], f[idx]
+                if recent is not None:  # half of every batch from the newest generation
+                    r = self.rng.integers(0, len(recent[1]), self.batch // 2)
+                    gb = np.concatenate([gb[: self.batch - len(r)], recent[0][r]])
+                    fb = np.concatenate([fb[: self.batch - len(r)], recent[1][r]])
+                gb = np.take_along_axis(gb, ORIENTATIONS[self.rng.integers(0, 8, len(gb))], axis=1)
+                loss = sg.train_step(gb, (fb - self.mu) / self.sd, step_lr)
             self.trained_steps += 1
         return loss
 
