@@ -231,14 +231,14 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
 }
 
 template <int AV, int BN>
-__device__ __forceinline__ void tc_load(const GemmArgs& g, uint8_t* as, uint8_t* bs, int m0, int k0) {
+__device__ __forceinline__ void tc_load(const GemmArgs& g, uint8_t* as, uint8_t* bs, int m0, int k0, int k_stop) {
     const int tid = threadIdx.x;
 #pragma unroll
     for (int t = 0; t < kTcM * (kTcK / 8) / kTcThreads; ++t) {
         const int i = tid + t * kTcThreads, row = i % kTcM, c = i / kTcM;
         const int gm = m0 + row, gk = k0 + c * 8;
         const bf16* src = nullptr;
-        if (gm < g.M && gk < g.K)
+        if (gm < g.M && gk < k_stop)
             src = AV == kIm2col ? im2col_chunk(g.A, g.lda, gm, gk, g.flip_a) : g.A + (size_t)gm * g.lda + gk;
         cp_async16(as + (c * (kTcM / 8) + row / 8) * 128 + (row % 8) * 16, src ? src : g.A, src != nullptr);
     }
@@ -248,7 +248,7 @@ __device__ __forceinline__ void tc_load(const GemmArgs& g, uint8_t* as, uint8_t*
         if (i >= BN * (kTcK / 8)) break;
         const int row = i % BN, c = i / BN;
         const int gk = k0 + c * 8;
-        const bool ok = row < g.N && gk < g.K;
+        const bool ok = row < g.N && gk < k_stop;
         cp_async16(bs + (c * (BN / 8) + row / 8) * 128 + (row % 8) * 16,
                    ok ? g.B + (size_t)row * g.ldb + gk : g.B, ok);
     }
@@ -263,7 +263,10 @@ __global__ void __launch_bounds__(kTcThreads) gemm_tc_kernel(const GemmArgs g, u
     constexpr uint32_t kStageBytes = tc_stage_bytes<BN>(), kCols = tc_tmem_cols<BN>();
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int m0 = blockIdx.x * kTcM;
-    const int nk = (g.K + kTcK - 1) / kTcK;
+    // split K: this CTA adds k in [k_begin, k_begin + k_chunk)
+    const int k_begin = blockIdx.y * g.k_chunk;
+    const int k_stop = min(g.K, k_begin + g.k_chunk);
+    const int nk = k_stop > k_begin ? (k_stop - k_begin + kTcK - 1) / kTcK : 0;
     if (tid == 0)
         for (int i = 0; i < kTcStages; ++i) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&bars[i])));
     if (warp == 0) {
@@ -284,7 +287,7 @@ __global__ void __launch_bounds__(kTcThreads) gemm_tc_kernel(const GemmArgs g, u
     };
     // prologue: tiles 0 .. kTcStages-2 in flight
     for (int kt = 0; kt < kTcStages - 1; ++kt) {
-        if (kt < nk) tc_load<AV, BN>(g, stage(kt), stage(kt) + kA, m0, kt * kTcK);
+        if (kt < nk) tc_load<AV, BN>(g, stage(kt), stage(kt) + kA, m0, k_begin + kt * kTcK, k_stop);
         cp_async_commit();
     }
     bool ok = true;
@@ -320,7 +323,7 @@ __global__ void __launch_bounds__(kTcThreads) gemm_tc_kernel(const GemmArgs g, u
                 ok = false;
                 break;
             }
-            tc_load<AV, BN>(g, stage(nt), stage(nt) + kA, m0, nt * kTcK);
+            tc_load<AV, BN>(g, stage(nt), stage(nt) + kA, m0, k_begin + nt * kTcK, k_stop);
         }
         cp_async_commit();
     }
@@ -349,7 +352,11 @@ __global__ void __launch_bounds__(kTcThreads) gemm_tc_kernel(const GemmArgs g, u
 #pragma unroll
                 for (int j = 0; j < 8; ++j) {
                     const int col = c0 + j;
-                    if (col < g.N) store(g, row, col, epilogue(g, row, col, __uint_as_float(r[j])));
+                    if (col >= g.N) continue;
+                    if (gridDim.y > 1)
+                        g.partial[((size_t)blockIdx.y * g.M + row) * g.N + col] = __uint_as_float(r[j]);
+                    else
+                        store(g, row, col, epilogue(g, row, col, __uint_as_float(r[j])));
                 }
             }
         }
@@ -359,6 +366,206 @@ __global__ void __launch_bounds__(kTcThreads) gemm_tc_kernel(const GemmArgs g, u
     if (warp == 0) {
         asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(kCols));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Planar implicit-GEMM convolution on tcgen05 (the forward 3x3x3 layers).
+//
+// Activations are stored per genome as planes of 8 channels over the 8x8x8
+// grid padded with a zero halo: element (genome b, plane c/8, padded voxel
+// p = (x+1) + 8(y+1) + 64(z+1), channel c%8) at ((b P + c/8) 512 + p) 8 +
+// c%8, so one padded voxel of one plane is a 16-byte row and consecutive
+// rows are 16 bytes apart -- exactly the K-major no-swizzle UMMA layout
+// with SBO = 128 bytes.  The input of output row p at offset o is row
+// p + delta(o), delta = dx + 8 dy + 64 dz: a shift of the descriptor's start
+// address.  A CTA loads, for an output tile of 128 padded rows, its 288-row
+// input window (tile - 80 .. tile + 208, zero outside the genome) once and
+// issues all the tile's MMAs from it: 27 offsets x 2 channel halves (K = 16
+// each, LBO = the plane stride) for 32 input channels; for 8 input channels
+// two offsets share one K = 16 MMA (LBO = the row distance between them).
+// The weights stay in shared memory for the CTA's whole run (persistent
+// CTAs).  Halo rows are computed and discarded: the epilogue writes zeros
+// there, so the next layer's halo is zero.
+constexpr int kCvRows = 288, kCvLead = 80, kCvTile = 128;
+
+__host__ __device__ constexpr int cv_delta(int o) { return (o % 3 - 1) + 8 * ((o / 3) % 3 - 1) + 64 * (o / 9 - 1); }
+
+struct ConvTcArgs {
+    const bf16* in;        // planar input [n][p_in][512][8]
+    int p_in;              // input planes: 1 (8 channels) or 4 (32)
+    const bf16* w;         // [32][27 * 8 * p_in], k = offset * 8 p_in + channel
+    const float* bias;     // [32]
+    int n;                 // genomes
+    bf16* out_planar;      // [n][4][512][8] or null
+    bf16* out_compact;     // [n][216][32] (voxel x + 6y + 36z) or null
+    uint32_t* err;
+};
+
+template <int P>
+__global__ void __launch_bounds__(128) conv_tc_kernel(const ConvTcArgs g) {
+    extern __shared__ __align__(1024) uint8_t cv_smem[];
+    __shared__ __align__(8) uint64_t bars[2];
+    __shared__ uint32_t tmem_slot;
+    constexpr int K = 27 * 8 * P;
+    constexpr int kWChunks = P == 1 ? 28 : K / 8;           // 8-element k chunks (one zero chunk pads K = 216)
+    constexpr uint32_t kWBytes = kWChunks * 512;             // 32 rows = 4 row groups x 128 B per chunk
+    constexpr uint32_t kABytes = P * kCvRows * 16;
+    constexpr uint32_t kPlane = kCvRows * 16;                // plane stride inside an A buffer
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    uint8_t* sw = cv_smem;
+    uint8_t* sa[2] = {cv_smem + kWBytes, cv_smem + kWBytes + kABytes};
+    const int tiles = g.n * (512 / kCvTile);
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&bars[0])));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&bars[1])));
+    }
+    if (warp == 0) {  // two 32-column accumulators: tile i uses columns 32 (i & 1)
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&tmem_slot)),
+                     "r"(64u));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+    }
+    // weights, in the K-major core-matrix layout: chunk c of row n at (c*4 + n/8)*128 + (n%8)*16
+    for (int i = tid; i < kWChunks * 32; i += 128) {
+        const int c = i >> 5, row = i & 31;
+        const bool ok = c * 8 < K;
+        cp_async16(sw + (c * 4 + row / 8) * 128 + (row % 8) * 16, ok ? g.w + (size_t)row * K + c * 8 : g.w, ok);
+    }
+    auto load_a = [&](int t, uint8_t* dst) {
+        const int b = t >> 2, r0 = (t & 3) * kCvTile;
+        for (int i = tid; i < P * kCvRows; i += 128) {
+            const int plane = i / kCvRows, rr = i - plane * kCvRows, row = r0 - kCvLead + rr;
+            const bool ok = row >= 0 && row < 512;
+            cp_async16(dst + plane * kPlane + rr * 16, ok ? g.in + (((size_t)b * P + plane) * 512 + row) * 8 : g.in, ok);
+        }
+    };
+    // epilogue of tile t from accumulator `acc`: row p of genome b from TMEM lane 32*warp + lane
+    auto epilogue = [&](int t, uint32_t acc) {
+        const int b = t >> 2, p = (t & 3) * kCvTile + warp * 32 + lane;
+        const int x = p % 8 - 1, y = (p / 8) % 8 - 1, z = p / 64 - 1;
+        const bool real = x >= 0 && x < 6 && y >= 0 && y < 6 && z >= 0 && z < 6;
+        const int v = x + 6 * y + 36 * z;
+#pragma unroll
+        for (int c0 = 0; c0 < 32; c0 += 8) {
+            uint32_t r[8];
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
+                         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                           "=r"(r[7])
+                         : "r"(acc + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0));
+            asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+            alignas(16) bf16 h[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j)
+                h[j] = __float2bfloat16_rn(real ? fmaxf(__uint_as_float(r[j]) + g.bias[c0 + j], 0.0f) : 0.0f);
+            const uint4 pk = *reinterpret_cast<const uint4*>(h);
+            if (g.out_planar) *reinterpret_cast<uint4*>(g.out_planar + (((size_t)b * 4 + c0 / 8) * 512 + p) * 8) = pk;
+            if (g.out_compact && real)
+                *reinterpret_cast<uint4*>(g.out_compact + ((size_t)b * 216 + v) * 32 + c0) = pk;
+        }
+    };
+    int t = blockIdx.x;
+    if (t < tiles) load_a(t, sa[0]);
+    cp_async_commit();
+    cp_async_wait_all();
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+    const uint32_t tmem = tmem_slot;
+    const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | (4u << 17) | (8u << 24);  // f32 <- bf16 x bf16, N 32, M 128
+    // Tile i: MMAs into accumulator i & 1 (commit on bars[i & 1], its
+    // (i >> 1)-th phase); meanwhile the epilogue of tile i - 1 and the load
+    // of tile i + 1 (into the A buffer tile i - 1 used).
+    bool ok = true;
+    int prev = -1;  // tile of the previous iteration, its epilogue pending
+    int i = 0;
+    for (; t < tiles; t += gridDim.x, ++i) {
+        const int s = i & 1;
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+            const uint32_t a0 = smem_u32(sa[s]), w0 = smem_u32(sw), d = tmem + 32u * (uint32_t)s;
+            auto mma = [&](uint64_t da, uint64_t db, uint32_t acc) {
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(d),
+                    "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+            };
+            // descriptors are linear in the start-address field (address >> 4):
+            // each MMA adds a compile-time byte offset >> 4 to a base
+            if (P == 4) {
+                const uint64_t da0 = umma_desc(a0, kPlane, 128), db0 = umma_desc(w0, 512, 128);
+#pragma unroll
+                for (int o = 0; o < 27; ++o) {
+#pragma unroll
+                    for (int q = 0; q < 2; ++q)
+                        mma(da0 + ((2 * q * kPlane + (kCvLead + cv_delta(o)) * 16) >> 4),
+                            db0 + (((o * 4 + 2 * q) * 512) >> 4), (o | q) ? 1u : 0u);
+                }
+            } else {
+                const uint64_t da0 = umma_desc(a0, 0, 128), db0 = umma_desc(w0, 512, 128);
+#pragma unroll
+                for (int pr = 0; pr < 14; ++pr) {
+                    const int o1 = 2 * pr, o2 = 2 * pr + 1;
+                    const int d1 = cv_delta(o1), d2 = o2 < 27 ? cv_delta(o2) : d1 + 1;  // offset 27: zero weights
+                    mma(da0 + ((uint64_t)(kCvLead + d1) * 16 >> 4) + ((uint64_t)(d2 - d1) << 16),
+                        db0 + ((2 * pr * 512) >> 4), pr ? 1u : 0u);
+                }
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                smem_u32(&bars[s])));
+        }
+        if (prev >= 0) {
+            // the previous tile's MMAs: done reading its A buffer, accumulator ready
+            const bool w = mbar_wait(smem_u32(&bars[s ^ 1]), (uint32_t)((i - 1) >> 1) & 1u);
+            if (!__syncthreads_and(w)) {
+                ok = false;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+            epilogue(prev, tmem + 32u * (uint32_t)(s ^ 1));
+        }
+        const int nt = t + gridDim.x;
+        if (nt < tiles) load_a(nt, sa[s ^ 1]);
+        cp_async_commit();
+        cp_async_wait_all();
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+        __syncthreads();
+        prev = t;
+    }
+    if (ok && prev >= 0) {  // the last tile
+        const bool w = mbar_wait(smem_u32(&bars[(i - 1) & 1]), (uint32_t)((i - 1) >> 1) & 1u);
+        ok = __syncthreads_and(w);
+        if (ok) {
+            asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+            epilogue(prev, tmem + 32u * (uint32_t)((i - 1) & 1));
+        }
+    } else if (!ok) {
+        // drain: the tile issued in the iteration that failed
+        mbar_wait(smem_u32(&bars[i & 1]), (uint32_t)(i >> 1) & 1u);
+    }
+    cp_async_wait_all();
+    if (!ok && tid == 0) atomicAdd(g.err, 1u);
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(64u));
+    }
+}
+
+// One-hot classes on the padded planar grid (8 channels, zero halo).
+__global__ void onehot_planar_kernel(const uint8_t* __restrict__ cls, uint32_t n, bf16* __restrict__ x) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n * 512; i += gridDim.x * blockDim.x) {
+        const uint32_t b = i / 512, p = i % 512;
+        const int xx = (int)(p % 8) - 1, yy = (int)((p / 8) % 8) - 1, zz = (int)(p / 64) - 1;
+        uint32_t c = 0xFFu;
+        if (xx >= 0 && xx < 6 && yy >= 0 && yy < 6 && zz >= 0 && zz < 6) c = cls[b * 216 + xx + 6 * yy + 36 * zz];
+        alignas(16) bf16 h[8];
+#pragma unroll
+        for (uint32_t k = 0; k < 8; ++k) h[k] = __float2bfloat16_rn(c == k && c < 5 ? 1.0f : 0.0f);
+        *reinterpret_cast<uint4*>(x + (size_t)i * 8) = *reinterpret_cast<const uint4*>(h);
     }
 }
 
@@ -494,8 +701,24 @@ cudaError_t gemm(GemmArgs g, int splits, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+template <int P>
+cudaError_t conv_tc(const ConvTcArgs& g, int num_sms, cudaStream_t s) {
+    constexpr uint32_t smem = (P == 1 ? 28 : 27 * P) * 512 + 2 * P * kCvRows * 16;
+    static bool prepared = false;
+    if (!prepared) {
+        cudaError_t e = cudaFuncSetAttribute(conv_tc_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        prepared = true;
+    }
+    const int tiles = g.n * 4;
+    if (tiles == 0) return cudaSuccess;
+    const int grid = std::min(tiles, (P == 1 ? 4 : 2) * num_sms);
+    conv_tc_kernel<P><<<grid, 128, smem, s>>>(g);
+    return cudaGetLastError();
+}
+
 template <int AV, int BN>
-cudaError_t gemm_tc(const GemmArgs& g, uint32_t* err, cudaStream_t s) {
+cudaError_t gemm_tc(GemmArgs g, uint32_t* err, cudaStream_t s, int splits = 1) {
     static bool prepared = false;
     if (!prepared) {
         cudaError_t e = cudaFuncSetAttribute(gemm_tc_kernel<AV, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -504,7 +727,15 @@ cudaError_t gemm_tc(const GemmArgs& g, uint32_t* err, cudaStream_t s) {
         prepared = true;
     }
     if (g.M <= 0 || g.N <= 0) return cudaSuccess;
-    gemm_tc_kernel<AV, BN><<<(g.M + kTcM - 1) / kTcM, kTcThreads, tc_smem_bytes<BN>(), s>>>(g, err);
+    splits = std::max(1, std::min<int>(splits, (int)(g.partial_cap / ((size_t)g.M * g.N))));
+    g.k_chunk = ((g.K + splits - 1) / splits + kTcK - 1) / kTcK * kTcK;
+    splits = std::max(1, (g.K + g.k_chunk - 1) / g.k_chunk);
+    const dim3 grid((g.M + kTcM - 1) / kTcM, splits);
+    gemm_tc_kernel<AV, BN><<<grid, kTcThreads, tc_smem_bytes<BN>(), s>>>(g, err);
+    if (splits > 1) {
+        const size_t n = (size_t)g.M * g.N;
+        splitk_reduce_kernel<<<(unsigned)std::min<size_t>((n + 255) / 256, 4096), 256, 0, s>>>(g, splits);
+    }
     return cudaGetLastError();
 }
 
@@ -570,7 +801,9 @@ struct mb_surrogate {
     uint64_t step = 0;
     float weight_decay = 0.0f;
     bool tcgen05 = true;   // forward GEMMs on the 5th-generation tensor cores
+    int num_sms = 148;
     Buf<uint32_t> tc_err;
+    Buf<bf16> x0p, a1p, a2p;  // padded planar activations of the tcgen05 convolutions
     Buf<float> w, m, v, g, loss, y, t, partial;
     Buf<bf16> wb, wt2, wt3, x0, a1, a2, a3, h1, h2, dz2h, dz1h, dz3, dz2c, dz1c;
     Buf<uint8_t> cls;
@@ -629,16 +862,32 @@ cudaError_t forward(mb_surrogate* s, uint32_t n) {
         a.c16 = out;
         return s->tcgen05 ? gemm_tc<kIm2col, 32>(a, s->tc_err.p, st) : gemm<kIm2col, kDenseK>(a, 1, st);
     };
+    // the flatten layer: K = 6912 split over CTAs (M is only the batch);
+    // the 128 x 128 layer is too small for the tensor-memory set-up to pay
     auto fc = [&](const bf16* x, int k, Tensor w, Tensor b, bf16* out) {
         GemmArgs a = args(s, x, k, PB(s, w), k, (int)n, 128, k);
         a.bias = P(s, b);
         a.relu = 1;
         a.c16 = out;
-        return s->tcgen05 ? gemm_tc<kDenseK, 128>(a, s->tc_err.p, st) : gemm<kDenseK, kDenseK>(a, 1, st);
+        if (s->tcgen05 && k > 1024) {
+            const int mt = ((int)n + kTcM - 1) / kTcM;
+            return gemm_tc<kDenseK, 128>(a, s->tc_err.p, st, std::max(1, std::min(k / kTcK / 4, 2 * s->num_sms / mt)));
+        }
+        return gemm<kDenseK, kDenseK>(a, 1, st);
     };
-    if ((e = conv(s->x0.p, 8, kW1, kB1, s->a1.p)) != cudaSuccess) return e;
-    if ((e = conv(s->a1.p, 32, kW2, kB2, s->a2.p)) != cudaSuccess) return e;
-    if ((e = conv(s->a2.p, 32, kW3, kB3, s->a3.p)) != cudaSuccess) return e;
+    if (s->tcgen05) {
+        onehot_planar_kernel<<<std::min<uint32_t>((n * 512 + 255) / 256, 4096), 256, 0, st>>>(s->cls.p, n, s->x0p.p);
+        const ConvTcArgs c1{s->x0p.p, 1, PB(s, kW1), P(s, kB1), (int)n, s->a1p.p, s->a1.p, s->tc_err.p};
+        const ConvTcArgs c2{s->a1p.p, 4, PB(s, kW2), P(s, kB2), (int)n, s->a2p.p, s->a2.p, s->tc_err.p};
+        const ConvTcArgs c3{s->a2p.p, 4, PB(s, kW3), P(s, kB3), (int)n, nullptr, s->a3.p, s->tc_err.p};
+        if ((e = conv_tc<1>(c1, s->num_sms, st)) != cudaSuccess) return e;
+        if ((e = conv_tc<4>(c2, s->num_sms, st)) != cudaSuccess) return e;
+        if ((e = conv_tc<4>(c3, s->num_sms, st)) != cudaSuccess) return e;
+    } else {
+        if ((e = conv(s->x0.p, 8, kW1, kB1, s->a1.p)) != cudaSuccess) return e;
+        if ((e = conv(s->a1.p, 32, kW2, kB2, s->a2.p)) != cudaSuccess) return e;
+        if ((e = conv(s->a2.p, 32, kW3, kB3, s->a3.p)) != cudaSuccess) return e;
+    }
     if ((e = fc(s->a3.p, 6912, kW4, kB4, s->h1.p)) != cudaSuccess) return e;
     if ((e = fc(s->h1.p, 128, kW5, kB5, s->h2.p)) != cudaSuccess) return e;
     head_kernel<<<(n + 7) / 8, 256, 0, st>>>(s->h2.p, PB(s, kW6), P(s, kB6), n, s->y.p);
@@ -769,9 +1018,12 @@ mb_status mb_surrogate_create(int device, uint32_t max_batch, uint64_t seed, mb_
           ok(s->a2.alloc(R * 32)) && ok(s->a3.alloc(R * 32)) && ok(s->h1.alloc((size_t)max_batch * 128)) &&
           ok(s->h2.alloc((size_t)max_batch * 128)) && ok(s->dz2h.alloc((size_t)max_batch * 128)) &&
           ok(s->dz1h.alloc((size_t)max_batch * 128)) && ok(s->dz3.alloc(R * 32)) && ok(s->dz2c.alloc(R * 32)) &&
-          ok(s->dz1c.alloc(R * 32)) && ok(s->cls.alloc(R)) && ok(s->tc_err.alloc(1))))
+          ok(s->dz1c.alloc(R * 32)) && ok(s->cls.alloc(R)) && ok(s->tc_err.alloc(1)) &&
+          ok(s->x0p.alloc((size_t)max_batch * 512 * 8)) && ok(s->a1p.alloc((size_t)max_batch * 4 * 512 * 8)) &&
+          ok(s->a2p.alloc((size_t)max_batch * 4 * 512 * 8))))
         return MB_ERR_CUDA;
     if (cudaMemset(s->tc_err.p, 0, sizeof(uint32_t)) != cudaSuccess) return MB_ERR_CUDA;
+    if (cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return MB_ERR_CUDA;
     // He-normal weights (fan-in of the real inputs), zero biases, zero
     // weights on the padding channels of W1; Box-Muller over SplitMix64.
     std::vector<float> w(np, 0.0f);
