@@ -71,21 +71,25 @@ def _time(sim, steps: int, track: bool) -> float:
 
 
 def tune(sim, batch, track: bool = False, steps: int = 300, use_cache: bool = True,
-         sms: int | None = None, verbose: bool = False) -> dict:
+         sms: int | None = None, verbose: bool = False, upload=None, key: str | None = None) -> dict:
     """Picks and applies the fastest launch configuration for `batch` on
     `sim` (a Simulator whose mode, materials and time step are set).  Returns
-    {"config": ..., "rate": spring-updates/s, "candidates": [...]}."""
+    {"config": ..., "rate": spring-updates/s, "candidates": [...]}.
+    `upload` (default: sim.set_batch(batch)) re-uploads the population after
+    each configuration change -- e.g. Simulator.set_voxel_population for a
+    population built on the device -- and `key` replaces the cache key."""
     import torch
 
     mode = ctypes.c_int()
     _lib.check(_lib.LIB.mb_get_mode(sim._ctx, ctypes.byref(mode)), sim._ctx)
     dt = sim.getDeltaT()
-    key = signature(batch, mode.value, track, dt)
+    upload = upload or (lambda: sim.set_batch(batch))
+    key = key or signature(batch, mode.value, track, dt)
     cache = _load_cache() if use_cache else {}
     if key in cache:
         cfg = cache[key]["config"]
         sim.set_launch_config(**cfg)
-        sim.set_batch(batch)
+        upload()
         return cache[key]
 
     if sms is None:
@@ -101,7 +105,7 @@ def tune(sim, batch, track: bool = False, steps: int = 300, use_cache: bool = Tr
                        use_graph=1, streamed=shape["streamed"])
             try:
                 sim.set_launch_config(**cfg)
-                sim.set_batch(batch)
+                upload()
             except _lib.MercuryError:
                 continue
             got = sim.launch_config()
@@ -118,7 +122,7 @@ def tune(sim, batch, track: bool = False, steps: int = 300, use_cache: bool = Tr
     best = max(cands, key=lambda c: c["rate"])
     cfg = dict(best["config"])
     sim.set_launch_config(**cfg)
-    sim.set_batch(batch)  # fresh state: tuning runs advanced the old one
+    upload()  # fresh state: tuning runs advanced the old one
     _lib.check(_lib.LIB.mb_set_total_time(sim._ctx, t0), sim._ctx)
     res = {"config": cfg, "rate": best["rate"], "candidates": cands}
     if use_cache:

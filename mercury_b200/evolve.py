@@ -71,10 +71,12 @@ class Evaluator:
     """Simulates genomes on one GPU; one Simulator per batch size so that
     each keeps its packing plan."""
 
-    def __init__(self, device: int = 0, duration: float = DURATION):
+    def __init__(self, device: int = 0, duration: float = DURATION, autotune: bool = True):
         self.device = device
         self.duration = duration
+        self.autotune = autotune
         self._sims: dict[int, S.Simulator] = {}
+        self._tuned: dict[int, dict] = {}
         self.simulated = 0
 
     def _sim(self, n: int) -> S.Simulator:
@@ -91,7 +93,15 @@ class Evaluator:
     def __call__(self, genomes: np.ndarray) -> np.ndarray:
         n = len(genomes)
         sim = self._sim(n)
-        sim.set_voxel_population(to_cells(genomes), CELL, MASS)
+        cells = to_cells(genomes)
+        if self.autotune and n not in self._tuned:
+            # launch configuration for this batch size, tuned once on these
+            # genomes (the packing plan is per batch size and grid)
+            from . import autotune
+            sim.set_voxel_population(cells, CELL, MASS)
+            up = lambda: sim.set_voxel_population(cells, CELL, MASS)  # noqa: E731
+            self._tuned[n] = autotune.tune(sim, sim.batch, steps=300, upload=up, use_cache=False)["config"]
+        sim.set_voxel_population(cells, CELL, MASS)
         sim.Reset()
         com0 = sim.CentreOfMass()
         steps = sim.Simulate(self.duration)
