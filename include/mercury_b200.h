@@ -273,6 +273,9 @@ typedef struct mb_plan_stats {
     uint64_t masses, active_springs, incidence_entries, incidence_padding;
     uint32_t aligned_slices, rank_slices, material_slots;
     uint32_t max_bin_springs, min_bin_springs;
+    /* CTAs of a step launch (CTA g runs bins g, g + ctas, ...) and the
+     * largest / smallest number of springs one CTA runs per step */
+    uint32_t ctas, max_cta_springs, min_cta_springs;
 } mb_plan_stats;
 MB_API mb_status mb_plan_population(const mb_batch_desc* batch, const mb_launch_config* cfg,
                                     uint32_t num_sms, uint32_t smem_bytes, mb_plan_stats* stats);

@@ -61,7 +61,8 @@ class PlanStats(ctypes.Structure):
                [(n, ctypes.c_uint64) for n in ("masses", "active_springs", "incidence_entries",
                                                "incidence_padding")] + \
                [(n, ctypes.c_uint32) for n in ("aligned_slices", "rank_slices", "material_slots",
-                                               "max_bin_springs", "min_bin_springs")]
+                                               "max_bin_springs", "min_bin_springs",
+                                               "ctas", "max_cta_springs", "min_cta_springs")]
 
 
 class LaunchConfig(ctypes.Structure):

@@ -124,6 +124,7 @@ struct mb_context {
     // packing result
     mb::KernelShape shape{512, 8, 2};
     uint32_t n_bins = 0;
+    uint32_t grid = 0;  // CTAs per step launch (0 = one per bin)
     uint32_t chunk = 1000;
     bool use_graph = true;
     uint32_t smem_bytes = 0;
@@ -305,6 +306,7 @@ mb_status upload_packed(mb_context* ctx, const mb::Packed& out) {
     ctx->clear_graphs();
     ctx->shape = out.shape;
     ctx->n_bins = out.n_bins;
+    ctx->grid = out.grid;
     ctx->smem_bytes = out.max_smem;
     ctx->streamed = out.streamed;
     ctx->stream_mpt = out.shape.mpt;
@@ -728,6 +730,12 @@ mb_status mb_plan_population(const mb_batch_desc* batch, const mb_launch_config*
     }
     stats->max_bin_springs = mx;
     stats->min_bin_springs = out.bins.empty() ? 0 : mn;
+    const uint32_t ctas = out.grid ? std::min(out.grid, out.n_bins) : out.n_bins;
+    std::vector<uint64_t> per(ctas, 0);
+    for (size_t b = 0; b < out.bins.size(); ++b) per[b % ctas] += out.bins[b].n_spring;
+    stats->ctas = ctas;
+    stats->max_cta_springs = per.empty() ? 0 : (uint32_t)*std::max_element(per.begin(), per.end());
+    stats->min_cta_springs = per.empty() ? 0 : (uint32_t)*std::min_element(per.begin(), per.end());
     return MB_OK;
 }
 
@@ -860,6 +868,7 @@ mb::StepParams make_params(mb_context* c, float t0, uint32_t steps, bool track) 
     mb::StepParams p{};
     p.bins = c->bins.p;
     p.n_bins = c->n_bins;
+    p.grid = c->grid;
     p.pos = c->pos.p;
     p.vel = c->vel.p;
     p.stress = c->stress.p;

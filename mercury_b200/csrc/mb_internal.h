@@ -33,14 +33,14 @@ struct BinDesc {
 struct StepParams {
     const BinDesc* bins;
     uint32_t n_bins;
+    uint32_t grid;                // CTAs of the launch (bins g, g + grid, ... on CTA g); 0 = n_bins
     float4* pos;                  // upload layout, w = mass
     float4* vel;                  // upload layout
     float* stress;                // upload layout, one per spring
     const uint32_t* mass_gidx;    // packed mass -> upload index
     const uint32_t* spring_gidx;  // packed spring -> upload index
-    const uint32_t* spring_pair;  // packed spring: a | b << 16 (bin-local)
+    const uint32_t* spring_pair;  // packed spring: a | b << 12 | material slot << 24 (bin-local)
     const float* spring_lbar;     // packed spring mean length
-    const uint8_t* spring_slot;   // packed spring material slot (bin-local)
     const uint32_t* slice_off;    // per slice: first entry relative to bin inc_begin
     const uint32_t* slice_width;  // per slice: entries per mass (row length)
     const uint16_t* inc;          // incidence entries: spring << 1 | (b end), or kPadEntry

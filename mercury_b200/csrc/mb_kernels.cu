@@ -83,6 +83,32 @@ __device__ __forceinline__ void force_integrate(const StepParams& p, float3& x, 
     x = make_float3(nx, ny, nz);
 }
 
+// Velocity of the reference step, v = (float)(0.99 * (double)delta / (double)dt)
+// (sim_kernel.cu:265-267): the double product, the correctly rounded double
+// quotient, then rounding to float -- without a double division in the
+// common case.  q = RN(a * inv_dt), with inv_dt = RN(1/dt), differs from
+// the exact a/dt by at most 2u + u^2 relative (u = 2^-53), so from the
+// correctly rounded quotient by less than 3.01 units in the last place of
+// q.  Rounding to float can only differ between q and that quotient if a
+// float rounding boundary -- the midpoint between two floats, whose low 29
+// significand bits are 1 << 28 in double -- lies between them.  So when
+// q's low 29 bits are more than 4 units from 1 << 28 and q lies in the
+// normal float range, (float)q is the result (Ziv's rounding test: Ziv,
+// "Fast evaluation of elementary mathematical functions with correctly
+// rounded last bit", ACM TOMS 17(3), 1991); otherwise -- about 9 inputs in
+// 2^29, zeros excepted -- the division itself is done.
+__device__ __forceinline__ float velocity_of(float delta, double dt, double inv_dt) {
+    const double a = __dmul_rn(0.99, (double)delta);
+    const double q = __dmul_rn(a, inv_dt);
+    const unsigned long long bits = (unsigned long long)__double_as_longlong(q);
+    const uint32_t e = (uint32_t)(bits >> 52) & 0x7FFu;
+    const uint32_t low29 = (uint32_t)bits & 0x1FFFFFFFu;
+    // normal float range 2^-126 <= |q| < 2^127 (biased double exponents 897..1149)
+    const bool clear = (e - 897u) < 253u && (low29 - (0x10000000u - 4u)) > 8u;
+    if (clear || (bits << 1) == 0) return __double2float_rn(q);
+    return __double2float_rn(__ddiv_rn(a, dt));
+}
+
 template <int T, int SPT, int MPT, int MODE, bool TRACK>
 __global__ void __launch_bounds__(T, 1024 / T) step_kernel(const StepParams p) {
     constexpr bool XPBD = MODE == kModeXpbd;
@@ -90,6 +116,7 @@ __global__ void __launch_bounds__(T, 1024 / T) step_kernel(const StepParams p) {
     const int tid = threadIdx.x;
     const float dt = p.dt;
     const double ddt = (double)dt;
+    const double inv_dt = __drcp_rn(ddt);
 
     for (uint32_t b = blockIdx.x; b < p.n_bins; b += gridDim.x) {
         const BinDesc bd = p.bins[b];
@@ -214,9 +241,9 @@ __global__ void __launch_bounds__(T, 1024 / T) step_kernel(const StepParams p) {
                     const float ny = __fadd_rn(xt.y, ay);
                     const float nz = __fadd_rn(xt.z, az);
                     // v = 0.99*(x~ - x)/dt in double (sim_kernel.cu:265-267)
-                    v[j].x = __double2float_rn(__ddiv_rn(__dmul_rn(0.99, (double)__fsub_rn(nx, x[j].x)), ddt));
-                    v[j].y = __double2float_rn(__ddiv_rn(__dmul_rn(0.99, (double)__fsub_rn(ny, x[j].y)), ddt));
-                    v[j].z = __double2float_rn(__ddiv_rn(__dmul_rn(0.99, (double)__fsub_rn(nz, x[j].z)), ddt));
+                    v[j].x = velocity_of(__fsub_rn(nx, x[j].x), ddt, inv_dt);
+                    v[j].y = velocity_of(__fsub_rn(ny, x[j].y), ddt, inv_dt);
+                    v[j].z = velocity_of(__fsub_rn(nz, x[j].z), ddt, inv_dt);
                     x[j] = make_float3(nx, ny, nz);
                 } else {
                     force_integrate<MODE>(p, x[j], v[j], mass[j], ax, ay, az);
@@ -261,6 +288,7 @@ __global__ void __launch_bounds__(T, 1024 / T) stream_kernel(const StepParams p)
     const int tid = threadIdx.x;
     const float dt = p.dt;
     const double ddt = (double)dt;
+    const double inv_dt = __drcp_rn(ddt);
 
     for (uint32_t b = blockIdx.x; b < p.n_bins; b += gridDim.x) {
         const BinDesc bd = p.bins[b];
@@ -359,9 +387,9 @@ __global__ void __launch_bounds__(T, 1024 / T) stream_kernel(const StepParams p)
                     const float nx = __fadd_rn(xt.x, ax);
                     const float ny = __fadd_rn(xt.y, ay);
                     const float nz = __fadd_rn(xt.z, az);
-                    v[j].x = __double2float_rn(__ddiv_rn(__dmul_rn(0.99, (double)__fsub_rn(nx, x[j].x)), ddt));
-                    v[j].y = __double2float_rn(__ddiv_rn(__dmul_rn(0.99, (double)__fsub_rn(ny, x[j].y)), ddt));
-                    v[j].z = __double2float_rn(__ddiv_rn(__dmul_rn(0.99, (double)__fsub_rn(nz, x[j].z)), ddt));
+                    v[j].x = velocity_of(__fsub_rn(nx, x[j].x), ddt, inv_dt);
+                    v[j].y = velocity_of(__fsub_rn(ny, x[j].y), ddt, inv_dt);
+                    v[j].z = velocity_of(__fsub_rn(nz, x[j].z), ddt, inv_dt);
                     x[j] = make_float3(nx, ny, nz);
                 } else {
                     force_integrate<MODE>(p, x[j], v[j], mass[j], ax, ay, az);
@@ -612,7 +640,8 @@ cudaError_t launch_step(const StepParams& p, const KernelShape& shape, cudaStrea
     if (!e) return cudaErrorInvalidValue;
     if (p.n_bins == 0) return cudaSuccess;
     if (p.mode > kModeForceWater) return cudaErrorInvalidValue;
-    e->fn[p.mode][p.track ? 1 : 0]<<<p.n_bins, shape.threads, p.smem_bytes, s>>>(p);
+    const uint32_t grid = p.grid ? std::min(p.grid, p.n_bins) : p.n_bins;
+    e->fn[p.mode][p.track ? 1 : 0]<<<grid, shape.threads, p.smem_bytes, s>>>(p);
     return cudaGetLastError();
 }
 

@@ -5,7 +5,10 @@
 // robots keep their own sizes and are grouped into bins, each simulated by
 // one CTA; bins are filled largest-robot-first onto the least loaded bin
 // (LPT), and the bin count is a whole number of waves (SMs x resident CTAs
-// per SM) so that every SM gets the same work.  Inside a bin:
+// per SM) so that every SM gets the same work.  With two or more waves the
+// launch has one CTA per group of bins that runs them one after another,
+// and robots are balanced over the groups first (plan_bins_grouped): a
+// group's load is what sets its SM's time.  Inside a bin:
 //   - masses keep robot order (robot r's masses, then robot r+1's ...);
 //   - non-air springs are sorted by (b - a, a) so that a warp's springs read
 //     consecutive positions (for a lattice: one direction, consecutive a);
@@ -161,6 +164,65 @@ bool plan_bins(const std::vector<RobotPack>& packs, uint32_t nb, const KernelSha
         bs[best] += p.springs.size();
         bi[best] += p.inc_estimate;
         plan[best].push_back(r);
+    }
+    for (auto& v : plan) std::sort(v.begin(), v.end());
+    return true;
+}
+
+// Two-level LPT for launches of more than one wave.  A launch of `groups`
+// CTAs runs bins g, g + groups, g + 2 groups ... one after another on CTA g,
+// so what has to be even is the load of a group, not of a bin: robots are
+// first spread over the groups by LPT (a group holds nb / groups bins'
+// capacity), then each group's robots are spread over its own bins by LPT
+// under the per-bin limits.  Returns false when a group cannot be split,
+// and the caller falls back to plan_bins.
+bool plan_bins_grouped(const std::vector<RobotPack>& packs, uint32_t nb, uint32_t groups,
+                       const KernelShape& sh, uint32_t smem_cap,
+                       std::vector<std::vector<uint32_t>>& plan) {
+    if (groups == 0 || nb <= groups || nb % groups) return false;
+    const uint32_t per = nb / groups;
+    const uint32_t n = (uint32_t)packs.size();
+    std::vector<uint32_t> order(n);
+    for (uint32_t i = 0; i < n; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](uint32_t a, uint32_t b) { return packs[a].cost > packs[b].cost; });
+    const uint64_t cap_s = std::min<uint64_t>((uint64_t)sh.threads * sh.spt, kMaxBinSprings);
+    const uint64_t cap_m = std::min<uint64_t>((uint64_t)sh.threads * sh.mpt, 4096);
+    std::vector<uint64_t> gload(groups, 0), gm(groups, 0), gs(groups, 0);
+    std::vector<std::vector<uint32_t>> members(groups);
+    for (uint32_t r : order) {
+        const auto& p = packs[r];
+        int best = -1;
+        for (uint32_t g = 0; g < groups; ++g) {
+            if (gm[g] + p.n_mass > per * cap_m || gs[g] + p.springs.size() > per * cap_s) continue;
+            if (best < 0 || gload[g] < gload[best]) best = (int)g;
+        }
+        if (best < 0) return false;
+        gload[best] += p.cost;
+        gm[best] += p.n_mass;
+        gs[best] += p.springs.size();
+        members[best].push_back(r);  // descending cost within the group
+    }
+    plan.assign(nb, {});
+    for (uint32_t g = 0; g < groups; ++g) {
+        std::vector<uint64_t> load(per, 0), bm(per, 0), bs(per, 0), bi(per, 0);
+        for (uint32_t r : members[g]) {
+            const auto& p = packs[r];
+            int best = -1;
+            for (uint32_t j = 0; j < per; ++j) {
+                if (bm[j] + p.n_mass > cap_m || bs[j] + p.springs.size() > cap_s) continue;
+                if (bin_smem_bytes((uint32_t)(bm[j] + p.n_mass), (uint32_t)(bs[j] + p.springs.size()),
+                                   (uint32_t)(bi[j] + p.inc_estimate)) > smem_cap)
+                    continue;
+                if (best < 0 || load[j] < load[best]) best = (int)j;
+            }
+            if (best < 0) return false;
+            load[best] += p.cost;
+            bm[best] += p.n_mass;
+            bs[best] += p.springs.size();
+            bi[best] += p.inc_estimate;
+            plan[(size_t)best * groups + g].push_back(r);
+        }
     }
     for (auto& v : plan) std::sort(v.begin(), v.end());
     return true;
@@ -437,25 +499,38 @@ mb_status pack_population(const mb_batch_desc* b, const PackOptions& o, Packed& 
         uint32_t nb = o.override.bins;
         const bool fixed = nb != 0;
         uint32_t wave = sms;
+        if (R >= sms) {
+            // One wave = SMs x resident CTAs per SM; shared memory is
+            // estimated at the even share of the population.
+            const uint32_t est_smem = std::min<uint32_t>(
+                o.smem_cap, bin_smem_bytes((uint32_t)std::min<uint64_t>(cap_m, tot_m / sms + 1),
+                                           (uint32_t)std::min<uint64_t>(cap_s, tot_s / sms + 1),
+                                           (uint32_t)std::min<uint64_t>(3 * cap_s, 3 * (tot_s / sms + 1))));
+            const int per_sm = o.ctas_per_sm ? std::max(1, o.ctas_per_sm(sh, est_smem)) : 1;
+            wave = sms * (uint32_t)per_sm;
+        }
         if (!nb) {
             const uint64_t need = std::max<uint64_t>((tot_s + cap_s - 1) / cap_s, (tot_m + cap_m - 1) / cap_m);
             nb = (uint32_t)std::max<uint64_t>(need, 1);
             if (R >= sms) {
-                // One wave = SMs x resident CTAs per SM; shared memory is
-                // estimated at the even share of the population.
-                const uint32_t est_smem = std::min<uint32_t>(
-                    o.smem_cap, bin_smem_bytes((uint32_t)std::min<uint64_t>(cap_m, tot_m / sms + 1),
-                                               (uint32_t)std::min<uint64_t>(cap_s, tot_s / sms + 1),
-                                               (uint32_t)std::min<uint64_t>(3 * cap_s, 3 * (tot_s / sms + 1))));
-                const int per_sm = o.ctas_per_sm ? std::max(1, o.ctas_per_sm(sh, est_smem)) : 1;
-                wave = sms * (uint32_t)per_sm;
                 nb = std::max<uint32_t>(nb, wave);
                 nb = (nb + wave - 1) / wave * wave;  // whole waves
             }
             nb = std::min<uint32_t>(nb, R);
         }
+        uint32_t grid = 0;
         for (uint32_t tries = 0; tries < 16; ++tries) {
-            if (plan_bins(packs, nb, sh, o.smem_cap, plan)) {
+            // Several waves: one CTA per group of bins, groups balanced
+            // (plan_bins_grouped); otherwise one CTA per bin.
+            grid = 0;
+            bool planned = false;
+            if (R >= sms && nb >= 2 * wave && nb % wave == 0 &&
+                plan_bins_grouped(packs, nb, wave, sh, o.smem_cap, plan)) {
+                planned = true;
+                grid = wave;
+            }
+            if (!planned) planned = plan_bins(packs, nb, sh, o.smem_cap, plan);
+            if (planned) {
                 build_all(b, packs, plan, slot_of, false, threads, out);
                 if (out.max_smem <= o.smem_cap) {
                     ok = true;
@@ -468,6 +543,7 @@ mb_status pack_population(const mb_batch_desc* b, const PackOptions& o, Packed& 
         if (ok) {
             out.shape = sh;
             out.n_bins = nb;
+            out.grid = grid;
             out.streamed = false;
             break;
         }
@@ -485,6 +561,7 @@ mb_status pack_population(const mb_batch_desc* b, const PackOptions& o, Packed& 
                 out.streamed = true;
                 out.shape = KernelShape{1024, 0, mpt};
                 out.n_bins = R;
+                out.grid = 0;
             }
         }
     }

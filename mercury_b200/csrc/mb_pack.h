@@ -25,6 +25,7 @@ struct PackOptions {
 struct Packed {
     KernelShape shape{0, 0, 0};
     uint32_t n_bins = 0;
+    uint32_t grid = 0;  // CTAs per launch, CTA g running bins g, g + grid, ...; 0 = one per bin
     bool streamed = false;
     uint32_t max_smem = 0;
     std::vector<BinDesc> bins;
