@@ -44,22 +44,26 @@ __device__ __forceinline__ uint32_t pk_slot(uint32_t w) { return w >> 24; }
 //          cancels the horizontal motion, F_h = -m v_h/dt) when |h| <= mu_s fn
 //          dt/m, else kinetic, mu_k fn against h.
 //   water: gravity balanced by buoyancy; quadratic drag -drag |v| v.
+// Divisions by m and dt are multiplications by the correctly rounded
+// reciprocals (inv_dt = RN(1/dt) per launch, RN(1/m) per mass and step);
+// only the kinetic friction divides.
 template <int MODE>
 __device__ __forceinline__ void force_integrate(const StepParams& p, float3& x, float3& v, float m,
-                                                float fx, float fy, float fz) {
+                                                float inv_dt, float fx, float fy, float fz) {
     const float dt = p.dt;
+    const float inv_m = __frcp_rn(m);
     if (MODE == kModeForceLand) {
         fz = __fsub_rn(fz, __fmul_rn(m, p.g));
         if (x.z < 0.0f) {
             const float fn = __fmul_rn(p.floor_stiffness, -x.z);
             fz = __fadd_rn(fz, fn);
-            const float hx = __fadd_rn(v.x, __fmul_rn(__fdiv_rn(fx, m), dt));
-            const float hy = __fadd_rn(v.y, __fmul_rn(__fdiv_rn(fy, m), dt));
+            const float hx = __fadd_rn(v.x, __fmul_rn(__fmul_rn(fx, inv_m), dt));
+            const float hy = __fadd_rn(v.y, __fmul_rn(__fmul_rn(fy, inv_m), dt));
             const float hs = __fsqrt_rn(__fmaf_rn(hx, hx, __fmul_rn(hy, hy)));
-            const float budget = __fmul_rn(__fdiv_rn(fn, m), dt);
+            const float budget = __fmul_rn(__fmul_rn(fn, inv_m), dt);
             if (hs <= __fmul_rn(p.mu_s, budget)) {
-                fx = __fdiv_rn(__fmul_rn(-m, v.x), dt);
-                fy = __fdiv_rn(__fmul_rn(-m, v.y), dt);
+                fx = __fmul_rn(__fmul_rn(-m, v.x), inv_dt);
+                fy = __fmul_rn(__fmul_rn(-m, v.y), inv_dt);
             } else {
                 const float s = __fdiv_rn(__fmul_rn(p.mu_k, fn), hs);
                 fx = __fsub_rn(fx, __fmul_rn(s, hx));
@@ -74,12 +78,12 @@ __device__ __forceinline__ void force_integrate(const StepParams& p, float3& x, 
         fz = __fsub_rn(fz, __fmul_rn(c, v.z));
     }
     const float dt2 = __fmul_rn(dt, dt);
-    const float nx = __fadd_rn(__fadd_rn(x.x, __fmul_rn(v.x, dt)), __fmul_rn(__fdiv_rn(fx, m), dt2));
-    const float ny = __fadd_rn(__fadd_rn(x.y, __fmul_rn(v.y, dt)), __fmul_rn(__fdiv_rn(fy, m), dt2));
-    const float nz = __fadd_rn(__fadd_rn(x.z, __fmul_rn(v.z, dt)), __fmul_rn(__fdiv_rn(fz, m), dt2));
-    v.x = __fmul_rn(p.damping, __fdiv_rn(__fsub_rn(nx, x.x), dt));
-    v.y = __fmul_rn(p.damping, __fdiv_rn(__fsub_rn(ny, x.y), dt));
-    v.z = __fmul_rn(p.damping, __fdiv_rn(__fsub_rn(nz, x.z), dt));
+    const float nx = __fadd_rn(__fadd_rn(x.x, __fmul_rn(v.x, dt)), __fmul_rn(__fmul_rn(fx, inv_m), dt2));
+    const float ny = __fadd_rn(__fadd_rn(x.y, __fmul_rn(v.y, dt)), __fmul_rn(__fmul_rn(fy, inv_m), dt2));
+    const float nz = __fadd_rn(__fadd_rn(x.z, __fmul_rn(v.z, dt)), __fmul_rn(__fmul_rn(fz, inv_m), dt2));
+    v.x = __fmul_rn(p.damping, __fmul_rn(__fsub_rn(nx, x.x), inv_dt));
+    v.y = __fmul_rn(p.damping, __fmul_rn(__fsub_rn(ny, x.y), inv_dt));
+    v.z = __fmul_rn(p.damping, __fmul_rn(__fsub_rn(nz, x.z), inv_dt));
     x = make_float3(nx, ny, nz);
 }
 
@@ -117,6 +121,7 @@ __global__ void __launch_bounds__(T, 1024 / T) step_kernel(const StepParams p) {
     const float dt = p.dt;
     const double ddt = (double)dt;
     const double inv_dt = __drcp_rn(ddt);
+    const float inv_dt_f = __frcp_rn(dt);
 
     for (uint32_t b = blockIdx.x; b < p.n_bins; b += gridDim.x) {
         const BinDesc bd = p.bins[b];
@@ -246,7 +251,7 @@ __global__ void __launch_bounds__(T, 1024 / T) step_kernel(const StepParams p) {
                     v[j].z = velocity_of(__fsub_rn(nz, x[j].z), ddt, inv_dt);
                     x[j] = make_float3(nx, ny, nz);
                 } else {
-                    force_integrate<MODE>(p, x[j], v[j], mass[j], ax, ay, az);
+                    force_integrate<MODE>(p, x[j], v[j], mass[j], inv_dt_f, ax, ay, az);
                 }
             }
         }
@@ -289,6 +294,7 @@ __global__ void __launch_bounds__(T, 1024 / T) stream_kernel(const StepParams p)
     const float dt = p.dt;
     const double ddt = (double)dt;
     const double inv_dt = __drcp_rn(ddt);
+    const float inv_dt_f = __frcp_rn(dt);
 
     for (uint32_t b = blockIdx.x; b < p.n_bins; b += gridDim.x) {
         const BinDesc bd = p.bins[b];
@@ -392,7 +398,7 @@ __global__ void __launch_bounds__(T, 1024 / T) stream_kernel(const StepParams p)
                     v[j].z = velocity_of(__fsub_rn(nz, x[j].z), ddt, inv_dt);
                     x[j] = make_float3(nx, ny, nz);
                 } else {
-                    force_integrate<MODE>(p, x[j], v[j], mass[j], ax, ay, az);
+                    force_integrate<MODE>(p, x[j], v[j], mass[j], inv_dt_f, ax, ay, az);
                 }
             }
         }

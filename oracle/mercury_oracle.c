@@ -400,6 +400,9 @@ int or_xpbd_run_f64(int n_robots, const int64_t* mass_off, double* pos, double* 
  * else kinetic mu_k fn against h; mode 2 (water): drag -c |v| v.  Then
  * x' = x + v dt + (F/m) dt^2, v' = damping (x' - x)/dt.  Stress accumulates
  * k (d - L)/Lbar.  The same fixed gather order as the reference step.
+ * In FP32 the divisions by m and dt are multiplications by the correctly
+ * rounded reciprocals 1/m and 1/dt (the law is this library's own, so its
+ * rounding is too); only the kinetic friction divides, by |h|.
  * env = {g, floor_stiffness, mu_s, mu_k, drag, damping}; m = pos.w. */
 static void force_robot_f32(int mode, int nm, float* pos, float* vel, int ns,
                             const uint16_t* pairs, const uint8_t* mat,
@@ -430,6 +433,7 @@ static void force_robot_f32(int mode, int nm, float* pos, float* vel, int ns,
     float* f = (float*)malloc(sizeof(float) * 3 * (size_t)(ns + 1));
     float rc[OR_COMPOSITE_COUNT];
     const float g = env[0], kfl = env[1], mus = env[2], muk = env[3], cdrag = env[4], damp = env[5];
+    const float inv_dt = 1.0f / dt;
     volatile float t = t0;
     for (uint32_t step = 0; step < steps; ++step) {
         float tn = t;
@@ -463,18 +467,19 @@ static void force_robot_f32(int mode, int nm, float* pos, float* vel, int ns,
             float* x = pos + 4 * i;
             float* v = vel + 4 * i;
             float mass = x[3];
+            float inv_m = 1.0f / mass;
             if (mode == 1) {
                 F[2] = F[2] - mass * g;
                 if (x[2] < 0.0f) {
                     float fn = kfl * (-x[2]);
                     F[2] = F[2] + fn;
-                    float hx = v[0] + (F[0] / mass) * dt;
-                    float hy = v[1] + (F[1] / mass) * dt;
+                    float hx = v[0] + (F[0] * inv_m) * dt;
+                    float hy = v[1] + (F[1] * inv_m) * dt;
                     float hs = sqrtf(fmaf(hx, hx, hy * hy));
-                    float budget = (fn / mass) * dt;
+                    float budget = (fn * inv_m) * dt;
                     if (hs <= mus * budget) {
-                        F[0] = ((-mass) * v[0]) / dt;
-                        F[1] = ((-mass) * v[1]) / dt;
+                        F[0] = ((-mass) * v[0]) * inv_dt;
+                        F[1] = ((-mass) * v[1]) * inv_dt;
                     } else {
                         float sc = (muk * fn) / hs;
                         F[0] = F[0] - sc * hx;
@@ -488,8 +493,8 @@ static void force_robot_f32(int mode, int nm, float* pos, float* vel, int ns,
             }
             float dt2 = dt * dt;
             for (int q = 0; q < 3; ++q) {
-                float xn = (x[q] + v[q] * dt) + (F[q] / mass) * dt2;
-                v[q] = damp * ((xn - x[q]) / dt);
+                float xn = (x[q] + v[q] * dt) + (F[q] * inv_m) * dt2;
+                v[q] = damp * ((xn - x[q]) * inv_dt);
                 x[q] = xn;
             }
         }
