@@ -271,6 +271,9 @@ def run_ours(args, rank, local_rank, world):
     out_st = pinned.empty((batch.n_springs,), np.float32)
     esim = mb.Simulator(local_rank)
     esim.setTimeStep(dt)
+    if tuned is not None:  # the launch configuration chosen above, as a user would reuse it
+        esim.set_launch_config(**{k: cfg[k] for k in ("threads", "springs_per_thread", "masses_per_thread",
+                                                      "bins", "chunk", "use_graph", "streamed")})
     esim.set_batch(hb)
     esim.Simulate(duration, track)  # warm: graph built for this clock
     esim.synchronize()
@@ -284,6 +287,7 @@ def run_ours(args, rank, local_rank, world):
         esim.collect_arrays((out_pos, out_vel, out_st))
         esim.CentreOfMass()
     e2e_t = dist.max_over_ranks(time.perf_counter() - t0, dev)
+    e2e_launch = esim.launch_config()
     e2e = dist.sum_over_ranks(float(active) * steps_per_eval * e_steps, dev) / e2e_t
     h2d = sum(a.nbytes for a in pinned.arrays.values())
     d2h = out_pos.nbytes + out_vel.nbytes + out_st.nbytes + 12 * batch.n_robots
@@ -332,7 +336,7 @@ def run_ours(args, rank, local_rank, world):
         "kernel_ms_per_launch": 1e3 * t_launch,
         "cpu_baseline": cpu,
         "e2e": {"value": e2e, "unit": "spring-updates/s", "h2d_bytes_per_step": int(h2d),
-                "d2h_bytes_per_step": int(d2h), "steps": e_steps},
+                "d2h_bytes_per_step": int(d2h), "steps": e_steps, "launch": e2e_launch},
         "gpu_launches": int(2 * launches_per_eval * args.steps),
         "gpu_launches_note": "per chunk of steps: one actuation-table launch and one step launch",
         "clocks": clocks,
