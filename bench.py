@@ -362,9 +362,10 @@ def _device_rate(sim, active, steps, track, dev):
 
 def secondary(args, batch, local_rank, dev, hbm_peak):
     """Beside the headline: the force modes (the benchmark configurations'
-    physics) on the same robots with 0.1 kg masses, and the streamed
-    workload (64 robots of 10x10x10 cells, 1,331 masses and 14,230 springs
-    each, stresses tracked) with its HBM-figure roofline."""
+    physics) on the same robots with 0.1 kg masses, the streamed workload
+    (64 robots of 10x10x10 cells, 1,331 masses and 14,230 springs each,
+    stresses tracked) and the point-cloud robots in water (256 robots of
+    500-2,000 masses, stresses tracked), with their HBM-figure rooflines."""
     import mercury_b200 as mb
     from mercury_b200 import robots
     from mercury_b200 import simulator as S
@@ -401,6 +402,27 @@ def secondary(args, batch, local_rank, dev, hbm_peak):
                                     "unit": "GB/s", "frac": rate * hbm_b / 1e9 / hbm_peak,
                                     "bytes_per_update": hbm_b}}
     del ss
+    # point-cloud robots in water (256 robots of 500-2,000 masses, 25 nearest
+    # neighbours, stresses tracked): springs built on the device
+    nb = mb.pack(robots.nn_population_device(256, mass=0.1, device=local_rank))
+    ns = mb.Simulator(local_rank)
+    ns.set_materials(mb.materials.force_table())
+    ns.set_mode(S.MODE_FORCE_WATER)
+    ns.set_environment(**S.WATER)
+    ns.setTimeStep(1e-4)
+    ns.set_batch(nb)
+    act = nb.active_springs()
+    rate = _device_rate(ns, act, 1000, True, dev)
+    hbm_b = HBM_TOPO_B + HBM_STRESS_B + HBM_MASS_B * nb.n_masses / act
+    p, _, _ = ns.collect_arrays()
+    out["nn_water"] = {"value": rate, "unit": "spring-updates/s", "steps": 1000, "finite": bool(np.isfinite(p).all()),
+                       "workload": f"256 point-cloud robots of 500-2,000 masses, 25 nearest-neighbour springs, "
+                                   f"{nb.n_masses} masses, {act} springs, water, stresses tracked, dt=1e-4",
+                       "config": ns.launch_config(),
+                       "roofline": {"bound": "hbm", "achieved": rate * hbm_b / 1e9, "peak": hbm_peak,
+                                    "unit": "GB/s", "frac": rate * hbm_b / 1e9 / hbm_peak,
+                                    "bytes_per_update": hbm_b}}
+    del ns
     out["devo"] = devo_bench(local_rank)
     out["build"] = build_bench(local_rank)
     out["surrogate"] = surrogate_bench(local_rank)

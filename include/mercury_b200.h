@@ -93,8 +93,13 @@ typedef struct mb_batch_desc {
 /* Launch configuration of the step kernel.  threads: CTA size; bins: number
  * of robot groups, each simulated by one CTA; chunk: steps per launch;
  * streamed: 1 = keep only positions in shared memory and stream springs,
- * rows and per-spring scratch through global memory (one robot per CTA; used
- * automatically when a robot does not fit a resident bin). */
+ * rows and per-spring scratch through global memory (one robot per CTA);
+ * cluster: 2, 4 or 8 = split every robot into that many parts, one CTA
+ * each, the parts of a robot forming a thread-block cluster that exchanges
+ * boundary positions through distributed shared memory; 1 = never split;
+ * 0 = automatic (split when a robot does not fit a resident bin and its
+ * parts fit a cluster of at most 8, else streamed).  Reading the
+ * configuration reports the cluster size in use (0 = not split). */
 typedef struct mb_launch_config {
     uint32_t threads;
     uint32_t springs_per_thread;
@@ -103,6 +108,7 @@ typedef struct mb_launch_config {
     uint32_t chunk;
     uint32_t use_graph;
     uint32_t streamed;
+    uint32_t cluster;
 } mb_launch_config;
 
 /* Creates a context on CUDA device `device` with its own stream.
@@ -276,6 +282,8 @@ typedef struct mb_plan_stats {
     /* CTAs of a step launch (CTA g runs bins g, g + ctas, ...) and the
      * largest / smallest number of springs one CTA runs per step */
     uint32_t ctas, max_cta_springs, min_cta_springs;
+    /* robots split over clusters of this many CTAs (0 = not split) */
+    uint32_t cluster;
 } mb_plan_stats;
 MB_API mb_status mb_plan_population(const mb_batch_desc* batch, const mb_launch_config* cfg,
                                     uint32_t num_sms, uint32_t smem_bytes, mb_plan_stats* stats);

@@ -62,7 +62,7 @@ class PlanStats(ctypes.Structure):
                                                "incidence_padding")] + \
                [(n, ctypes.c_uint32) for n in ("aligned_slices", "rank_slices", "material_slots",
                                                "max_bin_springs", "min_bin_springs",
-                                               "ctas", "max_cta_springs", "min_cta_springs")]
+                                               "ctas", "max_cta_springs", "min_cta_springs", "cluster")]
 
 
 class LaunchConfig(ctypes.Structure):
@@ -74,6 +74,7 @@ class LaunchConfig(ctypes.Structure):
         ("chunk", ctypes.c_uint32),
         ("use_graph", ctypes.c_uint32),
         ("streamed", ctypes.c_uint32),
+        ("cluster", ctypes.c_uint32),
     ]
 
 

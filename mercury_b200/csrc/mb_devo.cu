@@ -293,7 +293,7 @@ __global__ void __launch_bounds__(kRebuildThreads) rebuild_kernel(const RebuildP
     __shared__ uint32_t s_total;
     const uint32_t b = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const BinDesc bd = p.bins[b];
-    const uint32_t nm = bd.n_mass, ns = bd.n_spring, cap = bd.pad[0];
+    const uint32_t nm = bd.n_mass, ns = bd.n_spring, cap = bd.row_cap;
     if (tid == 0) {  // the free list after this call's takes
         const uint32_t c = p.free_count[b], t = p.free_taken[b];
         p.free_count[b] = c - min(t, c);

@@ -94,7 +94,7 @@ cudaError_t launch_build_pslot(const uint32_t* spring_gidx, uint32_t n_packed, u
 // Applies development records: pass 0 everything except air -> non-air,
 // pass 1 air -> non-air (takes freed slots).
 cudaError_t launch_devo_apply(const DevoApplyParams& p, int pass, cudaStream_t s);
-// Moves each bin's rows to a region of `cap` entries (bins[b].pad[0] =
+// Moves each bin's rows to a region of `cap` entries (bins[b].row_cap =
 // capacity); new_begin[b] is the new first entry.
 cudaError_t launch_relayout(const BinDesc* old_bins, const uint32_t* new_begin, uint32_t n_bins,
                             const void* src, void* dst, uint32_t entry_bytes, cudaStream_t s);

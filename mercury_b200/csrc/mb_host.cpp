@@ -143,6 +143,8 @@ struct mb_context {
     bool streamed = false;
     uint32_t stream_mpt = 2;
     mb::DevBuf<uint32_t> inc32;
+    mb::DevBuf<uint32_t> exports;          // split bins: halo positions each part writes into the others
+    uint32_t cluster = 0;                  // split bins: CTAs per robot (0 = not split)
     mb::DevBuf<float4> dp_scratch;
     mb::DevBuf<float> st_scratch;
     mb::DevBuf<float> spring_lbar;
@@ -277,12 +279,14 @@ namespace mb_detail {
 // context's device limits and launch override.  With `fallback_auto`, a
 // population that no longer fits the override (after development) is
 // re-planned automatically.
-mb_status pack(mb_context* ctx, const mb_batch_desc* b, bool fallback_auto, mb::Packed& out) {
+mb_status pack(mb_context* ctx, const mb_batch_desc* b, bool fallback_auto, mb::Packed& out,
+               bool allow_split) {
     mb::PackOptions po;
     po.sms = (uint32_t)std::max(ctx->num_sms, 1);
     po.smem_cap = mb::max_step_smem(ctx->device);
     po.mode = (uint32_t)ctx->mode;
     po.override = ctx->override_cfg;
+    if (!allow_split) po.override.cluster = 1;
     po.ctas_per_sm = [ctx](const mb::KernelShape& sh, uint32_t smem) {
         return mb::ctas_per_sm(sh, (uint32_t)ctx->mode, false, smem);
     };
@@ -294,6 +298,7 @@ mb_status pack(mb_context* ctx, const mb_batch_desc* b, bool fallback_auto, mb::
         po.override = none;
         po.override.chunk = ctx->override_cfg.chunk;
         po.override.use_graph = ctx->override_cfg.use_graph;
+        if (!allow_split) po.override.cluster = 1;
         pst = mb::pack_population(b, po, out, err);
     }
     if (pst != MB_OK) return fail(ctx, pst, "%s", err.c_str());
@@ -309,6 +314,7 @@ mb_status upload_packed(mb_context* ctx, const mb::Packed& out) {
     ctx->grid = out.grid;
     ctx->smem_bytes = out.max_smem;
     ctx->streamed = out.streamed;
+    ctx->cluster = out.cluster;
     ctx->stream_mpt = out.shape.mpt;
     const uint32_t nb = out.n_bins;
     cudaStream_t st = ctx->stream;
@@ -325,6 +331,7 @@ mb_status upload_packed(mb_context* ctx, const mb::Packed& out) {
     MB_CUDA(ctx, up(ctx->slice_off, out.slice_off.data(), out.slice_off.size()));
     MB_CUDA(ctx, up(ctx->slice_width, out.slice_width.data(), out.slice_width.size()));
     MB_CUDA(ctx, up(ctx->inc, out.inc.data(), out.inc.size()));
+    MB_CUDA(ctx, up(ctx->exports, out.exports.data(), out.exports.size()));
     if (out.streamed) {
         MB_CUDA(ctx, up(ctx->inc32, out.inc32.data(), out.inc32.size()));
         MB_CUDA(ctx, ctx->dp_scratch.alloc(std::max<size_t>(out.pair.size(), 1)));
@@ -402,7 +409,7 @@ mb_status devo_setup(mb_context* c) {
         const uint32_t cap = (n + n / 2 + 8 * mb::kSliceWidth + 31) / 32 * 32;
         begin[b] = (uint32_t)total;
         nbins[b].inc_begin = (uint32_t)total;
-        nbins[b].pad[0] = cap;
+        nbins[b].row_cap = cap;
         total += cap;
     }
     if (total >= (1ull << 32)) return fail(c, MB_ERR_CAPACITY, "rows too large for development");
@@ -433,11 +440,19 @@ mb_status devo_setup(mb_context* c) {
 
 // Host re-packing of the context's topology copy (fallback of development).
 mb_status host_repack(mb_context* c) {
-    const mb_batch_desc d{c->n_robots,       c->mass_off.data(),   nullptr,
+    // split robots are cut by their current positions
+    std::vector<float> pos;
+    if (c->cluster) {
+        pos.resize(4 * (size_t)c->n_mass);
+        MB_CUDA(c, cudaMemcpyAsync(pos.data(), c->pos.p, pos.size() * sizeof(float), cudaMemcpyDeviceToHost,
+                                   c->stream));
+        MB_CUDA(c, cudaStreamSynchronize(c->stream));
+    }
+    const mb_batch_desc d{c->n_robots,       c->mass_off.data(),   pos.empty() ? nullptr : pos.data(),
                           nullptr,           c->h_mass_mat.data(), c->spring_off.data(),
                           c->h_pairs.data(), c->h_spring_mat.data(), c->h_lbar.data()};
     mb::Packed out;
-    mb_status st = pack(c, &d, true, out);
+    mb_status st = pack(c, &d, true, out, true);
     if (st == MB_OK) st = upload_packed(c, out);
     if (st != MB_OK) c->loaded = false;  // topology and packed arrays disagree now
     c->vox.valid = false;
@@ -485,7 +500,7 @@ mb_status voxel_setup(mb_context* c, uint32_t R, int sx, int sy, int sz, float h
     std::vector<uint8_t> mm(M, 1), sm(S, 1);
     const mb_batch_desc d{R, mo.data(), nullptr, nullptr, mm.data(), so.data(), pairs.data(), sm.data(), lbar.data()};
     mb::Packed out;
-    mb_status st = pack(c, &d, false, out);
+    mb_status st = pack(c, &d, false, out, false);  // the device builder handles no split robots
     if (st != MB_OK) return st;
     // rows with their template size as capacity, plus spare slice columns
     {
@@ -501,7 +516,7 @@ mb_status voxel_setup(mb_context* c, uint32_t R, int sx, int sy, int sz, float h
             else
                 inc.insert(inc.end(), out.inc.begin() + bd.inc_begin, out.inc.begin() + bd.inc_begin + bd.n_inc);
             bd.inc_begin = (uint32_t)total;
-            bd.pad[0] = cap;
+            bd.row_cap = cap;
             total += cap;
             if (streamed)
                 inc32.resize(total, mb::kPadEntry32);
@@ -692,6 +707,7 @@ mb_status mb_get_launch_config(const mb_context* ctx, mb_launch_config* cfg) {
     cfg->chunk = ctx->chunk;
     cfg->use_graph = ctx->use_graph ? 1 : 0;
     cfg->streamed = ctx->streamed ? 1 : 0;
+    cfg->cluster = ctx->cluster;
     return MB_OK;
 }
 
@@ -715,6 +731,7 @@ mb_status mb_plan_population(const mb_batch_desc* batch, const mb_launch_config*
     stats->masses_per_thread = out.shape.mpt;
     stats->bins = out.n_bins;
     stats->streamed = out.streamed ? 1u : 0u;
+    stats->cluster = out.cluster;
     stats->max_smem_bytes = out.max_smem;
     stats->masses = out.masses;
     stats->active_springs = out.active_springs;
@@ -758,11 +775,14 @@ uint32_t mb_kernel_shapes(mb_launch_config* out, uint32_t capacity) {
 
 mb_status mb_set_launch_config(mb_context* ctx, const mb_launch_config* cfg) {
     if (!ctx || !cfg) return MB_ERR_ARGUMENT;
+    const uint32_t cl = cfg->cluster;
+    if (cl != 0 && cl != 1 && cl != 2 && cl != 4 && cl != 8)
+        return fail(ctx, MB_ERR_ARGUMENT, "cluster must be 0, 1, 2, 4 or 8");
     if (cfg->threads && !cfg->streamed) {
         mb::KernelShape s{cfg->threads, cfg->springs_per_thread, cfg->masses_per_thread};
-        if (!mb::shape_supported(s))
-            return fail(ctx, MB_ERR_ARGUMENT, "kernel shape %u/%u/%u not compiled", s.threads,
-                        s.spt, s.mpt);
+        if (cl > 1 ? !mb::split_supported(s) : !mb::shape_supported(s))
+            return fail(ctx, MB_ERR_ARGUMENT, "kernel shape %u/%u/%u not compiled%s", s.threads,
+                        s.spt, s.mpt, cl > 1 ? " for split robots" : "");
     }
     ctx->override_cfg = *cfg;
     if (cfg->chunk) {
@@ -806,7 +826,7 @@ mb_status mb_set_elements(mb_context* ctx, const mb_batch_desc* b) {
         }
     });
     mb::Packed out;
-    const mb_status pst = mb_detail::pack(ctx, b, false, out);
+    const mb_status pst = mb_detail::pack(ctx, b, false, out, true);
     copier.join();
     if (pst != MB_OK) return pst;
 
@@ -890,6 +910,7 @@ mb::StepParams make_params(mb_context* c, float t0, uint32_t steps, bool track) 
     p.smem_bytes = c->smem_bytes;
     p.mode = (uint32_t)c->mode;
     p.inc32 = c->inc32.p;
+    p.exports = c->exports.p;
     p.dp = c->dp_scratch.p;
     p.st = c->st_scratch.p;
     p.g = c->env.g;
@@ -920,8 +941,9 @@ cudaError_t issue_chunks(mb_context* c, float t0, uint32_t steps, bool track) {
         mb::StepParams p = make_params(c, t, n, track);
         MB_TRACE("launch bins=%u threads=%u spt=%u mpt=%u smem=%u steps=%u", p.n_bins, c->shape.threads,
                  c->shape.spt, c->shape.mpt, p.smem_bytes, n);
-        cudaError_t e = c->streamed ? mb::launch_stream(p, 1024, c->stream_mpt, c->stream)
-                                    : mb::launch_step(p, c->shape, c->stream);
+        cudaError_t e = c->streamed  ? mb::launch_stream(p, 1024, c->stream_mpt, c->stream)
+                        : c->cluster ? mb::launch_split(p, c->shape, c->cluster, c->stream)
+                                     : mb::launch_step(p, c->shape, c->stream);
         MB_TRACE("launch returned %d", (int)e);
         if (trace_on() && std::getenv("MB_SYNC")) {
             cudaError_t es = cudaStreamSynchronize(c->stream);
@@ -951,6 +973,7 @@ mb_status run(mb_context* c, uint32_t steps, bool track) {
             // kernel attributes cannot change inside a capture
             MB_TRACE("prepare");
             MB_CUDA(c, c->streamed ? mb::prepare_stream(1024, c->stream_mpt, (uint32_t)c->mode, track, c->smem_bytes)
+                                    : c->cluster ? mb::prepare_split(c->shape, (uint32_t)c->mode, track, c->smem_bytes)
                                     : mb::prepare_step(c->shape, (uint32_t)c->mode, track, c->smem_bytes));
             cudaGraph_t g;
             MB_TRACE("begin capture");
@@ -975,6 +998,7 @@ mb_status run(mb_context* c, uint32_t steps, bool track) {
     } else {
         MB_TRACE("prepare (no graph)");
         MB_CUDA(c, c->streamed ? mb::prepare_stream(1024, c->stream_mpt, (uint32_t)c->mode, track, c->smem_bytes)
+                                    : c->cluster ? mb::prepare_split(c->shape, (uint32_t)c->mode, track, c->smem_bytes)
                                     : mb::prepare_step(c->shape, (uint32_t)c->mode, track, c->smem_bytes));
         cudaError_t e = issue_chunks(c, t0, steps, track);
         if (e != cudaSuccess) return cuda_fail(c, e, "step launch");
@@ -1087,7 +1111,8 @@ mb_status mb_devo(mb_context* ctx, uint32_t replaced_per_robot, uint64_t seed, u
         if (s != MB_OK) return s;
     }
     const char* force_host = std::getenv("MB_DEVO_HOST_REPACK");
-    const bool on_device = !(force_host && force_host[0] == '1');
+    // split robots are re-packed on the host (their parts are planned there)
+    const bool on_device = !(force_host && force_host[0] == '1') && !ctx->cluster;
     if (on_device && !ctx->devo_ready) {
         const mb_status s = mb_detail::devo_setup(ctx);
         if (s != MB_OK) return s;

@@ -26,7 +26,12 @@ struct BinDesc {
     uint32_t inc_begin;    // first incidence entry (SELL-32 layout)
     uint32_t n_inc;        // incidence entries incl. padding
     uint32_t slice_begin;  // first slice descriptor
-    uint32_t pad[5];
+    uint32_t row_cap;      // incidence entries the bin's row region holds (device re-pack)
+    // split bins (one part of a robot simulated by a cluster of CTAs):
+    uint32_t x_stride;     // float4 slots of one predicted-position buffer (cluster maximum)
+    uint32_t export_begin; // first export entry (own mass | rank << 12 | slot << 15)
+    uint32_t n_export;
+    uint32_t n_all;        // own + halo masses
 };
 
 // Everything one step launch needs.  Pointers are device addresses.
@@ -44,6 +49,7 @@ struct StepParams {
     const uint32_t* slice_off;    // per slice: first entry relative to bin inc_begin
     const uint32_t* slice_width;  // per slice: entries per mass (row length)
     const uint16_t* inc;          // incidence entries: spring << 1 | (b end), or kPadEntry
+    const uint32_t* exports;      // split bins: own mass | part << 12 | halo slot << 15
     const uint32_t* n_mat;        // material slots used by the population (device scalar)
     const float* rates;           // [steps][n_mat]: dL0 * sin(omega t_n + phi) of this launch
     const float* invk;            // [n_mat]: 1 / (2 + 1/(k dt^2))
@@ -104,6 +110,10 @@ cudaError_t prepare_stream(uint32_t threads, uint32_t mpt, uint32_t mode, bool t
 cudaError_t launch_stream(const StepParams& p, uint32_t threads, uint32_t mpt, cudaStream_t s);
 uint32_t stream_smem_bytes(uint32_t n_mass);
 bool stream_supported(uint32_t threads, uint32_t mpt);
+// Whether the split (cluster) step kernel is compiled for a shape.
+bool split_supported(const KernelShape& shape);
+cudaError_t prepare_split(const KernelShape& shape, uint32_t mode, bool track, uint32_t smem_bytes);
+cudaError_t launch_split(const StepParams& p, const KernelShape& shape, uint32_t cluster, cudaStream_t s);
 
 // Compiled shapes of the resident (streamed = false) or streamed kernel;
 // writes up to cap entries, returns the count.
@@ -115,6 +125,13 @@ uint32_t bin_smem_bytes(uint32_t n_mass, uint32_t n_spring, uint32_t n_inc);
 // material factors of every slot, the rows as uint16 entries.
 __host__ __device__ inline uint32_t bin_smem_bytes_dev(uint32_t n_mass, uint32_t n_spring, uint32_t n_inc) {
     return 16u * n_mass + 16u * n_spring + 8u * kMaxMaterialSlots + 2u * n_inc;
+}
+
+// Split bins: two predicted-position buffers of x_stride slots, the
+// corrections, the material factors, the export list and the rows.
+__host__ __device__ inline uint32_t split_smem_bytes(uint32_t x_stride, uint32_t n_spring, uint32_t n_inc,
+                                                     uint32_t n_export) {
+    return 32u * x_stride + 16u * n_spring + 8u * kMaxMaterialSlots + 4u * n_export + 2u * n_inc;
 }
 
 // Largest dynamic shared memory the step kernel may use on this device.

@@ -22,10 +22,14 @@
 //
 // All arithmetic uses explicit round-to-nearest intrinsics so that the
 // result is bit-identical to the CPU restatement in the oracle.
+#include <cooperative_groups.h>
+
 #include "mb_internal.h"
 #include "mb_sin.cuh"
 
 namespace mb {
+
+namespace cg = cooperative_groups;
 
 namespace {
 
@@ -113,7 +117,7 @@ __device__ __forceinline__ float velocity_of(float delta, double dt, double inv_
     return __double2float_rn(__ddiv_rn(a, dt));
 }
 
-template <int T, int SPT, int MPT, int MODE, bool TRACK>
+template <int T, int SPT, int MPT, int MODE, bool TRACK, bool SPLIT>
 __global__ void __launch_bounds__(T, 1024 / T) step_kernel(const StepParams p) {
     constexpr bool XPBD = MODE == kModeXpbd;
     extern __shared__ float4 smem4[];
@@ -125,13 +129,18 @@ __global__ void __launch_bounds__(T, 1024 / T) step_kernel(const StepParams p) {
 
     for (uint32_t b = blockIdx.x; b < p.n_bins; b += gridDim.x) {
         const BinDesc bd = p.bins[b];
-        float4* sxt = smem4;                    // predicted positions x~, one float4 per mass
-        float4* sdp = sxt + bd.n_mass;          // corrections dp, one float4 per spring
+        // predicted positions x~, one float4 per mass (split bins: two
+        // buffers, own masses then halo, alternating by step)
+        float4* sxt = smem4;
+        float4* sdp = sxt + (SPLIT ? 2u * bd.x_stride : bd.n_mass);  // corrections dp, one float4 per spring
         float2* smat = reinterpret_cast<float2*>(sdp + bd.n_spring);  // {dL0 sin(..), 1/K} per slot
-        uint16_t* sinc = reinterpret_cast<uint16_t*>(smat + kMaxMaterialSlots);
+        uint32_t* sexp = reinterpret_cast<uint32_t*>(smat + kMaxMaterialSlots);  // split bins: exports
+        uint16_t* sinc = reinterpret_cast<uint16_t*>(sexp + (SPLIT ? bd.n_export : 0u));
 
         const uint32_t n_mat = *p.n_mat;
         for (uint32_t i = tid; i < bd.n_inc; i += T) sinc[i] = __ldg(&p.inc[bd.inc_begin + i]);
+        if (SPLIT)
+            for (uint32_t i = tid; i < bd.n_export; i += T) sexp[i] = __ldg(&p.exports[bd.export_begin + i]);
         float next_rate = 0.0f;  // actuation factor of material tid for the coming step
         if (tid < n_mat) {
             smat[tid].y = __ldg(&p.invk[tid]);  // 1/K (reference step) or k (force modes)
@@ -151,7 +160,7 @@ __global__ void __launch_bounds__(T, 1024 / T) step_kernel(const StepParams p) {
                 const uint32_t g = bd.spring_begin + s;
                 sw[j] = __ldg(&p.spring_pair[g]);
                 lb[j] = __ldg(&p.spring_lbar[g]);
-                if (TRACK) st[j] = p.stress[__ldg(&p.spring_gidx[g])];
+                if (TRACK) st[j] = p.stress[__ldg(&p.spring_gidx[g]) & 0x7FFFFFFFu];
             }
         }
         // Masses of this thread: x, v, mass and the SELL row (offset | width << 20).
@@ -175,9 +184,13 @@ __global__ void __launch_bounds__(T, 1024 / T) step_kernel(const StepParams p) {
                 row[j] = (__ldg(&p.slice_off[sl]) + (m % kSliceWidth)) | (__ldg(&p.slice_width[sl]) << 20);
             }
         }
-        __syncthreads();
+        if (SPLIT)
+            cg::this_cluster().sync();  // every part of the robot has started
+        else
+            __syncthreads();
 
         for (uint32_t step = 0; step < p.steps; ++step) {
+            float4* X = SPLIT ? sxt + (step & 1u) * bd.x_stride : sxt;
             // (1) actuation factors of this step (sim_kernel.cu:222), loaded one
             // step ahead from the launch's table
             if (tid < n_mat) {
@@ -191,19 +204,32 @@ __global__ void __launch_bounds__(T, 1024 / T) step_kernel(const StepParams p) {
                 const uint32_t m = tid + j * T;
                 if (m >= bd.n_mass) break;
                 if (XPBD)
-                    sxt[m] = make_float4(__fadd_rn(x[j].x, __fmul_rn(v[j].x, dt)),
-                                         __fadd_rn(x[j].y, __fmul_rn(v[j].y, dt)),
-                                         __fadd_rn(x[j].z, __fmul_rn(v[j].z, dt)), 0.0f);
+                    X[m] = make_float4(__fadd_rn(x[j].x, __fmul_rn(v[j].x, dt)),
+                                       __fadd_rn(x[j].y, __fmul_rn(v[j].y, dt)),
+                                       __fadd_rn(x[j].z, __fmul_rn(v[j].z, dt)), 0.0f);
                 else
-                    sxt[m] = make_float4(x[j].x, x[j].y, x[j].z, 0.0f);
+                    X[m] = make_float4(x[j].x, x[j].y, x[j].z, 0.0f);
             }
             __syncthreads();
+            if (SPLIT) {
+                // masses the other parts hold as halo, into their buffer of
+                // this step (same offset in every part); the cluster barrier
+                // makes them visible.  A part is at most one step ahead of
+                // another, so the other buffer is never read meanwhile.
+                cg::cluster_group cl = cg::this_cluster();
+                for (uint32_t i = tid; i < bd.n_export; i += T) {
+                    const uint32_t ex = sexp[i];
+                    float4* dst = cl.map_shared_rank(X, (ex >> 12) & 7u);
+                    dst[ex >> 15] = X[ex & 0xFFFu];
+                }
+                cl.sync();
+            }
             // (2) distance constraints (sim_kernel.cu:209-243)
 #pragma unroll
             for (int j = 0; j < SPT; ++j) {
                 const uint32_t s = tid + j * T;
                 if (s >= bd.n_spring) break;
-                const float4 pa = sxt[pk_a(sw[j])], pb = sxt[pk_b(sw[j])];
+                const float4 pa = X[pk_a(sw[j])], pb = X[pk_b(sw[j])];
                 const float2 mt = smat[pk_slot(sw[j])];
                 const float L = __fmaf_rn(lb[j], mt.x, lb[j]);
                 const float dx = __fsub_rn(pa.x, pb.x);
@@ -241,7 +267,7 @@ __global__ void __launch_bounds__(T, 1024 / T) step_kernel(const StepParams p) {
                     }
                 }
                 if (XPBD) {
-                    const float4 xt = sxt[m];
+                    const float4 xt = X[m];
                     const float nx = __fadd_rn(xt.x, ax);
                     const float ny = __fadd_rn(xt.y, ay);
                     const float nz = __fadd_rn(xt.z, az);
@@ -273,10 +299,14 @@ __global__ void __launch_bounds__(T, 1024 / T) step_kernel(const StepParams p) {
 #pragma unroll
             for (int j = 0; j < SPT; ++j) {
                 const uint32_t s = tid + j * T;
-                if (s < bd.n_spring) p.stress[__ldg(&p.spring_gidx[bd.spring_begin + s])] = st[j];
+                if (s < bd.n_spring) {
+                    const uint32_t g = __ldg(&p.spring_gidx[bd.spring_begin + s]);
+                    if (!(g >> 31)) p.stress[g] = st[j];  // bit 31: a copy in a split part
+                }
             }
         }
         if (__syncthreads_or(bad) && tid == 0) atomicOr(&p.bin_flags[b], 1u);
+        if (SPLIT) cg::this_cluster().sync();
     }
 }
 
@@ -524,20 +554,27 @@ struct ShapeEntry {
     StepFn fn[3][2];  // [mode][track]
 };
 
-#define MB_SHAPE(T, S, M)                                                                     \
-    {                                                                                         \
-        T, S, M, {                                                                            \
-            {step_kernel<T, S, M, kModeXpbd, false>, step_kernel<T, S, M, kModeXpbd, true>},  \
-                {step_kernel<T, S, M, kModeForceLand, false>,                                 \
-                 step_kernel<T, S, M, kModeForceLand, true>},                                 \
-                {step_kernel<T, S, M, kModeForceWater, false>,                                \
-                 step_kernel<T, S, M, kModeForceWater, true>},                                \
-        }                                                                                     \
+#define MB_SHAPE(T, S, M, SPLIT)                                                               \
+    {                                                                                          \
+        T, S, M, {                                                                             \
+            {step_kernel<T, S, M, kModeXpbd, false, SPLIT>,                                    \
+             step_kernel<T, S, M, kModeXpbd, true, SPLIT>},                                    \
+                {step_kernel<T, S, M, kModeForceLand, false, SPLIT>,                           \
+                 step_kernel<T, S, M, kModeForceLand, true, SPLIT>},                           \
+                {step_kernel<T, S, M, kModeForceWater, false, SPLIT>,                          \
+                 step_kernel<T, S, M, kModeForceWater, true, SPLIT>},                          \
+        }                                                                                      \
     }
 const ShapeEntry kShapes[] = {
-    MB_SHAPE(256, 8, 2),  MB_SHAPE(512, 4, 1),   MB_SHAPE(512, 8, 2),   MB_SHAPE(512, 16, 4),
-    MB_SHAPE(1024, 4, 1), MB_SHAPE(1024, 6, 2),  MB_SHAPE(1024, 8, 2),  MB_SHAPE(1024, 10, 2),
-    MB_SHAPE(1024, 12, 2),
+    MB_SHAPE(256, 8, 2, false),   MB_SHAPE(512, 4, 1, false),   MB_SHAPE(512, 8, 2, false),
+    MB_SHAPE(512, 16, 4, false),  MB_SHAPE(1024, 4, 1, false),  MB_SHAPE(1024, 6, 2, false),
+    MB_SHAPE(1024, 8, 2, false),  MB_SHAPE(1024, 10, 2, false), MB_SHAPE(1024, 12, 2, false),
+};
+// the parts of split robots (thread-block clusters)
+const ShapeEntry kSplitShapes[] = {
+    MB_SHAPE(1024, 8, 2, true),
+    MB_SHAPE(1024, 10, 2, true),
+    MB_SHAPE(1024, 12, 2, true),
 };
 #undef MB_SHAPE
 
@@ -572,6 +609,12 @@ const ShapeEntry* find_shape(const KernelShape& s) {
     return nullptr;
 }
 
+const ShapeEntry* find_split(const KernelShape& s) {
+    for (const auto& e : kSplitShapes)
+        if (e.threads == s.threads && e.spt == s.spt && e.mpt == s.mpt) return &e;
+    return nullptr;
+}
+
 }  // namespace
 
 uint32_t bin_smem_bytes(uint32_t n_mass, uint32_t n_spring, uint32_t n_inc) {
@@ -585,6 +628,37 @@ uint32_t max_step_smem(int device) {
 }
 
 bool shape_supported(const KernelShape& shape) { return find_shape(shape) != nullptr; }
+
+bool split_supported(const KernelShape& shape) { return find_split(shape) != nullptr; }
+
+cudaError_t prepare_split(const KernelShape& shape, uint32_t mode, bool track, uint32_t smem_bytes) {
+    const ShapeEntry* e = find_split(shape);
+    if (!e || mode > kModeForceWater) return cudaErrorInvalidValue;
+    return cudaFuncSetAttribute(e->fn[mode][track ? 1 : 0], cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)smem_bytes);
+}
+
+// One CTA per part, the parts of a robot (bins r*C .. r*C + C-1) forming a
+// cluster of C CTAs.
+cudaError_t launch_split(const StepParams& p, const KernelShape& shape, uint32_t cluster, cudaStream_t s) {
+    const ShapeEntry* e = find_split(shape);
+    if (!e || p.mode > kModeForceWater || cluster < 2 || cluster > 8 || p.n_bins % cluster)
+        return cudaErrorInvalidValue;
+    if (p.n_bins == 0) return cudaSuccess;
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(p.n_bins, 1, 1);
+    cfg.blockDim = dim3(shape.threads, 1, 1);
+    cfg.dynamicSmemBytes = p.smem_bytes;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, e->fn[p.mode][p.track ? 1 : 0], p);
+}
 
 cudaError_t prepare_step(const KernelShape& shape, uint32_t mode, bool track, uint32_t smem_bytes) {
     const ShapeEntry* e = find_shape(shape);

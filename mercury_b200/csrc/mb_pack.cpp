@@ -47,6 +47,9 @@ const KernelShape kAuto[] = {
     {1024, 6, 2},  {1024, 4, 1},  {512, 4, 1},  {256, 8, 2},
 };
 
+// Shapes for the parts of split robots, in order of preference.
+const KernelShape kSplit[] = {{1024, 8, 2}, {1024, 10, 2}, {1024, 12, 2}};
+
 template <typename F>
 void parallel_for(uint32_t n, unsigned threads, F&& f) {
     if (threads <= 1 || n <= 1) {
@@ -238,12 +241,109 @@ struct BinLocal {
 
 struct Ent {
     uint32_t other, orig, sign, packed;
+    // index of the other end used for column alignment; its order within a
+    // row must be the order of `other`, since aligned columns follow it
+    uint32_t align;
 };
 
 inline bool ent_less(const Ent& x, const Ent& y) {
     if (x.other != y.other) return x.other < y.other;
     if (x.orig != y.orig) return x.orig < y.orig;
     return x.sign < y.sign;
+}
+
+// Every row in summation order: (other end, spring index, a end first).
+void sort_rows(uint32_t nm, const std::vector<uint32_t>& row_start, std::vector<Ent>& ents) {
+    for (uint32_t i = 0; i < nm; ++i) {
+        Ent* first = ents.data() + row_start[i];
+        Ent* last = ents.data() + row_start[i + 1];
+        if (last - first > 24) {
+            std::sort(first, last, ent_less);
+        } else {
+            for (Ent* x = first + 1; x < last; ++x) {
+                const Ent e = *x;
+                Ent* y = x;
+                while (y > first && ent_less(e, *(y - 1))) {
+                    *y = *(y - 1);
+                    --y;
+                }
+                *y = e;
+            }
+        }
+    }
+}
+
+// SELL-32 rows of masses 0..nm-1 from their sorted entries (row_start:
+// CSR offsets into ents); fills L's slices and incidence arrays.
+void slice_rows(uint32_t nm, const std::vector<uint32_t>& row_start, const std::vector<Ent>& ents,
+                bool streamed, BinLocal& L) {
+    // SELL-32: columns aligned by the offset of the other end (other - i)
+    // when every row of the slice has distinct offsets -- then the k-th
+    // entries of a warp's 32 masses are springs of one direction with
+    // consecutive packed indices (conflict-free gather) -- otherwise, or
+    // when alignment would widen the slice by more than 4 columns, ranks.
+    // the union of a slice's offsets as a bitset over [lo, hi]: an entry's
+    // aligned column is the rank of its offset (prefix popcounts per word)
+    std::vector<uint64_t> bits;
+    std::vector<uint32_t> before;
+    for (uint32_t i0 = 0; i0 < nm; i0 += kSliceWidth) {
+        const uint32_t i1 = std::min<uint32_t>(i0 + kSliceWidth, nm);
+        uint32_t w_rank = 0;
+        bool distinct = true;
+        int lo = INT32_MAX, hi = INT32_MIN;
+        for (uint32_t i = i0; i < i1; ++i) {
+            const uint32_t r0 = row_start[i], r1 = row_start[i + 1];
+            w_rank = std::max(w_rank, r1 - r0);
+            for (uint32_t q = r0; q < r1; ++q) {
+                if (q > r0 && ents[q].other == ents[q - 1].other) distinct = false;
+                const int o = (int)ents[q].align - (int)i;
+                lo = std::min(lo, o);
+                hi = std::max(hi, o);
+            }
+        }
+        uint32_t n_union = 0;
+        if (distinct && lo <= hi) {
+            const size_t words = (size_t)(hi - lo) / 64 + 1;
+            bits.assign(words, 0);
+            for (uint32_t i = i0; i < i1; ++i)
+                for (uint32_t q = row_start[i]; q < row_start[i + 1]; ++q) {
+                    const int o = (int)ents[q].align - (int)i - lo;
+                    bits[o >> 6] |= 1ull << (o & 63);
+                }
+            before.assign(words, 0);
+            for (size_t wd = 0; wd < words; ++wd) {
+                before[wd] = n_union;
+                n_union += (uint32_t)__builtin_popcountll(bits[wd]);
+            }
+        }
+        const bool aligned = distinct && n_union <= w_rank + 4;
+        const uint32_t w = aligned ? n_union : w_rank;
+        aligned ? ++L.aligned : ++L.ranked;
+        const size_t base = streamed ? L.inc32.size() : L.inc.size();
+        L.slice_off.push_back((uint32_t)base);
+        L.slice_width.push_back(w);
+        if (streamed)
+            L.inc32.resize(base + (size_t)w * kSliceWidth, kPadEntry32);
+        else
+            L.inc.resize(base + (size_t)w * kSliceWidth, kPadEntry);
+        for (uint32_t i = i0; i < i1; ++i)
+            for (uint32_t q = row_start[i]; q < row_start[i + 1]; ++q) {
+                const Ent& e = ents[q];
+                uint32_t col = q - row_start[i];
+                if (aligned) {
+                    const int o = (int)e.align - (int)i - lo;
+                    const uint64_t below = bits[o >> 6] & ((1ull << (o & 63)) - 1ull);
+                    col = before[o >> 6] + (uint32_t)__builtin_popcountll(below);
+                }
+                const size_t at = base + (size_t)col * kSliceWidth + (i - i0);
+                if (streamed)
+                    L.inc32[at] = (e.packed << 1) | e.sign;
+                else
+                    L.inc[at] = (uint16_t)((e.packed << 1) | e.sign);
+            }
+    }
+    L.n_inc = (uint32_t)(streamed ? L.inc32.size() : L.inc.size());
+    L.padding = L.n_inc - (uint64_t)row_start[nm];
 }
 
 void build_bin(const mb_batch_desc* b, const std::vector<RobotPack>& packs,
@@ -285,115 +385,28 @@ void build_bin(const mb_batch_desc* b, const std::vector<RobotPack>& packs,
             for (uint32_t k = 0; k < sp.size(); ++k) {
                 const int64_t g = s0 + sp[k];
                 const uint32_t a = b->pairs[2 * g], c = b->pairs[2 * g + 1];
-                ents[fill[base + a]++] = {c, sp[k], 0u, sb + k};
-                ents[fill[base + c]++] = {a, sp[k], 1u, sb + k};
+                ents[fill[base + a]++] = {c, sp[k], 0u, sb + k, c};
+                ents[fill[base + c]++] = {a, sp[k], 1u, sb + k, a};
             }
             base += packs[r].n_mass;
             sb += (uint32_t)sp.size();
         }
     }
-    for (uint32_t i = 0; i < nm; ++i) {  // summation order within each row
-        Ent* first = ents.data() + row_start[i];
-        Ent* last = ents.data() + row_start[i + 1];
-        if (last - first > 24) {
-            std::sort(first, last, ent_less);
-        } else {
-            for (Ent* x = first + 1; x < last; ++x) {
-                const Ent e = *x;
-                Ent* y = x;
-                while (y > first && ent_less(e, *(y - 1))) {
-                    *y = *(y - 1);
-                    --y;
-                }
-                *y = e;
-            }
-        }
-    }
+    sort_rows(nm, row_start, ents);
     L.n_mass = nm;
     L.n_spring = ns;
-    // SELL-32: columns aligned by the offset of the other end (other - i)
-    // when every row of the slice has distinct offsets -- then the k-th
-    // entries of a warp's 32 masses are springs of one direction with
-    // consecutive packed indices (conflict-free gather) -- otherwise, or
-    // when alignment would widen the slice by more than 4 columns, ranks.
-    // the union of a slice's offsets as a bitset over [lo, hi]: an entry's
-    // aligned column is the rank of its offset (prefix popcounts per word)
-    std::vector<uint64_t> bits;
-    std::vector<uint32_t> before;
-    for (uint32_t i0 = 0; i0 < nm; i0 += kSliceWidth) {
-        const uint32_t i1 = std::min<uint32_t>(i0 + kSliceWidth, nm);
-        uint32_t w_rank = 0;
-        bool distinct = true;
-        int lo = INT32_MAX, hi = INT32_MIN;
-        for (uint32_t i = i0; i < i1; ++i) {
-            const uint32_t r0 = row_start[i], r1 = row_start[i + 1];
-            w_rank = std::max(w_rank, r1 - r0);
-            for (uint32_t q = r0; q < r1; ++q) {
-                if (q > r0 && ents[q].other == ents[q - 1].other) distinct = false;
-                const int o = (int)ents[q].other - (int)i;
-                lo = std::min(lo, o);
-                hi = std::max(hi, o);
-            }
-        }
-        uint32_t n_union = 0;
-        if (distinct && lo <= hi) {
-            const size_t words = (size_t)(hi - lo) / 64 + 1;
-            bits.assign(words, 0);
-            for (uint32_t i = i0; i < i1; ++i)
-                for (uint32_t q = row_start[i]; q < row_start[i + 1]; ++q) {
-                    const int o = (int)ents[q].other - (int)i - lo;
-                    bits[o >> 6] |= 1ull << (o & 63);
-                }
-            before.assign(words, 0);
-            for (size_t wd = 0; wd < words; ++wd) {
-                before[wd] = n_union;
-                n_union += (uint32_t)__builtin_popcountll(bits[wd]);
-            }
-        }
-        const bool aligned = distinct && n_union <= w_rank + 4;
-        const uint32_t w = aligned ? n_union : w_rank;
-        aligned ? ++L.aligned : ++L.ranked;
-        const size_t base = streamed ? L.inc32.size() : L.inc.size();
-        L.slice_off.push_back((uint32_t)base);
-        L.slice_width.push_back(w);
-        if (streamed)
-            L.inc32.resize(base + (size_t)w * kSliceWidth, kPadEntry32);
-        else
-            L.inc.resize(base + (size_t)w * kSliceWidth, kPadEntry);
-        for (uint32_t i = i0; i < i1; ++i)
-            for (uint32_t q = row_start[i]; q < row_start[i + 1]; ++q) {
-                const Ent& e = ents[q];
-                uint32_t col = q - row_start[i];
-                if (aligned) {
-                    const int o = (int)e.other - (int)i - lo;
-                    const uint64_t below = bits[o >> 6] & ((1ull << (o & 63)) - 1ull);
-                    col = before[o >> 6] + (uint32_t)__builtin_popcountll(below);
-                }
-                const size_t at = base + (size_t)col * kSliceWidth + (i - i0);
-                if (streamed)
-                    L.inc32[at] = (e.packed << 1) | e.sign;
-                else
-                    L.inc[at] = (uint16_t)((e.packed << 1) | e.sign);
-            }
-    }
-    L.n_inc = (uint32_t)(streamed ? L.inc32.size() : L.inc.size());
-    L.padding = L.n_inc - 2ull * ns;
+    slice_rows(nm, row_start, ents, streamed, L);
     L.smem = streamed ? stream_smem_bytes(nm) : bin_smem_bytes(nm, ns, L.n_inc);
 }
 
-void build_all(const mb_batch_desc* b, const std::vector<RobotPack>& packs,
-               const std::vector<std::vector<uint32_t>>& plan, const std::vector<int>& slot_of,
-               bool streamed, unsigned threads, Packed& out) {
-    const uint32_t nb = (uint32_t)plan.size(), R = (uint32_t)packs.size();
-    std::vector<BinLocal> locals(nb);
-    parallel_for(nb, threads, [&](uint32_t i) { build_bin(b, packs, plan[i], slot_of, streamed, locals[i]); });
+// Offsets of every bin, then every bin copied in parallel into sized
+// arrays; statistics.
+void assemble(const std::vector<BinLocal>& locals, Packed& out, bool streamed, unsigned threads) {
+    const uint32_t nb = (uint32_t)locals.size();
     out.bins.assign(nb, BinDesc{});
-    out.robot_bin.assign(R, 0);
-    out.robot_mass_base.assign(R, 0);
     out.max_smem = 0;
     out.inc_entries = out.inc_padding = 0;
     out.aligned_slices = out.rank_slices = 0;
-    // bin offsets, then every bin copied in parallel into sized arrays
     uint64_t nm = 0, ns = 0, nsl = 0, ninc = 0;
     for (uint32_t i = 0; i < nb; ++i) {
         const BinLocal& L = locals[i];
@@ -410,12 +423,6 @@ void build_all(const mb_batch_desc* b, const std::vector<RobotPack>& packs,
         ns += L.spring_gidx.size();
         nsl += L.slice_off.size();
         ninc += streamed ? L.inc32.size() : L.inc.size();
-        uint32_t base = 0;
-        for (uint32_t r : plan[i]) {
-            out.robot_bin[r] = i;
-            out.robot_mass_base[r] = base;
-            base += packs[r].n_mass;
-        }
         out.max_smem = std::max(out.max_smem, L.smem);
         out.inc_entries += L.n_inc;
         out.inc_padding += L.padding;
@@ -447,6 +454,225 @@ void build_all(const mb_batch_desc* b, const std::vector<RobotPack>& packs,
         else
             put(out.inc, d.inc_begin, L.inc);
     });
+}
+
+void build_all(const mb_batch_desc* b, const std::vector<RobotPack>& packs,
+               const std::vector<std::vector<uint32_t>>& plan, const std::vector<int>& slot_of,
+               bool streamed, unsigned threads, Packed& out) {
+    const uint32_t nb = (uint32_t)plan.size(), R = (uint32_t)packs.size();
+    std::vector<BinLocal> locals(nb);
+    parallel_for(nb, threads, [&](uint32_t i) { build_bin(b, packs, plan[i], slot_of, streamed, locals[i]); });
+    assemble(locals, out, streamed, threads);
+    out.robot_bin.assign(R, 0);
+    out.robot_mass_base.assign(R, 0);
+    for (uint32_t i = 0; i < nb; ++i) {
+        uint32_t base = 0;
+        for (uint32_t r : plan[i]) {
+            out.robot_bin[r] = i;
+            out.robot_mass_base[r] = base;
+            base += packs[r].n_mass;
+        }
+    }
+    out.exports.clear();
+    out.cluster = 0;
+}
+
+// ---- split bins: one robot simulated by a cluster of C CTAs ----
+//
+// A robot too large for one CTA's shared memory is cut into C = 2^levels
+// parts by recursive coordinate bisection of its initial positions (each
+// cut along the axis of largest extent, ties to the later axis, at the
+// median; ties in position by mass index).  Part p is one bin: its own
+// masses (ascending index), then a halo of the other parts' masses its
+// springs reach; every active spring with an end in the part, so a spring
+// across a cut is solved by both parts -- with the same operands, so with
+// the same bits -- and only the part holding its a end writes its stress
+// back (spring_gidx bit 31 marks the copies).  Rows exist for own masses
+// only, in the usual summation order.  Every step each part writes its
+// masses that others hold as halo into their predicted-position buffers
+// (export entries: own mass | part << 12 | slot << 15).
+
+// Part of every mass of robot r (positions: float4 per mass).
+void partition_robot(const mb_batch_desc* b, uint32_t r, uint32_t levels, std::vector<uint8_t>& part_of) {
+    const int64_t m0 = b->mass_offsets[r];
+    const uint32_t n = (uint32_t)(b->mass_offsets[r + 1] - m0);
+    std::vector<uint32_t> idx(n);
+    for (uint32_t i = 0; i < n; ++i) idx[i] = i;
+    part_of.assign(n, 0);
+    // without positions (a topology-only description): index order
+    auto coord = [&](uint32_t m, int axis) {
+        if (!b->pos) return axis == 2 ? (float)m : 0.0f;
+        const float v = b->pos[4 * (m0 + m) + axis];
+        return std::isfinite(v) ? v : INFINITY;
+    };
+    struct Range {
+        uint32_t lo, hi, level, part;
+    };
+    std::vector<Range> todo{{0, n, levels, 0}};
+    while (!todo.empty()) {
+        const Range q = todo.back();
+        todo.pop_back();
+        if (q.level == 0) {
+            for (uint32_t i = q.lo; i < q.hi; ++i) part_of[idx[i]] = (uint8_t)q.part;
+            continue;
+        }
+        int axis = 0;
+        float best = -1.0f;
+        for (int ax = 0; ax < 3; ++ax) {
+            float lo = INFINITY, hi = -INFINITY;
+            for (uint32_t i = q.lo; i < q.hi; ++i) {
+                const float v = coord(idx[i], ax);
+                if (v == INFINITY) continue;
+                lo = std::min(lo, v);
+                hi = std::max(hi, v);
+            }
+            const float ext = hi >= lo ? hi - lo : 0.0f;
+            if (ext >= best) {
+                best = ext;
+                axis = ax;
+            }
+        }
+        std::sort(idx.begin() + q.lo, idx.begin() + q.hi, [&](uint32_t x, uint32_t y) {
+            const float cx = coord(x, axis), cy = coord(y, axis);
+            return cx < cy || (cx == cy && x < y);
+        });
+        const uint32_t mid = q.lo + (q.hi - q.lo + 1) / 2;
+        todo.push_back({mid, q.hi, q.level - 1, 2 * q.part + 1});
+        todo.push_back({q.lo, mid, q.level - 1, 2 * q.part});
+    }
+}
+
+struct PartMasses {
+    std::vector<uint32_t> own, halo;  // robot-local indices, ascending
+};
+
+void build_part(const mb_batch_desc* b, uint32_t r, const RobotPack& pk, const std::vector<uint8_t>& part_of,
+                uint32_t p, const std::vector<int>& slot_of, std::vector<int32_t>& local_of, BinLocal& L,
+                PartMasses& pm) {
+    const int64_t m0 = b->mass_offsets[r], s0 = b->spring_offsets[r];
+    const uint32_t n = pk.n_mass;
+    pm.own.clear();
+    pm.halo.clear();
+    local_of.assign(n, -1);
+    for (uint32_t m = 0; m < n; ++m)
+        if (part_of[m] == p) {
+            local_of[m] = (int32_t)pm.own.size();
+            pm.own.push_back(m);
+        }
+    const uint32_t n_own = (uint32_t)pm.own.size();
+    std::vector<uint32_t> sp;
+    for (uint32_t ls : pk.springs) {
+        const int64_t g = s0 + ls;
+        const uint32_t a = b->pairs[2 * g], c = b->pairs[2 * g + 1];
+        if (part_of[a] != p && part_of[c] != p) continue;
+        sp.push_back(ls);
+        if (part_of[a] != p) pm.halo.push_back(a);
+        if (part_of[c] != p) pm.halo.push_back(c);
+    }
+    std::sort(pm.halo.begin(), pm.halo.end());
+    pm.halo.erase(std::unique(pm.halo.begin(), pm.halo.end()), pm.halo.end());
+    for (uint32_t j = 0; j < pm.halo.size(); ++j) local_of[pm.halo[j]] = (int32_t)(n_own + j);
+    L.mass_gidx.reserve(n_own);
+    for (uint32_t m : pm.own) L.mass_gidx.push_back((uint32_t)(m0 + m));
+    const uint32_t ns = (uint32_t)sp.size();
+    L.spring_gidx.reserve(ns);
+    L.pair.reserve(ns);
+    L.lbar.reserve(ns);
+    std::vector<uint32_t> row_start(n_own + 1, 0);
+    for (uint32_t ls : sp) {
+        const int64_t g = s0 + ls;
+        const uint32_t a = b->pairs[2 * g], c = b->pairs[2 * g + 1];
+        const uint32_t la = (uint32_t)local_of[a], lc = (uint32_t)local_of[c];
+        L.spring_gidx.push_back((uint32_t)g | (part_of[a] != p ? 0x80000000u : 0u));
+        L.pair.push_back(la | (lc << 12) | ((uint32_t)slot_of[b->spring_material[g]] << 24));
+        L.lbar.push_back(b->lbar[g]);
+        if (part_of[a] == p) row_start[la + 1]++;
+        if (part_of[c] == p) row_start[lc + 1]++;
+    }
+    for (uint32_t i = 0; i < n_own; ++i) row_start[i + 1] += row_start[i];
+    std::vector<Ent> ents(row_start[n_own]);
+    std::vector<uint32_t> fill(row_start.begin(), row_start.end() - 1);
+    for (uint32_t k = 0; k < ns; ++k) {
+        const int64_t g = s0 + sp[k];
+        const uint32_t a = b->pairs[2 * g], c = b->pairs[2 * g + 1];
+        const uint32_t la = (uint32_t)local_of[a], lc = (uint32_t)local_of[c];
+        // aligned by the robot-local index of the other end: a row's column
+        // order must stay its summation order (halo masses are numbered
+        // after the own ones, so part-local indices would not keep it)
+        if (part_of[a] == p) ents[fill[la]++] = {c, sp[k], 0u, k, c};
+        if (part_of[c] == p) ents[fill[lc]++] = {a, sp[k], 1u, k, a};
+    }
+    sort_rows(n_own, row_start, ents);
+    L.n_mass = n_own;
+    L.n_spring = ns;
+    slice_rows(n_own, row_start, ents, false, L);
+}
+
+// Split packing of every robot into C parts under the shape's and the
+// shared memory's limits; false (with the reason) when a part does not fit.
+bool build_split(const mb_batch_desc* b, const std::vector<RobotPack>& packs, uint32_t C, const KernelShape& sh,
+                 uint32_t smem_cap, const std::vector<int>& slot_of, unsigned threads, Packed& out,
+                 std::string& why) {
+    const uint32_t R = (uint32_t)packs.size();
+    uint32_t levels = 0;
+    while ((1u << levels) < C) ++levels;
+    const uint32_t nb = R * C;
+    const uint64_t cap_s = std::min<uint64_t>((uint64_t)sh.threads * sh.spt, kMaxBinSprings);
+    const uint64_t cap_m = std::min<uint64_t>((uint64_t)sh.threads * sh.mpt, 4096);
+    std::vector<BinLocal> locals(nb);
+    std::vector<std::vector<uint32_t>> exports(nb);
+    std::vector<uint32_t> n_all(nb), stride(R);
+    parallel_for(R, threads, [&](uint32_t r) {
+        std::vector<uint8_t> part_of;
+        partition_robot(b, r, levels, part_of);
+        std::vector<PartMasses> pm(C);
+        std::vector<int32_t> local_of;
+        for (uint32_t p = 0; p < C; ++p) {
+            build_part(b, r, packs[r], part_of, p, slot_of, local_of, locals[r * C + p], pm[p]);
+            n_all[r * C + p] = (uint32_t)(pm[p].own.size() + pm[p].halo.size());
+        }
+        for (uint32_t q = 0; q < C; ++q)
+            for (uint32_t j = 0; j < pm[q].halo.size(); ++j) {
+                const uint32_t m = pm[q].halo[j], owner = part_of[m];
+                const auto& own = pm[owner].own;
+                const uint32_t li = (uint32_t)(std::lower_bound(own.begin(), own.end(), m) - own.begin());
+                const uint32_t slot = (uint32_t)pm[q].own.size() + j;
+                exports[r * C + owner].push_back(li | (q << 12) | (slot << 15));
+            }
+        uint32_t st = 0;
+        for (uint32_t p = 0; p < C; ++p) {
+            std::sort(exports[r * C + p].begin(), exports[r * C + p].end());
+            st = std::max(st, n_all[r * C + p]);
+        }
+        stride[r] = st;
+    });
+    char buf[256];
+    for (uint32_t i = 0; i < nb; ++i) {
+        const BinLocal& L = locals[i];
+        const uint32_t smem = split_smem_bytes(stride[i / C], L.n_spring, L.n_inc, (uint32_t)exports[i].size());
+        if (L.n_spring > cap_s || L.n_mass > cap_m || n_all[i] > 4096 || smem > smem_cap) {
+            std::snprintf(buf, sizeof(buf), "part %u of robot %u: %u springs, %u + %u masses, %u B shared memory",
+                          i % C, i / C, L.n_spring, L.n_mass, n_all[i] - L.n_mass, smem);
+            why = buf;
+            return false;
+        }
+    }
+    assemble(locals, out, false, threads);
+    out.robot_bin.assign(R, 0);
+    out.robot_mass_base.assign(R, 0);
+    for (uint32_t r = 0; r < R; ++r) out.robot_bin[r] = r * C;
+    out.exports.clear();
+    out.max_smem = 0;
+    for (uint32_t i = 0; i < nb; ++i) {
+        BinDesc& d = out.bins[i];
+        d.x_stride = stride[i / C];
+        d.export_begin = (uint32_t)out.exports.size();
+        d.n_export = (uint32_t)exports[i].size();
+        d.n_all = n_all[i];
+        out.exports.insert(out.exports.end(), exports[i].begin(), exports[i].end());
+        out.max_smem = std::max(out.max_smem, split_smem_bytes(d.x_stride, d.n_spring, d.n_inc, d.n_export));
+    }
+    return true;
 }
 
 }  // namespace
@@ -483,10 +709,17 @@ mb_status pack_population(const mb_batch_desc* b, const PackOptions& o, Packed& 
             out.mat_ids.push_back((uint8_t)m);
         }
 
+    const uint32_t force_c = o.override.cluster;
+    if (force_c != 0 && force_c != 1 && force_c != 2 && force_c != 4 && force_c != 8) {
+        err = "cluster must be 0, 1, 2, 4 or 8";
+        return MB_ERR_ARGUMENT;
+    }
     std::vector<KernelShape> shapes;
-    if (o.override.threads && !o.override.streamed)
+    if (force_c > 1 || o.override.streamed)
+        ;  // split or streamed: no resident bins
+    else if (o.override.threads)
         shapes.push_back({o.override.threads, o.override.springs_per_thread, o.override.masses_per_thread});
-    else if (!o.override.streamed)
+    else
         for (const auto& s : kAuto) shapes.push_back(s);
     const uint32_t sms = std::max<uint32_t>(o.sms, 1);
     std::vector<std::vector<uint32_t>> plan;
@@ -548,8 +781,42 @@ mb_status pack_population(const mb_batch_desc* b, const PackOptions& o, Packed& 
             break;
         }
     }
-    // Streamed: when forced, or when no resident shape holds the largest
-    // robot.  One robot per bin.
+    // Split over a cluster: when forced, or when no resident shape holds the
+    // largest robot -- the fewest parts whose every part fits a shape.
+    std::string why;
+    if (!ok && !o.override.streamed && force_c != 1) {
+        std::vector<uint32_t> cs;
+        if (force_c > 1)
+            cs.push_back(force_c);
+        else
+            cs = {2u, 4u, 8u};
+        std::vector<KernelShape> sshapes;
+        if (o.override.threads)
+            sshapes.push_back({o.override.threads, o.override.springs_per_thread, o.override.masses_per_thread});
+        else
+            for (const auto& sh : kSplit) sshapes.push_back(sh);
+        for (uint32_t C : cs) {
+            for (const auto& sh : sshapes) {
+                if (!split_supported(sh)) continue;
+                if (build_split(b, packs, C, sh, o.smem_cap, slot_of, threads, out, why)) {
+                    ok = true;
+                    out.shape = sh;
+                    out.n_bins = R * C;
+                    out.grid = 0;
+                    out.cluster = C;
+                    out.streamed = false;
+                    break;
+                }
+            }
+            if (ok) break;
+        }
+        if (!ok && force_c > 1) {
+            err = "robots do not fit a split over " + std::to_string(force_c) + " CTAs: " + why;
+            return MB_ERR_CAPACITY;
+        }
+    }
+    // Streamed: when forced, or when neither a resident shape nor a split
+    // holds the largest robot.  One robot per bin.
     if (o.override.streamed || !ok) {
         const uint32_t mpt = max_m <= 2048 ? 2u : 4u;
         if (max_m <= 4096 && stream_supported(1024, mpt)) {
@@ -562,6 +829,8 @@ mb_status pack_population(const mb_batch_desc* b, const PackOptions& o, Packed& 
                 out.shape = KernelShape{1024, 0, mpt};
                 out.n_bins = R;
                 out.grid = 0;
+                out.cluster = 0;
+                out.exports.clear();
             }
         }
     }

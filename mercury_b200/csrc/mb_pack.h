@@ -26,6 +26,7 @@ struct Packed {
     KernelShape shape{0, 0, 0};
     uint32_t n_bins = 0;
     uint32_t grid = 0;  // CTAs per launch, CTA g running bins g, g + grid, ...; 0 = one per bin
+    uint32_t cluster = 0;  // split bins: CTAs per cluster (parts per robot); 0 = not split
     bool streamed = false;
     uint32_t max_smem = 0;
     std::vector<BinDesc> bins;
@@ -33,6 +34,7 @@ struct Packed {
     std::vector<uint32_t> robot_mass_base;  // bin-local index of each robot's first mass
     std::vector<uint16_t> inc;    // resident rows
     std::vector<uint32_t> inc32;  // streamed rows
+    std::vector<uint32_t> exports;  // split bins: own mass | part << 12 | halo slot << 15
     std::vector<float> lbar;
     std::vector<uint8_t> mat_ids;
     // statistics

@@ -302,9 +302,9 @@ class Simulator:
         return {f: getattr(c, f) for f, _ in c._fields_}
 
     def set_launch_config(self, threads=0, springs_per_thread=0, masses_per_thread=0, bins=0,
-                          chunk=0, use_graph=1, streamed=0) -> None:
+                          chunk=0, use_graph=1, streamed=0, cluster=0) -> None:
         c = _lib.LaunchConfig(threads, springs_per_thread, masses_per_thread, bins, chunk, use_graph,
-                              streamed)
+                              streamed, cluster)
         _lib.check(_lib.LIB.mb_set_launch_config(self._ctx, ctypes.byref(c)), self._ctx)
 
 
@@ -335,7 +335,7 @@ def plan(batch: Batch, num_sms: int = 148, smem_bytes: int = 0, **cfg) -> dict:
         _lib.ptr(batch.spring_material), _lib.ptr(batch.lbar))
     c = _lib.LaunchConfig(cfg.get("threads", 0), cfg.get("springs_per_thread", 0),
                           cfg.get("masses_per_thread", 0), cfg.get("bins", 0), cfg.get("chunk", 0),
-                          cfg.get("use_graph", 1), cfg.get("streamed", 0))
+                          cfg.get("use_graph", 1), cfg.get("streamed", 0), cfg.get("cluster", 0))
     st = _lib.PlanStats()
     _lib.check(_lib.LIB.mb_plan_population(ctypes.byref(d), ctypes.byref(c), num_sms, smem_bytes,
                                            ctypes.byref(st)))

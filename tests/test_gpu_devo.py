@@ -141,7 +141,7 @@ def test_devo_through_simulator_api():
 
 
 def test_devo_force_water_streamed_bit_exact():
-    """Point-cloud robots in water (streamed path), two cycles."""
+    """Point-cloud robots in water on the streamed path, two cycles."""
     b = robots.population_batch("nn", 3, mass=0.1)
     tab = mb.materials.force_table()
     sim = mb.Simulator(0)
@@ -149,6 +149,7 @@ def test_devo_force_water_streamed_bit_exact():
     sim.set_mode(2)
     sim.set_environment(**S.WATER)
     sim.setTimeStep(1e-4)
+    sim.set_launch_config(streamed=1)
     sim.set_batch(b)
     assert sim.launch_config()["streamed"] == 1
     orc = OracleRun(b, tab, np.float32(1e-4), mode=2, env=S.WATER)

@@ -71,17 +71,21 @@ def test_mode_switch_keeps_reference_step_exact():
     assert np.array_equal(bits(pos), bits(p))
 
 
-def test_nn_robots_in_water_streamed_bit_exact():
+@pytest.mark.parametrize("cfg", [dict(streamed=1), dict()], ids=["streamed", "split"])
+def test_nn_robots_in_water_bit_exact(cfg):
     """Point-cloud robots (25-NN springs, up to ~28k springs each) in water
-    with stress tracking: streamed path, bit-exact against the oracle."""
+    with stress tracking, streamed or split over clusters (the automatic
+    choice): bit-exact against the oracle."""
     b = robots.population_batch("nn", 4, mass=0.1)
     sim = mb.Simulator(0)
     sim.set_materials(mb.materials.force_table())
     sim.set_mode(2)
     sim.set_environment(**S.WATER)
     sim.setTimeStep(1e-4)
+    sim.set_launch_config(**cfg)
     sim.set_batch(b)
-    assert sim.launch_config()["streamed"] == 1
+    lc = sim.launch_config()
+    assert (lc["streamed"], lc["cluster"]) == ((1, 0) if cfg else (0, 4))
     sim.run_steps(200, True)
     pos, vel, stress = sim.collect_arrays()
     p, v, s = oracle(2, b, S.WATER, 200, True)

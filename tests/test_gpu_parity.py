@@ -218,12 +218,15 @@ def test_streamed_forced_bit_exact(track):
         assert bits_equal(stress, s)
 
 
-def test_large_robots_use_the_streamed_path():
+@pytest.mark.parametrize("cfg", [dict(cluster=1), dict()], ids=["streamed", "split"])
+def test_large_robots_bit_exact(cfg):
     """10x10x10-cell robots (1,331 masses, 14,230 springs) do not fit a
-    resident bin: the library streams them, with the same results."""
+    resident bin: never split, the library streams them; by default it splits
+    each over a two-CTA cluster.  Same results either way."""
     b = robots.population_batch("streamed", 6)
-    sim, pos, vel, stress = run_gpu(b, 1e-4, 150, True)
-    assert sim.launch_config()["streamed"] == 1
+    sim, pos, vel, stress = run_gpu(b, 1e-4, 150, True, cfg=cfg)
+    lc = sim.launch_config()
+    assert (lc["streamed"], lc["cluster"]) == ((1, 0) if cfg else (0, 2))
     p, v, s = run_oracle(b, 1e-4, 150, True)
     assert bits_equal(pos, p) and bits_equal(vel, v) and bits_equal(stress, s)
 

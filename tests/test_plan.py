@@ -18,9 +18,30 @@ def test_uneven_population_fills_whole_waves_evenly():
     assert st["aligned_slices"] > 5 * st["rank_slices"]
 
 
-def test_large_robots_are_streamed():
-    st = mb.plan(robots.population_batch("streamed", 8))
-    assert st["streamed"] == 1 and st["bins"] == 8 and st["threads"] == 1024
+def test_large_robots_are_split_over_clusters():
+    b = robots.population_batch("streamed", 8)
+    st = mb.plan(b)  # 10x10x10 cells: two parts of at most 8,192 springs
+    assert (st["cluster"], st["bins"], st["streamed"], st["threads"]) == (2, 16, 0, 1024)
+    assert st["max_bin_springs"] <= 8192 and st["max_smem_bytes"] <= 232448
+    # a part holds every spring touching it: the cut's springs are in both
+    assert st["active_springs"] == b.active_springs()
+    st4 = mb.plan(b, cluster=4)
+    assert (st4["cluster"], st4["bins"]) == (4, 32)
+    assert st4["max_bin_springs"] < st["max_bin_springs"]
+
+
+def test_large_robots_are_streamed_when_never_split():
+    st = mb.plan(robots.population_batch("streamed", 8), cluster=1)
+    assert st["streamed"] == 1 and st["bins"] == 8 and st["threads"] == 1024 and st["cluster"] == 0
+
+
+def test_point_cloud_robots_need_four_part_clusters():
+    b = robots.population_batch("nn", 6)
+    assert mb.plan(b)["cluster"] == 4
+    with pytest.raises(mb._lib.MercuryError):
+        mb.plan(b, cluster=2)
+    with pytest.raises(mb._lib.MercuryError):
+        mb.plan(b, cluster=3)
 
 
 def test_forced_shape_and_bins():
@@ -39,7 +60,7 @@ def test_bins_follow_the_sm_count():
 
 def test_oversized_robot_is_rejected():
     grid = np.full((20, 20, 20), 22, np.uint8)
-    with pytest.raises(mb.MercuryError) as e:
+    with pytest.raises(mb._lib.MercuryError) as e:
         mb.plan(mb.pack([robots.lattice_robot(grid)]))
     assert e.value.status == 3
 
@@ -47,6 +68,6 @@ def test_oversized_robot_is_rejected():
 def test_bad_topology_is_rejected():
     b = robots.population_batch("small", 2)
     b.pairs[0, 0] = 999
-    with pytest.raises(mb.MercuryError) as e:
+    with pytest.raises(mb._lib.MercuryError) as e:
         mb.plan(b)
     assert e.value.status == 1
