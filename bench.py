@@ -362,10 +362,11 @@ def _device_rate(sim, active, steps, track, dev):
 
 def secondary(args, batch, local_rank, dev, hbm_peak):
     """Beside the headline: the force modes (the benchmark configurations'
-    physics) on the same robots with 0.1 kg masses, the streamed workload
-    (64 robots of 10x10x10 cells, 1,331 masses and 14,230 springs each,
-    stresses tracked) and the point-cloud robots in water (256 robots of
-    500-2,000 masses, stresses tracked), with their HBM-figure rooflines."""
+    physics) on the same robots with 0.1 kg masses, and the robots too large
+    for one CTA -- 64 of 10x10x10 cells (1,331 masses, 14,230 springs each)
+    and 256 point clouds of 500-2,000 masses in water, stresses tracked --
+    on the default path (split over thread-block clusters) and on the
+    streamed kernel, with the streaming step's HBM figure."""
     import mercury_b200 as mb
     from mercury_b200 import robots
     from mercury_b200 import simulator as S
@@ -387,42 +388,44 @@ def secondary(args, batch, local_rank, dev, hbm_peak):
         out[name] = {"value": rate, "unit": "spring-updates/s", "steps": 5000,
                      "finite": bool(np.isfinite(p).all()), "config": fs.launch_config()}
         del fs
+    def large(batch, mode, env, workload):
+        """Default path (robots split over thread-block clusters) and, for
+        comparison, the streamed kernel (never split)."""
+        act = batch.active_springs()
+        hbm_b = HBM_TOPO_B + HBM_STRESS_B + HBM_MASS_B * batch.n_masses / act
+        res = {}
+        for key, cfg in (("split", {}), ("streamed", {"cluster": 1})):
+            sim = mb.Simulator(local_rank)
+            if mode:
+                sim.set_materials(mb.materials.force_table())
+                sim.set_mode(mode)
+                sim.set_environment(**env)
+            sim.setTimeStep(1e-4)
+            sim.set_launch_config(**cfg)
+            sim.set_batch(batch)
+            rate = _device_rate(sim, act, 1000, True, dev)
+            p, _, _ = sim.collect_arrays()
+            res[key] = {"value": rate, "config": sim.launch_config(), "finite": bool(np.isfinite(p).all()),
+                        "roofline": {"bound": "hbm", "achieved": rate * hbm_b / 1e9, "peak": hbm_peak,
+                                     "unit": "GB/s", "frac": rate * hbm_b / 1e9 / hbm_peak,
+                                     "bytes_per_update": hbm_b,
+                                     "note": "HBM bytes a streaming step moves per spring-update"}}
+            del sim
+        return {"value": res["split"]["value"], "unit": "spring-updates/s", "steps": 1000,
+                "workload": workload, "config": res["split"]["config"], "finite": res["split"]["finite"],
+                "vs_streamed": res["split"]["value"] / res["streamed"]["value"], "streamed_kernel": res["streamed"]}
+
     sb = robots.population_batch("streamed", 64, seed_base=4000)
-    ss = mb.Simulator(local_rank)
-    ss.setTimeStep(1e-4)
-    ss.set_batch(sb)
-    act = sb.active_springs()
-    rate = _device_rate(ss, act, 1000, True, dev)
-    hbm_b = HBM_TOPO_B + HBM_STRESS_B + HBM_MASS_B * sb.n_masses / act
-    out["streamed"] = {"value": rate, "unit": "spring-updates/s", "steps": 1000,
-                       "workload": f"64 robots of 10x10x10 cells, {sb.n_masses} masses, {act} springs, "
-                                   f"stresses tracked, reference step, dt=1e-4",
-                       "config": ss.launch_config(),
-                       "roofline": {"bound": "hbm", "achieved": rate * hbm_b / 1e9, "peak": hbm_peak,
-                                    "unit": "GB/s", "frac": rate * hbm_b / 1e9 / hbm_peak,
-                                    "bytes_per_update": hbm_b}}
-    del ss
+    out["streamed"] = large(sb, 0, None,
+                            f"64 robots of 10x10x10 cells, {sb.n_masses} masses, {sb.active_springs()} springs, "
+                            f"stresses tracked, reference step, dt=1e-4")
     # point-cloud robots in water (256 robots of 500-2,000 masses, 25 nearest
     # neighbours, stresses tracked): springs built on the device
     nb = mb.pack(robots.nn_population_device(256, mass=0.1, device=local_rank))
-    ns = mb.Simulator(local_rank)
-    ns.set_materials(mb.materials.force_table())
-    ns.set_mode(S.MODE_FORCE_WATER)
-    ns.set_environment(**S.WATER)
-    ns.setTimeStep(1e-4)
-    ns.set_batch(nb)
-    act = nb.active_springs()
-    rate = _device_rate(ns, act, 1000, True, dev)
-    hbm_b = HBM_TOPO_B + HBM_STRESS_B + HBM_MASS_B * nb.n_masses / act
-    p, _, _ = ns.collect_arrays()
-    out["nn_water"] = {"value": rate, "unit": "spring-updates/s", "steps": 1000, "finite": bool(np.isfinite(p).all()),
-                       "workload": f"256 point-cloud robots of 500-2,000 masses, 25 nearest-neighbour springs, "
-                                   f"{nb.n_masses} masses, {act} springs, water, stresses tracked, dt=1e-4",
-                       "config": ns.launch_config(),
-                       "roofline": {"bound": "hbm", "achieved": rate * hbm_b / 1e9, "peak": hbm_peak,
-                                    "unit": "GB/s", "frac": rate * hbm_b / 1e9 / hbm_peak,
-                                    "bytes_per_update": hbm_b}}
-    del ns
+    out["nn_water"] = large(nb, S.MODE_FORCE_WATER, S.WATER,
+                            f"256 point-cloud robots of 500-2,000 masses, 25 nearest-neighbour springs, "
+                            f"{nb.n_masses} masses, {nb.active_springs()} springs, water, stresses tracked, "
+                            f"dt=1e-4")
     out["devo"] = devo_bench(local_rank)
     out["build"] = build_bench(local_rank)
     out["surrogate"] = surrogate_bench(local_rank)

@@ -3,7 +3,9 @@ threads and springs per thread, and the shared-memory-vs-streamed cutover.
 
 For a population, every compiled shape that can hold its largest robot is
 tried with a few bin counts (whole waves of the GPU) and, as the streamed
-alternative, one robot per CTA; each candidate runs a short burst of steps
+alternative, one robot per CTA; when robots are too large for one CTA,
+also every split over a thread-block cluster (2, 4 or 8 parts, each part
+shape); each candidate runs a short burst of steps
 timed with CUDA events on the context's stream.  The simulator's state and
 clock are restored afterwards, the fastest candidate is applied, and the
 choice is cached per population signature (robot sizes, mode, stress
@@ -97,26 +99,35 @@ def tune(sim, batch, track: bool = False, steps: int = 300, use_cache: bool = Tr
     active = batch.active_springs()
     t0 = sim.getTotalTime()
     cands = []
+    configs = []
     for shape in kernel_shapes():
         bin_options = [0] if shape["streamed"] else [0, sms, 2 * sms, 3 * sms]
         for bins in bin_options:
-            cfg = dict(threads=shape["threads"], springs_per_thread=shape["springs_per_thread"],
-                       masses_per_thread=shape["masses_per_thread"], bins=bins, chunk=1000,
-                       use_graph=1, streamed=shape["streamed"])
-            try:
-                sim.set_launch_config(**cfg)
-                upload()
-            except _lib.MercuryError:
-                continue
-            got = sim.launch_config()
-            if any(c["config"] == got for c in cands):
-                continue
-            sim.run_steps(min(50, steps), track)  # warm-up: module load, graph
-            el = _time(sim, steps, track)
-            rate = active * steps / el
-            cands.append({"config": got, "rate": rate})
-            if verbose:
-                print(f"  {got} -> {rate:.3e} spring-updates/s", flush=True)
+            configs.append(dict(threads=shape["threads"], springs_per_thread=shape["springs_per_thread"],
+                                masses_per_thread=shape["masses_per_thread"], bins=bins, chunk=1000,
+                                use_graph=1, streamed=shape["streamed"], cluster=0))
+    from .simulator import plan
+    if plan(batch, num_sms=sms)["cluster"]:
+        # robots too large for one CTA: every cluster size and part shape
+        for cluster in (2, 4, 8):
+            for spt in (8, 10, 12):
+                configs.append(dict(threads=1024, springs_per_thread=spt, masses_per_thread=2, bins=0,
+                                    chunk=1000, use_graph=1, streamed=0, cluster=cluster))
+    for cfg in configs:
+        try:
+            sim.set_launch_config(**cfg)
+            upload()
+        except _lib.MercuryError:
+            continue
+        got = sim.launch_config()
+        if any(c["config"] == got for c in cands):
+            continue
+        sim.run_steps(min(50, steps), track)  # warm-up: module load, graph
+        el = _time(sim, steps, track)
+        rate = active * steps / el
+        cands.append({"config": got, "rate": rate})
+        if verbose:
+            print(f"  {got} -> {rate:.3e} spring-updates/s", flush=True)
     if not cands:
         raise _lib.MercuryError(3, "no launch configuration holds this population")
     best = max(cands, key=lambda c: c["rate"])
