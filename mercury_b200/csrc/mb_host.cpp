@@ -505,8 +505,8 @@ mb_status voxel_setup(mb_context* c, uint32_t R, int sx, int sy, int sz, float h
     // rows with their template size as capacity, plus spare slice columns
     {
         const bool streamed = out.streamed;
-        std::vector<uint16_t> inc;
-        std::vector<uint32_t> inc32;
+        mb::raw_vector<uint16_t> inc;
+        mb::raw_vector<uint32_t> inc32;
         uint64_t total = 0;
         for (auto& bd : out.bins) {
             const uint32_t cap = (bd.n_inc + 8 * mb::kSliceWidth + 31) / 32 * 32;

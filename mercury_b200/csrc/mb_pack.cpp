@@ -118,15 +118,25 @@ void preprocess(const mb_batch_desc* b, uint32_t r, RobotPack& p) {
         deg[a]++;
         deg[c]++;
     }
-    // order (b - a, a), ties by spring index: one unique 64-bit key each
-    std::vector<uint64_t> keys(sp.size());
-    for (size_t q = 0; q < sp.size(); ++q) {
-        const int64_t g = s0 + sp[q];
-        const int dx = (int)b->pairs[2 * g + 1] - (int)b->pairs[2 * g];
-        keys[q] = ((uint64_t)(dx + 4096) << 48) | ((uint64_t)b->pairs[2 * g] << 32) | sp[q];  // |dx| < 4096
+    // order (b - a, a), ties by spring index: sp is in index order, so two
+    // stable counting passes -- by a, then by b - a -- give exactly that
+    {
+        const size_t n = sp.size();
+        std::vector<uint32_t> tmp(n), cnt(8193);
+        auto pass = [&](const std::vector<uint32_t>& src, std::vector<uint32_t>& dst, uint32_t buckets,
+                        auto key) {
+            std::fill(cnt.begin(), cnt.begin() + buckets + 1, 0u);
+            for (uint32_t x : src) cnt[key(x) + 1]++;
+            for (uint32_t k = 0; k < buckets; ++k) cnt[k + 1] += cnt[k];
+            for (uint32_t x : src) dst[cnt[key(x)]++] = x;
+        };
+        auto key_a = [&](uint32_t ls) { return (uint32_t)b->pairs[2 * (s0 + ls)]; };
+        auto key_dx = [&](uint32_t ls) {  // |b - a| < 4096
+            return (uint32_t)((int)b->pairs[2 * (s0 + ls) + 1] - (int)b->pairs[2 * (s0 + ls)] + 4096);
+        };
+        pass(sp, tmp, 4096, key_a);
+        pass(tmp, sp, 8192, key_dx);
     }
-    std::sort(keys.begin(), keys.end());
-    for (size_t q = 0; q < sp.size(); ++q) sp[q] = (uint32_t)keys[q];
     p.n_mass = (uint32_t)cm;
     p.cost = (uint64_t)sp.size() * 4 + (uint64_t)cm;
     uint64_t est = 0;  // incidence entries with rows padded to the slice maximum
@@ -382,11 +392,18 @@ void build_bin(const mb_batch_desc* b, const std::vector<RobotPack>& packs,
         for (uint32_t r : robots) {
             const int64_t s0 = b->spring_offsets[r];
             const auto& sp = packs[r].springs;
+            // b ends in reverse spring order, then a ends in spring order:
+            // with springs ordered by (b - a, a), every row of a lattice whose
+            // springs point forward (b > a) arrives in summation order
+            for (uint32_t k = (uint32_t)sp.size(); k-- > 0;) {
+                const int64_t g = s0 + sp[k];
+                const uint32_t a = b->pairs[2 * g], c = b->pairs[2 * g + 1];
+                ents[fill[base + c]++] = {a, sp[k], 1u, sb + k, a};
+            }
             for (uint32_t k = 0; k < sp.size(); ++k) {
                 const int64_t g = s0 + sp[k];
                 const uint32_t a = b->pairs[2 * g], c = b->pairs[2 * g + 1];
                 ents[fill[base + a]++] = {c, sp[k], 0u, sb + k, c};
-                ents[fill[base + c]++] = {a, sp[k], 1u, sb + k, a};
             }
             base += packs[r].n_mass;
             sb += (uint32_t)sp.size();
@@ -435,8 +452,8 @@ void assemble(const std::vector<BinLocal>& locals, Packed& out, bool streamed, u
     out.lbar.resize(ns);
     out.slice_off.resize(nsl);
     out.slice_width.resize(nsl);
-    out.inc.assign(streamed ? 0 : ninc, 0);
-    out.inc32.assign(streamed ? ninc : 0, 0);
+    out.inc.resize(streamed ? 0 : ninc);  // every entry is copied below
+    out.inc32.resize(streamed ? ninc : 0);
     parallel_for(nb, threads, [&](uint32_t i) {
         const BinLocal& L = locals[i];
         const BinDesc& d = out.bins[i];
@@ -592,15 +609,20 @@ void build_part(const mb_batch_desc* b, uint32_t r, const RobotPack& pk, const s
     for (uint32_t i = 0; i < n_own; ++i) row_start[i + 1] += row_start[i];
     std::vector<Ent> ents(row_start[n_own]);
     std::vector<uint32_t> fill(row_start.begin(), row_start.end() - 1);
+    // b ends in reverse, then a ends in spring order (rows mostly arrive
+    // sorted, as in build_bin).  Aligned by the robot-local index of the
+    // other end: a row's column order must stay its summation order (halo
+    // masses are numbered after the own ones, so part-local indices would
+    // not keep it).
+    for (uint32_t k = ns; k-- > 0;) {
+        const int64_t g = s0 + sp[k];
+        const uint32_t a = b->pairs[2 * g], c = b->pairs[2 * g + 1];
+        if (part_of[c] == p) ents[fill[(uint32_t)local_of[c]]++] = {a, sp[k], 1u, k, a};
+    }
     for (uint32_t k = 0; k < ns; ++k) {
         const int64_t g = s0 + sp[k];
         const uint32_t a = b->pairs[2 * g], c = b->pairs[2 * g + 1];
-        const uint32_t la = (uint32_t)local_of[a], lc = (uint32_t)local_of[c];
-        // aligned by the robot-local index of the other end: a row's column
-        // order must stay its summation order (halo masses are numbered
-        // after the own ones, so part-local indices would not keep it)
-        if (part_of[a] == p) ents[fill[la]++] = {c, sp[k], 0u, k, c};
-        if (part_of[c] == p) ents[fill[lc]++] = {a, sp[k], 1u, k, a};
+        if (part_of[a] == p) ents[fill[(uint32_t)local_of[a]]++] = {c, sp[k], 0u, k, c};
     }
     sort_rows(n_own, row_start, ents);
     L.n_mass = n_own;
@@ -608,56 +630,152 @@ void build_part(const mb_batch_desc* b, uint32_t r, const RobotPack& pk, const s
     slice_rows(n_own, row_start, ents, false, L);
 }
 
-// Split packing of every robot into C parts under the shape's and the
-// shared memory's limits; false (with the reason) when a part does not fit.
-bool build_split(const mb_batch_desc* b, const std::vector<RobotPack>& packs, uint32_t C, const KernelShape& sh,
-                 uint32_t smem_cap, const std::vector<int>& slot_of, unsigned threads, Packed& out,
-                 std::string& why) {
+// Parts of every robot cut into C (the shape does not change them).
+struct SplitParts {
+    uint32_t C = 0;
+    std::vector<BinLocal> locals;                // bin r * C + p
+    std::vector<std::vector<uint32_t>> exports;  // per bin
+    std::vector<uint32_t> n_all, stride;         // per bin; per robot
+};
+
+// Cuts every robot into C parts and checks, from counts alone, that each
+// part could fit the largest of `shapes` (springs, masses, a lower bound of
+// its shared memory); false with the reason otherwise, before any rows are
+// built.
+bool split_partition(const mb_batch_desc* b, const std::vector<RobotPack>& packs, uint32_t C,
+                     const std::vector<KernelShape>& shapes, uint32_t smem_cap, unsigned threads,
+                     std::vector<std::vector<uint8_t>>& part_of, std::string& why) {
     const uint32_t R = (uint32_t)packs.size();
     uint32_t levels = 0;
     while ((1u << levels) < C) ++levels;
-    const uint32_t nb = R * C;
-    const uint64_t cap_s = std::min<uint64_t>((uint64_t)sh.threads * sh.spt, kMaxBinSprings);
-    const uint64_t cap_m = std::min<uint64_t>((uint64_t)sh.threads * sh.mpt, 4096);
-    std::vector<BinLocal> locals(nb);
-    std::vector<std::vector<uint32_t>> exports(nb);
-    std::vector<uint32_t> n_all(nb), stride(R);
+    uint64_t cap_s = 0, cap_m = 0;
+    for (const auto& sh : shapes) {
+        cap_s = std::max<uint64_t>(cap_s, std::min<uint64_t>((uint64_t)sh.threads * sh.spt, kMaxBinSprings));
+        cap_m = std::max<uint64_t>(cap_m, std::min<uint64_t>((uint64_t)sh.threads * sh.mpt, 4096));
+    }
+    part_of.assign(R, {});
+    std::atomic<bool> fits{true};
+    std::vector<std::string> reason(R);
     parallel_for(R, threads, [&](uint32_t r) {
-        std::vector<uint8_t> part_of;
-        partition_robot(b, r, levels, part_of);
+        if (!fits.load(std::memory_order_relaxed)) return;
+        partition_robot(b, r, levels, part_of[r]);
+        const auto& po = part_of[r];
+        const int64_t s0 = b->spring_offsets[r];
+        const uint32_t n = packs[r].n_mass;
+        std::vector<uint32_t> own(C, 0), ns(C, 0), halo(C, 0), exp(C, 0), mark(n, 0), deg(n, 0);
+        for (uint32_t m = 0; m < n; ++m) own[po[m]]++;
+        for (uint32_t ls : packs[r].springs) {
+            const int64_t g = s0 + ls;
+            const uint32_t a = b->pairs[2 * g], c = b->pairs[2 * g + 1];
+            const uint32_t pa = po[a], pc = po[c];
+            deg[a]++;
+            deg[c]++;
+            ns[pa]++;
+            if (pc != pa) {
+                ns[pc]++;
+                // halo marks: bit p of mark[m] once m is counted in part p
+                if (!(mark[c] & (1u << pa))) { mark[c] |= 1u << pa; halo[pa]++; }
+                if (!(mark[a] & (1u << pc))) { mark[a] |= 1u << pc; halo[pc]++; }
+            }
+        }
+        // rows: rank-layout slices of 32 own masses, as wide as their longest
+        // row (an aligned slice is never narrower); exports: one per halo copy
+        std::vector<uint32_t> rows(C, 0), in_slice(C, 0), slice_max(C, 0);
+        for (uint32_t m = 0; m < n; ++m) {
+            const uint32_t p = po[m];
+            exp[p] += (uint32_t)__builtin_popcount(mark[m]);
+            slice_max[p] = std::max(slice_max[p], deg[m]);
+            if (++in_slice[p] == kSliceWidth) {
+                rows[p] += kSliceWidth * slice_max[p];
+                in_slice[p] = slice_max[p] = 0;
+            }
+        }
+        for (uint32_t p = 0; p < C; ++p)
+            if (in_slice[p]) rows[p] += kSliceWidth * slice_max[p];
+        uint32_t stride = 0;
+        for (uint32_t p = 0; p < C; ++p) stride = std::max(stride, own[p] + halo[p]);
+        for (uint32_t p = 0; p < C; ++p) {
+            const uint64_t smem_lb = 32ull * stride + 16ull * ns[p] + 8ull * kMaxMaterialSlots + 4ull * exp[p] +
+                                     2ull * rows[p];
+            if (ns[p] > cap_s || own[p] > cap_m || own[p] + halo[p] > 4096 || smem_lb > smem_cap) {
+                char buf[256];
+                std::snprintf(buf, sizeof(buf), "part %u of robot %u: %u springs, %u + %u masses, >= %llu B shared memory",
+                              p, r, ns[p], own[p], halo[p], (unsigned long long)smem_lb);
+                reason[r] = buf;
+                fits = false;
+                return;
+            }
+        }
+    });
+    if (!fits) {
+        for (const auto& w : reason)
+            if (!w.empty()) {
+                why = w;
+                break;
+            }
+        return false;
+    }
+    return true;
+}
+
+// Builds every part (rows, halos, export lists) from a partition.
+void build_split_parts(const mb_batch_desc* b, const std::vector<RobotPack>& packs, uint32_t C,
+                       const std::vector<std::vector<uint8_t>>& part_of, const std::vector<int>& slot_of,
+                       unsigned threads, SplitParts& sp) {
+    const uint32_t R = (uint32_t)packs.size();
+    const uint32_t nb = R * C;
+    sp.C = C;
+    sp.locals.assign(nb, BinLocal{});
+    sp.exports.assign(nb, {});
+    sp.n_all.assign(nb, 0);
+    sp.stride.assign(R, 0);
+    parallel_for(R, threads, [&](uint32_t r) {
         std::vector<PartMasses> pm(C);
         std::vector<int32_t> local_of;
         for (uint32_t p = 0; p < C; ++p) {
-            build_part(b, r, packs[r], part_of, p, slot_of, local_of, locals[r * C + p], pm[p]);
-            n_all[r * C + p] = (uint32_t)(pm[p].own.size() + pm[p].halo.size());
+            build_part(b, r, packs[r], part_of[r], p, slot_of, local_of, sp.locals[r * C + p], pm[p]);
+            sp.n_all[r * C + p] = (uint32_t)(pm[p].own.size() + pm[p].halo.size());
         }
         for (uint32_t q = 0; q < C; ++q)
             for (uint32_t j = 0; j < pm[q].halo.size(); ++j) {
-                const uint32_t m = pm[q].halo[j], owner = part_of[m];
+                const uint32_t m = pm[q].halo[j], owner = part_of[r][m];
                 const auto& own = pm[owner].own;
                 const uint32_t li = (uint32_t)(std::lower_bound(own.begin(), own.end(), m) - own.begin());
                 const uint32_t slot = (uint32_t)pm[q].own.size() + j;
-                exports[r * C + owner].push_back(li | (q << 12) | (slot << 15));
+                sp.exports[r * C + owner].push_back(li | (q << 12) | (slot << 15));
             }
         uint32_t st = 0;
         for (uint32_t p = 0; p < C; ++p) {
-            std::sort(exports[r * C + p].begin(), exports[r * C + p].end());
-            st = std::max(st, n_all[r * C + p]);
+            std::sort(sp.exports[r * C + p].begin(), sp.exports[r * C + p].end());
+            st = std::max(st, sp.n_all[r * C + p]);
         }
-        stride[r] = st;
+        sp.stride[r] = st;
     });
-    char buf[256];
-    for (uint32_t i = 0; i < nb; ++i) {
-        const BinLocal& L = locals[i];
-        const uint32_t smem = split_smem_bytes(stride[i / C], L.n_spring, L.n_inc, (uint32_t)exports[i].size());
-        if (L.n_spring > cap_s || L.n_mass > cap_m || n_all[i] > 4096 || smem > smem_cap) {
+}
+
+// Whether every part fits the shape and the shared memory; the reason if not.
+bool split_fits(const SplitParts& sp, const KernelShape& sh, uint32_t smem_cap, std::string& why) {
+    const uint32_t C = sp.C;
+    const uint64_t cap_s = std::min<uint64_t>((uint64_t)sh.threads * sh.spt, kMaxBinSprings);
+    const uint64_t cap_m = std::min<uint64_t>((uint64_t)sh.threads * sh.mpt, 4096);
+    for (uint32_t i = 0; i < sp.locals.size(); ++i) {
+        const BinLocal& L = sp.locals[i];
+        const uint32_t smem = split_smem_bytes(sp.stride[i / C], L.n_spring, L.n_inc, (uint32_t)sp.exports[i].size());
+        if (L.n_spring > cap_s || L.n_mass > cap_m || sp.n_all[i] > 4096 || smem > smem_cap) {
+            char buf[256];
             std::snprintf(buf, sizeof(buf), "part %u of robot %u: %u springs, %u + %u masses, %u B shared memory",
-                          i % C, i / C, L.n_spring, L.n_mass, n_all[i] - L.n_mass, smem);
+                          i % C, i / C, L.n_spring, L.n_mass, sp.n_all[i] - L.n_mass, smem);
             why = buf;
             return false;
         }
     }
-    assemble(locals, out, false, threads);
+    return true;
+}
+
+// The packed arrays of split parts.
+void assemble_split(const SplitParts& sp, uint32_t R, unsigned threads, Packed& out) {
+    const uint32_t C = sp.C, nb = (uint32_t)sp.locals.size();
+    assemble(sp.locals, out, false, threads);
     out.robot_bin.assign(R, 0);
     out.robot_mass_base.assign(R, 0);
     for (uint32_t r = 0; r < R; ++r) out.robot_bin[r] = r * C;
@@ -665,14 +783,13 @@ bool build_split(const mb_batch_desc* b, const std::vector<RobotPack>& packs, ui
     out.max_smem = 0;
     for (uint32_t i = 0; i < nb; ++i) {
         BinDesc& d = out.bins[i];
-        d.x_stride = stride[i / C];
+        d.x_stride = sp.stride[i / C];
         d.export_begin = (uint32_t)out.exports.size();
-        d.n_export = (uint32_t)exports[i].size();
-        d.n_all = n_all[i];
-        out.exports.insert(out.exports.end(), exports[i].begin(), exports[i].end());
+        d.n_export = (uint32_t)sp.exports[i].size();
+        d.n_all = sp.n_all[i];
+        out.exports.insert(out.exports.end(), sp.exports[i].begin(), sp.exports[i].end());
         out.max_smem = std::max(out.max_smem, split_smem_bytes(d.x_stride, d.n_spring, d.n_inc, d.n_export));
     }
-    return true;
 }
 
 }  // namespace
@@ -795,18 +912,25 @@ mb_status pack_population(const mb_batch_desc* b, const PackOptions& o, Packed& 
             sshapes.push_back({o.override.threads, o.override.springs_per_thread, o.override.masses_per_thread});
         else
             for (const auto& sh : kSplit) sshapes.push_back(sh);
+        std::vector<KernelShape> compiled;
+        for (const auto& sh : sshapes)
+            if (split_supported(sh)) compiled.push_back(sh);
         for (uint32_t C : cs) {
-            for (const auto& sh : sshapes) {
-                if (!split_supported(sh)) continue;
-                if (build_split(b, packs, C, sh, o.smem_cap, slot_of, threads, out, why)) {
-                    ok = true;
-                    out.shape = sh;
-                    out.n_bins = R * C;
-                    out.grid = 0;
-                    out.cluster = C;
-                    out.streamed = false;
-                    break;
-                }
+            if (compiled.empty()) break;
+            std::vector<std::vector<uint8_t>> part_of;
+            if (!split_partition(b, packs, C, compiled, o.smem_cap, threads, part_of, why)) continue;
+            SplitParts sp;
+            build_split_parts(b, packs, C, part_of, slot_of, threads, sp);
+            for (const auto& sh : compiled) {
+                if (!split_fits(sp, sh, o.smem_cap, why)) continue;
+                assemble_split(sp, R, threads, out);
+                ok = true;
+                out.shape = sh;
+                out.n_bins = R * C;
+                out.grid = 0;
+                out.cluster = C;
+                out.streamed = false;
+                break;
             }
             if (ok) break;
         }

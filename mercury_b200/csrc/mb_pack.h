@@ -4,12 +4,37 @@
 #include <cstdint>
 #include <functional>
 #include <string>
+#include <memory>
+#include <utility>
 #include <vector>
 
 #include "../../include/mercury_b200.h"
 #include "mb_internal.h"
 
 namespace mb {
+
+// std::vector whose resize leaves new elements uninitialised: the packed
+// arrays are written in full after they are sized.
+template <class T>
+struct NoInitAlloc : std::allocator<T> {
+    template <class U>
+    struct rebind {
+        using other = NoInitAlloc<U>;
+    };
+    NoInitAlloc() = default;
+    template <class U>
+    NoInitAlloc(const NoInitAlloc<U>&) {}
+    template <class U>
+    void construct(U* p) {
+        ::new ((void*)p) U;
+    }
+    template <class U, class... A>
+    void construct(U* p, A&&... a) {
+        ::new ((void*)p) U(std::forward<A>(a)...);
+    }
+};
+template <class T>
+using raw_vector = std::vector<T, NoInitAlloc<T>>;
 
 struct PackOptions {
     uint32_t sms = 148;            // SMs of the device
@@ -30,12 +55,13 @@ struct Packed {
     bool streamed = false;
     uint32_t max_smem = 0;
     std::vector<BinDesc> bins;
-    std::vector<uint32_t> mass_gidx, spring_gidx, pair, slice_off, slice_width, robot_bin;
+    raw_vector<uint32_t> mass_gidx, spring_gidx, pair, slice_off, slice_width;
+    std::vector<uint32_t> robot_bin;
     std::vector<uint32_t> robot_mass_base;  // bin-local index of each robot's first mass
-    std::vector<uint16_t> inc;    // resident rows
-    std::vector<uint32_t> inc32;  // streamed rows
+    raw_vector<uint16_t> inc;    // resident rows
+    raw_vector<uint32_t> inc32;  // streamed rows
     std::vector<uint32_t> exports;  // split bins: own mass | part << 12 | halo slot << 15
-    std::vector<float> lbar;
+    raw_vector<float> lbar;
     std::vector<uint8_t> mat_ids;
     // statistics
     uint64_t masses = 0, active_springs = 0, inc_entries = 0, inc_padding = 0;
