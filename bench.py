@@ -296,7 +296,9 @@ def run_ours(args, rank, local_rank, world):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(batch, dt, track)
 
-    extra = {} if args.no_extra else secondary(args, batch, local_rank, dev, hbm_peak)
+    # single-GPU lines beside the headline: measured at N = 1 only (at N > 1
+    # every GPU would repeat them while all are held)
+    extra = {} if (args.no_extra or world > 1) else secondary(args, batch, local_rank, dev, hbm_peak)
 
     line = {
         "metric": "spring-updates/s",
