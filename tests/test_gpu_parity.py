@@ -85,20 +85,20 @@ def test_nonzero_start_clock_and_velocity():
 
 
 SHAPES = [
-    dict(threads=256, springs_per_thread=16, masses_per_thread=4),
+    dict(threads=256, springs_per_thread=8, masses_per_thread=2),
     dict(threads=512, springs_per_thread=16, masses_per_thread=4),
     dict(threads=512, springs_per_thread=8, masses_per_thread=2),
     dict(threads=1024, springs_per_thread=8, masses_per_thread=2),
     dict(threads=1024, springs_per_thread=4, masses_per_thread=1),
+    dict(threads=1024, springs_per_thread=12, masses_per_thread=2),
 ]
 
 
 @pytest.mark.parametrize("shape", SHAPES, ids=lambda s: f"{s['threads']}x{s['springs_per_thread']}")
 def test_launch_shape_does_not_change_bits(shape):
+    """Every compiled shape.  Robots larger than the shape's capacity are
+    split over clusters (1,024-thread shapes) or streamed: same bits."""
     b = robots.population_batch("uneven", 24, seed_base=500)
-    cap = shape["threads"] * shape["springs_per_thread"]
-    if max(int(np.count_nonzero(b.spring_material[b.robot_slices(r)[1]])) for r in range(b.n_robots)) > cap:
-        pytest.skip("robot larger than this shape")
     # automatic bin count: several robots per CTA, within the shape's capacity
     _, pos, vel, stress = run_gpu(b, 1e-3, 120, True, cfg=dict(shape, chunk=37))
     p, v, s = run_oracle(b, 1e-3, 120, True)
