@@ -144,6 +144,7 @@ struct mb_context {
     uint32_t stream_mpt = 2;
     mb::DevBuf<uint32_t> inc32;
     mb::DevBuf<uint32_t> exports;          // split bins: halo positions each part writes into the others
+    mb::Packed upload_pack;                // host packing of the last mb_set_elements (reused)
     uint32_t cluster = 0;                  // split bins: CTAs per robot (0 = not split)
     mb::DevBuf<float4> dp_scratch;
     mb::DevBuf<float> st_scratch;
@@ -825,7 +826,8 @@ mb_status mb_set_elements(mb_context* ctx, const mb_batch_desc* b) {
             h_lbar.assign(b->lbar, b->lbar + S);
         }
     });
-    mb::Packed out;
+    // kept in the context: its arrays keep their capacity across uploads
+    mb::Packed& out = ctx->upload_pack;
     const mb_status pst = mb_detail::pack(ctx, b, false, out, true);
     copier.join();
     if (pst != MB_OK) return pst;
