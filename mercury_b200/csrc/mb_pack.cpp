@@ -630,82 +630,101 @@ void build_part(const mb_batch_desc* b, uint32_t r, const RobotPack& pk, const s
     slice_rows(n_own, row_start, ents, false, L);
 }
 
-// Parts of every robot cut into C (the shape does not change them).
+// Split robots placed in clusters of C CTAs: robot r has parts[r] parts in
+// bins first[r] .. first[r] + parts[r] - 1, all inside one cluster (bins
+// k*C .. k*C + C-1); slots no robot uses stay empty bins.
 struct SplitParts {
     uint32_t C = 0;
-    std::vector<BinLocal> locals;                // bin r * C + p
+    std::vector<uint32_t> parts, first;          // per robot
+    std::vector<BinLocal> locals;                // per bin
     std::vector<std::vector<uint32_t>> exports;  // per bin
-    std::vector<uint32_t> n_all, stride;         // per bin; per robot
+    std::vector<uint32_t> n_all;                 // per bin
+    std::vector<uint32_t> stride;                // per cluster
 };
 
-// Cuts every robot into C parts and checks, from counts alone, that each
-// part could fit the largest of `shapes` (springs, masses, a lower bound of
-// its shared memory); false with the reason otherwise, before any rows are
-// built.
-bool split_partition(const mb_batch_desc* b, const std::vector<RobotPack>& packs, uint32_t C,
-                     const std::vector<KernelShape>& shapes, uint32_t smem_cap, unsigned threads,
-                     std::vector<std::vector<uint8_t>>& part_of, std::string& why) {
-    const uint32_t R = (uint32_t)packs.size();
+// Cuts robot r into P parts (part_of) and checks, from counts alone, that
+// each could fit cap_s springs, cap_m own masses and the shared memory (a
+// lower bound: the rank-layout rows, the exact halo and export counts).
+bool robot_parts_fit(const mb_batch_desc* b, const RobotPack& pk, uint32_t r, uint32_t P, uint64_t cap_s,
+                     uint64_t cap_m, uint32_t smem_cap, std::vector<uint8_t>& part_of, std::string* reason) {
     uint32_t levels = 0;
-    while ((1u << levels) < C) ++levels;
-    uint64_t cap_s = 0, cap_m = 0;
+    while ((1u << levels) < P) ++levels;
+    partition_robot(b, r, levels, part_of);
+    const auto& po = part_of;
+    const int64_t s0 = b->spring_offsets[r];
+    const uint32_t n = pk.n_mass;
+    std::vector<uint32_t> own(P, 0), ns(P, 0), halo(P, 0), exp(P, 0), mark(n, 0), deg(n, 0);
+    for (uint32_t m = 0; m < n; ++m) own[po[m]]++;
+    for (uint32_t ls : pk.springs) {
+        const int64_t g = s0 + ls;
+        const uint32_t a = b->pairs[2 * g], c = b->pairs[2 * g + 1];
+        const uint32_t pa = po[a], pc = po[c];
+        deg[a]++;
+        deg[c]++;
+        ns[pa]++;
+        if (pc != pa) {
+            ns[pc]++;
+            // halo marks: bit p of mark[m] once m is counted in part p
+            if (!(mark[c] & (1u << pa))) { mark[c] |= 1u << pa; halo[pa]++; }
+            if (!(mark[a] & (1u << pc))) { mark[a] |= 1u << pc; halo[pc]++; }
+        }
+    }
+    // rows: rank-layout slices of 32 own masses, as wide as their longest
+    // row (an aligned slice is never narrower); exports: one per halo copy
+    std::vector<uint32_t> rows(P, 0), in_slice(P, 0), slice_max(P, 0);
+    for (uint32_t m = 0; m < n; ++m) {
+        const uint32_t p = po[m];
+        exp[p] += (uint32_t)__builtin_popcount(mark[m]);
+        slice_max[p] = std::max(slice_max[p], deg[m]);
+        if (++in_slice[p] == kSliceWidth) {
+            rows[p] += kSliceWidth * slice_max[p];
+            in_slice[p] = slice_max[p] = 0;
+        }
+    }
+    for (uint32_t p = 0; p < P; ++p)
+        if (in_slice[p]) rows[p] += kSliceWidth * slice_max[p];
+    uint32_t stride = 0;
+    for (uint32_t p = 0; p < P; ++p) stride = std::max(stride, own[p] + halo[p]);
+    for (uint32_t p = 0; p < P; ++p) {
+        const uint64_t smem_lb = 32ull * stride + 16ull * ns[p] + 8ull * kMaxMaterialSlots + 4ull * exp[p] +
+                                 2ull * rows[p];
+        if (ns[p] > cap_s || own[p] > cap_m || own[p] + halo[p] > 4096 || smem_lb > smem_cap) {
+            if (reason) {
+                char buf[256];
+                std::snprintf(buf, sizeof(buf),
+                              "part %u of robot %u: %u springs, %u + %u masses, >= %llu B shared memory", p, r,
+                              ns[p], own[p], halo[p], (unsigned long long)smem_lb);
+                *reason = buf;
+            }
+            return false;
+        }
+    }
+    return true;
+}
+
+// Capacity of the largest of `shapes`.
+void split_caps(const std::vector<KernelShape>& shapes, uint64_t& cap_s, uint64_t& cap_m) {
+    cap_s = cap_m = 0;
     for (const auto& sh : shapes) {
         cap_s = std::max<uint64_t>(cap_s, std::min<uint64_t>((uint64_t)sh.threads * sh.spt, kMaxBinSprings));
         cap_m = std::max<uint64_t>(cap_m, std::min<uint64_t>((uint64_t)sh.threads * sh.mpt, 4096));
     }
+}
+
+// Every robot cut into C parts (one cluster each), checked from counts
+// before any rows are built; false with the reason otherwise.
+bool split_partition(const mb_batch_desc* b, const std::vector<RobotPack>& packs, uint32_t C,
+                     const std::vector<KernelShape>& shapes, uint32_t smem_cap, unsigned threads,
+                     std::vector<std::vector<uint8_t>>& part_of, std::string& why) {
+    const uint32_t R = (uint32_t)packs.size();
+    uint64_t cap_s, cap_m;
+    split_caps(shapes, cap_s, cap_m);
     part_of.assign(R, {});
     std::atomic<bool> fits{true};
     std::vector<std::string> reason(R);
     parallel_for(R, threads, [&](uint32_t r) {
         if (!fits.load(std::memory_order_relaxed)) return;
-        partition_robot(b, r, levels, part_of[r]);
-        const auto& po = part_of[r];
-        const int64_t s0 = b->spring_offsets[r];
-        const uint32_t n = packs[r].n_mass;
-        std::vector<uint32_t> own(C, 0), ns(C, 0), halo(C, 0), exp(C, 0), mark(n, 0), deg(n, 0);
-        for (uint32_t m = 0; m < n; ++m) own[po[m]]++;
-        for (uint32_t ls : packs[r].springs) {
-            const int64_t g = s0 + ls;
-            const uint32_t a = b->pairs[2 * g], c = b->pairs[2 * g + 1];
-            const uint32_t pa = po[a], pc = po[c];
-            deg[a]++;
-            deg[c]++;
-            ns[pa]++;
-            if (pc != pa) {
-                ns[pc]++;
-                // halo marks: bit p of mark[m] once m is counted in part p
-                if (!(mark[c] & (1u << pa))) { mark[c] |= 1u << pa; halo[pa]++; }
-                if (!(mark[a] & (1u << pc))) { mark[a] |= 1u << pc; halo[pc]++; }
-            }
-        }
-        // rows: rank-layout slices of 32 own masses, as wide as their longest
-        // row (an aligned slice is never narrower); exports: one per halo copy
-        std::vector<uint32_t> rows(C, 0), in_slice(C, 0), slice_max(C, 0);
-        for (uint32_t m = 0; m < n; ++m) {
-            const uint32_t p = po[m];
-            exp[p] += (uint32_t)__builtin_popcount(mark[m]);
-            slice_max[p] = std::max(slice_max[p], deg[m]);
-            if (++in_slice[p] == kSliceWidth) {
-                rows[p] += kSliceWidth * slice_max[p];
-                in_slice[p] = slice_max[p] = 0;
-            }
-        }
-        for (uint32_t p = 0; p < C; ++p)
-            if (in_slice[p]) rows[p] += kSliceWidth * slice_max[p];
-        uint32_t stride = 0;
-        for (uint32_t p = 0; p < C; ++p) stride = std::max(stride, own[p] + halo[p]);
-        for (uint32_t p = 0; p < C; ++p) {
-            const uint64_t smem_lb = 32ull * stride + 16ull * ns[p] + 8ull * kMaxMaterialSlots + 4ull * exp[p] +
-                                     2ull * rows[p];
-            if (ns[p] > cap_s || own[p] > cap_m || own[p] + halo[p] > 4096 || smem_lb > smem_cap) {
-                char buf[256];
-                std::snprintf(buf, sizeof(buf), "part %u of robot %u: %u springs, %u + %u masses, >= %llu B shared memory",
-                              p, r, ns[p], own[p], halo[p], (unsigned long long)smem_lb);
-                reason[r] = buf;
-                fits = false;
-                return;
-            }
-        }
+        if (!robot_parts_fit(b, packs[r], r, C, cap_s, cap_m, smem_cap, part_of[r], &reason[r])) fits = false;
     });
     if (!fits) {
         for (const auto& w : reason)
@@ -718,39 +737,81 @@ bool split_partition(const mb_batch_desc* b, const std::vector<RobotPack>& packs
     return true;
 }
 
-// Builds every part (rows, halos, export lists) from a partition.
-void build_split_parts(const mb_batch_desc* b, const std::vector<RobotPack>& packs, uint32_t C,
+// Each robot at its fewest parts (1, 2, 4 or 8) that fit `shape` by the
+// counts; false if some robot needs more than 8.
+bool split_partition_mixed(const mb_batch_desc* b, const std::vector<RobotPack>& packs, const KernelShape& shape,
+                           uint32_t smem_cap, unsigned threads, std::vector<std::vector<uint8_t>>& part_of,
+                           std::vector<uint32_t>& parts) {
+    const uint32_t R = (uint32_t)packs.size();
+    uint64_t cap_s, cap_m;
+    split_caps({shape}, cap_s, cap_m);
+    part_of.assign(R, {});
+    parts.assign(R, 0);
+    std::atomic<bool> fits{true};
+    parallel_for(R, threads, [&](uint32_t r) {
+        if (!fits.load(std::memory_order_relaxed)) return;
+        for (uint32_t P = 1; P <= 8; P *= 2)
+            if (robot_parts_fit(b, packs[r], r, P, cap_s, cap_m, smem_cap, part_of[r], nullptr)) {
+                parts[r] = P;
+                return;
+            }
+        fits = false;
+    });
+    return fits;
+}
+
+// Places robots in clusters of C slots, robots with more parts first (parts
+// are powers of two, so the slots fill without gaps but in the last
+// cluster); returns the number of clusters.
+uint32_t place_parts(const std::vector<uint32_t>& parts, uint32_t C, std::vector<uint32_t>& first) {
+    const uint32_t R = (uint32_t)parts.size();
+    std::vector<uint32_t> order(R);
+    for (uint32_t i = 0; i < R; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) { return parts[x] > parts[y]; });
+    first.assign(R, 0);
+    uint32_t cluster = 0, slot = 0;
+    for (uint32_t r : order) {
+        if (slot + parts[r] > C) {
+            ++cluster;
+            slot = 0;
+        }
+        first[r] = cluster * C + slot;
+        slot += parts[r];
+    }
+    return R ? cluster + 1 : 0;
+}
+
+// Builds every part (rows, halos, export lists) from a partition and a
+// placement (sp.C, sp.parts, sp.first set).
+void build_split_parts(const mb_batch_desc* b, const std::vector<RobotPack>& packs, uint32_t n_clusters,
                        const std::vector<std::vector<uint8_t>>& part_of, const std::vector<int>& slot_of,
                        unsigned threads, SplitParts& sp) {
     const uint32_t R = (uint32_t)packs.size();
-    const uint32_t nb = R * C;
-    sp.C = C;
+    const uint32_t C = sp.C, nb = n_clusters * C;
     sp.locals.assign(nb, BinLocal{});
     sp.exports.assign(nb, {});
     sp.n_all.assign(nb, 0);
-    sp.stride.assign(R, 0);
+    sp.stride.assign(n_clusters, 0);
     parallel_for(R, threads, [&](uint32_t r) {
-        std::vector<PartMasses> pm(C);
+        const uint32_t P = sp.parts[r], base = sp.first[r], slot0 = base % C;
+        std::vector<PartMasses> pm(P);
         std::vector<int32_t> local_of;
-        for (uint32_t p = 0; p < C; ++p) {
-            build_part(b, r, packs[r], part_of[r], p, slot_of, local_of, sp.locals[r * C + p], pm[p]);
-            sp.n_all[r * C + p] = (uint32_t)(pm[p].own.size() + pm[p].halo.size());
+        for (uint32_t p = 0; p < P; ++p) {
+            build_part(b, r, packs[r], part_of[r], p, slot_of, local_of, sp.locals[base + p], pm[p]);
+            sp.n_all[base + p] = (uint32_t)(pm[p].own.size() + pm[p].halo.size());
         }
-        for (uint32_t q = 0; q < C; ++q)
+        // export entries name the destination by its rank in the cluster
+        for (uint32_t q = 0; q < P; ++q)
             for (uint32_t j = 0; j < pm[q].halo.size(); ++j) {
                 const uint32_t m = pm[q].halo[j], owner = part_of[r][m];
                 const auto& own = pm[owner].own;
                 const uint32_t li = (uint32_t)(std::lower_bound(own.begin(), own.end(), m) - own.begin());
                 const uint32_t slot = (uint32_t)pm[q].own.size() + j;
-                sp.exports[r * C + owner].push_back(li | (q << 12) | (slot << 15));
+                sp.exports[base + owner].push_back(li | ((slot0 + q) << 12) | (slot << 15));
             }
-        uint32_t st = 0;
-        for (uint32_t p = 0; p < C; ++p) {
-            std::sort(sp.exports[r * C + p].begin(), sp.exports[r * C + p].end());
-            st = std::max(st, sp.n_all[r * C + p]);
-        }
-        sp.stride[r] = st;
+        for (uint32_t p = 0; p < P; ++p) std::sort(sp.exports[base + p].begin(), sp.exports[base + p].end());
     });
+    for (uint32_t i = 0; i < nb; ++i) sp.stride[i / C] = std::max(sp.stride[i / C], sp.n_all[i]);
 }
 
 // Whether every part fits the shape and the shared memory; the reason if not.
@@ -763,8 +824,8 @@ bool split_fits(const SplitParts& sp, const KernelShape& sh, uint32_t smem_cap, 
         const uint32_t smem = split_smem_bytes(sp.stride[i / C], L.n_spring, L.n_inc, (uint32_t)sp.exports[i].size());
         if (L.n_spring > cap_s || L.n_mass > cap_m || sp.n_all[i] > 4096 || smem > smem_cap) {
             char buf[256];
-            std::snprintf(buf, sizeof(buf), "part %u of robot %u: %u springs, %u + %u masses, %u B shared memory",
-                          i % C, i / C, L.n_spring, L.n_mass, sp.n_all[i] - L.n_mass, smem);
+            std::snprintf(buf, sizeof(buf), "part in bin %u (cluster %u): %u springs, %u + %u masses, %u B shared memory",
+                          i, i / C, L.n_spring, L.n_mass, sp.n_all[i] - L.n_mass, smem);
             why = buf;
             return false;
         }
@@ -778,7 +839,7 @@ void assemble_split(const SplitParts& sp, uint32_t R, unsigned threads, Packed& 
     assemble(sp.locals, out, false, threads);
     out.robot_bin.assign(R, 0);
     out.robot_mass_base.assign(R, 0);
-    for (uint32_t r = 0; r < R; ++r) out.robot_bin[r] = r * C;
+    for (uint32_t r = 0; r < R; ++r) out.robot_bin[r] = sp.first[r];
     out.exports.clear();
     out.max_smem = 0;
     for (uint32_t i = 0; i < nb; ++i) {
@@ -915,24 +976,45 @@ mb_status pack_population(const mb_batch_desc* b, const PackOptions& o, Packed& 
         std::vector<KernelShape> compiled;
         for (const auto& sh : sshapes)
             if (split_supported(sh)) compiled.push_back(sh);
+        auto accept = [&](SplitParts& sp, const KernelShape& sh, uint32_t n_clusters) {
+            assemble_split(sp, R, threads, out);
+            ok = true;
+            out.shape = sh;
+            out.n_bins = n_clusters * sp.C;
+            out.grid = 0;
+            out.cluster = sp.C;
+            out.streamed = false;
+        };
+        // automatic: every robot at its fewest parts, robots sharing clusters
+        if (force_c == 0)
+            for (const auto& sh : compiled) {
+                std::vector<std::vector<uint8_t>> part_of;
+                SplitParts sp;
+                if (!split_partition_mixed(b, packs, sh, o.smem_cap, threads, part_of, sp.parts)) continue;
+                sp.C = *std::max_element(sp.parts.begin(), sp.parts.end());
+                if (sp.C < 2) continue;  // every robot fits a CTA alone: not a split population
+                const uint32_t ncl = place_parts(sp.parts, sp.C, sp.first);
+                build_split_parts(b, packs, ncl, part_of, slot_of, threads, sp);
+                if (!split_fits(sp, sh, o.smem_cap, why)) continue;
+                accept(sp, sh, ncl);
+                break;
+            }
+        // forced (or when the mixed placement fails): every robot in C parts
         for (uint32_t C : cs) {
-            if (compiled.empty()) break;
+            if (ok || compiled.empty()) break;
             std::vector<std::vector<uint8_t>> part_of;
             if (!split_partition(b, packs, C, compiled, o.smem_cap, threads, part_of, why)) continue;
             SplitParts sp;
-            build_split_parts(b, packs, C, part_of, slot_of, threads, sp);
+            sp.C = C;
+            sp.parts.assign(R, C);
+            sp.first.resize(R);
+            for (uint32_t r = 0; r < R; ++r) sp.first[r] = r * C;
+            build_split_parts(b, packs, R, part_of, slot_of, threads, sp);
             for (const auto& sh : compiled) {
                 if (!split_fits(sp, sh, o.smem_cap, why)) continue;
-                assemble_split(sp, R, threads, out);
-                ok = true;
-                out.shape = sh;
-                out.n_bins = R * C;
-                out.grid = 0;
-                out.cluster = C;
-                out.streamed = false;
+                accept(sp, sh, R);
                 break;
             }
-            if (ok) break;
         }
         if (!ok && force_c > 1) {
             err = "robots do not fit a split over " + std::to_string(force_c) + " CTAs: " + why;

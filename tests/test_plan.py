@@ -71,3 +71,14 @@ def test_bad_topology_is_rejected():
     with pytest.raises(mb._lib.MercuryError) as e:
         mb.plan(b)
     assert e.value.status == 1
+
+
+def test_split_robots_take_their_fewest_parts_and_share_clusters():
+    """Automatic split: each robot is cut into as few parts as fit, and
+    robots with fewer parts than the cluster size share a cluster."""
+    b = robots.population_batch("nn", 24)
+    auto, uniform = mb.plan(b), mb.plan(b, cluster=4)
+    assert auto["cluster"] == uniform["cluster"] == 4
+    assert auto["bins"] % 4 == 0 and auto["bins"] < uniform["bins"] == 96
+    assert auto["active_springs"] == uniform["active_springs"] == b.active_springs()
+    assert auto["max_smem_bytes"] <= 232448
