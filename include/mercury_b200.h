@@ -97,8 +97,9 @@ typedef struct mb_batch_desc {
  * cluster: 2, 4 or 8 = split every robot into that many parts, one CTA
  * each, the parts of a robot forming a thread-block cluster that exchanges
  * boundary positions through distributed shared memory; 1 = never split;
- * 0 = automatic (split when a robot does not fit a resident bin and its
- * parts fit a cluster of at most 8, else streamed).  Reading the
+ * 0 = automatic (split when a robot does not fit a resident bin: each
+ * robot into the fewest parts that fit, at most 8, robots with fewer parts
+ * sharing a cluster; streamed when no split fits).  Reading the
  * configuration reports the cluster size in use (0 = not split). */
 typedef struct mb_launch_config {
     uint32_t threads;
