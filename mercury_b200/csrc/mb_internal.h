@@ -28,7 +28,7 @@ struct BinDesc {
     uint32_t slice_begin;  // first slice descriptor
     uint32_t row_cap;      // incidence entries the bin's row region holds (device re-pack)
     // split bins (one part of a robot simulated by a cluster of CTAs):
-    uint32_t x_stride;     // float4 slots of one predicted-position buffer (cluster maximum)
+    uint32_t x_stride;     // float4 slots of one predicted-position buffer (own + halo masses)
     uint32_t export_begin; // first export entry (own mass | rank << 12 | slot << 15)
     uint32_t n_export;
     uint32_t n_all;        // own + halo masses
@@ -128,10 +128,13 @@ __host__ __device__ inline uint32_t bin_smem_bytes_dev(uint32_t n_mass, uint32_t
 }
 
 // Split bins: two predicted-position buffers of x_stride slots, the
-// corrections, the material factors, the export list and the rows.
+// corrections, the material factors, the buffer strides of the cluster's
+// parts, the export list and the rows.
+constexpr uint32_t kMaxClusterParts = 8;
 __host__ __device__ inline uint32_t split_smem_bytes(uint32_t x_stride, uint32_t n_spring, uint32_t n_inc,
                                                      uint32_t n_export) {
-    return 32u * x_stride + 16u * n_spring + 8u * kMaxMaterialSlots + 4u * n_export + 2u * n_inc;
+    return 32u * x_stride + 16u * n_spring + 8u * kMaxMaterialSlots + 4u * kMaxClusterParts + 4u * n_export +
+           2u * n_inc;
 }
 
 // Largest dynamic shared memory the step kernel may use on this device.

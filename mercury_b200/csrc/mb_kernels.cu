@@ -134,13 +134,19 @@ __global__ void __launch_bounds__(T, 1024 / T) step_kernel(const StepParams p) {
         float4* sxt = smem4;
         float4* sdp = sxt + (SPLIT ? 2u * bd.x_stride : bd.n_mass);  // corrections dp, one float4 per spring
         float2* smat = reinterpret_cast<float2*>(sdp + bd.n_spring);  // {dL0 sin(..), 1/K} per slot
-        uint32_t* sexp = reinterpret_cast<uint32_t*>(smat + kMaxMaterialSlots);  // split bins: exports
+        // split bins: the buffer stride of every part of the cluster, then
+        // the export list
+        uint32_t* sstride = reinterpret_cast<uint32_t*>(smat + kMaxMaterialSlots);
+        uint32_t* sexp = sstride + (SPLIT ? kMaxClusterParts : 0u);
         uint16_t* sinc = reinterpret_cast<uint16_t*>(sexp + (SPLIT ? bd.n_export : 0u));
 
         const uint32_t n_mat = *p.n_mat;
         for (uint32_t i = tid; i < bd.n_inc; i += T) sinc[i] = __ldg(&p.inc[bd.inc_begin + i]);
-        if (SPLIT)
+        if (SPLIT) {
             for (uint32_t i = tid; i < bd.n_export; i += T) sexp[i] = __ldg(&p.exports[bd.export_begin + i]);
+            const cg::cluster_group cl = cg::this_cluster();
+            if (tid < cl.num_blocks()) sstride[tid] = p.bins[b - cl.block_rank() + tid].x_stride;
+        }
         float next_rate = 0.0f;  // actuation factor of material tid for the coming step
         if (tid < n_mat) {
             smat[tid].y = __ldg(&p.invk[tid]);  // 1/K (reference step) or k (force modes)
@@ -213,13 +219,13 @@ __global__ void __launch_bounds__(T, 1024 / T) step_kernel(const StepParams p) {
             __syncthreads();
             if (SPLIT) {
                 // masses the other parts hold as halo, into their buffer of
-                // this step (same offset in every part); the cluster barrier
+                // this step (at the part's own stride); the cluster barrier
                 // makes them visible.  A part is at most one step ahead of
                 // another, so the other buffer is never read meanwhile.
                 cg::cluster_group cl = cg::this_cluster();
                 for (uint32_t i = tid; i < bd.n_export; i += T) {
-                    const uint32_t ex = sexp[i];
-                    float4* dst = cl.map_shared_rank(X, (ex >> 12) & 7u);
+                    const uint32_t ex = sexp[i], q = (ex >> 12) & 7u;
+                    float4* dst = cl.map_shared_rank(sxt, q) + (step & 1u) * sstride[q];
                     dst[ex >> 15] = X[ex & 0xFFFu];
                 }
                 cl.sync();

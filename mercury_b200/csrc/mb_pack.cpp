@@ -632,21 +632,24 @@ void build_part(const mb_batch_desc* b, uint32_t r, const RobotPack& pk, const s
 
 // Split robots placed in clusters of C CTAs: robot r has parts[r] parts in
 // bins first[r] .. first[r] + parts[r] - 1, all inside one cluster (bins
-// k*C .. k*C + C-1); slots no robot uses stay empty bins.
+// k*C .. k*C + C-1); slots no robot uses stay empty bins.  A part's
+// predicted-position buffers hold its own and halo masses (n_all).
 struct SplitParts {
     uint32_t C = 0;
     std::vector<uint32_t> parts, first;          // per robot
     std::vector<BinLocal> locals;                // per bin
     std::vector<std::vector<uint32_t>> exports;  // per bin
     std::vector<uint32_t> n_all;                 // per bin
-    std::vector<uint32_t> stride;                // per cluster
 };
 
 // Cuts robot r into P parts (part_of) and checks, from counts alone, that
-// each could fit cap_s springs, cap_m own masses and the shared memory (a
-// lower bound: the rank-layout rows, the exact halo and export counts).
+// each could fit cap_s springs, cap_m own masses and the shared memory.
+// Springs, halo and exports are counted exactly; a slice of rows is as wide
+// as its longest row in the rank layout and at most 4 columns wider when
+// aligned, so `upper` makes the check sufficient, otherwise necessary.
 bool robot_parts_fit(const mb_batch_desc* b, const RobotPack& pk, uint32_t r, uint32_t P, uint64_t cap_s,
-                     uint64_t cap_m, uint32_t smem_cap, std::vector<uint8_t>& part_of, std::string* reason) {
+                     uint64_t cap_m, uint32_t smem_cap, bool upper, std::vector<uint8_t>& part_of,
+                     std::string* reason) {
     uint32_t levels = 0;
     while ((1u << levels) < P) ++levels;
     partition_robot(b, r, levels, part_of);
@@ -669,25 +672,22 @@ bool robot_parts_fit(const mb_batch_desc* b, const RobotPack& pk, uint32_t r, ui
             if (!(mark[a] & (1u << pc))) { mark[a] |= 1u << pc; halo[pc]++; }
         }
     }
-    // rows: rank-layout slices of 32 own masses, as wide as their longest
-    // row (an aligned slice is never narrower); exports: one per halo copy
+    // rows: slices of 32 own masses (see above); exports: one per halo copy
+    const uint32_t widen = upper ? 4u : 0u;
     std::vector<uint32_t> rows(P, 0), in_slice(P, 0), slice_max(P, 0);
     for (uint32_t m = 0; m < n; ++m) {
         const uint32_t p = po[m];
         exp[p] += (uint32_t)__builtin_popcount(mark[m]);
         slice_max[p] = std::max(slice_max[p], deg[m]);
         if (++in_slice[p] == kSliceWidth) {
-            rows[p] += kSliceWidth * slice_max[p];
+            rows[p] += kSliceWidth * (slice_max[p] + widen);
             in_slice[p] = slice_max[p] = 0;
         }
     }
     for (uint32_t p = 0; p < P; ++p)
-        if (in_slice[p]) rows[p] += kSliceWidth * slice_max[p];
-    uint32_t stride = 0;
-    for (uint32_t p = 0; p < P; ++p) stride = std::max(stride, own[p] + halo[p]);
+        if (in_slice[p]) rows[p] += kSliceWidth * (slice_max[p] + widen);
     for (uint32_t p = 0; p < P; ++p) {
-        const uint64_t smem_lb = 32ull * stride + 16ull * ns[p] + 8ull * kMaxMaterialSlots + 4ull * exp[p] +
-                                 2ull * rows[p];
+        const uint64_t smem_lb = split_smem_bytes(own[p] + halo[p], ns[p], 0, exp[p]) + 2ull * rows[p];
         if (ns[p] > cap_s || own[p] > cap_m || own[p] + halo[p] > 4096 || smem_lb > smem_cap) {
             if (reason) {
                 char buf[256];
@@ -724,7 +724,8 @@ bool split_partition(const mb_batch_desc* b, const std::vector<RobotPack>& packs
     std::vector<std::string> reason(R);
     parallel_for(R, threads, [&](uint32_t r) {
         if (!fits.load(std::memory_order_relaxed)) return;
-        if (!robot_parts_fit(b, packs[r], r, C, cap_s, cap_m, smem_cap, part_of[r], &reason[r])) fits = false;
+        if (!robot_parts_fit(b, packs[r], r, C, cap_s, cap_m, smem_cap, false, part_of[r], &reason[r]))
+            fits = false;
     });
     if (!fits) {
         for (const auto& w : reason)
@@ -737,8 +738,8 @@ bool split_partition(const mb_batch_desc* b, const std::vector<RobotPack>& packs
     return true;
 }
 
-// Each robot at its fewest parts (1, 2, 4 or 8) that fit `shape` by the
-// counts; false if some robot needs more than 8.
+// Each robot at its fewest parts (1, 2, 4 or 8) that surely fit `shape`
+// (the sufficient check); false if some robot needs more than 8.
 bool split_partition_mixed(const mb_batch_desc* b, const std::vector<RobotPack>& packs, const KernelShape& shape,
                            uint32_t smem_cap, unsigned threads, std::vector<std::vector<uint8_t>>& part_of,
                            std::vector<uint32_t>& parts) {
@@ -751,7 +752,7 @@ bool split_partition_mixed(const mb_batch_desc* b, const std::vector<RobotPack>&
     parallel_for(R, threads, [&](uint32_t r) {
         if (!fits.load(std::memory_order_relaxed)) return;
         for (uint32_t P = 1; P <= 8; P *= 2)
-            if (robot_parts_fit(b, packs[r], r, P, cap_s, cap_m, smem_cap, part_of[r], nullptr)) {
+            if (robot_parts_fit(b, packs[r], r, P, cap_s, cap_m, smem_cap, true, part_of[r], nullptr)) {
                 parts[r] = P;
                 return;
             }
@@ -791,7 +792,6 @@ void build_split_parts(const mb_batch_desc* b, const std::vector<RobotPack>& pac
     sp.locals.assign(nb, BinLocal{});
     sp.exports.assign(nb, {});
     sp.n_all.assign(nb, 0);
-    sp.stride.assign(n_clusters, 0);
     parallel_for(R, threads, [&](uint32_t r) {
         const uint32_t P = sp.parts[r], base = sp.first[r], slot0 = base % C;
         std::vector<PartMasses> pm(P);
@@ -811,7 +811,6 @@ void build_split_parts(const mb_batch_desc* b, const std::vector<RobotPack>& pac
             }
         for (uint32_t p = 0; p < P; ++p) std::sort(sp.exports[base + p].begin(), sp.exports[base + p].end());
     });
-    for (uint32_t i = 0; i < nb; ++i) sp.stride[i / C] = std::max(sp.stride[i / C], sp.n_all[i]);
 }
 
 // Whether every part fits the shape and the shared memory; the reason if not.
@@ -821,7 +820,7 @@ bool split_fits(const SplitParts& sp, const KernelShape& sh, uint32_t smem_cap, 
     const uint64_t cap_m = std::min<uint64_t>((uint64_t)sh.threads * sh.mpt, 4096);
     for (uint32_t i = 0; i < sp.locals.size(); ++i) {
         const BinLocal& L = sp.locals[i];
-        const uint32_t smem = split_smem_bytes(sp.stride[i / C], L.n_spring, L.n_inc, (uint32_t)sp.exports[i].size());
+        const uint32_t smem = split_smem_bytes(sp.n_all[i], L.n_spring, L.n_inc, (uint32_t)sp.exports[i].size());
         if (L.n_spring > cap_s || L.n_mass > cap_m || sp.n_all[i] > 4096 || smem > smem_cap) {
             char buf[256];
             std::snprintf(buf, sizeof(buf), "part in bin %u (cluster %u): %u springs, %u + %u masses, %u B shared memory",
@@ -844,7 +843,7 @@ void assemble_split(const SplitParts& sp, uint32_t R, unsigned threads, Packed& 
     out.max_smem = 0;
     for (uint32_t i = 0; i < nb; ++i) {
         BinDesc& d = out.bins[i];
-        d.x_stride = sp.stride[i / C];
+        d.x_stride = sp.n_all[i];
         d.export_begin = (uint32_t)out.exports.size();
         d.n_export = (uint32_t)sp.exports[i].size();
         d.n_all = sp.n_all[i];
