@@ -281,8 +281,9 @@ namespace mb_detail {
 // population that no longer fits the override (after development) is
 // re-planned automatically.
 mb_status pack(mb_context* ctx, const mb_batch_desc* b, bool fallback_auto, mb::Packed& out,
-               bool allow_split) {
+               bool allow_split, bool rows_on_device = false) {
     mb::PackOptions po;
+    po.rows_on_device = rows_on_device;
     po.sms = (uint32_t)std::max(ctx->num_sms, 1);
     po.smem_cap = mb::max_step_smem(ctx->device);
     po.mode = (uint32_t)ctx->mode;
@@ -307,8 +308,11 @@ mb_status pack(mb_context* ctx, const mb_batch_desc* b, bool fallback_auto, mb::
 }
 
 // Uploads the packed arrays of `out` and the per-launch buffers sized by
-// them; positions, velocities and stresses are not touched.
-mb_status upload_packed(mb_context* ctx, const mb::Packed& out) {
+// them; positions, velocities and stresses are not touched.  Rows the host
+// did not build are built on the device (the development re-pack kernel);
+// if they do not fit their regions or the shared memory, *rows_failed is
+// set and the caller packs again with host-built rows.
+mb_status upload_packed(mb_context* ctx, const mb::Packed& out, bool* rows_failed = nullptr) {
     ctx->clear_graphs();
     ctx->shape = out.shape;
     ctx->n_bins = out.n_bins;
@@ -351,6 +355,33 @@ mb_status upload_packed(mb_context* ctx, const mb::Packed& out) {
     ctx->devo_ready = false;
     MB_CUDA(ctx, ctx->bin_flags.alloc(nb));
     MB_CUDA(ctx, cudaMemsetAsync(ctx->bin_flags.p, 0, nb * sizeof(uint32_t), st));
+    if (out.rows_on_device) {
+        MB_CUDA(ctx, ctx->inc.alloc(std::max<uint64_t>(out.row_total, 1)));
+        MB_CUDA(ctx, ctx->rows_scratch.alloc(2 * std::max<size_t>(out.pair.size(), 1)));
+        MB_CUDA(ctx, ctx->free_count.alloc(nb));
+        MB_CUDA(ctx, ctx->free_taken.alloc(nb));
+        MB_CUDA(ctx, ctx->devo_status.alloc(2));
+        MB_CUDA(ctx, cudaMemsetAsync(ctx->free_count.p, 0, nb * sizeof(uint32_t), st));
+        MB_CUDA(ctx, cudaMemsetAsync(ctx->free_taken.p, 0, nb * sizeof(uint32_t), st));
+        MB_CUDA(ctx, cudaMemsetAsync(ctx->devo_status.p, 0, 2 * sizeof(uint32_t), st));
+        // no packed slot is inert here: spring_gidx < n_spring everywhere
+        const mb::RebuildParams rp{ctx->bins.p,        nb,                   ctx->spring_pair.p,
+                                   ctx->spring_gidx.p, (uint32_t)ctx->n_spring, ctx->slice_off.p,
+                                   ctx->slice_width.p, ctx->inc.p,           ctx->inc32.p,
+                                   0u,                 ctx->rows_scratch.p,  ctx->free_count.p,
+                                   ctx->free_taken.p,  ctx->devo_status.p};
+        MB_CUDA(ctx, mb::launch_rebuild(rp, st));
+        uint32_t status[2] = {0, 0};
+        MB_CUDA(ctx, cudaMemcpyAsync(status, ctx->devo_status.p, sizeof(status), cudaMemcpyDeviceToHost, st));
+        MB_CUDA(ctx, cudaMemcpyAsync(ctx->h_bins.data(), ctx->bins.p, nb * sizeof(mb::BinDesc),
+                                     cudaMemcpyDeviceToHost, st));
+        MB_CUDA(ctx, cudaStreamSynchronize(st));
+        if (status[0] || status[1] > mb::max_step_smem(ctx->device)) {
+            if (rows_failed) *rows_failed = true;
+            return MB_OK;
+        }
+        ctx->smem_bytes = status[1];  // the largest bin's need, exactly
+    }
     // the host vectors of `out` may die after this call: wait for the copies
     MB_CUDA(ctx, cudaStreamSynchronize(st));
     return MB_OK;
@@ -826,9 +857,12 @@ mb_status mb_set_elements(mb_context* ctx, const mb_batch_desc* b) {
             h_lbar.assign(b->lbar, b->lbar + S);
         }
     });
-    // kept in the context: its arrays keep their capacity across uploads
+    // kept in the context: its arrays keep their capacity across uploads.
+    // Resident rows are built on the device unless MB_HOST_ROWS=1.
     mb::Packed& out = ctx->upload_pack;
-    const mb_status pst = mb_detail::pack(ctx, b, false, out, true);
+    const char* host_rows = std::getenv("MB_HOST_ROWS");
+    const bool device_rows = !(host_rows && host_rows[0] == '1');
+    const mb_status pst = mb_detail::pack(ctx, b, false, out, true, device_rows);
     copier.join();
     if (pst != MB_OK) return pst;
 
@@ -864,7 +898,13 @@ mb_status mb_set_elements(mb_context* ctx, const mb_batch_desc* b) {
     MB_CUDA(ctx, cudaMemsetAsync(ctx->stress.p, 0, (S + 1) * sizeof(float), st));
     MB_CUDA(ctx, ctx->robot_flags.alloc(R));
     MB_CUDA(ctx, ctx->com.alloc(3 * (size_t)R));
-    const mb_status ust = mb_detail::upload_packed(ctx, out);
+    bool rows_failed = false;
+    mb_status ust = mb_detail::upload_packed(ctx, out, &rows_failed);
+    if (ust == MB_OK && rows_failed) {  // rare: the host builds the rows
+        MB_TRACE("device rows did not fit; host rows");
+        ust = mb_detail::pack(ctx, b, false, out, true, false);
+        if (ust == MB_OK) ust = mb_detail::upload_packed(ctx, out);
+    }
     if (ust != MB_OK) return ust;
     ctx->loaded = true;
     return MB_OK;

@@ -356,9 +356,12 @@ void slice_rows(uint32_t nm, const std::vector<uint32_t>& row_start, const std::
     L.padding = L.n_inc - (uint64_t)row_start[nm];
 }
 
+// rows_on_device: only the springs and masses; the rows get a region of
+// generous capacity (twice the rank-layout estimate plus the alignment
+// slack) for the device to build them in.
 void build_bin(const mb_batch_desc* b, const std::vector<RobotPack>& packs,
                const std::vector<uint32_t>& robots, const std::vector<int>& slot_of, bool streamed,
-               BinLocal& L) {
+               bool rows_on_device, BinLocal& L) {
     uint32_t nm = 0, ns = 0;
     for (uint32_t r : robots) {
         nm += packs[r].n_mass;
@@ -383,6 +386,19 @@ void build_bin(const mb_batch_desc* b, const std::vector<RobotPack>& packs,
             row_start[pc + 1]++;
         }
         mbase += packs[r].n_mass;
+    }
+    if (rows_on_device) {
+        uint64_t est = 0;
+        for (uint32_t r : robots) est += packs[r].inc_estimate;
+        const uint32_t n_sl = (nm + kSliceWidth - 1) / kSliceWidth;
+        const uint64_t cap = (2 * est + 4ull * kSliceWidth * n_sl + 31) / 32 * 32;
+        L.n_mass = nm;
+        L.n_spring = ns;
+        L.n_inc = (uint32_t)std::min<uint64_t>(cap, 0xFFFFFFFFu);
+        L.slice_off.assign(n_sl, 0);
+        L.slice_width.assign(n_sl, 0);
+        L.smem = bin_smem_bytes(nm, ns, (uint32_t)std::min<uint64_t>(est, 0xFFFFFFFFu));
+        return;
     }
     for (uint32_t i = 0; i < nm; ++i) row_start[i + 1] += row_start[i];
     std::vector<Ent> ents(row_start[nm]);
@@ -418,7 +434,8 @@ void build_bin(const mb_batch_desc* b, const std::vector<RobotPack>& packs,
 
 // Offsets of every bin, then every bin copied in parallel into sized
 // arrays; statistics.
-void assemble(const std::vector<BinLocal>& locals, Packed& out, bool streamed, unsigned threads) {
+void assemble(const std::vector<BinLocal>& locals, Packed& out, bool streamed, unsigned threads,
+              bool rows_on_device = false) {
     const uint32_t nb = (uint32_t)locals.size();
     out.bins.assign(nb, BinDesc{});
     out.max_smem = 0;
@@ -436,10 +453,11 @@ void assemble(const std::vector<BinLocal>& locals, Packed& out, bool streamed, u
         d.inc_begin = (uint32_t)ninc;
         d.n_inc = L.n_inc;
         d.slice_begin = (uint32_t)nsl;
+        d.row_cap = rows_on_device ? L.n_inc : 0u;
         nm += L.mass_gidx.size();
         ns += L.spring_gidx.size();
         nsl += L.slice_off.size();
-        ninc += streamed ? L.inc32.size() : L.inc.size();
+        ninc += rows_on_device ? L.n_inc : streamed ? L.inc32.size() : L.inc.size();
         out.max_smem = std::max(out.max_smem, L.smem);
         out.inc_entries += L.n_inc;
         out.inc_padding += L.padding;
@@ -452,8 +470,10 @@ void assemble(const std::vector<BinLocal>& locals, Packed& out, bool streamed, u
     out.lbar.resize(ns);
     out.slice_off.resize(nsl);
     out.slice_width.resize(nsl);
-    out.inc.resize(streamed ? 0 : ninc);  // every entry is copied below
+    out.inc.resize(streamed || rows_on_device ? 0 : ninc);  // every entry is copied below
     out.inc32.resize(streamed ? ninc : 0);
+    out.rows_on_device = rows_on_device;
+    out.row_total = ninc;
     parallel_for(nb, threads, [&](uint32_t i) {
         const BinLocal& L = locals[i];
         const BinDesc& d = out.bins[i];
@@ -475,11 +495,13 @@ void assemble(const std::vector<BinLocal>& locals, Packed& out, bool streamed, u
 
 void build_all(const mb_batch_desc* b, const std::vector<RobotPack>& packs,
                const std::vector<std::vector<uint32_t>>& plan, const std::vector<int>& slot_of,
-               bool streamed, unsigned threads, Packed& out) {
+               bool streamed, unsigned threads, Packed& out, bool rows_on_device = false) {
     const uint32_t nb = (uint32_t)plan.size(), R = (uint32_t)packs.size();
     std::vector<BinLocal> locals(nb);
-    parallel_for(nb, threads, [&](uint32_t i) { build_bin(b, packs, plan[i], slot_of, streamed, locals[i]); });
-    assemble(locals, out, streamed, threads);
+    parallel_for(nb, threads, [&](uint32_t i) {
+        build_bin(b, packs, plan[i], slot_of, streamed, rows_on_device, locals[i]);
+    });
+    assemble(locals, out, streamed, threads, rows_on_device);
     out.robot_bin.assign(R, 0);
     out.robot_mass_base.assign(R, 0);
     for (uint32_t i = 0; i < nb; ++i) {
@@ -941,7 +963,7 @@ mb_status pack_population(const mb_batch_desc* b, const PackOptions& o, Packed& 
             }
             if (!planned) planned = plan_bins(packs, nb, sh, o.smem_cap, plan);
             if (planned) {
-                build_all(b, packs, plan, slot_of, false, threads, out);
+                build_all(b, packs, plan, slot_of, false, threads, out, o.rows_on_device);
                 if (out.max_smem <= o.smem_cap) {
                     ok = true;
                     break;

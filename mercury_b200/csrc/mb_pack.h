@@ -45,6 +45,9 @@ struct PackOptions {
     // empty = 1
     std::function<int(const KernelShape&, uint32_t)> ctas_per_sm;
     unsigned threads = 0;          // host threads (0 = hardware concurrency)
+    // resident bins only: lay out springs and masses, leave the rows to the
+    // device (bins[b].row_cap entries reserved per bin)
+    bool rows_on_device = false;
 };
 
 struct Packed {
@@ -52,6 +55,8 @@ struct Packed {
     uint32_t n_bins = 0;
     uint32_t grid = 0;  // CTAs per launch, CTA g running bins g, g + grid, ...; 0 = one per bin
     uint32_t cluster = 0;  // split bins: CTAs per cluster (parts per robot); 0 = not split
+    bool rows_on_device = false;  // rows not built: row_total entries reserved (bins[b].row_cap each)
+    uint64_t row_total = 0;
     bool streamed = false;
     uint32_t max_smem = 0;
     std::vector<BinDesc> bins;

@@ -249,3 +249,17 @@ def test_streamed_force_modes_bit_exact(mode):
     keys = ("g", "floor_stiffness", "friction_static", "friction_kinetic", "drag", "damping")
     core.force_run(mode, b, p, v, s, mb.materials.force_table(), [env[k] for k in keys], 1e-4, 0.0, 300, True)
     assert bits_equal(pos, p) and bits_equal(vel, v) and bits_equal(stress, s)
+
+
+@pytest.mark.parametrize("track", [False, True])
+def test_rows_built_on_device_or_host_same_bits(monkeypatch, track):
+    """Uploads build the incidence rows on the device (the development
+    re-pack kernel); MB_HOST_ROWS=1 has the host packer build them."""
+    b = robots.population_batch("uneven", 40, seed_base=77)
+    _, p1, v1, s1 = run_gpu(b, 1e-3, 150, track)
+    monkeypatch.setenv("MB_HOST_ROWS", "1")
+    _, p2, v2, s2 = run_gpu(b, 1e-3, 150, track)
+    p, v, s = run_oracle(b, 1e-3, 150, track)
+    assert bits_equal(p1, p) and bits_equal(v1, v) and bits_equal(p2, p) and bits_equal(v2, v)
+    if track:
+        assert bits_equal(s1, s) and bits_equal(s2, s)
