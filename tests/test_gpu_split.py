@@ -141,3 +141,33 @@ def test_cluster_config_validation():
     sim.set_batch(robots.population_batch("streamed", 1))
     cfg = sim.launch_config()
     assert cfg["cluster"] == 0 and cfg["streamed"] == 1
+
+
+def _degenerate_elements():
+    """Robots of one and two masses with no active spring (their parts of a
+    cluster stay empty) beside ordinary robots."""
+    one = mb.Element(np.zeros((1, 3), np.float32), np.array([1]), np.array([[0, 0]]), np.ones(1),
+                     np.zeros(1, np.uint8), vel=np.array([[0.1, 0.0, 0.0]], np.float32))
+    two = mb.Element(np.array([[0, 0, 0], [0.1, 0, 0]], np.float32), np.array([1, 2]), np.array([[0, 1]]),
+                     np.array([0.1], np.float32), np.zeros(1, np.uint8))
+    els = robots.population("uneven", 5)
+    return [one, els[0], two, els[1], els[2], one, els[3], els[4]]
+
+
+@pytest.mark.parametrize("cfg", [{"cluster": 8}, {"cluster": 2}], ids=["cluster8", "cluster2"])
+def test_degenerate_robots_split(cfg):
+    check(mb.pack(_degenerate_elements()), 1e-3, 200, True, cfg, cluster=cfg["cluster"])
+
+
+def test_degenerate_robots_beside_large_ones():
+    """Automatic plan: the large robots take two parts, the others one each,
+    sharing clusters (with empty slots)."""
+    b = mb.pack(robots.population("streamed", 2) + _degenerate_elements())
+    check(b, 1e-4, 150, True, cluster=2)
+
+
+def test_largest_robot_splits_over_eight():
+    """4,096 masses (15x15x15 cells, 46,620 springs): eight parts."""
+    rng = np.random.default_rng(3)
+    e = robots.voxel_robot(robots.FOUR[rng.integers(0, 4, size=(15, 15, 15))], mass=1.0)
+    check(mb.pack([e]), 1e-4, 60, True, cluster=8)
