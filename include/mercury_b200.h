@@ -249,8 +249,9 @@ MB_API mb_status mb_set_voxel_population(mb_context* ctx, uint32_t n_robots, int
  * distance as mean length and the composite material of the two masses.
  * pos: 3 floats per mass (host); at most 4,096 masses per robot, k <= 32.
  * spring_offsets (n_robots + 1) is always written; with pairs == NULL the
- * call only counts.  Synchronous; allocates its own device scratch.  No
- * context needed. */
+ * call only counts.  Synchronous.  Its device scratch and stream are kept
+ * per device for later calls (grown when a call needs more, held until the
+ * process exits); calls on one device are serialised.  No context needed. */
 MB_API mb_status mb_knn_springs(int device, uint32_t n_robots, const int64_t* mass_offsets, const float* pos,
                                 const uint8_t* mass_material, uint32_t k, int64_t* spring_offsets,
                                 uint16_t* pairs, uint8_t* spring_material, float* lbar, uint64_t capacity);

@@ -20,6 +20,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <vector>
 
@@ -149,14 +150,45 @@ __global__ void emit_kernel(const EmitArgs a) {
     }
 }
 
+// Grow-only device buffer, kept between calls.
 template <typename T>
 struct Dev {
     T* p = nullptr;
-    ~Dev() {
+    size_t n = 0;
+    cudaError_t alloc(size_t count) {
+        if (count <= n && p) return cudaSuccess;
         if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+        const size_t c = std::max<size_t>(count, 1);
+        const cudaError_t e = cudaMalloc(&p, c * sizeof(T));
+        if (e == cudaSuccess) n = c;
+        return e;
     }
-    cudaError_t alloc(size_t n) { return cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)); }
 };
+
+// Scratch and stream of one device, kept for the process: calls reuse them
+// (one call at a time per device, under the lock), so a call allocates only
+// when it needs more than any earlier one.
+struct KnnScratch {
+    std::mutex lock;
+    cudaStream_t stream = nullptr;
+    Dev<float> pos, lbar;
+    Dev<uint8_t> mm, mat;
+    Dev<int64_t> off;
+    Dev<uint16_t> nn, pairs;
+    Dev<uint32_t> bits, rc;
+    Dev<uint64_t> boff, first;
+};
+
+KnnScratch& knn_scratch(int device) {
+    static std::mutex registry_lock;
+    static std::vector<std::unique_ptr<KnnScratch>> per_device;
+    std::lock_guard<std::mutex> g(registry_lock);
+    if ((size_t)device >= per_device.size()) per_device.resize(device + 1);
+    if (!per_device[device]) per_device[device] = std::make_unique<KnnScratch>();
+    return *per_device[device];
+}
 
 }  // namespace
 }  // namespace mb
@@ -177,19 +209,25 @@ extern "C" mb_status mb_knn_springs(int device, uint32_t n_robots, const int64_t
         bit_off[r + 1] = bit_off[r] + m * ((m + 31) / 32);
     }
     const uint64_t M = (uint64_t)mass_offsets[n_robots];
-    if (cudaSetDevice(device) != cudaSuccess) return MB_ERR_CUDA;
-    cudaStream_t st;
-    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return MB_ERR_CUDA;
-    struct StreamGuard {
-        cudaStream_t s;
-        ~StreamGuard() { cudaStreamDestroy(s); }
-    } guard{st};
-    Dev<float> d_pos, d_lbar;
-    Dev<uint8_t> d_mm, d_mat;
-    Dev<int64_t> d_off;
-    Dev<uint16_t> d_nn, d_pairs;
-    Dev<uint32_t> d_bits, d_rc;
-    Dev<uint64_t> d_boff, d_first;
+    if (device < 0 || cudaSetDevice(device) != cudaSuccess) return MB_ERR_CUDA;
+    KnnScratch& sc = knn_scratch(device);
+    std::lock_guard<std::mutex> held(sc.lock);
+    if (!sc.stream && cudaStreamCreateWithFlags(&sc.stream, cudaStreamNonBlocking) != cudaSuccess) {
+        sc.stream = nullptr;
+        return MB_ERR_CUDA;
+    }
+    cudaStream_t st = sc.stream;
+    auto& d_pos = sc.pos;
+    auto& d_lbar = sc.lbar;
+    auto& d_mm = sc.mm;
+    auto& d_mat = sc.mat;
+    auto& d_off = sc.off;
+    auto& d_nn = sc.nn;
+    auto& d_pairs = sc.pairs;
+    auto& d_bits = sc.bits;
+    auto& d_rc = sc.rc;
+    auto& d_boff = sc.boff;
+    auto& d_first = sc.first;
 #define KNN_CUDA(x)                               \
     do {                                          \
         if ((x) != cudaSuccess) return MB_ERR_CUDA; \

@@ -129,15 +129,16 @@ def knn_springs(points: list, materials: list, k: int = 25, device: int = 0):
     pos = np.ascontiguousarray(np.concatenate(points), np.float32)
     mm = np.ascontiguousarray(np.concatenate(materials), np.uint8)
     so = np.zeros(R + 1, np.int64)
+    # one call: a mass has at most k springs of its own, so M * k bounds the
+    # count (the arrays are not touched beyond what the call writes)
+    cap = int(mo[-1]) * k
+    pairs = np.empty((cap, 2), np.uint16)
+    smat = np.empty(cap, np.uint8)
+    lbar = np.empty(cap, np.float32)
     _lib.check(_lib.LIB.mb_knn_springs(device, R, _lib.ptr(mo), _lib.ptr(pos), _lib.ptr(mm), k, _lib.ptr(so),
-                                       None, None, None, 0))
+                                       _lib.ptr(pairs), _lib.ptr(smat), _lib.ptr(lbar), cap))
     S = int(so[-1])
-    pairs = np.empty((S, 2), np.uint16)
-    smat = np.empty(S, np.uint8)
-    lbar = np.empty(S, np.float32)
-    _lib.check(_lib.LIB.mb_knn_springs(device, R, _lib.ptr(mo), _lib.ptr(pos), _lib.ptr(mm), k, _lib.ptr(so),
-                                       _lib.ptr(pairs), _lib.ptr(smat), _lib.ptr(lbar), S))
-    return so, pairs, smat, lbar
+    return so, pairs[:S], smat[:S], lbar[:S]
 
 
 def nn_population_device(n_robots: int = 256, seed_base: int = 2000, mass: float = 0.1, k: int = 25,
