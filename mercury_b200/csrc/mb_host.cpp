@@ -292,6 +292,9 @@ mb_status pack(mb_context* ctx, const mb_batch_desc* b, bool fallback_auto, mb::
     po.ctas_per_sm = [ctx](const mb::KernelShape& sh, uint32_t smem) {
         return mb::ctas_per_sm(sh, (uint32_t)ctx->mode, false, smem);
     };
+    po.cluster_fits = [ctx](const mb::KernelShape& sh, uint32_t cluster, uint32_t smem) {
+        return mb::max_active_clusters(sh, (uint32_t)ctx->mode, cluster, smem) > 0;
+    };
     std::string err;
     mb_status pst = mb::pack_population(b, po, out, err);
     const mb_launch_config none{};

@@ -101,6 +101,9 @@ cudaError_t launch_step(const StepParams& p, const KernelShape& shape, cudaStrea
 // Resident CTAs per SM of a kernel variant with `smem_bytes` of dynamic
 // shared memory (0 if the shape is not compiled or does not fit).
 int ctas_per_sm(const KernelShape& shape, uint32_t mode, bool track, uint32_t smem_bytes);
+// Clusters of `cluster` split-kernel CTAs that can be resident at once on
+// the current device (0: such a cluster cannot be scheduled).
+int max_active_clusters(const KernelShape& shape, uint32_t mode, uint32_t cluster, uint32_t smem_bytes);
 
 // Streamed variant for bins whose springs do not fit in shared memory:
 // only predicted positions live in shared memory; springs, rows and the

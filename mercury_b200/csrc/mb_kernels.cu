@@ -685,6 +685,31 @@ int ctas_per_sm(const KernelShape& shape, uint32_t mode, bool track, uint32_t sm
     return n;
 }
 
+int max_active_clusters(const KernelShape& shape, uint32_t mode, uint32_t cluster, uint32_t smem_bytes) {
+    const ShapeEntry* e = find_split(shape);
+    if (!e || mode > kModeForceWater || cluster < 1 || cluster > kMaxClusterParts) return 0;
+    StepFn fn = e->fn[mode][0];
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes) != cudaSuccess)
+        return 0;
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(cluster, 1, 1);
+    cfg.blockDim = dim3(shape.threads, 1, 1);
+    cfg.dynamicSmemBytes = smem_bytes;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, fn, &cfg) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+
 uint32_t list_shapes(KernelShape* out, uint32_t cap, bool streamed) {
     uint32_t n = 0;
     if (streamed) {

@@ -997,6 +997,17 @@ mb_status pack_population(const mb_batch_desc* b, const PackOptions& o, Packed& 
         std::vector<KernelShape> compiled;
         for (const auto& sh : sshapes)
             if (split_supported(sh)) compiled.push_back(sh);
+        // the device must be able to hold one such cluster at a time
+        auto schedulable = [&](const SplitParts& sp, const KernelShape& sh) {
+            if (!o.cluster_fits) return true;
+            uint32_t smem = 0;
+            for (uint32_t i = 0; i < sp.locals.size(); ++i)
+                smem = std::max(smem, split_smem_bytes(sp.n_all[i], sp.locals[i].n_spring, sp.locals[i].n_inc,
+                                                       (uint32_t)sp.exports[i].size()));
+            if (o.cluster_fits(sh, sp.C, smem)) return true;
+            why = "clusters of " + std::to_string(sp.C) + " CTAs cannot be scheduled on this device";
+            return false;
+        };
         auto accept = [&](SplitParts& sp, const KernelShape& sh, uint32_t n_clusters) {
             assemble_split(sp, R, threads, out);
             ok = true;
@@ -1016,7 +1027,7 @@ mb_status pack_population(const mb_batch_desc* b, const PackOptions& o, Packed& 
                 if (sp.C < 2) continue;  // every robot fits a CTA alone: not a split population
                 const uint32_t ncl = place_parts(sp.parts, sp.C, sp.first);
                 build_split_parts(b, packs, ncl, part_of, slot_of, threads, sp);
-                if (!split_fits(sp, sh, o.smem_cap, why)) continue;
+                if (!split_fits(sp, sh, o.smem_cap, why) || !schedulable(sp, sh)) continue;
                 accept(sp, sh, ncl);
                 break;
             }
@@ -1032,7 +1043,7 @@ mb_status pack_population(const mb_batch_desc* b, const PackOptions& o, Packed& 
             for (uint32_t r = 0; r < R; ++r) sp.first[r] = r * C;
             build_split_parts(b, packs, R, part_of, slot_of, threads, sp);
             for (const auto& sh : compiled) {
-                if (!split_fits(sp, sh, o.smem_cap, why)) continue;
+                if (!split_fits(sp, sh, o.smem_cap, why) || !schedulable(sp, sh)) continue;
                 accept(sp, sh, R);
                 break;
             }

@@ -44,6 +44,9 @@ struct PackOptions {
     // resident CTAs per SM of a shape with a given dynamic shared memory;
     // empty = 1
     std::function<int(const KernelShape&, uint32_t)> ctas_per_sm;
+    // whether clusters of that many CTAs of a split shape with that shared
+    // memory can be scheduled at all; empty = yes
+    std::function<bool(const KernelShape&, uint32_t, uint32_t)> cluster_fits;
     unsigned threads = 0;          // host threads (0 = hardware concurrency)
     // resident bins only: lay out springs and masses, leave the rows to the
     // device (bins[b].row_cap entries reserved per bin)
