@@ -328,7 +328,7 @@ def run_ours(args, rank, local_rank, world):
             "parallelism": f"population sharded over {world} GPU(s), no collective in the step",
         },
         "roofline": {"bound": "hbm", "achieved": hbm_ach, "peak": hbm_peak, "unit": "GB/s",
-                     "frac": hbm_ach / hbm_peak, "traffic": None,
+                     "frac": hbm_ach / hbm_peak, **_step_traffic(args.workload, cfg, active, hbm_b),
                      "bytes_per_update": hbm_b, "peak_source": hbm_src,
                      "note": "HBM bytes a streaming step must move per spring-update; this kernel keeps "
                              "robots on chip for a whole launch, see roofline_smem"},
@@ -360,6 +360,25 @@ def _device_rate(sim, active, steps, track, dev):
     e1.record(st)
     e1.synchronize()
     return active * steps / (e0.elapsed_time(e1) / 1e3)
+
+
+# DRAM bytes (read + write) of one 1,000-step launch of the step kernel on
+# the uneven population in its tuned configuration, from the ncu capture in
+# profiles/step_kernel_1024x8x2_grouped296_uneven512.md
+STEP_TRAFFIC = {("uneven", 1024, 8, 2, 296, 1000): 24.65e6 + 12.0e3}
+
+
+def _step_traffic(workload, cfg, active, bytes_per_update):
+    """Measured DRAM bytes per launch beside the algorithmic (streaming)
+    bytes of the same launch, when the bench runs the profiled configuration."""
+    key = (workload, cfg["threads"], cfg["springs_per_thread"], cfg["masses_per_thread"], cfg["bins"], cfg["chunk"])
+    t = STEP_TRAFFIC.get(key)
+    if t is None:
+        return {"traffic": None}
+    return {"traffic": t, "traffic_unit": "bytes per launch",
+            "traffic_source": "ncu capture of the same configuration "
+                              "(profiles/step_kernel_1024x8x2_grouped296_uneven512.md)",
+            "algorithmic_bytes_per_launch": bytes_per_update * active * cfg["chunk"]}
 
 
 def secondary(args, batch, local_rank, dev, hbm_peak):
