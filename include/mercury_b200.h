@@ -284,8 +284,10 @@ typedef struct mb_plan_stats {
     /* CTAs of a step launch (CTA g runs bins g, g + ctas, ...) and the
      * largest / smallest number of springs one CTA runs per step */
     uint32_t ctas, max_cta_springs, min_cta_springs;
-    /* robots split over clusters of this many CTAs (0 = not split) */
-    uint32_t cluster;
+    /* robots split over clusters of this many CTAs (0 = not split); with
+     * cluster2 = 2, the robots of at most two parts run in two-CTA clusters
+     * from bin split_bins0 on, launched beside the first group */
+    uint32_t cluster, cluster2, split_bins0;
 } mb_plan_stats;
 MB_API mb_status mb_plan_population(const mb_batch_desc* batch, const mb_launch_config* cfg,
                                     uint32_t num_sms, uint32_t smem_bytes, mb_plan_stats* stats);

@@ -62,7 +62,8 @@ class PlanStats(ctypes.Structure):
                                                "incidence_padding")] + \
                [(n, ctypes.c_uint32) for n in ("aligned_slices", "rank_slices", "material_slots",
                                                "max_bin_springs", "min_bin_springs",
-                                               "ctas", "max_cta_springs", "min_cta_springs", "cluster")]
+                                               "ctas", "max_cta_springs", "min_cta_springs", "cluster",
+                                               "cluster2", "split_bins0")]
 
 
 class LaunchConfig(ctypes.Structure):

@@ -146,6 +146,12 @@ struct mb_context {
     mb::DevBuf<uint32_t> exports;          // split bins: halo positions each part writes into the others
     mb::Packed upload_pack;                // host packing of the last mb_set_elements (reused)
     uint32_t cluster = 0;                  // split bins: CTAs per robot (0 = not split)
+    // split bins in two groups: bins from split_bins0 in clusters of
+    // cluster2, launched on stream2 beside the first group (fork and join
+    // through the two events)
+    uint32_t cluster2 = 0, split_bins0 = 0;
+    cudaStream_t stream2 = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     mb::DevBuf<float4> dp_scratch;
     mb::DevBuf<float> st_scratch;
     mb::DevBuf<float> spring_lbar;
@@ -206,6 +212,9 @@ struct mb_context {
     }
     ~mb_context() {
         clear_graphs();
+        if (stream2) cudaStreamDestroy(stream2);
+        if (ev_fork) cudaEventDestroy(ev_fork);
+        if (ev_join) cudaEventDestroy(ev_join);
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -323,6 +332,13 @@ mb_status upload_packed(mb_context* ctx, const mb::Packed& out, bool* rows_faile
     ctx->smem_bytes = out.max_smem;
     ctx->streamed = out.streamed;
     ctx->cluster = out.cluster;
+    ctx->cluster2 = out.cluster2;
+    ctx->split_bins0 = out.split_bins0;
+    if (ctx->cluster2 && !ctx->stream2) {  // created once, outside any capture
+        MB_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->stream2, cudaStreamNonBlocking));
+        MB_CUDA(ctx, cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
+        MB_CUDA(ctx, cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming));
+    }
     ctx->stream_mpt = out.shape.mpt;
     const uint32_t nb = out.n_bins;
     cudaStream_t st = ctx->stream;
@@ -767,6 +783,8 @@ mb_status mb_plan_population(const mb_batch_desc* batch, const mb_launch_config*
     stats->bins = out.n_bins;
     stats->streamed = out.streamed ? 1u : 0u;
     stats->cluster = out.cluster;
+    stats->cluster2 = out.cluster2;
+    stats->split_bins0 = out.split_bins0;
     stats->max_smem_bytes = out.max_smem;
     stats->masses = out.masses;
     stats->active_springs = out.active_springs;
@@ -975,6 +993,24 @@ float advance(float t, float dt, uint32_t n) {
 }
 
 // Issues the chunk launches for `steps` steps from clock t0 on the stream.
+// Split bins: one launch, or the two groups side by side (the second on
+// stream2, forked after the actuation table and joined before the next).
+cudaError_t launch_split_groups(mb_context* c, const mb::StepParams& p) {
+    if (!c->cluster2) return mb::launch_split(p, c->shape, c->cluster, c->stream);
+    cudaError_t e = cudaEventRecord(c->ev_fork, c->stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(c->stream2, c->ev_fork, 0);
+    mb::StepParams p0 = p, p1 = p;
+    p0.n_bins = c->split_bins0;
+    p1.bins = p.bins + c->split_bins0;
+    p1.bin_flags = p.bin_flags + c->split_bins0;
+    p1.n_bins = p.n_bins - c->split_bins0;
+    if (e == cudaSuccess) e = mb::launch_split(p0, c->shape, c->cluster, c->stream);
+    if (e == cudaSuccess) e = mb::launch_split(p1, c->shape, c->cluster2, c->stream2);
+    if (e == cudaSuccess) e = cudaEventRecord(c->ev_join, c->stream2);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(c->stream, c->ev_join, 0);
+    return e;
+}
+
 cudaError_t issue_chunks(mb_context* c, float t0, uint32_t steps, bool track) {
     float t = t0;
     uint32_t done = 0;
@@ -987,7 +1023,7 @@ cudaError_t issue_chunks(mb_context* c, float t0, uint32_t steps, bool track) {
         MB_TRACE("launch bins=%u threads=%u spt=%u mpt=%u smem=%u steps=%u", p.n_bins, c->shape.threads,
                  c->shape.spt, c->shape.mpt, p.smem_bytes, n);
         cudaError_t e = c->streamed  ? mb::launch_stream(p, 1024, c->stream_mpt, c->stream)
-                        : c->cluster ? mb::launch_split(p, c->shape, c->cluster, c->stream)
+                        : c->cluster ? launch_split_groups(c, p)
                                      : mb::launch_step(p, c->shape, c->stream);
         MB_TRACE("launch returned %d", (int)e);
         if (trace_on() && std::getenv("MB_SYNC")) {

@@ -513,7 +513,7 @@ void build_all(const mb_batch_desc* b, const std::vector<RobotPack>& packs,
         }
     }
     out.exports.clear();
-    out.cluster = 0;
+    out.cluster = out.cluster2 = out.split_bins0 = 0;
 }
 
 // ---- split bins: one robot simulated by a cluster of C CTAs ----
@@ -658,7 +658,10 @@ void build_part(const mb_batch_desc* b, uint32_t r, const RobotPack& pk, const s
 // predicted-position buffers hold its own and halo masses (n_all).
 struct SplitParts {
     uint32_t C = 0;
-    std::vector<uint32_t> parts, first;          // per robot
+    // second group (robots of at most two parts in two-CTA clusters, after
+    // bin bins0), launched beside the first: 0 = one group
+    uint32_t C2 = 0, bins0 = 0;
+    std::vector<uint32_t> parts, first, slot0;   // per robot (slot0: rank of its first part)
     std::vector<BinLocal> locals;                // per bin
     std::vector<std::vector<uint32_t>> exports;  // per bin
     std::vector<uint32_t> n_all;                 // per bin
@@ -783,39 +786,58 @@ bool split_partition_mixed(const mb_batch_desc* b, const std::vector<RobotPack>&
     return fits;
 }
 
-// Places robots in clusters of C slots, robots with more parts first (parts
-// are powers of two, so the slots fill without gaps but in the last
-// cluster); returns the number of clusters.
-uint32_t place_parts(const std::vector<uint32_t>& parts, uint32_t C, std::vector<uint32_t>& first) {
-    const uint32_t R = (uint32_t)parts.size();
-    std::vector<uint32_t> order(R);
-    for (uint32_t i = 0; i < R; ++i) order[i] = i;
+// Places `robots` in clusters of C slots from bin `base`, robots with more
+// parts first (parts are powers of two, so the slots fill without gaps but
+// in the last cluster); returns the number of bins used.
+uint32_t place_parts(const std::vector<uint32_t>& robots, const std::vector<uint32_t>& parts, uint32_t C,
+                     uint32_t base, std::vector<uint32_t>& first, std::vector<uint32_t>& slot0) {
+    std::vector<uint32_t> order(robots);
     std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) { return parts[x] > parts[y]; });
-    first.assign(R, 0);
     uint32_t cluster = 0, slot = 0;
     for (uint32_t r : order) {
         if (slot + parts[r] > C) {
             ++cluster;
             slot = 0;
         }
-        first[r] = cluster * C + slot;
+        first[r] = base + cluster * C + slot;
+        slot0[r] = slot;
         slot += parts[r];
     }
-    return R ? cluster + 1 : 0;
+    return order.empty() ? 0 : (cluster + 1) * C;
+}
+
+// Placement of every robot: one group in clusters of C, or -- when some
+// robots need more than two parts and others at most two -- the large ones
+// in clusters of C and the others after them in clusters of two, which the
+// device packs more densely (launched side by side).  Returns the bins.
+uint32_t place_split(SplitParts& sp) {
+    const uint32_t R = (uint32_t)sp.parts.size();
+    sp.first.assign(R, 0);
+    sp.slot0.assign(R, 0);
+    std::vector<uint32_t> big, small;
+    for (uint32_t r = 0; r < R; ++r) (sp.C > 2 && sp.parts[r] > 2 ? big : small).push_back(r);
+    if (big.empty() || small.empty()) {
+        sp.C2 = sp.bins0 = 0;
+        std::vector<uint32_t> all(R);
+        for (uint32_t r = 0; r < R; ++r) all[r] = r;
+        return place_parts(all, sp.parts, sp.C, 0, sp.first, sp.slot0);
+    }
+    sp.bins0 = place_parts(big, sp.parts, sp.C, 0, sp.first, sp.slot0);
+    sp.C2 = 2;
+    return sp.bins0 + place_parts(small, sp.parts, 2, sp.bins0, sp.first, sp.slot0);
 }
 
 // Builds every part (rows, halos, export lists) from a partition and a
-// placement (sp.C, sp.parts, sp.first set).
-void build_split_parts(const mb_batch_desc* b, const std::vector<RobotPack>& packs, uint32_t n_clusters,
+// placement (sp.parts, sp.first, sp.slot0 set) over `nb` bins.
+void build_split_parts(const mb_batch_desc* b, const std::vector<RobotPack>& packs, uint32_t nb,
                        const std::vector<std::vector<uint8_t>>& part_of, const std::vector<int>& slot_of,
                        unsigned threads, SplitParts& sp) {
     const uint32_t R = (uint32_t)packs.size();
-    const uint32_t C = sp.C, nb = n_clusters * C;
     sp.locals.assign(nb, BinLocal{});
     sp.exports.assign(nb, {});
     sp.n_all.assign(nb, 0);
     parallel_for(R, threads, [&](uint32_t r) {
-        const uint32_t P = sp.parts[r], base = sp.first[r], slot0 = base % C;
+        const uint32_t P = sp.parts[r], base = sp.first[r], slot0 = sp.slot0[r];
         std::vector<PartMasses> pm(P);
         std::vector<int32_t> local_of;
         for (uint32_t p = 0; p < P; ++p) {
@@ -837,7 +859,6 @@ void build_split_parts(const mb_batch_desc* b, const std::vector<RobotPack>& pac
 
 // Whether every part fits the shape and the shared memory; the reason if not.
 bool split_fits(const SplitParts& sp, const KernelShape& sh, uint32_t smem_cap, std::string& why) {
-    const uint32_t C = sp.C;
     const uint64_t cap_s = std::min<uint64_t>((uint64_t)sh.threads * sh.spt, kMaxBinSprings);
     const uint64_t cap_m = std::min<uint64_t>((uint64_t)sh.threads * sh.mpt, 4096);
     for (uint32_t i = 0; i < sp.locals.size(); ++i) {
@@ -845,8 +866,8 @@ bool split_fits(const SplitParts& sp, const KernelShape& sh, uint32_t smem_cap, 
         const uint32_t smem = split_smem_bytes(sp.n_all[i], L.n_spring, L.n_inc, (uint32_t)sp.exports[i].size());
         if (L.n_spring > cap_s || L.n_mass > cap_m || sp.n_all[i] > 4096 || smem > smem_cap) {
             char buf[256];
-            std::snprintf(buf, sizeof(buf), "part in bin %u (cluster %u): %u springs, %u + %u masses, %u B shared memory",
-                          i, i / C, L.n_spring, L.n_mass, sp.n_all[i] - L.n_mass, smem);
+            std::snprintf(buf, sizeof(buf), "part in bin %u: %u springs, %u + %u masses, %u B shared memory", i,
+                          L.n_spring, L.n_mass, sp.n_all[i] - L.n_mass, smem);
             why = buf;
             return false;
         }
@@ -856,7 +877,7 @@ bool split_fits(const SplitParts& sp, const KernelShape& sh, uint32_t smem_cap, 
 
 // The packed arrays of split parts.
 void assemble_split(const SplitParts& sp, uint32_t R, unsigned threads, Packed& out) {
-    const uint32_t C = sp.C, nb = (uint32_t)sp.locals.size();
+    const uint32_t nb = (uint32_t)sp.locals.size();
     assemble(sp.locals, out, false, threads);
     out.robot_bin.assign(R, 0);
     out.robot_mass_base.assign(R, 0);
@@ -1008,13 +1029,15 @@ mb_status pack_population(const mb_batch_desc* b, const PackOptions& o, Packed& 
             why = "clusters of " + std::to_string(sp.C) + " CTAs cannot be scheduled on this device";
             return false;
         };
-        auto accept = [&](SplitParts& sp, const KernelShape& sh, uint32_t n_clusters) {
+        auto accept = [&](SplitParts& sp, const KernelShape& sh, uint32_t nb) {
             assemble_split(sp, R, threads, out);
             ok = true;
             out.shape = sh;
-            out.n_bins = n_clusters * sp.C;
+            out.n_bins = nb;
             out.grid = 0;
             out.cluster = sp.C;
+            out.cluster2 = sp.C2;
+            out.split_bins0 = sp.bins0;
             out.streamed = false;
         };
         // automatic: every robot at its fewest parts, robots sharing clusters
@@ -1025,10 +1048,10 @@ mb_status pack_population(const mb_batch_desc* b, const PackOptions& o, Packed& 
                 if (!split_partition_mixed(b, packs, sh, o.smem_cap, threads, part_of, sp.parts)) continue;
                 sp.C = *std::max_element(sp.parts.begin(), sp.parts.end());
                 if (sp.C < 2) continue;  // every robot fits a CTA alone: not a split population
-                const uint32_t ncl = place_parts(sp.parts, sp.C, sp.first);
-                build_split_parts(b, packs, ncl, part_of, slot_of, threads, sp);
+                const uint32_t nb = place_split(sp);
+                build_split_parts(b, packs, nb, part_of, slot_of, threads, sp);
                 if (!split_fits(sp, sh, o.smem_cap, why) || !schedulable(sp, sh)) continue;
-                accept(sp, sh, ncl);
+                accept(sp, sh, nb);
                 break;
             }
         // forced (or when the mixed placement fails): every robot in C parts
@@ -1040,11 +1063,12 @@ mb_status pack_population(const mb_batch_desc* b, const PackOptions& o, Packed& 
             sp.C = C;
             sp.parts.assign(R, C);
             sp.first.resize(R);
+            sp.slot0.assign(R, 0);
             for (uint32_t r = 0; r < R; ++r) sp.first[r] = r * C;
-            build_split_parts(b, packs, R, part_of, slot_of, threads, sp);
+            build_split_parts(b, packs, R * C, part_of, slot_of, threads, sp);
             for (const auto& sh : compiled) {
                 if (!split_fits(sp, sh, o.smem_cap, why) || !schedulable(sp, sh)) continue;
-                accept(sp, sh, R);
+                accept(sp, sh, R * C);
                 break;
             }
         }
@@ -1067,7 +1091,7 @@ mb_status pack_population(const mb_batch_desc* b, const PackOptions& o, Packed& 
                 out.shape = KernelShape{1024, 0, mpt};
                 out.n_bins = R;
                 out.grid = 0;
-                out.cluster = 0;
+                out.cluster = out.cluster2 = out.split_bins0 = 0;
                 out.exports.clear();
             }
         }

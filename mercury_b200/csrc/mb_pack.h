@@ -58,6 +58,9 @@ struct Packed {
     uint32_t n_bins = 0;
     uint32_t grid = 0;  // CTAs per launch, CTA g running bins g, g + grid, ...; 0 = one per bin
     uint32_t cluster = 0;  // split bins: CTAs per cluster (parts per robot); 0 = not split
+    // split bins in two groups: bins [0, split_bins0) in clusters of `cluster`,
+    // the rest in clusters of `cluster2`, launched side by side; 0 = one group
+    uint32_t cluster2 = 0, split_bins0 = 0;
     bool rows_on_device = false;  // rows not built: row_total entries reserved (bins[b].row_cap each)
     uint64_t row_total = 0;
     bool streamed = false;

@@ -171,3 +171,14 @@ def test_largest_robot_splits_over_eight():
     rng = np.random.default_rng(3)
     e = robots.voxel_robot(robots.FOUR[rng.integers(0, 4, size=(15, 15, 15))], mass=1.0)
     check(mb.pack([e]), 1e-4, 60, True, cluster=8)
+
+
+@pytest.mark.parametrize("graph", [1, 0], ids=["graph", "no_graph"])
+def test_two_cluster_groups_side_by_side(graph):
+    """Point clouds of one, two and four parts: four-part robots launch in
+    clusters of four, the others beside them in clusters of two (a second
+    stream, forked and joined around every launch of 37 steps)."""
+    b = mb.pack(robots.nn_population_device(6, seed_base=2100, mass=0.1))
+    pl = mb.plan(b)
+    assert pl["cluster"] == 4 and pl["cluster2"] == 2 and 0 < pl["split_bins0"] < pl["bins"]
+    check(b, 1e-4, 150, True, {"chunk": 37, "use_graph": graph}, mode=S.MODE_FORCE_WATER, cluster=4)

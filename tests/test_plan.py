@@ -79,6 +79,10 @@ def test_split_robots_take_their_fewest_parts_and_share_clusters():
     b = robots.population_batch("nn", 24)
     auto, uniform = mb.plan(b), mb.plan(b, cluster=4)
     assert auto["cluster"] == uniform["cluster"] == 4
-    assert auto["bins"] % 4 == 0 and auto["bins"] < uniform["bins"] == 96
+    assert auto["bins"] < uniform["bins"] == 96 and uniform["cluster2"] == 0
+    # robots of more than two parts in clusters of four from bin 0; the rest
+    # in two-CTA clusters from split_bins0 on
+    assert auto["cluster2"] == 2 and auto["split_bins0"] % 4 == 0
+    assert 0 < auto["split_bins0"] < auto["bins"] and (auto["bins"] - auto["split_bins0"]) % 2 == 0
     assert auto["active_springs"] == uniform["active_springs"] == b.active_springs()
     assert auto["max_smem_bytes"] <= 232448
