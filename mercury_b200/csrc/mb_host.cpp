@@ -992,25 +992,28 @@ float advance(float t, float dt, uint32_t n) {
     return v;
 }
 
-// Issues the chunk launches for `steps` steps from clock t0 on the stream.
 // Split bins: one launch, or the two groups side by side (the second on
-// stream2, forked after the actuation table and joined before the next).
+// stream2, forked from the main stream and joined back before the next
+// launch).  Once forked, stream2 is joined back even when a launch failed,
+// so that a stream capture never ends with an unjoined fork.
 cudaError_t launch_split_groups(mb_context* c, const mb::StepParams& p) {
     if (!c->cluster2) return mb::launch_split(p, c->shape, c->cluster, c->stream);
     cudaError_t e = cudaEventRecord(c->ev_fork, c->stream);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(c->stream2, c->ev_fork, 0);
+    if (e != cudaSuccess) return e;
     mb::StepParams p0 = p, p1 = p;
     p0.n_bins = c->split_bins0;
     p1.bins = p.bins + c->split_bins0;
     p1.bin_flags = p.bin_flags + c->split_bins0;
     p1.n_bins = p.n_bins - c->split_bins0;
-    if (e == cudaSuccess) e = mb::launch_split(p0, c->shape, c->cluster, c->stream);
-    if (e == cudaSuccess) e = mb::launch_split(p1, c->shape, c->cluster2, c->stream2);
-    if (e == cudaSuccess) e = cudaEventRecord(c->ev_join, c->stream2);
-    if (e == cudaSuccess) e = cudaStreamWaitEvent(c->stream, c->ev_join, 0);
-    return e;
+    e = mb::launch_split(p0, c->shape, c->cluster, c->stream);
+    const cudaError_t e1 = mb::launch_split(p1, c->shape, c->cluster2, c->stream2);
+    cudaError_t j = cudaEventRecord(c->ev_join, c->stream2);
+    if (j == cudaSuccess) j = cudaStreamWaitEvent(c->stream, c->ev_join, 0);
+    return e != cudaSuccess ? e : e1 != cudaSuccess ? e1 : j;
 }
 
+// Issues the chunk launches for `steps` steps from clock t0 on the stream.
 cudaError_t issue_chunks(mb_context* c, float t0, uint32_t steps, bool track) {
     float t = t0;
     uint32_t done = 0;
