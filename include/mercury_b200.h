@@ -65,6 +65,15 @@ typedef enum mb_mode {
  *   friction_static, friction_kinetic   Coulomb coefficients (land)
  *   drag             0.5 * rho * Cd * A of the quadratic drag per mass (water)
  *   damping          velocity factor per step
+ *   face_drag        fluid density rho of the drag on the robots' surface
+ *                    triangles (water; 0 = faces exert no drag).  Each face
+ *                    (i0, i1, i2) with mean vertex velocity v, N = (x1 - x0)
+ *                    x (x2 - x0), A = |N| and unit normal n = N/(A + 1e-12)
+ *                    turned so that v.n > 0, pushes
+ *                    -rho/2 A ((v.n) v + 0.2 |v|^2 n) / 3 on each vertex: the
+ *                    face law of the reference's surfaceDragForce
+ *                    (sim_kernel.cu:96-121), whose result never reaches the
+ *                    reference's integrator, added here to the spring forces.
  * Force modes integrate x' = x + v dt + (F/m) dt^2, v' = damping (x' - x)/dt
  * with m the w component of the position. */
 typedef struct mb_environment {
@@ -74,10 +83,15 @@ typedef struct mb_environment {
     float friction_kinetic;
     float drag;
     float damping;
+    float face_drag;
 } mb_environment;
 
 /* One population on the host.  Offsets have n_robots + 1 entries and index
- * the flat arrays; pairs are local to their robot. */
+ * the flat arrays; pairs and faces are local to their robot.  Faces are the
+ * robots' surface triangles (Face m0, m1, m2, face.h:6-10; Element::faces,
+ * element.h:12), used only by the face drag of the water mode; both face
+ * pointers NULL = no faces.  A face with two equal corners is skipped, as
+ * the reference skips it (sim_kernel.cu:99). */
 typedef struct mb_batch_desc {
     uint32_t n_robots;
     const int64_t* mass_offsets;
@@ -88,6 +102,8 @@ typedef struct mb_batch_desc {
     const uint16_t* pairs;          /* 2 per spring */
     const uint8_t* spring_material; /* composite material id per spring */
     const float* lbar;              /* mean length per spring */
+    const int64_t* face_offsets;    /* n_robots + 1, or NULL */
+    const uint16_t* faces;          /* 3 per face, or NULL */
 } mb_batch_desc;
 
 /* Launch configuration of the step kernel.  threads: CTA size; bins: number

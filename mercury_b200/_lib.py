@@ -47,12 +47,14 @@ class BatchDesc(ctypes.Structure):
         ("pairs", ctypes.c_void_p),
         ("spring_material", ctypes.c_void_p),
         ("lbar", ctypes.c_void_p),
+        ("face_offsets", ctypes.c_void_p),
+        ("faces", ctypes.c_void_p),
     ]
 
 
 class Environment(ctypes.Structure):
     _fields_ = [(n, ctypes.c_float) for n in ("g", "floor_stiffness", "friction_static",
-                                              "friction_kinetic", "drag", "damping")]
+                                              "friction_kinetic", "drag", "damping", "face_drag")]
 
 
 class PlanStats(ctypes.Structure):

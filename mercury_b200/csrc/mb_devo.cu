@@ -444,7 +444,7 @@ __global__ void __launch_bounds__(kRebuildThreads) rebuild_kernel(const RebuildP
     if (tid == 0) {
         p.bins[b].n_inc = n_inc;
         if (!p.streamed)
-            atomicMax(&p.status[1], bin_smem_bytes_dev(nm, ns, n_inc));
+            atomicMax(&p.status[1], bin_smem_bytes_dev(nm, ns, n_inc) + face_smem_bytes(nm, bd.n_face, bd.n_face_inc));
     }
 }
 

@@ -111,7 +111,7 @@ struct mb_context {
     float dt = 0.0001f;  // Simulator.h:55
     float total_time = 0.0f;
     mb_mode mode = MB_MODE_REF_XPBD;
-    mb_environment env{9.81f, 1.0e6f, 1.0f, 0.8f, 0.05f, 0.999f};
+    mb_environment env{9.81f, 1.0e6f, 1.0f, 0.8f, 0.05f, 0.999f, 0.0f};
     float table[4 * MB_COMPOSITE_COUNT] = {};
     bool have_table = false;
 
@@ -144,6 +144,12 @@ struct mb_context {
     uint32_t stream_mpt = 2;
     mb::DevBuf<uint32_t> inc32;
     mb::DevBuf<uint32_t> exports;          // split bins: halo positions each part writes into the others
+    // face drag (resident bins): corners, rows per packed mass, incidence
+    mb::DevBuf<uint2> faces;
+    mb::DevBuf<uint32_t> face_row;
+    mb::DevBuf<uint16_t> face_inc;
+    uint64_t n_faces = 0;          // faces of the population (three distinct corners)
+    bool faces_resident = false;   // the packed bins hold them (not split, not streamed)
     mb::Packed upload_pack;                // host packing of the last mb_set_elements (reused)
     uint32_t cluster = 0;                  // split bins: CTAs per robot (0 = not split)
     // split bins in two groups: bins from split_bins0 in clusters of
@@ -167,6 +173,8 @@ struct mb_context {
     std::vector<uint16_t> h_pairs;
     std::vector<uint8_t> h_spring_mat, h_mass_mat;
     std::vector<float> h_lbar;
+    std::vector<int64_t> h_face_off;  // empty: no faces
+    std::vector<uint16_t> h_faces;
     mb::DevBuf<int64_t> d_spring_off;
     mb::DevBuf<mb::DevoRecord> devo_out;
     std::vector<mb::DevoRecord> h_devo;
@@ -356,6 +364,11 @@ mb_status upload_packed(mb_context* ctx, const mb::Packed& out, bool* rows_faile
     MB_CUDA(ctx, up(ctx->slice_width, out.slice_width.data(), out.slice_width.size()));
     MB_CUDA(ctx, up(ctx->inc, out.inc.data(), out.inc.size()));
     MB_CUDA(ctx, up(ctx->exports, out.exports.data(), out.exports.size()));
+    MB_CUDA(ctx, up(ctx->faces, reinterpret_cast<const uint2*>(out.faces.data()), out.faces.size() / 2));
+    MB_CUDA(ctx, up(ctx->face_row, out.face_row.data(), out.face_row.size()));
+    MB_CUDA(ctx, up(ctx->face_inc, out.face_inc.data(), out.face_inc.size()));
+    ctx->n_faces = out.n_faces;
+    ctx->faces_resident = !out.face_row.empty();
     if (out.streamed) {
         MB_CUDA(ctx, up(ctx->inc32, out.inc32.data(), out.inc32.size()));
         MB_CUDA(ctx, ctx->dp_scratch.alloc(std::max<size_t>(out.pair.size(), 1)));
@@ -499,9 +512,18 @@ mb_status host_repack(mb_context* c) {
                                    c->stream));
         MB_CUDA(c, cudaStreamSynchronize(c->stream));
     }
-    const mb_batch_desc d{c->n_robots,       c->mass_off.data(),   pos.empty() ? nullptr : pos.data(),
-                          nullptr,           c->h_mass_mat.data(), c->spring_off.data(),
-                          c->h_pairs.data(), c->h_spring_mat.data(), c->h_lbar.data()};
+    const bool faces = !c->h_face_off.empty();
+    const mb_batch_desc d{c->n_robots,
+                          c->mass_off.data(),
+                          pos.empty() ? nullptr : pos.data(),
+                          nullptr,
+                          c->h_mass_mat.data(),
+                          c->spring_off.data(),
+                          c->h_pairs.data(),
+                          c->h_spring_mat.data(),
+                          c->h_lbar.data(),
+                          faces ? c->h_face_off.data() : nullptr,
+                          faces ? c->h_faces.data() : nullptr};
     mb::Packed out;
     mb_status st = pack(c, &d, true, out, true);
     if (st == MB_OK) st = upload_packed(c, out);
@@ -589,6 +611,8 @@ mb_status voxel_setup(mb_context* c, uint32_t R, int sx, int sy, int sz, float h
     c->h_lbar.swap(lbar);
     c->h_mass_mat.assign(M, 0);
     c->h_spring_mat.assign(S, 0);
+    c->h_face_off.clear();  // voxel robots carry no faces
+    c->h_faces.clear();
     st = upload_packed(c, out);
     if (st != MB_OK) return st;
     cudaStream_t cs = c->stream;
@@ -732,8 +756,8 @@ mb_status mb_get_mode(const mb_context* ctx, mb_mode* mode) {
 
 mb_status mb_set_environment(mb_context* ctx, const mb_environment* env) {
     if (!ctx || !env) return fail(ctx, MB_ERR_ARGUMENT, "null argument");
-    const float v[6] = {env->g, env->floor_stiffness, env->friction_static, env->friction_kinetic,
-                        env->drag, env->damping};
+    const float v[7] = {env->g,    env->floor_stiffness, env->friction_static, env->friction_kinetic,
+                        env->drag, env->damping,         env->face_drag};
     for (float f : v)
         if (!std::isfinite(f) || f < 0.0f) return fail(ctx, MB_ERR_ARGUMENT, "environment values must be finite and >= 0");
     ctx->env = *env;
@@ -864,13 +888,25 @@ mb_status mb_set_elements(mb_context* ctx, const mb_batch_desc* b) {
     if (S && (!b->pairs || !b->spring_material || !b->lbar))
         return fail(ctx, MB_ERR_ARGUMENT, "null spring array");
     if (M >= (1ull << 31) || S >= (1ull << 31)) return fail(ctx, MB_ERR_CAPACITY, "population too large");
+    const bool faces = b->face_offsets && b->faces;
+    if ((b->face_offsets != nullptr) != (b->faces != nullptr))
+        return fail(ctx, MB_ERR_ARGUMENT, "face_offsets and faces must both be given or both be NULL");
+    if (faces && b->face_offsets[0] != 0) return fail(ctx, MB_ERR_ARGUMENT, "offsets must start at 0");
+    const uint64_t F = faces ? (uint64_t)b->face_offsets[R] : 0;
+    if (F >= (1ull << 31)) return fail(ctx, MB_ERR_CAPACITY, "population too large");
 
     cudaSetDevice(ctx->device);
     // the host copy of the topology is taken while the population is packed
     std::vector<uint8_t> h_mass_mat, h_spring_mat;
     std::vector<uint16_t> h_pairs;
     std::vector<float> h_lbar;
+    std::vector<int64_t> h_face_off;
+    std::vector<uint16_t> h_faces;
     std::thread copier([&] {
+        if (F) {
+            h_face_off.assign(b->face_offsets, b->face_offsets + R + 1);
+            h_faces.assign(b->faces, b->faces + 3 * F);
+        }
         h_mass_mat.assign(b->mass_material, b->mass_material + M);
         if (S) {
             h_pairs.assign(b->pairs, b->pairs + 2 * S);
@@ -903,6 +939,8 @@ mb_status mb_set_elements(mb_context* ctx, const mb_batch_desc* b) {
     ctx->h_pairs = std::move(h_pairs);
     ctx->h_spring_mat = std::move(h_spring_mat);
     ctx->h_lbar = std::move(h_lbar);
+    ctx->h_face_off = std::move(h_face_off);
+    ctx->h_faces = std::move(h_faces);
     cudaStream_t st = ctx->stream;
     auto up = [&](auto& buf, const auto* src, size_t n) -> cudaError_t {
         cudaError_t e = buf.alloc(n);
@@ -982,6 +1020,11 @@ mb::StepParams make_params(mb_context* c, float t0, uint32_t steps, bool track) 
     p.mu_k = c->env.friction_kinetic;
     p.drag = c->env.drag;
     p.damping = c->env.damping;
+    p.faces = c->faces.p;
+    p.face_row = c->face_row.p;
+    p.face_inc = c->face_inc.p;
+    p.face_coef = (float)(-(double)c->env.face_drag / 6.0);
+    p.face_on = c->mode == MB_MODE_FORCE_WATER && c->env.face_drag != 0.0f && c->faces_resident ? 1u : 0u;
     return p;
 }
 
@@ -1045,6 +1088,9 @@ cudaError_t issue_chunks(mb_context* c, float t0, uint32_t steps, bool track) {
 mb_status run(mb_context* c, uint32_t steps, bool track) {
     if (!c->loaded) return fail(c, MB_ERR_STATE, "no population uploaded");
     if (steps == 0) return MB_OK;
+    if (c->mode == MB_MODE_FORCE_WATER && c->env.face_drag != 0.0f && c->n_faces && !c->faces_resident)
+        return fail(c, MB_ERR_CAPACITY,
+                    "face drag needs every robot with faces in one CTA (this population is split or streamed)");
     cudaSetDevice(c->device);
     const float t0 = c->total_time;
     if (c->use_graph) {

@@ -32,6 +32,13 @@ struct BinDesc {
     uint32_t export_begin; // first export entry (own mass | rank << 12 | slot << 15)
     uint32_t n_export;
     uint32_t n_all;        // own + halo masses
+    // surface triangles of the bin's robots (face drag of the water mode;
+    // resident bins only): bin-local corners, and per mass the faces it is
+    // a corner of, in face order
+    uint32_t face_begin;   // first packed face
+    uint32_t n_face;
+    uint32_t face_inc_begin;  // first face incidence entry
+    uint32_t n_face_inc;
 };
 
 // Everything one step launch needs.  Pointers are device addresses.
@@ -71,9 +78,18 @@ struct StepParams {
     float mu_s, mu_k;             // static / kinetic friction coefficients (land)
     float drag;                   // 0.5 rho Cd A of the quadratic drag per mass (water)
     float damping;                // velocity factor per step
+    // face drag (water, resident bins)
+    const uint2* faces;           // packed face: {c0 | c1 << 16, c2}, bin-local corners
+    const uint32_t* face_row;     // packed mass: first entry (bin-relative) | count << 24
+    const uint16_t* face_inc;     // face incidence entries: bin-local face index
+    float face_coef;              // -rho/6: -rho/2 of the face law and the 1/3 per corner
+    uint32_t face_on;             // face drag active (water mode, rho != 0)
 };
 
 enum StepMode : uint32_t { kModeXpbd = 0, kModeForceLand = 1, kModeForceWater = 2 };
+// Kernel variant of the water mode with the face drag compiled in (chosen
+// by launch_step when StepParams::face_on is set; never a StepParams mode).
+constexpr uint32_t kModeForceWaterFaces = 3;
 
 struct KernelShape {
     uint32_t threads;
@@ -129,6 +145,14 @@ uint32_t bin_smem_bytes(uint32_t n_mass, uint32_t n_spring, uint32_t n_inc);
 __host__ __device__ inline uint32_t bin_smem_bytes_dev(uint32_t n_mass, uint32_t n_spring, uint32_t n_inc) {
     return 16u * n_mass + 16u * n_spring + 8u * kMaxMaterialSlots + 2u * n_inc;
 }
+
+// Face drag of a resident bin, after its rows (16-byte aligned): the
+// velocities of its masses, the forces and corners of its faces, and their
+// incidence entries.
+__host__ __device__ inline uint32_t face_smem_bytes(uint32_t n_mass, uint32_t n_face, uint32_t n_face_inc) {
+    return n_face ? 16u + 16u * n_mass + 24u * n_face + 2u * n_face_inc : 0u;
+}
+constexpr uint32_t kMaxFacesPerMass = 255;  // 8-bit count in face_row
 
 // Split bins: two predicted-position buffers of x_stride slots, the
 // corrections, the material factors, the buffer strides of the cluster's

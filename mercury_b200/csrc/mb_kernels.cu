@@ -117,9 +117,43 @@ __device__ __forceinline__ float velocity_of(float delta, double dt, double inv_
     return __double2float_rn(__ddiv_rn(a, dt));
 }
 
+// Face drag of one surface triangle (water), the share of each corner:
+// mean corner velocity v, N = (x1 - x0) x (x2 - x0), A = |N|, unit normal
+// n = N * RN(1/(A + eps)) turned so that v.n > 0 (sim_kernel.cu:106-109),
+// force coef * A * ((v.n) v + 0.2 |v|^2 n) with coef = -rho/6, i.e.
+// -rho/2 A (...) / 3 (sim_kernel.cu:110-111).  Every operation rounds once,
+// in this order.
+__device__ __forceinline__ float4 face_force(const float4 x0, const float4 x1, const float4 x2, const float4 v0,
+                                             const float4 v1, const float4 v2, const float coef) {
+    const float vx = __fdiv_rn(__fadd_rn(__fadd_rn(v0.x, v1.x), v2.x), 3.0f);
+    const float vy = __fdiv_rn(__fadd_rn(__fadd_rn(v0.y, v1.y), v2.y), 3.0f);
+    const float vz = __fdiv_rn(__fadd_rn(__fadd_rn(v0.z, v1.z), v2.z), 3.0f);
+    const float ax = __fsub_rn(x1.x, x0.x), ay = __fsub_rn(x1.y, x0.y), az = __fsub_rn(x1.z, x0.z);
+    const float bx = __fsub_rn(x2.x, x0.x), by = __fsub_rn(x2.y, x0.y), bz = __fsub_rn(x2.z, x0.z);
+    const float nx = __fsub_rn(__fmul_rn(ay, bz), __fmul_rn(az, by));
+    const float ny = __fsub_rn(__fmul_rn(az, bx), __fmul_rn(ax, bz));
+    const float nz = __fsub_rn(__fmul_rn(ax, by), __fmul_rn(ay, bx));
+    const float area = __fsqrt_rn(__fmaf_rn(nx, nx, __fmaf_rn(ny, ny, __fmul_rn(nz, nz))));
+    const float r = __frcp_rn(__fadd_rn(area, kEps));
+    float ux = __fmul_rn(nx, r), uy = __fmul_rn(ny, r), uz = __fmul_rn(nz, r);
+    float vn = __fmaf_rn(ux, vx, __fmaf_rn(uy, vy, __fmul_rn(uz, vz)));
+    if (!(vn > 0.0f)) {  // negating n negates the rounded dot product exactly
+        ux = -ux;
+        uy = -uy;
+        uz = -uz;
+        vn = -vn;
+    }
+    const float lift = __fmul_rn(0.2f, __fmaf_rn(vx, vx, __fmaf_rn(vy, vy, __fmul_rn(vz, vz))));
+    const float c = __fmul_rn(coef, area);
+    return make_float4(__fmul_rn(c, __fmaf_rn(lift, ux, __fmul_rn(vn, vx))),
+                       __fmul_rn(c, __fmaf_rn(lift, uy, __fmul_rn(vn, vy))),
+                       __fmul_rn(c, __fmaf_rn(lift, uz, __fmul_rn(vn, vz))), 0.0f);
+}
+
 template <int T, int SPT, int MPT, int MODE, bool TRACK, bool SPLIT>
 __global__ void __launch_bounds__(T, 1024 / T) step_kernel(const StepParams p) {
     constexpr bool XPBD = MODE == kModeXpbd;
+    constexpr bool FACES = MODE == kModeForceWaterFaces && !SPLIT;  // face drag compiled in
     extern __shared__ float4 smem4[];
     const int tid = threadIdx.x;
     const float dt = p.dt;
@@ -139,9 +173,20 @@ __global__ void __launch_bounds__(T, 1024 / T) step_kernel(const StepParams p) {
         uint32_t* sstride = reinterpret_cast<uint32_t*>(smat + kMaxMaterialSlots);
         uint32_t* sexp = sstride + (SPLIT ? kMaxClusterParts : 0u);
         uint16_t* sinc = reinterpret_cast<uint16_t*>(sexp + (SPLIT ? bd.n_export : 0u));
+        // face drag (water, resident bins with faces), after the rows at a
+        // 16-byte boundary: velocities, face forces, corners, incidence
+        const uint32_t n_face = FACES && p.face_on ? bd.n_face : 0u;
+        float4* sv = reinterpret_cast<float4*>((reinterpret_cast<uintptr_t>(sinc + bd.n_inc) + 15u) & ~uintptr_t(15));
+        float4* sfd = sv + bd.n_mass;
+        uint2* sface = reinterpret_cast<uint2*>(sfd + n_face);
+        uint16_t* sfinc = reinterpret_cast<uint16_t*>(sface + n_face);
 
         const uint32_t n_mat = *p.n_mat;
         for (uint32_t i = tid; i < bd.n_inc; i += T) sinc[i] = __ldg(&p.inc[bd.inc_begin + i]);
+        if (n_face) {
+            for (uint32_t i = tid; i < n_face; i += T) sface[i] = __ldg(&p.faces[bd.face_begin + i]);
+            for (uint32_t i = tid; i < bd.n_face_inc; i += T) sfinc[i] = __ldg(&p.face_inc[bd.face_inc_begin + i]);
+        }
         if (SPLIT) {
             for (uint32_t i = tid; i < bd.n_export; i += T) sexp[i] = __ldg(&p.exports[bd.export_begin + i]);
             const cg::cluster_group cl = cg::this_cluster();
@@ -169,17 +214,20 @@ __global__ void __launch_bounds__(T, 1024 / T) step_kernel(const StepParams p) {
                 if (TRACK) st[j] = p.stress[__ldg(&p.spring_gidx[g]) & 0x7FFFFFFFu];
             }
         }
-        // Masses of this thread: x, v, mass and the SELL row (offset | width << 20).
+        // Masses of this thread: x, v, mass, the SELL row (offset | width << 20)
+        // and the face row (first entry | count << 24).
         float3 x[MPT], v[MPT];
         float mass[MPT];
-        uint32_t row[MPT];
+        uint32_t row[MPT], frow[MPT];
 #pragma unroll
         for (int j = 0; j < MPT; ++j) {
             const uint32_t m = tid + j * T;
             x[j] = make_float3(0.f, 0.f, 0.f);
             v[j] = make_float3(0.f, 0.f, 0.f);
             row[j] = 0;
+            frow[j] = 0;
             mass[j] = 1.0f;
+            if (n_face && m < bd.n_mass) frow[j] = __ldg(&p.face_row[bd.mass_begin + m]);
             if (m < bd.n_mass) {
                 const uint32_t g = __ldg(&p.mass_gidx[bd.mass_begin + m]);
                 const float4 P = p.pos[g], V = p.vel[g];
@@ -215,6 +263,7 @@ __global__ void __launch_bounds__(T, 1024 / T) step_kernel(const StepParams p) {
                                        __fadd_rn(x[j].z, __fmul_rn(v[j].z, dt)), 0.0f);
                 else
                     X[m] = make_float4(x[j].x, x[j].y, x[j].z, 0.0f);
+                if (n_face) sv[m] = make_float4(v[j].x, v[j].y, v[j].z, 0.0f);
             }
             __syncthreads();
             if (SPLIT) {
@@ -251,6 +300,12 @@ __global__ void __launch_bounds__(T, 1024 / T) step_kernel(const StepParams p) {
                 // stress: lambda/Lbar (reference, sim_kernel.cu:234); k (d - L)/Lbar (force)
                 if (TRACK) st[j] = __fadd_rn(st[j], __fmul_rn(XPBD ? lam : -lam, __frcp_rn(lb[j])));
             }
+            // face drag: the share of each corner, per face
+            for (uint32_t f = tid; f < n_face; f += T) {
+                const uint2 c = sface[f];
+                const uint32_t i0 = c.x & 0xFFFFu, i1 = c.x >> 16, i2 = c.y;
+                sfd[f] = face_force(X[i0], X[i1], X[i2], sv[i0], sv[i1], sv[i2], p.face_coef);
+            }
             __syncthreads();
             // (3) gather in summation order and integrate (sim_kernel.cu:246-268).
             // acc + (+-c) is computed as fma(c, +-1, acc): c*(+-1) is exact, so
@@ -283,6 +338,14 @@ __global__ void __launch_bounds__(T, 1024 / T) step_kernel(const StepParams p) {
                     v[j].z = velocity_of(__fsub_rn(nz, x[j].z), ddt, inv_dt);
                     x[j] = make_float3(nx, ny, nz);
                 } else {
+                    // face drag after the springs, faces in ascending order
+                    const uint16_t* fp = sfinc + (frow[j] & 0xFFFFFFu);
+                    for (uint32_t k = 0; k < (frow[j] >> 24); ++k) {
+                        const float4 c = sfd[fp[k]];
+                        ax = __fadd_rn(ax, c.x);
+                        ay = __fadd_rn(ay, c.y);
+                        az = __fadd_rn(az, c.z);
+                    }
                     force_integrate<MODE>(p, x[j], v[j], mass[j], inv_dt_f, ax, ay, az);
                 }
             }
@@ -557,7 +620,7 @@ using StepFn = void (*)(const StepParams);
 
 struct ShapeEntry {
     uint32_t threads, spt, mpt;
-    StepFn fn[3][2];  // [mode][track]
+    StepFn fn[4][2];  // [mode][track]; mode 3: water with face drag
 };
 
 #define MB_SHAPE(T, S, M, SPLIT)                                                               \
@@ -569,6 +632,8 @@ struct ShapeEntry {
                  step_kernel<T, S, M, kModeForceLand, true, SPLIT>},                           \
                 {step_kernel<T, S, M, kModeForceWater, false, SPLIT>,                          \
                  step_kernel<T, S, M, kModeForceWater, true, SPLIT>},                          \
+                {step_kernel<T, S, M, SPLIT ? kModeForceWater : kModeForceWaterFaces, false, SPLIT>, \
+                 step_kernel<T, S, M, SPLIT ? kModeForceWater : kModeForceWaterFaces, true, SPLIT>},  \
         }                                                                                      \
     }
 const ShapeEntry kShapes[] = {
@@ -669,8 +734,12 @@ cudaError_t launch_split(const StepParams& p, const KernelShape& shape, uint32_t
 cudaError_t prepare_step(const KernelShape& shape, uint32_t mode, bool track, uint32_t smem_bytes) {
     const ShapeEntry* e = find_shape(shape);
     if (!e || mode > kModeForceWater) return cudaErrorInvalidValue;
-    return cudaFuncSetAttribute(e->fn[mode][track ? 1 : 0], cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)smem_bytes);
+    cudaError_t r = cudaFuncSetAttribute(e->fn[mode][track ? 1 : 0], cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem_bytes);
+    if (r == cudaSuccess && mode == kModeForceWater)  // and the face-drag variant
+        r = cudaFuncSetAttribute(e->fn[kModeForceWaterFaces][track ? 1 : 0],
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
+    return r;
 }
 
 int ctas_per_sm(const KernelShape& shape, uint32_t mode, bool track, uint32_t smem_bytes) {
@@ -752,7 +821,8 @@ cudaError_t launch_step(const StepParams& p, const KernelShape& shape, cudaStrea
     if (p.n_bins == 0) return cudaSuccess;
     if (p.mode > kModeForceWater) return cudaErrorInvalidValue;
     const uint32_t grid = p.grid ? std::min(p.grid, p.n_bins) : p.n_bins;
-    e->fn[p.mode][p.track ? 1 : 0]<<<grid, shape.threads, p.smem_bytes, s>>>(p);
+    const uint32_t variant = p.mode == kModeForceWater && p.face_on ? kModeForceWaterFaces : p.mode;
+    e->fn[variant][p.track ? 1 : 0]<<<grid, shape.threads, p.smem_bytes, s>>>(p);
     return cudaGetLastError();
 }
 

@@ -36,6 +36,8 @@ struct RobotPack {
     uint32_t n_mass = 0;
     uint64_t cost = 0;
     uint64_t inc_estimate = 0;
+    uint32_t n_face = 0;     // faces with three distinct corners
+    uint32_t face_smem = 0;  // shared memory of the face drag, bytes (upper bound)
     std::string error;
     mb_status status = MB_OK;
 };
@@ -137,8 +139,45 @@ void preprocess(const mb_batch_desc* b, uint32_t r, RobotPack& p) {
         pass(sp, tmp, 4096, key_a);
         pass(tmp, sp, 8192, key_dx);
     }
+    // faces: corners in range, at most kMaxFacesPerMass faces per mass;
+    // faces with two equal corners are skipped (sim_kernel.cu:99)
+    if (b->faces && b->face_offsets && b->face_offsets[b->n_robots] > 0) {
+        const int64_t f0 = b->face_offsets[r], f1 = b->face_offsets[r + 1];
+        if (f1 < f0) {
+            std::snprintf(buf, sizeof(buf), "face offsets decrease at robot %u", r);
+            p.error = buf;
+            p.status = MB_ERR_ARGUMENT;
+            return;
+        }
+        std::vector<uint32_t> fdeg((size_t)cm, 0);
+        uint32_t nf = 0;
+        for (int64_t f = f0; f < f1; ++f) {
+            const uint16_t* c = b->faces + 3 * f;
+            if (c[0] >= cm || c[1] >= cm || c[2] >= cm) {
+                std::snprintf(buf, sizeof(buf), "face %lld of robot %u has a corner out of %lld masses",
+                              (long long)(f - f0), r, (long long)cm);
+                p.error = buf;
+                p.status = MB_ERR_ARGUMENT;
+                return;
+            }
+            if (c[0] == c[1] || c[0] == c[2] || c[1] == c[2]) continue;
+            ++nf;
+            for (int k = 0; k < 3; ++k)
+                if (++fdeg[c[k]] > kMaxFacesPerMass) {
+                    std::snprintf(buf, sizeof(buf), "mass %u of robot %u is a corner of more than %u faces",
+                                  c[k], r, kMaxFacesPerMass);
+                    p.error = buf;
+                    p.status = MB_ERR_CAPACITY;
+                    return;
+                }
+        }
+        p.n_face = nf;
+        // velocities of every mass of a bin that has faces, alignment, the
+        // faces (force, corners) and their three incidence entries
+        p.face_smem = 16u + 16u * (uint32_t)cm + 30u * nf;
+    }
     p.n_mass = (uint32_t)cm;
-    p.cost = (uint64_t)sp.size() * 4 + (uint64_t)cm;
+    p.cost = (uint64_t)sp.size() * 4 + (uint64_t)cm + 2ull * p.n_face;
     uint64_t est = 0;  // incidence entries with rows padded to the slice maximum
     for (int64_t i = 0; i < cm; i += 32) {
         uint32_t w = 0;
@@ -157,7 +196,7 @@ bool plan_bins(const std::vector<RobotPack>& packs, uint32_t nb, const KernelSha
     for (uint32_t i = 0; i < n; ++i) order[i] = i;
     std::stable_sort(order.begin(), order.end(),
                      [&](uint32_t a, uint32_t b) { return packs[a].cost > packs[b].cost; });
-    std::vector<uint64_t> load(nb, 0), bm(nb, 0), bs(nb, 0), bi(nb, 0);
+    std::vector<uint64_t> load(nb, 0), bm(nb, 0), bs(nb, 0), bi(nb, 0), bx(nb, 0);
     plan.assign(nb, {});
     const uint64_t cap_s = std::min<uint64_t>((uint64_t)sh.threads * sh.spt, kMaxBinSprings);
     const uint64_t cap_m = std::min<uint64_t>((uint64_t)sh.threads * sh.mpt, 4096);
@@ -167,7 +206,7 @@ bool plan_bins(const std::vector<RobotPack>& packs, uint32_t nb, const KernelSha
         for (uint32_t b = 0; b < nb; ++b) {
             if (bm[b] + p.n_mass > cap_m || bs[b] + p.springs.size() > cap_s) continue;
             if (bin_smem_bytes((uint32_t)(bm[b] + p.n_mass), (uint32_t)(bs[b] + p.springs.size()),
-                               (uint32_t)(bi[b] + p.inc_estimate)) > smem_cap)
+                               (uint32_t)(bi[b] + p.inc_estimate)) + bx[b] + p.face_smem > smem_cap)
                 continue;
             if (best < 0 || load[b] < load[best]) best = (int)b;
         }
@@ -176,6 +215,7 @@ bool plan_bins(const std::vector<RobotPack>& packs, uint32_t nb, const KernelSha
         bm[best] += p.n_mass;
         bs[best] += p.springs.size();
         bi[best] += p.inc_estimate;
+        bx[best] += p.face_smem;
         plan[best].push_back(r);
     }
     for (auto& v : plan) std::sort(v.begin(), v.end());
@@ -218,14 +258,14 @@ bool plan_bins_grouped(const std::vector<RobotPack>& packs, uint32_t nb, uint32_
     }
     plan.assign(nb, {});
     for (uint32_t g = 0; g < groups; ++g) {
-        std::vector<uint64_t> load(per, 0), bm(per, 0), bs(per, 0), bi(per, 0);
+        std::vector<uint64_t> load(per, 0), bm(per, 0), bs(per, 0), bi(per, 0), bx(per, 0);
         for (uint32_t r : members[g]) {
             const auto& p = packs[r];
             int best = -1;
             for (uint32_t j = 0; j < per; ++j) {
                 if (bm[j] + p.n_mass > cap_m || bs[j] + p.springs.size() > cap_s) continue;
                 if (bin_smem_bytes((uint32_t)(bm[j] + p.n_mass), (uint32_t)(bs[j] + p.springs.size()),
-                                   (uint32_t)(bi[j] + p.inc_estimate)) > smem_cap)
+                                   (uint32_t)(bi[j] + p.inc_estimate)) + bx[j] + p.face_smem > smem_cap)
                     continue;
                 if (best < 0 || load[j] < load[best]) best = (int)j;
             }
@@ -234,6 +274,7 @@ bool plan_bins_grouped(const std::vector<RobotPack>& packs, uint32_t nb, uint32_
             bm[best] += p.n_mass;
             bs[best] += p.springs.size();
             bi[best] += p.inc_estimate;
+            bx[best] += p.face_smem;
             plan[(size_t)best * groups + g].push_back(r);
         }
     }
@@ -244,6 +285,9 @@ bool plan_bins_grouped(const std::vector<RobotPack>& packs, uint32_t nb, uint32_
 struct BinLocal {
     std::vector<uint32_t> mass_gidx, spring_gidx, pair, slice_off, slice_width, inc32;
     std::vector<uint16_t> inc;
+    std::vector<uint32_t> faces, face_row;  // face drag: corners (2 words per face), rows per mass
+    std::vector<uint16_t> face_inc;
+    uint32_t n_face = 0;
     std::vector<float> lbar;
     uint32_t n_mass = 0, n_spring = 0, n_inc = 0, smem = 0, aligned = 0, ranked = 0;
     uint64_t padding = 0;
@@ -356,6 +400,46 @@ void slice_rows(uint32_t nm, const std::vector<uint32_t>& row_start, const std::
     L.padding = L.n_inc - (uint64_t)row_start[nm];
 }
 
+// Faces of a resident bin: the bin-local corners {c0 | c1 << 16, c2} of
+// every face with three distinct corners, robot by robot in face order,
+// and per mass the faces it is a corner of in ascending order -- the
+// summation order of the face drag -- as incidence entries (bin-local face
+// index) and a row per mass: first entry | count << 24.
+void build_faces(const mb_batch_desc* b, const std::vector<RobotPack>& packs,
+                 const std::vector<uint32_t>& robots, uint32_t nm, BinLocal& L) {
+    uint32_t nf = 0;
+    for (uint32_t r : robots) nf += packs[r].n_face;
+    if (!nf) return;
+    L.faces.reserve(2 * (size_t)nf);
+    std::vector<uint32_t> start(nm + 1, 0);
+    uint32_t mbase = 0;
+    for (uint32_t r : robots) {
+        for (int64_t f = b->face_offsets[r]; f < b->face_offsets[r + 1]; ++f) {
+            const uint16_t* c = b->faces + 3 * f;
+            if (c[0] == c[1] || c[0] == c[2] || c[1] == c[2]) continue;
+            const uint32_t c0 = mbase + c[0], c1 = mbase + c[1], c2 = mbase + c[2];
+            L.faces.push_back(c0 | (c1 << 16));
+            L.faces.push_back(c2);
+            start[c0 + 1]++;
+            start[c1 + 1]++;
+            start[c2 + 1]++;
+        }
+        mbase += packs[r].n_mass;
+    }
+    for (uint32_t i = 0; i < nm; ++i) start[i + 1] += start[i];
+    L.face_inc.resize(start[nm]);
+    L.face_row.resize(nm);
+    std::vector<uint32_t> fill(start.begin(), start.end() - 1);
+    for (uint32_t f = 0; f < nf; ++f) {
+        const uint32_t w = L.faces[2 * f];
+        L.face_inc[fill[w & 0xFFFFu]++] = (uint16_t)f;
+        L.face_inc[fill[w >> 16]++] = (uint16_t)f;
+        L.face_inc[fill[L.faces[2 * f + 1]]++] = (uint16_t)f;
+    }
+    for (uint32_t i = 0; i < nm; ++i) L.face_row[i] = start[i] | ((start[i + 1] - start[i]) << 24);
+    L.n_face = nf;
+}
+
 // rows_on_device: only the springs and masses; the rows get a region of
 // generous capacity (twice the rank-layout estimate plus the alignment
 // slack) for the device to build them in.
@@ -387,6 +471,8 @@ void build_bin(const mb_batch_desc* b, const std::vector<RobotPack>& packs,
         }
         mbase += packs[r].n_mass;
     }
+    if (!streamed) build_faces(b, packs, robots, nm, L);
+    const uint32_t face_smem = face_smem_bytes(nm, L.n_face, (uint32_t)L.face_inc.size());
     if (rows_on_device) {
         uint64_t est = 0;
         for (uint32_t r : robots) est += packs[r].inc_estimate;
@@ -397,7 +483,7 @@ void build_bin(const mb_batch_desc* b, const std::vector<RobotPack>& packs,
         L.n_inc = (uint32_t)std::min<uint64_t>(cap, 0xFFFFFFFFu);
         L.slice_off.assign(n_sl, 0);
         L.slice_width.assign(n_sl, 0);
-        L.smem = bin_smem_bytes(nm, ns, (uint32_t)std::min<uint64_t>(est, 0xFFFFFFFFu));
+        L.smem = bin_smem_bytes(nm, ns, (uint32_t)std::min<uint64_t>(est, 0xFFFFFFFFu)) + face_smem;
         return;
     }
     for (uint32_t i = 0; i < nm; ++i) row_start[i + 1] += row_start[i];
@@ -429,7 +515,7 @@ void build_bin(const mb_batch_desc* b, const std::vector<RobotPack>& packs,
     L.n_mass = nm;
     L.n_spring = ns;
     slice_rows(nm, row_start, ents, streamed, L);
-    L.smem = streamed ? stream_smem_bytes(nm) : bin_smem_bytes(nm, ns, L.n_inc);
+    L.smem = streamed ? stream_smem_bytes(nm) : bin_smem_bytes(nm, ns, L.n_inc) + face_smem;
 }
 
 // Offsets of every bin, then every bin copied in parallel into sized
@@ -441,11 +527,17 @@ void assemble(const std::vector<BinLocal>& locals, Packed& out, bool streamed, u
     out.max_smem = 0;
     out.inc_entries = out.inc_padding = 0;
     out.aligned_slices = out.rank_slices = 0;
-    uint64_t nm = 0, ns = 0, nsl = 0, ninc = 0;
+    uint64_t nm = 0, ns = 0, nsl = 0, ninc = 0, nf = 0, nfi = 0;
     for (uint32_t i = 0; i < nb; ++i) {
         const BinLocal& L = locals[i];
         BinDesc& d = out.bins[i];
         std::memset(&d, 0, sizeof(d));
+        d.face_begin = (uint32_t)nf;
+        d.n_face = L.n_face;
+        d.face_inc_begin = (uint32_t)nfi;
+        d.n_face_inc = (uint32_t)L.face_inc.size();
+        nf += L.n_face;
+        nfi += L.face_inc.size();
         d.mass_begin = (uint32_t)nm;
         d.n_mass = L.n_mass;
         d.spring_begin = (uint32_t)ns;
@@ -474,6 +566,9 @@ void assemble(const std::vector<BinLocal>& locals, Packed& out, bool streamed, u
     out.inc32.resize(streamed ? ninc : 0);
     out.rows_on_device = rows_on_device;
     out.row_total = ninc;
+    out.faces.resize(2 * nf);
+    out.face_row.resize(nf ? nm : 0);
+    out.face_inc.resize(nfi);
     parallel_for(nb, threads, [&](uint32_t i) {
         const BinLocal& L = locals[i];
         const BinDesc& d = out.bins[i];
@@ -490,6 +585,14 @@ void assemble(const std::vector<BinLocal>& locals, Packed& out, bool streamed, u
             put(out.inc32, d.inc_begin, L.inc32);
         else
             put(out.inc, d.inc_begin, L.inc);
+        if (!out.face_row.empty()) {
+            put(out.faces, 2 * (size_t)d.face_begin, L.faces);
+            put(out.face_inc, d.face_inc_begin, L.face_inc);
+            if (L.n_face)
+                put(out.face_row, d.mass_begin, L.face_row);
+            else
+                std::memset(out.face_row.data() + d.mass_begin, 0, (size_t)d.n_mass * sizeof(uint32_t));
+        }
     });
 }
 
@@ -917,6 +1020,8 @@ mb_status pack_population(const mb_batch_desc* b, const PackOptions& o, Packed& 
     }
     out.masses = tot_m;
     out.active_springs = tot_s;
+    out.n_faces = 0;
+    for (const auto& p : packs) out.n_faces += p.n_face;
 
     // material slots: the composite ids used by the whole population
     std::vector<int> slot_of(MB_COMPOSITE_COUNT, -1);

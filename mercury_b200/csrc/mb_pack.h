@@ -72,6 +72,12 @@ struct Packed {
     raw_vector<uint16_t> inc;    // resident rows
     raw_vector<uint32_t> inc32;  // streamed rows
     std::vector<uint32_t> exports;  // split bins: own mass | part << 12 | halo slot << 15
+    // face drag (resident bins): corners {c0 | c1 << 16, c2} per face, row
+    // per packed mass (first entry | count << 24), incidence entries; empty
+    // when no bin has faces
+    raw_vector<uint32_t> faces, face_row;
+    raw_vector<uint16_t> face_inc;
+    uint64_t n_faces = 0;  // faces of the population with three distinct corners
     raw_vector<float> lbar;
     std::vector<uint8_t> mat_ids;
     // statistics

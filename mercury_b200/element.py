@@ -7,6 +7,9 @@ id, mass (M,) float32 (reference default 1.0, mass.h:17).
 Element.springs: pairs (S, 2) uint16 robot-local mass indices, mean_length
 (S,) float32, material (S,) composite id; rest_length mirrors mean_length as
 the reference initialises it (VoxelRobot.cpp:149).
+Element.faces: (F, 3) uint16 robot-local corners of the surface triangles
+(Face, face.h:6-10), or None; they act only through the face drag of the
+water mode.
 """
 from __future__ import annotations
 
@@ -27,6 +30,7 @@ class Element:
     stress: np.ndarray | None = None
     sim_time: float = 0.0
     total_sim_time: float = 0.0
+    faces: np.ndarray | None = None
 
     def __post_init__(self):
         self.pos = np.ascontiguousarray(self.pos, np.float32).reshape(-1, 3)
@@ -40,6 +44,8 @@ class Element:
                     else np.ascontiguousarray(self.vel, np.float32).reshape(m, 3))
         self.mass = (np.ones(m, np.float32) if self.mass is None
                      else np.ascontiguousarray(self.mass, np.float32).reshape(m))
+        if self.faces is not None:
+            self.faces = np.ascontiguousarray(self.faces, np.uint16).reshape(-1, 3)
 
     @property
     def n_masses(self) -> int:
@@ -54,7 +60,8 @@ class Element:
                        self.mean_length.copy(), self.spring_material.copy(),
                        self.vel.copy(), self.mass.copy(),
                        None if self.stress is None else self.stress.copy(),
-                       self.sim_time, self.total_sim_time)
+                       self.sim_time, self.total_sim_time,
+                       None if self.faces is None else self.faces.copy())
 
 
 @dataclass
@@ -69,6 +76,8 @@ class Batch:
     spring_material: np.ndarray# uint8 (S,)
     lbar: np.ndarray           # float32 (S,)
     extra: dict = field(default_factory=dict)
+    face_offsets: np.ndarray | None = None  # int64 (R+1,), or None: no faces
+    faces: np.ndarray | None = None         # uint16 (F, 3) robot-local corners
 
     @property
     def n_robots(self) -> int:
@@ -114,7 +123,15 @@ def pack(elements: list[Element]) -> Batch:
         pairs[c:d] = e.pairs
         sm[c:d] = e.spring_material
         lb[c:d] = e.mean_length
-    return Batch(mo, pos, vel, mm, so, pairs, sm, lb)
+    if all(e.faces is None for e in elements):
+        return Batch(mo, pos, vel, mm, so, pairs, sm, lb)
+    nf = np.array([0 if e.faces is None else len(e.faces) for e in elements], np.int64)
+    fo = np.concatenate([[0], np.cumsum(nf)]).astype(np.int64)
+    faces = np.zeros((int(fo[-1]), 3), np.uint16)
+    for r, e in enumerate(elements):
+        if e.faces is not None:
+            faces[fo[r]:fo[r + 1]] = e.faces
+    return Batch(mo, pos, vel, mm, so, pairs, sm, lb, face_offsets=fo, faces=faces)
 
 
 def unpack(batch: Batch, pos: np.ndarray, vel: np.ndarray, stress: np.ndarray | None,

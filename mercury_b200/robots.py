@@ -18,6 +18,10 @@ numpy PCG64):
              springs (deduplicated), materials from a random tanh MLP
              3 -> 25 -> 25 -> 4 over the position (argmax over bone, tissue,
              muscle_a, muscle_b)
+Surfaces (faces=True): voxel robots get the exposed faces of their occupied
+cells, two triangles per square (voxel_faces); point clouds get their
+convex hull (hull_faces), standing in for the alpha-shape surface the
+reference's NNRobot builds with CGAL (NNRobot.cpp:236-311, delaunay.cpp).
 For the reference step, muscle_a is adductor_muscle0 (phase 0) and muscle_b
 abductor_muscle0 (phase pi), material.h:112, 122.  The force-based
 configurations give every mass 0.1 kg (population(..., mass=0.1)) and use
@@ -69,6 +73,44 @@ def lattice_robot(grid: np.ndarray, h: float = CELL, mass: float = 1.0) -> Eleme
     s = ns.value
     return Element(pos.reshape(n, 3), mm, pairs[: 2 * s].reshape(s, 2), lbar[:s], sm[:s],
                    mass=np.full(n, mass, np.float32))
+
+
+def voxel_faces(cells: np.ndarray) -> np.ndarray:
+    """Surface of a voxel robot (voxel_robot(cells)): every face of an
+    occupied (non-air) cell whose neighbour across it is air or outside the
+    grid, as two triangles (p00, p10, p11), (p00, p11, p01) of its corner
+    grid points.  Order: axis x, y, z; the lower side, then the upper; cells
+    in [x, y, z] order.  Returns (F, 3) uint16 grid-point indices (x
+    fastest)."""
+    occ = np.asarray(cells) != AIR
+    sx, sy, sz = occ.shape
+    nx, ny = sx + 1, sy + 1
+    pad = np.pad(occ, 1)
+    out = []
+    for axis in range(3):
+        u, v = [a for a in range(3) if a != axis]
+        eu, ev = np.eye(3, dtype=np.int64)[u], np.eye(3, dtype=np.int64)[v]
+        for side in (0, 1):
+            sl = [slice(1, 1 + sx), slice(1, 1 + sy), slice(1, 1 + sz)]
+            d = 1 if side else -1
+            sl[axis] = slice(1 + d, 1 + d + occ.shape[axis])
+            cell = np.argwhere(occ & ~pad[tuple(sl)])
+            base = cell.copy()
+            base[:, axis] += side
+            corners = [base, base + eu, base + eu + ev, base + ev]
+            p00, p10, p11, p01 = [c[:, 0] + nx * (c[:, 1] + ny * c[:, 2]) for c in corners]
+            tri = np.stack([np.stack([p00, p10, p11], 1), np.stack([p00, p11, p01], 1)], 1).reshape(-1, 3)
+            out.append(tri)
+    return np.concatenate(out).astype(np.uint16) if out else np.zeros((0, 3), np.uint16)
+
+
+def hull_faces(points: np.ndarray) -> np.ndarray:
+    """Convex hull triangles of a point cloud (qhull through scipy), each
+    with ascending corners, sorted.  Returns (F, 3) uint16."""
+    from scipy.spatial import ConvexHull
+    t = np.sort(ConvexHull(np.asarray(points, np.float64)).simplices, axis=1)
+    t = t[np.lexsort((t[:, 2], t[:, 1], t[:, 0]))]
+    return t.astype(np.uint16)
 
 
 def random_cells(side: int, rng: np.random.Generator, choices=FIVE, p=FIVE_P) -> np.ndarray:
@@ -156,8 +198,9 @@ def nn_population_device(n_robots: int = 256, seed_base: int = 2000, mass: float
 
 
 def population(name: str, n_robots: int | None = None, seed_base: int | None = None,
-               mass: float = 1.0) -> list[Element]:
-    """One of the named synthetic populations (see module docstring)."""
+               mass: float = 1.0, faces: bool = False) -> list[Element]:
+    """One of the named synthetic populations (see module docstring); with
+    faces=True every robot carries its surface triangles."""
     spec = {
         "small": (0, 32),
         "uneven": (1, 512),
@@ -173,7 +216,10 @@ def population(name: str, n_robots: int | None = None, seed_base: int | None = N
     for r in range(n):
         rng = np.random.default_rng(seed0 + r)
         if name == "nn":
-            out.append(nn_robot(rng, int(rng.integers(500, 2001)), mass=mass))
+            e = nn_robot(rng, int(rng.integers(500, 2001)), mass=mass)
+            if faces:
+                e.faces = hull_faces(e.pos)
+            out.append(e)
             continue
         if name == "small":
             cells = random_cells(4, rng)
@@ -182,10 +228,13 @@ def population(name: str, n_robots: int | None = None, seed_base: int | None = N
             cells = random_cells(side, rng)
         else:
             cells = FOUR[rng.integers(0, 4, size=(10, 10, 10))]
-        out.append(voxel_robot(cells, mass=mass))
+        e = voxel_robot(cells, mass=mass)
+        if faces:
+            e.faces = voxel_faces(cells)
+        out.append(e)
     return out
 
 
 def population_batch(name: str, n_robots: int | None = None, seed_base: int | None = None,
-                     mass: float = 1.0):
-    return pack(population(name, n_robots, seed_base, mass))
+                     mass: float = 1.0, faces: bool = False):
+    return pack(population(name, n_robots, seed_base, mass, faces))

@@ -35,11 +35,23 @@ MODE_REF_XPBD, MODE_FORCE_LAND, MODE_FORCE_WATER = 0, 1, 2
 # Environments of the force-based benchmark configurations (land: g, the
 # reference's floor stiffness 1e6 (environment.h:15-22), mu_s 1.0, mu_k 0.8;
 # water: buoyancy cancels gravity, 0.5 rho Cd A = 0.5 * 1000 * 1 * 1e-4);
-# velocity damping 0.999 per step.
+# velocity damping 0.999 per step.  No face drag: the benchmark robots carry
+# no faces.  WATER_FACES drags on the robots' surface triangles instead of
+# per mass, with the density of water.
 LAND = dict(g=9.81, floor_stiffness=1.0e6, friction_static=1.0, friction_kinetic=0.8, drag=0.0,
-            damping=0.999)
+            damping=0.999, face_drag=0.0)
 WATER = dict(g=0.0, floor_stiffness=0.0, friction_static=0.0, friction_kinetic=0.0,
-             drag=0.5 * 1000.0 * 1.0 * 1e-4, damping=0.999)
+             drag=0.5 * 1000.0 * 1.0 * 1e-4, damping=0.999, face_drag=0.0)
+WATER_FACES = dict(WATER, drag=0.0, face_drag=1000.0)
+
+
+def _desc(batch: Batch) -> "_lib.BatchDesc":
+    fo, faces = getattr(batch, "face_offsets", None), getattr(batch, "faces", None)
+    return _lib.BatchDesc(
+        batch.n_robots, _lib.ptr(batch.mass_offsets), _lib.ptr(batch.pos), _lib.ptr(batch.vel),
+        _lib.ptr(batch.mass_material), _lib.ptr(batch.spring_offsets), _lib.ptr(batch.pairs),
+        _lib.ptr(batch.spring_material), _lib.ptr(batch.lbar),
+        _lib.ptr(fo) if faces is not None else None, _lib.ptr(faces) if faces is not None else None)
 
 
 @dataclass
@@ -167,10 +179,7 @@ class Simulator:
         self._batch = batch
         self._vox_batch_n = None
         self._topology_stale = False
-        d = _lib.BatchDesc(
-            batch.n_robots, _lib.ptr(batch.mass_offsets), _lib.ptr(batch.pos), _lib.ptr(batch.vel),
-            _lib.ptr(batch.mass_material), _lib.ptr(batch.spring_offsets), _lib.ptr(batch.pairs),
-            _lib.ptr(batch.spring_material), _lib.ptr(batch.lbar))
+        d = _desc(batch)
         _lib.check(_lib.LIB.mb_set_elements(self._ctx, ctypes.byref(d)), self._ctx)
 
     def devo(self, replaced_per_robot: int, seed: int, reference_ranks: bool = False) -> int:
@@ -329,10 +338,7 @@ def body_length(batch: Batch) -> np.ndarray:
 def plan(batch: Batch, num_sms: int = 148, smem_bytes: int = 0, **cfg) -> dict:
     """Launch plan of a population computed on the host, without a GPU
     (mb_plan_population): shape, bins, path and packed-layout statistics."""
-    d = _lib.BatchDesc(
-        batch.n_robots, _lib.ptr(batch.mass_offsets), _lib.ptr(batch.pos), _lib.ptr(batch.vel),
-        _lib.ptr(batch.mass_material), _lib.ptr(batch.spring_offsets), _lib.ptr(batch.pairs),
-        _lib.ptr(batch.spring_material), _lib.ptr(batch.lbar))
+    d = _desc(batch)
     c = _lib.LaunchConfig(cfg.get("threads", 0), cfg.get("springs_per_thread", 0),
                           cfg.get("masses_per_thread", 0), cfg.get("bins", 0), cfg.get("chunk", 0),
                           cfg.get("use_graph", 1), cfg.get("streamed", 0), cfg.get("cluster", 0))

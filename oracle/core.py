@@ -42,8 +42,10 @@ def lib() -> ctypes.CDLL:
         L.or_com_device.restype = None
         L.or_com_reference.argtypes = [I32, P, P, P, P]
         L.or_com_reference.restype = None
-        L.or_force_run.argtypes = [I32, I32, P, P, P, P, P, P, P, P, P, P, F32, F32, U32, I32, I32]
+        L.or_force_run.argtypes = [I32, I32, P, P, P, P, P, P, P, P, P, P, F32, F32, U32, I32, I32, P, P]
         L.or_force_run.restype = I32
+        L.or_face_force.argtypes = [P, P, P, P, P, P, F32, P]
+        L.or_face_force.restype = None
         L.or_force_run_f64.argtypes = [I32, I32, P, P, P, P, P, P, P, P, P, F64, F64, U32]
         L.or_force_run_f64.restype = I32
         U64 = ctypes.c_uint64
@@ -128,15 +130,29 @@ def com_reference(batch, pos) -> np.ndarray:
 
 def force_run(mode, batch, pos, vel, stress, table, env, dt, t0, steps, track, threads=0):
     """Force modes (1 land, 2 water), FP32, in place.  env = (g, floor
-    stiffness, mu_s, mu_k, drag, damping)."""
+    stiffness, mu_s, mu_k, drag, damping[, face_drag]); the batch's faces
+    (if any) drag in water when face_drag is given."""
     assert pos.dtype == np.float32 and vel.dtype == np.float32
     table = np.ascontiguousarray(table, np.float32)
     envf = np.ascontiguousarray(env, np.float32)
+    fo = getattr(batch, "face_offsets", None)
+    faces = len(envf) > 6 and fo is not None and int(fo[-1]) > 0
     rc = lib().or_force_run(mode, batch.n_robots, _p(batch.mass_offsets), _p(pos), _p(vel),
                             _p(batch.spring_offsets), _p(batch.pairs), _p(batch.spring_material),
                             _p(batch.lbar), _p(stress), _p(table), _p(envf), dt, t0, steps,
-                            int(bool(track)), threads)
+                            int(bool(track)), threads,
+                            _p(fo) if faces else None, _p(batch.faces) if faces else None)
     assert rc == 0
+
+
+def face_force(x, v, coef):
+    """Share per corner of the face drag of one triangle: x, v (3, 3) float32
+    corner positions and velocities, coef = -rho/6 (float32)."""
+    x = np.ascontiguousarray(x, np.float32).reshape(3, 3)
+    v = np.ascontiguousarray(v, np.float32).reshape(3, 3)
+    out = np.zeros(3, np.float32)
+    lib().or_face_force(_p(x[0]), _p(x[1]), _p(x[2]), _p(v[0]), _p(v[1]), _p(v[2]), np.float32(coef), _p(out))
+    return out
 
 
 def force_run_f64(mode, batch, pos, vel, table, env, dt, t0, steps):

@@ -19,6 +19,9 @@
  *   centre of mass .......... common/evolvables/SoftBody.cpp:112-121
  *   development (Devo) ...... common/simulator/Simulator.cu:597-668,
  *                             devo_kernel.cu:56-168 (see or_devo)
+ *   face drag ............... sim_kernel.cu:96-121 (the face law of
+ *                             surfaceDragForce; see face_force_f32), added
+ *                             to the forces of the water mode
  *
  * The reference accumulates the per-mass corrections with shared-memory
  * atomics, so its own summation order is unspecified and run-to-run
@@ -390,6 +393,37 @@ int or_xpbd_run_f64(int n_robots, const int64_t* mass_off, double* pos, double* 
 
 
 /* ------------------------------------------------------------------ */
+/* Face drag of one surface triangle (water mode), the share of each corner
+ * (this library's law after sim_kernel.cu:96-121): mean corner velocity v,
+ * N = (x1 - x0) x (x2 - x0), A = |N|, n = N * (1/(A + eps)) turned so that
+ * v.n > 0, out = coef * A * ((v.n) v + 0.2 |v|^2 n), coef = -rho/6.  Each
+ * operation rounds once, in this order. */
+static void face_force_f32(const float* x0, const float* x1, const float* x2, const float* v0,
+                           const float* v1, const float* v2, float coef, float* out) {
+    float v[3], a[3], b[3], u[3];
+    for (int q = 0; q < 3; ++q) {
+        v[q] = ((v0[q] + v1[q]) + v2[q]) / 3.0f;
+        a[q] = x1[q] - x0[q];
+        b[q] = x2[q] - x0[q];
+    }
+    const float nx = a[1] * b[2] - a[2] * b[1];
+    const float ny = a[2] * b[0] - a[0] * b[2];
+    const float nz = a[0] * b[1] - a[1] * b[0];
+    const float area = sqrtf(fmaf(nx, nx, fmaf(ny, ny, nz * nz)));
+    const float r = 1.0f / (area + OR_EPS);
+    u[0] = nx * r;
+    u[1] = ny * r;
+    u[2] = nz * r;
+    float vn = fmaf(u[0], v[0], fmaf(u[1], v[1], u[2] * v[2]));
+    if (!(vn > 0.0f)) {
+        for (int q = 0; q < 3; ++q) u[q] = -u[q];
+        vn = -vn;
+    }
+    const float lift = 0.2f * fmaf(v[0], v[0], fmaf(v[1], v[1], v[2] * v[2]));
+    const float c = coef * area;
+    for (int q = 0; q < 3; ++q) out[q] = c * fmaf(lift, u[q], vn * v[q]);
+}
+
 /* Force modes (no reference code: restated from the paper's Algorithm 1,
  * mercury_fall_2023.pdf section II.B, and the benchmark configurations):
  * Hooke springs F_a = -k (d - L) n, n = (x_a - x_b)/d, L = Lbar (1 + dL0
@@ -403,12 +437,15 @@ int or_xpbd_run_f64(int n_robots, const int64_t* mass_off, double* pos, double* 
  * In FP32 the divisions by m and dt are multiplications by the correctly
  * rounded reciprocals 1/m and 1/dt (the law is this library's own, so its
  * rounding is too); only the kinetic friction divides, by |h|.
- * env = {g, floor_stiffness, mu_s, mu_k, drag, damping}; m = pos.w. */
+ * env = {g, floor_stiffness, mu_s, mu_k, drag, damping[, face_drag]}; m = pos.w.
+ * Faces (nf triangles, robot-local corners; water only, when face_drag is
+ * given): each face with three distinct corners adds face_force_f32 to the
+ * force of each corner, after the springs, faces in ascending order. */
 static void force_robot_f32(int mode, int nm, float* pos, float* vel, int ns,
                             const uint16_t* pairs, const uint8_t* mat,
                             const float* lbar, float* stress,
                             const float* table, const float* env, float dt, float t0,
-                            uint32_t steps, int track) {
+                            uint32_t steps, int track, int nf, const uint16_t* faces) {
     int* deg = (int*)calloc((size_t)nm + 1, sizeof(int));
     for (int s = 0; s < ns; ++s) {
         if (!mat[s]) continue;
@@ -431,6 +468,28 @@ static void force_robot_f32(int mode, int nm, float* pos, float* vel, int ns,
             inc[k + 1] = h;
         }
     float* f = (float*)malloc(sizeof(float) * 3 * (size_t)(ns + 1));
+    /* per mass: the faces it is a corner of, ascending */
+    if (mode != 2 || !faces || env[6] == 0.0f) nf = 0;
+    int* fdeg = (int*)calloc((size_t)nm + 1, sizeof(int));
+    int* finc = (int*)malloc(sizeof(int) * (3 * (size_t)nf + 1));
+    float* ff = (float*)malloc(sizeof(float) * (3 * (size_t)nf + 1));
+    for (int q = 0; q < nf; ++q) {
+        const uint16_t* c = faces + 3 * q;
+        if (c[0] == c[1] || c[0] == c[2] || c[1] == c[2]) continue;
+        for (int k = 0; k < 3; ++k) fdeg[c[k] + 1]++;
+    }
+    for (int i = 0; i < nm; ++i) fdeg[i + 1] += fdeg[i];
+    {
+        int* ffill = (int*)malloc(sizeof(int) * ((size_t)nm + 1));
+        memcpy(ffill, fdeg, sizeof(int) * (size_t)nm);
+        for (int q = 0; q < nf; ++q) {
+            const uint16_t* c = faces + 3 * q;
+            if (c[0] == c[1] || c[0] == c[2] || c[1] == c[2]) continue;
+            for (int k = 0; k < 3; ++k) finc[ffill[c[k]]++] = q;
+        }
+        free(ffill);
+    }
+    const float fcoef = nf ? (float)(-(double)env[6] / 6.0) : 0.0f;
     float rc[OR_COMPOSITE_COUNT];
     const float g = env[0], kfl = env[1], mus = env[2], muk = env[3], cdrag = env[4], damp = env[5];
     const float inv_dt = 1.0f / dt;
@@ -458,12 +517,20 @@ static void force_robot_f32(int mode, int nm, float* pos, float* vel, int ns,
             f[3 * s + 2] = coef * dz;
             if (track) stress[s] = stress[s] + (-lam) * (1.0f / lbar[s]);
         }
+        for (int q = 0; q < nf; ++q) {
+            const uint16_t* c = faces + 3 * q;
+            if (c[0] == c[1] || c[0] == c[2] || c[1] == c[2]) continue;
+            face_force_f32(pos + 4 * c[0], pos + 4 * c[1], pos + 4 * c[2], vel + 4 * c[0], vel + 4 * c[1],
+                           vel + 4 * c[2], fcoef, ff + 3 * q);
+        }
         for (int i = 0; i < nm; ++i) {
             float F[3] = {0.0f, 0.0f, 0.0f};
             for (int e = deg[i]; e < deg[i + 1]; ++e) {
                 int h = inc[e], s = h >> 1;
                 for (int c = 0; c < 3; ++c) F[c] = (h & 1) ? F[c] - f[3 * s + c] : F[c] + f[3 * s + c];
             }
+            for (int e = fdeg[i]; e < fdeg[i + 1]; ++e)
+                for (int c = 0; c < 3; ++c) F[c] = F[c] + ff[3 * finc[e] + c];
             float* x = pos + 4 * i;
             float* v = vel + 4 * i;
             float mass = x[3];
@@ -501,12 +568,21 @@ static void force_robot_f32(int mode, int nm, float* pos, float* vel, int ns,
         t = t + dt;
     }
     free(deg); free(inc); free(fill); free(f);
+    free(fdeg); free(finc); free(ff);
 }
 
+/* One face's share per corner (face_force_f32), for tests. */
+void or_face_force(const float* x0, const float* x1, const float* x2, const float* v0, const float* v1,
+                   const float* v2, float coef, float* out) {
+    face_force_f32(x0, x1, x2, v0, v1, v2, coef, out);
+}
+
+/* face_off / faces may be NULL (no faces); with faces, env has 7 entries. */
 int or_force_run(int mode, int n_robots, const int64_t* mass_off, float* pos, float* vel,
                  const int64_t* spring_off, const uint16_t* pairs, const uint8_t* mat,
                  const float* lbar, float* stress, const float* table, const float* env,
-                 float dt, float t0, uint32_t steps, int track, int threads) {
+                 float dt, float t0, uint32_t steps, int track, int threads,
+                 const int64_t* face_off, const uint16_t* faces) {
     if (mode != 1 && mode != 2) return -1;
 #ifdef _OPENMP
     if (threads > 0) omp_set_num_threads(threads);
@@ -514,9 +590,12 @@ int or_force_run(int mode, int n_robots, const int64_t* mass_off, float* pos, fl
 #endif
     for (int r = 0; r < n_robots; ++r) {
         int64_t m0 = mass_off[r], s0 = spring_off[r];
+        const int64_t f0 = face_off ? face_off[r] : 0;
+        const int nf = face_off ? (int)(face_off[r + 1] - f0) : 0;
         force_robot_f32(mode, (int)(mass_off[r + 1] - m0), pos + 4 * m0, vel + 4 * m0,
                         (int)(spring_off[r + 1] - s0), pairs + 2 * s0, mat + s0, lbar + s0,
-                        stress ? stress + s0 : NULL, table, env, dt, t0, steps, track && stress);
+                        stress ? stress + s0 : NULL, table, env, dt, t0, steps, track && stress,
+                        nf, faces ? faces + 3 * f0 : NULL);
     }
     return 0;
 }
