@@ -149,7 +149,8 @@ struct mb_context {
     mb::DevBuf<uint32_t> face_row;
     mb::DevBuf<uint16_t> face_inc;
     uint64_t n_faces = 0;          // faces of the population (three distinct corners)
-    bool faces_resident = false;   // the packed bins hold them (not split, not streamed)
+    bool faces_packed = false;     // the packed bins hold them (resident or streamed bins, not split)
+    mb::DevBuf<float4> fd_scratch;  // streamed bins: face forces of a step
     mb::Packed upload_pack;                // host packing of the last mb_set_elements (reused)
     uint32_t cluster = 0;                  // split bins: CTAs per robot (0 = not split)
     // split bins in two groups: bins from split_bins0 in clusters of
@@ -368,7 +369,8 @@ mb_status upload_packed(mb_context* ctx, const mb::Packed& out, bool* rows_faile
     MB_CUDA(ctx, up(ctx->face_row, out.face_row.data(), out.face_row.size()));
     MB_CUDA(ctx, up(ctx->face_inc, out.face_inc.data(), out.face_inc.size()));
     ctx->n_faces = out.n_faces;
-    ctx->faces_resident = !out.face_row.empty();
+    ctx->faces_packed = !out.face_row.empty();
+    if (out.streamed && ctx->faces_packed) MB_CUDA(ctx, ctx->fd_scratch.alloc(out.faces.size() / 2));
     if (out.streamed) {
         MB_CUDA(ctx, up(ctx->inc32, out.inc32.data(), out.inc32.size()));
         MB_CUDA(ctx, ctx->dp_scratch.alloc(std::max<size_t>(out.pair.size(), 1)));
@@ -502,8 +504,14 @@ mb_status devo_setup(mb_context* c) {
     return MB_OK;
 }
 
-// Host re-packing of the context's topology copy (fallback of development).
-mb_status host_repack(mb_context* c) {
+// Whether the step applies the face drag (water mode, rho != 0): robots
+// with faces are then not split over clusters (split bins carry no faces).
+bool face_drag_on(const mb_context* c) { return c->mode == MB_MODE_FORCE_WATER && c->env.face_drag != 0.0f; }
+
+// Host re-packing of the context's topology copy: the fallback of
+// development (`devo`), or a re-plan without split robots when the face
+// drag is switched on for a split population.
+mb_status host_repack(mb_context* c, bool devo = true) {
     // split robots are cut by their current positions
     std::vector<float> pos;
     if (c->cluster) {
@@ -525,12 +533,12 @@ mb_status host_repack(mb_context* c) {
                           faces ? c->h_face_off.data() : nullptr,
                           faces ? c->h_faces.data() : nullptr};
     mb::Packed out;
-    mb_status st = pack(c, &d, true, out, true);
+    mb_status st = pack(c, &d, true, out, !(faces && face_drag_on(c)));
     if (st == MB_OK) st = upload_packed(c, out);
     if (st != MB_OK) c->loaded = false;  // topology and packed arrays disagree now
     c->vox.valid = false;
     c->vox_live = false;
-    ++c->devo_host_repacks;
+    if (devo) ++c->devo_host_repacks;
     return st;
 }
 
@@ -919,7 +927,8 @@ mb_status mb_set_elements(mb_context* ctx, const mb_batch_desc* b) {
     mb::Packed& out = ctx->upload_pack;
     const char* host_rows = std::getenv("MB_HOST_ROWS");
     const bool device_rows = !(host_rows && host_rows[0] == '1');
-    const mb_status pst = mb_detail::pack(ctx, b, false, out, true, device_rows);
+    const bool allow_split = !(F && mb_detail::face_drag_on(ctx));
+    const mb_status pst = mb_detail::pack(ctx, b, false, out, allow_split, device_rows);
     copier.join();
     if (pst != MB_OK) return pst;
 
@@ -961,7 +970,7 @@ mb_status mb_set_elements(mb_context* ctx, const mb_batch_desc* b) {
     mb_status ust = mb_detail::upload_packed(ctx, out, &rows_failed);
     if (ust == MB_OK && rows_failed) {  // rare: the host builds the rows
         MB_TRACE("device rows did not fit; host rows");
-        ust = mb_detail::pack(ctx, b, false, out, true, false);
+        ust = mb_detail::pack(ctx, b, false, out, allow_split, false);
         if (ust == MB_OK) ust = mb_detail::upload_packed(ctx, out);
     }
     if (ust != MB_OK) return ust;
@@ -1023,8 +1032,9 @@ mb::StepParams make_params(mb_context* c, float t0, uint32_t steps, bool track) 
     p.faces = c->faces.p;
     p.face_row = c->face_row.p;
     p.face_inc = c->face_inc.p;
+    p.fd = c->fd_scratch.p;
     p.face_coef = (float)(-(double)c->env.face_drag / 6.0);
-    p.face_on = c->mode == MB_MODE_FORCE_WATER && c->env.face_drag != 0.0f && c->faces_resident ? 1u : 0u;
+    p.face_on = c->mode == MB_MODE_FORCE_WATER && c->env.face_drag != 0.0f && c->faces_packed ? 1u : 0u;
     return p;
 }
 
@@ -1088,9 +1098,12 @@ cudaError_t issue_chunks(mb_context* c, float t0, uint32_t steps, bool track) {
 mb_status run(mb_context* c, uint32_t steps, bool track) {
     if (!c->loaded) return fail(c, MB_ERR_STATE, "no population uploaded");
     if (steps == 0) return MB_OK;
-    if (c->mode == MB_MODE_FORCE_WATER && c->env.face_drag != 0.0f && c->n_faces && !c->faces_resident)
-        return fail(c, MB_ERR_CAPACITY,
-                    "face drag needs every robot with faces in one CTA (this population is split or streamed)");
+    if (face_drag_on(c) && c->n_faces && !c->faces_packed) {
+        // split robots carry no faces: re-plan them streamed (once)
+        const mb_status rs = host_repack(c, false);
+        if (rs != MB_OK) return rs;
+        if (!c->faces_packed) return fail(c, MB_ERR_CAPACITY, "face drag: the faces do not fit the step kernels");
+    }
     cudaSetDevice(c->device);
     const float t0 = c->total_time;
     if (c->use_graph) {

@@ -82,6 +82,7 @@ struct StepParams {
     const uint2* faces;           // packed face: {c0 | c1 << 16, c2}, bin-local corners
     const uint32_t* face_row;     // packed mass: first entry (bin-relative) | count << 24
     const uint16_t* face_inc;     // face incidence entries: bin-local face index
+    float4* fd;                   // streamed kernel: face forces of the current step
     float face_coef;              // -rho/6: -rho/2 of the face law and the 1/3 per corner
     uint32_t face_on;             // face drag active (water mode, rho != 0)
 };
@@ -153,6 +154,12 @@ __host__ __device__ inline uint32_t face_smem_bytes(uint32_t n_mass, uint32_t n_
     return n_face ? 16u + 16u * n_mass + 24u * n_face + 2u * n_face_inc : 0u;
 }
 constexpr uint32_t kMaxFacesPerMass = 255;  // 8-bit count in face_row
+constexpr uint32_t kMaxRobotFaces = 65535;   // 16-bit face index in an entry
+// Streamed bins: the velocities after the material factors (face forces
+// go through global memory).
+__host__ __device__ inline uint32_t stream_face_smem_bytes(uint32_t n_mass, uint32_t n_face) {
+    return n_face ? 16u * n_mass : 0u;
+}
 
 // Split bins: two predicted-position buffers of x_stride slots, the
 // corrections, the material factors, the buffer strides of the cluster's

@@ -388,6 +388,7 @@ __global__ void __launch_bounds__(T, 1024 / T) step_kernel(const StepParams p) {
 template <int T, int MPT, int MODE, bool TRACK>
 __global__ void __launch_bounds__(T, 1024 / T) stream_kernel(const StepParams p) {
     constexpr bool XPBD = MODE == kModeXpbd;
+    constexpr bool FACES = MODE == kModeForceWaterFaces;  // face drag compiled in
     extern __shared__ float4 smem4[];
     const int tid = threadIdx.x;
     const float dt = p.dt;
@@ -404,6 +405,13 @@ __global__ void __launch_bounds__(T, 1024 / T) stream_kernel(const StepParams p)
         const uint32_t* pair = p.spring_pair + bd.spring_begin;
         const float* lbar = p.spring_lbar + bd.spring_begin;
         const uint32_t* inc = p.inc32 + bd.inc_begin;
+        // face drag: velocities in shared memory after the material factors,
+        // face forces through the global scratch like the corrections
+        const uint32_t n_face = FACES && p.face_on ? bd.n_face : 0u;
+        float4* sv = reinterpret_cast<float4*>(smat + kMaxMaterialSlots);
+        float4* fd = p.fd + bd.face_begin;
+        const uint2* fcorner = p.faces + bd.face_begin;
+        const uint16_t* finc = p.face_inc + bd.face_inc_begin;
         const uint32_t n_mat = *p.n_mat;
         float next_rate = 0.0f;
         if (tid < n_mat) {
@@ -416,7 +424,7 @@ __global__ void __launch_bounds__(T, 1024 / T) stream_kernel(const StepParams p)
 
         float3 x[MPT], v[MPT];
         float mass[MPT];
-        uint32_t roff[MPT], rwid[MPT];
+        uint32_t roff[MPT], rwid[MPT], frow[MPT];
 #pragma unroll
         for (int j = 0; j < MPT; ++j) {
             const uint32_t m = tid + j * T;
@@ -425,6 +433,8 @@ __global__ void __launch_bounds__(T, 1024 / T) stream_kernel(const StepParams p)
             mass[j] = 1.0f;
             roff[j] = 0;
             rwid[j] = 0;
+            frow[j] = 0;
+            if (n_face && m < bd.n_mass) frow[j] = __ldg(&p.face_row[bd.mass_begin + m]);
             if (m < bd.n_mass) {
                 const uint32_t g = __ldg(&p.mass_gidx[bd.mass_begin + m]);
                 const float4 P = p.pos[g], V = p.vel[g];
@@ -453,6 +463,7 @@ __global__ void __launch_bounds__(T, 1024 / T) stream_kernel(const StepParams p)
                                          __fadd_rn(x[j].z, __fmul_rn(v[j].z, dt)), 0.0f);
                 else
                     sxt[m] = make_float4(x[j].x, x[j].y, x[j].z, 0.0f);
+                if (n_face) sv[m] = make_float4(v[j].x, v[j].y, v[j].z, 0.0f);
             }
             __syncthreads();
             for (uint32_t s = tid; s < bd.n_spring; s += T) {
@@ -471,6 +482,11 @@ __global__ void __launch_bounds__(T, 1024 / T) stream_kernel(const StepParams p)
                 __stcg(&dp[s], make_float4(__fmul_rn(coef, dx), __fmul_rn(coef, dy), __fmul_rn(coef, dz), 0.0f));
                 if (TRACK) stp[s] = __fadd_rn(stp[s], __fmul_rn(XPBD ? lam : -lam, __frcp_rn(lb)));
             }
+            for (uint32_t f = tid; f < n_face; f += T) {
+                const uint2 c = __ldg(&fcorner[f]);
+                const uint32_t i0 = c.x & 0xFFFFu, i1 = c.x >> 16, i2 = c.y;
+                __stcg(&fd[f], face_force(sxt[i0], sxt[i1], sxt[i2], sv[i0], sv[i1], sv[i2], p.face_coef));
+            }
             __syncthreads();
 #pragma unroll
             for (int j = 0; j < MPT; ++j) {
@@ -486,6 +502,13 @@ __global__ void __launch_bounds__(T, 1024 / T) stream_kernel(const StepParams p)
                         ay = __fmaf_rn(c.y, sg, ay);
                         az = __fmaf_rn(c.z, sg, az);
                     }
+                }
+                // face drag after the springs, faces in ascending order
+                for (uint32_t k = 0; k < (frow[j] >> 24); ++k) {
+                    const float4 c = __ldcg(&fd[__ldg(&finc[(frow[j] & 0xFFFFFFu) + k])]);
+                    ax = __fadd_rn(ax, c.x);
+                    ay = __fadd_rn(ay, c.y);
+                    az = __fadd_rn(az, c.z);
                 }
                 if (XPBD) {
                     const float4 xt = sxt[m];
@@ -652,7 +675,7 @@ const ShapeEntry kSplitShapes[] = {
 
 struct StreamEntry {
     uint32_t threads, mpt;
-    StepFn fn[3][2];
+    StepFn fn[4][2];  // [mode][track]; mode 3: water with face drag
 };
 #define MB_STREAM(T, M)                                                                          \
     {                                                                                            \
@@ -662,6 +685,8 @@ struct StreamEntry {
                  stream_kernel<T, M, kModeForceLand, true>},                                     \
                 {stream_kernel<T, M, kModeForceWater, false>,                                    \
                  stream_kernel<T, M, kModeForceWater, true>},                                    \
+                {stream_kernel<T, M, kModeForceWaterFaces, false>,                               \
+                 stream_kernel<T, M, kModeForceWaterFaces, true>},                               \
         }                                                                                        \
     }
 // up to threads * MPT masses per bin (2,048 or 4,096 with 1,024 threads)
@@ -803,15 +828,20 @@ cudaError_t prepare_stream(uint32_t threads, uint32_t mpt, uint32_t mode, bool t
                            uint32_t smem_bytes) {
     const StreamEntry* e = find_stream(threads, mpt);
     if (!e || mode > kModeForceWater) return cudaErrorInvalidValue;
-    return cudaFuncSetAttribute(e->fn[mode][track ? 1 : 0],
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
+    cudaError_t r = cudaFuncSetAttribute(e->fn[mode][track ? 1 : 0],
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
+    if (r == cudaSuccess && mode == kModeForceWater)  // and the face-drag variant
+        r = cudaFuncSetAttribute(e->fn[kModeForceWaterFaces][track ? 1 : 0],
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
+    return r;
 }
 
 cudaError_t launch_stream(const StepParams& p, uint32_t threads, uint32_t mpt, cudaStream_t s) {
     const StreamEntry* e = find_stream(threads, mpt);
     if (!e || p.mode > kModeForceWater) return cudaErrorInvalidValue;
     if (p.n_bins == 0) return cudaSuccess;
-    e->fn[p.mode][p.track ? 1 : 0]<<<p.n_bins, threads, p.smem_bytes, s>>>(p);
+    const uint32_t variant = p.mode == kModeForceWater && p.face_on ? kModeForceWaterFaces : p.mode;
+    e->fn[variant][p.track ? 1 : 0]<<<p.n_bins, threads, p.smem_bytes, s>>>(p);
     return cudaGetLastError();
 }
 

@@ -171,6 +171,12 @@ void preprocess(const mb_batch_desc* b, uint32_t r, RobotPack& p) {
                     return;
                 }
         }
+        if (nf > kMaxRobotFaces) {
+            std::snprintf(buf, sizeof(buf), "robot %u has %u faces (max %u)", r, nf, kMaxRobotFaces);
+            p.error = buf;
+            p.status = MB_ERR_CAPACITY;
+            return;
+        }
         p.n_face = nf;
         // velocities of every mass of a bin that has faces, alignment, the
         // faces (force, corners) and their three incidence entries
@@ -471,8 +477,9 @@ void build_bin(const mb_batch_desc* b, const std::vector<RobotPack>& packs,
         }
         mbase += packs[r].n_mass;
     }
-    if (!streamed) build_faces(b, packs, robots, nm, L);
-    const uint32_t face_smem = face_smem_bytes(nm, L.n_face, (uint32_t)L.face_inc.size());
+    build_faces(b, packs, robots, nm, L);
+    const uint32_t face_smem = streamed ? stream_face_smem_bytes(nm, L.n_face)
+                                        : face_smem_bytes(nm, L.n_face, (uint32_t)L.face_inc.size());
     if (rows_on_device) {
         uint64_t est = 0;
         for (uint32_t r : robots) est += packs[r].inc_estimate;
@@ -515,7 +522,7 @@ void build_bin(const mb_batch_desc* b, const std::vector<RobotPack>& packs,
     L.n_mass = nm;
     L.n_spring = ns;
     slice_rows(nm, row_start, ents, streamed, L);
-    L.smem = streamed ? stream_smem_bytes(nm) : bin_smem_bytes(nm, ns, L.n_inc) + face_smem;
+    L.smem = (streamed ? stream_smem_bytes(nm) : bin_smem_bytes(nm, ns, L.n_inc)) + face_smem;
 }
 
 // Offsets of every bin, then every bin copied in parallel into sized

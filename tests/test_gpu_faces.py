@@ -115,17 +115,32 @@ def test_faces_after_development():
     same(sim, oracle(b2, env, 150, True, state=state, t0=t))
 
 
-def test_face_drag_needs_resident_bins():
-    els = robots.population("nn", 2, mass=0.1, faces=True)  # split over clusters
-    b = mb.pack(els)
+@pytest.mark.parametrize("track", [False, True])
+def test_streamed_bins_bit_exact(track):
+    b = moving(robots.population_batch("uneven", 12, mass=0.1, faces=True), 7)
+    sim = gpu(b, S.WATER_FACES, 300, track, {"streamed": 1, "chunk": 128})
+    assert sim.launch_config()["streamed"] == 1
+    same(sim, oracle(b, S.WATER_FACES, 300, track), track)
+
+
+def test_split_population_is_replanned_streamed_for_face_drag():
+    b = moving(mb.pack(robots.population("nn", 2, mass=0.1, faces=True)), 8)
     sim = mb.Simulator(0)
     sim.set_materials(mb.materials.force_table())
     sim.set_mode(S.MODE_FORCE_WATER)
-    sim.set_environment(**S.WATER_FACES)
+    sim.set_environment(**dict(S.WATER_FACES, face_drag=0.0))
+    sim.setTimeStep(1e-4)
     sim.set_batch(b)
-    assert sim.launch_config()["cluster"] > 0
-    with pytest.raises(mb._lib.MercuryError) as ex:
-        sim.run_steps(10, False)
-    assert ex.value.status == 3  # MB_ERR_CAPACITY
-    sim.set_environment(face_drag=0.0)
-    sim.run_steps(10, False)
+    assert sim.launch_config()["cluster"] > 0  # no face drag: split over clusters
+    sim.run_steps(100, True)
+    ref = oracle(b, dict(S.WATER_FACES, face_drag=0.0), 100, True)
+    same(sim, ref)
+    t = sim.getTotalTime()
+    sim.set_environment(face_drag=S.WATER_FACES["face_drag"])
+    sim.run_steps(200, True)  # re-planned without clusters, state kept
+    cfg = sim.launch_config()
+    assert cfg["cluster"] == 0 and cfg["streamed"] == 1
+    same(sim, oracle(b, S.WATER_FACES, 200, True, state=ref, t0=t))
+    # uploading while the face drag is on plans no split at all
+    sim.set_batch(b)
+    assert sim.launch_config()["cluster"] == 0
