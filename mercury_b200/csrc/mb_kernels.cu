@@ -118,16 +118,17 @@ __device__ __forceinline__ float velocity_of(float delta, double dt, double inv_
 }
 
 // Face drag of one surface triangle (water), the share of each corner:
-// mean corner velocity v, N = (x1 - x0) x (x2 - x0), A = |N|, unit normal
+// mean corner velocity v = (v0 + v1 + v2) * RN(1/3), N = (x1 - x0) x (x2 - x0), A = |N|, unit normal
 // n = N * RN(1/(A + eps)) turned so that v.n > 0 (sim_kernel.cu:106-109),
 // force coef * A * ((v.n) v + 0.2 |v|^2 n) with coef = -rho/6, i.e.
 // -rho/2 A (...) / 3 (sim_kernel.cu:110-111).  Every operation rounds once,
 // in this order.
 __device__ __forceinline__ float4 face_force(const float4 x0, const float4 x1, const float4 x2, const float4 v0,
                                              const float4 v1, const float4 v2, const float coef) {
-    const float vx = __fdiv_rn(__fadd_rn(__fadd_rn(v0.x, v1.x), v2.x), 3.0f);
-    const float vy = __fdiv_rn(__fadd_rn(__fadd_rn(v0.y, v1.y), v2.y), 3.0f);
-    const float vz = __fdiv_rn(__fadd_rn(__fadd_rn(v0.z, v1.z), v2.z), 3.0f);
+    constexpr float kThird = 0x1.555556p-2f;  // 1/3 rounded to nearest
+    const float vx = __fmul_rn(__fadd_rn(__fadd_rn(v0.x, v1.x), v2.x), kThird);
+    const float vy = __fmul_rn(__fadd_rn(__fadd_rn(v0.y, v1.y), v2.y), kThird);
+    const float vz = __fmul_rn(__fadd_rn(__fadd_rn(v0.z, v1.z), v2.z), kThird);
     const float ax = __fsub_rn(x1.x, x0.x), ay = __fsub_rn(x1.y, x0.y), az = __fsub_rn(x1.z, x0.z);
     const float bx = __fsub_rn(x2.x, x0.x), by = __fsub_rn(x2.y, x0.y), bz = __fsub_rn(x2.z, x0.z);
     const float nx = __fsub_rn(__fmul_rn(ay, bz), __fmul_rn(az, by));
@@ -214,20 +215,17 @@ __global__ void __launch_bounds__(T, 1024 / T) step_kernel(const StepParams p) {
                 if (TRACK) st[j] = p.stress[__ldg(&p.spring_gidx[g]) & 0x7FFFFFFFu];
             }
         }
-        // Masses of this thread: x, v, mass, the SELL row (offset | width << 20)
-        // and the face row (first entry | count << 24).
+        // Masses of this thread: x, v, mass and the SELL row (offset | width << 20).
         float3 x[MPT], v[MPT];
         float mass[MPT];
-        uint32_t row[MPT], frow[MPT];
+        uint32_t row[MPT];
 #pragma unroll
         for (int j = 0; j < MPT; ++j) {
             const uint32_t m = tid + j * T;
             x[j] = make_float3(0.f, 0.f, 0.f);
             v[j] = make_float3(0.f, 0.f, 0.f);
             row[j] = 0;
-            frow[j] = 0;
             mass[j] = 1.0f;
-            if (n_face && m < bd.n_mass) frow[j] = __ldg(&p.face_row[bd.mass_begin + m]);
             if (m < bd.n_mass) {
                 const uint32_t g = __ldg(&p.mass_gidx[bd.mass_begin + m]);
                 const float4 P = p.pos[g], V = p.vel[g];
@@ -339,8 +337,10 @@ __global__ void __launch_bounds__(T, 1024 / T) step_kernel(const StepParams p) {
                     x[j] = make_float3(nx, ny, nz);
                 } else {
                     // face drag after the springs, faces in ascending order
-                    const uint16_t* fp = sfinc + (frow[j] & 0xFFFFFFu);
-                    for (uint32_t k = 0; k < (frow[j] >> 24); ++k) {
+                    // (the face row: first entry | count << 24)
+                    const uint32_t fr = n_face ? __ldg(&p.face_row[bd.mass_begin + m]) : 0u;
+                    const uint16_t* fp = sfinc + (fr & 0xFFFFFFu);
+                    for (uint32_t k = 0; k < (fr >> 24); ++k) {
                         const float4 c = sfd[fp[k]];
                         ax = __fadd_rn(ax, c.x);
                         ay = __fadd_rn(ay, c.y);

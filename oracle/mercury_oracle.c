@@ -394,7 +394,8 @@ int or_xpbd_run_f64(int n_robots, const int64_t* mass_off, double* pos, double* 
 
 /* ------------------------------------------------------------------ */
 /* Face drag of one surface triangle (water mode), the share of each corner
- * (this library's law after sim_kernel.cu:96-121): mean corner velocity v,
+ * (this library's law after sim_kernel.cu:96-121): mean corner velocity
+ * v = (v0 + v1 + v2) * RN(1/3),
  * N = (x1 - x0) x (x2 - x0), A = |N|, n = N * (1/(A + eps)) turned so that
  * v.n > 0, out = coef * A * ((v.n) v + 0.2 |v|^2 n), coef = -rho/6.  Each
  * operation rounds once, in this order. */
@@ -402,7 +403,7 @@ static void face_force_f32(const float* x0, const float* x1, const float* x2, co
                            const float* v1, const float* v2, float coef, float* out) {
     float v[3], a[3], b[3], u[3];
     for (int q = 0; q < 3; ++q) {
-        v[q] = ((v0[q] + v1[q]) + v2[q]) / 3.0f;
+        v[q] = ((v0[q] + v1[q]) + v2[q]) * 0x1.555556p-2f; /* RN(1/3) */
         a[q] = x1[q] - x0[q];
         b[q] = x2[q] - x0[q];
     }
