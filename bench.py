@@ -409,6 +409,26 @@ def secondary(args, batch, local_rank, dev, hbm_peak):
         out[name] = {"value": rate, "unit": "spring-updates/s", "steps": 5000,
                      "finite": bool(np.isfinite(p).all()), "config": fs.launch_config()}
         del fs
+    # water with the face drag: the same robots with their exposed cell faces
+    # (two triangles per square), drag on the faces instead of per mass
+    els = robots.population("uneven", batch.n_robots, mass=0.1, faces=True)
+    wb = mb.pack(els)
+    fs = mb.Simulator(local_rank)
+    fs.set_materials(mb.materials.force_table())
+    fs.set_mode(S.MODE_FORCE_WATER)
+    fs.set_environment(**S.WATER_FACES)
+    fs.setTimeStep(1e-4)
+    fs.set_batch(wb)
+    rate = _device_rate(fs, wb.active_springs(), 5000, False, dev)
+    p, _, _ = fs.collect_arrays()
+    n_faces = int(wb.face_offsets[-1])
+    out["force_water_faces"] = {
+        "value": rate, "unit": "spring-updates/s", "steps": 5000, "finite": bool(np.isfinite(p).all()),
+        "faces": n_faces, "face_updates_per_s": rate * n_faces / wb.active_springs(),
+        "workload": f"the headline robots with 0.1 kg masses and {n_faces} surface triangles, water, "
+                    f"face drag rho = {S.WATER_FACES['face_drag']:g} (no per-mass drag)",
+        "config": fs.launch_config()}
+    del fs
     def large(batch, mode, env, workload):
         """Default path (robots split over thread-block clusters) and, for
         comparison, the streamed kernel (never split)."""
