@@ -148,10 +148,10 @@ __host__ __device__ inline uint32_t bin_smem_bytes_dev(uint32_t n_mass, uint32_t
 }
 
 // Face drag of a resident bin, after its rows (16-byte aligned): the
-// velocities of its masses, the forces and corners of its faces, and their
-// incidence entries.
+// velocities of its masses, the forces and corners of its faces, the face
+// row of each mass and the incidence entries.
 __host__ __device__ inline uint32_t face_smem_bytes(uint32_t n_mass, uint32_t n_face, uint32_t n_face_inc) {
-    return n_face ? 16u + 16u * n_mass + 24u * n_face + 2u * n_face_inc : 0u;
+    return n_face ? 16u + 20u * n_mass + 24u * n_face + 2u * n_face_inc : 0u;
 }
 constexpr uint32_t kMaxFacesPerMass = 255;  // 8-bit count in face_row
 constexpr uint32_t kMaxRobotFaces = 65535;   // 16-bit face index in an entry

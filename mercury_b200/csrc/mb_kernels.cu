@@ -175,17 +175,20 @@ __global__ void __launch_bounds__(T, 1024 / T) step_kernel(const StepParams p) {
         uint32_t* sexp = sstride + (SPLIT ? kMaxClusterParts : 0u);
         uint16_t* sinc = reinterpret_cast<uint16_t*>(sexp + (SPLIT ? bd.n_export : 0u));
         // face drag (water, resident bins with faces), after the rows at a
-        // 16-byte boundary: velocities, face forces, corners, incidence
+        // 16-byte boundary: velocities, face forces, corners, face rows
+        // (first entry | count << 24), incidence
         const uint32_t n_face = FACES && p.face_on ? bd.n_face : 0u;
         float4* sv = reinterpret_cast<float4*>((reinterpret_cast<uintptr_t>(sinc + bd.n_inc) + 15u) & ~uintptr_t(15));
         float4* sfd = sv + bd.n_mass;
         uint2* sface = reinterpret_cast<uint2*>(sfd + n_face);
-        uint16_t* sfinc = reinterpret_cast<uint16_t*>(sface + n_face);
+        uint32_t* sfrow = reinterpret_cast<uint32_t*>(sface + n_face);
+        uint16_t* sfinc = reinterpret_cast<uint16_t*>(sfrow + bd.n_mass);
 
         const uint32_t n_mat = *p.n_mat;
         for (uint32_t i = tid; i < bd.n_inc; i += T) sinc[i] = __ldg(&p.inc[bd.inc_begin + i]);
         if (n_face) {
             for (uint32_t i = tid; i < n_face; i += T) sface[i] = __ldg(&p.faces[bd.face_begin + i]);
+            for (uint32_t i = tid; i < bd.n_mass; i += T) sfrow[i] = __ldg(&p.face_row[bd.mass_begin + i]);
             for (uint32_t i = tid; i < bd.n_face_inc; i += T) sfinc[i] = __ldg(&p.face_inc[bd.face_inc_begin + i]);
         }
         if (SPLIT) {
@@ -338,7 +341,7 @@ __global__ void __launch_bounds__(T, 1024 / T) step_kernel(const StepParams p) {
                 } else {
                     // face drag after the springs, faces in ascending order
                     // (the face row: first entry | count << 24)
-                    const uint32_t fr = n_face ? __ldg(&p.face_row[bd.mass_begin + m]) : 0u;
+                    const uint32_t fr = n_face ? sfrow[m] : 0u;
                     const uint16_t* fp = sfinc + (fr & 0xFFFFFFu);
                     for (uint32_t k = 0; k < (fr >> 24); ++k) {
                         const float4 c = sfd[fp[k]];

@@ -178,9 +178,10 @@ void preprocess(const mb_batch_desc* b, uint32_t r, RobotPack& p) {
             return;
         }
         p.n_face = nf;
-        // velocities of every mass of a bin that has faces, alignment, the
-        // faces (force, corners) and their three incidence entries
-        p.face_smem = 16u + 16u * (uint32_t)cm + 30u * nf;
+        // velocities and face rows of every mass of a bin that has faces,
+        // alignment, the faces (force, corners) and their three incidence
+        // entries
+        p.face_smem = 16u + 20u * (uint32_t)cm + 30u * nf;
     }
     p.n_mass = (uint32_t)cm;
     p.cost = (uint64_t)sp.size() * 4 + (uint64_t)cm + 2ull * p.n_face;
