@@ -56,6 +56,23 @@ void Simulator::Reset() { check(ctx_, mb_set_total_time(ctx_, 0.0f), "mb_set_tot
 
 void Simulator::setMode(int mode) { check(ctx_, mb_set_mode(ctx_, (mb_mode)mode), "mb_set_mode"); }
 
+void Simulator::setEnvironment(const Environment& env) {
+    mb_environment e;
+    check(ctx_, mb_get_environment(ctx_, &e), "mb_get_environment");
+    e.g = env.g;
+    e.floor_stiffness = env.floor_stiffness;
+    e.friction_kinetic = env.friction;
+    if (env.type == ENVIRONMENT_WATER) {
+        // the reference's water drag is the density of its face law
+        // (EnvironmentWater.drag = 1000 reaches surfaceDragForce as rho)
+        e.drag = 0.0f;
+        e.face_drag = env.drag;
+    } else {
+        e.face_drag = 0.0f;
+    }
+    check(ctx_, mb_set_environment(ctx_, &e), "mb_set_environment");
+}
+
 ElementTracker Simulator::SetElement(const Element& element) {
     return SetElements(std::vector<Element>{element})[0];
 }
@@ -86,13 +103,21 @@ void Simulator::upload() {
     const size_t R = elements_.size();
     massOff_.assign(1, 0);
     springOff_.assign(1, 0);
+    faceOff_.assign(1, 0);
     massBuf_.clear();
     springBuf_.clear();
+    faces_.clear();
     for (const Element& e : elements_) {
         massBuf_.insert(massBuf_.end(), e.masses.begin(), e.masses.end());
         springBuf_.insert(springBuf_.end(), e.springs.begin(), e.springs.end());
+        for (const Face& f : e.faces) {  // Simulator.cu:310-317
+            faces_.push_back(f.m0);
+            faces_.push_back(f.m1);
+            faces_.push_back(f.m2);
+        }
         massOff_.push_back((int64_t)massBuf_.size());
         springOff_.push_back((int64_t)springBuf_.size());
+        faceOff_.push_back((int64_t)(faces_.size() / 3));
     }
     const size_t M = massBuf_.size(), S = springBuf_.size();
     pos_.assign(4 * M, 0.0f);
@@ -120,8 +145,18 @@ void Simulator::upload() {
         springMat_[s] = sp.material.id;
         lbar_[s] = sp.mean_length;
     }
-    mb_batch_desc d{(uint32_t)R, massOff_.data(), pos_.data(), vel_.data(), massMat_.data(),
-                    springOff_.data(), pairs_.data(), springMat_.data(), lbar_.data()};
+    const bool faces = !faces_.empty();
+    mb_batch_desc d{(uint32_t)R,
+                    massOff_.data(),
+                    pos_.data(),
+                    vel_.data(),
+                    massMat_.data(),
+                    springOff_.data(),
+                    pairs_.data(),
+                    springMat_.data(),
+                    lbar_.data(),
+                    faces ? faceOff_.data() : nullptr,
+                    faces ? faces_.data() : nullptr};
     check(ctx_, mb_set_elements(ctx_, &d), "mb_set_elements");
 }
 

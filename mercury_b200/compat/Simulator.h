@@ -57,11 +57,15 @@ public:
     float getTotalTime() const;
     void Reset();
 
-    // Not in the reference: stresses of a robot's springs after Collect, and
-    // the step semantics (0 = the reference's XPBD step, 1 = force + land,
-    // 2 = force + water; see include/mercury_b200.h).
+    // Not in the reference: stresses of a robot's springs after Collect, the
+    // step semantics (0 = the reference's XPBD step, 1 = force + land,
+    // 2 = force + water; see include/mercury_b200.h), and the environment of
+    // the force modes from the reference's Environment (g, floor stiffness,
+    // friction as the kinetic coefficient; water: drag is the density of
+    // the face drag on the elements' faces).
     std::vector<float> Stresses(const ElementTracker& tracker) const;
     void setMode(int mode);
+    void setEnvironment(const Environment& env);
 
 private:
     void upload();
@@ -73,10 +77,10 @@ private:
     std::vector<Element> elements_;
     std::vector<Mass> massBuf_;
     std::vector<Spring> springBuf_;
-    std::vector<int64_t> massOff_, springOff_;
+    std::vector<int64_t> massOff_, springOff_, faceOff_;
     std::vector<float> pos_, vel_, stress_, lbar_;
     std::vector<uint8_t> massMat_, springMat_;
-    std::vector<uint16_t> pairs_;
+    std::vector<uint16_t> pairs_, faces_;
     uint64_t devoSeed_ = 0;
 };
 
