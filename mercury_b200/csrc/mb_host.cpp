@@ -149,7 +149,7 @@ struct mb_context {
     mb::DevBuf<uint32_t> face_row;
     mb::DevBuf<uint16_t> face_inc;
     uint64_t n_faces = 0;          // faces of the population (three distinct corners)
-    bool faces_packed = false;     // the packed bins hold them (resident or streamed bins, not split)
+    bool faces_packed = false;     // the packed bins hold them
     mb::DevBuf<float4> fd_scratch;  // streamed bins: face forces of a step
     mb::Packed upload_pack;                // host packing of the last mb_set_elements (reused)
     uint32_t cluster = 0;                  // split bins: CTAs per robot (0 = not split)
@@ -294,6 +294,11 @@ mb_status cuda_fail(mb_context* c, cudaError_t e, const char* what) {
 
 namespace mb_detail {
 
+// Whether the step applies the face drag (water mode, rho != 0): split
+// robots are then packed with their faces (velocities exchanged with the
+// positions).
+bool face_drag_on(const mb_context* c) { return c->mode == MB_MODE_FORCE_WATER && c->env.face_drag != 0.0f; }
+
 // Packs a population (caller's arrays or the context's host copy) with the
 // context's device limits and launch override.  With `fallback_auto`, a
 // population that no longer fits the override (after development) is
@@ -306,6 +311,7 @@ mb_status pack(mb_context* ctx, const mb_batch_desc* b, bool fallback_auto, mb::
     po.smem_cap = mb::max_step_smem(ctx->device);
     po.mode = (uint32_t)ctx->mode;
     po.override = ctx->override_cfg;
+    po.split_faces = face_drag_on(ctx);
     if (!allow_split) po.override.cluster = 1;
     po.ctas_per_sm = [ctx](const mb::KernelShape& sh, uint32_t smem) {
         return mb::ctas_per_sm(sh, (uint32_t)ctx->mode, false, smem);
@@ -504,13 +510,9 @@ mb_status devo_setup(mb_context* c) {
     return MB_OK;
 }
 
-// Whether the step applies the face drag (water mode, rho != 0): robots
-// with faces are then not split over clusters (split bins carry no faces).
-bool face_drag_on(const mb_context* c) { return c->mode == MB_MODE_FORCE_WATER && c->env.face_drag != 0.0f; }
-
 // Host re-packing of the context's topology copy: the fallback of
-// development (`devo`), or a re-plan without split robots when the face
-// drag is switched on for a split population.
+// development (`devo`), or a re-plan with the faces in the split parts when
+// the face drag is switched on for a split population.
 mb_status host_repack(mb_context* c, bool devo = true) {
     // split robots are cut by their current positions
     std::vector<float> pos;
@@ -533,7 +535,7 @@ mb_status host_repack(mb_context* c, bool devo = true) {
                           faces ? c->h_face_off.data() : nullptr,
                           faces ? c->h_faces.data() : nullptr};
     mb::Packed out;
-    mb_status st = pack(c, &d, true, out, !(faces && face_drag_on(c)));
+    mb_status st = pack(c, &d, true, out, true);
     if (st == MB_OK) st = upload_packed(c, out);
     if (st != MB_OK) c->loaded = false;  // topology and packed arrays disagree now
     c->vox.valid = false;
@@ -927,8 +929,7 @@ mb_status mb_set_elements(mb_context* ctx, const mb_batch_desc* b) {
     mb::Packed& out = ctx->upload_pack;
     const char* host_rows = std::getenv("MB_HOST_ROWS");
     const bool device_rows = !(host_rows && host_rows[0] == '1');
-    const bool allow_split = !(F && mb_detail::face_drag_on(ctx));
-    const mb_status pst = mb_detail::pack(ctx, b, false, out, allow_split, device_rows);
+    const mb_status pst = mb_detail::pack(ctx, b, false, out, true, device_rows);
     copier.join();
     if (pst != MB_OK) return pst;
 
@@ -970,7 +971,7 @@ mb_status mb_set_elements(mb_context* ctx, const mb_batch_desc* b) {
     mb_status ust = mb_detail::upload_packed(ctx, out, &rows_failed);
     if (ust == MB_OK && rows_failed) {  // rare: the host builds the rows
         MB_TRACE("device rows did not fit; host rows");
-        ust = mb_detail::pack(ctx, b, false, out, allow_split, false);
+        ust = mb_detail::pack(ctx, b, false, out, true, false);
         if (ust == MB_OK) ust = mb_detail::upload_packed(ctx, out);
     }
     if (ust != MB_OK) return ust;
@@ -1099,7 +1100,7 @@ mb_status run(mb_context* c, uint32_t steps, bool track) {
     if (!c->loaded) return fail(c, MB_ERR_STATE, "no population uploaded");
     if (steps == 0) return MB_OK;
     if (face_drag_on(c) && c->n_faces && !c->faces_packed) {
-        // split robots carry no faces: re-plan them streamed (once)
+        // split robots packed without their faces: re-plan them with (once)
         const mb_status rs = host_repack(c, false);
         if (rs != MB_OK) return rs;
         if (!c->faces_packed) return fail(c, MB_ERR_CAPACITY, "face drag: the faces do not fit the step kernels");

@@ -171,6 +171,15 @@ __host__ __device__ inline uint32_t split_smem_bytes(uint32_t x_stride, uint32_t
            2u * n_inc;
 }
 
+// Split bins with the face layout (the face drag on a split population):
+// two velocity buffers of x_stride slots after the position buffers, and
+// after the rows (16-byte aligned) the face forces and corners, the face
+// rows of the own masses and the incidence entries.
+__host__ __device__ inline uint32_t split_face_smem_bytes(uint32_t x_stride, uint32_t n_own, uint32_t n_face,
+                                                          uint32_t n_face_inc) {
+    return 32u * x_stride + 16u + 24u * n_face + 4u * n_own + 2u * n_face_inc;
+}
+
 // Largest dynamic shared memory the step kernel may use on this device.
 uint32_t max_step_smem(int device);
 

@@ -154,7 +154,7 @@ __device__ __forceinline__ float4 face_force(const float4 x0, const float4 x1, c
 template <int T, int SPT, int MPT, int MODE, bool TRACK, bool SPLIT>
 __global__ void __launch_bounds__(T, 1024 / T) step_kernel(const StepParams p) {
     constexpr bool XPBD = MODE == kModeXpbd;
-    constexpr bool FACES = MODE == kModeForceWaterFaces && !SPLIT;  // face drag compiled in
+    constexpr bool FACES = MODE == kModeForceWaterFaces;  // face drag compiled in
     extern __shared__ float4 smem4[];
     const int tid = threadIdx.x;
     const float dt = p.dt;
@@ -165,21 +165,24 @@ __global__ void __launch_bounds__(T, 1024 / T) step_kernel(const StepParams p) {
     for (uint32_t b = blockIdx.x; b < p.n_bins; b += gridDim.x) {
         const BinDesc bd = p.bins[b];
         // predicted positions x~, one float4 per mass (split bins: two
-        // buffers, own masses then halo, alternating by step)
+        // buffers, own masses then halo, alternating by step; with faces,
+        // two velocity buffers of the same shape follow)
         float4* sxt = smem4;
-        float4* sdp = sxt + (SPLIT ? 2u * bd.x_stride : bd.n_mass);  // corrections dp, one float4 per spring
+        float4* sdp = sxt + (SPLIT ? (FACES ? 4u : 2u) * bd.x_stride : bd.n_mass);  // corrections dp, one float4 per spring
         float2* smat = reinterpret_cast<float2*>(sdp + bd.n_spring);  // {dL0 sin(..), 1/K} per slot
         // split bins: the buffer stride of every part of the cluster, then
         // the export list
         uint32_t* sstride = reinterpret_cast<uint32_t*>(smat + kMaxMaterialSlots);
         uint32_t* sexp = sstride + (SPLIT ? kMaxClusterParts : 0u);
         uint16_t* sinc = reinterpret_cast<uint16_t*>(sexp + (SPLIT ? bd.n_export : 0u));
-        // face drag (water, resident bins with faces), after the rows at a
-        // 16-byte boundary: velocities, face forces, corners, face rows
-        // (first entry | count << 24), incidence
+        // face drag (water, bins with faces), after the rows at a 16-byte
+        // boundary: velocities (resident bins; split bins keep them after
+        // the positions), face forces, corners, face rows (first entry |
+        // count << 24), incidence
         const uint32_t n_face = FACES && p.face_on ? bd.n_face : 0u;
         float4* sv = reinterpret_cast<float4*>((reinterpret_cast<uintptr_t>(sinc + bd.n_inc) + 15u) & ~uintptr_t(15));
-        float4* sfd = sv + bd.n_mass;
+        float4* sfd = SPLIT ? sv : sv + bd.n_mass;
+        if (SPLIT) sv = sxt + 2u * bd.x_stride;
         uint2* sface = reinterpret_cast<uint2*>(sfd + n_face);
         uint32_t* sfrow = reinterpret_cast<uint32_t*>(sface + n_face);
         uint16_t* sfinc = reinterpret_cast<uint16_t*>(sfrow + bd.n_mass);
@@ -246,6 +249,7 @@ __global__ void __launch_bounds__(T, 1024 / T) step_kernel(const StepParams p) {
 
         for (uint32_t step = 0; step < p.steps; ++step) {
             float4* X = SPLIT ? sxt + (step & 1u) * bd.x_stride : sxt;
+            float4* V = SPLIT ? sv + (step & 1u) * bd.x_stride : sv;  // velocities (face drag)
             // (1) actuation factors of this step (sim_kernel.cu:222), loaded one
             // step ahead from the launch's table
             if (tid < n_mat) {
@@ -264,7 +268,9 @@ __global__ void __launch_bounds__(T, 1024 / T) step_kernel(const StepParams p) {
                                        __fadd_rn(x[j].z, __fmul_rn(v[j].z, dt)), 0.0f);
                 else
                     X[m] = make_float4(x[j].x, x[j].y, x[j].z, 0.0f);
-                if (n_face) sv[m] = make_float4(v[j].x, v[j].y, v[j].z, 0.0f);
+                // split bins publish every velocity: other parts' faces may
+                // have corners here
+                if (FACES && (SPLIT || n_face)) V[m] = make_float4(v[j].x, v[j].y, v[j].z, 0.0f);
             }
             __syncthreads();
             if (SPLIT) {
@@ -277,6 +283,7 @@ __global__ void __launch_bounds__(T, 1024 / T) step_kernel(const StepParams p) {
                     const uint32_t ex = sexp[i], q = (ex >> 12) & 7u;
                     float4* dst = cl.map_shared_rank(sxt, q) + (step & 1u) * sstride[q];
                     dst[ex >> 15] = X[ex & 0xFFFu];
+                    if (FACES) dst[2u * sstride[q] + (ex >> 15)] = V[ex & 0xFFFu];  // the velocity buffer
                 }
                 cl.sync();
             }
@@ -305,7 +312,7 @@ __global__ void __launch_bounds__(T, 1024 / T) step_kernel(const StepParams p) {
             for (uint32_t f = tid; f < n_face; f += T) {
                 const uint2 c = sface[f];
                 const uint32_t i0 = c.x & 0xFFFFu, i1 = c.x >> 16, i2 = c.y;
-                sfd[f] = face_force(X[i0], X[i1], X[i2], sv[i0], sv[i1], sv[i2], p.face_coef);
+                sfd[f] = face_force(X[i0], X[i1], X[i2], V[i0], V[i1], V[i2], p.face_coef);
             }
             __syncthreads();
             // (3) gather in summation order and integrate (sim_kernel.cu:246-268).
@@ -658,8 +665,8 @@ struct ShapeEntry {
                  step_kernel<T, S, M, kModeForceLand, true, SPLIT>},                           \
                 {step_kernel<T, S, M, kModeForceWater, false, SPLIT>,                          \
                  step_kernel<T, S, M, kModeForceWater, true, SPLIT>},                          \
-                {step_kernel<T, S, M, SPLIT ? kModeForceWater : kModeForceWaterFaces, false, SPLIT>, \
-                 step_kernel<T, S, M, SPLIT ? kModeForceWater : kModeForceWaterFaces, true, SPLIT>},  \
+                {step_kernel<T, S, M, kModeForceWaterFaces, false, SPLIT>,                     \
+                 step_kernel<T, S, M, kModeForceWaterFaces, true, SPLIT>},                     \
         }                                                                                      \
     }
 const ShapeEntry kShapes[] = {
@@ -733,8 +740,12 @@ bool split_supported(const KernelShape& shape) { return find_split(shape) != nul
 cudaError_t prepare_split(const KernelShape& shape, uint32_t mode, bool track, uint32_t smem_bytes) {
     const ShapeEntry* e = find_split(shape);
     if (!e || mode > kModeForceWater) return cudaErrorInvalidValue;
-    return cudaFuncSetAttribute(e->fn[mode][track ? 1 : 0], cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)smem_bytes);
+    cudaError_t r = cudaFuncSetAttribute(e->fn[mode][track ? 1 : 0], cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem_bytes);
+    if (r == cudaSuccess && mode == kModeForceWater)  // and the face-drag variant
+        r = cudaFuncSetAttribute(e->fn[kModeForceWaterFaces][track ? 1 : 0],
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_bytes);
+    return r;
 }
 
 // One CTA per part, the parts of a robot (bins r*C .. r*C + C-1) forming a
@@ -756,7 +767,8 @@ cudaError_t launch_split(const StepParams& p, const KernelShape& shape, uint32_t
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, e->fn[p.mode][p.track ? 1 : 0], p);
+    const uint32_t variant = p.mode == kModeForceWater && p.face_on ? kModeForceWaterFaces : p.mode;
+    return cudaLaunchKernelEx(&cfg, e->fn[variant][p.track ? 1 : 0], p);
 }
 
 cudaError_t prepare_step(const KernelShape& shape, uint32_t mode, bool track, uint32_t smem_bytes) {

@@ -697,8 +697,8 @@ struct PartMasses {
 };
 
 void build_part(const mb_batch_desc* b, uint32_t r, const RobotPack& pk, const std::vector<uint8_t>& part_of,
-                uint32_t p, const std::vector<int>& slot_of, std::vector<int32_t>& local_of, BinLocal& L,
-                PartMasses& pm) {
+                uint32_t p, const std::vector<int>& slot_of, bool faces, std::vector<int32_t>& local_of,
+                BinLocal& L, PartMasses& pm) {
     const int64_t m0 = b->mass_offsets[r], s0 = b->spring_offsets[r];
     const uint32_t n = pk.n_mass;
     pm.own.clear();
@@ -719,9 +719,45 @@ void build_part(const mb_batch_desc* b, uint32_t r, const RobotPack& pk, const s
         if (part_of[a] != p) pm.halo.push_back(a);
         if (part_of[c] != p) pm.halo.push_back(c);
     }
+    // faces with a corner in the part (robot face order); their other
+    // corners join the halo
+    std::vector<uint32_t> fl;
+    const int64_t f0 = faces && pk.n_face ? b->face_offsets[r] : 0;
+    const int64_t f1 = faces && pk.n_face ? b->face_offsets[r + 1] : 0;
+    for (int64_t f = f0; f < f1; ++f) {
+        const uint16_t* c = b->faces + 3 * f;
+        if (c[0] == c[1] || c[0] == c[2] || c[1] == c[2]) continue;
+        if (part_of[c[0]] != p && part_of[c[1]] != p && part_of[c[2]] != p) continue;
+        fl.push_back((uint32_t)f);
+        for (int k = 0; k < 3; ++k)
+            if (part_of[c[k]] != p) pm.halo.push_back(c[k]);
+    }
     std::sort(pm.halo.begin(), pm.halo.end());
     pm.halo.erase(std::unique(pm.halo.begin(), pm.halo.end()), pm.halo.end());
     for (uint32_t j = 0; j < pm.halo.size(); ++j) local_of[pm.halo[j]] = (int32_t)(n_own + j);
+    if (!fl.empty()) {
+        // part-local corners; rows (ascending face order) for own masses
+        std::vector<uint32_t> start(n_own + 1, 0);
+        L.faces.reserve(2 * fl.size());
+        for (uint32_t f : fl) {
+            const uint16_t* c = b->faces + 3 * f;
+            L.faces.push_back((uint32_t)local_of[c[0]] | ((uint32_t)local_of[c[1]] << 16));
+            L.faces.push_back((uint32_t)local_of[c[2]]);
+            for (int k = 0; k < 3; ++k)
+                if (part_of[c[k]] == p) start[(uint32_t)local_of[c[k]] + 1]++;
+        }
+        for (uint32_t i = 0; i < n_own; ++i) start[i + 1] += start[i];
+        L.face_inc.resize(start[n_own]);
+        L.face_row.resize(n_own);
+        std::vector<uint32_t> ffill(start.begin(), start.end() - 1);
+        for (uint32_t q = 0; q < fl.size(); ++q) {
+            const uint16_t* c = b->faces + 3 * fl[q];
+            for (int k = 0; k < 3; ++k)
+                if (part_of[c[k]] == p) L.face_inc[ffill[(uint32_t)local_of[c[k]]]++] = (uint16_t)q;
+        }
+        for (uint32_t i = 0; i < n_own; ++i) L.face_row[i] = start[i] | ((start[i + 1] - start[i]) << 24);
+        L.n_face = (uint32_t)fl.size();
+    }
     L.mass_gidx.reserve(n_own);
     for (uint32_t m : pm.own) L.mass_gidx.push_back((uint32_t)(m0 + m));
     const uint32_t ns = (uint32_t)sp.size();
@@ -769,6 +805,7 @@ void build_part(const mb_batch_desc* b, uint32_t r, const RobotPack& pk, const s
 // predicted-position buffers hold its own and halo masses (n_all).
 struct SplitParts {
     uint32_t C = 0;
+    bool faces = false;  // the face layout (split_face_smem_bytes) in every part
     // second group (robots of at most two parts in two-CTA clusters, after
     // bin bins0), launched beside the first: 0 = one group
     uint32_t C2 = 0, bins0 = 0;
@@ -784,7 +821,7 @@ struct SplitParts {
 // as its longest row in the rank layout and at most 4 columns wider when
 // aligned, so `upper` makes the check sufficient, otherwise necessary.
 bool robot_parts_fit(const mb_batch_desc* b, const RobotPack& pk, uint32_t r, uint32_t P, uint64_t cap_s,
-                     uint64_t cap_m, uint32_t smem_cap, bool upper, std::vector<uint8_t>& part_of,
+                     uint64_t cap_m, uint32_t smem_cap, bool upper, bool faces, std::vector<uint8_t>& part_of,
                      std::string* reason) {
     uint32_t levels = 0;
     while ((1u << levels) < P) ++levels;
@@ -808,6 +845,27 @@ bool robot_parts_fit(const mb_batch_desc* b, const RobotPack& pk, uint32_t r, ui
             if (!(mark[a] & (1u << pc))) { mark[a] |= 1u << pc; halo[pc]++; }
         }
     }
+    // faces (face layout): counted in every part owning a corner, their
+    // other corners in its halo
+    std::vector<uint32_t> nf(P, 0), nfi(P, 0);
+    if (faces && pk.n_face)
+        for (int64_t f = b->face_offsets[r]; f < b->face_offsets[r + 1]; ++f) {
+            const uint16_t* c = b->faces + 3 * f;
+            if (c[0] == c[1] || c[0] == c[2] || c[1] == c[2]) continue;
+            const uint32_t in = (1u << po[c[0]]) | (1u << po[c[1]]) | (1u << po[c[2]]);
+            for (uint32_t p = 0; p < P; ++p) {
+                if (!(in & (1u << p))) continue;
+                nf[p]++;
+                for (int k = 0; k < 3; ++k) {
+                    if (po[c[k]] == p)
+                        nfi[p]++;
+                    else if (!(mark[c[k]] & (1u << p))) {
+                        mark[c[k]] |= 1u << p;
+                        halo[p]++;
+                    }
+                }
+            }
+        }
     // rows: slices of 32 own masses (see above); exports: one per halo copy
     const uint32_t widen = upper ? 4u : 0u;
     std::vector<uint32_t> rows(P, 0), in_slice(P, 0), slice_max(P, 0);
@@ -823,7 +881,8 @@ bool robot_parts_fit(const mb_batch_desc* b, const RobotPack& pk, uint32_t r, ui
     for (uint32_t p = 0; p < P; ++p)
         if (in_slice[p]) rows[p] += kSliceWidth * (slice_max[p] + widen);
     for (uint32_t p = 0; p < P; ++p) {
-        const uint64_t smem_lb = split_smem_bytes(own[p] + halo[p], ns[p], 0, exp[p]) + 2ull * rows[p];
+        const uint64_t smem_lb = split_smem_bytes(own[p] + halo[p], ns[p], 0, exp[p]) + 2ull * rows[p] +
+                                 (faces ? split_face_smem_bytes(own[p] + halo[p], own[p], nf[p], nfi[p]) : 0u);
         if (ns[p] > cap_s || own[p] > cap_m || own[p] + halo[p] > 4096 || smem_lb > smem_cap) {
             if (reason) {
                 char buf[256];
@@ -850,7 +909,7 @@ void split_caps(const std::vector<KernelShape>& shapes, uint64_t& cap_s, uint64_
 // Every robot cut into C parts (one cluster each), checked from counts
 // before any rows are built; false with the reason otherwise.
 bool split_partition(const mb_batch_desc* b, const std::vector<RobotPack>& packs, uint32_t C,
-                     const std::vector<KernelShape>& shapes, uint32_t smem_cap, unsigned threads,
+                     const std::vector<KernelShape>& shapes, uint32_t smem_cap, bool faces, unsigned threads,
                      std::vector<std::vector<uint8_t>>& part_of, std::string& why) {
     const uint32_t R = (uint32_t)packs.size();
     uint64_t cap_s, cap_m;
@@ -860,7 +919,7 @@ bool split_partition(const mb_batch_desc* b, const std::vector<RobotPack>& packs
     std::vector<std::string> reason(R);
     parallel_for(R, threads, [&](uint32_t r) {
         if (!fits.load(std::memory_order_relaxed)) return;
-        if (!robot_parts_fit(b, packs[r], r, C, cap_s, cap_m, smem_cap, false, part_of[r], &reason[r]))
+        if (!robot_parts_fit(b, packs[r], r, C, cap_s, cap_m, smem_cap, false, faces, part_of[r], &reason[r]))
             fits = false;
     });
     if (!fits) {
@@ -877,8 +936,8 @@ bool split_partition(const mb_batch_desc* b, const std::vector<RobotPack>& packs
 // Each robot at its fewest parts (1, 2, 4 or 8) that surely fit `shape`
 // (the sufficient check); false if some robot needs more than 8.
 bool split_partition_mixed(const mb_batch_desc* b, const std::vector<RobotPack>& packs, const KernelShape& shape,
-                           uint32_t smem_cap, unsigned threads, std::vector<std::vector<uint8_t>>& part_of,
-                           std::vector<uint32_t>& parts) {
+                           uint32_t smem_cap, bool faces, unsigned threads,
+                           std::vector<std::vector<uint8_t>>& part_of, std::vector<uint32_t>& parts) {
     const uint32_t R = (uint32_t)packs.size();
     uint64_t cap_s, cap_m;
     split_caps({shape}, cap_s, cap_m);
@@ -888,7 +947,7 @@ bool split_partition_mixed(const mb_batch_desc* b, const std::vector<RobotPack>&
     parallel_for(R, threads, [&](uint32_t r) {
         if (!fits.load(std::memory_order_relaxed)) return;
         for (uint32_t P = 1; P <= 8; P *= 2)
-            if (robot_parts_fit(b, packs[r], r, P, cap_s, cap_m, smem_cap, true, part_of[r], nullptr)) {
+            if (robot_parts_fit(b, packs[r], r, P, cap_s, cap_m, smem_cap, true, faces, part_of[r], nullptr)) {
                 parts[r] = P;
                 return;
             }
@@ -952,7 +1011,7 @@ void build_split_parts(const mb_batch_desc* b, const std::vector<RobotPack>& pac
         std::vector<PartMasses> pm(P);
         std::vector<int32_t> local_of;
         for (uint32_t p = 0; p < P; ++p) {
-            build_part(b, r, packs[r], part_of[r], p, slot_of, local_of, sp.locals[base + p], pm[p]);
+            build_part(b, r, packs[r], part_of[r], p, slot_of, sp.faces, local_of, sp.locals[base + p], pm[p]);
             sp.n_all[base + p] = (uint32_t)(pm[p].own.size() + pm[p].halo.size());
         }
         // export entries name the destination by its rank in the cluster
@@ -969,12 +1028,19 @@ void build_split_parts(const mb_batch_desc* b, const std::vector<RobotPack>& pac
 }
 
 // Whether every part fits the shape and the shared memory; the reason if not.
+// Shared memory of split bin i.
+uint32_t split_bin_smem(const SplitParts& sp, uint32_t i) {
+    const BinLocal& L = sp.locals[i];
+    return split_smem_bytes(sp.n_all[i], L.n_spring, L.n_inc, (uint32_t)sp.exports[i].size()) +
+           (sp.faces ? split_face_smem_bytes(sp.n_all[i], L.n_mass, L.n_face, (uint32_t)L.face_inc.size()) : 0u);
+}
+
 bool split_fits(const SplitParts& sp, const KernelShape& sh, uint32_t smem_cap, std::string& why) {
     const uint64_t cap_s = std::min<uint64_t>((uint64_t)sh.threads * sh.spt, kMaxBinSprings);
     const uint64_t cap_m = std::min<uint64_t>((uint64_t)sh.threads * sh.mpt, 4096);
     for (uint32_t i = 0; i < sp.locals.size(); ++i) {
         const BinLocal& L = sp.locals[i];
-        const uint32_t smem = split_smem_bytes(sp.n_all[i], L.n_spring, L.n_inc, (uint32_t)sp.exports[i].size());
+        const uint32_t smem = split_bin_smem(sp, i);
         if (L.n_spring > cap_s || L.n_mass > cap_m || sp.n_all[i] > 4096 || smem > smem_cap) {
             char buf[256];
             std::snprintf(buf, sizeof(buf), "part in bin %u: %u springs, %u + %u masses, %u B shared memory", i,
@@ -1002,7 +1068,7 @@ void assemble_split(const SplitParts& sp, uint32_t R, unsigned threads, Packed& 
         d.n_export = (uint32_t)sp.exports[i].size();
         d.n_all = sp.n_all[i];
         out.exports.insert(out.exports.end(), sp.exports[i].begin(), sp.exports[i].end());
-        out.max_smem = std::max(out.max_smem, split_smem_bytes(d.x_stride, d.n_spring, d.n_inc, d.n_export));
+        out.max_smem = std::max(out.max_smem, split_bin_smem(sp, i));
     }
 }
 
@@ -1117,6 +1183,7 @@ mb_status pack_population(const mb_batch_desc* b, const PackOptions& o, Packed& 
     // Split over a cluster: when forced, or when no resident shape holds the
     // largest robot -- the fewest parts whose every part fits a shape.
     std::string why;
+    const bool split_faces = o.split_faces && out.n_faces > 0;
     if (!ok && !o.override.streamed && force_c != 1) {
         std::vector<uint32_t> cs;
         if (force_c > 1)
@@ -1136,8 +1203,7 @@ mb_status pack_population(const mb_batch_desc* b, const PackOptions& o, Packed& 
             if (!o.cluster_fits) return true;
             uint32_t smem = 0;
             for (uint32_t i = 0; i < sp.locals.size(); ++i)
-                smem = std::max(smem, split_smem_bytes(sp.n_all[i], sp.locals[i].n_spring, sp.locals[i].n_inc,
-                                                       (uint32_t)sp.exports[i].size()));
+                smem = std::max(smem, split_bin_smem(sp, i));
             if (o.cluster_fits(sh, sp.C, smem)) return true;
             why = "clusters of " + std::to_string(sp.C) + " CTAs cannot be scheduled on this device";
             return false;
@@ -1158,7 +1224,9 @@ mb_status pack_population(const mb_batch_desc* b, const PackOptions& o, Packed& 
             for (const auto& sh : compiled) {
                 std::vector<std::vector<uint8_t>> part_of;
                 SplitParts sp;
-                if (!split_partition_mixed(b, packs, sh, o.smem_cap, threads, part_of, sp.parts)) continue;
+                sp.faces = split_faces;
+                if (!split_partition_mixed(b, packs, sh, o.smem_cap, split_faces, threads, part_of, sp.parts))
+                    continue;
                 sp.C = *std::max_element(sp.parts.begin(), sp.parts.end());
                 if (sp.C < 2) continue;  // every robot fits a CTA alone: not a split population
                 const uint32_t nb = place_split(sp);
@@ -1171,9 +1239,10 @@ mb_status pack_population(const mb_batch_desc* b, const PackOptions& o, Packed& 
         for (uint32_t C : cs) {
             if (ok || compiled.empty()) break;
             std::vector<std::vector<uint8_t>> part_of;
-            if (!split_partition(b, packs, C, compiled, o.smem_cap, threads, part_of, why)) continue;
+            if (!split_partition(b, packs, C, compiled, o.smem_cap, split_faces, threads, part_of, why)) continue;
             SplitParts sp;
             sp.C = C;
+            sp.faces = split_faces;
             sp.parts.assign(R, C);
             sp.first.resize(R);
             sp.slot0.assign(R, 0);

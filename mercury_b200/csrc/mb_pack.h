@@ -51,6 +51,10 @@ struct PackOptions {
     // resident bins only: lay out springs and masses, leave the rows to the
     // device (bins[b].row_cap entries reserved per bin)
     bool rows_on_device = false;
+    // split robots carry their faces (the face drag is on): velocities are
+    // exchanged with the positions and each part computes the faces that
+    // touch its own masses
+    bool split_faces = false;
 };
 
 struct Packed {

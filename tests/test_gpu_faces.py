@@ -123,7 +123,27 @@ def test_streamed_bins_bit_exact(track):
     same(sim, oracle(b, S.WATER_FACES, 300, track), track)
 
 
-def test_split_population_is_replanned_streamed_for_face_drag():
+@pytest.mark.parametrize("track", [False, True])
+@pytest.mark.parametrize("cfg", [None, {"chunk": 97, "use_graph": 0}], ids=["graph", "chunks"])
+def test_split_point_clouds_bit_exact(track, cfg):
+    """Point clouds too large for one CTA, with their convex hulls: split
+    over clusters, velocities exchanged with the positions, faces across a
+    cut computed in every part that holds one of their corners."""
+    b = moving(mb.pack(robots.population("nn", 6, mass=0.1, faces=True)), 9)
+    sim = gpu(b, S.WATER_FACES, 200, track, cfg)
+    assert sim.launch_config()["cluster"] > 0
+    same(sim, oracle(b, S.WATER_FACES, 200, track), track)
+
+
+@pytest.mark.parametrize("cluster", [2, 4, 8])
+def test_forced_split_with_faces_bit_exact(cluster):
+    b = moving(robots.population_batch("uneven", 8, mass=0.1, faces=True), 10)
+    sim = gpu(b, S.WATER_FACES, 200, True, {"cluster": cluster})
+    assert sim.launch_config()["cluster"] == cluster
+    same(sim, oracle(b, S.WATER_FACES, 200, True))
+
+
+def test_face_drag_switched_on_for_a_split_population():
     b = moving(mb.pack(robots.population("nn", 2, mass=0.1, faces=True)), 8)
     sim = mb.Simulator(0)
     sim.set_materials(mb.materials.force_table())
@@ -131,16 +151,12 @@ def test_split_population_is_replanned_streamed_for_face_drag():
     sim.set_environment(**dict(S.WATER_FACES, face_drag=0.0))
     sim.setTimeStep(1e-4)
     sim.set_batch(b)
-    assert sim.launch_config()["cluster"] > 0  # no face drag: split over clusters
+    assert sim.launch_config()["cluster"] > 0
     sim.run_steps(100, True)
     ref = oracle(b, dict(S.WATER_FACES, face_drag=0.0), 100, True)
     same(sim, ref)
     t = sim.getTotalTime()
     sim.set_environment(face_drag=S.WATER_FACES["face_drag"])
-    sim.run_steps(200, True)  # re-planned without clusters, state kept
-    cfg = sim.launch_config()
-    assert cfg["cluster"] == 0 and cfg["streamed"] == 1
+    sim.run_steps(200, True)  # re-packed with the faces in the parts, state kept
+    assert sim.launch_config()["cluster"] > 0
     same(sim, oracle(b, S.WATER_FACES, 200, True, state=ref, t0=t))
-    # uploading while the face drag is on plans no split at all
-    sim.set_batch(b)
-    assert sim.launch_config()["cluster"] == 0
