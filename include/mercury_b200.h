@@ -158,7 +158,10 @@ MB_API mb_status mb_get_mode(const mb_context* ctx, mb_mode* mode);
 
 /* Environment of the force modes; the default is land with g = 9.81,
  * floor_stiffness = 1e6 (environment.h:15-22), friction 1.0 / 0.8, drag 0.05,
- * damping 0.999.  Replaces Simulator::_initialize's environment choice
+ * damping 0.999, face_drag 0.  A population whose robots carry faces is
+ * packed with them when the face drag is on (water, face_drag != 0); one
+ * packed while it was off is re-packed at the next mb_simulate after it is
+ * switched on.  Replaces Simulator::_initialize's environment choice
  * (Simulator.cu:191-196). */
 MB_API mb_status mb_set_environment(mb_context* ctx, const mb_environment* env);
 MB_API mb_status mb_get_environment(const mb_context* ctx, mb_environment* env);
