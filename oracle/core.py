@@ -46,6 +46,8 @@ def lib() -> ctypes.CDLL:
         L.or_force_run.restype = I32
         L.or_face_force.argtypes = [P, P, P, P, P, P, F32, P]
         L.or_face_force.restype = None
+        L.or_face_forces.argtypes = [I32, P, P, I32, P, F32, P]
+        L.or_face_forces.restype = None
         L.or_force_run_f64.argtypes = [I32, I32, P, P, P, P, P, P, P, P, P, F64, F64, U32]
         L.or_force_run_f64.restype = I32
         U64 = ctypes.c_uint64
@@ -152,6 +154,17 @@ def face_force(x, v, coef):
     v = np.ascontiguousarray(v, np.float32).reshape(3, 3)
     out = np.zeros(3, np.float32)
     lib().or_face_force(_p(x[0]), _p(x[1]), _p(x[2]), _p(v[0]), _p(v[1]), _p(v[2]), np.float32(coef), _p(out))
+    return out
+
+
+def face_forces(pos4, vel4, faces, coef):
+    """Per-mass sums of the face shares of one robot (faces ascending):
+    pos4, vel4 (M, 4) float32, faces (F, 3) uint16.  Returns (M, 3)."""
+    pos4 = np.ascontiguousarray(pos4, np.float32)
+    vel4 = np.ascontiguousarray(vel4, np.float32)
+    faces = np.ascontiguousarray(faces, np.uint16)
+    out = np.zeros((len(pos4), 3), np.float32)
+    lib().or_face_forces(len(pos4), _p(pos4), _p(vel4), len(faces), _p(faces), np.float32(coef), _p(out))
     return out
 
 

@@ -578,6 +578,23 @@ void or_face_force(const float* x0, const float* x1, const float* x2, const floa
     face_force_f32(x0, x1, x2, v0, v1, v2, coef, out);
 }
 
+/* Face forces of one robot: per mass the sum of the shares of its faces
+ * (three distinct corners), faces in ascending order -- the term the water
+ * step adds after the springs.  out: 3 per mass. */
+void or_face_forces(int n_mass, const float* pos4, const float* vel4, int n_face, const uint16_t* faces3,
+                    float coef, float* out) {
+    memset(out, 0, sizeof(float) * 3 * (size_t)n_mass);
+    for (int f = 0; f < n_face; ++f) {
+        const uint16_t* c = faces3 + 3 * f;
+        if (c[0] == c[1] || c[0] == c[2] || c[1] == c[2]) continue;
+        float F[3];
+        face_force_f32(pos4 + 4 * c[0], pos4 + 4 * c[1], pos4 + 4 * c[2], vel4 + 4 * c[0], vel4 + 4 * c[1],
+                       vel4 + 4 * c[2], coef, F);
+        for (int k = 0; k < 3; ++k)
+            for (int q = 0; q < 3; ++q) out[3 * c[k] + q] = out[3 * c[k] + q] + F[q];
+    }
+}
+
 /* face_off / faces may be NULL (no faces); with faces, env has 7 entries. */
 int or_force_run(int mode, int n_robots, const int64_t* mass_off, float* pos, float* vel,
                  const int64_t* spring_off, const uint16_t* pairs, const uint8_t* mat,
