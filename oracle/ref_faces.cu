@@ -7,6 +7,12 @@
 // The kernel writes x + v dt + F dt^2 for every mass (F = the sum of the
 // shares of its faces, accumulated with shared-memory atomics); with dt = 1
 // and a large density the caller reads F back as newPos - x - v.
+//
+// It is launched with one warp: the kernel has no barrier between loading
+// the masses into shared memory, accumulating the faces and writing back
+// (sim_kernel.cu:82-131), so with several warps a warp reads corners another
+// has not loaded yet, or its shares are zeroed by the owner's late load
+// (measured here: whole shares lost at 256 threads).
 #include "sim_kernel.cu"
 
 #include <cstdint>
@@ -44,7 +50,7 @@ extern "C" int ref_surface_drag(int n_mass, const float* pos4, const float* vel4
     if (e == cudaSuccess) e = cudaMemcpy(d_new, pos4, mb, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(d_faces, f4.data(), sizeof(ushort4) * (size_t)n_face, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) {
-        surfaceDragForce<<<1, 256, 36 * (size_t)n_mass>>>(d_pos, d_new, d_vel, d_faces);
+        surfaceDragForce<<<1, 32, 36 * (size_t)n_mass>>>(d_pos, d_new, d_vel, d_faces);
         e = cudaDeviceSynchronize();
     }
     if (e == cudaSuccess) e = cudaMemcpy(new_pos4, d_new, mb, cudaMemcpyDeviceToHost);
