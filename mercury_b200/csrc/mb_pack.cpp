@@ -314,7 +314,7 @@ inline bool ent_less(const Ent& x, const Ent& y) {
 }
 
 // Every row in summation order: (other end, spring index, a end first).
-void sort_rows(uint32_t nm, const std::vector<uint32_t>& row_start, std::vector<Ent>& ents) {
+void sort_rows(uint32_t nm, const std::vector<uint32_t>& row_start, raw_vector<Ent>& ents) {
     for (uint32_t i = 0; i < nm; ++i) {
         Ent* first = ents.data() + row_start[i];
         Ent* last = ents.data() + row_start[i + 1];
@@ -336,7 +336,7 @@ void sort_rows(uint32_t nm, const std::vector<uint32_t>& row_start, std::vector<
 
 // SELL-32 rows of masses 0..nm-1 from their sorted entries (row_start:
 // CSR offsets into ents); fills L's slices and incidence arrays.
-void slice_rows(uint32_t nm, const std::vector<uint32_t>& row_start, const std::vector<Ent>& ents,
+void slice_rows(uint32_t nm, const std::vector<uint32_t>& row_start, const raw_vector<Ent>& ents,
                 bool streamed, BinLocal& L) {
     // SELL-32: columns aligned by the offset of the other end (other - i)
     // when every row of the slice has distinct offsets -- then the k-th
@@ -495,7 +495,7 @@ void build_bin(const mb_batch_desc* b, const std::vector<RobotPack>& packs,
         return;
     }
     for (uint32_t i = 0; i < nm; ++i) row_start[i + 1] += row_start[i];
-    std::vector<Ent> ents(row_start[nm]);
+    raw_vector<Ent> ents(row_start[nm]);
     std::vector<uint32_t> fill(row_start.begin(), row_start.end() - 1);
     {
         uint32_t base = 0, sb = 0;
@@ -710,14 +710,23 @@ void build_part(const mb_batch_desc* b, uint32_t r, const RobotPack& pk, const s
             pm.own.push_back(m);
         }
     const uint32_t n_own = (uint32_t)pm.own.size();
+    // halo masses are collected once each (local_of = -2 marks them)
+    auto to_halo = [&](uint32_t m) {
+        if (local_of[m] == -1) {
+            local_of[m] = -2;
+            pm.halo.push_back(m);
+        }
+    };
     std::vector<uint32_t> sp;
+    sp.reserve(pk.springs.size());
     for (uint32_t ls : pk.springs) {
         const int64_t g = s0 + ls;
         const uint32_t a = b->pairs[2 * g], c = b->pairs[2 * g + 1];
-        if (part_of[a] != p && part_of[c] != p) continue;
+        const bool ia = part_of[a] == p, ic = part_of[c] == p;
+        if (!ia && !ic) continue;
         sp.push_back(ls);
-        if (part_of[a] != p) pm.halo.push_back(a);
-        if (part_of[c] != p) pm.halo.push_back(c);
+        if (!ia) to_halo(a);
+        if (!ic) to_halo(c);
     }
     // faces with a corner in the part (robot face order); their other
     // corners join the halo
@@ -730,10 +739,9 @@ void build_part(const mb_batch_desc* b, uint32_t r, const RobotPack& pk, const s
         if (part_of[c[0]] != p && part_of[c[1]] != p && part_of[c[2]] != p) continue;
         fl.push_back((uint32_t)f);
         for (int k = 0; k < 3; ++k)
-            if (part_of[c[k]] != p) pm.halo.push_back(c[k]);
+            if (part_of[c[k]] != p) to_halo(c[k]);
     }
     std::sort(pm.halo.begin(), pm.halo.end());
-    pm.halo.erase(std::unique(pm.halo.begin(), pm.halo.end()), pm.halo.end());
     for (uint32_t j = 0; j < pm.halo.size(); ++j) local_of[pm.halo[j]] = (int32_t)(n_own + j);
     if (!fl.empty()) {
         // part-local corners; rows (ascending face order) for own masses
@@ -776,7 +784,7 @@ void build_part(const mb_batch_desc* b, uint32_t r, const RobotPack& pk, const s
         if (part_of[c] == p) row_start[lc + 1]++;
     }
     for (uint32_t i = 0; i < n_own; ++i) row_start[i + 1] += row_start[i];
-    std::vector<Ent> ents(row_start[n_own]);
+    raw_vector<Ent> ents(row_start[n_own]);
     std::vector<uint32_t> fill(row_start.begin(), row_start.end() - 1);
     // b ends in reverse, then a ends in spring order (rows mostly arrive
     // sorted, as in build_bin).  Aligned by the robot-local index of the
