@@ -467,6 +467,28 @@ def secondary(args, batch, local_rank, dev, hbm_peak):
                             f"256 point-cloud robots of 500-2,000 masses, 25 nearest-neighbour springs, "
                             f"{nb.n_masses} masses, {nb.active_springs()} springs, water, stresses tracked, "
                             f"dt=1e-4")
+    # the same point clouds with their convex hulls as surfaces and the face
+    # drag on (split over clusters, velocities exchanged with positions)
+    hb = mb.Batch(**{k: getattr(nb, k) for k in ("mass_offsets", "pos", "vel", "mass_material",
+                                                 "spring_offsets", "pairs", "spring_material", "lbar")})
+    hulls = [robots.hull_faces(nb.pos[int(nb.mass_offsets[r]):int(nb.mass_offsets[r + 1]), :3])
+             for r in range(nb.n_robots)]
+    hb.face_offsets = np.concatenate([[0], np.cumsum([len(h) for h in hulls])]).astype(np.int64)
+    hb.faces = np.ascontiguousarray(np.concatenate(hulls), np.uint16)
+    fs = mb.Simulator(local_rank)
+    fs.set_materials(mb.materials.force_table())
+    fs.set_mode(S.MODE_FORCE_WATER)
+    fs.set_environment(**S.WATER_FACES)
+    fs.setTimeStep(1e-4)
+    fs.set_batch(hb)
+    rate = _device_rate(fs, hb.active_springs(), 1000, True, dev)
+    p, _, _ = fs.collect_arrays()
+    out["nn_water_faces"] = {
+        "value": rate, "unit": "spring-updates/s", "steps": 1000, "finite": bool(np.isfinite(p).all()),
+        "faces": int(hb.face_offsets[-1]), "config": fs.launch_config(),
+        "workload": "the nn_water robots with their convex hulls as surfaces, face drag rho = 1000 "
+                    "(no per-mass drag), stresses tracked"}
+    del fs
     out["devo"] = devo_bench(local_rank)
     out["build"] = build_bench(local_rank)
     out["surrogate"] = surrogate_bench(local_rank)
