@@ -46,16 +46,17 @@ WORKLOADS = {
 }
 
 # Algorithmic bytes per spring-update.
-#   HBM (a streaming step that keeps nothing on chip, the reference design):
+#   Shared memory (the binding resource of the resident step kernel, which
+#   keeps every robot on chip for a whole launch): 24 B for the two endpoint
+#   positions (2 x 3 floats) + 12 B for the correction the spring stores
+#   (3 floats) + 24 B for the two reads of that correction when its ends
+#   gather it (2 x 3 floats) = 60 B.
+#   HBM, for a step that keeps nothing on chip (the reference's design):
 #   9 B topology (2 x u16 pair, u8 material, f32 mean length) + 8 B stress
 #   read+write when tracking + per-mass state (pos and vel, 3 floats each,
 #   read and write: 48 B) x masses/springs.
-#   Shared memory (this kernel, per spring-update): 24 B endpoint positions +
-#   12 B correction store + 2 x (4 B incidence entry + 12 B correction) gather
-#   + 8 B material factors; per mass 12 B position store.
+SMEM_B = 60.0
 HBM_TOPO_B, HBM_STRESS_B, HBM_MASS_B = 9.0, 8.0, 48.0
-SMEM_SPRING_B, SMEM_MASS_B = 76.0, 12.0
-SMEM_BYTES_PER_CLK_SM = 128.0
 
 
 def peaks():
@@ -231,17 +232,16 @@ def run_ours(args, rank, local_rank, world):
     value = updates_all / t_max
     ms_per_step = 1e3 * t_max / args.steps
 
-    # roofline of the step kernel (per launch)
+    # roofline of the step kernel (per launch): shared-memory bound, against
+    # the shared-memory read bandwidth measured on this GPU by the probe kernel
     t_launch = t_local / (args.steps * launches_per_eval)
     upd_launch = float(active) * steps_per_eval / launches_per_eval
     hbm_b = HBM_TOPO_B + (HBM_STRESS_B if track else 0.0) + HBM_MASS_B * batch.n_masses / active
-    smem_b = SMEM_SPRING_B + SMEM_MASS_B * batch.n_masses / active
     hbm_peak, hbm_src = peaks()
     clocks = clk.summary()
-    sm_clk = clocks.get("sm_mhz") or 1965.0
-    smem_peak = SMEM_BYTES_PER_CLK_SM * torch.cuda.get_device_properties(dev).multi_processor_count * sm_clk * 1e6 / 1e9
+    smem_peak, smem_clk = smem_peak_gbs(local_rank)
     hbm_ach = hbm_b * upd_launch / t_launch / 1e9
-    smem_ach = smem_b * upd_launch / t_launch / 1e9
+    smem_ach = SMEM_B * upd_launch / t_launch / 1e9
 
     # plain configuration: one robot per CTA, one step per launch, no graph
     plain = None
@@ -327,14 +327,17 @@ def run_ours(args, rank, local_rank, world):
             "l2": "flushed between timed iterations (256 MB write)",
             "parallelism": f"population sharded over {world} GPU(s), no collective in the step",
         },
-        "roofline": {"bound": "hbm", "achieved": hbm_ach, "peak": hbm_peak, "unit": "GB/s",
-                     "frac": hbm_ach / hbm_peak, **_step_traffic(args.workload, cfg, active, hbm_b),
-                     "bytes_per_update": hbm_b, "peak_source": hbm_src,
-                     "note": "HBM bytes a streaming step must move per spring-update; this kernel keeps "
-                             "robots on chip for a whole launch, see roofline_smem"},
-        "roofline_smem": {"bound": "smem", "achieved": smem_ach, "peak": smem_peak, "unit": "GB/s",
-                          "frac": smem_ach / smem_peak, "bytes_per_update": smem_b,
-                          "peak_source": f"nominal 128 B/clk/SM x SMs x median SM clock {sm_clk} MHz"},
+        "roofline": {"bound": "smem", "achieved": smem_ach, "peak": smem_peak, "unit": "GB/s",
+                     "frac": smem_ach / smem_peak, **_step_traffic(args.workload, cfg, active),
+                     "bytes_per_update": SMEM_B,
+                     "peak_source": f"measured: shared-memory read probe (mb_measure_smem_bandwidth) on this GPU, "
+                                    f"{smem_clk:.1f} B/clk/SM",
+                     "kernel": "step_kernel (resident: robots on chip for the whole launch)"},
+        "roofline_hbm": {"bound": "hbm", "achieved": hbm_ach, "peak": hbm_peak, "unit": "GB/s",
+                         "frac": hbm_ach / hbm_peak, "bytes_per_update": hbm_b, "peak_source": hbm_src,
+                         "note": "the HBM bytes a step that keeps nothing on chip (the reference's design) "
+                                 "must move per spring-update; this kernel moves the state and topology "
+                                 "once per launch (traffic)"},
         "kernel_ms_per_launch": 1e3 * t_launch,
         "cpu_baseline": cpu,
         "e2e": {"value": e2e, "unit": "spring-updates/s", "h2d_bytes_per_step": int(h2d),
@@ -363,22 +366,31 @@ def _device_rate(sim, active, steps, track, dev):
 
 
 # DRAM bytes (read + write) of one 1,000-step launch of the step kernel on
-# the uneven population in its tuned configuration, from the ncu capture in
-# profiles/step_kernel_1024x8x2_grouped296_uneven512.md
+# the uneven population in its tuned configuration (ncu, dram__bytes_read.sum
+# + dram__bytes_write.sum): the state and topology, read once per launch.
 STEP_TRAFFIC = {("uneven", 1024, 8, 2, 296, 1000): 24.65e6 + 12.0e3}
 
 
-def _step_traffic(workload, cfg, active, bytes_per_update):
-    """Measured DRAM bytes per launch beside the algorithmic (streaming)
-    bytes of the same launch, when the bench runs the profiled configuration."""
+def _step_traffic(workload, cfg, active):
+    """Measured DRAM bytes per launch, when the bench runs the profiled
+    configuration."""
     key = (workload, cfg["threads"], cfg["springs_per_thread"], cfg["masses_per_thread"], cfg["bins"], cfg["chunk"])
     t = STEP_TRAFFIC.get(key)
     if t is None:
         return {"traffic": None}
-    return {"traffic": t, "traffic_unit": "bytes per launch",
-            "traffic_source": "ncu capture of the same configuration "
-                              "(profiles/step_kernel_1024x8x2_grouped296_uneven512.md)",
-            "algorithmic_bytes_per_launch": bytes_per_update * active * cfg["chunk"]}
+    return {"traffic": t, "traffic_unit": "DRAM bytes per launch",
+            "traffic_source": "ncu capture of the same configuration (dram__bytes_read.sum + dram__bytes_write.sum)"}
+
+
+def smem_peak_gbs(device):
+    """Shared-memory read bandwidth of this GPU (GB/s) and bytes per clock
+    per SM, from the library's probe kernel."""
+    import ctypes
+
+    from mercury_b200 import _lib
+    bps, bpc = ctypes.c_double(), ctypes.c_double()
+    _lib.check(_lib.LIB.mb_measure_smem_bandwidth(device, ctypes.byref(bps), ctypes.byref(bpc)))
+    return bps.value / 1e9, bpc.value
 
 
 def secondary(args, batch, local_rank, dev, hbm_peak):
@@ -460,6 +472,8 @@ def secondary(args, batch, local_rank, dev, hbm_peak):
     out["streamed"] = large(sb, 0, None,
                             f"64 robots of 10x10x10 cells, {sb.n_masses} masses, {sb.active_springs()} springs, "
                             f"stresses tracked, reference step, dt=1e-4")
+    out["long_horizon"] = long_horizon(sb, local_rank, dev, hbm_peak)
+    out["force_land_divergence"] = land_divergence(local_rank)
     # point-cloud robots in water (256 robots of 500-2,000 masses, 25 nearest
     # neighbours, stresses tracked): springs built on the device
     nb = mb.pack(robots.nn_population_device(256, mass=0.1, device=local_rank))
@@ -493,6 +507,84 @@ def secondary(args, batch, local_rank, dev, hbm_peak):
     out["build"] = build_bench(local_rank)
     out["surrogate"] = surrogate_bench(local_rank)
     return out
+
+
+def long_horizon(sb, local_rank, dev, hbm_peak):
+    """The streamed long-horizon configuration as specified: 64 robots of
+    10x10x10 cells, stresses tracked, Simulate(10 s) at dt = 1e-4 (99,937
+    steps of the float clock), device-timed on the default path (robots split
+    over thread-block clusters); with the drift of the FP32 positions from
+    the oracle's FP64 transcription over the first 1,000 steps."""
+    import torch
+
+    import mercury_b200 as mb
+    from oracle import core
+    act = sb.active_springs()
+    sim = mb.Simulator(local_rank)
+    sim.setTimeStep(1e-4)
+    sim.set_batch(sb)
+    sim.run_steps(1000, True)
+    pos, _, _ = sim.collect_arrays()
+    pd, vd = sb.pos.astype(np.float64), sb.vel.astype(np.float64)
+    sd = np.zeros(sb.n_springs, np.float64)
+    core.xpbd_run_f64(sb, pd, vd, sd, core.material_table(), 1e-4, 0.0, 1000, True)
+    drift = float(np.abs(pos[:, :3] - pd[:, :3]).max())
+    motion = float(np.abs(pd[:, :3] - sb.pos[:, :3]).max())
+    sim.set_state(sb.pos, sb.vel)
+    sim.Reset()
+    st = torch.cuda.ExternalStream(sim.stream, device=dev)
+    sim.Simulate(0.01, trackStresses=True)  # warm: graph of the chunk
+    sim.set_state(sb.pos, sb.vel)
+    sim.Reset()
+    sim.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    steps = sim.Simulate(10.0, trackStresses=True)
+    e1.record(st)
+    e1.synchronize()
+    secs = e0.elapsed_time(e1) / 1e3
+    p, _, _ = sim.collect_arrays()
+    rate = act * steps / secs
+    hbm_b = HBM_TOPO_B + HBM_STRESS_B + HBM_MASS_B * sb.n_masses / act
+    return {"value": rate, "unit": "spring-updates/s", "steps": steps, "seconds": secs,
+            "simulated_s": 10.0, "finite": bool(np.isfinite(p).all()), "config": sim.launch_config(),
+            "roofline": {"bound": "hbm", "achieved": rate * hbm_b / 1e9, "peak": hbm_peak, "unit": "GB/s",
+                         "frac": rate * hbm_b / 1e9 / hbm_peak, "bytes_per_update": hbm_b,
+                         "note": "HBM bytes a streaming step moves per spring-update (the split kernel keeps "
+                                 "each robot on chip over two SMs)"},
+            "drift_vs_fp64_first_1000_steps_m": drift, "fp64_motion_first_1000_steps_m": motion,
+            "workload": f"64 robots of 10x10x10 cells ({sb.n_masses} masses, {act} springs), stresses tracked, "
+                        f"reference step, dt=1e-4, Simulate(10 s)"}
+
+
+def land_divergence(local_rank):
+    """Contact chaos: max |x_fp32 - x_fp64| of the land mode on 32 uneven
+    robots (0.1 kg masses), the CUDA step against the oracle's FP64
+    transcription of the same law, after 10 ... 3,000 steps."""
+    import mercury_b200 as mb
+    from mercury_b200 import robots
+    from mercury_b200 import simulator as S
+    from oracle import core
+    keys = ("g", "floor_stiffness", "friction_static", "friction_kinetic", "drag", "damping")
+    b = robots.population_batch("uneven", 32, mass=0.1)
+    sim = mb.Simulator(local_rank)
+    sim.set_materials(mb.materials.force_table())
+    sim.set_mode(S.MODE_FORCE_LAND)
+    sim.set_environment(**S.LAND)
+    sim.setTimeStep(1e-4)
+    sim.set_batch(b)
+    pd, vd = b.pos.astype(np.float64), b.vel.astype(np.float64)
+    done, curve = 0, {}
+    for n in (10, 30, 100, 300, 1000, 3000):
+        sim.run_steps(n - done, False)
+        core.force_run_f64(1, b, pd, vd, mb.materials.force_table(), [S.LAND[k] for k in keys], 1e-4,
+                           done * 1e-4, n - done)
+        done = n
+        pos, _, _ = sim.collect_arrays()
+        curve[str(n)] = float(np.abs(pos[:, :3] - pd[:, :3]).max())
+    g = np.log(curve["1000"] / curve["30"]) / 970.0
+    return {"max_abs_dx_m": curve, "growth_per_step": float(g), "efold_steps": float(1.0 / g),
+            "workload": "32 uneven voxel robots, 0.1 kg masses, land (penalty ground, Coulomb friction), dt=1e-4"}
 
 
 def build_bench(local_rank):
@@ -638,17 +730,17 @@ def devo_bench(local_rank, calls=3):
 
 
 def run_reference(args, rank, local_rank, world):
-    """Reference arm: rank 0 only."""
-    import mercury_b200 as mb  # noqa: F401
-    from mercury_b200 import robots
+    """Reference arm, rank 0 only.  Nothing of the product is loaded here:
+    the population is built by the reference's own VoxelRobot::Build
+    (oracle/population.py through oracle/_ref), the material table and the
+    timed step are the oracle's."""
     if rank != 0:
         return None
+    from oracle import core, population
     pop, duration, dt, track = WORKLOADS[args.workload]
-    batch = robots.population_batch(pop, seed_base=1000 * {"small": 0, "uneven": 1, "streamed": 4}[pop])
+    batch = population.population_batch(pop, seed_base=1000 * {"small": 0, "uneven": 1, "streamed": 4}[pop])
     active = batch.active_springs()
-    from oracle import core
-    import mercury_b200 as mbm
-    table = mbm.material_table()
+    table = core.material_table()
     threads = os.cpu_count() or 1
     steps_total = core.step_count(duration, dt)
     # bounded sample per bench step: all robots, `sample` steps
@@ -694,50 +786,17 @@ def run_reference(args, rank, local_rank, world):
         "dtype": "f32",
         "data": "synthetic",
         "config": {"workload": f"{args.workload}: {batch.n_robots} voxel robots, {active} non-air springs, "
-                               f"reference XPBD step, dt={dt}; each bench step = all robots x {sample} of the "
-                               f"{steps_total} steps",
-                   "parallelism": "CPU, OpenMP over robots"},
+                               f"reference XPBD step, dt={dt}, {duration} s = {steps_total} steps per "
+                               f"evaluation; the rate is per spring-update, measured on a bounded sample "
+                               f"of {sample} of those steps for all robots per bench step",
+                   "parallelism": "CPU, OpenMP over robots",
+                   "robots": "built by the reference's VoxelRobot::Build (oracle/_ref)"},
         "cpu_baseline": {"value": value, "unit": "spring-updates/s", "cores": threads, "kind": "port",
-                         "sample": f"all {batch.n_robots} robots x {sample} steps per bench step"},
+                         "sample": f"all {batch.n_robots} robots x {sample} of {steps_total} steps per bench step"},
         "e2e": {"value": value, "unit": "spring-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "reference_cuda": ref_cuda,
         "reference_cuda_devo": ref_devo,
     }
-
-
-def reference_cuda(batch, dt, duration, track):
-    """The reference's own CUDA simulator (oracle/_ref, built from its
-    sources) on the same population: SetElements + Simulate + Collect, wall
-    time around Simulate as optimize/benchmark.cpp:96-109 measures it."""
-    import ctypes
-    path = os.path.join(ROOT, "oracle", "_ref", "libmercury_ref.so")
-    if not os.path.exists(path):
-        return {"unavailable": "oracle/_ref/libmercury_ref.so not built"}
-    L = ctypes.CDLL(path)
-    L.ref_decode_id.argtypes = [ctypes.c_uint32]
-    L.ref_decode_id(1)
-    L.ref_simulate.argtypes = [ctypes.c_int] + [ctypes.c_void_p] * 8 + [ctypes.c_float, ctypes.c_float, ctypes.c_int] + [ctypes.c_void_p] * 4
-    L.ref_simulate.restype = ctypes.c_int
-    mo = batch.mass_offsets.astype(np.int32)
-    so = batch.spring_offsets.astype(np.int32)
-    pos3 = np.ascontiguousarray(batch.pos[:, :3])
-    vel3 = np.ascontiguousarray(batch.vel[:, :3])
-    po, vo = np.zeros_like(pos3), np.zeros_like(vel3)
-    st = np.zeros(batch.n_springs, np.float32)
-    tt = np.zeros(1, np.float32)
-    P = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
-    args = (batch.n_robots, P(mo), P(pos3), P(vel3), P(batch.mass_material), P(so),
-            P(np.ascontiguousarray(batch.pairs)), P(batch.lbar), P(batch.spring_material))
-    short = min(duration, 0.01)
-    L.ref_simulate(*args, dt, short, int(track), P(po), P(vo), P(st), P(tt))  # warm-up
-    t0 = time.perf_counter()
-    steps = L.ref_simulate(*args, dt, duration, int(track), P(po), P(vo), P(st), P(tt))
-    wall = time.perf_counter() - t0
-    active = batch.active_springs()
-    return {"value": active * steps / wall, "unit": "spring-updates/s", "steps": steps, "wall_s": wall,
-            "value_all_springs": batch.n_springs * steps / wall,
-            "note": "wall time of SetElements+Simulate+Collect (host packing, H2D, 4 launches and 4 syncs "
-                    "per step, D2H); masses padded per robot to the largest count"}
 
 
 def _ref_lib():
@@ -745,26 +804,70 @@ def _ref_lib():
     path = os.path.join(ROOT, "oracle", "_ref", "libmercury_ref.so")
     if not os.path.exists(path):
         return None
-    return ctypes.CDLL(path)
+    L = ctypes.CDLL(path)
+    L.ref_decode_id.argtypes = [ctypes.c_uint32]
+    L.ref_decode_id(1)
+    return L
 
 
-def reference_devo(calls=3):
-    """The reference's Simulator::Devo (oracle/_ref) on the population of
-    devo_bench, timed per call on the host clock as DevoBenchmark does."""
+def reference_cuda(batch, dt, duration, track):
+    """The reference's own CUDA simulator (oracle/_ref, built from its
+    sources) on the same population.  `value` times Simulate(duration) alone
+    on the host clock, as optimize/benchmark.cpp:96-99 does (Simulate
+    synchronises after every launch); `wall_*` adds SetElements (host
+    packing, allocation, H2D) and Collect (D2H)."""
     import ctypes
     L = _ref_lib()
     if L is None:
         return {"unavailable": "oracle/_ref/libmercury_ref.so not built"}
-    b = devo_population()
+    L.ref_simulate_timed.argtypes = ([ctypes.c_int] + [ctypes.c_void_p] * 8 +
+                                     [ctypes.c_float, ctypes.c_float, ctypes.c_int] + [ctypes.c_void_p] * 3)
+    L.ref_simulate_timed.restype = ctypes.c_int
+    mo = batch.mass_offsets.astype(np.int32)
+    so = batch.spring_offsets.astype(np.int32)
+    pos3 = np.ascontiguousarray(batch.pos[:, :3])
+    vel3 = np.ascontiguousarray(batch.vel[:, :3])
+    po, vo = np.zeros_like(pos3), np.zeros_like(vel3)
+    secs = np.zeros(2, np.float64)
+    P = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+    args = (batch.n_robots, P(mo), P(pos3), P(vel3), P(batch.mass_material), P(so),
+            P(np.ascontiguousarray(batch.pairs)), P(batch.lbar), P(batch.spring_material))
+    short = min(duration, 0.01)
+    L.ref_simulate_timed(*args, dt, short, int(track), P(po), P(vo), P(secs))  # warm-up
+    steps = L.ref_simulate_timed(*args, dt, duration, int(track), P(po), P(vo), P(secs))
+    active = batch.active_springs()
+    return {"value": active * steps / secs[0], "unit": "spring-updates/s", "steps": steps,
+            "simulate_s": float(secs[0]), "value_all_springs": batch.n_springs * steps / secs[0],
+            "wall_value": active * steps / secs[1], "wall_s": float(secs[1]),
+            "note": "value: Simulate alone (4 launches and 4 syncs per step), host clock, as the reference's "
+                    "benchmark times it; wall_value: SetElements + Simulate + Collect; masses padded per "
+                    "robot to the largest count"}
+
+
+def reference_devo(calls=3):
+    """The reference's Simulator::Devo (oracle/_ref) on the population of
+    devo_bench (copies of the reference's default robot, built by its own
+    VoxelRobot::Build), timed per call on the host clock as DevoBenchmark
+    does."""
+    import ctypes
+    from oracle import population
+    L = _ref_lib()
+    if L is None:
+        return {"unavailable": "oracle/_ref/libmercury_ref.so not built"}
+    pos, mm, pairs, lbar, sm, _, _ = population.build_cells(np.full((11, 11, 11), population.BONE, np.uint8), 1.0)
+    R = DEVO_ROBOTS
+    nm, ns = len(pos), len(lbar)
+    mo = (np.arange(R + 1) * nm).astype(np.int32)
+    so = (np.arange(R + 1) * ns).astype(np.int32)
+    pos3 = np.ascontiguousarray(np.tile(pos, (R, 1)))
+    vel3 = np.zeros_like(pos3)
     L.ref_devo_time.argtypes = ([ctypes.c_int] + [ctypes.c_void_p] * 8 +
                                 [ctypes.c_uint, ctypes.c_float, ctypes.c_float, ctypes.c_int, ctypes.c_void_p])
     L.ref_devo_time.restype = ctypes.c_int
     P = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
-    mo, so = b.mass_offsets.astype(np.int32), b.spring_offsets.astype(np.int32)
-    pos3, vel3 = np.ascontiguousarray(b.pos[:, :3]), np.ascontiguousarray(b.vel[:, :3])
     secs = np.zeros(calls, np.float64)
-    L.ref_devo_time(b.n_robots, P(mo), P(pos3), P(vel3), P(b.mass_material), P(so),
-                    P(np.ascontiguousarray(b.pairs)), P(b.lbar), P(b.spring_material),
+    L.ref_devo_time(R, P(mo), P(pos3), P(vel3), P(np.tile(mm, R)), P(so),
+                    P(np.ascontiguousarray(np.tile(pairs, (R, 1)))), P(np.tile(lbar, R)), P(np.tile(sm, R)),
                     DEVO_K, 1e-4, 0.01, calls, P(secs))
     w = float(np.median(secs))
     n = DEVO_ROBOTS * DEVO_K
@@ -790,14 +893,15 @@ def main():
                     help="reuse (and store) the autotuner's choice in its cache file instead of re-tuning")
     args = ap.parse_args()
 
-    from mercury_b200 import dist
-    rank, local_rank, world = dist.env_rank()
-    if args.impl == "reference":
+    rank, local_rank, world = (int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)),
+                               int(os.environ.get("WORLD_SIZE", 1)))
+    if args.impl == "reference":  # loads nothing of the product
         if rank != 0:
             return
         line = run_reference(args, rank, local_rank, world)
         print(json.dumps(line), flush=True)
         return
+    from mercury_b200 import dist
     dist.init("nccl" if world > 1 else "gloo")
     try:
         line = run_ours(args, rank, local_rank, world)

@@ -352,8 +352,9 @@ MB_API mb_status mb_voxel_build(int nx, int ny, int nz, float h, const uint8_t* 
  * image: every GPU that loads the library holds it until the process exits.
  * The call calls no cudaMalloc, cudaFree or other allocating routine.
  *
- * The first call on a device looks up the scratch array's device address;
- * make that first call before any stream capture.  Every call shares the
+ * The first call on a device looks up the scratch array's device address
+ * and keeps it for the life of the process: make that first call before any
+ * stream capture, and do not reset the device (cudaDeviceReset) after it.  Every call shares the
  * scratch array and keeps the last call's contents, so calls that overlap on
  * the GPU (different streams or host threads) race: serialise them.  The
  * call synchronises `stream` to read its status. */
@@ -405,6 +406,18 @@ MB_API mb_status mb_surrogate_set_weight_decay(mb_surrogate* s, float weight_dec
 MB_API mb_status mb_surrogate_use_tcgen05(mb_surrogate* s, int on);
 MB_API mb_status mb_surrogate_train_step(mb_surrogate* s, const uint8_t* genomes, const float* targets, uint32_t n,
                                          float lr, float* loss);
+
+/* ----------------------------------------------------------------------
+ * Measurement (no reference counterpart).
+ *
+ * Shared-memory read bandwidth of `device`: one 1,024-thread CTA per SM
+ * streams conflict-free 128-bit shared loads; bytes_per_s from CUDA events
+ * (best of 5 launches), bytes_per_clk_sm (may be NULL) from the SMs' own
+ * clock counters.  The roofline denominator of the resident step kernel,
+ * which keeps robots in shared memory for a whole launch.  Allocates a few
+ * bytes of device memory and synchronises.
+ * -------------------------------------------------------------------- */
+MB_API mb_status mb_measure_smem_bandwidth(int device, double* bytes_per_s, double* bytes_per_clk_sm);
 
 /* Library version string. */
 MB_API const char* mb_version(void);

@@ -12,8 +12,7 @@ import os
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-# MB_LIBRARY selects another build of the library (A/B timing of variants)
-LIB_PATH = os.environ.get("MB_LIBRARY") or os.path.join(_HERE, "libmercury_b200.so")
+LIB_PATH = os.path.join(_HERE, "libmercury_b200.so")
 
 MB_OK = 0
 STATUS_NAMES = {
@@ -135,6 +134,7 @@ def _load() -> ctypes.CDLL:
         "mb_surrogate_train_step": (I32, [P, P, P, U32, F32, P]),
         "mb_surrogate_set_weight_decay": (I32, [P, F32]),
         "mb_surrogate_use_tcgen05": (I32, [P, I32]),
+        "mb_measure_smem_bandwidth": (I32, [I32, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
         "mb_version": (ctypes.c_char_p, []),
     }
     for name, (res, args) in sigs.items():

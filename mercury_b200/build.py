@@ -13,7 +13,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 SRC = [os.path.join(HERE, "csrc", f) for f in ("mb_kernels.cu", "mb_host.cpp", "mb_pack.cpp",
-                                               "mb_voxel.cpp", "mb_noalloc.cu", "mb_devo.cu", "mb_voxel_dev.cu", "mb_surrogate.cu", "mb_knn.cu")]
+                                               "mb_voxel.cpp", "mb_noalloc.cu", "mb_devo.cu", "mb_voxel_dev.cu", "mb_surrogate.cu", "mb_knn.cu", "mb_probe.cu")]
 DEPS = SRC + [os.path.join(HERE, "csrc", f) for f in ("mb_internal.h", "mb_sin.cuh", "mb_pack.h", "mb_devo.h", "mb_voxel.h", "mb_voxel_dev.h", "mb_sg_kernels.cuh")] + [
     os.path.join(ROOT, "include", "mercury_b200.h")]
 OUT = os.path.join(HERE, "libmercury_b200.so")

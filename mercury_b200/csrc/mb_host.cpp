@@ -29,10 +29,6 @@
 #include <vector>
 
 #include <cuda_runtime.h>
-#include <execinfo.h>
-#include <signal.h>
-#include <sys/syscall.h>
-#include <unistd.h>
 
 #include "../../include/mercury_b200.h"
 #include "mb_devo.h"
@@ -240,46 +236,6 @@ mb_status fail(mb_context* c, mb_status s, const char* fmt, ...) {
     return s;
 }
 
-// Stage log on stderr when MB_TRACE is set (diagnostics of host crashes).
-bool trace_on() {
-    static const bool on = std::getenv("MB_TRACE") != nullptr;
-    return on;
-}
-#define MB_TRACE(...)                                   \
-    do {                                                \
-        if (trace_on()) {                               \
-            std::fprintf(stderr, "[mb] " __VA_ARGS__);  \
-            std::fputc('\n', stderr);                   \
-            std::fflush(stderr);                        \
-        }                                               \
-    } while (0)
-
-// Under MB_TRACE: on SIGSEGV print the faulting address, thread and native
-// backtrace to stderr, then re-raise with the default action.
-void segv_report(int sig, siginfo_t* si, void*) {
-    char buf[160];
-    int n = std::snprintf(buf, sizeof(buf), "[mb] signal %d at address %p in thread %ld\n", sig,
-                          si ? si->si_addr : nullptr, (long)syscall(SYS_gettid));
-    if (n > 0) (void)!write(2, buf, (size_t)n);
-    void* frames[64];
-    int k = backtrace(frames, 64);
-    backtrace_symbols_fd(frames, k, 2);
-    signal(sig, SIG_DFL);
-    raise(sig);
-}
-
-struct SegvReporter {
-    SegvReporter() {
-        if (!std::getenv("MB_TRACE")) return;
-        struct sigaction sa;
-        std::memset(&sa, 0, sizeof(sa));
-        sa.sa_sigaction = segv_report;
-        sa.sa_flags = SA_SIGINFO;
-        sigaction(SIGSEGV, &sa, nullptr);
-    }
-};
-const SegvReporter kSegvReporter;
-
 mb_status cuda_fail(mb_context* c, cudaError_t e, const char* what) {
     return fail(c, MB_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
 }
@@ -323,7 +279,6 @@ mb_status pack(mb_context* ctx, const mb_batch_desc* b, bool fallback_auto, mb::
     mb_status pst = mb::pack_population(b, po, out, err);
     const mb_launch_config none{};
     if (pst == MB_ERR_CAPACITY && fallback_auto && std::memcmp(&po.override, &none, sizeof(none)) != 0) {
-        MB_TRACE("override no longer fits (%s); automatic plan", err.c_str());
         po.override = none;
         po.override.chunk = ctx->override_cfg.chunk;
         po.override.use_graph = ctx->override_cfg.use_graph;
@@ -970,7 +925,6 @@ mb_status mb_set_elements(mb_context* ctx, const mb_batch_desc* b) {
     bool rows_failed = false;
     mb_status ust = mb_detail::upload_packed(ctx, out, &rows_failed);
     if (ust == MB_OK && rows_failed) {  // rare: the host builds the rows
-        MB_TRACE("device rows did not fit; host rows");
         ust = mb_detail::pack(ctx, b, false, out, true, false);
         if (ust == MB_OK) ust = mb_detail::upload_packed(ctx, out);
     }
@@ -1077,22 +1031,13 @@ cudaError_t issue_chunks(mb_context* c, float t0, uint32_t steps, bool track) {
                                               (uint32_t)c->mode, c->rates.p, c->invk.p, c->stream);
         if (ea != cudaSuccess) return ea;
         mb::StepParams p = make_params(c, t, n, track);
-        MB_TRACE("launch bins=%u threads=%u spt=%u mpt=%u smem=%u steps=%u", p.n_bins, c->shape.threads,
-                 c->shape.spt, c->shape.mpt, p.smem_bytes, n);
         cudaError_t e = c->streamed  ? mb::launch_stream(p, 1024, c->stream_mpt, c->stream)
                         : c->cluster ? launch_split_groups(c, p)
                                      : mb::launch_step(p, c->shape, c->stream);
-        MB_TRACE("launch returned %d", (int)e);
-        if (trace_on() && std::getenv("MB_SYNC")) {
-            cudaError_t es = cudaStreamSynchronize(c->stream);
-            MB_TRACE("sync after launch: %d %s", (int)es, cudaGetErrorString(es));
-        }
         if (e != cudaSuccess) return e;
         t = advance(t, c->dt, n);
         done += n;
-        MB_TRACE("chunk done");
     }
-    MB_TRACE("chunks issued");
     return cudaSuccess;
 }
 
@@ -1115,16 +1060,13 @@ mb_status run(mb_context* c, uint32_t steps, bool track) {
         if (it == c->graphs.end()) {
             if (c->graphs.size() >= 16) c->clear_graphs();
             // kernel attributes cannot change inside a capture
-            MB_TRACE("prepare");
             MB_CUDA(c, c->streamed ? mb::prepare_stream(1024, c->stream_mpt, (uint32_t)c->mode, track, c->smem_bytes)
                                     : c->cluster ? mb::prepare_split(c->shape, (uint32_t)c->mode, track, c->smem_bytes)
                                     : mb::prepare_step(c->shape, (uint32_t)c->mode, track, c->smem_bytes));
             cudaGraph_t g;
-            MB_TRACE("begin capture");
             MB_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
             cudaError_t e = issue_chunks(c, t0, steps, track);
             cudaError_t e2 = cudaStreamEndCapture(c->stream, &g);
-            MB_TRACE("end capture %d %d", (int)e, (int)e2);
             if (e != cudaSuccess) {
                 if (e2 == cudaSuccess) cudaGraphDestroy(g);
                 return cuda_fail(c, e, "capture of step launches");
@@ -1132,15 +1074,12 @@ mb_status run(mb_context* c, uint32_t steps, bool track) {
             if (e2 != cudaSuccess) return cuda_fail(c, e2, "cudaStreamEndCapture");
             cudaGraphExec_t ex;
             cudaError_t e3 = cudaGraphInstantiate(&ex, g, 0);
-            MB_TRACE("instantiate %d", (int)e3);
             cudaGraphDestroy(g);
             if (e3 != cudaSuccess) return cuda_fail(c, e3, "cudaGraphInstantiate");
             it = c->graphs.emplace(key, ex).first;
         }
         MB_CUDA(c, cudaGraphLaunch(it->second, c->stream));
-        MB_TRACE("graph launched");
     } else {
-        MB_TRACE("prepare (no graph)");
         MB_CUDA(c, c->streamed ? mb::prepare_stream(1024, c->stream_mpt, (uint32_t)c->mode, track, c->smem_bytes)
                                     : c->cluster ? mb::prepare_split(c->shape, (uint32_t)c->mode, track, c->smem_bytes)
                                     : mb::prepare_step(c->shape, (uint32_t)c->mode, track, c->smem_bytes));
@@ -1148,7 +1087,6 @@ mb_status run(mb_context* c, uint32_t steps, bool track) {
         if (e != cudaSuccess) return cuda_fail(c, e, "step launch");
     }
     c->total_time = advance(t0, c->dt, steps);
-    MB_TRACE("run returns");
     return MB_OK;
 }
 
@@ -1194,7 +1132,6 @@ mb_status mb_centre_of_mass(mb_context* ctx, float* com) {
     if (!ctx || !com) return fail(ctx, MB_ERR_ARGUMENT, "null argument");
     if (!ctx->loaded) return fail(ctx, MB_ERR_STATE, "no population uploaded");
     cudaSetDevice(ctx->device);
-    MB_TRACE("com launch robots=%u", ctx->n_robots);
     MB_CUDA(ctx, mb::launch_com(ctx->pos.p, ctx->mass_mat.p, ctx->d_mass_off.p, ctx->n_robots,
                                 ctx->com.p, ctx->stream));
     MB_CUDA(ctx, cudaMemcpyAsync(com, ctx->com.p, 3 * sizeof(float) * ctx->n_robots,
@@ -1265,7 +1202,6 @@ mb_status mb_devo(mb_context* ctx, uint32_t replaced_per_robot, uint64_t seed, u
     MB_CUDA(ctx, ctx->devo_out.alloc(nrec));
     mb::DevoParams p{ctx->stress.p, ctx->d_mass_off.p, ctx->d_spring_off.p, ctx->pos.p, ctx->mass_mat.p,
                      ctx->d_table.p, ctx->total_time, replaced_per_robot, seed, flags, ctx->devo_out.p};
-    MB_TRACE("devo launch robots=%u k=%u device=%d", ctx->n_robots, replaced_per_robot, (int)on_device);
     MB_CUDA(ctx, mb::launch_devo(p, ctx->n_robots, st));
     uint32_t status[2] = {0, 0};
     if (on_device) {
@@ -1313,7 +1249,6 @@ mb_status mb_devo(mb_context* ctx, uint32_t replaced_per_robot, uint64_t seed, u
         }
     }
     if (repack) {
-        MB_TRACE("devo: host re-pack (problems %u)", status[0]);
         const mb_status s = mb_detail::host_repack(ctx);
         if (s != MB_OK) return s;
     }

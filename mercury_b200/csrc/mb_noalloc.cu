@@ -1,9 +1,8 @@
 // Entry point for callers that cannot allocate device memory.
 //
 // Some hosts of this library may not call cudaMalloc at all: an engine that
-// owns every device allocation through its own pool, code that runs while a
-// CUDA graph is being built around it, or a plugin sandbox whose memory
-// budget is fixed up front.  mb_simulate_robot_noalloc serves them: the
+// owns every device allocation through its own pool, or a plugin sandbox
+// whose memory budget is fixed up front.  mb_simulate_robot_noalloc serves them: the
 // caller passes the robot's arrays already on the device, and the packed
 // topology the step kernel needs (bin descriptor, packed springs, incidence
 // rows) is built on the device inside one fixed scratch array that is part of
@@ -33,6 +32,14 @@ constexpr uint32_t kNaMaxIncidence = MB_NOALLOC_MAX_INCIDENCE;
 constexpr uint32_t kNaSlices = kNaMaxMasses / kSliceWidth;
 constexpr uint32_t kBuildThreads = 1024;
 constexpr uint32_t kNaChunk = 128;  // steps per launch: bounds the actuation table
+
+// The step kernel shape used below (1,024 threads x 8 springs x 2 masses)
+// must hold the largest robot accepted, and the packed spring word has
+// 12-bit mass indices.
+static_assert(1024u * 8u >= kNaMaxSprings, "step shape must hold MB_NOALLOC_MAX_SPRINGS springs");
+static_assert(1024u * 2u >= kNaMaxMasses, "step shape must hold MB_NOALLOC_MAX_MASSES masses");
+static_assert(kNaMaxMasses <= 4096u, "mass indices of packed springs have 12 bits");
+static_assert(kNaMaxMasses % kSliceWidth == 0, "whole slices");
 
 // Status bits written by the build kernel.
 constexpr uint32_t kNaBadTopology = 1u;  // index or material out of range
@@ -255,7 +262,9 @@ __global__ void __launch_bounds__(kBuildThreads) noalloc_build(const BuildArgs a
 }
 
 // Device address of the scratch array, looked up once per device with the
-// device current.
+// device current (the first call on a device).  The address is kept for the
+// life of the process, so a device must not be reset (cudaDeviceReset)
+// after the first call on it.
 std::mutex g_addr_mutex;
 unsigned char* g_addr[64] = {};
 
@@ -296,7 +305,7 @@ extern "C" mb_status mb_simulate_robot_noalloc(void* stream, const float* table,
     if (cudaGetLastError() != cudaSuccess) return MB_ERR_CUDA;
 
     // the step kernel of the batched path, on one bin that lives in the scratch
-    const KernelShape shape{1024, 8, 2};  // holds kNaMaxSprings springs, kNaMaxMasses masses
+    const KernelShape shape{1024, 8, 2};  // holds kNaMaxSprings springs, kNaMaxMasses masses (asserted above)
     StepParams p{};
     p.bins = reinterpret_cast<const BinDesc*>(sc + kOffBin);
     p.n_bins = 1;

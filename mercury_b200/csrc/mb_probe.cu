@@ -1,0 +1,109 @@
+// Shared-memory read bandwidth of the device: the roofline denominator of
+// the resident step kernel, whose binding resource is shared memory (it keeps
+// every robot on chip for a whole launch, so HBM carries only the state and
+// topology once per launch).
+//
+// One 1,024-thread CTA per SM (the step kernel's shape) streams 128-bit
+// loads from a 32 KB shared buffer: consecutive lanes read consecutive
+// 16-byte words, so each warp load is four conflict-free 128-byte
+// wavefronts.  The loaded words are folded into an XOR that is written out,
+// so no load can be dropped.  Bytes counted = 16 x loads; time from CUDA
+// events on the launching stream, and the SM clock cycles of each CTA from
+// clock64 (bytes per clock per SM).
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+#include "../../include/mercury_b200.h"
+
+namespace {
+
+constexpr int kThreads = 1024;
+constexpr int kWords = 2048;  // 16-byte words: 32 KB
+constexpr int kUnroll = 8;
+
+__global__ void __launch_bounds__(kThreads, 1)
+smem_read_kernel(uint32_t iters, uint32_t* sink, unsigned long long* cycles) {
+    __shared__ uint4 buf[kWords];
+    const uint32_t tid = threadIdx.x;
+    for (uint32_t i = tid; i < kWords; i += kThreads) buf[i] = make_uint4(i, 3 * i + 1, 5 * i + 2, 7 * i + 3);
+    __syncthreads();
+    const uint32_t base = (uint32_t)__cvta_generic_to_shared(buf);
+    uint32_t acc = 0;
+    const long long c0 = clock64();
+    for (uint32_t it = 0; it < iters; ++it) {
+#pragma unroll
+        for (int k = 0; k < kUnroll; ++k) {
+            // lanes of a warp: 32 consecutive words; the offset moves each
+            // iteration so the loads cannot be hoisted
+            const uint32_t idx = (tid + (uint32_t)k * kThreads + it * 32u) & (kWords - 1);
+            uint32_t a, b, c, d;
+            asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];"
+                         : "=r"(a), "=r"(b), "=r"(c), "=r"(d)
+                         : "r"(base + idx * 16u));
+            acc ^= a ^ b ^ c ^ d;
+        }
+    }
+    const long long c1 = clock64();
+    __syncthreads();
+    if (tid == 0) cycles[blockIdx.x] = (unsigned long long)(c1 - c0);
+    if (acc == 0x9e3779b9u) sink[blockIdx.x] = acc;  // keeps the loads live
+}
+
+}  // namespace
+
+extern "C" {
+
+mb_status mb_measure_smem_bandwidth(int device, double* bytes_per_s, double* bytes_per_clk_sm) {
+    if (!bytes_per_s) return MB_ERR_ARGUMENT;
+    if (cudaSetDevice(device) != cudaSuccess) return MB_ERR_CUDA;
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || sms <= 0)
+        return MB_ERR_CUDA;
+    uint32_t* sink = nullptr;
+    unsigned long long* cycles = nullptr;
+    cudaStream_t st = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    mb_status rc = MB_ERR_CUDA;
+    const uint32_t iters = 4096;
+    const double bytes = 16.0 * kUnroll * (double)iters * kThreads * sms;
+    float best_ms = 0.0f;
+    double best_cycles = 0.0;
+    unsigned long long* host_cycles = new unsigned long long[sms];
+    if (cudaMalloc(&sink, sizeof(uint32_t) * sms) != cudaSuccess) goto done;
+    if (cudaMalloc(&cycles, sizeof(unsigned long long) * sms) != cudaSuccess) goto done;
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) goto done;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) goto done;
+    smem_read_kernel<<<sms, kThreads, 0, st>>>(iters / 8, sink, cycles);  // warm-up
+    for (int rep = 0; rep < 5; ++rep) {
+        cudaEventRecord(e0, st);
+        smem_read_kernel<<<sms, kThreads, 0, st>>>(iters, sink, cycles);
+        cudaEventRecord(e1, st);
+        if (cudaEventSynchronize(e1) != cudaSuccess) goto done;
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (cudaMemcpy(host_cycles, cycles, sizeof(unsigned long long) * sms, cudaMemcpyDeviceToHost) !=
+            cudaSuccess)
+            goto done;
+        double mean_cycles = 0.0;
+        for (int i = 0; i < sms; ++i) mean_cycles += (double)host_cycles[i] / sms;
+        if (best_ms == 0.0f || ms < best_ms) {
+            best_ms = ms;
+            best_cycles = mean_cycles;
+        }
+    }
+    if (cudaGetLastError() != cudaSuccess || best_ms <= 0.0f) goto done;
+    *bytes_per_s = bytes / (best_ms * 1e-3);
+    if (bytes_per_clk_sm) *bytes_per_clk_sm = bytes / sms / best_cycles;
+    rc = MB_OK;
+done:
+    delete[] host_cycles;
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (st) cudaStreamDestroy(st);
+    if (sink) cudaFree(sink);
+    if (cycles) cudaFree(cycles);
+    return rc;
+}
+
+}  // extern "C"

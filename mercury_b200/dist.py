@@ -69,6 +69,41 @@ def gather_fitness(local: torch.Tensor) -> torch.Tensor:
     return torch.cat(out)
 
 
+def gather_per_robot(local: torch.Tensor, n_total: int) -> torch.Tensor:
+    """All-gathers per-robot rows (shape (k, ...)) of the contiguous shards of
+    shard(n_total, rank, world), which may differ in size by one: each rank
+    pads its rows to the largest shard, and the padding is dropped after the
+    gather.  Returns the (n_total, ...) rows in robot order on every rank."""
+    if not dist.is_initialized():
+        return local
+    world = dist.get_world_size()
+    sizes = [len(shard(n_total, r, world)) for r in range(world)]
+    if local.shape[0] != sizes[dist.get_rank()]:
+        raise ValueError(f"rank {dist.get_rank()} holds {local.shape[0]} rows, its shard has {sizes[dist.get_rank()]}")
+    padded = torch.zeros((max(sizes), *local.shape[1:]), dtype=local.dtype, device=local.device)
+    padded[: local.shape[0]] = local
+    out = [torch.empty_like(padded) for _ in range(world)]
+    dist.all_gather(out, padded)
+    return torch.cat([o[:n] for o, n in zip(out, sizes)])
+
+
+def shard_batch(batch, robots: range):
+    """The robots `robots` (a contiguous range) of a packed population, as a
+    population of their own (offsets rebased; faces kept)."""
+    from .element import Batch
+    r0, r1 = robots.start, robots.stop
+    m0, m1 = int(batch.mass_offsets[r0]), int(batch.mass_offsets[r1])
+    s0, s1 = int(batch.spring_offsets[r0]), int(batch.spring_offsets[r1])
+    out = Batch(batch.mass_offsets[r0:r1 + 1] - m0, batch.pos[m0:m1].copy(), batch.vel[m0:m1].copy(),
+                batch.mass_material[m0:m1].copy(), batch.spring_offsets[r0:r1 + 1] - s0,
+                batch.pairs[s0:s1].copy(), batch.spring_material[s0:s1].copy(), batch.lbar[s0:s1].copy())
+    if batch.face_offsets is not None:
+        f0, f1 = int(batch.face_offsets[r0]), int(batch.face_offsets[r1])
+        out.face_offsets = batch.face_offsets[r0:r1 + 1] - f0
+        out.faces = batch.faces[f0:f1].copy()
+    return out
+
+
 def barrier() -> None:
     if dist.is_initialized():
         dist.barrier()

@@ -11,6 +11,8 @@
 //                      (common/simulator/Simulator.cu:206-458, 537-580) on a
 //                      batch of robots given as flat arrays and returns the
 //                      collected state and spring stresses.  Needs a GPU.
+//   ref_simulate_timed - the same, timing Simulate alone as the reference's
+//                      benchmark does (optimize/benchmark.cpp:96-99).
 //   ref_devo_time    - times the reference's Simulator::Devo
 //                      (Simulator.cu:597-668) after a stress-tracked run.
 //                      Needs a GPU.
@@ -161,6 +163,46 @@ int ref_simulate(int n_robots,
             for (int s = spring_off[r]; s < spring_off[r + 1]; ++s)
                 stress_out[s] = st[(size_t)r * spe + (s - spring_off[r])];
     }
+    return steps;
+}
+
+// ref_simulate with timings: seconds[0] = Simulate(duration) alone on the
+// host clock, as the reference's own benchmark times it
+// (optimize/benchmark.cpp:96-99; Simulate synchronises the device after
+// every launch, Simulator.cu:428-449 with sim_kernel.cu:271-325);
+// seconds[1] = SetElements + Reset + Simulate + Collect.
+int ref_simulate_timed(int n_robots,
+                       const int* mass_off, const float* pos, const float* vel,
+                       const uint8_t* mass_mat,
+                       const int* spring_off, const uint16_t* pairs,
+                       const float* lbar, const uint8_t* spring_mat,
+                       float dt, float duration, int track_stresses,
+                       float* pos_out, float* vel_out, double* seconds) {
+    std::vector<Element> elements =
+        make_elements(n_robots, mass_off, pos, vel, mass_mat, spring_off, pairs, lbar, spring_mat);
+    HarnessSimulator* sim = harness_sim();
+    sim->setTimeStep(dt);
+    auto t0 = std::chrono::steady_clock::now();
+    std::vector<ElementTracker> trackers = sim->SetElements(elements);
+    sim->Reset();
+    auto t1 = std::chrono::steady_clock::now();
+    sim->Simulate(duration, track_stresses != 0);
+    auto t2 = std::chrono::steady_clock::now();
+    std::vector<Element> out = sim->Collect(trackers);
+    auto t3 = std::chrono::steady_clock::now();
+    seconds[0] = std::chrono::duration<double>(t2 - t1).count();
+    seconds[1] = std::chrono::duration<double>(t3 - t0).count();
+    int steps = 0;
+    {
+        float rem = duration;
+        while (rem > 0.0f) { rem -= dt; ++steps; }
+    }
+    for (int r = 0; r < n_robots; ++r)
+        for (int i = mass_off[r]; i < mass_off[r + 1]; ++i) {
+            const Mass& m = out[r].masses[i - mass_off[r]];
+            pos_out[3 * i] = m.pos.x(); pos_out[3 * i + 1] = m.pos.y(); pos_out[3 * i + 2] = m.pos.z();
+            vel_out[3 * i] = m.vel.x(); vel_out[3 * i + 1] = m.vel.y(); vel_out[3 * i + 2] = m.vel.z();
+        }
     return steps;
 }
 

@@ -4,6 +4,7 @@ reference's TestSimulator does gets deterministic fitness and states equal
 to the oracle's bit for bit."""
 import os
 import subprocess
+import sys
 
 import numpy as np
 import pytest
@@ -12,10 +13,16 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 BIN = os.path.join(ROOT, "tests", "cpp", "_bin", "test_dropin")
 
 
-@pytest.mark.skipif(not os.path.isdir("/root/reference"), reason="needs the reference sources")
+def _reference_dir():
+    sys.path.insert(0, ROOT)
+    import __graft_entry__
+    return __graft_entry__.reference_dir()
+
+
+@pytest.mark.skipif(_reference_dir() is None, reason="needs the reference sources")
 def test_reference_callers_compile_against_dropin():
-    r = subprocess.run(["make", "-C", os.path.join(ROOT, "tests", "cpp"), "check-callers"],
-                       capture_output=True, text=True)
+    r = subprocess.run(["make", "-C", os.path.join(ROOT, "tests", "cpp"), "check-callers",
+                        f"REF={_reference_dir()}"], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr[-2000:]
 
 

@@ -84,3 +84,21 @@ def test_force_modes_are_robot_independent(mode):
         pi, vi, si = run32(mode, bi, e, 300)
         ms, ss = b.robot_slices(r)
         assert np.array_equal(p[ms], pi) and np.array_equal(s[ss], si)
+
+
+def test_land_fp32_tracks_fp64_early():
+    """The land law's FP32/FP64 divergence curve starts at rounding level and
+    grows about e-fold every 200 steps (contact chaos); its early part is
+    bounded here, on the oracle whose bits the kernel reproduces."""
+    b = robots.population_batch("uneven", 16, mass=0.1)
+    p, v = b.pos.copy(), b.vel.copy()
+    s = np.zeros(b.n_springs, np.float32)
+    pd, vd = b.pos.astype(np.float64), b.vel.astype(np.float64)
+    done, curve = 0, {}
+    for n in (10, 100, 300):
+        core.force_run(1, b, p, v, s, mb.materials.force_table(), env(S.LAND), 1e-4,
+                       core.advance_clock(0.0, 1e-4, done), n - done, False)
+        core.force_run_f64(1, b, pd, vd, mb.materials.force_table(), env(S.LAND), 1e-4, done * 1e-4, n - done)
+        done = n
+        curve[n] = float(np.abs(p[:, :3] - pd[:, :3]).max())
+    assert curve[10] < 1e-5 and curve[100] < 5e-4 and curve[300] < 5e-3, curve

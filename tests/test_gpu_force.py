@@ -91,3 +91,30 @@ def test_nn_robots_in_water_bit_exact(cfg):
     p, v, s = oracle(2, b, S.WATER, 200, True)
     assert np.array_equal(bits(pos), bits(p)) and np.array_equal(bits(vel), bits(v))
     assert np.array_equal(bits(stress), bits(s))
+
+
+def test_land_divergence_from_fp64():
+    """Contact chaos: the CUDA land step (FP32) against the oracle's FP64
+    transcription of the same law, on 32 uneven robots.  The static/kinetic
+    friction switch and the penalty ground amplify rounding differences
+    (about e-fold every 200 steps, 20 ms); the early part of the curve is
+    bounded, the rest is printed."""
+    b = robots.population_batch("uneven", 32, mass=0.1)
+    sim = mb.Simulator(0)
+    sim.set_materials(mb.materials.force_table())
+    sim.set_mode(1)
+    sim.set_environment(**S.LAND)
+    sim.setTimeStep(1e-4)
+    sim.set_batch(b)
+    pd, vd = b.pos.astype(np.float64), b.vel.astype(np.float64)
+    done, curve = 0, {}
+    for n in (10, 100, 300, 1000, 3000):
+        sim.run_steps(n - done, False)
+        core.force_run_f64(1, b, pd, vd, mb.materials.force_table(), [S.LAND[k] for k in ENV_KEYS], 1e-4,
+                           done * 1e-4, n - done)
+        done = n
+        pos, _, _ = sim.collect_arrays()
+        curve[n] = float(np.abs(pos[:, :3] - pd[:, :3]).max())
+    print("\nland, max |x_fp32 - x_fp64| (m): " + ", ".join(f"{k} steps {v:.2e}" for k, v in curve.items()))
+    assert curve[10] < 1e-5 and curve[100] < 5e-4 and curve[300] < 5e-3
+    assert np.isfinite(pos).all()

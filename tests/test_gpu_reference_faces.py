@@ -61,3 +61,9 @@ def test_face_law_matches_the_reference_kernel(velocity):
         scale = np.abs(ref).max()
         assert scale > 0
         assert np.abs(ours - ref).max() <= 1e-4 * scale, name
+        # per mass and component: relative to the force itself, with a floor
+        # of 1e-5 of the largest force for sums that cancel -- a wrong sign or
+        # a missing share on a mass with a small force fails here
+        err = np.abs(ours - ref)
+        bound = 1e-5 * np.abs(ref) + 1e-5 * scale
+        assert (err <= bound).all(), (name, float((err / bound).max()))

@@ -88,3 +88,47 @@ def test_noalloc_rejects_robot_over_the_limit():
     st = _fn()(None, z.data_ptr(), b.n_masses, z.data_ptr(), z.data_ptr(), b.n_springs, z.data_ptr(),
                z.data_ptr(), z.data_ptr(), None, 1e-3, 0.0, 1, 0, None)
     assert st == 3  # MB_ERR_CAPACITY, nothing launched
+
+
+def _call(torch, batch, pairs, table_dev, dt=1e-3, steps=50):
+    dev = torch.device("cuda", 0)
+    pos = torch.from_numpy(batch.pos.copy()).to(dev)
+    vel = torch.from_numpy(batch.vel.copy()).to(dev)
+    pr = torch.from_numpy(np.ascontiguousarray(pairs).view(np.int16).copy()).to(dev)
+    mat = torch.from_numpy(batch.spring_material.copy()).to(dev)
+    lbar = torch.from_numpy(batch.lbar.copy()).to(dev)
+    return _fn()(torch.cuda.current_stream(dev).cuda_stream, table_dev.data_ptr(), batch.n_masses,
+                 pos.data_ptr(), vel.data_ptr(), batch.n_springs, pr.data_ptr(), mat.data_ptr(),
+                 lbar.data_ptr(), None, dt, 0.0, steps, 0, None)
+
+
+def test_noalloc_device_side_rejections_then_a_valid_call():
+    """The statuses the build and step kernels report, each followed by a
+    valid call that must still match the batched path bit for bit (the
+    scratch keeps what the rejected call left): a spring whose end is out
+    of range (MB_ERR_ARGUMENT: the build kernel's bounds check leaves the bin
+    empty), a hub mass whose incidence row is too wide for the scratch
+    (MB_ERR_CAPACITY), and a non-finite position (MB_ERR_NONFINITE)."""
+    torch = pytest.importorskip("torch")
+    table_dev = torch.from_numpy(mb.material_table()).to("cuda:0")
+    good = mb.pack([robots.voxel_robot(robots.random_cells(5, np.random.default_rng(93)))])
+
+    bad = good.pairs.copy()
+    bad[3, 1] = good.n_masses  # one past the last mass
+    hub_n = 1500  # mass 0 joined to every other: a slice of width 1,499 > the incidence limit
+    hub = mb.Batch(np.array([0, hub_n], np.int64), np.zeros((hub_n, 4), np.float32),
+                   np.zeros((hub_n, 4), np.float32), np.full(hub_n, 22, np.uint8),
+                   np.array([0, hub_n - 1], np.int64),
+                   np.stack([np.zeros(hub_n - 1), np.arange(1, hub_n)], 1).astype(np.uint16),
+                   np.full(hub_n - 1, 22, np.uint8), np.full(hub_n - 1, 0.1, np.float32))
+    hub.pos[:, 0] = np.linspace(0.0, 1.0, hub_n, dtype=np.float32)
+    hub.pos[:, 3] = 1.0
+    nan = mb.Batch(**{k: getattr(good, k) for k in ("mass_offsets", "pos", "vel", "mass_material",
+                                                    "spring_offsets", "pairs", "spring_material", "lbar")})
+    nan.pos = good.pos.copy()
+    nan.pos[7, 0] = np.nan
+    for batch, pairs, expect in ((good, bad, 1), (hub, hub.pairs, 3), (nan, nan.pairs, 5)):
+        assert _call(torch, batch, pairs, table_dev) == expect
+        p, v, _, t = _noalloc(torch, good, table_dev, 1e-3, 0.25, 300, False)
+        rp, rv, _, rt = _batched(good, 1e-3, 0.25, 300, False)
+        assert np.array_equal(_bits(p), _bits(rp)) and np.array_equal(_bits(v), _bits(rv)) and t == rt
