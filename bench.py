@@ -56,6 +56,7 @@ WORKLOADS = {
 #   read+write when tracking + per-mass state (pos and vel, 3 floats each,
 #   read and write: 48 B) x masses/springs.
 SMEM_B = 60.0
+SMEM_NOMINAL_B_PER_CLK = 128.0  # shared-memory bandwidth of an SM (32 banks x 4 B per clock)
 HBM_TOPO_B, HBM_STRESS_B, HBM_MASS_B = 9.0, 8.0, 48.0
 
 
@@ -390,6 +391,9 @@ def smem_peak_gbs(device):
     from mercury_b200 import _lib
     bps, bpc = ctypes.c_double(), ctypes.c_double()
     _lib.check(_lib.LIB.mb_measure_smem_bandwidth(device, ctypes.byref(bps), ctypes.byref(bpc)))
+    if bpc.value > 1.05 * SMEM_NOMINAL_B_PER_CLK:
+        raise RuntimeError(f"shared-memory probe measured {bpc.value:.1f} B/clk/SM, above the "
+                           f"{SMEM_NOMINAL_B_PER_CLK:.0f} B/clk/SM the SM can serve: loads were merged")
     return bps.value / 1e9, bpc.value
 
 

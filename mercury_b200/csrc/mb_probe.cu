@@ -34,11 +34,13 @@ smem_read_kernel(uint32_t iters, uint32_t* sink, unsigned long long* cycles) {
     for (uint32_t it = 0; it < iters; ++it) {
 #pragma unroll
         for (int k = 0; k < kUnroll; ++k) {
-            // lanes of a warp: 32 consecutive words; the offset moves each
-            // iteration so the loads cannot be hoisted
-            const uint32_t idx = (tid + (uint32_t)k * kThreads + it * 32u) & (kWords - 1);
+            // lanes of a warp: 32 consecutive words; the 8 loads of an
+            // iteration read 8 distinct words of each thread and the offset
+            // moves each iteration; volatile loads, so that none is merged
+            // with another or hoisted
+            const uint32_t idx = (tid + (uint32_t)k * 128u + it * 32u) & (kWords - 1);
             uint32_t a, b, c, d;
-            asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];"
+            asm volatile("ld.volatile.shared.v4.u32 {%0, %1, %2, %3}, [%4];"
                          : "=r"(a), "=r"(b), "=r"(c), "=r"(d)
                          : "r"(base + idx * 16u));
             acc ^= a ^ b ^ c ^ d;
