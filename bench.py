@@ -637,15 +637,17 @@ def build_bench(local_rank):
 
 
 DEVO_ROBOTS, DEVO_K = 512, 128
-SG_CHILDREN, SG_WARMUP_BATCHES = 4096, 13
+SG_CHILDREN, SG_WARMUP_BATCHES, SG_RACE_S = 4096, 13, 4.0
 
 
 def surrogate_bench(local_rank, generations: int = 8, plain_generations: int = 3, seed: int = 0):
     """Surrogate-screened evolution (4096 children of 6x6x6 voxel genomes
     per generation; the surrogate's top 25% plus a 5% random audit are
     simulated for 1 s on land) against plain evolution (all 4096
-    simulated), after a warm-up of 13 x 4096 = 53,248 simulated random
-    genomes.  Generations/s from host wall time per generation (children,
+    simulated), after a warm-up of 13 x 4096 = 53,248 simulated genomes
+    (3 random batches, then plain-evolution children).  First a race: both
+    methods from the warm-up's pool for the same wall-time budget (best
+    fitness against time).  Generations/s from host wall time per generation (children,
     screening, device builds, simulation, online training) over timed
     generations after one untimed warm-up generation per method; the screen's
     quality from every child of the screened generations also simulated,
@@ -658,6 +660,17 @@ def surrogate_bench(local_rank, generations: int = 8, plain_generations: int = 3
     scr = evolve.ScreenedEvolution(ev, sg, seed=seed + 1, children=SG_CHILDREN)
     warm = scr.warmup(SG_WARMUP_BATCHES * SG_CHILDREN, batch=SG_CHILDREN)
     plain = evolve.PlainEvolution(ev, seed=seed + 2, children=SG_CHILDREN, pool=copy.deepcopy(scr.pool))
+    # best fitness against wall time, both from the pool the warm-up left,
+    # for the same budget (one untimed generation each first: a new batch
+    # size plans its packing once)
+    rs = evolve.ScreenedEvolution(ev, sg, seed=seed + 3, children=SG_CHILDREN)
+    rs.data, rs.pool, rs.mu, rs.sd = scr.data, copy.deepcopy(scr.pool), scr.mu, scr.sd
+    rp = evolve.PlainEvolution(ev, seed=seed + 4, children=SG_CHILDREN, pool=copy.deepcopy(scr.pool))
+    start_best = float(scr.pool.fitness[0])
+    curves = evolve.race({"screened": rs, "plain": rp}, SG_RACE_S)
+    race = {"budget_s": SG_RACE_S, "start_best": start_best, "curves": curves,
+            "best_at_budget": {k: evolve.best_at(v, SG_RACE_S) for k, v in curves.items()},
+            "note": "both from the warm-up's elite pool; elapsed = sum of generation wall times"}
     # one untimed generation per method first: a new batch size plans its
     # packing once (warm-up, like the headline's warm-up steps)
     warm_s = scr.generation(truth=True)
@@ -673,6 +686,7 @@ def surrogate_bench(local_rank, generations: int = 8, plain_generations: int = 3
             "per_generation": [{k: round(v, 4) for k, v in g.items()} for g in gens],
             "plain_per_generation": [{k: round(v, 4) for k, v in g.items()} for g in pgens],
             "best_fitness": {"screened": gens[-1]["best"], "plain": pgens[-1]["best"]},
+            "race": race,
             "warmup": warm, "warmup_generation_s": {"screened": warm_s["wall_s"], "plain": warm_p["wall_s"]},
             "simulated_per_generation": {"screened": gens[0]["simulated"],
                                                          "plain": pgens[0]["simulated"]},

@@ -46,3 +46,61 @@ def test_quality_metrics():
     assert q["spearman"] == pytest.approx(1.0) and q["top10_recall"] == 1.0 and q["top10_recall_top10"] == 1.0
     q = evolve.quality(-truth, truth, np.arange(0, 10), 0.25)
     assert q["top10_recall"] == 0.0 and q["random_screen_recall"] == 0.1
+
+
+class _FakeEvaluator:
+    """Fitness = share of muscle voxels (classes 3, 4): a stand-in for the
+    simulator in host-logic tests."""
+
+    def __init__(self):
+        self.calls = []
+
+    def __call__(self, g):
+        self.calls.append(np.array(g, copy=True))
+        return ((g >= 3).mean(1)).astype(np.float32)
+
+
+class _FakeSurrogate:
+    def __init__(self):
+        self.steps = 0
+
+    def predict(self, g):
+        return ((g >= 3).mean(1) - 0.4).astype(np.float32)
+
+    def train_step(self, g, t, lr):
+        self.steps += 1
+        return 0.0
+
+
+def test_warmup_draws_random_batches_then_children_of_the_pool():
+    ev = _FakeEvaluator()
+    scr = evolve.ScreenedEvolution(ev, _FakeSurrogate(), seed=0, children=256, batch=64)
+    w = scr.warmup(5 * 256, batch=256, epochs=1.0, random_batches=2)
+    assert w["robots"] == 1280 and w["random_batches"] == 2 and len(ev.calls) == 5
+    # children of an elite pool of muscle-rich genomes are muscle-richer than
+    # random genomes (random: 0.35 on average)
+    rand_share = np.mean([(c >= 3).mean() for c in ev.calls[:2]])
+    kid_share = np.mean([(c >= 3).mean() for c in ev.calls[2:]])
+    assert abs(rand_share - 0.35) < 0.02 and kid_share > rand_share + 0.05
+    # all random when asked
+    ev2 = _FakeEvaluator()
+    evolve.ScreenedEvolution(ev2, _FakeSurrogate(), seed=0, children=256, batch=64).warmup(
+        3 * 256, batch=256, epochs=1.0, random_batches=None)
+    assert all(abs((c >= 3).mean() - 0.35) < 0.03 for c in ev2.calls)
+
+
+def test_race_gives_each_method_the_same_budget():
+    class Steady:
+        def __init__(self, dt, gain):
+            self.dt, self.gain, self.best = dt, gain, 0.0
+
+        def generation(self):
+            self.best += self.gain
+            return {"wall_s": self.dt, "best": self.best}
+
+    curves = evolve.race({"fast": Steady(0.25, 0.1), "slow": Steady(1.0, 0.3)}, 2.0)
+    assert [t for t, _ in curves["fast"]] == [0.25, 0.5, 0.75, 1.0, 1.25, 1.5, 1.75, 2.0]
+    assert [t for t, _ in curves["slow"]] == [1.0, 2.0]
+    assert evolve.best_at(curves["fast"], 2.0) == pytest.approx(0.8)
+    assert evolve.best_at(curves["slow"], 2.0) == pytest.approx(0.6)
+    assert evolve.best_at(curves["slow"], 0.5) == float("-inf")
