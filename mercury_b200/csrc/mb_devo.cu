@@ -242,7 +242,14 @@ __global__ void relayout_kernel(const BinDesc* __restrict__ old_bins, const uint
     for (size_t i = threadIdx.x; i < (size_t)bd.n_inc * eb; i += blockDim.x) dst[to + i] = src[from + i];
 }
 
-__device__ __forceinline__ uint32_t row_other(unsigned long long e) { return (uint32_t)(e >> 52); }
+// Row entries while rebuilding: key of the other end << 47 | spring index
+// (upload order) << 16 | (1 at the b end) << 15 | packed slot in the bin.
+// The key is the bin-local index of a resident bin's mass (robots are
+// contiguous and in order inside a bin) and the robot-local index in a split
+// part (whose halo masses are numbered after its own), so sorting entries
+// sorts every row into the summation order (other end, spring, a end first).
+constexpr uint32_t kKeyOffset = 1u << 16;  // keys are < 65536
+__device__ __forceinline__ uint32_t row_other(unsigned long long e) { return (uint32_t)(e >> 47); }
 
 // Exclusive scan of v[0..n) in place (n <= kRebuildMaxMass); returns the total.
 __device__ uint32_t block_scan(uint32_t* v, uint32_t n, uint32_t* warp_tot) {
@@ -294,24 +301,28 @@ __global__ void __launch_bounds__(kRebuildThreads) rebuild_kernel(const RebuildP
     const uint32_t b = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const BinDesc bd = p.bins[b];
     const uint32_t nm = bd.n_mass, ns = bd.n_spring, cap = bd.row_cap;
+    // split parts: keys of their local masses (own, then halo); resident
+    // bins: the local index itself
+    const uint32_t* keys = p.keys ? p.keys + p.key_begin[b] : nullptr;
+    auto key_of = [&](uint32_t local) { return keys ? keys[local] : local; };
     if (tid == 0) {  // the free list after this call's takes
         const uint32_t c = p.free_count[b], t = p.free_taken[b];
         p.free_count[b] = c - min(t, c);
         p.free_taken[b] = 0;
     }
-    if (nm > kRebuildMaxMass || ns >= (1u << 20)) {
+    if (nm > kRebuildMaxMass || ns > kMaxBinSprings) {
         if (tid == 0) atomicAdd(&p.status[0], 1u);
         return;
     }
-    // 1. degrees
+    // 1. degrees (rows exist for the bin's own masses only)
     for (uint32_t i = tid; i < nm; i += kRebuildThreads) start[i] = 0;
     __syncthreads();
     for (uint32_t j = tid; j < ns; j += kRebuildThreads) {
         const uint32_t q = bd.spring_begin + j;
         if (p.spring_gidx[q] == p.inert) continue;
-        const uint32_t w = p.spring_pair[q];
-        atomicAdd(&start[w & 0xFFFu], 1u);
-        atomicAdd(&start[(w >> 12) & 0xFFFu], 1u);
+        const uint32_t w = p.spring_pair[q], a = w & 0xFFFu, c = (w >> 12) & 0xFFFu;
+        if (a < nm) atomicAdd(&start[a], 1u);
+        if (c < nm) atomicAdd(&start[c], 1u);
     }
     __syncthreads();
     // 2. row starts
@@ -319,15 +330,15 @@ __global__ void __launch_bounds__(kRebuildThreads) rebuild_kernel(const RebuildP
     if (tid == 0) start[nm] = n_ent;
     for (uint32_t i = tid; i < nm; i += kRebuildThreads) cur[i] = start[i];
     __syncthreads();
-    // 3. entries: other end << 52 | spring << 21 | (b end) << 20 | packed slot
+    // 3. entries: key of the other end << 47 | spring << 16 | (b end) << 15 | packed slot
     unsigned long long* rows = p.rows + 2ull * bd.spring_begin;
     for (uint32_t j = tid; j < ns; j += kRebuildThreads) {
-        const uint32_t q = bd.spring_begin + j, g = p.spring_gidx[q];
-        if (g == p.inert) continue;
+        const uint32_t q = bd.spring_begin + j, gw = p.spring_gidx[q];
+        if (gw == p.inert) continue;
         const uint32_t w = p.spring_pair[q], a = w & 0xFFFu, c = (w >> 12) & 0xFFFu;
-        const unsigned long long sg = (unsigned long long)g << 21;
-        rows[atomicAdd(&cur[a], 1u)] = ((unsigned long long)c << 52) | sg | j;
-        rows[atomicAdd(&cur[c], 1u)] = ((unsigned long long)a << 52) | sg | (1ull << 20) | j;
+        const unsigned long long sg = (unsigned long long)(gw & 0x7FFFFFFFu) << 16;  // bit 31: a split copy
+        if (a < nm) rows[atomicAdd(&cur[a], 1u)] = ((unsigned long long)key_of(c) << 47) | sg | j;
+        if (c < nm) rows[atomicAdd(&cur[c], 1u)] = ((unsigned long long)key_of(a) << 47) | sg | (1ull << 15) | j;
     }
     __syncthreads();
     // 4. summation order within each row
@@ -375,7 +386,8 @@ __global__ void __launch_bounds__(kRebuildThreads) rebuild_kernel(const RebuildP
         if (aligned) {
             uint32_t h = r0;
             while (true) {
-                const uint32_t head = h < r1 ? row_other(rows[h]) + kRebuildMaxMass - i : 0xFFFFFFFFu;
+                const uint32_t head =
+                    h < r1 ? row_other(rows[h]) + kKeyOffset - (i < nm ? key_of(i) : 0u) : 0xFFFFFFFFu;
                 const uint32_t m = __reduce_min_sync(0xffffffffu, head);
                 if (m == 0xFFFFFFFFu) break;
                 if (head == m) ++h;
@@ -418,7 +430,7 @@ __global__ void __launch_bounds__(kRebuildThreads) rebuild_kernel(const RebuildP
         const bool aligned = (swidth[sl] & 0x80000000u) != 0;
         const uint32_t base = bd.inc_begin + soff[sl] + lane;
         auto put = [&](uint32_t col, unsigned long long e) {
-            const uint32_t v = ((uint32_t)(e & 0xFFFFFu) << 1) | (uint32_t)((e >> 20) & 1u);
+            const uint32_t v = ((uint32_t)(e & 0x7FFFu) << 1) | (uint32_t)((e >> 15) & 1u);
             if (p.streamed)
                 p.inc32[base + col * kSliceWidth] = v;
             else
@@ -428,7 +440,7 @@ __global__ void __launch_bounds__(kRebuildThreads) rebuild_kernel(const RebuildP
             uint32_t h = r0, col = 0;
             while (true) {
                 const unsigned long long e = h < r1 ? rows[h] : 0ull;
-                const uint32_t head = h < r1 ? row_other(e) + kRebuildMaxMass - i : 0xFFFFFFFFu;
+                const uint32_t head = h < r1 ? row_other(e) + kKeyOffset - key_of(i) : 0xFFFFFFFFu;
                 const uint32_t m = __reduce_min_sync(0xffffffffu, head);
                 if (m == 0xFFFFFFFFu) break;
                 if (head == m) {
@@ -443,12 +455,281 @@ __global__ void __launch_bounds__(kRebuildThreads) rebuild_kernel(const RebuildP
     }
     if (tid == 0) {
         p.bins[b].n_inc = n_inc;
-        if (!p.streamed)
+        if (keys)
+            atomicMax(&p.status[1], split_smem_bytes(bd.x_stride, ns, n_inc, bd.n_export));
+        else if (!p.streamed)
             atomicMax(&p.status[1], bin_smem_bytes_dev(nm, ns, n_inc) + face_smem_bytes(nm, bd.n_face, bd.n_face_inc));
     }
 }
 
+// --- development of split robots -------------------------------------------
+
+constexpr uint32_t kPending = 0xFFFFFFFEu;  // map: a halo mass a part needs, not numbered yet
+constexpr uint32_t kSplitThreads = 256;
+
+__device__ __forceinline__ uint32_t part_of_mass(const SplitDevoParams& p, uint32_t r, uint32_t m) {
+    return p.part_of[p.mass_off[r] + m];
+}
+
+// Own masses of each bin into its map and keys; the spring slots beyond the
+// packed ones become the free list (the lowest slot last, so taken first).
+__global__ void __launch_bounds__(kSplitThreads) split_setup_bins_kernel(const SplitDevoParams p) {
+    const uint32_t b = blockIdx.x, tid = threadIdx.x;
+    const uint32_t r = p.bin_robot[b];
+    const BinDesc bd = p.bins[b];
+    const uint32_t cap = p.spring_cap[b];
+    const uint32_t n_free = cap - bd.n_spring;
+    for (uint32_t i = tid; i < n_free; i += kSplitThreads) {
+        const uint32_t slot = cap - 1 - i, q = bd.spring_begin + slot;
+        p.free_slots[bd.spring_begin + i] = slot;
+        p.spring_gidx[q] = p.inert;
+        p.spring_pair[q] = 0;
+        p.spring_lbar[q] = 0.0f;
+    }
+    if (tid == 0) {
+        p.free_count[b] = n_free;
+        p.free_taken[b] = 0;
+    }
+    if (r == kNoSlot) return;
+    const int64_t m0 = p.mass_off[r];
+    uint32_t* map = p.map + p.map_begin[b];
+    uint32_t* keys = p.keys + p.key_begin[b];
+    for (uint32_t i = tid; i < bd.n_mass; i += kSplitThreads) {
+        const uint32_t m = (uint32_t)(p.mass_gidx[bd.mass_begin + i] - m0);
+        map[m] = i;
+        keys[i] = m;
+    }
+}
+
+// Halo masses of every bin from the export lists of the parts that own them.
+__global__ void __launch_bounds__(kSplitThreads) split_setup_halo_kernel(const SplitDevoParams p) {
+    const uint32_t q = blockIdx.x, tid = threadIdx.x;
+    const uint32_t r = p.bin_robot[q];
+    if (r == kNoSlot) return;
+    const BinDesc bd = p.bins[q];
+    const int64_t m0 = p.mass_off[r];
+    const uint32_t cluster_first = p.robot_bin[r] - p.robot_slot0[r];
+    for (uint32_t i = tid; i < bd.n_export; i += kSplitThreads) {
+        const uint32_t e = p.exports[bd.export_begin + i];
+        const uint32_t li = e & 0xFFFu, rank = (e >> 12) & 7u, slot = e >> 15;
+        const uint32_t dst = cluster_first + rank;
+        if (dst >= p.n_bins || p.bin_robot[dst] != r || li >= bd.n_mass) {
+            atomicAdd(&p.status[0], 1u);
+            continue;
+        }
+        const uint32_t m = (uint32_t)(p.mass_gidx[bd.mass_begin + li] - m0);
+        p.map[p.map_begin[dst] + m] = slot;
+        p.keys[p.key_begin[dst] + slot] = m;
+    }
+}
+
+// The slot of every spring in the part of each of its ends.
+__global__ void __launch_bounds__(kSplitThreads) split_setup_slots_kernel(const SplitDevoParams p) {
+    const uint32_t b = blockIdx.x, tid = threadIdx.x;
+    const uint32_t r = p.bin_robot[b];
+    if (r == kNoSlot) return;
+    const BinDesc bd = p.bins[b];
+    const uint32_t part = b - p.robot_bin[r];
+    for (uint32_t j = tid; j < bd.n_spring; j += kSplitThreads) {
+        const uint32_t gw = p.spring_gidx[bd.spring_begin + j];
+        if (gw == p.inert) continue;
+        const uint32_t g = gw & 0x7FFFFFFFu;
+        const uint32_t a = p.pairs[2 * (size_t)g], c = p.pairs[2 * (size_t)g + 1];
+        if (part_of_mass(p, r, a) == part) p.slot_a[g] = j;
+        if (part_of_mass(p, r, c) == part) p.slot_b[g] = j;
+    }
+}
+
+// Pass 0 frees the slots of parts a spring leaves (it becomes air, or no end
+// stays in the part); pass 1 keeps or takes a slot in every part that holds
+// one of its new ends and marks the halo masses those parts now need.
+__global__ void split_apply_kernel(const SplitDevoParams p, int pass) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.n_rec) return;
+    const DevoRecord rec = p.rec[i];
+    if (rec.spring == 0xFFFFFFFFu) return;
+    const uint32_t g = rec.spring, r = i / p.k, fb = p.robot_bin[r];
+    const uint32_t a0 = p.pairs[2 * (size_t)g], b0 = p.pairs[2 * (size_t)g + 1], mo = p.spring_mat[g];
+    const uint32_t a1 = rec.pair & 0xFFFFu, b1 = rec.pair >> 16, mn = rec.material;
+    const uint32_t pa0 = part_of_mass(p, r, a0), pb0 = part_of_mass(p, r, b0);
+    const uint32_t pa1 = part_of_mass(p, r, a1), pb1 = part_of_mass(p, r, b1);
+    const uint32_t sa = p.slot_a[g], sb = p.slot_b[g];
+    auto in_old = [&](uint32_t q) { return mo != 0 && (q == pa0 || q == pb0); };
+    auto in_new = [&](uint32_t q) { return mn != 0 && (q == pa1 || q == pb1); };
+    auto old_slot = [&](uint32_t q) { return q == pa0 ? sa : sb; };
+    if (pass == 0) {
+        const uint32_t qs[2] = {pa0, pb0};
+        for (int k = 0; k < 2; ++k) {
+            const uint32_t q = qs[k];
+            if (mo == 0 || (k == 1 && q == pa0) || in_new(q)) continue;
+            const uint32_t slot = old_slot(q), bin = fb + q;
+            if (slot == kNoSlot) {
+                atomicAdd(&p.status[0], 1u);
+                continue;
+            }
+            const uint32_t first = p.bins[bin].spring_begin;
+            p.spring_gidx[first + slot] = p.inert;
+            p.free_slots[first + atomicAdd(&p.free_count[bin], 1u)] = slot;
+        }
+        return;
+    }
+    uint32_t nsa = kNoSlot, nsb = kNoSlot;
+    if (mn != 0) {
+        const uint32_t qs[2] = {pa1, pb1};
+        for (int k = 0; k < 2; ++k) {
+            const uint32_t q = qs[k];
+            if (k == 1 && q == pa1) {
+                nsb = nsa;
+                continue;
+            }
+            const uint32_t bin = fb + q;
+            uint32_t slot;
+            if (in_old(q)) {
+                slot = old_slot(q);
+            } else {
+                const uint32_t t = atomicAdd(&p.free_taken[bin], 1u), c = p.free_count[bin];
+                if (t >= c) {
+                    atomicAdd(&p.status[0], 1u);
+                    slot = kNoSlot;
+                } else {
+                    slot = p.free_slots[p.bins[bin].spring_begin + c - 1 - t];
+                }
+            }
+            (k == 0 ? nsa : nsb) = slot;
+            // ends the part does not own join its halo
+            uint32_t* map = p.map + p.map_begin[bin];
+            if (pa1 != q) atomicCAS(&map[a1], kNoSlot, kPending);
+            if (pb1 != q) atomicCAS(&map[b1], kNoSlot, kPending);
+        }
+    }
+    p.slot_a[g] = nsa;
+    p.slot_b[g] = nsb;
+}
+
+// Numbers the halo masses each bin now needs (after its local masses, in
+// robot order) and appends their export entries to the parts that own them.
+__global__ void __launch_bounds__(kSplitThreads) split_halo_kernel(const SplitDevoParams p) {
+    __shared__ uint32_t warp_cnt[kSplitThreads / 32];
+    __shared__ uint32_t s_base;
+    const uint32_t b = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t r = p.bin_robot[b];
+    if (r == kNoSlot) return;
+    const uint32_t fb = p.robot_bin[r], rank = p.robot_slot0[r] + (b - fb);
+    const uint32_t nm = (uint32_t)(p.mass_off[r + 1] - p.mass_off[r]);
+    const uint32_t cap_x = p.bins[b].x_stride;
+    uint32_t* map = p.map + p.map_begin[b];
+    uint32_t* keys = p.keys + p.key_begin[b];
+    if (tid == 0) s_base = p.bins[b].n_all;
+    __syncthreads();
+    for (uint32_t base = 0; base < nm; base += kSplitThreads) {
+        const uint32_t m = base + tid;
+        const bool need = m < nm && map[m] == kPending;
+        const uint32_t bal = __ballot_sync(0xffffffffu, need);
+        if (lane == 0) warp_cnt[warp] = __popc(bal);
+        __syncthreads();
+        uint32_t before = 0, total = 0;
+        for (uint32_t w = 0; w < kSplitThreads / 32; ++w) {
+            before += w < warp ? warp_cnt[w] : 0u;
+            total += warp_cnt[w];
+        }
+        const uint32_t local = s_base + before + __popc(bal & ((1u << lane) - 1u));
+        if (need) {
+            if (local >= cap_x) {
+                atomicAdd(&p.status[0], 1u);
+                map[m] = kNoSlot;
+            } else {
+                map[m] = local;
+                keys[local] = m;
+                const uint32_t ob = fb + part_of_mass(p, r, m);
+                const uint32_t li = p.map[p.map_begin[ob] + m];
+                const uint32_t x = atomicAdd(&p.bins[ob].n_export, 1u);
+                if (li >= 4096u || x >= p.export_cap[ob])
+                    atomicAdd(&p.status[0], 1u);
+                else
+                    p.exports[p.bins[ob].export_begin + x] = li | (rank << 12) | (local << 15);
+            }
+        }
+        __syncthreads();
+        if (tid == 0) s_base += total;
+        __syncthreads();
+    }
+    if (tid == 0) p.bins[b].n_all = min(s_base, cap_x);
+}
+
+// Writes the packed springs of every part holding a new end, then the
+// canonical topology.
+__global__ void split_write_kernel(const SplitDevoParams p) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.n_rec) return;
+    const DevoRecord rec = p.rec[i];
+    if (rec.spring == 0xFFFFFFFFu) return;
+    const uint32_t g = rec.spring, r = i / p.k, fb = p.robot_bin[r];
+    const uint32_t a1 = rec.pair & 0xFFFFu, b1 = rec.pair >> 16, mn = rec.material;
+    if (mn != 0) {
+        const uint32_t pa1 = part_of_mass(p, r, a1), pb1 = part_of_mass(p, r, b1);
+        const uint32_t ms = p.slot_of[mn];
+        const uint32_t qs[2] = {pa1, pb1}, slots[2] = {p.slot_a[g], p.slot_b[g]};
+        for (int k = 0; k < 2; ++k) {
+            const uint32_t q = qs[k];
+            if (k == 1 && q == pa1) continue;
+            const uint32_t bin = fb + q, slot = slots[k];
+            const uint32_t* map = p.map + p.map_begin[bin];
+            const uint32_t la = map[a1], lb = map[b1], cap_x = p.bins[bin].x_stride;
+            if (slot == kNoSlot || ms == kNoMatSlot || la >= cap_x || lb >= cap_x) {
+                atomicAdd(&p.status[0], 1u);
+                continue;
+            }
+            const uint32_t at = p.bins[bin].spring_begin + slot;
+            p.spring_pair[at] = la | (lb << 12) | (ms << 24);
+            p.spring_lbar[at] = rec.lbar;
+            p.spring_gidx[at] = g | (q != pa1 ? 0x80000000u : 0u);  // the part of the a end writes the stress
+            atomicMax(&p.bins[bin].n_spring, slot + 1);
+        }
+    }
+    p.pairs[2 * (size_t)g] = (uint16_t)a1;
+    p.pairs[2 * (size_t)g + 1] = (uint16_t)b1;
+    p.spring_mat[g] = (uint8_t)mn;
+    p.lbar[g] = rec.lbar;
+}
+
+__global__ void relayout_ranges_kernel(const uint32_t* __restrict__ old_begin, const uint32_t* __restrict__ count,
+                                       const uint32_t* __restrict__ new_begin, const uint8_t* __restrict__ src,
+                                       uint8_t* __restrict__ dst, uint32_t eb) {
+    const size_t from = (size_t)old_begin[blockIdx.x] * eb, to = (size_t)new_begin[blockIdx.x] * eb;
+    for (size_t i = threadIdx.x; i < (size_t)count[blockIdx.x] * eb; i += blockDim.x) dst[to + i] = src[from + i];
+}
+
 }  // namespace
+
+cudaError_t launch_split_devo_setup(const SplitDevoParams& p, uint32_t n_bins, uint32_t n_springs, cudaStream_t s) {
+    if (n_bins == 0) return cudaSuccess;
+    cudaError_t e = cudaMemsetAsync(p.slot_a, 0xFF, (size_t)n_springs * sizeof(uint32_t), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(p.slot_b, 0xFF, (size_t)n_springs * sizeof(uint32_t), s);
+    if (e != cudaSuccess) return e;
+    split_setup_bins_kernel<<<n_bins, kSplitThreads, 0, s>>>(p);
+    split_setup_halo_kernel<<<n_bins, kSplitThreads, 0, s>>>(p);
+    split_setup_slots_kernel<<<n_bins, kSplitThreads, 0, s>>>(p);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_split_devo_apply(const SplitDevoParams& p, uint32_t n_bins, cudaStream_t s) {
+    if (p.n_rec == 0) return cudaSuccess;
+    const uint32_t grid = (p.n_rec + 255) / 256;
+    split_apply_kernel<<<grid, 256, 0, s>>>(p, 0);
+    split_apply_kernel<<<grid, 256, 0, s>>>(p, 1);
+    split_halo_kernel<<<n_bins, kSplitThreads, 0, s>>>(p);
+    split_write_kernel<<<grid, 256, 0, s>>>(p);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_relayout_ranges(const uint32_t* old_begin, const uint32_t* count, const uint32_t* new_begin,
+                                   uint32_t n_bins, const void* src, void* dst, uint32_t entry_bytes,
+                                   cudaStream_t s) {
+    if (n_bins == 0) return cudaSuccess;
+    relayout_ranges_kernel<<<n_bins, 256, 0, s>>>(old_begin, count, new_begin, static_cast<const uint8_t*>(src),
+                                                  static_cast<uint8_t*>(dst), entry_bytes);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_build_pslot(const uint32_t* spring_gidx, uint32_t n_packed, uint32_t n_springs,
                                uint32_t* pslot, cudaStream_t s) {

@@ -86,6 +86,10 @@ struct RebuildParams {
     uint32_t* free_count;
     uint32_t* free_taken;
     uint32_t* status;
+    // split parts: per bin the first entry of its key table (robot-local
+    // index of every local mass); nullptr for resident and streamed bins
+    const uint32_t* keys;
+    const uint32_t* key_begin;
 };
 
 // Canonical spring -> packed slot map from spring_gidx (n_packed slots).
@@ -99,7 +103,71 @@ cudaError_t launch_devo_apply(const DevoApplyParams& p, int pass, cudaStream_t s
 cudaError_t launch_relayout(const BinDesc* old_bins, const uint32_t* new_begin, uint32_t n_bins,
                             const void* src, void* dst, uint32_t entry_bytes, cudaStream_t s);
 // Rebuilds every bin's rows; status[1] gets the largest shared memory a
-// resident bin needs.
+// bin needs.
 cudaError_t launch_rebuild(const RebuildParams& p, cudaStream_t s);
+
+// ---------------------------------------------------------------------------
+// Development of robots split over thread-block clusters (one part per bin).
+// The partition of each robot's masses into parts stays as packed; after the
+// records are applied, every spring is in the parts that hold one of its
+// ends, every part holds as halo the other parts' masses its springs reach,
+// and every part exports those of its masses that other parts hold.
+//
+// Per bin, regions with spare capacity are set up once (first development
+// of a split population): spring slots (spring_cap; unused ones on the free
+// list), export entries (export_cap), local masses (x_stride: own, then halo),
+// and the local index of every robot mass in the bin (map: kNoSlot when the
+// bin does not hold it).  Springs keep their slots as long as they stay in a
+// part; halo masses are appended (never renumbered); rows are rebuilt by
+// rebuild_kernel keyed by robot-local index.  Anything that does not fit is
+// counted in status[0] and the host re-packs instead.
+struct SplitDevoParams {
+    const DevoRecord* rec;
+    uint32_t n_rec;
+    uint32_t k;                    // records per robot
+    uint32_t n_bins;
+    uint16_t* pairs;               // canonical topology, upload order
+    uint8_t* spring_mat;
+    float* lbar;
+    const int64_t* mass_off;       // n_robots + 1
+    const uint8_t* part_of;        // per mass (upload order): its part
+    const uint32_t* robot_bin;     // bin of each robot's part 0
+    const uint32_t* robot_parts;
+    const uint32_t* robot_slot0;   // cluster rank of each robot's part 0
+    const uint32_t* bin_robot;     // robot of each bin (kNoSlot: empty bin)
+    const uint32_t* mass_gidx;     // packed own mass -> upload index
+    const uint8_t* slot_of;        // composite id -> material slot, or kNoMatSlot
+    BinDesc* bins;
+    uint32_t* spring_pair;         // packed
+    float* spring_lbar;
+    uint32_t* spring_gidx;
+    uint32_t inert;                // spring_gidx of an inert slot
+    uint32_t* slot_a;              // per spring: bin-relative slot in the part of its a end
+    uint32_t* slot_b;              // ... of its b end (the same slot when both are in one part)
+    const uint32_t* spring_cap;    // per bin
+    const uint32_t* export_cap;    // per bin
+    uint32_t* exports;
+    uint32_t* map;                 // per bin, per robot mass: local index, kNoSlot, or kPending
+    const uint32_t* map_begin;     // per bin
+    uint32_t* keys;                // per bin, per local mass: robot-local index
+    const uint32_t* key_begin;     // per bin
+    uint32_t* free_count;          // per bin
+    uint32_t* free_taken;          // per bin
+    uint32_t* free_slots;          // per bin, spring_cap entries from spring_begin
+    uint32_t* status;              // [0] problems
+};
+
+// One-time set-up of a split population's development state (maps, keys,
+// slots, free lists) from its packed arrays.
+cudaError_t launch_split_devo_setup(const SplitDevoParams& p, uint32_t n_bins, uint32_t n_springs, cudaStream_t s);
+// Applies the records: frees slots of parts a spring leaves, takes slots in
+// parts it joins, appends halo masses and exports, writes the packed springs
+// and the canonical topology.
+cudaError_t launch_split_devo_apply(const SplitDevoParams& p, uint32_t n_bins, cudaStream_t s);
+// Moves per-bin ranges [old_begin, old_begin + count) to new_begin (entries
+// of entry_bytes bytes).
+cudaError_t launch_relayout_ranges(const uint32_t* old_begin, const uint32_t* count, const uint32_t* new_begin,
+                                   uint32_t n_bins, const void* src, void* dst, uint32_t entry_bytes,
+                                   cudaStream_t s);
 
 }  // namespace mb

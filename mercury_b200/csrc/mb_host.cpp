@@ -191,6 +191,15 @@ struct mb_context {
     mb::DevBuf<float> d_lbar;
     mb::DevBuf<uint32_t> pslot, robot_mass_base, free_count, free_taken, free_slots, devo_status, new_begin;
     mb::DevBuf<unsigned long long> rows_scratch;
+    // development of split populations on the device (the partition of the
+    // last packing; regions with spare capacity per bin, set up by the first
+    // mb_devo after an upload)
+    std::vector<uint8_t> h_part_of;
+    std::vector<uint32_t> h_robot_parts, h_robot_slot0, h_robot_bin_first;
+    bool split_devo = false;  // devo_ready holds the split state
+    mb::DevBuf<uint8_t> d_part_of;
+    mb::DevBuf<uint32_t> d_robot_parts, d_robot_slot0, d_bin_robot, sp_spring_cap, sp_export_cap, sp_map,
+        sp_map_begin, sp_keys, sp_key_begin, slot_a, slot_b;
 
     // voxel populations built on the device (mb_set_voxel_population): the
     // template packing of one grid, reused while the key matches
@@ -345,6 +354,11 @@ mb_status upload_packed(mb_context* ctx, const mb::Packed& out, bool* rows_faile
     MB_CUDA(ctx, up(ctx->robot_bin, out.robot_bin.data(), out.robot_bin.size()));
     ctx->h_bins = out.bins;
     ctx->h_robot_mass_base = out.robot_mass_base;
+    ctx->h_part_of = out.part_of;
+    ctx->h_robot_parts = out.robot_parts;
+    ctx->h_robot_slot0 = out.robot_slot0;
+    ctx->h_robot_bin_first = out.robot_bin;
+    ctx->split_devo = false;
     ctx->h_mat_ids = out.mat_ids;
     ctx->n_packed = (uint32_t)out.pair.size();
     ctx->devo_ready = false;
@@ -383,25 +397,16 @@ mb_status upload_packed(mb_context* ctx, const mb::Packed& out, bool* rows_faile
 }
 
 
-// One-time state of device re-packing (first mb_devo after an upload).
-mb_status devo_setup(mb_context* c) {
+// Material slots for every composite development can create: pairs of the
+// base materials the masses carry.  Extra slots only widen the per-launch
+// actuation table.
+mb_status devo_material_slots(mb_context* c) {
     cudaStream_t st = c->stream;
-    const uint64_t S = c->n_spring;
-    const uint32_t nb = c->n_bins, R = c->n_robots;
     auto up = [&](auto& buf, const auto* src, size_t n) -> cudaError_t {
         cudaError_t e = buf.alloc(n);
         if (e != cudaSuccess || n == 0) return e;
         return cudaMemcpyAsync(buf.p, src, n * sizeof(*src), cudaMemcpyHostToDevice, st);
     };
-    MB_CUDA(c, up(c->d_pairs, c->h_pairs.data(), 2 * S));
-    MB_CUDA(c, up(c->d_spring_mat, c->h_spring_mat.data(), S));
-    MB_CUDA(c, up(c->d_lbar, c->h_lbar.data(), S));
-    MB_CUDA(c, c->pslot.alloc(S));
-    MB_CUDA(c, mb::launch_build_pslot(c->spring_gidx.p, c->n_packed, (uint32_t)S, c->pslot.p, st));
-    MB_CUDA(c, up(c->robot_mass_base, c->h_robot_mass_base.data(), R));
-    // Material slots for every composite development can create: pairs of
-    // the base materials the masses carry.  Extra slots only widen the
-    // per-launch actuation table.
     bool base[23] = {};
     for (uint8_t m : c->h_mass_mat) base[m] = true;
     std::vector<uint8_t> slot(256, mb::kNoMatSlot);
@@ -420,6 +425,209 @@ mb_status devo_setup(mb_context* c) {
     MB_CUDA(c, c->invk.alloc(c->n_mat_host));
     MB_CUDA(c, c->rates.alloc((size_t)c->n_mat_host * c->chunk));
     MB_CUDA(c, up(c->slot_of, slot.data(), 256));
+    return MB_OK;
+}
+
+// Whether the split launch groups can still be scheduled with `smem` bytes
+// of shared memory per CTA.
+bool split_schedulable(const mb_context* c, uint32_t smem) {
+    if (mb::max_active_clusters(c->shape, (uint32_t)c->mode, c->cluster, smem) <= 0) return false;
+    return !c->cluster2 || mb::max_active_clusters(c->shape, (uint32_t)c->mode, c->cluster2, smem) > 0;
+}
+
+// Device pointers of the split development state.
+mb::SplitDevoParams split_params(mb_context* c, const mb::DevoRecord* rec, uint32_t n_rec, uint32_t k) {
+    mb::SplitDevoParams p{};
+    p.rec = rec;
+    p.n_rec = n_rec;
+    p.k = k;
+    p.n_bins = c->n_bins;
+    p.pairs = c->d_pairs.p;
+    p.spring_mat = c->d_spring_mat.p;
+    p.lbar = c->d_lbar.p;
+    p.mass_off = c->d_mass_off.p;
+    p.part_of = c->d_part_of.p;
+    p.robot_bin = c->robot_bin.p;
+    p.robot_parts = c->d_robot_parts.p;
+    p.robot_slot0 = c->d_robot_slot0.p;
+    p.bin_robot = c->d_bin_robot.p;
+    p.mass_gidx = c->mass_gidx.p;
+    p.slot_of = c->slot_of.p;
+    p.bins = c->bins.p;
+    p.spring_pair = c->spring_pair.p;
+    p.spring_lbar = c->spring_lbar.p;
+    p.spring_gidx = c->spring_gidx.p;
+    p.inert = (uint32_t)c->n_spring;
+    p.slot_a = c->slot_a.p;
+    p.slot_b = c->slot_b.p;
+    p.spring_cap = c->sp_spring_cap.p;
+    p.export_cap = c->sp_export_cap.p;
+    p.exports = c->exports.p;
+    p.map = c->sp_map.p;
+    p.map_begin = c->sp_map_begin.p;
+    p.keys = c->sp_keys.p;
+    p.key_begin = c->sp_key_begin.p;
+    p.free_count = c->free_count.p;
+    p.free_taken = c->free_taken.p;
+    p.free_slots = c->free_slots.p;
+    p.status = c->devo_status.p;
+    return p;
+}
+
+// One-time state of development on the device for a split population
+// (first mb_devo after an upload): every bin's springs, exports and rows
+// move to regions with spare capacity, its predicted-position buffers get
+// room for more halo masses, and the maps from robot masses to local
+// indices, the key tables and the slots of every spring are built.
+// MB_ERR_CAPACITY: not possible here (faces, limits); the caller re-packs on
+// the host instead.
+mb_status split_devo_setup(mb_context* c) {
+    if (c->faces_packed || c->h_part_of.size() != c->n_mass) return MB_ERR_CAPACITY;
+    cudaStream_t st = c->stream;
+    const uint64_t S = c->n_spring;
+    const uint32_t nb = c->n_bins, R = c->n_robots;
+    auto up = [&](auto& buf, const auto* src, size_t n) -> cudaError_t {
+        cudaError_t e = buf.alloc(std::max<size_t>(n, 1));
+        if (e != cudaSuccess || n == 0) return e;
+        return cudaMemcpyAsync(buf.p, src, n * sizeof(*src), cudaMemcpyHostToDevice, st);
+    };
+    for (uint32_t r = 0; r < R; ++r)
+        if (c->mass_off[r + 1] - c->mass_off[r] >= 65536) return MB_ERR_CAPACITY;
+    MB_CUDA(c, up(c->d_pairs, c->h_pairs.data(), 2 * S));
+    MB_CUDA(c, up(c->d_spring_mat, c->h_spring_mat.data(), S));
+    MB_CUDA(c, up(c->d_lbar, c->h_lbar.data(), S));
+    {
+        const mb_status ms = devo_material_slots(c);
+        if (ms != MB_OK) return ms;
+    }
+    // capacities and new regions
+    const uint32_t smem_max = mb::max_step_smem(c->device);
+    const uint32_t shape_cap = std::min<uint32_t>(c->shape.threads * c->shape.spt, mb::kMaxBinSprings);
+    std::vector<uint32_t> bin_robot(nb, mb::kNoSlot), scap(nb), ecap(nb), kbeg(nb), mbeg(nb);
+    std::vector<uint32_t> old_s(nb), cnt_s(nb), new_s(nb), old_e(nb), cnt_e(nb), new_e(nb);
+    std::vector<uint32_t> new_i(nb);
+    for (uint32_t r = 0; r < R; ++r)
+        for (uint32_t q = 0; q < c->h_robot_parts[r]; ++q) bin_robot[c->h_robot_bin_first[r] + q] = r;
+    std::vector<mb::BinDesc> nbins = c->h_bins;
+    uint64_t ts = 0, te = 0, ti = 0, tk = 0, tm = 0;
+    uint32_t smem = 0;
+    for (uint32_t b = 0; b < nb; ++b) {
+        mb::BinDesc& d = nbins[b];
+        const uint32_t ns = d.n_spring;
+        if (ns > shape_cap) return MB_ERR_CAPACITY;
+        scap[b] = std::max(ns, std::min(shape_cap, ns + std::max(256u, ns / 4)));
+        ecap[b] = d.n_export + 256 + d.n_export / 4;
+        uint32_t xc = bin_robot[b] == mb::kNoSlot ? d.n_all : std::max(d.n_all, std::min(4096u, d.n_all + 128 + d.n_all / 8));
+        while (xc > d.n_all && mb::split_smem_bytes(xc, ns, d.n_inc, d.n_export) > smem_max) --xc;
+        const uint32_t rc = (d.n_inc + d.n_inc / 2 + 8 * mb::kSliceWidth + 31) / 32 * 32;
+        old_s[b] = d.spring_begin;
+        cnt_s[b] = ns;
+        new_s[b] = (uint32_t)ts;
+        old_e[b] = d.export_begin;
+        cnt_e[b] = d.n_export;
+        new_e[b] = (uint32_t)te;
+        new_i[b] = (uint32_t)ti;
+        kbeg[b] = (uint32_t)tk;
+        mbeg[b] = (uint32_t)tm;
+        d.spring_begin = (uint32_t)ts;
+        d.export_begin = (uint32_t)te;
+        d.inc_begin = (uint32_t)ti;
+        d.row_cap = rc;
+        d.x_stride = xc;
+        ts += scap[b];
+        te += ecap[b];
+        ti += rc;
+        tk += xc;
+        if (bin_robot[b] != mb::kNoSlot)
+            tm += (uint64_t)(c->mass_off[bin_robot[b] + 1] - c->mass_off[bin_robot[b]]);
+        smem = std::max(smem, mb::split_smem_bytes(xc, ns, d.n_inc, d.n_export));
+    }
+    if (ts >= (1ull << 31) || te >= (1ull << 31) || ti >= (1ull << 31) || tk >= (1ull << 31) ||
+        tm >= (1ull << 31))
+        return MB_ERR_CAPACITY;
+    if (smem > smem_max || !split_schedulable(c, smem)) return MB_ERR_CAPACITY;
+    // move the packed arrays into the new regions
+    mb::DevBuf<uint32_t> d_old, d_cnt, d_new;
+    auto relayout = [&](auto& buf, const std::vector<uint32_t>& ob, const std::vector<uint32_t>& cn,
+                        const std::vector<uint32_t>& nbg, uint64_t total) -> cudaError_t {
+        using T = std::remove_reference_t<decltype(*buf.p)>;
+        cudaError_t e = up(d_old, ob.data(), nb);
+        if (e == cudaSuccess) e = up(d_cnt, cn.data(), nb);
+        if (e == cudaSuccess) e = up(d_new, nbg.data(), nb);
+        mb::DevBuf<T> fresh;
+        if (e == cudaSuccess) e = fresh.alloc(std::max<uint64_t>(total, 1));
+        if (e == cudaSuccess)
+            e = mb::launch_relayout_ranges(d_old.p, d_cnt.p, d_new.p, nb, buf.p, fresh.p, sizeof(T), st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e == cudaSuccess) {
+            std::swap(buf.p, fresh.p);
+            std::swap(buf.n, fresh.n);
+        }
+        return e;
+    };
+    MB_CUDA(c, relayout(c->spring_pair, old_s, cnt_s, new_s, ts));
+    MB_CUDA(c, relayout(c->spring_lbar, old_s, cnt_s, new_s, ts));
+    MB_CUDA(c, relayout(c->spring_gidx, old_s, cnt_s, new_s, ts));
+    MB_CUDA(c, relayout(c->exports, old_e, cnt_e, new_e, te));
+    {
+        std::vector<uint32_t> old_i(nb), cnt_i(nb);
+        for (uint32_t b = 0; b < nb; ++b) {
+            old_i[b] = c->h_bins[b].inc_begin;
+            cnt_i[b] = c->h_bins[b].n_inc;
+        }
+        MB_CUDA(c, relayout(c->inc, old_i, cnt_i, new_i, ti));
+    }
+    c->h_bins = nbins;
+    MB_CUDA(c, up(c->bins, c->h_bins.data(), nb));
+    MB_CUDA(c, up(c->d_part_of, c->h_part_of.data(), c->h_part_of.size()));
+    MB_CUDA(c, up(c->d_robot_parts, c->h_robot_parts.data(), R));
+    MB_CUDA(c, up(c->d_robot_slot0, c->h_robot_slot0.data(), R));
+    MB_CUDA(c, up(c->d_bin_robot, bin_robot.data(), nb));
+    MB_CUDA(c, up(c->sp_spring_cap, scap.data(), nb));
+    MB_CUDA(c, up(c->sp_export_cap, ecap.data(), nb));
+    MB_CUDA(c, up(c->sp_map_begin, mbeg.data(), nb));
+    MB_CUDA(c, up(c->sp_key_begin, kbeg.data(), nb));
+    MB_CUDA(c, c->sp_map.alloc(std::max<uint64_t>(tm, 1)));
+    MB_CUDA(c, cudaMemsetAsync(c->sp_map.p, 0xFF, std::max<uint64_t>(tm, 1) * sizeof(uint32_t), st));
+    MB_CUDA(c, c->sp_keys.alloc(std::max<uint64_t>(tk, 1)));
+    MB_CUDA(c, cudaMemsetAsync(c->sp_keys.p, 0, std::max<uint64_t>(tk, 1) * sizeof(uint32_t), st));
+    MB_CUDA(c, c->slot_a.alloc(std::max<uint64_t>(S, 1)));
+    MB_CUDA(c, c->slot_b.alloc(std::max<uint64_t>(S, 1)));
+    MB_CUDA(c, c->free_count.alloc(nb));
+    MB_CUDA(c, c->free_taken.alloc(nb));
+    MB_CUDA(c, c->free_slots.alloc(std::max<uint64_t>(ts, 1)));
+    MB_CUDA(c, c->rows_scratch.alloc(2 * std::max<uint64_t>(ts, 1)));
+    MB_CUDA(c, c->devo_status.alloc(2));
+    MB_CUDA(c, mb::launch_split_devo_setup(split_params(c, nullptr, 0, 0), nb, (uint32_t)S, st));
+    MB_CUDA(c, cudaStreamSynchronize(st));
+    c->n_packed = (uint32_t)ts;
+    c->smem_bytes = smem;
+    c->clear_graphs();
+    c->devo_ready = true;
+    c->split_devo = true;
+    return MB_OK;
+}
+
+// One-time state of device re-packing (first mb_devo after an upload).
+mb_status devo_setup(mb_context* c) {
+    cudaStream_t st = c->stream;
+    const uint64_t S = c->n_spring;
+    const uint32_t nb = c->n_bins, R = c->n_robots;
+    auto up = [&](auto& buf, const auto* src, size_t n) -> cudaError_t {
+        cudaError_t e = buf.alloc(n);
+        if (e != cudaSuccess || n == 0) return e;
+        return cudaMemcpyAsync(buf.p, src, n * sizeof(*src), cudaMemcpyHostToDevice, st);
+    };
+    MB_CUDA(c, up(c->d_pairs, c->h_pairs.data(), 2 * S));
+    MB_CUDA(c, up(c->d_spring_mat, c->h_spring_mat.data(), S));
+    MB_CUDA(c, up(c->d_lbar, c->h_lbar.data(), S));
+    MB_CUDA(c, c->pslot.alloc(S));
+    MB_CUDA(c, mb::launch_build_pslot(c->spring_gidx.p, c->n_packed, (uint32_t)S, c->pslot.p, st));
+    MB_CUDA(c, up(c->robot_mass_base, c->h_robot_mass_base.data(), R));
+    {
+        const mb_status ms = devo_material_slots(c);
+        if (ms != MB_OK) return ms;
+    }
     MB_CUDA(c, c->free_count.alloc(nb));
     MB_CUDA(c, c->free_taken.alloc(nb));
     MB_CUDA(c, cudaMemsetAsync(c->free_count.p, 0, nb * sizeof(uint32_t), st));
@@ -1192,11 +1400,17 @@ mb_status mb_devo(mb_context* ctx, uint32_t replaced_per_robot, uint64_t seed, u
         if (s != MB_OK) return s;
     }
     const char* force_host = std::getenv("MB_DEVO_HOST_REPACK");
-    // split robots are re-packed on the host (their parts are planned there)
-    const bool on_device = !(force_host && force_host[0] == '1') && !ctx->cluster;
+    bool on_device = !(force_host && force_host[0] == '1');
+    // split robots keep their partition; their parts are re-derived on the
+    // device (split_devo_setup prepares it once; MB_ERR_CAPACITY there, for
+    // split populations with faces or beyond its limits: host re-pack)
+    const bool split = ctx->cluster != 0;
     if (on_device && !ctx->devo_ready) {
-        const mb_status s = mb_detail::devo_setup(ctx);
-        if (s != MB_OK) return s;
+        const mb_status s = split ? mb_detail::split_devo_setup(ctx) : mb_detail::devo_setup(ctx);
+        if (s == MB_ERR_CAPACITY && split)
+            on_device = false;
+        else if (s != MB_OK)
+            return s;
     }
     const size_t nrec = (size_t)ctx->n_robots * replaced_per_robot;
     MB_CUDA(ctx, ctx->devo_out.alloc(nrec));
@@ -1204,7 +1418,22 @@ mb_status mb_devo(mb_context* ctx, uint32_t replaced_per_robot, uint64_t seed, u
                      ctx->d_table.p, ctx->total_time, replaced_per_robot, seed, flags, ctx->devo_out.p};
     MB_CUDA(ctx, mb::launch_devo(p, ctx->n_robots, st));
     uint32_t status[2] = {0, 0};
-    if (on_device) {
+    if (on_device && split) {
+        MB_CUDA(ctx, cudaMemsetAsync(ctx->devo_status.p, 0, 2 * sizeof(uint32_t), st));
+        MB_CUDA(ctx, mb::launch_split_devo_apply(
+                         mb_detail::split_params(ctx, ctx->devo_out.p, (uint32_t)nrec, replaced_per_robot),
+                         ctx->n_bins, st));
+        mb::RebuildParams rp{ctx->bins.p,        ctx->n_bins,          ctx->spring_pair.p,
+                             ctx->spring_gidx.p, (uint32_t)ctx->n_spring, ctx->slice_off.p,
+                             ctx->slice_width.p, ctx->inc.p,           ctx->inc32.p,
+                             0u,                 ctx->rows_scratch.p,  ctx->free_count.p,
+                             ctx->free_taken.p,  ctx->devo_status.p,   ctx->sp_keys.p,
+                             ctx->sp_key_begin.p};
+        MB_CUDA(ctx, mb::launch_rebuild(rp, st));
+        MB_CUDA(ctx, cudaMemcpyAsync(status, ctx->devo_status.p, sizeof(status), cudaMemcpyDeviceToHost, st));
+        MB_CUDA(ctx, cudaMemcpyAsync(ctx->h_bins.data(), ctx->bins.p, ctx->h_bins.size() * sizeof(mb::BinDesc),
+                                     cudaMemcpyDeviceToHost, st));
+    } else if (on_device) {
         MB_CUDA(ctx, cudaMemsetAsync(ctx->devo_status.p, 0, 2 * sizeof(uint32_t), st));
         mb::DevoApplyParams ap{ctx->devo_out.p,      (uint32_t)nrec,        replaced_per_robot,
                                ctx->d_pairs.p,       ctx->d_spring_mat.p,   ctx->d_lbar.p,
@@ -1241,7 +1470,7 @@ mb_status mb_devo(mb_context* ctx, uint32_t replaced_per_robot, uint64_t seed, u
     const auto t1 = clock::now();
     bool repack = !on_device || status[0] != 0;
     if (!repack && !ctx->streamed && status[1] > ctx->smem_bytes) {
-        if (status[1] > mb::max_step_smem(ctx->device)) {
+        if (status[1] > mb::max_step_smem(ctx->device) || (split && !mb_detail::split_schedulable(ctx, status[1]))) {
             repack = true;
         } else {
             ctx->smem_bytes = status[1];

@@ -1102,6 +1102,9 @@ mb_status pack_population(const mb_batch_desc* b, const PackOptions& o, Packed& 
     }
     out.masses = tot_m;
     out.active_springs = tot_s;
+    out.part_of.clear();
+    out.robot_parts.clear();
+    out.robot_slot0.clear();
     out.n_faces = 0;
     for (const auto& p : packs) out.n_faces += p.n_face;
 
@@ -1216,8 +1219,15 @@ mb_status pack_population(const mb_batch_desc* b, const PackOptions& o, Packed& 
             why = "clusters of " + std::to_string(sp.C) + " CTAs cannot be scheduled on this device";
             return false;
         };
-        auto accept = [&](SplitParts& sp, const KernelShape& sh, uint32_t nb) {
+        auto accept = [&](SplitParts& sp, const KernelShape& sh, uint32_t nb,
+                          const std::vector<std::vector<uint8_t>>& part_of) {
             assemble_split(sp, R, threads, out);
+            // the partition, for re-packing on the device after development
+            out.part_of.resize((size_t)b->mass_offsets[R]);
+            for (uint32_t r = 0; r < R; ++r)
+                std::copy(part_of[r].begin(), part_of[r].end(), out.part_of.begin() + b->mass_offsets[r]);
+            out.robot_parts = sp.parts;
+            out.robot_slot0 = sp.slot0;
             ok = true;
             out.shape = sh;
             out.n_bins = nb;
@@ -1240,7 +1250,7 @@ mb_status pack_population(const mb_batch_desc* b, const PackOptions& o, Packed& 
                 const uint32_t nb = place_split(sp);
                 build_split_parts(b, packs, nb, part_of, slot_of, threads, sp);
                 if (!split_fits(sp, sh, o.smem_cap, why) || !schedulable(sp, sh)) continue;
-                accept(sp, sh, nb);
+                accept(sp, sh, nb, part_of);
                 break;
             }
         // forced (or when the mixed placement fails): every robot in C parts
@@ -1258,7 +1268,7 @@ mb_status pack_population(const mb_batch_desc* b, const PackOptions& o, Packed& 
             build_split_parts(b, packs, R * C, part_of, slot_of, threads, sp);
             for (const auto& sh : compiled) {
                 if (!split_fits(sp, sh, o.smem_cap, why) || !schedulable(sp, sh)) continue;
-                accept(sp, sh, R * C);
+                accept(sp, sh, R * C, part_of);
                 break;
             }
         }

@@ -76,6 +76,10 @@ struct Packed {
     raw_vector<uint16_t> inc;    // resident rows
     raw_vector<uint32_t> inc32;  // streamed rows
     std::vector<uint32_t> exports;  // split bins: own mass | part << 12 | halo slot << 15
+    // split populations: the part of every mass (upload order), and per robot
+    // its part count and the cluster rank of its first part
+    std::vector<uint8_t> part_of;
+    std::vector<uint32_t> robot_parts, robot_slot0;
     // face drag (resident bins): corners {c0 | c1 << 16, c2} per face, row
     // per packed mass (first entry | count << 24), incidence entries; empty
     // when no bin has faces

@@ -400,6 +400,10 @@ struct ConvTcArgs {
     bf16* out_planar;      // [n][4][512][8] or null
     bf16* out_compact;     // [n][216][32] (voxel x + 6y + 36z) or null
     uint32_t* err;
+    // input gradient of a layer (the backward): no bias and no ReLU; the
+    // output keeps the product where the forward activation mask[n][216][32]
+    // (compact) is positive and is zero elsewhere
+    const bf16* mask;
 };
 
 template <int P>
@@ -454,9 +458,18 @@ __global__ void __launch_bounds__(128) conv_tc_kernel(const ConvTcArgs g) {
                          : "r"(acc + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0));
             asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
             alignas(16) bf16 h[8];
+            if (g.mask) {
+                alignas(16) bf16 mk[8];
+                *reinterpret_cast<uint4*>(mk) =
+                    real ? *reinterpret_cast<const uint4*>(g.mask + ((size_t)b * 216 + v) * 32 + c0) : make_uint4(0, 0, 0, 0);
 #pragma unroll
-            for (int j = 0; j < 8; ++j)
-                h[j] = __float2bfloat16_rn(real ? fmaxf(__uint_as_float(r[j]) + g.bias[c0 + j], 0.0f) : 0.0f);
+                for (int j = 0; j < 8; ++j)
+                    h[j] = __float2bfloat16_rn(__bfloat162float(mk[j]) > 0.0f ? __uint_as_float(r[j]) : 0.0f);
+            } else {
+#pragma unroll
+                for (int j = 0; j < 8; ++j)
+                    h[j] = __float2bfloat16_rn(real ? fmaxf(__uint_as_float(r[j]) + g.bias[c0 + j], 0.0f) : 0.0f);
+            }
             const uint4 pk = *reinterpret_cast<const uint4*>(h);
             if (g.out_planar) *reinterpret_cast<uint4*>(g.out_planar + (((size_t)b * 4 + c0 / 8) * 512 + p) * 8) = pk;
             if (g.out_compact && real)
@@ -552,6 +565,29 @@ __global__ void __launch_bounds__(128) conv_tc_kernel(const ConvTcArgs g) {
     if (warp == 0) {
         asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(64u));
+    }
+}
+
+// Compact [n][216][32] (voxel x + 6y + 36z) to padded planar [n][4][512][8]
+// with a zero halo: the layout conv_tc_kernel reads.
+__global__ void planar_from_compact_kernel(const bf16* __restrict__ c, uint32_t n, bf16* __restrict__ x) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n * 4 * 512; i += gridDim.x * blockDim.x) {
+        const uint32_t p = i % 512, plane = (i / 512) % 4, b = i / 2048;
+        const int xx = (int)(p % 8) - 1, yy = (int)((p / 8) % 8) - 1, zz = (int)(p / 64) - 1;
+        uint4 v = make_uint4(0, 0, 0, 0);
+        if (xx >= 0 && xx < 6 && yy >= 0 && yy < 6 && zz >= 0 && zz < 6)
+            v = *reinterpret_cast<const uint4*>(c + ((size_t)b * 216 + xx + 6 * yy + 36 * zz) * 32 + plane * 8);
+        *reinterpret_cast<uint4*>(x + (size_t)i * 8) = v;
+    }
+}
+
+// Weights of the input-gradient convolution of a 32 -> 32 layer:
+// wf[ci][o * 32 + co] = w[co][(26 - o) * 32 + ci] (the transposed kernel,
+// offsets mirrored: offset 26 - o is offset o reflected through the centre).
+__global__ void conv_weight_flip_kernel(const bf16* __restrict__ w, bf16* __restrict__ wf) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < 32 * 27 * 32; i += gridDim.x * blockDim.x) {
+        const uint32_t ci = i / 864, k = i % 864, o = k / 32, co = k % 32;
+        wf[i] = w[co * 864 + (26 - o) * 32 + ci];
     }
 }
 
@@ -804,6 +840,7 @@ struct mb_surrogate {
     int num_sms = 148;
     Buf<uint32_t> tc_err;
     Buf<bf16> x0p, a1p, a2p;  // padded planar activations of the tcgen05 convolutions
+    Buf<bf16> dz3p, dz2p, wf2, wf3;  // backward on tcgen05: planar gradients, mirrored weights
     Buf<float> w, m, v, g, loss, y, t, partial;
     Buf<bf16> wb, wt2, wt3, x0, a1, a2, a3, h1, h2, dz2h, dz1h, dz3, dz2c, dz1c;
     Buf<uint8_t> cls;
@@ -948,8 +985,17 @@ cudaError_t backward(mb_surrogate* s, uint32_t n) {
         if ((e = gemm<kDenseMN, kIm2col>(a, splits_for(R), st)) != cudaSuccess) return e;
     }
     colsum_kernel<<<32, 256, 0, st>>>(s->dz3.p, (uint32_t)R, 32, G(s, kB3));
-    conv_weight_t_kernel<<<108, 256, 0, st>>>(PB(s, kW3), 32, s->wt3.p);
-    {
+    if (s->tcgen05) {
+        // input gradient as the forward convolution of the gradient with the
+        // mirrored, transposed kernel, on tcgen05; masked by a2 > 0
+        planar_from_compact_kernel<<<std::min<uint32_t>((n * 2048 + 255) / 256, 4096), 256, 0, st>>>(s->dz3.p, n,
+                                                                                                      s->dz3p.p);
+        conv_weight_flip_kernel<<<108, 256, 0, st>>>(PB(s, kW3), s->wf3.p);
+        ConvTcArgs c{s->dz3p.p, 4, s->wf3.p, nullptr, (int)n, s->dz2p.p, s->dz2c.p, s->tc_err.p};
+        c.mask = s->a2.p;
+        if ((e = conv_tc<4>(c, s->num_sms, st)) != cudaSuccess) return e;
+    } else {
+        conv_weight_t_kernel<<<108, 256, 0, st>>>(PB(s, kW3), 32, s->wt3.p);
         GemmArgs a = args(s, s->dz3.p, 32, s->wt3.p, 32, R, 32, 27 * 32);
         a.flip_a = 1;
         a.mask = s->a2.p;
@@ -963,8 +1009,13 @@ cudaError_t backward(mb_surrogate* s, uint32_t n) {
         if ((e = gemm<kDenseMN, kIm2col>(a, splits_for(R), st)) != cudaSuccess) return e;
     }
     colsum_kernel<<<32, 256, 0, st>>>(s->dz2c.p, (uint32_t)R, 32, G(s, kB2));
-    conv_weight_t_kernel<<<108, 256, 0, st>>>(PB(s, kW2), 32, s->wt2.p);
-    {
+    if (s->tcgen05) {
+        conv_weight_flip_kernel<<<108, 256, 0, st>>>(PB(s, kW2), s->wf2.p);
+        ConvTcArgs c{s->dz2p.p, 4, s->wf2.p, nullptr, (int)n, nullptr, s->dz1c.p, s->tc_err.p};
+        c.mask = s->a1.p;
+        if ((e = conv_tc<4>(c, s->num_sms, st)) != cudaSuccess) return e;
+    } else {
+        conv_weight_t_kernel<<<108, 256, 0, st>>>(PB(s, kW2), 32, s->wt2.p);
         GemmArgs a = args(s, s->dz2c.p, 32, s->wt2.p, 32, R, 32, 27 * 32);
         a.flip_a = 1;
         a.mask = s->a1.p;
@@ -1020,7 +1071,9 @@ mb_status mb_surrogate_create(int device, uint32_t max_batch, uint64_t seed, mb_
           ok(s->dz1h.alloc((size_t)max_batch * 128)) && ok(s->dz3.alloc(R * 32)) && ok(s->dz2c.alloc(R * 32)) &&
           ok(s->dz1c.alloc(R * 32)) && ok(s->cls.alloc(R)) && ok(s->tc_err.alloc(1)) &&
           ok(s->x0p.alloc((size_t)max_batch * 512 * 8)) && ok(s->a1p.alloc((size_t)max_batch * 4 * 512 * 8)) &&
-          ok(s->a2p.alloc((size_t)max_batch * 4 * 512 * 8))))
+          ok(s->a2p.alloc((size_t)max_batch * 4 * 512 * 8)) && ok(s->dz3p.alloc((size_t)max_batch * 4 * 512 * 8)) &&
+          ok(s->dz2p.alloc((size_t)max_batch * 4 * 512 * 8)) && ok(s->wf2.alloc(32 * 864)) &&
+          ok(s->wf3.alloc(32 * 864))))
         return MB_ERR_CUDA;
     if (cudaMemset(s->tc_err.p, 0, sizeof(uint32_t)) != cudaSuccess) return MB_ERR_CUDA;
     if (cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return MB_ERR_CUDA;

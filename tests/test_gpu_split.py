@@ -182,3 +182,62 @@ def test_two_cluster_groups_side_by_side(graph):
     pl = mb.plan(b)
     assert pl["cluster"] == 4 and pl["cluster2"] == 2 and 0 < pl["split_bins0"] < pl["bins"]
     check(b, 1e-4, 150, True, {"chunk": 37, "use_graph": graph}, mode=S.MODE_FORCE_WATER, cluster=4)
+
+
+def _devo_cycles(b, cfg, k, cycles, dt=1e-3, steps=100, expect_device=True):
+    sim = mb.Simulator(0)
+    sim.setTimeStep(dt)
+    if cfg:
+        sim.set_launch_config(**cfg)
+    sim.set_batch(b)
+    cl = sim.launch_config()["cluster"]
+    assert cl >= 2
+    p, v = b.pos.copy(), b.vel.copy()
+    s = np.zeros(b.n_springs, np.float32)
+    t, ob = 0.0, b
+    for cycle in range(cycles):
+        sim.run_steps(steps, True)
+        core.xpbd_run(ob, p, v, s, mb.material_table(), np.float32(dt), t, steps, True)
+        t = core.advance_clock(t, np.float32(dt), steps)
+        n = sim.devo(k, seed=100 + cycle)
+        pairs, mat, lbar, recs = core.devo(ob, p, s, mb.material_table(), t, k, 100 + cycle)
+        assert n == len(recs)
+        ob = dataclasses.replace(ob, pairs=pairs, spring_material=mat, lbar=lbar)
+        assert sim.launch_config()["cluster"] == cl  # still split, same clusters
+        if expect_device:
+            assert sim.devo_profile()["host_repacks"] == 0, sim.devo_profile()
+    sim.run_steps(steps, True)
+    core.xpbd_run(ob, p, v, s, mb.material_table(), np.float32(dt), t, steps, True)
+    pos, vel, st = sim.collect_arrays()
+    assert bits_equal(pos, p) and bits_equal(vel, v) and bits_equal(st, s)
+    # the topology the device holds is the oracle's
+    pr, sm, lb = sim.collect_springs()
+    assert np.array_equal(pr, ob.pairs) and np.array_equal(sm, ob.spring_material) and bits_equal(lb, ob.lbar)
+    return sim
+
+
+@pytest.mark.parametrize("cluster", [2, 4])
+def test_split_devo_on_the_device_large_robots(cluster):
+    """Development of robots split over clusters re-derives every part on the
+    device (the partition stays): springs that leave or join a part, new
+    halo masses and their exports, rows; bit for bit the oracle through
+    several development cycles, stresses tracked."""
+    b = robots.population_batch("streamed", 4)
+    _devo_cycles(b, {"cluster": cluster}, 96, 3)
+
+
+def test_split_devo_on_the_device_shared_clusters():
+    """Uneven robots in two-CTA clusters, small ones sharing a cluster, and
+    point clouds split automatically (one, two or four parts)."""
+    _devo_cycles(robots.population_batch("uneven", 10, seed_base=3100), {"cluster": 2}, 24, 3)
+    nb = mb.pack(robots.nn_population_device(6, seed_base=2300))
+    _devo_cycles(nb, None, 64, 2)
+
+
+def test_split_devo_device_equals_host_repack(monkeypatch):
+    b = robots.population_batch("streamed", 3, seed_base=4400)
+    dev = _devo_cycles(b, {"cluster": 2}, 48, 2)
+    monkeypatch.setenv("MB_DEVO_HOST_REPACK", "1")
+    host = _devo_cycles(b, {"cluster": 2}, 48, 2, expect_device=False)
+    for a, c in zip(dev.collect_arrays(), host.collect_arrays()):
+        assert bits_equal(a, c)

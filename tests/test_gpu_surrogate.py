@@ -67,6 +67,32 @@ def test_gradients_match_oracle():
         assert a @ b / (np.linalg.norm(a) * np.linalg.norm(b) + 1e-30) > 0.999, name
 
 
+@pytest.mark.parametrize("n", [1, 77, 256])
+def test_tcgen05_backward_matches_mma_sync(n):
+    """The input gradients of the 32 -> 32 convolutions on tcgen05 (the
+    forward convolution kernel with the mirrored, transposed weights and a
+    ReLU-mask epilogue) against the mma.sync implicit GEMMs and the oracle:
+    every parameter gradient, partial tiles included."""
+    rng = np.random.default_rng(20 + n)
+    flat = so.init_params(9)
+    s = Surrogate(0, max_batch=256)
+    s.set_params(flat)
+    genomes = rng.integers(0, 5, (n, 216)).astype(np.uint8)
+    targets = rng.normal(size=n).astype(np.float32)
+    s.use_tcgen05(True)
+    l_tc, g_tc = s.gradients(genomes, targets)
+    s.use_tcgen05(False)
+    l_ms, g_ms = s.gradients(genomes, targets)
+    lo, _, go = so.Net(flat).loss_and_grads(genomes, targets)
+    a, b = so.unflatten(g_tc), so.unflatten(g_ms)
+    for name in so.NAMES:
+        x, y = a[name].astype(np.float64), b[name].astype(np.float64)
+        z = np.asarray(go[name], np.float64).reshape(-1)
+        assert rel(x, y) < 3e-2, name
+        assert rel(x, z) < 3e-2, name
+        assert x @ z / (np.linalg.norm(x) * np.linalg.norm(z) + 1e-30) > 0.999, name
+
+
 def test_gradients_are_deterministic():
     rng = np.random.default_rng(2)
     s = Surrogate(0, max_batch=128, seed=3)
