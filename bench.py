@@ -692,7 +692,8 @@ def surrogate_bench(local_rank, generations: int = 8, plain_generations: int = 3
                                                          "plain": pgens[0]["simulated"]},
             "workload": f"{SG_CHILDREN} children of 6x6x6 voxel genomes per generation, 1 s on land "
                         f"(dt 1e-4, 10,000 steps), screen 25% + 5% audit; warm-up "
-                        f"{SG_WARMUP_BATCHES * SG_CHILDREN} random genomes"}
+                        f"{SG_WARMUP_BATCHES * SG_CHILDREN} simulated genomes (3 random batches, then "
+                        f"plain-evolution children)"}
 
 
 def devo_population():
@@ -711,11 +712,12 @@ def devo_population():
 def devo_bench(local_rank, calls=3):
     """Springs replaced per second by Devo() with the reference's default
     replaced_springs_per_element (128, config.h:18) on 512 default robots,
-    after 100 stress-tracked steps; wall time of the synchronous call.  The
-    robots are too large for one CTA: on the streamed layout development
-    runs on the device (selection, rewiring, re-packing); on the split layout
-    (the default for stepping such robots) the parts are re-planned on the
-    host, timed beside it."""
+    after 100 stress-tracked steps; wall time of the synchronous call,
+    median of 3 calls (the first call on a population also sets up the
+    device re-packing).  The robots are too large for one CTA: development
+    runs on the device on the streamed layout and on the split layout (the
+    default for stepping such robots; their parts are re-derived with the
+    partition kept), timed beside it."""
     import mercury_b200 as mb
 
     def run(cfg, n_calls):
@@ -738,7 +740,7 @@ def devo_bench(local_rank, calls=3):
         return n, w, ph, not sim.robot_flags().any(), sim.launch_config()
 
     n, w, ph, finite, cfg = run({"cluster": 1}, calls)
-    _, ws, phs, fin_s, cfg_s = run({}, 2)
+    _, ws, phs, fin_s, cfg_s = run({}, calls)
     return {"metric": "springs replaced/s", "value": n / w, "unit": "springs/s", "replaced_per_call": n,
             "ms_per_call": 1e3 * w, "phases": ph, "finite_after": finite and fin_s,
             "workload": f"{DEVO_ROBOTS} default voxel robots (1,728 masses, 18,788 springs), "

@@ -43,7 +43,7 @@ def main():
             s.train_step(g, t, 1e-4)
         el = time.perf_counter() - t0
         n = args.reps * 50 * args.batch
-        print(f"train ({path} forward, mma.sync backward): {n / el:.3e} genomes/s, "
+        print(f"train ({path} forward and input gradients; weight gradients on mma.sync): {n / el:.3e} genomes/s, "
               f"{3 * FWD_FLOP * n / el / 1e12:.1f} TFLOP/s, {el / (args.reps * 50) * 1e3:.3f} ms per step")
         return
     g = rng.integers(0, 5, (args.n, 216)).astype(np.uint8)
