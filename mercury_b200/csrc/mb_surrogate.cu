@@ -675,20 +675,35 @@ __global__ void head_backward_kernel(const float* __restrict__ y, const float* _
     }
 }
 
-// Column sums of a bf16 [rows][cols] matrix, one block per column, fixed
-// order: thread t adds rows t, t+256, ...; then a tree over the block.
-__global__ void colsum_kernel(const bf16* __restrict__ a, uint32_t rows, uint32_t cols, float* __restrict__ out) {
+// Column sums in two fixed-order stages (coalesced rows): block b sums rows
+// [b chunk, (b+1) chunk); thread t takes column t % cols and every
+// (256 / cols)-th row from phase t / cols, the phases are added in order,
+// and colsum_final_kernel adds the blocks' partial sums in block order.
+constexpr int kColsumBlocks = 256;
+__global__ void __launch_bounds__(256) colsum_partial_kernel(const bf16* __restrict__ a, uint32_t rows, uint32_t cols,
+                                                             uint32_t chunk, float* __restrict__ partial) {
     __shared__ float red[256];
-    const uint32_t c = blockIdx.x, t = threadIdx.x;
+    const uint32_t t = threadIdx.x, phases = 256 / cols, c = t % cols, ph = t / cols;
+    const uint32_t r0 = blockIdx.x * chunk, r1 = min(rows, r0 + chunk);
     float s = 0.0f;
-    for (uint32_t r = t; r < rows; r += 256) s += __bfloat162float(a[(size_t)r * cols + c]);
+    if (ph < phases)
+        for (uint32_t r = r0 + ph; r < r1; r += phases) s += __bfloat162float(a[(size_t)r * cols + c]);
     red[t] = s;
     __syncthreads();
-    for (uint32_t o = 128; o; o >>= 1) {
-        if (t < o) red[t] += red[t + o];
-        __syncthreads();
+    if (t < cols) {
+        float v = 0.0f;
+        for (uint32_t q = 0; q < phases; ++q) v += red[q * cols + t];
+        partial[(size_t)blockIdx.x * cols + t] = v;
     }
-    if (t == 0) out[c] = red[0];
+}
+
+__global__ void colsum_final_kernel(const float* __restrict__ partial, uint32_t blocks, uint32_t cols,
+                                    float* __restrict__ out) {
+    const uint32_t c = threadIdx.x;
+    if (c >= cols) return;
+    float v = 0.0f;
+    for (uint32_t b = 0; b < blocks; ++b) v += partial[(size_t)b * cols + c];
+    out[c] = v;
 }
 
 // wt[(o*32 + co) * cin + ci] = w[co * 27*cin + o*cin + ci]: the weights of
@@ -945,6 +960,15 @@ mb_status check_tc(mb_surrogate* s) {
 
 int splits_for(int K) { return std::max(1, std::min(64, K / 1024)); }
 
+// Bias gradients: column sums of a [rows][cols] gradient (cols 32 or 128),
+// in a fixed order (partial sums in the split-K scratch).
+void colsum(mb_surrogate* s, const bf16* a, uint32_t rows, uint32_t cols, float* out) {
+    const uint32_t chunk = std::max<uint32_t>(1, (rows + kColsumBlocks - 1) / kColsumBlocks);
+    const uint32_t blocks = (rows + chunk - 1) / chunk;
+    colsum_partial_kernel<<<blocks, 256, 0, s->stream>>>(a, rows, cols, chunk, s->partial.p);
+    colsum_final_kernel<<<1, 128, 0, s->stream>>>(s->partial.p, blocks, cols, out);
+}
+
 // Backward of the last forward against targets s->t; gradients into s->g.
 cudaError_t backward(mb_surrogate* s, uint32_t n) {
     cudaStream_t st = s->stream;
@@ -958,7 +982,7 @@ cudaError_t backward(mb_surrogate* s, uint32_t n) {
         a.c32 = G(s, kW5);
         if ((e = gemm<kDenseMN, kDenseMN>(a, splits_for((int)n), st)) != cudaSuccess) return e;
     }
-    colsum_kernel<<<128, 256, 0, st>>>(s->dz2h.p, n, 128, G(s, kB5));
+    colsum(s, s->dz2h.p, n, 128, G(s, kB5));
     {
         GemmArgs a = args(s, s->dz2h.p, 128, PB(s, kW5), 128, (int)n, 128, 128);
         a.mask = s->h1.p;
@@ -971,7 +995,7 @@ cudaError_t backward(mb_surrogate* s, uint32_t n) {
         a.c32 = G(s, kW4);
         if ((e = gemm<kDenseMN, kDenseMN>(a, splits_for((int)n), st)) != cudaSuccess) return e;
     }
-    colsum_kernel<<<128, 256, 0, st>>>(s->dz1h.p, n, 128, G(s, kB4));
+    colsum(s, s->dz1h.p, n, 128, G(s, kB4));
     {
         GemmArgs a = args(s, s->dz1h.p, 128, PB(s, kW4), 6912, (int)n, 6912, 128);
         a.mask = s->a3.p;
@@ -984,7 +1008,7 @@ cudaError_t backward(mb_surrogate* s, uint32_t n) {
         a.c32 = G(s, kW3);
         if ((e = gemm<kDenseMN, kIm2col>(a, splits_for(R), st)) != cudaSuccess) return e;
     }
-    colsum_kernel<<<32, 256, 0, st>>>(s->dz3.p, (uint32_t)R, 32, G(s, kB3));
+    colsum(s, s->dz3.p, (uint32_t)R, 32, G(s, kB3));
     if (s->tcgen05) {
         // input gradient as the forward convolution of the gradient with the
         // mirrored, transposed kernel, on tcgen05; masked by a2 > 0
@@ -1008,7 +1032,7 @@ cudaError_t backward(mb_surrogate* s, uint32_t n) {
         a.c32 = G(s, kW2);
         if ((e = gemm<kDenseMN, kIm2col>(a, splits_for(R), st)) != cudaSuccess) return e;
     }
-    colsum_kernel<<<32, 256, 0, st>>>(s->dz2c.p, (uint32_t)R, 32, G(s, kB2));
+    colsum(s, s->dz2c.p, (uint32_t)R, 32, G(s, kB2));
     if (s->tcgen05) {
         conv_weight_flip_kernel<<<108, 256, 0, st>>>(PB(s, kW2), s->wf2.p);
         ConvTcArgs c{s->dz2p.p, 4, s->wf2.p, nullptr, (int)n, nullptr, s->dz1c.p, s->tc_err.p};
@@ -1028,7 +1052,7 @@ cudaError_t backward(mb_surrogate* s, uint32_t n) {
         a.c32 = G(s, kW1);
         if ((e = gemm<kDenseMN, kIm2col>(a, splits_for(R), st)) != cudaSuccess) return e;
     }
-    colsum_kernel<<<32, 256, 0, st>>>(s->dz1c.p, (uint32_t)R, 32, G(s, kB1));
+    colsum(s, s->dz1c.p, (uint32_t)R, 32, G(s, kB1));
     return cudaGetLastError();
 }
 

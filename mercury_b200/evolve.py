@@ -22,8 +22,9 @@ alone: top-10% recall 0.78; this warm-up: about 0.88) -- then 60 epochs
 with a cosine learning rate.
 
 Screened: the surrogate predicts all children (the mean over the 8
-horizontal orientations of each), its top `screen` fraction plus a random
-`audit` fraction of the rest are simulated, and the surrogate trains on the
+horizontal orientations of each, plus `kappa` times their spread: children
+the orientations disagree on are the least certain), its top `screen`
+fraction plus a random `audit` fraction of the rest are simulated, and the surrogate trains on the
 new (genome, fitness) pairs; the others are discarded unsimulated.  A
 child differs from its (simulated) parents in a few voxels, so each
 prediction is corrected by the surrogate's error on the parents, weighted
@@ -202,7 +203,8 @@ class ScreenedEvolution:
 
     def __init__(self, evaluator: Evaluator, surrogate, seed: int = 0, children: int = 4096,
                  screen: float = 0.25, audit: float = 0.05, batch: int = 256, lr: float = 1e-3,
-                 steps_per_generation: int = 60, finetune_lr: float = 3e-4, lineage_correction: bool = True):
+                 steps_per_generation: int = 60, finetune_lr: float = 3e-4, lineage_correction: bool = True,
+                 kappa: float = 1.0):
         """`surrogate`: one Surrogate or a list of them (an ensemble: each
         member trains on its own minibatches, predictions are averaged)."""
         self.ev = evaluator
@@ -212,15 +214,19 @@ class ScreenedEvolution:
         self.children, self.screen, self.audit = children, screen, audit
         self.batch, self.lr, self.steps, self.finetune_lr = batch, lr, steps_per_generation, finetune_lr
         self.lineage_correction = lineage_correction
+        self.kappa = kappa  # screening bonus per unit of spread over the orientations
         self.data = Dataset()
         self.pool = Pool()
         self.mu, self.sd = 0.0, 1.0
         self.trained_steps = 0
 
-    def predict(self, genomes: np.ndarray) -> np.ndarray:
+    def predict(self, genomes: np.ndarray, spread: bool = False):
+        """Mean prediction over the 8 orientations (and the members); with
+        `spread`, also the standard deviation over them."""
         g = np.asarray(genomes, np.uint8)
         views = [np.ascontiguousarray(g[:, p]) for p in ORIENTATIONS]
-        return np.mean([sg.predict(v) for sg in self.members for v in views], axis=0)
+        preds = np.array([sg.predict(v) for sg in self.members for v in views])
+        return (preds.mean(0), preds.std(0)) if spread else preds.mean(0)
 
     def _norm(self):
         _, f = self.data.arrays()
@@ -279,13 +285,15 @@ class ScreenedEvolution:
         kids, ia, ib, sb = make_children(self.rng, self.pool.genomes, self.pool.fitness, self.children,
                                          lineage=True)
         t1 = time.perf_counter()
-        pred = self.predict(kids)
+        pred, spread = self.predict(kids, spread=True)
         if self.lineage_correction:
             # a child is a near copy of simulated parents: carry over the
             # surrogate's error on them
             res = self.pool.fitness - self.predict(self.pool.genomes) * self.sd - self.mu
             pred = pred * self.sd + self.mu + (1.0 - sb) * res[ia] + sb * res[ib]
-        sel = self.select(pred)
+        # children the orientations disagree on get a bonus (their fitness is
+        # the least certain), in fitness units
+        sel = self.select(pred + self.kappa * self.sd * spread)
         t2 = time.perf_counter()
         f = self.ev(kids[sel])
         t3 = time.perf_counter()
