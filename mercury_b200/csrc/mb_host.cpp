@@ -219,6 +219,10 @@ struct mb_context {
     bool host_topology_stale = false;  // h_mass_mat / h_spring_mat / h_bins behind the device
 
     std::map<mb::GraphKey, cudaGraphExec_t> graphs;
+    // pinned staging of the packed arrays an upload copies to the device
+    // (grown on demand, kept across uploads)
+    void* stage = nullptr;
+    size_t stage_bytes = 0;
 
     void clear_graphs() {
         for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
@@ -226,6 +230,7 @@ struct mb_context {
     }
     ~mb_context() {
         clear_graphs();
+        if (stage) cudaFreeHost(stage);
         if (stream2) cudaStreamDestroy(stream2);
         if (ev_fork) cudaEventDestroy(ev_fork);
         if (ev_join) cudaEventDestroy(ev_join);
@@ -326,14 +331,59 @@ mb_status upload_packed(mb_context* ctx, const mb::Packed& out, bool* rows_faile
         if (e != cudaSuccess || n == 0) return e;
         return cudaMemcpyAsync(buf.p, src, n * sizeof(*src), cudaMemcpyHostToDevice, st);
     };
+    // the large packed arrays go through the pinned stage: copied into it by
+    // host threads, then one DMA copy each
+    {
+        struct Item {
+            void* dst;
+            const void* src;
+            size_t bytes, off;
+        };
+        std::vector<Item> items;
+        size_t total = 0;
+        auto add = [&](auto& buf, const auto& vec) -> cudaError_t {
+            cudaError_t e = buf.alloc(vec.size());
+            if (e != cudaSuccess || vec.empty()) return e;
+            const size_t bytes = vec.size() * sizeof(vec[0]);
+            items.push_back({buf.p, vec.data(), bytes, total});
+            total += (bytes + 255) & ~size_t(255);
+            return cudaSuccess;
+        };
+        MB_CUDA(ctx, add(ctx->mass_gidx, out.mass_gidx));
+        MB_CUDA(ctx, add(ctx->spring_gidx, out.spring_gidx));
+        MB_CUDA(ctx, add(ctx->spring_pair, out.pair));
+        MB_CUDA(ctx, add(ctx->spring_lbar, out.lbar));
+        MB_CUDA(ctx, add(ctx->inc, out.inc));
+        if (total > ctx->stage_bytes) {
+            if (ctx->stage) cudaFreeHost(ctx->stage);
+            ctx->stage = nullptr;
+            ctx->stage_bytes = 0;
+            MB_CUDA(ctx, cudaHostAlloc(&ctx->stage, total + total / 4, cudaHostAllocDefault));
+            ctx->stage_bytes = total + total / 4;
+        }
+        // nothing may still read the stage (or the buffers being replaced)
+        MB_CUDA(ctx, cudaStreamSynchronize(st));
+        const unsigned nt = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+        const size_t piece = std::max<size_t>(1 << 20, (total + nt - 1) / nt);
+        std::vector<std::thread> pool;
+        for (unsigned t = 0; t < nt; ++t)
+            pool.emplace_back([&, t] {
+                const size_t lo = t * piece, hi = std::min(total, lo + piece);
+                for (const Item& it : items) {
+                    const size_t a = std::max(lo, it.off), z = std::min(hi, it.off + it.bytes);
+                    if (a < z)
+                        std::memcpy(static_cast<char*>(ctx->stage) + a, static_cast<const char*>(it.src) + (a - it.off),
+                                    z - a);
+                }
+            });
+        for (auto& th : pool) th.join();
+        for (const Item& it : items)
+            MB_CUDA(ctx, cudaMemcpyAsync(it.dst, static_cast<char*>(ctx->stage) + it.off, it.bytes,
+                                         cudaMemcpyHostToDevice, st));
+    }
     MB_CUDA(ctx, up(ctx->bins, out.bins.data(), out.bins.size()));
-    MB_CUDA(ctx, up(ctx->mass_gidx, out.mass_gidx.data(), out.mass_gidx.size()));
-    MB_CUDA(ctx, up(ctx->spring_gidx, out.spring_gidx.data(), out.spring_gidx.size()));
-    MB_CUDA(ctx, up(ctx->spring_pair, out.pair.data(), out.pair.size()));
-    MB_CUDA(ctx, up(ctx->spring_lbar, out.lbar.data(), out.lbar.size()));
     MB_CUDA(ctx, up(ctx->slice_off, out.slice_off.data(), out.slice_off.size()));
     MB_CUDA(ctx, up(ctx->slice_width, out.slice_width.data(), out.slice_width.size()));
-    MB_CUDA(ctx, up(ctx->inc, out.inc.data(), out.inc.size()));
     MB_CUDA(ctx, up(ctx->exports, out.exports.data(), out.exports.size()));
     MB_CUDA(ctx, up(ctx->faces, reinterpret_cast<const uint2*>(out.faces.data()), out.faces.size() / 2));
     MB_CUDA(ctx, up(ctx->face_row, out.face_row.data(), out.face_row.size()));
@@ -1075,17 +1125,20 @@ mb_status mb_set_elements(mb_context* ctx, const mb_batch_desc* b) {
     std::vector<float> h_lbar;
     std::vector<int64_t> h_face_off;
     std::vector<uint16_t> h_faces;
+    // three copier threads (the pairs alone are the largest array)
     std::thread copier([&] {
         if (F) {
             h_face_off.assign(b->face_offsets, b->face_offsets + R + 1);
             h_faces.assign(b->faces, b->faces + 3 * F);
         }
         h_mass_mat.assign(b->mass_material, b->mass_material + M);
-        if (S) {
-            h_pairs.assign(b->pairs, b->pairs + 2 * S);
-            h_spring_mat.assign(b->spring_material, b->spring_material + S);
-            h_lbar.assign(b->lbar, b->lbar + S);
-        }
+        if (S) h_spring_mat.assign(b->spring_material, b->spring_material + S);
+    });
+    std::thread copier_pairs([&] {
+        if (S) h_pairs.assign(b->pairs, b->pairs + 2 * S);
+    });
+    std::thread copier_lbar([&] {
+        if (S) h_lbar.assign(b->lbar, b->lbar + S);
     });
     // kept in the context: its arrays keep their capacity across uploads.
     // Resident rows are built on the device unless MB_HOST_ROWS=1.
@@ -1094,6 +1147,8 @@ mb_status mb_set_elements(mb_context* ctx, const mb_batch_desc* b) {
     const bool device_rows = !(host_rows && host_rows[0] == '1');
     const mb_status pst = mb_detail::pack(ctx, b, false, out, true, device_rows);
     copier.join();
+    copier_pairs.join();
+    copier_lbar.join();
     if (pst != MB_OK) return pst;
 
     // the population is accepted: keep its topology on the host (for

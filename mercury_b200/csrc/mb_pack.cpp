@@ -38,6 +38,7 @@ struct RobotPack {
     uint64_t inc_estimate = 0;
     uint32_t n_face = 0;     // faces with three distinct corners
     uint32_t face_smem = 0;  // shared memory of the face drag, bytes (upper bound)
+    uint64_t mats[4] = {0, 0, 0, 0};  // composite ids of its non-air springs (bit set)
     std::string error;
     mb_status status = MB_OK;
 };
@@ -116,6 +117,7 @@ void preprocess(const mb_batch_desc* b, uint32_t r, RobotPack& p) {
             return;
         }
         if (b->spring_material[s] == 0) continue;  // air springs never act (sim_kernel.cu:211)
+        p.mats[b->spring_material[s] >> 6] |= 1ull << (b->spring_material[s] & 63);
         sp.push_back((uint32_t)(s - s0));
         deg[a]++;
         deg[c]++;
@@ -1110,8 +1112,13 @@ mb_status pack_population(const mb_batch_desc* b, const PackOptions& o, Packed& 
 
     // material slots: the composite ids used by the whole population
     std::vector<int> slot_of(MB_COMPOSITE_COUNT, -1);
-    for (uint32_t r = 0; r < R; ++r)
-        for (uint32_t ls : packs[r].springs) slot_of[b->spring_material[b->spring_offsets[r] + ls]] = 0;
+    {
+        uint64_t used[4] = {0, 0, 0, 0};
+        for (uint32_t r = 0; r < R; ++r)
+            for (int w = 0; w < 4; ++w) used[w] |= packs[r].mats[w];
+        for (int m = 0; m < MB_COMPOSITE_COUNT; ++m)
+            if ((used[m >> 6] >> (m & 63)) & 1ull) slot_of[m] = 0;
+    }
     out.mat_ids.clear();
     for (int m = 0; m < MB_COMPOSITE_COUNT; ++m)
         if (slot_of[m] == 0) {
