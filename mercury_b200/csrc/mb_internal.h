@@ -143,7 +143,7 @@ uint32_t list_shapes(KernelShape* out, uint32_t cap, bool streamed);
 uint32_t bin_smem_bytes(uint32_t n_mass, uint32_t n_spring, uint32_t n_inc);
 // The same on the device: x~ and dp as float4 per mass and spring, the
 // material factors of every slot, the rows as uint16 entries.
-__host__ __device__ inline uint32_t bin_smem_bytes_dev(uint32_t n_mass, uint32_t n_spring, uint32_t n_inc) {
+__host__ __device__ constexpr uint32_t bin_smem_bytes_dev(uint32_t n_mass, uint32_t n_spring, uint32_t n_inc) {
     return 16u * n_mass + 16u * n_spring + 8u * kMaxMaterialSlots + 2u * n_inc;
 }
 

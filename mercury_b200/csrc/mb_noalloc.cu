@@ -40,6 +40,9 @@ static_assert(1024u * 8u >= kNaMaxSprings, "step shape must hold MB_NOALLOC_MAX_
 static_assert(1024u * 2u >= kNaMaxMasses, "step shape must hold MB_NOALLOC_MAX_MASSES masses");
 static_assert(kNaMaxMasses <= 4096u, "mass indices of packed springs have 12 bits");
 static_assert(kNaMaxMasses % kSliceWidth == 0, "whole slices");
+// the largest robot accepted fits the 227 KB of shared memory a CTA may use
+static_assert(bin_smem_bytes_dev(kNaMaxMasses, kNaMaxSprings, kNaMaxIncidence) <= 227u * 1024u,
+              "the step kernel's shared memory at the limits");
 
 // Status bits written by the build kernel.
 constexpr uint32_t kNaBadTopology = 1u;  // index or material out of range
