@@ -74,3 +74,27 @@ def test_matches_live_reference_uneven(flavour, dt):
     # ill-conditioned)
     ref_com = core.com_reference(b, np.concatenate([po, np.ones((len(po), 1), np.float32)], 1))
     assert np.abs(com - ref_com).max() < 2e-4 * length.max()
+
+
+def test_headline_population_matches_live_reference():
+    """The bench's whole population (512 uneven robots, the headline
+    workload's seeds) against the reference's own CUDA simulator over the
+    first 1,000 steps at dt = 1e-4 (IEEE flavour): every robot within the
+    stated tolerance."""
+    path = FLAVOURS["ieee"]
+    if not os.path.exists(path):
+        pytest.skip("reference build absent")
+    L = mf.load(path)
+    b = robots.population_batch("uneven", seed_base=1000)
+    assert b.n_robots == 512
+    length = mb.body_length(b)
+    dur = float(np.float32(1e-4) * np.float32(999.5))
+    po, _, _, tt, steps = mf.ref_simulate(L, b, 1e-4, dur, False)
+    pos, _, _, n, t, _ = _gpu(b, 1e-4, dur, False)
+    assert n == steps == 1000 and t == tt
+    worst = 0.0
+    for r in range(b.n_robots):
+        ms, _ = b.robot_slices(r)
+        worst = max(worst, float(np.abs(pos[ms, :3] - po[ms]).max() / length[r]))
+    print(f"\n512 robots, 1,000 steps: max |x - x_ref| / body length = {worst:.2e}")
+    assert worst < 2e-4
