@@ -21,6 +21,7 @@
 #include "mb_pack.h"
 
 #include <algorithm>
+#include <tuple>
 #include <climits>
 #include <atomic>
 #include <cmath>
@@ -419,31 +420,52 @@ void build_faces(const mb_batch_desc* b, const std::vector<RobotPack>& packs,
     uint32_t nf = 0;
     for (uint32_t r : robots) nf += packs[r].n_face;
     if (!nf) return;
-    L.faces.reserve(2 * (size_t)nf);
-    std::vector<uint32_t> start(nm + 1, 0);
-    uint32_t mbase = 0;
-    for (uint32_t r : robots) {
-        for (int64_t f = b->face_offsets[r]; f < b->face_offsets[r + 1]; ++f) {
-            const uint16_t* c = b->faces + 3 * f;
-            if (c[0] == c[1] || c[0] == c[2] || c[1] == c[2]) continue;
-            const uint32_t c0 = mbase + c[0], c1 = mbase + c[1], c2 = mbase + c[2];
-            L.faces.push_back(c0 | (c1 << 16));
-            L.faces.push_back(c2);
-            start[c0 + 1]++;
-            start[c1 + 1]++;
-            start[c2 + 1]++;
+    // the bin's faces in robot face order (bin-local corners)
+    std::vector<uint32_t> c0s(nf), c1s(nf), c2s(nf);
+    {
+        uint32_t mbase = 0, f = 0;
+        for (uint32_t r : robots) {
+            for (int64_t g = b->face_offsets[r]; g < b->face_offsets[r + 1]; ++g) {
+                const uint16_t* c = b->faces + 3 * g;
+                if (c[0] == c[1] || c[0] == c[2] || c[1] == c[2]) continue;
+                c0s[f] = mbase + c[0];
+                c1s[f] = mbase + c[1];
+                c2s[f] = mbase + c[2];
+                ++f;
+            }
+            mbase += packs[r].n_mass;
         }
-        mbase += packs[r].n_mass;
+    }
+    // storage order: faces of one shape (corner offsets) together, by first
+    // corner, so that consecutive threads of the face pass read consecutive
+    // masses; the rows below keep every mass's faces in robot face order
+    std::vector<uint32_t> order(nf), slot(nf);
+    for (uint32_t f = 0; f < nf; ++f) order[f] = f;
+    auto key = [&](uint32_t f) {
+        return std::make_tuple((int32_t)c1s[f] - (int32_t)c0s[f], (int32_t)c2s[f] - (int32_t)c0s[f], c0s[f], f);
+    };
+    std::sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) { return key(x) < key(y); });
+    L.faces.resize(2 * (size_t)nf);
+    for (uint32_t s = 0; s < nf; ++s) {
+        const uint32_t f = order[s];
+        slot[f] = s;
+        L.faces[2 * s] = c0s[f] | (c1s[f] << 16);
+        L.faces[2 * s + 1] = c2s[f];
+    }
+    std::vector<uint32_t> start(nm + 1, 0);
+    for (uint32_t f = 0; f < nf; ++f) {
+        start[c0s[f] + 1]++;
+        start[c1s[f] + 1]++;
+        start[c2s[f] + 1]++;
     }
     for (uint32_t i = 0; i < nm; ++i) start[i + 1] += start[i];
     L.face_inc.resize(start[nm]);
     L.face_row.resize(nm);
     std::vector<uint32_t> fill(start.begin(), start.end() - 1);
     for (uint32_t f = 0; f < nf; ++f) {
-        const uint32_t w = L.faces[2 * f];
-        L.face_inc[fill[w & 0xFFFFu]++] = (uint16_t)f;
-        L.face_inc[fill[w >> 16]++] = (uint16_t)f;
-        L.face_inc[fill[L.faces[2 * f + 1]]++] = (uint16_t)f;
+        L.face_inc[fill[c0s[f]]++] = (uint16_t)slot[f];
+        L.face_inc[fill[c1s[f]]++] = (uint16_t)slot[f];
+        L.face_inc[fill[c2s[f]]++] = (uint16_t)slot[f];
     }
     for (uint32_t i = 0; i < nm; ++i) L.face_row[i] = start[i] | ((start[i + 1] - start[i]) << 24);
     L.n_face = nf;
