@@ -19,6 +19,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cassert>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -678,7 +679,7 @@ __global__ void head_backward_kernel(const float* __restrict__ y, const float* _
 // Column sums in two fixed-order stages (coalesced rows): block b sums rows
 // [b chunk, (b+1) chunk); thread t takes column t % cols and every
 // (256 / cols)-th row from phase t / cols, the phases are added in order,
-// and colsum_final_kernel adds the blocks' partial sums in block order.
+// and colsum_final_kernel adds the blocks' partial sums the same way.
 constexpr int kColsumBlocks = 256;
 __global__ void __launch_bounds__(256) colsum_partial_kernel(const bf16* __restrict__ a, uint32_t rows, uint32_t cols,
                                                              uint32_t chunk, float* __restrict__ partial) {
@@ -697,13 +698,23 @@ __global__ void __launch_bounds__(256) colsum_partial_kernel(const bf16* __restr
     }
 }
 
-__global__ void colsum_final_kernel(const float* __restrict__ partial, uint32_t blocks, uint32_t cols,
-                                    float* __restrict__ out) {
-    const uint32_t c = threadIdx.x;
-    if (c >= cols) return;
+// 256 threads: thread t adds, for column t % cols, the partial sums of blocks
+// p, p + parts, ... (p = t / cols, parts = 256 / cols); the parts are then
+// added in order.
+__global__ void __launch_bounds__(256) colsum_final_kernel(const float* __restrict__ partial, uint32_t blocks,
+                                                           uint32_t cols, float* __restrict__ out) {
+    __shared__ float red[256];
+    const uint32_t t = threadIdx.x, parts = 256 / cols, c = t % cols, p = t / cols;
     float v = 0.0f;
-    for (uint32_t b = 0; b < blocks; ++b) v += partial[(size_t)b * cols + c];
-    out[c] = v;
+    if (p < parts)
+        for (uint32_t b = p; b < blocks; b += parts) v += partial[(size_t)b * cols + c];
+    red[t] = v;
+    __syncthreads();
+    if (t < cols) {
+        float s = 0.0f;
+        for (uint32_t q = 0; q < parts; ++q) s += red[q * cols + t];
+        out[t] = s;
+    }
 }
 
 // wt[(o*32 + co) * cin + ci] = w[co * 27*cin + o*cin + ci]: the weights of
@@ -963,10 +974,11 @@ int splits_for(int K) { return std::max(1, std::min(64, K / 1024)); }
 // Bias gradients: column sums of a [rows][cols] gradient (cols 32 or 128),
 // in a fixed order (partial sums in the split-K scratch).
 void colsum(mb_surrogate* s, const bf16* a, uint32_t rows, uint32_t cols, float* out) {
+    assert(cols <= 256 && 256 % cols == 0);
     const uint32_t chunk = std::max<uint32_t>(1, (rows + kColsumBlocks - 1) / kColsumBlocks);
     const uint32_t blocks = (rows + chunk - 1) / chunk;
     colsum_partial_kernel<<<blocks, 256, 0, s->stream>>>(a, rows, cols, chunk, s->partial.p);
-    colsum_final_kernel<<<1, 128, 0, s->stream>>>(s->partial.p, blocks, cols, out);
+    colsum_final_kernel<<<1, 256, 0, s->stream>>>(s->partial.p, blocks, cols, out);
 }
 
 // Backward of the last forward against targets s->t; gradients into s->g.
