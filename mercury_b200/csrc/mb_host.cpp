@@ -172,6 +172,14 @@ struct mb_context {
     std::vector<float> h_lbar;
     std::vector<int64_t> h_face_off;  // empty: no faces
     std::vector<uint16_t> h_faces;
+    // the next upload's copies are taken into these and swapped in when the
+    // population is accepted: both sets keep their capacity, so a repeated
+    // upload writes to memory that is already mapped
+    std::vector<uint16_t> nx_pairs;
+    std::vector<uint8_t> nx_spring_mat, nx_mass_mat;
+    std::vector<float> nx_lbar;
+    std::vector<int64_t> nx_face_off;
+    std::vector<uint16_t> nx_faces;
     mb::DevBuf<int64_t> d_spring_off;
     mb::DevBuf<mb::DevoRecord> devo_out;
     std::vector<mb::DevoRecord> h_devo;
@@ -1119,27 +1127,20 @@ mb_status mb_set_elements(mb_context* ctx, const mb_batch_desc* b) {
     if (F >= (1ull << 31)) return fail(ctx, MB_ERR_CAPACITY, "population too large");
 
     cudaSetDevice(ctx->device);
-    // the host copy of the topology is taken while the population is packed
-    std::vector<uint8_t> h_mass_mat, h_spring_mat;
-    std::vector<uint16_t> h_pairs;
-    std::vector<float> h_lbar;
-    std::vector<int64_t> h_face_off;
-    std::vector<uint16_t> h_faces;
-    // three copier threads (the pairs alone are the largest array)
+    // the host copy of the topology is taken while the population is
+    // packed, by three copier threads (the pairs alone are the largest array)
     std::thread copier([&] {
+        ctx->nx_face_off.clear();
+        ctx->nx_faces.clear();
         if (F) {
-            h_face_off.assign(b->face_offsets, b->face_offsets + R + 1);
-            h_faces.assign(b->faces, b->faces + 3 * F);
+            ctx->nx_face_off.assign(b->face_offsets, b->face_offsets + R + 1);
+            ctx->nx_faces.assign(b->faces, b->faces + 3 * F);
         }
-        h_mass_mat.assign(b->mass_material, b->mass_material + M);
-        if (S) h_spring_mat.assign(b->spring_material, b->spring_material + S);
+        ctx->nx_mass_mat.assign(b->mass_material, b->mass_material + M);
+        ctx->nx_spring_mat.assign(b->spring_material, b->spring_material + S);
     });
-    std::thread copier_pairs([&] {
-        if (S) h_pairs.assign(b->pairs, b->pairs + 2 * S);
-    });
-    std::thread copier_lbar([&] {
-        if (S) h_lbar.assign(b->lbar, b->lbar + S);
-    });
+    std::thread copier_pairs([&] { ctx->nx_pairs.assign(b->pairs, b->pairs + 2 * S); });
+    std::thread copier_lbar([&] { ctx->nx_lbar.assign(b->lbar, b->lbar + S); });
     // kept in the context: its arrays keep their capacity across uploads.
     // Resident rows are built on the device unless MB_HOST_ROWS=1.
     mb::Packed& out = ctx->upload_pack;
@@ -1163,12 +1164,12 @@ mb_status mb_set_elements(mb_context* ctx, const mb_batch_desc* b) {
     ctx->n_spring = S;
     ctx->mass_off.assign(b->mass_offsets, b->mass_offsets + R + 1);
     ctx->spring_off.assign(b->spring_offsets, b->spring_offsets + R + 1);
-    ctx->h_mass_mat = std::move(h_mass_mat);
-    ctx->h_pairs = std::move(h_pairs);
-    ctx->h_spring_mat = std::move(h_spring_mat);
-    ctx->h_lbar = std::move(h_lbar);
-    ctx->h_face_off = std::move(h_face_off);
-    ctx->h_faces = std::move(h_faces);
+    ctx->h_mass_mat.swap(ctx->nx_mass_mat);
+    ctx->h_pairs.swap(ctx->nx_pairs);
+    ctx->h_spring_mat.swap(ctx->nx_spring_mat);
+    ctx->h_lbar.swap(ctx->nx_lbar);
+    ctx->h_face_off.swap(ctx->nx_face_off);
+    ctx->h_faces.swap(ctx->nx_faces);
     cudaStream_t st = ctx->stream;
     auto up = [&](auto& buf, const auto* src, size_t n) -> cudaError_t {
         cudaError_t e = buf.alloc(n);
