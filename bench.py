@@ -681,10 +681,17 @@ def surrogate_bench(local_rank, generations: int = 8, plain_generations: int = 3
     t_p = float(np.mean([g["wall_s"] for g in pgens]))
     q = {k: float(np.mean([g[k] for g in gens])) for k in ("spearman", "top10_recall", "top10_recall_top10",
                                                           "random_screen_recall")}
+    # recall of the screen's top fraction alone (no audit), per fraction
+    q["top10_recall_at"] = {fr: float(np.mean([g["top10_recall_at"][fr] for g in gens]))
+                            for fr in gens[0]["top10_recall_at"]}
+
+    def rounded(g):
+        return {k: ({a: round(b, 4) for a, b in v.items()} if isinstance(v, dict) else round(v, 4))
+                for k, v in g.items()}
     return {"metric": "generations/s", "screened": 1.0 / t_s, "plain": 1.0 / t_p, "speedup": t_p / t_s,
             "unit": "generations/s", **q,
-            "per_generation": [{k: round(v, 4) for k, v in g.items()} for g in gens],
-            "plain_per_generation": [{k: round(v, 4) for k, v in g.items()} for g in pgens],
+            "per_generation": [rounded(g) for g in gens],
+            "plain_per_generation": [rounded(g) for g in pgens],
             "best_fitness": {"screened": gens[-1]["best"], "plain": pgens[-1]["best"]},
             "race": race,
             "warmup": warm, "warmup_generation_s": {"screened": warm_s["wall_s"], "plain": warm_p["wall_s"]},

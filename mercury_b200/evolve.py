@@ -293,7 +293,8 @@ class ScreenedEvolution:
             pred = pred * self.sd + self.mu + (1.0 - sb) * res[ia] + sb * res[ib]
         # children the orientations disagree on get a bonus (their fitness is
         # the least certain), in fitness units
-        sel = self.select(pred + self.kappa * self.sd * spread)
+        score = pred + self.kappa * self.sd * spread
+        sel = self.select(score)
         t2 = time.perf_counter()
         f = self.ev(kids[sel])
         t3 = time.perf_counter()
@@ -305,7 +306,7 @@ class ScreenedEvolution:
                "train_s": t4 - t3, "simulated": len(sel), "best": float(self.pool.fitness[0])}
         if truth:  # ground truth for every child, outside the timed region
             ft = self.ev(kids)
-            out.update(quality(pred, ft, sel, self.screen))
+            out.update(quality(pred, ft, sel, self.screen, score))
         return out
 
 
@@ -349,12 +350,15 @@ def best_at(curve: list, seconds: float) -> float:
     return max(best) if best else float("-inf")
 
 
-def quality(pred: np.ndarray, truth: np.ndarray, selected: np.ndarray, screen: float) -> dict:
+def quality(pred: np.ndarray, truth: np.ndarray, selected: np.ndarray, screen: float,
+            score: np.ndarray | None = None, fractions=(0.2, 0.25, 0.3, 0.35, 0.4, 0.5)) -> dict:
     """Spearman rank correlation of predictions and simulated fitness over
     all children; top-10% recall: the share of the truly best 10% that the
     screen sends to simulation (selected = surrogate top `screen` + audit);
     also the share inside the surrogate's own top 10%, and what random
-    screening of the same size would give."""
+    screening of the same size would give.  With the screening `score`:
+    the recall of its top fraction alone (no audit) for each of
+    `fractions`."""
     from scipy.stats import spearmanr
     n = len(truth)
     top = set(np.argsort(-truth, kind="stable")[: n // 10].tolist())
@@ -365,4 +369,7 @@ def quality(pred: np.ndarray, truth: np.ndarray, selected: np.ndarray, screen: f
         "top10_recall": len(top & sel) / len(top),
         "top10_recall_top10": len(top & own) / len(top),
         "random_screen_recall": len(sel) / n,
+        **({"top10_recall_at": {str(fr): len(top & set(np.argsort(-score, kind="stable")[: int(round(fr * n))]
+                                                        .tolist())) / len(top) for fr in fractions}}
+           if score is not None else {}),
     }

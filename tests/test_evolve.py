@@ -46,6 +46,14 @@ def test_quality_metrics():
     assert q["spearman"] == pytest.approx(1.0) and q["top10_recall"] == 1.0 and q["top10_recall_top10"] == 1.0
     q = evolve.quality(-truth, truth, np.arange(0, 10), 0.25)
     assert q["top10_recall"] == 0.0 and q["random_screen_recall"] == 0.1
+    # recall of the score's top fraction: the true top 10 (indices 90-99)
+    # sit at score ranks 0-4 (95-99) and 26, 28, ..., 34 (90-94, between
+    # indices 20-24), so the top 5 % holds half of them, the top 30 % seven
+    score = -np.arange(100, dtype=np.float64)
+    score[95:] = 10.0 + np.arange(5)
+    score[90:95] = -20.5 - np.arange(5)
+    q = evolve.quality(truth, truth, np.arange(90, 100), 0.25, score, fractions=(0.05, 0.3, 0.35))
+    assert q["top10_recall_at"] == {"0.05": 0.5, "0.3": 0.7, "0.35": 1.0}
 
 
 class _FakeEvaluator:
