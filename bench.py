@@ -638,11 +638,14 @@ def build_bench(local_rank):
 
 DEVO_ROBOTS, DEVO_K = 512, 128
 SG_CHILDREN, SG_WARMUP_BATCHES, SG_RACE_S = 4096, 13, 4.0
+# the surrogate's top 35 % (plus a 5 % audit) is simulated: over three
+# seeds its top-10 % recall averages 0.92 there, against 0.85 at 25 %
+SG_SCREEN = 0.35
 
 
 def surrogate_bench(local_rank, generations: int = 8, plain_generations: int = 3, seed: int = 0):
     """Surrogate-screened evolution (4096 children of 6x6x6 voxel genomes
-    per generation; the surrogate's top 25% plus a 5% random audit are
+    per generation; the surrogate's top 35% plus a 5% random audit are
     simulated for 1 s on land) against plain evolution (all 4096
     simulated), after a warm-up of 13 x 4096 = 53,248 simulated genomes
     (3 random batches, then plain-evolution children).  First a race: both
@@ -657,13 +660,13 @@ def surrogate_bench(local_rank, generations: int = 8, plain_generations: int = 3
     from mercury_b200.surrogate import Surrogate
     ev = evolve.Evaluator(local_rank)
     sg = Surrogate(local_rank, max_batch=1024, seed=seed)
-    scr = evolve.ScreenedEvolution(ev, sg, seed=seed + 1, children=SG_CHILDREN)
+    scr = evolve.ScreenedEvolution(ev, sg, seed=seed + 1, children=SG_CHILDREN, screen=SG_SCREEN)
     warm = scr.warmup(SG_WARMUP_BATCHES * SG_CHILDREN, batch=SG_CHILDREN)
     plain = evolve.PlainEvolution(ev, seed=seed + 2, children=SG_CHILDREN, pool=copy.deepcopy(scr.pool))
     # best fitness against wall time, both from the pool the warm-up left,
     # for the same budget (one untimed generation each first: a new batch
     # size plans its packing once)
-    rs = evolve.ScreenedEvolution(ev, sg, seed=seed + 3, children=SG_CHILDREN)
+    rs = evolve.ScreenedEvolution(ev, sg, seed=seed + 3, children=SG_CHILDREN, screen=SG_SCREEN)
     rs.data, rs.pool, rs.mu, rs.sd = scr.data, copy.deepcopy(scr.pool), scr.mu, scr.sd
     rp = evolve.PlainEvolution(ev, seed=seed + 4, children=SG_CHILDREN, pool=copy.deepcopy(scr.pool))
     start_best = float(scr.pool.fitness[0])
@@ -698,7 +701,7 @@ def surrogate_bench(local_rank, generations: int = 8, plain_generations: int = 3
             "simulated_per_generation": {"screened": gens[0]["simulated"],
                                                          "plain": pgens[0]["simulated"]},
             "workload": f"{SG_CHILDREN} children of 6x6x6 voxel genomes per generation, 1 s on land "
-                        f"(dt 1e-4, 10,000 steps), screen 25% + 5% audit; warm-up "
+                        f"(dt 1e-4, 10,000 steps), screen {round(100 * SG_SCREEN)}% + 5% audit; warm-up "
                         f"{SG_WARMUP_BATCHES * SG_CHILDREN} simulated genomes (3 random batches, then "
                         f"plain-evolution children)"}
 

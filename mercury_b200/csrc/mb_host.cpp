@@ -373,18 +373,15 @@ mb_status upload_packed(mb_context* ctx, const mb::Packed& out, bool* rows_faile
         MB_CUDA(ctx, cudaStreamSynchronize(st));
         const unsigned nt = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
         const size_t piece = std::max<size_t>(1 << 20, (total + nt - 1) / nt);
-        std::vector<std::thread> pool;
-        for (unsigned t = 0; t < nt; ++t)
-            pool.emplace_back([&, t] {
-                const size_t lo = t * piece, hi = std::min(total, lo + piece);
-                for (const Item& it : items) {
-                    const size_t a = std::max(lo, it.off), z = std::min(hi, it.off + it.bytes);
-                    if (a < z)
-                        std::memcpy(static_cast<char*>(ctx->stage) + a, static_cast<const char*>(it.src) + (a - it.off),
-                                    z - a);
-                }
-            });
-        for (auto& th : pool) th.join();
+        mb::parallel_for(nt, nt, [&](uint32_t t) {
+            const size_t lo = t * piece, hi = std::min(total, lo + piece);
+            for (const Item& it : items) {
+                const size_t a = std::max(lo, it.off), z = std::min(hi, it.off + it.bytes);
+                if (a < z)
+                    std::memcpy(static_cast<char*>(ctx->stage) + a, static_cast<const char*>(it.src) + (a - it.off),
+                                z - a);
+            }
+        });
         for (const Item& it : items)
             MB_CUDA(ctx, cudaMemcpyAsync(it.dst, static_cast<char*>(ctx->stage) + it.off, it.bytes,
                                          cudaMemcpyHostToDevice, st));

@@ -26,10 +26,105 @@
 #include <atomic>
 #include <cmath>
 #include <cstdio>
+#include <condition_variable>
 #include <cstring>
+#include <mutex>
 #include <thread>
+#include <unistd.h>
 
 namespace mb {
+
+// ---- worker pool ----
+//
+// Host threads are started once per process and reused: an upload runs
+// several parallel loops, and starting 16 threads costs about as much as
+// a loop's work.  One loop runs at a time (callers on other host threads
+// wait); a loop started from inside a worker, or in a child process
+// forked after the pool started (it has no workers), runs on the calling
+// thread.  The pool is never torn down: its threads wait on a condition
+// variable until the process ends.
+namespace {
+
+thread_local bool t_in_pool = false;
+
+class WorkerPool {
+  public:
+    explicit WorkerPool(unsigned n) : pid_(getpid()) {
+        for (unsigned k = 0; k < n; ++k) workers_.emplace_back([this, k] { work(k); });
+    }
+    unsigned size() const { return (unsigned)workers_.size(); }
+    bool usable() const { return getpid() == pid_; }
+
+    void run(uint32_t n, unsigned threads, const std::function<void(uint32_t)>& f) {
+        std::lock_guard<std::mutex> one(run_mu_);
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            job_ = &f;
+            n_ = n;
+            next_.store(0);
+            want_ = std::min<unsigned>(threads - 1, size());
+            active_ = want_;
+            ++generation_;
+        }
+        cv_.notify_all();
+        t_in_pool = true;
+        for (uint32_t i = next_++; i < n; i = next_++) f(i);
+        t_in_pool = false;
+        std::unique_lock<std::mutex> lk(mu_);
+        done_.wait(lk, [this] { return active_ == 0; });
+        job_ = nullptr;
+    }
+
+  private:
+    void work(unsigned index) {
+        t_in_pool = true;
+        uint64_t seen = 0;
+        for (;;) {
+            std::unique_lock<std::mutex> lk(mu_);
+            cv_.wait(lk, [&] { return generation_ != seen; });
+            seen = generation_;
+            if (index >= want_) continue;  // not needed by this loop
+            const std::function<void(uint32_t)>& f = *job_;
+            const uint32_t n = n_;
+            lk.unlock();
+            for (uint32_t i = next_++; i < n; i = next_++) f(i);
+            lk.lock();
+            if (--active_ == 0) done_.notify_one();
+        }
+    }
+
+    const pid_t pid_;
+    std::vector<std::thread> workers_;
+    std::mutex run_mu_, mu_;
+    std::condition_variable cv_, done_;
+    const std::function<void(uint32_t)>* job_ = nullptr;
+    std::atomic<uint32_t> next_{0};
+    uint32_t n_ = 0;
+    unsigned want_ = 0, active_ = 0;
+    uint64_t generation_ = 0;
+};
+
+WorkerPool& worker_pool() {
+    static WorkerPool* pool =
+        new WorkerPool(std::max(1u, std::thread::hardware_concurrency()) - 1);  // the caller is the last
+    return *pool;
+}
+
+}  // namespace
+
+void parallel_for(uint32_t n, unsigned threads, const std::function<void(uint32_t)>& f) {
+    if (threads <= 1 || n <= 1 || t_in_pool) {
+        for (uint32_t i = 0; i < n; ++i) f(i);
+        return;
+    }
+    WorkerPool& pool = worker_pool();
+    if (!pool.usable() || pool.size() == 0) {
+        for (uint32_t i = 0; i < n; ++i) f(i);
+        return;
+    }
+    pool.run(n, std::min<unsigned>(threads, n), f);
+}
+
 namespace {
 
 struct RobotPack {
@@ -53,22 +148,6 @@ const KernelShape kAuto[] = {
 
 // Shapes for the parts of split robots, in order of preference.
 const KernelShape kSplit[] = {{1024, 8, 2}, {1024, 10, 2}, {1024, 12, 2}};
-
-template <typename F>
-void parallel_for(uint32_t n, unsigned threads, F&& f) {
-    if (threads <= 1 || n <= 1) {
-        for (uint32_t i = 0; i < n; ++i) f(i);
-        return;
-    }
-    std::atomic<uint32_t> next{0};
-    std::vector<std::thread> pool;
-    const unsigned t = std::min<unsigned>(threads, n);
-    for (unsigned k = 0; k < t; ++k)
-        pool.emplace_back([&] {
-            for (uint32_t i = next++; i < n; i = next++) f(i);
-        });
-    for (auto& th : pool) th.join();
-}
 
 void preprocess(const mb_batch_desc* b, uint32_t r, RobotPack& p) {
     const int64_t m0 = b->mass_offsets[r], m1 = b->mass_offsets[r + 1];

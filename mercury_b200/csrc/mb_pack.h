@@ -93,6 +93,11 @@ struct Packed {
     uint32_t aligned_slices = 0, rank_slices = 0;
 };
 
+// Runs f(i) for every i in [0, n) on up to `threads` host threads of a
+// process-wide worker pool (the calling thread among them), in any order;
+// returns when all are done.
+void parallel_for(uint32_t n, unsigned threads, const std::function<void(uint32_t)>& f);
+
 // Validates `b`, chooses the launch shape and bin count (or applies the
 // override), and builds the packed arrays.  On failure returns the status
 // and a message in `err`.

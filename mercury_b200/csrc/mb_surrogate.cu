@@ -678,8 +678,9 @@ __global__ void head_backward_kernel(const float* __restrict__ y, const float* _
 
 // Column sums in two fixed-order stages (coalesced rows): block b sums rows
 // [b chunk, (b+1) chunk); thread t takes column t % cols and every
-// (256 / cols)-th row from phase t / cols, the phases are added in order,
-// and colsum_final_kernel adds the blocks' partial sums the same way.
+// (256 / cols)-th row from phase t / cols, the phases are added in order;
+// colsum_final_kernel then adds the blocks' partial sums in contiguous
+// ranges of blocks and the ranges in order.
 constexpr int kColsumBlocks = 256;
 __global__ void __launch_bounds__(256) colsum_partial_kernel(const bf16* __restrict__ a, uint32_t rows, uint32_t cols,
                                                              uint32_t chunk, float* __restrict__ partial) {
@@ -698,16 +699,17 @@ __global__ void __launch_bounds__(256) colsum_partial_kernel(const bf16* __restr
     }
 }
 
-// 256 threads: thread t adds, for column t % cols, the partial sums of blocks
-// p, p + parts, ... (p = t / cols, parts = 256 / cols); the parts are then
-// added in order.
-__global__ void __launch_bounds__(256) colsum_final_kernel(const float* __restrict__ partial, uint32_t blocks,
-                                                           uint32_t cols, float* __restrict__ out) {
-    __shared__ float red[256];
-    const uint32_t t = threadIdx.x, parts = 256 / cols, c = t % cols, p = t / cols;
+// 1,024 threads: thread t adds, for column t % cols, the partial sums of a
+// contiguous range of blocks (part t / cols of 1024 / cols); the parts are
+// then added in order.  Every load of a thread is independent of the others,
+// so the stage costs about one memory latency.
+__global__ void __launch_bounds__(1024) colsum_final_kernel(const float* __restrict__ partial, uint32_t blocks,
+                                                            uint32_t cols, float* __restrict__ out) {
+    __shared__ float red[1024];
+    const uint32_t t = threadIdx.x, parts = 1024 / cols, c = t % cols, p = t / cols;
+    const uint32_t per = (blocks + parts - 1) / parts, b0 = p * per, b1 = min(blocks, b0 + per);
     float v = 0.0f;
-    if (p < parts)
-        for (uint32_t b = p; b < blocks; b += parts) v += partial[(size_t)b * cols + c];
+    for (uint32_t b = b0; b < b1; ++b) v += partial[(size_t)b * cols + c];
     red[t] = v;
     __syncthreads();
     if (t < cols) {
@@ -974,11 +976,11 @@ int splits_for(int K) { return std::max(1, std::min(64, K / 1024)); }
 // Bias gradients: column sums of a [rows][cols] gradient (cols 32 or 128),
 // in a fixed order (partial sums in the split-K scratch).
 void colsum(mb_surrogate* s, const bf16* a, uint32_t rows, uint32_t cols, float* out) {
-    assert(cols <= 256 && 256 % cols == 0);
+    assert(cols <= 256 && 256 % cols == 0);  // both stages split 256 / 1024 threads into whole columns
     const uint32_t chunk = std::max<uint32_t>(1, (rows + kColsumBlocks - 1) / kColsumBlocks);
     const uint32_t blocks = (rows + chunk - 1) / chunk;
     colsum_partial_kernel<<<blocks, 256, 0, s->stream>>>(a, rows, cols, chunk, s->partial.p);
-    colsum_final_kernel<<<1, 256, 0, s->stream>>>(s->partial.p, blocks, cols, out);
+    colsum_final_kernel<<<1, 1024, 0, s->stream>>>(s->partial.p, blocks, cols, out);
 }
 
 // Backward of the last forward against targets s->t; gradients into s->g.
