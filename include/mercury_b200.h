@@ -289,6 +289,14 @@ MB_API mb_status mb_collect_springs(mb_context* ctx, uint16_t* pairs, uint8_t* m
 MB_API mb_status mb_get_launch_config(const mb_context* ctx, mb_launch_config* cfg);
 MB_API mb_status mb_set_launch_config(mb_context* ctx, const mb_launch_config* cfg);
 
+/* The step kernel the next launches of the uploaded batch use:
+ * *register_rows = 1 when each mass's row of incident springs is held in
+ * registers (resident bins of a 1,024-thread shape with at most one mass per
+ * thread, no face drag, and room for 8 more bytes of shared memory per
+ * spring), else 0; *smem_bytes = the dynamic shared memory per CTA of those
+ * launches.  Either pointer may be NULL.  No reference counterpart. */
+MB_API mb_status mb_get_step_variant(const mb_context* ctx, uint32_t* register_rows, uint32_t* smem_bytes);
+
 /* Launch plan of a population, computed on the host without a device:
  * the shape, bin count and path the automatic choice (or `cfg`, may be
  * NULL) would use on a GPU with `num_sms` SMs and `smem_bytes` of dynamic

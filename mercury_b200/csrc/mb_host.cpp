@@ -120,6 +120,8 @@ struct mb_context {
     // packing result
     mb::KernelShape shape{512, 8, 2};
     uint32_t n_bins = 0;
+    uint32_t max_bin_mass = 0, max_bin_springs = 0;  // most masses / springs in one bin
+    uint32_t smem_optin = 0;    // the device's shared memory per CTA (opt-in)
     uint32_t grid = 0;  // CTAs per step launch (0 = one per bin)
     uint32_t chunk = 1000;
     bool use_graph = true;
@@ -272,6 +274,8 @@ mb_status cuda_fail(mb_context* c, cudaError_t e, const char* what) {
 
 namespace mb_detail {
 
+uint32_t row_reg_smem(const mb_context* c);
+
 // Whether the step applies the face drag (water mode, rho != 0): split
 // robots are then packed with their faces (velocities exchanged with the
 // positions).
@@ -321,6 +325,12 @@ mb_status upload_packed(mb_context* ctx, const mb::Packed& out, bool* rows_faile
     ctx->shape = out.shape;
     ctx->n_bins = out.n_bins;
     ctx->grid = out.grid;
+    ctx->max_bin_mass = ctx->max_bin_springs = 0;
+    for (const mb::BinDesc& d : out.bins) {
+        ctx->max_bin_mass = std::max(ctx->max_bin_mass, d.n_mass);
+        ctx->max_bin_springs = std::max(ctx->max_bin_springs, d.n_spring);
+    }
+    if (!ctx->smem_optin) ctx->smem_optin = mb::max_step_smem(ctx->device);
     ctx->smem_bytes = out.max_smem;
     ctx->streamed = out.streamed;
     ctx->cluster = out.cluster;
@@ -1014,6 +1024,15 @@ mb_status mb_get_launch_config(const mb_context* ctx, mb_launch_config* cfg) {
     return MB_OK;
 }
 
+mb_status mb_get_step_variant(const mb_context* ctx, uint32_t* register_rows, uint32_t* smem_bytes) {
+    if (!ctx) return MB_ERR_ARGUMENT;
+    if (!ctx->loaded) return MB_ERR_STATE;
+    const uint32_t rr = mb_detail::row_reg_smem(ctx);
+    if (register_rows) *register_rows = rr ? 1u : 0u;
+    if (smem_bytes) *smem_bytes = rr ? rr : ctx->smem_bytes;
+    return MB_OK;
+}
+
 mb_status mb_plan_population(const mb_batch_desc* batch, const mb_launch_config* cfg, uint32_t num_sms,
                              uint32_t smem_bytes, mb_plan_stats* stats) {
     if (!batch || !stats || batch->n_robots == 0 || !batch->mass_offsets || !batch->spring_offsets ||
@@ -1210,6 +1229,19 @@ mb_status mb_set_state(mb_context* ctx, const float* pos, const float* vel) {
 // Internal helpers: C++ linkage, internal to this file.
 namespace mb_detail {
 
+// Shared memory of the register-row step kernel (every bin's usual need plus
+// 8 bytes per spring), or 0 when it does not apply: split or streamed bins,
+// a bin of more than one mass per thread, face drag, or too little shared
+// memory.
+uint32_t row_reg_smem(const mb_context* c) {
+    const bool faces = face_drag_on(c) && c->faces_packed;
+    if (c->streamed || c->cluster || faces || !mb::row_reg_supported(c->shape) ||
+        c->max_bin_mass > c->shape.threads)
+        return 0;
+    const uint64_t need = (uint64_t)c->smem_bytes + 8ull * c->max_bin_springs + 8ull;
+    return need <= c->smem_optin ? (uint32_t)need : 0u;
+}
+
 mb::StepParams make_params(mb_context* c, float t0, uint32_t steps, bool track) {
     mb::StepParams p{};
     p.bins = c->bins.p;
@@ -1251,6 +1283,10 @@ mb::StepParams make_params(mb_context* c, float t0, uint32_t steps, bool track) 
     p.fd = c->fd_scratch.p;
     p.face_coef = (float)(-(double)c->env.face_drag / 6.0);
     p.face_on = c->mode == MB_MODE_FORCE_WATER && c->env.face_drag != 0.0f && c->faces_packed ? 1u : 0u;
+    if (const uint32_t rr = row_reg_smem(c)) {
+        p.one_mass_per_thread = 1u;
+        p.smem_bytes = rr;
+    }
     return p;
 }
 
@@ -1323,7 +1359,8 @@ mb_status run(mb_context* c, uint32_t steps, bool track) {
             // kernel attributes cannot change inside a capture
             MB_CUDA(c, c->streamed ? mb::prepare_stream(1024, c->stream_mpt, (uint32_t)c->mode, track, c->smem_bytes)
                                     : c->cluster ? mb::prepare_split(c->shape, (uint32_t)c->mode, track, c->smem_bytes)
-                                    : mb::prepare_step(c->shape, (uint32_t)c->mode, track, c->smem_bytes));
+                                    : mb::prepare_step(c->shape, (uint32_t)c->mode, track,
+                                                       std::max(c->smem_bytes, row_reg_smem(c))));
             cudaGraph_t g;
             MB_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
             cudaError_t e = issue_chunks(c, t0, steps, track);
@@ -1343,7 +1380,8 @@ mb_status run(mb_context* c, uint32_t steps, bool track) {
     } else {
         MB_CUDA(c, c->streamed ? mb::prepare_stream(1024, c->stream_mpt, (uint32_t)c->mode, track, c->smem_bytes)
                                     : c->cluster ? mb::prepare_split(c->shape, (uint32_t)c->mode, track, c->smem_bytes)
-                                    : mb::prepare_step(c->shape, (uint32_t)c->mode, track, c->smem_bytes));
+                                    : mb::prepare_step(c->shape, (uint32_t)c->mode, track,
+                                                       std::max(c->smem_bytes, row_reg_smem(c))));
         cudaError_t e = issue_chunks(c, t0, steps, track);
         if (e != cudaSuccess) return cuda_fail(c, e, "step launch");
     }

@@ -85,6 +85,7 @@ struct StepParams {
     float4* fd;                   // streamed kernel: face forces of the current step
     float face_coef;              // -rho/6: -rho/2 of the face law and the 1/3 per corner
     uint32_t face_on;             // face drag active (water mode, rho != 0)
+    uint32_t one_mass_per_thread; // every bin has at most 1,024 masses (0 = unknown)
 };
 
 enum StepMode : uint32_t { kModeXpbd = 0, kModeForceLand = 1, kModeForceWater = 2 };
@@ -185,6 +186,10 @@ uint32_t max_step_smem(int device);
 
 // Whether a kernel shape is compiled in.
 bool shape_supported(const KernelShape& shape);
+// Whether the shape has a register-row twin (one mass per thread, rows of
+// incident springs in registers), which launch_step uses when
+// StepParams::one_mass_per_thread is set.
+bool row_reg_supported(const KernelShape& shape);
 
 // Centre of mass of the non-air masses of each robot: one warp per robot.
 cudaError_t launch_com(const float4* pos, const uint8_t* mass_mat,

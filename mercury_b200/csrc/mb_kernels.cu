@@ -151,10 +151,21 @@ __device__ __forceinline__ float4 face_force(const float4 x0, const float4 x1, c
                        __fmul_rn(c, __fmaf_rn(lift, uz, __fmul_rn(vn, vz))), 0.0f);
 }
 
-template <int T, int SPT, int MPT, int MODE, bool TRACK, bool SPLIT>
+// RW > 0 (register rows): each thread's row of up to RW entries is kept in
+// registers (two 16-bit entries per register, loaded once per bin), so that
+// the gather's correction loads no longer wait on a row-entry load and
+// issue RG at a time; a slice wider than RW reads its row from global
+// memory.  To make room, the springs leave the registers for {packed word,
+// mean length} pairs in shared memory after the rows' region (launched with
+// 8 bytes per spring more than the bin's usual shared memory).  One mass per
+// thread (MPT = 1), no face drag, no split bins.  Same operations in the same
+// order: same bits.
+template <int T, int SPT, int MPT, int MODE, bool TRACK, bool SPLIT, int RW = 0>
 __global__ void __launch_bounds__(T, 1024 / T) step_kernel(const StepParams p) {
     constexpr bool XPBD = MODE == kModeXpbd;
     constexpr bool FACES = MODE == kModeForceWaterFaces;  // face drag compiled in
+    constexpr int RG = 2;  // correction loads in flight per group
+    static_assert(RW == 0 || (MPT == 1 && !SPLIT && !FACES && RW % RG == 0), "register rows: one mass per thread");
     extern __shared__ float4 smem4[];
     const int tid = threadIdx.x;
     const float dt = p.dt;
@@ -188,7 +199,16 @@ __global__ void __launch_bounds__(T, 1024 / T) step_kernel(const StepParams p) {
         uint16_t* sfinc = reinterpret_cast<uint16_t*>(sfrow + bd.n_mass);
 
         const uint32_t n_mat = *p.n_mat;
-        for (uint32_t i = tid; i < bd.n_inc; i += T) sinc[i] = __ldg(&p.inc[bd.inc_begin + i]);
+        // register rows: the springs leave the registers to make room, into
+        // {packed word, mean length} pairs after the rows' region (8 bytes per
+        // spring beyond the bin's usual shared memory)
+        uint2* ssl = reinterpret_cast<uint2*>((reinterpret_cast<uintptr_t>(sinc + bd.n_inc) + 7u) & ~uintptr_t(7));
+        if (RW > 0)
+            for (uint32_t i = tid; i < bd.n_spring; i += T)
+                ssl[i] = make_uint2(__ldg(&p.spring_pair[bd.spring_begin + i]),
+                                    __float_as_uint(__ldg(&p.spring_lbar[bd.spring_begin + i])));
+        else
+            for (uint32_t i = tid; i < bd.n_inc; i += T) sinc[i] = __ldg(&p.inc[bd.inc_begin + i]);
         if (n_face) {
             for (uint32_t i = tid; i < n_face; i += T) sface[i] = __ldg(&p.faces[bd.face_begin + i]);
             for (uint32_t i = tid; i < bd.n_mass; i += T) sfrow[i] = __ldg(&p.face_row[bd.mass_begin + i]);
@@ -216,8 +236,10 @@ __global__ void __launch_bounds__(T, 1024 / T) step_kernel(const StepParams p) {
             st[j] = 0.0f;
             if (s < bd.n_spring) {
                 const uint32_t g = bd.spring_begin + s;
-                sw[j] = __ldg(&p.spring_pair[g]);
-                lb[j] = __ldg(&p.spring_lbar[g]);
+                if (RW == 0) {
+                    sw[j] = __ldg(&p.spring_pair[g]);
+                    lb[j] = __ldg(&p.spring_lbar[g]);
+                }
                 if (TRACK) st[j] = p.stress[__ldg(&p.spring_gidx[g]) & 0x7FFFFFFFu];
             }
         }
@@ -240,6 +262,18 @@ __global__ void __launch_bounds__(T, 1024 / T) step_kernel(const StepParams p) {
                 v[j] = make_float3(V.x, V.y, V.z);
                 const uint32_t sl = bd.slice_begin + m / kSliceWidth;
                 row[j] = (__ldg(&p.slice_off[sl]) + (m % kSliceWidth)) | (__ldg(&p.slice_width[sl]) << 20);
+            }
+        }
+        // register rows: entry k of this thread's mass in half k & 1 of rr[k / 2]
+        uint32_t rr[RW > 0 ? RW / 2 : 1];
+        if constexpr (RW > 0) {
+            const uint32_t w = row[0] >> 20;
+            const uint16_t* gp = p.inc + bd.inc_begin + (row[0] & 0xFFFFFu);
+#pragma unroll
+            for (int k = 0; k < RW; k += 2) {
+                const uint32_t lo = (uint32_t)k < w ? (uint32_t)__ldg(gp + k * kSliceWidth) : kPadEntry;
+                const uint32_t hi = (uint32_t)k + 1u < w ? (uint32_t)__ldg(gp + (k + 1) * kSliceWidth) : kPadEntry;
+                rr[k / 2] = lo | hi << 16;
             }
         }
         if (SPLIT)
@@ -292,9 +326,12 @@ __global__ void __launch_bounds__(T, 1024 / T) step_kernel(const StepParams p) {
             for (int j = 0; j < SPT; ++j) {
                 const uint32_t s = tid + j * T;
                 if (s >= bd.n_spring) break;
-                const float4 pa = X[pk_a(sw[j])], pb = X[pk_b(sw[j])];
-                const float2 mt = smat[pk_slot(sw[j])];
-                const float L = __fmaf_rn(lb[j], mt.x, lb[j]);
+                const uint2 q = RW > 0 ? ssl[s] : make_uint2(sw[j], __float_as_uint(lb[j]));
+                const uint32_t wj = q.x;
+                const float4 pa = X[pk_a(wj)], pb = X[pk_b(wj)];
+                const float2 mt = smat[pk_slot(wj)];
+                const float lbj = __uint_as_float(q.y);
+                const float L = __fmaf_rn(lbj, mt.x, lbj);
                 const float dx = __fsub_rn(pa.x, pb.x);
                 const float dy = __fsub_rn(pa.y, pb.y);
                 const float dz = __fsub_rn(pa.z, pb.z);
@@ -306,7 +343,7 @@ __global__ void __launch_bounds__(T, 1024 / T) step_kernel(const StepParams p) {
                 const float coef = __fmul_rn(lam, r);
                 sdp[s] = make_float4(__fmul_rn(coef, dx), __fmul_rn(coef, dy), __fmul_rn(coef, dz), 0.0f);
                 // stress: lambda/Lbar (reference, sim_kernel.cu:234); k (d - L)/Lbar (force)
-                if (TRACK) st[j] = __fadd_rn(st[j], __fmul_rn(XPBD ? lam : -lam, __frcp_rn(lb[j])));
+                if (TRACK) st[j] = __fadd_rn(st[j], __fmul_rn(XPBD ? lam : -lam, __frcp_rn(lbj)));
             }
             // face drag: the share of each corner, per face
             for (uint32_t f = tid; f < n_face; f += T) {
@@ -324,9 +361,34 @@ __global__ void __launch_bounds__(T, 1024 / T) step_kernel(const StepParams p) {
                 if (m >= bd.n_mass) break;
                 float ax = 0.0f, ay = 0.0f, az = 0.0f;
                 const uint16_t* rp = sinc + (row[j] & 0xFFFFFu);
-                const uint32_t w = row[j] >> 20;
+                const uint32_t w = row[j] >> 20;  // the same for the warp (one slice)
+                if (RW > 0 && w <= (uint32_t)RW) {
+                    // entries in [w, RW) are padding; a padding entry adds a
+                    // zero (acc + -0 == acc: a sum that starts at +0 is never -0)
+#pragma unroll
+                    for (int k0 = 0; k0 < RW; k0 += RG) {
+                        if ((uint32_t)k0 >= w) break;
+                        float4 c[RG];
+                        float sg[RG];
+#pragma unroll
+                        for (int u = 0; u < RG; ++u) {
+                            const int k = k0 + u;
+                            const uint32_t e = (k & 1) ? rr[k / 2] >> 16 : rr[k / 2] & 0xFFFFu;
+                            c[u] = e != kPadEntry ? sdp[e >> 1] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                            sg[u] = __uint_as_float(0x3f800000u | ((e & 1u) << 31));
+                        }
+#pragma unroll
+                        for (int u = 0; u < RG; ++u) {
+                            ax = __fmaf_rn(c[u].x, sg[u], ax);
+                            ay = __fmaf_rn(c[u].y, sg[u], ay);
+                            az = __fmaf_rn(c[u].z, sg[u], az);
+                        }
+                    }
+                } else
                 for (uint32_t k = 0; k < w; ++k) {
-                    const uint32_t e = rp[k * kSliceWidth];
+                    // (register rows: a slice wider than RW reads its row from global memory)
+                    const uint32_t e = RW > 0 ? __ldg(p.inc + bd.inc_begin + (row[j] & 0xFFFFFu) + k * kSliceWidth)
+                                              : rp[k * kSliceWidth];
                     if (e != kPadEntry) {
                         const float4 c = sdp[e >> 1];
                         const float sg = __uint_as_float(0x3f800000u | ((e & 1u) << 31));
@@ -674,6 +736,24 @@ const ShapeEntry kShapes[] = {
     MB_SHAPE(512, 16, 4, false),  MB_SHAPE(1024, 4, 1, false),  MB_SHAPE(1024, 6, 2, false),
     MB_SHAPE(1024, 8, 2, false),  MB_SHAPE(1024, 10, 2, false), MB_SHAPE(1024, 12, 2, false),
 };
+// register-row twins of the 1,024-thread shapes (one mass per thread; no
+// face drag): launch_step uses one when every bin has at most 1,024 masses
+#define MB_RR(T, S, RW)                                                                          \
+    {                                                                                            \
+        T, S, 1, {                                                                               \
+            {step_kernel<T, S, 1, kModeXpbd, false, false, RW>,                                  \
+             step_kernel<T, S, 1, kModeXpbd, true, false, RW>},                                  \
+                {step_kernel<T, S, 1, kModeForceLand, false, false, RW>,                         \
+                 step_kernel<T, S, 1, kModeForceLand, true, false, RW>},                         \
+                {step_kernel<T, S, 1, kModeForceWater, false, false, RW>,                        \
+                 step_kernel<T, S, 1, kModeForceWater, true, false, RW>},                        \
+                {nullptr, nullptr},                                                              \
+        }                                                                                        \
+    }
+constexpr int kRowRegWidth = 26;  // register rows: entries per mass (lattice robots: at most 26)
+const ShapeEntry kRowRegShapes[] = {MB_RR(1024, 8, kRowRegWidth), MB_RR(1024, 10, kRowRegWidth),
+                                    MB_RR(1024, 12, kRowRegWidth)};
+#undef MB_RR
 // the parts of split robots (thread-block clusters)
 const ShapeEntry kSplitShapes[] = {
     MB_SHAPE(1024, 8, 2, true),
@@ -715,6 +795,15 @@ const ShapeEntry* find_shape(const KernelShape& s) {
     return nullptr;
 }
 
+// The register-row twin of a 1,024-thread shape, for launches whose bins all
+// hold at most 1,024 masses and that have no face drag.
+const ShapeEntry* find_row_reg(const KernelShape& s, const StepParams& p) {
+    if (s.threads != 1024 || !p.one_mass_per_thread || p.face_on) return nullptr;
+    for (const auto& e : kRowRegShapes)
+        if (e.spt == s.spt) return &e;
+    return nullptr;
+}
+
 const ShapeEntry* find_split(const KernelShape& s) {
     for (const auto& e : kSplitShapes)
         if (e.threads == s.threads && e.spt == s.spt && e.mpt == s.mpt) return &e;
@@ -734,6 +823,13 @@ uint32_t max_step_smem(int device) {
 }
 
 bool shape_supported(const KernelShape& shape) { return find_shape(shape) != nullptr; }
+
+bool row_reg_supported(const KernelShape& shape) {
+    if (shape.threads != 1024) return false;
+    for (const auto& e : kRowRegShapes)
+        if (e.spt == shape.spt) return true;
+    return false;
+}
 
 bool split_supported(const KernelShape& shape) { return find_split(shape) != nullptr; }
 
@@ -775,6 +871,11 @@ cudaError_t prepare_step(const KernelShape& shape, uint32_t mode, bool track, ui
     const ShapeEntry* e = find_shape(shape);
     if (!e || mode > kModeForceWater) return cudaErrorInvalidValue;
     cudaError_t r = cudaFuncSetAttribute(e->fn[mode][track ? 1 : 0], cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem_bytes);
+    if (shape.threads == 1024)  // the register-row twin, when there is one
+        for (const auto& t : kRowRegShapes)
+            if (r == cudaSuccess && t.spt == shape.spt)
+                r = cudaFuncSetAttribute(t.fn[mode][track ? 1 : 0], cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem_bytes);
     if (r == cudaSuccess && mode == kModeForceWater)  // and the face-drag variant
         r = cudaFuncSetAttribute(e->fn[kModeForceWaterFaces][track ? 1 : 0],
@@ -867,6 +968,7 @@ cudaError_t launch_step(const StepParams& p, const KernelShape& shape, cudaStrea
     if (p.mode > kModeForceWater) return cudaErrorInvalidValue;
     const uint32_t grid = p.grid ? std::min(p.grid, p.n_bins) : p.n_bins;
     const uint32_t variant = p.mode == kModeForceWater && p.face_on ? kModeForceWaterFaces : p.mode;
+    if (const ShapeEntry* rr = find_row_reg(shape, p)) e = rr;
     e->fn[variant][p.track ? 1 : 0]<<<grid, shape.threads, p.smem_bytes, s>>>(p);
     return cudaGetLastError();
 }

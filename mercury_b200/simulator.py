@@ -310,6 +310,14 @@ class Simulator:
         _lib.check(_lib.LIB.mb_get_launch_config(self._ctx, ctypes.byref(c)), self._ctx)
         return {f: getattr(c, f) for f, _ in c._fields_}
 
+    def step_variant(self) -> dict:
+        """The step kernel the next launches use (mb_get_step_variant):
+        register_rows (each mass's row held in registers) and the dynamic
+        shared memory per CTA."""
+        rr, smem = ctypes.c_uint32(), ctypes.c_uint32()
+        _lib.check(_lib.LIB.mb_get_step_variant(self._ctx, ctypes.byref(rr), ctypes.byref(smem)), self._ctx)
+        return {"register_rows": rr.value, "smem_bytes": smem.value}
+
     def set_launch_config(self, threads=0, springs_per_thread=0, masses_per_thread=0, bins=0,
                           chunk=0, use_graph=1, streamed=0, cluster=0) -> None:
         c = _lib.LaunchConfig(threads, springs_per_thread, masses_per_thread, bins, chunk, use_graph,
