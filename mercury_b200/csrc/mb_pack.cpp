@@ -553,6 +553,46 @@ void build_faces(const mb_batch_desc* b, const std::vector<RobotPack>& packs,
 // rows_on_device: only the springs and masses; the rows get a region of
 // generous capacity (twice the rank-layout estimate plus the alignment
 // slack) for the device to build them in.
+// Placement of a resident bin's springs (packed words a | b << 12 | ...)
+// for the step kernel's endpoint loads: lanes 8q .. 8q + 7 of a warp form
+// one shared-memory wavefront of 16-byte loads, conflict-free when their
+// masses differ mod 8.  Greedy, in order: each group of 8 slots takes the
+// earliest springs, within a window of the next kWindow unplaced ones, whose
+// a and b are both new mod 8 in the group, then fills any slot left with the
+// earliest unplaced spring.  Returns order[new position] = old position.
+std::vector<uint32_t> bank_order(const std::vector<uint32_t>& words) {
+    constexpr uint32_t kWindow = 64;
+    const uint32_t n = (uint32_t)words.size();
+    std::vector<uint32_t> order;
+    order.reserve(n);
+    std::vector<uint8_t> taken(n, 0);
+    uint32_t head = 0;
+    while (order.size() < n) {
+        while (taken[head]) ++head;
+        uint32_t used_a = 0, used_b = 0, got = 0;
+        const uint32_t want = std::min<uint32_t>(8, n - (uint32_t)order.size());
+        uint32_t seen = 0;
+        for (uint32_t i = head; i < n && seen < kWindow && got < want; ++i) {
+            if (taken[i]) continue;
+            ++seen;
+            const uint32_t ba = 1u << (words[i] & 7u), bb = 1u << ((words[i] >> 12) & 7u);
+            if ((used_a & ba) || (used_b & bb)) continue;
+            used_a |= ba;
+            used_b |= bb;
+            taken[i] = 1;
+            order.push_back(i);
+            ++got;
+        }
+        for (uint32_t i = head; i < n && got < want; ++i)
+            if (!taken[i]) {
+                taken[i] = 1;
+                order.push_back(i);
+                ++got;
+            }
+    }
+    return order;
+}
+
 void build_bin(const mb_batch_desc* b, const std::vector<RobotPack>& packs,
                const std::vector<uint32_t>& robots, const std::vector<int>& slot_of, bool streamed,
                bool rows_on_device, BinLocal& L) {
@@ -566,20 +606,33 @@ void build_bin(const mb_batch_desc* b, const std::vector<RobotPack>& packs,
     L.pair.reserve(ns);
     L.lbar.reserve(ns);
     std::vector<uint32_t> row_start(nm + 1, 0);
-    uint32_t mbase = 0;
+    // the bin's springs robot by robot, each robot's in (b - a, a) order
+    std::vector<uint32_t> words(ns), gids(ns);
+    uint32_t mbase = 0, k = 0;
     for (uint32_t r : robots) {
         const int64_t m0 = b->mass_offsets[r], s0 = b->spring_offsets[r];
         for (uint32_t i = 0; i < packs[r].n_mass; ++i) L.mass_gidx.push_back((uint32_t)(m0 + i));
         for (uint32_t ls : packs[r].springs) {
             const int64_t g = s0 + ls;
             const uint32_t pa = mbase + b->pairs[2 * g], pc = mbase + b->pairs[2 * g + 1];
-            L.spring_gidx.push_back((uint32_t)g);
-            L.pair.push_back(pa | (pc << 12) | ((uint32_t)slot_of[b->spring_material[g]] << 24));
-            L.lbar.push_back(b->lbar[g]);
+            gids[k] = (uint32_t)g;
+            words[k++] = pa | (pc << 12) | ((uint32_t)slot_of[b->spring_material[g]] << 24);
             row_start[pa + 1]++;
             row_start[pc + 1]++;
         }
         mbase += packs[r].n_mass;
+    }
+    // resident bins: springs placed so that the 8 springs of every
+    // quarter-warp read distinct 16-byte bank groups of the predicted
+    // positions at both ends (newpos: old position -> packed position)
+    std::vector<uint32_t> order = streamed ? std::vector<uint32_t>{} : bank_order(words);
+    std::vector<uint32_t> newpos(ns);
+    for (uint32_t i = 0; i < ns; ++i) {
+        const uint32_t o = order.empty() ? i : order[i];
+        newpos[o] = i;
+        L.spring_gidx.push_back(gids[o]);
+        L.pair.push_back(words[o]);
+        L.lbar.push_back(b->lbar[gids[o]]);
     }
     build_faces(b, packs, robots, nm, L);
     const uint32_t face_smem = streamed ? stream_face_smem_bytes(nm, L.n_face)
@@ -611,12 +664,12 @@ void build_bin(const mb_batch_desc* b, const std::vector<RobotPack>& packs,
             for (uint32_t k = (uint32_t)sp.size(); k-- > 0;) {
                 const int64_t g = s0 + sp[k];
                 const uint32_t a = b->pairs[2 * g], c = b->pairs[2 * g + 1];
-                ents[fill[base + c]++] = {a, sp[k], 1u, sb + k, a};
+                ents[fill[base + c]++] = {a, sp[k], 1u, newpos[sb + k], a};
             }
             for (uint32_t k = 0; k < sp.size(); ++k) {
                 const int64_t g = s0 + sp[k];
                 const uint32_t a = b->pairs[2 * g], c = b->pairs[2 * g + 1];
-                ents[fill[base + a]++] = {c, sp[k], 0u, sb + k, c};
+                ents[fill[base + a]++] = {c, sp[k], 0u, newpos[sb + k], c};
             }
             base += packs[r].n_mass;
             sb += (uint32_t)sp.size();
