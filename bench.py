@@ -367,9 +367,11 @@ def _device_rate(sim, active, steps, track, dev):
 
 
 # DRAM bytes (read + write) of one 1,000-step launch of the step kernel on
-# the uneven population in its tuned configuration (ncu, dram__bytes_read.sum
-# + dram__bytes_write.sum): the state and topology, read once per launch.
-STEP_TRAFFIC = {("uneven", 1024, 8, 2, 296, 1000): 24.65e6 + 12.0e3}
+# the uneven population in the configurations the tuner picks (ncu,
+# dram__bytes_read.sum + dram__bytes_write.sum): the state and topology, read
+# once per launch.
+STEP_TRAFFIC = {("uneven", 1024, 8, 2, 296, 1000): 24.66e6 + 2.0e3,
+                ("uneven", 1024, 10, 2, 296, 1000): 24.67e6 + 0.0}
 
 
 def _step_traffic(workload, cfg, active):

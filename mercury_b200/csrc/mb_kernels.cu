@@ -203,6 +203,16 @@ __global__ void __launch_bounds__(T, 1024 / T) step_kernel(const StepParams p) {
         // {packed word, mean length} pairs after the rows' region (8 bytes per
         // spring beyond the bin's usual shared memory)
         uint2* ssl = reinterpret_cast<uint2*>((reinterpret_cast<uintptr_t>(sinc + bd.n_inc) + 7u) & ~uintptr_t(7));
+        if (RW > 0) {
+            // the host sizes the launch for every bin; a bin that would still
+            // not fit is skipped and flagged (bit 1) rather than overrun
+            uint32_t dyn;
+            asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
+            if (reinterpret_cast<const char*>(ssl + bd.n_spring) - reinterpret_cast<const char*>(smem4) > dyn) {
+                if (tid == 0) atomicOr(&p.bin_flags[b], 2u);
+                continue;
+            }
+        }
         if (RW > 0)
             for (uint32_t i = tid; i < bd.n_spring; i += T)
                 ssl[i] = make_uint2(__ldg(&p.spring_pair[bd.spring_begin + i]),

@@ -278,8 +278,10 @@ void preprocess(const mb_batch_desc* b, uint32_t r, RobotPack& p) {
 
 // LPT assignment of robots to `nb` bins by cost, within the shape's and the
 // shared memory's capacity.
+// spring_extra: shared-memory bytes a bin needs per spring beyond
+// bin_smem_bytes (plus 8 bytes of alignment when nonzero).
 bool plan_bins(const std::vector<RobotPack>& packs, uint32_t nb, const KernelShape& sh,
-               uint32_t smem_cap, std::vector<std::vector<uint32_t>>& plan) {
+               uint32_t smem_cap, std::vector<std::vector<uint32_t>>& plan, uint32_t spring_extra = 0) {
     const uint32_t n = (uint32_t)packs.size();
     std::vector<uint32_t> order(n);
     for (uint32_t i = 0; i < n; ++i) order[i] = i;
@@ -295,7 +297,9 @@ bool plan_bins(const std::vector<RobotPack>& packs, uint32_t nb, const KernelSha
         for (uint32_t b = 0; b < nb; ++b) {
             if (bm[b] + p.n_mass > cap_m || bs[b] + p.springs.size() > cap_s) continue;
             if (bin_smem_bytes((uint32_t)(bm[b] + p.n_mass), (uint32_t)(bs[b] + p.springs.size()),
-                               (uint32_t)(bi[b] + p.inc_estimate)) + bx[b] + p.face_smem > smem_cap)
+                               (uint32_t)(bi[b] + p.inc_estimate)) + bx[b] + p.face_smem +
+                    (spring_extra ? spring_extra * (bs[b] + p.springs.size()) + 8u : 0u) >
+                smem_cap)
                 continue;
             if (best < 0 || load[b] < load[best]) best = (int)b;
         }
@@ -320,7 +324,7 @@ bool plan_bins(const std::vector<RobotPack>& packs, uint32_t nb, const KernelSha
 // and the caller falls back to plan_bins.
 bool plan_bins_grouped(const std::vector<RobotPack>& packs, uint32_t nb, uint32_t groups,
                        const KernelShape& sh, uint32_t smem_cap,
-                       std::vector<std::vector<uint32_t>>& plan) {
+                       std::vector<std::vector<uint32_t>>& plan, uint32_t spring_extra = 0) {
     if (groups == 0 || nb <= groups || nb % groups) return false;
     const uint32_t per = nb / groups;
     const uint32_t n = (uint32_t)packs.size();
@@ -354,7 +358,9 @@ bool plan_bins_grouped(const std::vector<RobotPack>& packs, uint32_t nb, uint32_
             for (uint32_t j = 0; j < per; ++j) {
                 if (bm[j] + p.n_mass > cap_m || bs[j] + p.springs.size() > cap_s) continue;
                 if (bin_smem_bytes((uint32_t)(bm[j] + p.n_mass), (uint32_t)(bs[j] + p.springs.size()),
-                                   (uint32_t)(bi[j] + p.inc_estimate)) + bx[j] + p.face_smem > smem_cap)
+                                   (uint32_t)(bi[j] + p.inc_estimate)) + bx[j] + p.face_smem +
+                        (spring_extra ? spring_extra * (bs[j] + p.springs.size()) + 8u : 0u) >
+                    smem_cap)
                     continue;
                 if (best < 0 || load[j] < load[best]) best = (int)j;
             }
@@ -1295,10 +1301,19 @@ mb_status pack_population(const mb_batch_desc* b, const PackOptions& o, Packed& 
     const uint32_t sms = std::max<uint32_t>(o.sms, 1);
     std::vector<std::vector<uint32_t>> plan;
     bool ok = false;
+    // Automatic choice: a shape with a register-row variant is first planned
+    // for it -- at most one mass per thread in every bin and room for its 8
+    // bytes of shared memory per spring -- then, if that fails, as usual.
+    std::vector<std::pair<KernelShape, bool>> attempts;
     for (const auto& sh : shapes) {
+        if (!o.override.threads && out.n_faces == 0 && max_m <= sh.threads && row_reg_supported(sh))
+            attempts.push_back({sh, true});
+        attempts.push_back({sh, false});
+    }
+    for (const auto& [sh, one_mass] : attempts) {
         if (!shape_supported(sh)) continue;
         const uint64_t cap_s = std::min<uint64_t>((uint64_t)sh.threads * sh.spt, kMaxBinSprings);
-        const uint64_t cap_m = std::min<uint64_t>((uint64_t)sh.threads * sh.mpt, 4096);
+        const uint64_t cap_m = std::min<uint64_t>((uint64_t)sh.threads * (one_mass ? 1u : sh.mpt), 4096);
         if (max_s > cap_s || max_m > cap_m) continue;
         uint32_t nb = o.override.bins;
         const bool fixed = nb != 0;
@@ -1328,15 +1343,23 @@ mb_status pack_population(const mb_batch_desc* b, const PackOptions& o, Packed& 
             // (plan_bins_grouped); otherwise one CTA per bin.
             grid = 0;
             bool planned = false;
+            const KernelShape psh{sh.threads, sh.spt, one_mass ? 1u : sh.mpt};
+            const uint32_t extra = one_mass ? 8u : 0u;
             if (R >= sms && nb >= 2 * wave && nb % wave == 0 &&
-                plan_bins_grouped(packs, nb, wave, sh, o.smem_cap, plan)) {
+                plan_bins_grouped(packs, nb, wave, psh, o.smem_cap, plan, extra)) {
                 planned = true;
                 grid = wave;
             }
-            if (!planned) planned = plan_bins(packs, nb, sh, o.smem_cap, plan);
+            if (!planned) planned = plan_bins(packs, nb, psh, o.smem_cap, plan, extra);
             if (planned) {
                 build_all(b, packs, plan, slot_of, false, threads, out, o.rows_on_device);
-                if (out.max_smem <= o.smem_cap) {
+                uint64_t need = out.max_smem;
+                if (one_mass) {
+                    uint32_t most = 0;
+                    for (const BinDesc& d : out.bins) most = std::max(most, d.n_spring);
+                    need += 8ull * most + 8ull;
+                }
+                if (need <= o.smem_cap) {
                     ok = true;
                     break;
                 }

@@ -12,10 +12,23 @@ def test_uneven_population_fills_whole_waves_evenly():
     st = mb.plan(b)
     assert st["streamed"] == 0 and st["bins"] % 148 == 0
     assert st["active_springs"] == b.active_springs() and st["masses"] == b.n_masses
-    assert st["max_bin_springs"] <= 1.1 * st["min_bin_springs"]
+    # several waves: one CTA per group of bins, and the groups are what must be even
+    if st["ctas"] < st["bins"]:
+        assert st["ctas"] == 148 and st["max_cta_springs"] <= 1.05 * st["min_cta_springs"]
+    else:
+        assert st["max_bin_springs"] <= 1.1 * st["min_bin_springs"]
     assert st["max_smem_bytes"] <= 232448
     assert st["incidence_entries"] - st["incidence_padding"] == 2 * st["active_springs"]
     assert st["aligned_slices"] > 5 * st["rank_slices"]
+
+
+def test_automatic_plan_leaves_room_for_register_rows():
+    """Bins of a 1,024-thread shape hold at most 1,024 masses, with room for
+    the register-row kernel's 8 bytes of shared memory per spring."""
+    b = robots.population_batch("uneven")
+    st = mb.plan(b)
+    assert st["threads"] == 1024 and st["masses"] / st["bins"] <= 1024
+    assert st["max_smem_bytes"] + 8 * st["max_bin_springs"] + 8 <= 232448
 
 
 def test_large_robots_are_split_over_clusters():
