@@ -32,6 +32,14 @@ by the share of voxels from each (lineage correction).  Training
 draws every sample in a random orientation; per generation, a few steps
 whose batches are half from the newest generation.
 Plain: every child is simulated.
+
+Both methods keep the fitness of every genome they have simulated (the
+simulator is deterministic to the bit, so a copy needs no simulation): a
+child identical to a simulated genome -- about a quarter of the children,
+the unchanged copies of a parent and the crossovers of a parent with
+itself -- takes its known fitness, and only the new children are simulated
+or, when screened, ranked by the surrogate.  The elite pool holds distinct
+genomes.
 """
 from __future__ import annotations
 
@@ -74,13 +82,15 @@ def random_genomes(rng: np.random.Generator, n: int) -> np.ndarray:
 
 
 class Evaluator:
-    """Simulates genomes on one GPU; one Simulator per batch size so that
-    each keeps its packing plan.  With `autotune`, the launch configuration
+    """Simulates genomes on one GPU; one Simulator per batch size (rounded
+    up to a multiple of `bucket` with copies of the first genome, whose
+    results are dropped) so that each keeps its packing plan.  With `autotune`, the launch configuration
     of each batch size is tuned on its first call (measured on 6x6x6 genomes:
     no faster than the automatic plan, and seconds of tuning per size)."""
 
-    def __init__(self, device: int = 0, duration: float = DURATION, autotune: bool = False):
+    def __init__(self, device: int = 0, duration: float = DURATION, autotune: bool = False, bucket: int = 256):
         self.device = device
+        self.bucket = bucket
         self.duration = duration
         self.autotune = autotune
         self._sims: dict[int, S.Simulator] = {}
@@ -100,7 +110,12 @@ class Evaluator:
 
     def __call__(self, genomes: np.ndarray) -> np.ndarray:
         n = len(genomes)
-        sim = self._sim(n)
+        if n == 0:
+            return np.zeros(0, np.float32)
+        size = -(-n // self.bucket) * self.bucket
+        if size > n:
+            genomes = np.concatenate([genomes, np.repeat(genomes[:1], size - n, axis=0)])
+        sim = self._sim(size)
         cells = to_cells(genomes)
         if self.autotune and n not in self._tuned:
             # launch configuration for this batch size, tuned once on these
@@ -119,7 +134,7 @@ class Evaluator:
         fit[~np.isfinite(fit)] = 0.0
         self.simulated += n
         self.last_steps = steps
-        return fit.astype(np.float32)
+        return fit[:n].astype(np.float32)
 
 
 def make_children(rng: np.random.Generator, parents: np.ndarray, fitness: np.ndarray, n: int,
@@ -164,16 +179,44 @@ def make_children(rng: np.random.Generator, parents: np.ndarray, fitness: np.nda
 
 @dataclass
 class Pool:
-    """Elite pool of simulated genomes and the surrogate's training set."""
+    """Elite pool: the best distinct simulated genomes."""
     size: int = 256
     genomes: np.ndarray = field(default_factory=lambda: np.zeros((0, 216), np.uint8))
     fitness: np.ndarray = field(default_factory=lambda: np.zeros(0, np.float32))
 
     def add(self, g: np.ndarray, f: np.ndarray) -> None:
-        G = np.concatenate([self.genomes, g])
-        F = np.concatenate([self.fitness, f])
-        keep = np.argsort(-F, kind="stable")[: self.size]
+        G = np.concatenate([self.genomes, np.asarray(g, np.uint8)])
+        F = np.concatenate([self.fitness, np.asarray(f, np.float32)])
+        order = np.argsort(-F, kind="stable")
+        keep, seen = [], set()
+        for i in order:  # best first; a genome already kept is a copy
+            k = G[i].tobytes()
+            if k in seen:
+                continue
+            seen.add(k)
+            keep.append(i)
+            if len(keep) == self.size:
+                break
         self.genomes, self.fitness = G[keep], F[keep]
+
+
+class Memo:
+    """Fitness of every simulated genome, by genome bytes."""
+
+    def __init__(self):
+        self.d: dict[bytes, float] = {}
+
+    def add(self, g: np.ndarray, f: np.ndarray) -> None:
+        for row, v in zip(np.asarray(g, np.uint8), f):
+            self.d[row.tobytes()] = float(v)
+
+    def lookup(self, g: np.ndarray):
+        """(known mask, fitness with NaN where unknown)."""
+        f = np.array([self.d.get(row.tobytes(), np.nan) for row in np.asarray(g, np.uint8)], np.float32)
+        return ~np.isnan(f), f
+
+    def __len__(self):
+        return len(self.d)
 
 
 class Dataset:
@@ -217,6 +260,7 @@ class ScreenedEvolution:
         self.kappa = kappa  # screening bonus per unit of spread over the orientations
         self.data = Dataset()
         self.pool = Pool()
+        self.memo = Memo()
         self.mu, self.sd = 0.0, 1.0
         self.trained_steps = 0
 
@@ -266,6 +310,7 @@ class ScreenedEvolution:
             f = self.ev(g)
             self.data.add(g, f)
             self.pool.add(g, f)
+            self.memo.add(g, f)
         t1 = time.perf_counter()
         self._norm()
         loss = self.train(int(epochs * n / self.batch), self.lr, cosine=True)
@@ -284,48 +329,67 @@ class ScreenedEvolution:
         t0 = time.perf_counter()
         kids, ia, ib, sb = make_children(self.rng, self.pool.genomes, self.pool.fitness, self.children,
                                          lineage=True)
+        known, fk = self.memo.lookup(kids)
+        nov = np.nonzero(~known)[0]
         t1 = time.perf_counter()
-        pred, spread = self.predict(kids, spread=True)
-        if self.lineage_correction:
-            # a child is a near copy of simulated parents: carry over the
-            # surrogate's error on them
-            res = self.pool.fitness - self.predict(self.pool.genomes) * self.sd - self.mu
-            pred = pred * self.sd + self.mu + (1.0 - sb) * res[ia] + sb * res[ib]
-        # children the orientations disagree on get a bonus (their fitness is
-        # the least certain), in fitness units
-        score = pred + self.kappa * self.sd * spread
-        sel = self.select(score)
+        pred = np.full(len(kids), np.nan)
+        score = np.full(len(kids), np.nan)
+        sel = nov[:0]
+        if len(nov):
+            p, spread = self.predict(kids[nov], spread=True)
+            if self.lineage_correction:
+                # a child is a near copy of simulated parents: carry over the
+                # surrogate's error on them
+                res = self.pool.fitness - self.predict(self.pool.genomes) * self.sd - self.mu
+                p = p * self.sd + self.mu + (1.0 - sb[nov]) * res[ia[nov]] + sb[nov] * res[ib[nov]]
+            pred[nov] = p
+            # children the orientations disagree on get a bonus (their fitness
+            # is the least certain), in fitness units
+            score[nov] = p + self.kappa * self.sd * spread
+            sel = nov[self.select(score[nov])]
         t2 = time.perf_counter()
         f = self.ev(kids[sel])
         t3 = time.perf_counter()
         self.data.add(kids[sel], f)
+        self.memo.add(kids[sel], f)
         self.pool.add(kids[sel], f)
-        self.train(self.steps, self.finetune_lr, recent=(kids[sel], f))
+        if len(sel):
+            self.train(self.steps, self.finetune_lr, recent=(kids[sel], f))
         t4 = time.perf_counter()
         out = {"wall_s": t4 - t0, "children_s": t1 - t0, "screen_s": t2 - t1, "simulate_s": t3 - t2,
-               "train_s": t4 - t3, "simulated": len(sel), "best": float(self.pool.fitness[0])}
-        if truth:  # ground truth for every child, outside the timed region
-            ft = self.ev(kids)
-            out.update(quality(pred, ft, sel, self.screen, score))
+               "train_s": t4 - t3, "simulated": len(sel), "known": int(known.sum()),
+               "best": float(self.pool.fitness[0])}
+        if truth:  # ground truth for every new child, outside the timed region
+            ft = fk.copy()
+            ft[nov] = self.ev(kids[nov])
+            out.update(quality(pred, ft, sel, self.screen, score, known=known))
         return out
 
 
 class PlainEvolution:
-    def __init__(self, evaluator: Evaluator, seed: int = 0, children: int = 4096, pool: Pool | None = None):
+    """Every new child simulated (copies of simulated genomes take their
+    known fitness)."""
+
+    def __init__(self, evaluator: Evaluator, seed: int = 0, children: int = 4096, pool: Pool | None = None,
+                 memo: Memo | None = None):
         self.ev = evaluator
         self.rng = np.random.default_rng(seed)
         self.children = children
         self.pool = pool or Pool()
+        self.memo = memo or Memo()
 
     def generation(self) -> dict:
         t0 = time.perf_counter()
         kids = make_children(self.rng, self.pool.genomes, self.pool.fitness, self.children)
+        known, f = self.memo.lookup(kids)
+        nov = np.nonzero(~known)[0]
         t1 = time.perf_counter()
-        f = self.ev(kids)
+        f[nov] = self.ev(kids[nov])
         t2 = time.perf_counter()
+        self.memo.add(kids[nov], f[nov])
         self.pool.add(kids, f)
         return {"wall_s": time.perf_counter() - t0, "children_s": t1 - t0, "simulate_s": t2 - t1,
-                "simulated": len(kids), "best": float(self.pool.fitness[0])}
+                "simulated": len(nov), "known": int(known.sum()), "best": float(self.pool.fitness[0])}
 
 
 def race(methods: dict, seconds: float) -> dict:
@@ -351,25 +415,50 @@ def best_at(curve: list, seconds: float) -> float:
 
 
 def quality(pred: np.ndarray, truth: np.ndarray, selected: np.ndarray, screen: float,
-            score: np.ndarray | None = None, fractions=(0.2, 0.25, 0.3, 0.35, 0.4, 0.5)) -> dict:
-    """Spearman rank correlation of predictions and simulated fitness over
-    all children; top-10% recall: the share of the truly best 10% that the
-    screen sends to simulation (selected = surrogate top `screen` + audit);
-    also the share inside the surrogate's own top 10%, and what random
-    screening of the same size would give.  With the screening `score`:
-    the recall of its top fraction alone (no audit) for each of
-    `fractions`."""
+            score: np.ndarray | None = None, fractions=(0.2, 0.25, 0.3, 0.35, 0.4, 0.5),
+            known: np.ndarray | None = None) -> dict:
+    """Quality of a screen over the children of one generation.  `known`
+    marks children whose fitness was known without simulation (copies of
+    simulated genomes); the others are new, and only they are predicted,
+    ranked and screened.
+
+    - top10_recall: the share of the truly best 10% of all children whose
+      fitness the generation obtained -- known, or simulated because the
+      screen (surrogate top `screen` + audit) selected them;
+    - top10_recall_new: the share of the truly best 10% of the new children
+      that the screen selected (the surrogate's own part);
+    - top10_recall_top10: the share of that best 10% inside the surrogate's
+      own top 10% of the new children;
+    - random_screen_recall: what random screening of the same size would
+      give on the new children;
+    - spearman: rank correlation of predictions and simulated fitness over
+      the new children;
+    - with the screening `score`: top10_recall_at, the recall on the new
+      children of the score's top fraction alone (no audit) for each of
+      `fractions`."""
     from scipy.stats import spearmanr
     n = len(truth)
-    top = set(np.argsort(-truth, kind="stable")[: n // 10].tolist())
+    known = np.zeros(n, bool) if known is None else np.asarray(known, bool)
+    new = np.nonzero(~known)[0]
+    m = len(new)
     sel = set(np.asarray(selected).tolist())
-    own = set(np.argsort(-pred, kind="stable")[: n // 10].tolist())
-    return {
-        "spearman": float(spearmanr(pred, truth).correlation),
-        "top10_recall": len(top & sel) / len(top),
-        "top10_recall_top10": len(top & own) / len(top),
-        "random_screen_recall": len(sel) / n,
-        **({"top10_recall_at": {str(fr): len(top & set(np.argsort(-score, kind="stable")[: int(round(fr * n))]
-                                                        .tolist())) / len(top) for fr in fractions}}
-           if score is not None else {}),
+    top = np.argsort(-truth, kind="stable")[: n // 10]
+    top_new = new[np.argsort(-truth[new], kind="stable")[: m // 10]]
+    own = new[np.argsort(-pred[new], kind="stable")[: m // 10]]
+    tn = set(top_new.tolist())
+
+    def rec(s):
+        return len(tn & s) / len(tn) if tn else 1.0
+    out = {
+        "spearman": float(spearmanr(pred[new], truth[new]).correlation) if m > 1 else float("nan"),
+        "top10_recall": float(np.mean([(i in sel) or known[i] for i in top])) if len(top) else 1.0,
+        "top10_recall_new": rec(sel),
+        "top10_recall_top10": rec(set(own.tolist())),
+        "random_screen_recall": len(sel) / m if m else 1.0,
+        "known_share": float(known.mean()) if n else 0.0,
+        "known_in_top10": float(np.mean(known[top])) if len(top) else 0.0,
     }
+    if score is not None:
+        ranked = new[np.argsort(-score[new], kind="stable")]
+        out["top10_recall_at"] = {str(fr): rec(set(ranked[: int(round(fr * m))].tolist())) for fr in fractions}
+    return out

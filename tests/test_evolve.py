@@ -40,6 +40,37 @@ def test_pool_keeps_the_best():
     assert (pool.genomes[0] == 9).all()
 
 
+def test_pool_holds_distinct_genomes():
+    pool = evolve.Pool(size=3)
+    g = np.arange(4, dtype=np.uint8)[:, None].repeat(216, 1)
+    pool.add(np.concatenate([g, g]), np.array([1, 5, 3, 2, 1, 5, 3, 2], np.float32))
+    assert list(pool.fitness) == [5, 3, 2]
+    assert [int(x[0]) for x in pool.genomes] == [1, 2, 3]
+
+
+def test_memo_finds_copies():
+    m = evolve.Memo()
+    g = np.random.default_rng(0).integers(0, 5, (5, 216)).astype(np.uint8)
+    m.add(g[:3], np.array([0.1, 0.2, 0.3], np.float32))
+    known, f = m.lookup(np.concatenate([g[2:], g[:1]]))
+    assert list(known) == [True, False, False, True]
+    assert f[0] == np.float32(0.3) and f[3] == np.float32(0.1) and np.isnan(f[1:3]).all()
+
+
+def test_quality_counts_known_children_as_evaluated():
+    truth = np.arange(100, dtype=np.float32)
+    known = np.zeros(100, bool)
+    known[95:] = True  # half of the best 10 known, never screened
+    pred = truth.copy()
+    pred[known] = np.nan
+    q = evolve.quality(pred, truth, np.arange(90, 95), 0.25, pred, fractions=(0.1,), known=known)
+    # the best 10 % of the 95 new children: indices 86-94 (9 of them)
+    assert q["top10_recall"] == 1.0 and q["known_share"] == 0.05 and q["known_in_top10"] == 0.5
+    assert q["top10_recall_new"] == pytest.approx(5 / 9)
+    assert q["top10_recall_at"] == {"0.1": 1.0}
+    assert q["random_screen_recall"] == pytest.approx(5 / 95)
+
+
 def test_quality_metrics():
     truth = np.arange(100, dtype=np.float32)
     q = evolve.quality(truth.copy(), truth, np.arange(90, 100), 0.25)
@@ -112,3 +143,21 @@ def test_race_gives_each_method_the_same_budget():
     assert evolve.best_at(curves["fast"], 2.0) == pytest.approx(0.8)
     assert evolve.best_at(curves["slow"], 2.0) == pytest.approx(0.6)
     assert evolve.best_at(curves["slow"], 0.5) == float("-inf")
+
+
+def test_plain_and_screened_simulate_only_new_children():
+    ev = _FakeEvaluator()
+    scr = evolve.ScreenedEvolution(ev, _FakeSurrogate(), seed=0, children=256, batch=64, screen=0.25)
+    scr.warmup(2 * 256, batch=256, epochs=1.0, random_batches=1)
+    n0 = len(ev.calls)
+    before = set(scr.memo.d)
+    g = scr.generation(truth=True)
+    new = 256 - g["known"]
+    assert g["known"] > 0 and g["simulated"] == round(0.25 * new) + round(0.05 * new)
+    # every simulated genome was new, and the truth pass simulated only new children
+    assert not any(row.tobytes() in before for c in ev.calls[n0:] for row in c)
+    assert len(ev.calls[n0]) == g["simulated"] and len(ev.calls[n0 + 1]) == new
+    plain = evolve.PlainEvolution(ev, seed=1, children=256, pool=scr.pool, memo=scr.memo)
+    k = len(ev.calls)
+    p = plain.generation()
+    assert p["simulated"] == len(ev.calls[k]) == 256 - p["known"] and p["known"] > 0
