@@ -120,7 +120,9 @@ struct mb_context {
     // packing result
     mb::KernelShape shape{512, 8, 2};
     uint32_t n_bins = 0;
-    uint32_t max_bin_mass = 0, max_bin_springs = 0;  // most masses / springs in one bin
+    uint32_t max_bin_mass = 0;  // most (own) masses in one bin
+    uint32_t rr_smem = 0;       // shared memory of the register-row kernel over every bin
+    uint32_t max_degree = 0;    // most springs at one mass when uploaded
     uint32_t smem_optin = 0;    // the device's shared memory per CTA (opt-in)
     uint32_t grid = 0;  // CTAs per step launch (0 = one per bin)
     uint32_t chunk = 1000;
@@ -325,10 +327,13 @@ mb_status upload_packed(mb_context* ctx, const mb::Packed& out, bool* rows_faile
     ctx->shape = out.shape;
     ctx->n_bins = out.n_bins;
     ctx->grid = out.grid;
-    ctx->max_bin_mass = ctx->max_bin_springs = 0;
+    // the register-row kernel's layout: the usual one without the rows, 8
+    // bytes of alignment, 8 bytes per spring (mb::row_reg_supported)
+    ctx->max_bin_mass = ctx->rr_smem = 0;
+    ctx->max_degree = out.max_degree;
     for (const mb::BinDesc& d : out.bins) {
         ctx->max_bin_mass = std::max(ctx->max_bin_mass, d.n_mass);
-        ctx->max_bin_springs = std::max(ctx->max_bin_springs, d.n_spring);
+        ctx->rr_smem = std::max(ctx->rr_smem, mb::bin_smem_bytes(d.n_mass, d.n_spring, 0) + 8u + 8u * d.n_spring);
     }
     if (!ctx->smem_optin) ctx->smem_optin = mb::max_step_smem(ctx->device);
     ctx->smem_bytes = out.max_smem;
@@ -1229,17 +1234,20 @@ mb_status mb_set_state(mb_context* ctx, const float* pos, const float* vel) {
 // Internal helpers: C++ linkage, internal to this file.
 namespace mb_detail {
 
-// Shared memory of the register-row step kernel (every bin's usual need plus
-// 8 bytes per spring), or 0 when it does not apply: split or streamed bins,
-// a bin of more than one mass per thread, face drag, or too little shared
-// memory.
+// Shared memory of the register-row step kernel, or 0 when it does not
+// apply: streamed or split bins, a bin of more than one mass per thread, a
+// mass with more springs than the registers hold rows for (at upload: the
+// kernel stays correct when development adds springs, reading longer rows
+// from global memory), face drag, a shape without the variant, or too little
+// shared memory.  Device development of resident bins keeps every bin's
+// spring count, and the device voxel builder only removes springs, so the
+// planned bins bound the need.
 uint32_t row_reg_smem(const mb_context* c) {
     const bool faces = face_drag_on(c) && c->faces_packed;
     if (c->streamed || c->cluster || faces || !mb::row_reg_supported(c->shape) ||
-        c->max_bin_mass > c->shape.threads)
+        c->max_bin_mass > c->shape.threads || c->max_degree > mb::row_reg_width())
         return 0;
-    const uint64_t need = (uint64_t)c->smem_bytes + 8ull * c->max_bin_springs + 8ull;
-    return need <= c->smem_optin ? (uint32_t)need : 0u;
+    return c->rr_smem <= c->smem_optin ? c->rr_smem : 0u;
 }
 
 mb::StepParams make_params(mb_context* c, float t0, uint32_t steps, bool track) {

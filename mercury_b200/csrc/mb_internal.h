@@ -186,10 +186,14 @@ uint32_t max_step_smem(int device);
 
 // Whether a kernel shape is compiled in.
 bool shape_supported(const KernelShape& shape);
-// Whether the shape has a register-row twin (one mass per thread, rows of
-// incident springs in registers), which launch_step uses when
-// StepParams::one_mass_per_thread is set.
+// Whether the shape of resident bins has a register-row twin (one mass per
+// thread, rows of incident springs in registers), which launch_step uses
+// when StepParams::one_mass_per_thread is set.  Its shared memory per bin:
+// the usual layout without the rows, 8 bytes of alignment, then 8 bytes per
+// spring.  Rows longer than row_reg_width() entries are read from global
+// memory, so the host uses it only when no mass has more incident springs.
 bool row_reg_supported(const KernelShape& shape);
+uint32_t row_reg_width();
 
 // Centre of mass of the non-air masses of each robot: one warp per robot.
 cudaError_t launch_com(const float4* pos, const uint8_t* mass_mat,

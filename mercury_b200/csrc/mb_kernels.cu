@@ -155,11 +155,12 @@ __device__ __forceinline__ float4 face_force(const float4 x0, const float4 x1, c
 // registers (two 16-bit entries per register, loaded once per bin), so that
 // the gather's correction loads no longer wait on a row-entry load and
 // issue RG at a time; a slice wider than RW reads its row from global
-// memory.  To make room, the springs leave the registers for {packed word,
-// mean length} pairs in shared memory after the rows' region (launched with
-// 8 bytes per spring more than the bin's usual shared memory).  One mass per
-// thread (MPT = 1), no face drag, no split bins.  Same operations in the same
-// order: same bits.
+// memory.  The rows are not staged in shared memory; to make room, the
+// springs leave the registers for {packed word, mean length} pairs in
+// shared memory where the rows would start (8 bytes per spring in place of
+// 2 per row entry).  One mass per thread (MPT = 1), no face drag.  Same
+// operations in the same order: same bits.  Resident bins only: on the
+// parts of split robots it measured slower.
 template <int T, int SPT, int MPT, int MODE, bool TRACK, bool SPLIT, int RW = 0>
 __global__ void __launch_bounds__(T, 1024 / T) step_kernel(const StepParams p) {
     constexpr bool XPBD = MODE == kModeXpbd;
@@ -199,10 +200,10 @@ __global__ void __launch_bounds__(T, 1024 / T) step_kernel(const StepParams p) {
         uint16_t* sfinc = reinterpret_cast<uint16_t*>(sfrow + bd.n_mass);
 
         const uint32_t n_mat = *p.n_mat;
-        // register rows: the springs leave the registers to make room, into
-        // {packed word, mean length} pairs after the rows' region (8 bytes per
-        // spring beyond the bin's usual shared memory)
-        uint2* ssl = reinterpret_cast<uint2*>((reinterpret_cast<uintptr_t>(sinc + bd.n_inc) + 7u) & ~uintptr_t(7));
+        // register rows: the rows are not staged in shared memory; the springs
+        // leave the registers to make room, into {packed word, mean length}
+        // pairs where the rows would start (8-byte aligned)
+        uint2* ssl = reinterpret_cast<uint2*>((reinterpret_cast<uintptr_t>(sinc) + 7u) & ~uintptr_t(7));
         if (RW > 0) {
             // the host sizes the launch for every bin; a bin that would still
             // not fit is skipped and flagged (bit 1) rather than overrun
@@ -748,21 +749,21 @@ const ShapeEntry kShapes[] = {
 };
 // register-row twins of the 1,024-thread shapes (one mass per thread; no
 // face drag): launch_step uses one when every bin has at most 1,024 masses
-#define MB_RR(T, S, RW)                                                                          \
+#define MB_RR(T, S, RW, SPLIT)                                                                   \
     {                                                                                            \
         T, S, 1, {                                                                               \
-            {step_kernel<T, S, 1, kModeXpbd, false, false, RW>,                                  \
-             step_kernel<T, S, 1, kModeXpbd, true, false, RW>},                                  \
-                {step_kernel<T, S, 1, kModeForceLand, false, false, RW>,                         \
-                 step_kernel<T, S, 1, kModeForceLand, true, false, RW>},                         \
-                {step_kernel<T, S, 1, kModeForceWater, false, false, RW>,                        \
-                 step_kernel<T, S, 1, kModeForceWater, true, false, RW>},                        \
+            {step_kernel<T, S, 1, kModeXpbd, false, SPLIT, RW>,                                  \
+             step_kernel<T, S, 1, kModeXpbd, true, SPLIT, RW>},                                  \
+                {step_kernel<T, S, 1, kModeForceLand, false, SPLIT, RW>,                         \
+                 step_kernel<T, S, 1, kModeForceLand, true, SPLIT, RW>},                         \
+                {step_kernel<T, S, 1, kModeForceWater, false, SPLIT, RW>,                        \
+                 step_kernel<T, S, 1, kModeForceWater, true, SPLIT, RW>},                        \
                 {nullptr, nullptr},                                                              \
         }                                                                                        \
     }
 constexpr int kRowRegWidth = 26;  // register rows: entries per mass (lattice robots: at most 26)
-const ShapeEntry kRowRegShapes[] = {MB_RR(1024, 8, kRowRegWidth), MB_RR(1024, 10, kRowRegWidth),
-                                    MB_RR(1024, 12, kRowRegWidth)};
+const ShapeEntry kRowRegShapes[] = {MB_RR(1024, 8, kRowRegWidth, false), MB_RR(1024, 10, kRowRegWidth, false),
+                                    MB_RR(1024, 12, kRowRegWidth, false)};
 #undef MB_RR
 // the parts of split robots (thread-block clusters)
 const ShapeEntry kSplitShapes[] = {
@@ -820,6 +821,7 @@ const ShapeEntry* find_split(const KernelShape& s) {
     return nullptr;
 }
 
+
 }  // namespace
 
 uint32_t bin_smem_bytes(uint32_t n_mass, uint32_t n_spring, uint32_t n_inc) {
@@ -840,6 +842,8 @@ bool row_reg_supported(const KernelShape& shape) {
         if (e.spt == shape.spt) return true;
     return false;
 }
+
+uint32_t row_reg_width() { return kRowRegWidth; }
 
 bool split_supported(const KernelShape& shape) { return find_split(shape) != nullptr; }
 

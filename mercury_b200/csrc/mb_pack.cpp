@@ -134,6 +134,7 @@ struct RobotPack {
     uint64_t inc_estimate = 0;
     uint32_t n_face = 0;     // faces with three distinct corners
     uint32_t face_smem = 0;  // shared memory of the face drag, bytes (upper bound)
+    uint32_t max_degree = 0;  // most non-air springs at one mass
     uint64_t mats[4] = {0, 0, 0, 0};  // composite ids of its non-air springs (bit set)
     std::string error;
     mb_status status = MB_OK;
@@ -272,14 +273,16 @@ void preprocess(const mb_batch_desc* b, uint32_t r, RobotPack& p) {
         uint32_t w = 0;
         for (int64_t k = i; k < std::min<int64_t>(i + 32, cm); ++k) w = std::max(w, deg[k]);
         est += 32ull * w;
+        p.max_degree = std::max(p.max_degree, w);
     }
     p.inc_estimate = est + 64;  // slack for slices straddling robots
 }
 
 // LPT assignment of robots to `nb` bins by cost, within the shape's and the
 // shared memory's capacity.
-// spring_extra: shared-memory bytes a bin needs per spring beyond
-// bin_smem_bytes (plus 8 bytes of alignment when nonzero).
+// spring_extra (the register-row kernel, when nonzero): the bin must also
+// fit that kernel's layout -- the usual one without the rows, 8 bytes of
+// alignment, spring_extra bytes per spring.
 bool plan_bins(const std::vector<RobotPack>& packs, uint32_t nb, const KernelShape& sh,
                uint32_t smem_cap, std::vector<std::vector<uint32_t>>& plan, uint32_t spring_extra = 0) {
     const uint32_t n = (uint32_t)packs.size();
@@ -296,10 +299,9 @@ bool plan_bins(const std::vector<RobotPack>& packs, uint32_t nb, const KernelSha
         int best = -1;
         for (uint32_t b = 0; b < nb; ++b) {
             if (bm[b] + p.n_mass > cap_m || bs[b] + p.springs.size() > cap_s) continue;
-            if (bin_smem_bytes((uint32_t)(bm[b] + p.n_mass), (uint32_t)(bs[b] + p.springs.size()),
-                               (uint32_t)(bi[b] + p.inc_estimate)) + bx[b] + p.face_smem +
-                    (spring_extra ? spring_extra * (bs[b] + p.springs.size()) + 8u : 0u) >
-                smem_cap)
+            const uint32_t m1 = (uint32_t)(bm[b] + p.n_mass), s1 = (uint32_t)(bs[b] + p.springs.size());
+            if (bin_smem_bytes(m1, s1, (uint32_t)(bi[b] + p.inc_estimate)) + bx[b] + p.face_smem > smem_cap ||
+                (spring_extra && bin_smem_bytes(m1, s1, 0) + 8u + spring_extra * s1 > smem_cap))
                 continue;
             if (best < 0 || load[b] < load[best]) best = (int)b;
         }
@@ -357,10 +359,9 @@ bool plan_bins_grouped(const std::vector<RobotPack>& packs, uint32_t nb, uint32_
             int best = -1;
             for (uint32_t j = 0; j < per; ++j) {
                 if (bm[j] + p.n_mass > cap_m || bs[j] + p.springs.size() > cap_s) continue;
-                if (bin_smem_bytes((uint32_t)(bm[j] + p.n_mass), (uint32_t)(bs[j] + p.springs.size()),
-                                   (uint32_t)(bi[j] + p.inc_estimate)) + bx[j] + p.face_smem +
-                        (spring_extra ? spring_extra * (bs[j] + p.springs.size()) + 8u : 0u) >
-                    smem_cap)
+                const uint32_t m1 = (uint32_t)(bm[j] + p.n_mass), s1 = (uint32_t)(bs[j] + p.springs.size());
+                if (bin_smem_bytes(m1, s1, (uint32_t)(bi[j] + p.inc_estimate)) + bx[j] + p.face_smem > smem_cap ||
+                    (spring_extra && bin_smem_bytes(m1, s1, 0) + 8u + spring_extra * s1 > smem_cap))
                     continue;
                 if (best < 0 || load[j] < load[best]) best = (int)j;
             }
@@ -1256,11 +1257,13 @@ mb_status pack_population(const mb_batch_desc* b, const PackOptions& o, Packed& 
         }
     uint64_t tot_s = 0, tot_m = 0;
     uint32_t max_s = 0, max_m = 0;
+    out.max_degree = 0;
     for (const auto& p : packs) {
         tot_s += p.springs.size();
         tot_m += p.n_mass;
         max_s = std::max<uint32_t>(max_s, (uint32_t)p.springs.size());
         max_m = std::max(max_m, p.n_mass);
+        out.max_degree = std::max(out.max_degree, p.max_degree);
     }
     out.masses = tot_m;
     out.active_springs = tot_s;
@@ -1306,7 +1309,8 @@ mb_status pack_population(const mb_batch_desc* b, const PackOptions& o, Packed& 
     // bytes of shared memory per spring -- then, if that fails, as usual.
     std::vector<std::pair<KernelShape, bool>> attempts;
     for (const auto& sh : shapes) {
-        if (!o.override.threads && out.n_faces == 0 && max_m <= sh.threads && row_reg_supported(sh))
+        if (!o.override.threads && out.n_faces == 0 && max_m <= sh.threads && row_reg_supported(sh) &&
+            out.max_degree <= row_reg_width())
             attempts.push_back({sh, true});
         attempts.push_back({sh, false});
     }
@@ -1354,11 +1358,10 @@ mb_status pack_population(const mb_batch_desc* b, const PackOptions& o, Packed& 
             if (planned) {
                 build_all(b, packs, plan, slot_of, false, threads, out, o.rows_on_device);
                 uint64_t need = out.max_smem;
-                if (one_mass) {
-                    uint32_t most = 0;
-                    for (const BinDesc& d : out.bins) most = std::max(most, d.n_spring);
-                    need += 8ull * most + 8ull;
-                }
+                if (one_mass)
+                    for (const BinDesc& d : out.bins)
+                        need = std::max<uint64_t>(need, bin_smem_bytes(d.n_mass, d.n_spring, 0) + 8ull +
+                                                            8ull * d.n_spring);
                 if (need <= o.smem_cap) {
                     ok = true;
                     break;

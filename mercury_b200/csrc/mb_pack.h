@@ -86,6 +86,7 @@ struct Packed {
     raw_vector<uint32_t> faces, face_row;
     raw_vector<uint16_t> face_inc;
     uint64_t n_faces = 0;  // faces of the population with three distinct corners
+    uint32_t max_degree = 0;  // most non-air springs at one mass
     raw_vector<float> lbar;
     std::vector<uint8_t> mat_ids;
     // statistics

@@ -14,6 +14,7 @@ import mercury_b200 as mb
 from mercury_b200 import robots
 from mercury_b200 import simulator as S
 from oracle import core
+from test_gpu_devo import OracleRun, check_same
 
 pytestmark = pytest.mark.gpu
 
@@ -66,19 +67,36 @@ def test_register_rows_bit_exact(mode, track, spt):
         assert np.array_equal(bits(stress), bits(s))
 
 
-def test_rows_wider_than_registers_bit_exact():
-    """Point clouds with 25 nearest-neighbour springs per mass: most rows are
-    longer than the 26 entries the registers hold and are read from global
-    memory instead."""
-    rng = np.random.default_rng(11)
-    els = [robots.nn_robot(rng, int(rng.integers(150, 301))) for _ in range(6)]
-    b = mb.pack(els)
-    variant, (pos, vel, stress) = run(b, 0, 200, True, 1e-3,
-                                      dict(threads=1024, springs_per_thread=12, masses_per_thread=2, bins=6, chunk=64))
-    assert variant["register_rows"] == 1
-    p, v, s = oracle(b, 0, 200, True, 1e-3)
-    assert np.array_equal(bits(pos), bits(p)) and np.array_equal(bits(vel), bits(v))
-    assert np.array_equal(bits(stress), bits(s))
+def test_rows_grown_past_the_registers_by_development_bit_exact():
+    """Development rewires springs to random pairs, so after it a mass can
+    have more incident springs than the registers hold rows for: those rows
+    are read from global memory, with the same bits."""
+    b = robots.population_batch("small", 8, seed_base=40)
+    dt = 1e-3
+    sim = mb.Simulator(0)
+    sim.setTimeStep(dt)
+    sim.set_launch_config(threads=1024, springs_per_thread=8, masses_per_thread=2, bins=8, chunk=64)
+    sim.set_batch(b)
+    assert sim.step_variant()["register_rows"] == 1
+    orc = OracleRun(b, mb.material_table(), dt)
+    widest = 0
+    for cycle in range(3):
+        sim.run_steps(100, True)
+        orc.steps(100)
+        assert sim.devo(120, seed=cycle) == orc.devo(120, cycle)
+        check_same(sim, orc)
+        deg = np.zeros(b.n_masses, np.int64)
+        act = orc.b.spring_material != 0
+        so = np.repeat(b.mass_offsets[:-1], np.diff(b.spring_offsets))
+        np.add.at(deg, (orc.b.pairs[:, 0] + so)[act], 1)
+        np.add.at(deg, (orc.b.pairs[:, 1] + so)[act], 1)
+        widest = max(widest, int(deg.max()))
+    assert sim.devo_profile()["host_repacks"] == 0  # re-packed on the device, bins kept
+    assert sim.step_variant()["register_rows"] == 1
+    assert widest > 26  # some rows no longer fit the registers
+    sim.run_steps(150, True)
+    orc.steps(150)
+    check_same(sim, orc)
 
 
 def test_two_masses_per_thread_keeps_shared_memory_rows():
