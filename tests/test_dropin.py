@@ -88,3 +88,22 @@ def test_dropin_matches_oracle(tmp_path):
         assert np.array_equal(np.array([d[1] for d in devo], np.uint8), mat[ss])
         assert np.array_equal(np.array([d[2] for d in devo], np.float32).view(np.uint32),
                               lbar[ss].view(np.uint32))
+
+
+@pytest.mark.gpu
+def test_screened_evaluation_in_the_reference_evaluator_loop():
+    """ScreenedEvaluator<VoxelRobot> (mercury_b200/compat/ScreenedEvaluator.h)
+    in place of Evaluator<VoxelRobot>::BatchEvaluate, on children of the
+    reference's own VoxelRobot::Crossover: warm-up evaluations equal the full
+    ones, then only the screened children are evaluated (bit for bit what the
+    full evaluation gives them), the rest carry fitness 0, a child outside the
+    surrogate's classes is always evaluated, and the screen finds the best
+    children better than chance (tests/cpp/test_screened.cpp)."""
+    exe = os.path.join(ROOT, "tests", "cpp", "_bin", "test_screened")
+    if not os.path.exists(exe):
+        pytest.skip("tests/cpp/_bin/test_screened not built")
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    kv = dict(x.split("=") for x in r.stdout.strip().splitlines()[-1].split())
+    assert kv["ok"] == "1" and int(kv["unrepresentable"]) == 1
+    assert float(kv["recall"]) > float(kv["chance"]) + 0.1, r.stdout
