@@ -373,32 +373,43 @@ __global__ void __launch_bounds__(kTcThreads) gemm_tc_kernel(const GemmArgs g, u
 // ---------------------------------------------------------------------------
 // Planar implicit-GEMM convolution on tcgen05 (the forward 3x3x3 layers).
 //
-// Activations are stored per genome as planes of 8 channels over the 8x8x8
-// grid padded with a zero halo: element (genome b, plane c/8, padded voxel
-// p = (x+1) + 8(y+1) + 64(z+1), channel c%8) at ((b P + c/8) 512 + p) 8 +
-// c%8, so one padded voxel of one plane is a 16-byte row and consecutive
-// rows are 16 bytes apart -- exactly the K-major no-swizzle UMMA layout
-// with SBO = 128 bytes.  The input of output row p at offset o is row
-// p + delta(o), delta = dx + 8 dy + 64 dz: a shift of the descriptor's start
-// address.  A CTA loads, for an output tile of 128 padded rows, its 288-row
-// input window (tile - 80 .. tile + 208, zero outside the genome) once and
-// issues all the tile's MMAs from it: 27 offsets x 2 channel halves (K = 16
-// each, LBO = the plane stride) for 32 input channels; for 8 input channels
-// two offsets share one K = 16 MMA (LBO = the row distance between them).
-// The weights stay in shared memory for the CTA's whole run (persistent
-// CTAs).  Halo rows are computed and discarded: the epilogue writes zeros
-// there, so the next layer's halo is zero.
-constexpr int kCvRows = 288, kCvLead = 80, kCvTile = 128;
+// Activations are stored as planes of 8 channels over the genomes' 7x7x7
+// grids laid end to end: the 6x6x6 cells of genome b at padded row
+// p = 343 b + x + 7y + 49z, and the rows with x, y or z = 6 zero.  That zero
+// layer is the halo of both sides: x = -1 of a row is x = 6 of the row
+// before, y = -1 of a plane is y = 6 of the plane before, z = -1 of a genome
+// is z = 6 of the genome before.  Element (plane c/8, row p, channel c%8)
+// at (c/8 * rows + p) 8 + c%8 (rows = the plane stride, a whole number of
+// tiles), so one row of one plane is 16 bytes and consecutive rows are 16
+// bytes apart -- exactly the K-major no-swizzle UMMA layout with SBO = 128
+// bytes.  The input of output row p at offset o is row p + delta(o),
+// delta = dx + 7 dy + 49 dz: a shift of the descriptor's start address.  A
+// CTA loads, for an output tile of 128 rows, its 248-row input window
+// (tile - 57 .. tile + 191, zero outside the genomes) once and issues all
+// the tile's MMAs from it: 27 offsets x 2 channel halves (K = 16 each, LBO =
+// the plane stride) for 32 input channels; for 8 input channels two offsets
+// share one K = 16 MMA (LBO = the row distance between them).  The weights
+// stay in shared memory for the CTA's whole run (persistent CTAs).  Halo
+// rows are computed and discarded: the epilogue writes zeros there, so the
+// next layer's halo is zero.  216 of every 343 rows are cells (an 8x8x8 grid
+// per genome would have 216 of 512).
+constexpr int kCvRows = 248, kCvLead = 57, kCvTile = 128, kCvSide = 7, kCvGenome = 343;
 
-__host__ __device__ constexpr int cv_delta(int o) { return (o % 3 - 1) + 8 * ((o / 3) % 3 - 1) + 64 * (o / 9 - 1); }
+__host__ __device__ constexpr int cv_delta(int o) {
+    return (o % 3 - 1) + kCvSide * ((o / 3) % 3 - 1) + kCvSide * kCvSide * (o / 9 - 1);
+}
+// rows of the planar layout of n genomes: whole tiles
+__host__ __device__ constexpr uint32_t cv_rows(uint32_t n) {
+    return (n * (uint32_t)kCvGenome + kCvTile - 1) / kCvTile * kCvTile;
+}
 
 struct ConvTcArgs {
-    const bf16* in;        // planar input [n][p_in][512][8]
+    const bf16* in;        // planar input [p_in][cv_rows(n)][8]
     int p_in;              // input planes: 1 (8 channels) or 4 (32)
     const bf16* w;         // [32][27 * 8 * p_in], k = offset * 8 p_in + channel
     const float* bias;     // [32]
     int n;                 // genomes
-    bf16* out_planar;      // [n][4][512][8] or null
+    bf16* out_planar;      // [4][cv_rows(n)][8] or null
     bf16* out_compact;     // [n][216][32] (voxel x + 6y + 36z) or null
     uint32_t* err;
     // input gradient of a layer (the backward): no bias and no ReLU; the
@@ -420,7 +431,7 @@ __global__ void __launch_bounds__(128) conv_tc_kernel(const ConvTcArgs g) {
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     uint8_t* sw = cv_smem;
     uint8_t* sa[2] = {cv_smem + kWBytes, cv_smem + kWBytes + kABytes};
-    const int tiles = g.n * (512 / kCvTile);
+    const int rows = (int)cv_rows((uint32_t)g.n), tiles = rows / kCvTile, real_rows = g.n * kCvGenome;
     if (tid == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&bars[0])));
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&bars[1])));
@@ -437,18 +448,18 @@ __global__ void __launch_bounds__(128) conv_tc_kernel(const ConvTcArgs g) {
         cp_async16(sw + (c * 4 + row / 8) * 128 + (row % 8) * 16, ok ? g.w + (size_t)row * K + c * 8 : g.w, ok);
     }
     auto load_a = [&](int t, uint8_t* dst) {
-        const int b = t >> 2, r0 = (t & 3) * kCvTile;
+        const int r0 = t * kCvTile;
         for (int i = tid; i < P * kCvRows; i += 128) {
             const int plane = i / kCvRows, rr = i - plane * kCvRows, row = r0 - kCvLead + rr;
-            const bool ok = row >= 0 && row < 512;
-            cp_async16(dst + plane * kPlane + rr * 16, ok ? g.in + (((size_t)b * P + plane) * 512 + row) * 8 : g.in, ok);
+            const bool ok = row >= 0 && row < real_rows;
+            cp_async16(dst + plane * kPlane + rr * 16, ok ? g.in + ((size_t)plane * rows + row) * 8 : g.in, ok);
         }
     };
-    // epilogue of tile t from accumulator `acc`: row p of genome b from TMEM lane 32*warp + lane
+    // epilogue of tile t from accumulator `acc`: row p from TMEM lane 32*warp + lane
     auto epilogue = [&](int t, uint32_t acc) {
-        const int b = t >> 2, p = (t & 3) * kCvTile + warp * 32 + lane;
-        const int x = p % 8 - 1, y = (p / 8) % 8 - 1, z = p / 64 - 1;
-        const bool real = x >= 0 && x < 6 && y >= 0 && y < 6 && z >= 0 && z < 6;
+        const int p = t * kCvTile + warp * 32 + lane, b = p / kCvGenome, loc = p - b * kCvGenome;
+        const int x = loc % kCvSide, y = (loc / kCvSide) % kCvSide, z = loc / (kCvSide * kCvSide);
+        const bool real = b < g.n && x < 6 && y < 6 && z < 6;
         const int v = x + 6 * y + 36 * z;
 #pragma unroll
         for (int c0 = 0; c0 < 32; c0 += 8) {
@@ -472,7 +483,7 @@ __global__ void __launch_bounds__(128) conv_tc_kernel(const ConvTcArgs g) {
                     h[j] = __float2bfloat16_rn(real ? fmaxf(__uint_as_float(r[j]) + g.bias[c0 + j], 0.0f) : 0.0f);
             }
             const uint4 pk = *reinterpret_cast<const uint4*>(h);
-            if (g.out_planar) *reinterpret_cast<uint4*>(g.out_planar + (((size_t)b * 4 + c0 / 8) * 512 + p) * 8) = pk;
+            if (g.out_planar) *reinterpret_cast<uint4*>(g.out_planar + ((size_t)(c0 / 8) * rows + p) * 8) = pk;
             if (g.out_compact && real)
                 *reinterpret_cast<uint4*>(g.out_compact + ((size_t)b * 216 + v) * 32 + c0) = pk;
         }
@@ -569,14 +580,15 @@ __global__ void __launch_bounds__(128) conv_tc_kernel(const ConvTcArgs g) {
     }
 }
 
-// Compact [n][216][32] (voxel x + 6y + 36z) to padded planar [n][4][512][8]
-// with a zero halo: the layout conv_tc_kernel reads.
+// Compact [n][216][32] (voxel x + 6y + 36z) to the planar layout
+// [4][cv_rows(n)][8] with zero halo rows: the layout conv_tc_kernel reads.
 __global__ void planar_from_compact_kernel(const bf16* __restrict__ c, uint32_t n, bf16* __restrict__ x) {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n * 4 * 512; i += gridDim.x * blockDim.x) {
-        const uint32_t p = i % 512, plane = (i / 512) % 4, b = i / 2048;
-        const int xx = (int)(p % 8) - 1, yy = (int)((p / 8) % 8) - 1, zz = (int)(p / 64) - 1;
+    const uint32_t rows = cv_rows(n);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < 4 * rows; i += gridDim.x * blockDim.x) {
+        const uint32_t plane = i / rows, p = i % rows, b = p / kCvGenome, loc = p % kCvGenome;
+        const uint32_t xx = loc % kCvSide, yy = (loc / kCvSide) % kCvSide, zz = loc / (kCvSide * kCvSide);
         uint4 v = make_uint4(0, 0, 0, 0);
-        if (xx >= 0 && xx < 6 && yy >= 0 && yy < 6 && zz >= 0 && zz < 6)
+        if (b < n && xx < 6 && yy < 6 && zz < 6)
             v = *reinterpret_cast<const uint4*>(c + ((size_t)b * 216 + xx + 6 * yy + 36 * zz) * 32 + plane * 8);
         *reinterpret_cast<uint4*>(x + (size_t)i * 8) = v;
     }
@@ -592,13 +604,14 @@ __global__ void conv_weight_flip_kernel(const bf16* __restrict__ w, bf16* __rest
     }
 }
 
-// One-hot classes on the padded planar grid (8 channels, zero halo).
+// One-hot classes in the planar layout (8 channels, zero halo rows).
 __global__ void onehot_planar_kernel(const uint8_t* __restrict__ cls, uint32_t n, bf16* __restrict__ x) {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n * 512; i += gridDim.x * blockDim.x) {
-        const uint32_t b = i / 512, p = i % 512;
-        const int xx = (int)(p % 8) - 1, yy = (int)((p / 8) % 8) - 1, zz = (int)(p / 64) - 1;
+    const uint32_t rows = cv_rows(n);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += gridDim.x * blockDim.x) {
+        const uint32_t b = i / kCvGenome, loc = i % kCvGenome;
+        const uint32_t xx = loc % kCvSide, yy = (loc / kCvSide) % kCvSide, zz = loc / (kCvSide * kCvSide);
         uint32_t c = 0xFFu;
-        if (xx >= 0 && xx < 6 && yy >= 0 && yy < 6 && zz >= 0 && zz < 6) c = cls[b * 216 + xx + 6 * yy + 36 * zz];
+        if (b < n && xx < 6 && yy < 6 && zz < 6) c = cls[b * 216 + xx + 6 * yy + 36 * zz];
         alignas(16) bf16 h[8];
 #pragma unroll
         for (uint32_t k = 0; k < 8; ++k) h[k] = __float2bfloat16_rn(c == k && c < 5 ? 1.0f : 0.0f);
@@ -774,7 +787,7 @@ cudaError_t conv_tc(const ConvTcArgs& g, int num_sms, cudaStream_t s) {
         if (e != cudaSuccess) return e;
         prepared = true;
     }
-    const int tiles = g.n * 4;
+    const int tiles = (int)(cv_rows((uint32_t)g.n) / kCvTile);
     if (tiles == 0) return cudaSuccess;
     const int grid = std::min(tiles, (P == 1 ? 4 : 2) * num_sms);
     conv_tc_kernel<P><<<grid, 128, smem, s>>>(g);
@@ -941,7 +954,7 @@ cudaError_t forward(mb_surrogate* s, uint32_t n) {
         return gemm<kDenseK, kDenseK>(a, 1, st);
     };
     if (s->tcgen05) {
-        onehot_planar_kernel<<<std::min<uint32_t>((n * 512 + 255) / 256, 4096), 256, 0, st>>>(s->cls.p, n, s->x0p.p);
+        onehot_planar_kernel<<<std::min<uint32_t>((cv_rows(n) + 255) / 256, 4096), 256, 0, st>>>(s->cls.p, n, s->x0p.p);
         const ConvTcArgs c1{s->x0p.p, 1, PB(s, kW1), P(s, kB1), (int)n, s->a1p.p, s->a1.p, s->tc_err.p};
         const ConvTcArgs c2{s->a1p.p, 4, PB(s, kW2), P(s, kB2), (int)n, s->a2p.p, s->a2.p, s->tc_err.p};
         const ConvTcArgs c3{s->a2p.p, 4, PB(s, kW3), P(s, kB3), (int)n, nullptr, s->a3.p, s->tc_err.p};
@@ -1026,7 +1039,7 @@ cudaError_t backward(mb_surrogate* s, uint32_t n) {
     if (s->tcgen05) {
         // input gradient as the forward convolution of the gradient with the
         // mirrored, transposed kernel, on tcgen05; masked by a2 > 0
-        planar_from_compact_kernel<<<std::min<uint32_t>((n * 2048 + 255) / 256, 4096), 256, 0, st>>>(s->dz3.p, n,
+        planar_from_compact_kernel<<<std::min<uint32_t>((4 * cv_rows(n) + 255) / 256, 4096), 256, 0, st>>>(s->dz3.p, n,
                                                                                                       s->dz3p.p);
         conv_weight_flip_kernel<<<108, 256, 0, st>>>(PB(s, kW3), s->wf3.p);
         ConvTcArgs c{s->dz3p.p, 4, s->wf3.p, nullptr, (int)n, s->dz2p.p, s->dz2c.p, s->tc_err.p};
@@ -1108,9 +1121,9 @@ mb_status mb_surrogate_create(int device, uint32_t max_batch, uint64_t seed, mb_
           ok(s->h2.alloc((size_t)max_batch * 128)) && ok(s->dz2h.alloc((size_t)max_batch * 128)) &&
           ok(s->dz1h.alloc((size_t)max_batch * 128)) && ok(s->dz3.alloc(R * 32)) && ok(s->dz2c.alloc(R * 32)) &&
           ok(s->dz1c.alloc(R * 32)) && ok(s->cls.alloc(R)) && ok(s->tc_err.alloc(1)) &&
-          ok(s->x0p.alloc((size_t)max_batch * 512 * 8)) && ok(s->a1p.alloc((size_t)max_batch * 4 * 512 * 8)) &&
-          ok(s->a2p.alloc((size_t)max_batch * 4 * 512 * 8)) && ok(s->dz3p.alloc((size_t)max_batch * 4 * 512 * 8)) &&
-          ok(s->dz2p.alloc((size_t)max_batch * 4 * 512 * 8)) && ok(s->wf2.alloc(32 * 864)) &&
+          ok(s->x0p.alloc((size_t)cv_rows(max_batch) * 8)) && ok(s->a1p.alloc((size_t)cv_rows(max_batch) * 4 * 8)) &&
+          ok(s->a2p.alloc((size_t)cv_rows(max_batch) * 4 * 8)) && ok(s->dz3p.alloc((size_t)cv_rows(max_batch) * 4 * 8)) &&
+          ok(s->dz2p.alloc((size_t)cv_rows(max_batch) * 4 * 8)) && ok(s->wf2.alloc(32 * 864)) &&
           ok(s->wf3.alloc(32 * 864))))
         return MB_ERR_CUDA;
     if (cudaMemset(s->tc_err.p, 0, sizeof(uint32_t)) != cudaSuccess) return MB_ERR_CUDA;
