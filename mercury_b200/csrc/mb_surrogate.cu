@@ -548,11 +548,13 @@ __global__ void __launch_bounds__(128) conv_tc_kernel(const ConvTcArgs g) {
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
-            epilogue(prev, tmem + 32u * (uint32_t)(s ^ 1));
         }
+        // the next tile's input into the freed buffer, in flight during the
+        // previous tile's epilogue
         const int nt = t + gridDim.x;
         if (nt < tiles) load_a(nt, sa[s ^ 1]);
         cp_async_commit();
+        if (prev >= 0) epilogue(prev, tmem + 32u * (uint32_t)(s ^ 1));
         cp_async_wait_all();
         asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
         asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
