@@ -370,8 +370,8 @@ def _device_rate(sim, active, steps, track, dev):
 # the uneven population in the configurations the tuner picks (ncu,
 # dram__bytes_read.sum + dram__bytes_write.sum): the state and topology, read
 # once per launch.
-STEP_TRAFFIC = {("uneven", 1024, 8, 2, 296, 1000): 24.66e6 + 2.0e3,
-                ("uneven", 1024, 10, 2, 296, 1000): 24.67e6 + 0.0}
+STEP_TRAFFIC = {("uneven", 1024, 8, 2, 296, 1000): 24.664e6 + 0.0,
+                ("uneven", 1024, 10, 2, 296, 1000): 24.666e6 + 0.0}
 
 
 def _step_traffic(workload, cfg, active):
