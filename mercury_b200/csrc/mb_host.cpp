@@ -9,8 +9,9 @@
 // (LPT), and the bin count is a multiple of the SM count so that every SM
 // gets the same work.  Inside a bin:
 //   - masses keep robot order (robot r's masses, then robot r+1's ...);
-//   - non-air springs are sorted by (b - a, a) so that a warp's springs read
-//     consecutive positions (for a lattice: one direction, consecutive a);
+//   - non-air springs of each robot are sorted by (b - a, a) (for a lattice:
+//     one direction, consecutive a), then placed so that the 8 springs of a
+//     quarter-warp read distinct shared-memory bank groups at both ends;
 //   - every mass gets a row of incident springs sorted by (other end,
 //     spring index, a end before b end) -- the fixed summation order -- and
 //     rows are stored 32 masses per slice, column-major (SELL-32), so that a

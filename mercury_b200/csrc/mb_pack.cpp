@@ -10,8 +10,9 @@
 // and robots are balanced over the groups first (plan_bins_grouped): a
 // group's load is what sets its SM's time.  Inside a bin:
 //   - masses keep robot order (robot r's masses, then robot r+1's ...);
-//   - non-air springs are sorted by (b - a, a) so that a warp's springs read
-//     consecutive positions (for a lattice: one direction, consecutive a);
+//   - non-air springs of each robot are sorted by (b - a, a) (for a lattice:
+//     one direction, consecutive a), then placed so that the 8 springs of a
+//     quarter-warp read distinct bank groups at both ends (bank_order);
 //   - every mass gets a row of incident springs sorted by (other end,
 //     spring index, a end before b end) -- the fixed summation order -- and
 //     rows are stored 32 masses per slice, column-major (SELL-32), with
