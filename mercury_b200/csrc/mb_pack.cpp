@@ -573,30 +573,35 @@ std::vector<uint32_t> bank_order(const std::vector<uint32_t>& words) {
     const uint32_t n = (uint32_t)words.size();
     std::vector<uint32_t> order;
     order.reserve(n);
-    std::vector<uint8_t> taken(n, 0);
-    uint32_t head = 0;
+    // the window: the earliest unplaced springs, in order
+    uint32_t win[kWindow], len = 0, next = 0;
     while (order.size() < n) {
-        while (taken[head]) ++head;
-        uint32_t used_a = 0, used_b = 0, got = 0;
+        while (len < kWindow && next < n) win[len++] = next++;
         const uint32_t want = std::min<uint32_t>(8, n - (uint32_t)order.size());
-        uint32_t seen = 0;
-        for (uint32_t i = head; i < n && seen < kWindow && got < want; ++i) {
-            if (taken[i]) continue;
-            ++seen;
-            const uint32_t ba = 1u << (words[i] & 7u), bb = 1u << ((words[i] >> 12) & 7u);
+        uint32_t used_a = 0, used_b = 0, got = 0;
+        uint64_t picked = 0;  // bit k: win[k] placed in this group
+        for (uint32_t k = 0; k < len && got < want; ++k) {
+            const uint32_t w = words[win[k]];
+            const uint32_t ba = 1u << (w & 7u), bb = 1u << ((w >> 12) & 7u);
             if ((used_a & ba) || (used_b & bb)) continue;
             used_a |= ba;
             used_b |= bb;
-            taken[i] = 1;
-            order.push_back(i);
+            picked |= 1ull << k;
             ++got;
         }
-        for (uint32_t i = head; i < n && got < want; ++i)
-            if (!taken[i]) {
-                taken[i] = 1;
-                order.push_back(i);
+        for (uint32_t k = 0; k < len && got < want; ++k)
+            if (!((picked >> k) & 1ull)) {
+                picked |= 1ull << k;
                 ++got;
             }
+        // the group in window order (= spring order), then the window compacted
+        uint32_t keep = 0;
+        for (uint32_t k = 0; k < len; ++k)
+            if ((picked >> k) & 1ull)
+                order.push_back(win[k]);
+            else
+                win[keep++] = win[k];
+        len = keep;
     }
     return order;
 }
