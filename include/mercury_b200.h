@@ -198,8 +198,11 @@ MB_API mb_status mb_collect(mb_context* ctx, float* pos, float* vel, float* stre
  * SoftBody::updateCOM after Collect (SoftBody.cpp:112-121). */
 MB_API mb_status mb_centre_of_mass(mb_context* ctx, float* com);
 
-/* Per-robot status after the last run: bit 0 = a position became NaN/Inf.
- * Synchronous.  The reference asserts on NaN in Collect (Simulator.cu:550). */
+/* Per-robot status after the last run: bit 0 = a position became NaN/Inf;
+ * bit 1 = the robot's bin did not fit the shared memory the launch was
+ * sized for and was not stepped (a safeguard of the register-row kernel;
+ * the host sizes every launch so that it does not happen).  Synchronous.
+ * The reference asserts on NaN in Collect (Simulator.cu:550). */
 MB_API mb_status mb_robot_flags(mb_context* ctx, uint32_t* flags);
 
 /* Waits for all work on the context's stream. */

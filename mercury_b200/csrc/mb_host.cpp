@@ -1454,6 +1454,9 @@ mb_status mb_robot_flags(mb_context* ctx, uint32_t* flags) {
     cudaSetDevice(ctx->device);
     MB_CUDA(ctx, mb::launch_flags(ctx->pos.p, ctx->d_mass_off.p, ctx->n_robots,
                                   ctx->robot_flags.p, ctx->stream));
+    if (!ctx->streamed && !ctx->cluster)
+        MB_CUDA(ctx, mb::launch_bin_flags(ctx->bin_flags.p, ctx->robot_bin.p, ctx->n_robots, ctx->robot_flags.p,
+                                          ctx->stream));
     MB_CUDA(ctx, cudaMemcpyAsync(flags, ctx->robot_flags.p, sizeof(uint32_t) * ctx->n_robots,
                                  cudaMemcpyDeviceToHost, ctx->stream));
     MB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));

@@ -201,6 +201,9 @@ cudaError_t launch_com(const float4* pos, const uint8_t* mass_mat,
                        cudaStream_t s);
 
 // Per-robot flags: bit 0 = a position is NaN or Inf.  One warp per robot.
+// ORs bit 1 of each robot's first bin's step flags into out[robot].
+cudaError_t launch_bin_flags(const uint32_t* bin_flags, const uint32_t* robot_bin, uint32_t n_robots,
+                             uint32_t* out, cudaStream_t s);
 cudaError_t launch_flags(const float4* pos, const int64_t* mass_off, uint32_t n_robots,
                          uint32_t* robot_flags, cudaStream_t s);
 

@@ -722,6 +722,13 @@ __global__ void flags_kernel(const float4* __restrict__ pos, const int64_t* __re
     if (lane == 0) out[warp] = bad ? 1u : 0u;
 }
 
+// Bit 1 of a robot's status: its (first) bin was skipped by the step kernel.
+__global__ void bin_flags_kernel(const uint32_t* __restrict__ bin_flags, const uint32_t* __restrict__ robot_bin,
+                                 uint32_t n_robots, uint32_t* __restrict__ out) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < n_robots) out[r] |= bin_flags[robot_bin[r]] & 2u;
+}
+
 using StepFn = void (*)(const StepParams);
 
 struct ShapeEntry {
@@ -1002,6 +1009,13 @@ cudaError_t launch_com(const float4* pos, const uint8_t* mass_mat, const int64_t
     const uint32_t threads = 256, warps = threads / 32;
     com_kernel<<<(n_robots + warps - 1) / warps, threads, 0, s>>>(pos, mass_mat, mass_off,
                                                                    n_robots, com);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_bin_flags(const uint32_t* bin_flags, const uint32_t* robot_bin, uint32_t n_robots,
+                             uint32_t* out, cudaStream_t s) {
+    if (n_robots == 0) return cudaSuccess;
+    bin_flags_kernel<<<(n_robots + 255) / 256, 256, 0, s>>>(bin_flags, robot_bin, n_robots, out);
     return cudaGetLastError();
 }
 
