@@ -755,22 +755,23 @@ const ShapeEntry kShapes[] = {
     MB_SHAPE(1024, 8, 2, false),  MB_SHAPE(1024, 10, 2, false), MB_SHAPE(1024, 12, 2, false),
 };
 // register-row twins of the 1,024-thread shapes (one mass per thread; no
-// face drag): launch_step uses one when every bin has at most 1,024 masses
-#define MB_RR(T, S, RW, SPLIT)                                                                   \
+// face drag): launch_step uses one when the host marks the launch eligible
+// (StepParams::one_mass_per_thread)
+#define MB_RR(T, S, RW)                                                                          \
     {                                                                                            \
         T, S, 1, {                                                                               \
-            {step_kernel<T, S, 1, kModeXpbd, false, SPLIT, RW>,                                  \
-             step_kernel<T, S, 1, kModeXpbd, true, SPLIT, RW>},                                  \
-                {step_kernel<T, S, 1, kModeForceLand, false, SPLIT, RW>,                         \
-                 step_kernel<T, S, 1, kModeForceLand, true, SPLIT, RW>},                         \
-                {step_kernel<T, S, 1, kModeForceWater, false, SPLIT, RW>,                        \
-                 step_kernel<T, S, 1, kModeForceWater, true, SPLIT, RW>},                        \
+            {step_kernel<T, S, 1, kModeXpbd, false, false, RW>,                                  \
+             step_kernel<T, S, 1, kModeXpbd, true, false, RW>},                                  \
+                {step_kernel<T, S, 1, kModeForceLand, false, false, RW>,                         \
+                 step_kernel<T, S, 1, kModeForceLand, true, false, RW>},                         \
+                {step_kernel<T, S, 1, kModeForceWater, false, false, RW>,                        \
+                 step_kernel<T, S, 1, kModeForceWater, true, false, RW>},                        \
                 {nullptr, nullptr},                                                              \
         }                                                                                        \
     }
 constexpr int kRowRegWidth = 26;  // register rows: entries per mass (lattice robots: at most 26)
-const ShapeEntry kRowRegShapes[] = {MB_RR(1024, 8, kRowRegWidth, false), MB_RR(1024, 10, kRowRegWidth, false),
-                                    MB_RR(1024, 12, kRowRegWidth, false)};
+const ShapeEntry kRowRegShapes[] = {MB_RR(1024, 8, kRowRegWidth), MB_RR(1024, 10, kRowRegWidth),
+                                    MB_RR(1024, 12, kRowRegWidth)};
 #undef MB_RR
 // the parts of split robots (thread-block clusters)
 const ShapeEntry kSplitShapes[] = {
@@ -813,8 +814,8 @@ const ShapeEntry* find_shape(const KernelShape& s) {
     return nullptr;
 }
 
-// The register-row twin of a 1,024-thread shape, for launches whose bins all
-// hold at most 1,024 masses and that have no face drag.
+// The register-row twin of a 1,024-thread shape, for the launches the host
+// marks eligible (no face drag).
 const ShapeEntry* find_row_reg(const KernelShape& s, const StepParams& p) {
     if (s.threads != 1024 || !p.one_mass_per_thread || p.face_on) return nullptr;
     for (const auto& e : kRowRegShapes)
@@ -827,7 +828,6 @@ const ShapeEntry* find_split(const KernelShape& s) {
         if (e.threads == s.threads && e.spt == s.spt && e.mpt == s.mpt) return &e;
     return nullptr;
 }
-
 
 }  // namespace
 
