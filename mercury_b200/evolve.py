@@ -17,29 +17,27 @@ evaluated, and the pool keeps the best simulated genomes.
 
 Warm-up: 53,248 simulated robots -- three batches of 4096 random genomes,
 then batches of children of the elite pool so far (plain evolution), so that
-the surrogate trains on the distribution it will screen (random genomes
-alone: top-10% recall 0.78; this warm-up: about 0.88) -- then 60 epochs
+the surrogate trains on the distribution it will screen -- then 60 epochs
 with a cosine learning rate.
-
-Screened: the surrogate predicts all children (the mean over the 8
-horizontal orientations of each, plus `kappa` times their spread: children
-the orientations disagree on are the least certain), its top `screen`
-fraction plus a random `audit` fraction of the rest are simulated, and the surrogate trains on the
-new (genome, fitness) pairs; the others are discarded unsimulated.  A
-child differs from its (simulated) parents in a few voxels, so each
-prediction is corrected by the surrogate's error on the parents, weighted
-by the share of voxels from each (lineage correction).  Training
-draws every sample in a random orientation; per generation, a few steps
-whose batches are half from the newest generation.
-Plain: every child is simulated.
 
 Both methods keep the fitness of every genome they have simulated (the
 simulator is deterministic to the bit, so a copy needs no simulation): a
-child identical to a simulated genome -- about a quarter of the children,
-the unchanged copies of a parent and the crossovers of a parent with
-itself -- takes its known fitness, and only the new children are simulated
-or, when screened, ranked by the surrogate.  The elite pool holds distinct
+child identical to a simulated genome -- a fifth to a quarter of the
+children, the unchanged copies of a parent and the crossovers of a parent
+with itself -- takes its known fitness.  The elite pool holds distinct
 genomes.
+
+Screened: the surrogate predicts the new children (the mean over the 8
+horizontal orientations of each, plus `kappa` times their spread: children
+the orientations disagree on are the least certain), its top `screen`
+fraction plus a random `audit` fraction of the rest are simulated, and the
+surrogate trains on the new (genome, fitness) pairs; the others are
+discarded unsimulated.  A child differs from its (simulated) parents in a
+few voxels, so each prediction is corrected by the surrogate's error on the
+parents, weighted by the share of voxels from each (lineage correction).
+Training draws every sample in a random orientation; per generation, a few
+steps whose batches are half from the newest generation.
+Plain: every new child is simulated.
 """
 from __future__ import annotations
 
