@@ -775,6 +775,8 @@ const ShapeEntry kRowRegShapes[] = {MB_RR(1024, 8, kRowRegWidth), MB_RR(1024, 10
 #undef MB_RR
 // the parts of split robots (thread-block clusters)
 const ShapeEntry kSplitShapes[] = {
+    MB_SHAPE(1024, 8, 1, true),
+    MB_SHAPE(1024, 10, 1, true),
     MB_SHAPE(1024, 8, 2, true),
     MB_SHAPE(1024, 10, 2, true),
     MB_SHAPE(1024, 12, 2, true),

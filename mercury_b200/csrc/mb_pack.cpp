@@ -148,8 +148,9 @@ const KernelShape kAuto[] = {
     {1024, 6, 2},  {1024, 4, 1},  {512, 4, 1},  {256, 8, 2},
 };
 
-// Shapes for the parts of split robots, in order of preference.
-const KernelShape kSplit[] = {{1024, 8, 2}, {1024, 10, 2}, {1024, 12, 2}};
+// Shapes for the parts of split robots, in order of preference: one own mass
+// per thread first (fewer registers, no spills at the 64-register cap).
+const KernelShape kSplit[] = {{1024, 8, 1}, {1024, 10, 1}, {1024, 8, 2}, {1024, 10, 2}, {1024, 12, 2}};
 
 void preprocess(const mb_batch_desc* b, uint32_t r, RobotPack& p) {
     const int64_t m0 = b->mass_offsets[r], m1 = b->mass_offsets[r + 1];
