@@ -1440,6 +1440,21 @@ mb_status pack_population(const mb_batch_desc* b, const PackOptions& o, Packed& 
                 if (!split_partition_mixed(b, packs, sh, o.smem_cap, split_faces, threads, part_of, sp.parts))
                     continue;
                 sp.C = *std::max_element(sp.parts.begin(), sp.parts.end());
+                if (sh.mpt == 1 && sp.C >= 2) {
+                    // one own mass per thread only where it costs no CTAs: if two
+                    // masses per thread place the robots in fewer bins, take that shape
+                    const KernelShape sh2{sh.threads, sh.spt, 2};
+                    std::vector<std::vector<uint8_t>> part_of2;
+                    SplitParts sp2;
+                    if (split_supported(sh2) &&
+                        split_partition_mixed(b, packs, sh2, o.smem_cap, split_faces, threads, part_of2, sp2.parts)) {
+                        sp2.C = *std::max_element(sp2.parts.begin(), sp2.parts.end());
+                        SplitParts sp1;
+                        sp1.parts = sp.parts;
+                        sp1.C = sp.C;
+                        if (place_split(sp2) < place_split(sp1)) continue;
+                    }
+                }
                 if (sp.C < 2) continue;  // every robot fits a CTA alone: not a split population
                 const uint32_t nb = place_split(sp);
                 build_split_parts(b, packs, nb, part_of, slot_of, threads, sp);

@@ -87,6 +87,22 @@ def test_point_cloud_robots_in_water():
     check(b, 1e-4, 150, True, mode=S.MODE_FORCE_WATER, cluster=4)
 
 
+@pytest.mark.parametrize("chains", [1, 2])
+def test_parts_of_one_and_two_masses_per_thread(chains):
+    """A large robot beside 1,500-mass chains: one own mass per thread with
+    one chain, two with two chains (fewer CTAs); bit for bit either way."""
+    n = 1500
+    pos = np.zeros((n, 3), np.float32)
+    pos[:, 0] = 0.1 * np.arange(n)
+    pos[:, 2] = 0.02 * np.sin(np.arange(n))
+    pairs = np.stack([np.arange(n - 1), np.arange(1, n)], 1)
+    chain = mb.Element(pos, np.full(n, 1, np.uint8), pairs, np.full(n - 1, 0.1, np.float32),
+                       np.full(n - 1, 1, np.uint8))
+    b = mb.pack(robots.population("streamed", 1, seed_base=4200) + [chain] * chains)
+    sim = check(b, 1e-3, 150, True, cluster=2)
+    assert sim.launch_config()["masses_per_thread"] == chains
+
+
 def test_split_and_streamed_agree_on_large_robots():
     b = robots.population_batch("streamed", 2, seed_base=4100)
     _, p1, v1, s1 = simulate(b, 1e-4, 300, True)

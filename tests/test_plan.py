@@ -43,6 +43,28 @@ def test_large_robots_are_split_over_clusters():
     assert st4["max_bin_springs"] < st["max_bin_springs"]
 
 
+def _chain(n):
+    """A robot of n masses in a line, one spring between neighbours."""
+    pos = np.zeros((n, 3), np.float32)
+    pos[:, 0] = 0.1 * np.arange(n)
+    pairs = np.stack([np.arange(n - 1), np.arange(1, n)], 1)
+    return mb.Element(pos, np.full(n, 1, np.uint8), pairs, np.full(n - 1, 0.1, np.float32),
+                      np.full(n - 1, 1, np.uint8))
+
+
+def test_split_parts_take_one_mass_per_thread_unless_that_costs_ctas():
+    """Parts of split robots run one own mass per thread, except when two per
+    thread would place the population in fewer CTAs: 1,500-mass chains fit a
+    CTA whole at two masses per thread but need two parts at one."""
+    big = robots.population("streamed", 1)[0]
+    st = mb.plan(mb.pack([big, big]))
+    assert (st["masses_per_thread"], st["bins"], st["cluster"]) == (1, 4, 2)
+    st = mb.plan(mb.pack([big, _chain(1500)]))  # four bins either way
+    assert (st["masses_per_thread"], st["bins"]) == (1, 4)
+    st = mb.plan(mb.pack([big, _chain(1500), _chain(1500)]))  # four bins, not six
+    assert (st["masses_per_thread"], st["bins"], st["cluster"]) == (2, 4, 2)
+
+
 def test_large_robots_are_streamed_when_never_split():
     st = mb.plan(robots.population_batch("streamed", 8), cluster=1)
     assert st["streamed"] == 1 and st["bins"] == 8 and st["threads"] == 1024 and st["cluster"] == 0
