@@ -300,6 +300,14 @@ MB_API mb_status mb_set_launch_config(mb_context* ctx, const mb_launch_config* c
  * launches.  Either pointer may be NULL.  No reference counterpart. */
 MB_API mb_status mb_get_step_variant(const mb_context* ctx, uint32_t* register_rows, uint32_t* smem_bytes);
 
+/* The packed spring slots of the uploaded batch, in device order: *count =
+ * the number of slots; when `words` is not NULL and capacity >= *count, the
+ * packed word of every slot (a | b << 12 | material slot << 24, bin-local
+ * mass indices) is copied into it, else MB_ERR_CAPACITY.  For tests and
+ * tools that check how springs are placed.  No reference counterpart. */
+MB_API mb_status mb_get_packed_springs(const mb_context* ctx, uint32_t* words, uint64_t capacity,
+                                       uint64_t* count);
+
 /* Launch plan of a population, computed on the host without a device:
  * the shape, bin count and path the automatic choice (or `cfg`, may be
  * NULL) would use on a GPU with `num_sms` SMs and `smem_bytes` of dynamic

@@ -112,6 +112,7 @@ def _load() -> ctypes.CDLL:
         "mb_device_state": (I32, [P, ctypes.POINTER(P), ctypes.POINTER(P), ctypes.POINTER(P)]),
         "mb_get_launch_config": (I32, [P, ctypes.POINTER(LaunchConfig)]),
         "mb_get_step_variant": (I32, [P, ctypes.POINTER(U32), ctypes.POINTER(U32)]),
+        "mb_get_packed_springs": (I32, [P, P, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)]),
         "mb_set_launch_config": (I32, [P, ctypes.POINTER(LaunchConfig)]),
         "mb_kernel_shapes": (U32, [ctypes.POINTER(LaunchConfig), U32]),
         "mb_plan_population": (I32, [ctypes.POINTER(BatchDesc), ctypes.POINTER(LaunchConfig), U32, U32,

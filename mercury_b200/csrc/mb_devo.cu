@@ -753,6 +753,103 @@ cudaError_t launch_relayout(const BinDesc* old_bins, const uint32_t* new_begin, 
     return cudaGetLastError();
 }
 
+// Placement of a resident bin's springs (one warp per bin), the rule of the
+// host packer's bank_order: lanes 8q .. 8q + 7 of a warp form one shared-
+// memory wavefront of the step kernel's 16-byte endpoint loads, conflict-
+// free when their masses differ mod 8.  Each group of 8 slots takes, in
+// order, the earliest springs of a window of the next 64 unplaced ones whose
+// a and b are both new mod 8 in the group (the first such spring under the
+// group's used residues, repeatedly: a spring passed over stays blocked,
+// since the used sets only grow), then fills any slot left with the earliest
+// unplaced spring.  The window holds positions 0..63 as two per lane
+// (lane, lane + 32); picks are found by ballot.  The loop touches shared
+// memory only (the bin's packed words and the slot order); then the three
+// arrays are permuted in place, gidx and lbar read from the scratch copy.
+__global__ void __launch_bounds__(32) bank_place_kernel(const BinDesc* __restrict__ bins, uint32_t* pair,
+                                                         uint32_t* gidx, float* lbar,
+                                                         unsigned long long* scratch) {
+    extern __shared__ uint32_t sword[];  // the bin's packed words, in upload order; then the slot order (u16)
+    __shared__ uint32_t win[64];         // bin-local spring indices, window order
+    const uint32_t lane = threadIdx.x;
+    const uint32_t s0 = bins[blockIdx.x].spring_begin, n = bins[blockIdx.x].n_spring;
+    uint16_t* sorder = reinterpret_cast<uint16_t*>(sword + n);  // slot -> upload index (n <= kMaxBinSprings)
+    for (uint32_t i = lane; i < n; i += 32) {
+        sword[i] = pair[s0 + i];
+        scratch[s0 + i] = (unsigned long long)gidx[s0 + i] | (unsigned long long)__float_as_uint(lbar[s0 + i]) << 32;
+    }
+    __syncwarp();
+    uint32_t len = 0, next = 0, placed = 0;
+    while (placed < n) {
+        const uint32_t add = min(64u - len, n - next);
+        for (uint32_t k = lane; k < add; k += 32) win[len + k] = next + k;
+        __syncwarp();
+        len += add;
+        next += add;
+        const uint32_t want = min(8u, n - placed);  // <= len
+        const bool v0 = lane < len, v1 = lane + 32u < len;
+        const uint32_t i0 = v0 ? win[lane] : 0u, i1 = v1 ? win[lane + 32] : 0u;
+        const uint32_t w0 = v0 ? sword[i0] : 0u, w1 = v1 ? sword[i1] : 0u;
+        const uint32_t a0 = w0 & 7u, b0 = (w0 >> 12) & 7u, a1 = w1 & 7u, b1 = (w1 >> 12) & 7u;
+        uint32_t ua = 0, ub = 0, got = 0;  // residues used by the group, mod 8
+        unsigned long long picked = 0;     // bit p: window position p placed in this group
+        while (got < want) {
+            const uint32_t m0 = __ballot_sync(0xFFFFFFFFu, v0 && !((ua >> a0) & 1u) && !((ub >> b0) & 1u));
+            const uint32_t m1 = __ballot_sync(0xFFFFFFFFu, v1 && !((ua >> a1) & 1u) && !((ub >> b1) & 1u));
+            if (!(m0 | m1)) break;
+            const uint32_t p = m0 ? (uint32_t)__ffs(m0) - 1u : 31u + (uint32_t)__ffs(m1);
+            const uint32_t wp = __shfl_sync(0xFFFFFFFFu, p < 32u ? w0 : w1, p & 31u);
+            ua |= 1u << (wp & 7u);
+            ub |= 1u << ((wp >> 12) & 7u);
+            picked |= 1ull << p;
+            ++got;
+        }
+        const unsigned long long valid = len >= 64u ? ~0ull : (1ull << len) - 1ull;
+        for (unsigned long long rest = valid & ~picked; got < want; rest &= rest - 1ull, ++got)
+            picked |= rest & (~rest + 1ull);
+        // the group in window order into slots placed.., the rest compacted
+        const unsigned long long kept = valid & ~picked;
+        __syncwarp();  // every lane has read its window entries
+        if (v0) {
+            const unsigned long long below = (1ull << lane) - 1ull;
+            if ((picked >> lane) & 1ull)
+                sorder[placed + (uint32_t)__popcll(picked & below)] = (uint16_t)i0;
+            else
+                win[__popcll(kept & below)] = i0;
+        }
+        if (v1) {
+            const unsigned long long below = (1ull << (lane + 32u)) - 1ull;
+            if ((picked >> (lane + 32u)) & 1ull)
+                sorder[placed + (uint32_t)__popcll(picked & below)] = (uint16_t)i1;
+            else
+                win[__popcll(kept & below)] = i1;
+        }
+        __syncwarp();
+        len -= got;
+        placed += got;
+    }
+    for (uint32_t d = lane; d < n; d += 32) {
+        const uint32_t i = sorder[d];
+        const unsigned long long x = scratch[s0 + i];
+        pair[s0 + d] = sword[i];
+        gidx[s0 + d] = (uint32_t)x;
+        lbar[s0 + d] = __uint_as_float((uint32_t)(x >> 32));
+    }
+}
+
+cudaError_t launch_bank_place(const BinDesc* bins, uint32_t n_bins, uint32_t max_springs, uint32_t* pair,
+                              uint32_t* gidx, float* lbar, unsigned long long* scratch, cudaStream_t s) {
+    if (n_bins == 0 || max_springs == 0) return cudaSuccess;
+    if (max_springs > kMaxBinSprings) return cudaErrorInvalidValue;
+    const size_t smem = (size_t)max_springs * (sizeof(uint32_t) + sizeof(uint16_t)) + 4u;
+    if (smem > 48u * 1024u) {
+        cudaError_t e = cudaFuncSetAttribute(bank_place_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    bank_place_kernel<<<n_bins, 32, smem, s>>>(bins, pair, gidx, lbar, scratch);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_rebuild(const RebuildParams& p, cudaStream_t s) {
     if (p.n_bins == 0) return cudaSuccess;
     rebuild_kernel<<<p.n_bins, kRebuildThreads, 0, s>>>(p);

@@ -105,6 +105,12 @@ cudaError_t launch_relayout(const BinDesc* old_bins, const uint32_t* new_begin, 
 // Rebuilds every bin's rows; status[1] gets the largest shared memory a
 // bin needs.
 cudaError_t launch_rebuild(const RebuildParams& p, cudaStream_t s);
+// Places the springs of every resident bin for the step kernel's endpoint
+// loads (the host packer's bank_order rule, same result): pair, gidx and
+// lbar are permuted in place within each bin; scratch holds one u64 per
+// packed slot; max_springs is the largest bin's spring count.
+cudaError_t launch_bank_place(const BinDesc* bins, uint32_t n_bins, uint32_t max_springs, uint32_t* pair,
+                              uint32_t* gidx, float* lbar, unsigned long long* scratch, cudaStream_t s);
 
 // ---------------------------------------------------------------------------
 // Development of robots split over thread-block clusters (one part per bin).

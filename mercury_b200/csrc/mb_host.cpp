@@ -444,6 +444,12 @@ mb_status upload_packed(mb_context* ctx, const mb::Packed& out, bool* rows_faile
         MB_CUDA(ctx, cudaMemsetAsync(ctx->free_count.p, 0, nb * sizeof(uint32_t), st));
         MB_CUDA(ctx, cudaMemsetAsync(ctx->free_taken.p, 0, nb * sizeof(uint32_t), st));
         MB_CUDA(ctx, cudaMemsetAsync(ctx->devo_status.p, 0, 2 * sizeof(uint32_t), st));
+        // the springs of every bin placed for the endpoint loads (the host
+        // packer left them in upload order), then the rows built
+        uint32_t max_springs = 0;
+        for (const mb::BinDesc& d : out.bins) max_springs = std::max(max_springs, d.n_spring);
+        MB_CUDA(ctx, mb::launch_bank_place(ctx->bins.p, nb, max_springs, ctx->spring_pair.p, ctx->spring_gidx.p,
+                                           ctx->spring_lbar.p, ctx->rows_scratch.p, st));
         // no packed slot is inert here: spring_gidx < n_spring everywhere
         const mb::RebuildParams rp{ctx->bins.p,        nb,                   ctx->spring_pair.p,
                                    ctx->spring_gidx.p, (uint32_t)ctx->n_spring, ctx->slice_off.p,
@@ -1037,6 +1043,20 @@ mb_status mb_get_step_variant(const mb_context* ctx, uint32_t* register_rows, ui
     if (register_rows) *register_rows = rr ? 1u : 0u;
     if (smem_bytes) *smem_bytes = rr ? rr : ctx->smem_bytes;
     return MB_OK;
+}
+
+mb_status mb_get_packed_springs(const mb_context* ctx, uint32_t* words, uint64_t capacity, uint64_t* count) {
+    if (!ctx || !count) return MB_ERR_ARGUMENT;
+    if (!ctx->loaded) return MB_ERR_STATE;
+    *count = ctx->n_packed;
+    if (!words) return MB_OK;
+    if (capacity < ctx->n_packed) return MB_ERR_CAPACITY;
+    cudaSetDevice(ctx->device);
+    if (ctx->n_packed &&
+        cudaMemcpyAsync(words, ctx->spring_pair.p, ctx->n_packed * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                        ctx->stream) != cudaSuccess)
+        return MB_ERR_CUDA;
+    return cudaStreamSynchronize(ctx->stream) == cudaSuccess ? MB_OK : MB_ERR_CUDA;
 }
 
 mb_status mb_plan_population(const mb_batch_desc* batch, const mb_launch_config* cfg, uint32_t num_sms,

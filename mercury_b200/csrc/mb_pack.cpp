@@ -638,8 +638,10 @@ void build_bin(const mb_batch_desc* b, const std::vector<RobotPack>& packs,
     }
     // resident bins: springs placed so that the 8 springs of every
     // quarter-warp read distinct 16-byte bank groups of the predicted
-    // positions at both ends (newpos: old position -> packed position)
-    std::vector<uint32_t> order = streamed ? std::vector<uint32_t>{} : bank_order(words);
+    // positions at both ends (newpos: old position -> packed position); with
+    // the rows built on the device, the device places them too
+    // (launch_bank_place, the same rule)
+    std::vector<uint32_t> order = streamed || rows_on_device ? std::vector<uint32_t>{} : bank_order(words);
     std::vector<uint32_t> newpos(ns);
     for (uint32_t i = 0; i < ns; ++i) {
         const uint32_t o = order.empty() ? i : order[i];

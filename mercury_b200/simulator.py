@@ -318,6 +318,16 @@ class Simulator:
         _lib.check(_lib.LIB.mb_get_step_variant(self._ctx, ctypes.byref(rr), ctypes.byref(smem)), self._ctx)
         return {"register_rows": rr.value, "smem_bytes": smem.value}
 
+    def packed_springs(self) -> np.ndarray:
+        """The packed word of every spring slot on the device, in slot order
+        (mb_get_packed_springs): a | b << 12 | material slot << 24."""
+        n = ctypes.c_uint64()
+        _lib.check(_lib.LIB.mb_get_packed_springs(self._ctx, None, 0, ctypes.byref(n)), self._ctx)
+        out = np.empty(n.value, np.uint32)
+        _lib.check(_lib.LIB.mb_get_packed_springs(self._ctx, _lib.ptr(out), n.value, ctypes.byref(n)),
+                   self._ctx)
+        return out
+
     def set_launch_config(self, threads=0, springs_per_thread=0, masses_per_thread=0, bins=0,
                           chunk=0, use_graph=1, streamed=0, cluster=0) -> None:
         c = _lib.LaunchConfig(threads, springs_per_thread, masses_per_thread, bins, chunk, use_graph,

@@ -263,3 +263,21 @@ def test_rows_built_on_device_or_host_same_bits(monkeypatch, track):
     assert bits_equal(p1, p) and bits_equal(v1, v) and bits_equal(p2, p) and bits_equal(v2, v)
     if track:
         assert bits_equal(s1, s) and bits_equal(s2, s)
+
+
+@pytest.mark.parametrize("name,n", [("uneven", 40), ("uneven", 512), ("small", 300)])
+def test_springs_placed_on_device_as_on_host(monkeypatch, name, n):
+    """With the rows built on the device the springs are placed there too
+    (launch_bank_place); the slots must hold the same springs as the host
+    packer's placement (MB_HOST_ROWS=1), word for word."""
+    b = robots.population_batch(name, n, seed_base=5)
+    sim = mb.Simulator(0)
+    sim.set_batch(b)
+    dev = sim.packed_springs()
+    monkeypatch.setenv("MB_HOST_ROWS", "1")
+    sim2 = mb.Simulator(0)
+    sim2.set_batch(b)
+    host = sim2.packed_springs()
+    assert sim.launch_config() == sim2.launch_config()
+    assert len(dev) == len(host) >= b.active_springs()
+    assert np.array_equal(dev, host)
