@@ -762,23 +762,26 @@ cudaError_t launch_relayout(const BinDesc* old_bins, const uint32_t* new_begin, 
 // group's used residues, repeatedly: a spring passed over stays blocked,
 // since the used sets only grow), then fills any slot left with the earliest
 // unplaced spring.  The window holds positions 0..63 as two per lane
-// (lane, lane + 32); picks are found by ballot.  The loop touches shared
-// memory only (the bin's packed words and the slot order); then the three
-// arrays are permuted in place, gidx and lbar read from the scratch copy.
-__global__ void __launch_bounds__(32) bank_place_kernel(const BinDesc* __restrict__ bins, uint32_t* pair,
-                                                         uint32_t* gidx, float* lbar,
-                                                         unsigned long long* scratch) {
+// (lane, lane + 32); picks are found by ballot.  The loop (warp 0) touches
+// shared memory only (the bin's packed words and the slot order); the whole
+// CTA copies the bin in before and permutes the three arrays in place after
+// it, gidx and lbar read from the scratch copy.
+constexpr uint32_t kPlaceThreads = 256;  // copies by every thread, the placement by warp 0
+
+__global__ void __launch_bounds__(kPlaceThreads) bank_place_kernel(const BinDesc* __restrict__ bins,
+                                                                    uint32_t* pair, uint32_t* gidx, float* lbar,
+                                                                    unsigned long long* scratch) {
     extern __shared__ uint32_t sword[];  // the bin's packed words, in upload order; then the slot order (u16)
     __shared__ uint32_t win[64];         // bin-local spring indices, window order
-    const uint32_t lane = threadIdx.x;
+    const uint32_t tid = threadIdx.x, lane = tid & 31u;
     const uint32_t s0 = bins[blockIdx.x].spring_begin, n = bins[blockIdx.x].n_spring;
     uint16_t* sorder = reinterpret_cast<uint16_t*>(sword + n);  // slot -> upload index (n <= kMaxBinSprings)
-    for (uint32_t i = lane; i < n; i += 32) {
+    for (uint32_t i = tid; i < n; i += kPlaceThreads) {
         sword[i] = pair[s0 + i];
         scratch[s0 + i] = (unsigned long long)gidx[s0 + i] | (unsigned long long)__float_as_uint(lbar[s0 + i]) << 32;
     }
-    __syncwarp();
-    uint32_t len = 0, next = 0, placed = 0;
+    __syncthreads();
+    uint32_t len = 0, next = 0, placed = tid < 32u ? 0u : n;  // warp 0 places
     while (placed < n) {
         const uint32_t add = min(64u - len, n - next);
         for (uint32_t k = lane; k < add; k += 32) win[len + k] = next + k;
@@ -790,13 +793,28 @@ __global__ void __launch_bounds__(32) bank_place_kernel(const BinDesc* __restric
         const uint32_t i0 = v0 ? win[lane] : 0u, i1 = v1 ? win[lane + 32] : 0u;
         const uint32_t w0 = v0 ? sword[i0] : 0u, w1 = v1 ? sword[i1] : 0u;
         const uint32_t a0 = w0 & 7u, b0 = (w0 >> 12) & 7u, a1 = w1 & 7u, b1 = (w1 >> 12) & 7u;
-        uint32_t ua = 0, ub = 0, got = 0;  // residues used by the group, mod 8
-        unsigned long long picked = 0;     // bit p: window position p placed in this group
+        // the longest prefix of the window whose residues are pairwise new
+        // is what the greedy picks first, one after another: taken at once
+        // (both matches run on every lane: a short-circuit would leave lanes
+        // out of a full-warp match)
+        const uint32_t below_lane = (1u << lane) - 1u;
+        const uint32_t same_a = __match_any_sync(0xFFFFFFFFu, a0);
+        const uint32_t same_b = __match_any_sync(0xFFFFFFFFu, b0);
+        const uint32_t cm = __ballot_sync(0xFFFFFFFFu, lane < want && ((same_a | same_b) & below_lane) != 0u);
+        uint32_t got = cm ? (uint32_t)__ffs(cm) - 1u : want;  // >= 1: lane 0 never clashes
+        uint32_t ua = __reduce_or_sync(0xFFFFFFFFu, lane < got ? 1u << a0 : 0u);  // residues used, mod 8
+        uint32_t ub = __reduce_or_sync(0xFFFFFFFFu, lane < got ? 1u << b0 : 0u);
+        unsigned long long picked = (1ull << got) - 1ull;  // bit p: window position p placed in this group
         while (got < want) {
             const uint32_t m0 = __ballot_sync(0xFFFFFFFFu, v0 && !((ua >> a0) & 1u) && !((ub >> b0) & 1u));
-            const uint32_t m1 = __ballot_sync(0xFFFFFFFFu, v1 && !((ua >> a1) & 1u) && !((ub >> b1) & 1u));
-            if (!(m0 | m1)) break;
-            const uint32_t p = m0 ? (uint32_t)__ffs(m0) - 1u : 31u + (uint32_t)__ffs(m1);
+            uint32_t p;
+            if (m0) {
+                p = (uint32_t)__ffs(m0) - 1u;
+            } else {
+                const uint32_t m1 = __ballot_sync(0xFFFFFFFFu, v1 && !((ua >> a1) & 1u) && !((ub >> b1) & 1u));
+                if (!m1) break;
+                p = 31u + (uint32_t)__ffs(m1);
+            }
             const uint32_t wp = __shfl_sync(0xFFFFFFFFu, p < 32u ? w0 : w1, p & 31u);
             ua |= 1u << (wp & 7u);
             ub |= 1u << ((wp >> 12) & 7u);
@@ -827,7 +845,8 @@ __global__ void __launch_bounds__(32) bank_place_kernel(const BinDesc* __restric
         len -= got;
         placed += got;
     }
-    for (uint32_t d = lane; d < n; d += 32) {
+    __syncthreads();
+    for (uint32_t d = tid; d < n; d += kPlaceThreads) {
         const uint32_t i = sorder[d];
         const unsigned long long x = scratch[s0 + i];
         pair[s0 + d] = sword[i];
@@ -846,7 +865,7 @@ cudaError_t launch_bank_place(const BinDesc* bins, uint32_t n_bins, uint32_t max
                                              (int)smem);
         if (e != cudaSuccess) return e;
     }
-    bank_place_kernel<<<n_bins, 32, smem, s>>>(bins, pair, gidx, lbar, scratch);
+    bank_place_kernel<<<n_bins, kPlaceThreads, smem, s>>>(bins, pair, gidx, lbar, scratch);
     return cudaGetLastError();
 }
 
