@@ -387,20 +387,31 @@ mb_status upload_packed(mb_context* ctx, const mb::Packed& out, bool* rows_faile
         }
         // nothing may still read the stage (or the buffers being replaced)
         MB_CUDA(ctx, cudaStreamSynchronize(st));
+        // in four rounds, so that the DMA of one round overlaps the host copy
+        // of the next (each round fills its own range of the stage)
         const unsigned nt = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
-        const size_t piece = std::max<size_t>(1 << 20, (total + nt - 1) / nt);
-        mb::parallel_for(nt, nt, [&](uint32_t t) {
-            const size_t lo = t * piece, hi = std::min(total, lo + piece);
+        constexpr size_t kRounds = 4;
+        const size_t round = std::max<size_t>(4 << 20, (total + kRounds - 1) / kRounds);
+        for (size_t r0 = 0; r0 < total; r0 += round) {
+            const size_t r1 = std::min(total, r0 + round);
+            const size_t piece = (r1 - r0 + nt - 1) / nt;
+            mb::parallel_for(nt, nt, [&](uint32_t t) {
+                const size_t lo = r0 + t * piece, hi = std::min(r1, lo + piece);
+                for (const Item& it : items) {
+                    const size_t a = std::max(lo, it.off), z = std::min(hi, it.off + it.bytes);
+                    if (a < z)
+                        std::memcpy(static_cast<char*>(ctx->stage) + a,
+                                    static_cast<const char*>(it.src) + (a - it.off), z - a);
+                }
+            });
             for (const Item& it : items) {
-                const size_t a = std::max(lo, it.off), z = std::min(hi, it.off + it.bytes);
+                const size_t a = std::max(r0, it.off), z = std::min(r1, it.off + it.bytes);
                 if (a < z)
-                    std::memcpy(static_cast<char*>(ctx->stage) + a, static_cast<const char*>(it.src) + (a - it.off),
-                                z - a);
+                    MB_CUDA(ctx, cudaMemcpyAsync(static_cast<char*>(it.dst) + (a - it.off),
+                                                 static_cast<char*>(ctx->stage) + a, z - a,
+                                                 cudaMemcpyHostToDevice, st));
             }
-        });
-        for (const Item& it : items)
-            MB_CUDA(ctx, cudaMemcpyAsync(it.dst, static_cast<char*>(ctx->stage) + it.off, it.bytes,
-                                         cudaMemcpyHostToDevice, st));
+        }
     }
     MB_CUDA(ctx, up(ctx->bins, out.bins.data(), out.bins.size()));
     MB_CUDA(ctx, up(ctx->slice_off, out.slice_off.data(), out.slice_off.size()));

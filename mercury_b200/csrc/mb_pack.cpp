@@ -209,7 +209,8 @@ void preprocess(const mb_batch_desc* b, uint32_t r, RobotPack& p) {
     // stable counting passes -- by a, then by b - a -- give exactly that
     {
         const size_t n = sp.size();
-        std::vector<uint32_t> tmp(n), cnt(8193);
+        const uint32_t nm = (uint32_t)cm;  // a, b < nm, so |b - a| < nm
+        std::vector<uint32_t> tmp(n), cnt(2 * (size_t)nm + 1);
         auto pass = [&](const std::vector<uint32_t>& src, std::vector<uint32_t>& dst, uint32_t buckets,
                         auto key) {
             std::fill(cnt.begin(), cnt.begin() + buckets + 1, 0u);
@@ -218,11 +219,11 @@ void preprocess(const mb_batch_desc* b, uint32_t r, RobotPack& p) {
             for (uint32_t x : src) dst[cnt[key(x)]++] = x;
         };
         auto key_a = [&](uint32_t ls) { return (uint32_t)b->pairs[2 * (s0 + ls)]; };
-        auto key_dx = [&](uint32_t ls) {  // |b - a| < 4096
-            return (uint32_t)((int)b->pairs[2 * (s0 + ls) + 1] - (int)b->pairs[2 * (s0 + ls)] + 4096);
+        auto key_dx = [&](uint32_t ls) {
+            return (uint32_t)((int)b->pairs[2 * (s0 + ls) + 1] - (int)b->pairs[2 * (s0 + ls)] + (int)nm);
         };
-        pass(sp, tmp, 4096, key_a);
-        pass(tmp, sp, 8192, key_dx);
+        pass(sp, tmp, nm, key_a);
+        pass(tmp, sp, 2 * nm, key_dx);
     }
     // faces: corners in range, at most kMaxFacesPerMass faces per mass;
     // faces with two equal corners are skipped (sim_kernel.cu:99)
