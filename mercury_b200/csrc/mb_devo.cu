@@ -762,18 +762,20 @@ cudaError_t launch_relayout(const BinDesc* old_bins, const uint32_t* new_begin, 
 // group's used residues, repeatedly: a spring passed over stays blocked,
 // since the used sets only grow), then fills any slot left with the earliest
 // unplaced spring.  The window holds positions 0..63 as two per lane
-// (lane, lane + 32); picks are found by ballot.  The loop (warp 0) touches
-// shared memory only (the bin's packed words and the slot order); the whole
-// CTA copies the bin in before and permutes the three arrays in place after
-// it, gidx and lbar read from the scratch copy.
-constexpr uint32_t kPlaceThreads = 256;  // copies by every thread, the placement by warp 0
+// (lane, lane + 32); picks are found by ballot.  Each chunk of kPlaceChunk
+// springs is placed on its own, by one warp (chunks w, w + 16, ... by warp
+// w); the loop touches shared memory only (the bin's packed words and the
+// slot order); the whole CTA copies the bin in before and permutes the
+// three arrays in place after it, gidx and lbar read from the scratch copy.
+constexpr uint32_t kPlaceThreads = 512;
 
 __global__ void __launch_bounds__(kPlaceThreads) bank_place_kernel(const BinDesc* __restrict__ bins,
                                                                     uint32_t* pair, uint32_t* gidx, float* lbar,
                                                                     unsigned long long* scratch) {
     extern __shared__ uint32_t sword[];  // the bin's packed words, in upload order; then the slot order (u16)
-    __shared__ uint32_t win[64];         // bin-local spring indices, window order
+    __shared__ uint32_t swin[kPlaceThreads / 32][64];  // per warp: bin-local spring indices, window order
     const uint32_t tid = threadIdx.x, lane = tid & 31u;
+    uint32_t* win = swin[tid >> 5];
     const uint32_t s0 = bins[blockIdx.x].spring_begin, n = bins[blockIdx.x].n_spring;
     uint16_t* sorder = reinterpret_cast<uint16_t*>(sword + n);  // slot -> upload index (n <= kMaxBinSprings)
     for (uint32_t i = tid; i < n; i += kPlaceThreads) {
@@ -781,69 +783,72 @@ __global__ void __launch_bounds__(kPlaceThreads) bank_place_kernel(const BinDesc
         scratch[s0 + i] = (unsigned long long)gidx[s0 + i] | (unsigned long long)__float_as_uint(lbar[s0 + i]) << 32;
     }
     __syncthreads();
-    uint32_t len = 0, next = 0, placed = tid < 32u ? 0u : n;  // warp 0 places
-    while (placed < n) {
-        const uint32_t add = min(64u - len, n - next);
-        for (uint32_t k = lane; k < add; k += 32) win[len + k] = next + k;
-        __syncwarp();
-        len += add;
-        next += add;
-        const uint32_t want = min(8u, n - placed);  // <= len
-        const bool v0 = lane < len, v1 = lane + 32u < len;
-        const uint32_t i0 = v0 ? win[lane] : 0u, i1 = v1 ? win[lane + 32] : 0u;
-        const uint32_t w0 = v0 ? sword[i0] : 0u, w1 = v1 ? sword[i1] : 0u;
-        const uint32_t a0 = w0 & 7u, b0 = (w0 >> 12) & 7u, a1 = w1 & 7u, b1 = (w1 >> 12) & 7u;
-        // the longest prefix of the window whose residues are pairwise new
-        // is what the greedy picks first, one after another: taken at once
-        // (both matches run on every lane: a short-circuit would leave lanes
-        // out of a full-warp match)
-        const uint32_t below_lane = (1u << lane) - 1u;
-        const uint32_t same_a = __match_any_sync(0xFFFFFFFFu, a0);
-        const uint32_t same_b = __match_any_sync(0xFFFFFFFFu, b0);
-        const uint32_t cm = __ballot_sync(0xFFFFFFFFu, lane < want && ((same_a | same_b) & below_lane) != 0u);
-        uint32_t got = cm ? (uint32_t)__ffs(cm) - 1u : want;  // >= 1: lane 0 never clashes
-        uint32_t ua = __reduce_or_sync(0xFFFFFFFFu, lane < got ? 1u << a0 : 0u);  // residues used, mod 8
-        uint32_t ub = __reduce_or_sync(0xFFFFFFFFu, lane < got ? 1u << b0 : 0u);
-        unsigned long long picked = (1ull << got) - 1ull;  // bit p: window position p placed in this group
-        while (got < want) {
-            const uint32_t m0 = __ballot_sync(0xFFFFFFFFu, v0 && !((ua >> a0) & 1u) && !((ub >> b0) & 1u));
-            uint32_t p;
-            if (m0) {
-                p = (uint32_t)__ffs(m0) - 1u;
-            } else {
-                const uint32_t m1 = __ballot_sync(0xFFFFFFFFu, v1 && !((ua >> a1) & 1u) && !((ub >> b1) & 1u));
-                if (!m1) break;
-                p = 31u + (uint32_t)__ffs(m1);
+    for (uint32_t c0 = (tid >> 5) * kPlaceChunk; c0 < n; c0 += kPlaceThreads / 32u * kPlaceChunk) {
+        const uint32_t c1 = min(n, c0 + kPlaceChunk);
+        uint32_t len = 0, next = c0, placed = c0;
+        while (placed < c1) {
+            const uint32_t add = min(64u - len, c1 - next);
+            for (uint32_t k = lane; k < add; k += 32) win[len + k] = next + k;
+            __syncwarp();
+            len += add;
+            next += add;
+            const uint32_t want = min(8u, c1 - placed);  // <= len
+            const bool v0 = lane < len, v1 = lane + 32u < len;
+            const uint32_t i0 = v0 ? win[lane] : 0u, i1 = v1 ? win[lane + 32] : 0u;
+            const uint32_t w0 = v0 ? sword[i0] : 0u, w1 = v1 ? sword[i1] : 0u;
+            const uint32_t a0 = w0 & 7u, b0 = (w0 >> 12) & 7u, a1 = w1 & 7u, b1 = (w1 >> 12) & 7u;
+            // the longest prefix of the window whose residues are pairwise new
+            // is what the greedy picks first, one after another: taken at once
+            // (both matches run on every lane: a short-circuit would leave lanes
+            // out of a full-warp match)
+            const uint32_t below_lane = (1u << lane) - 1u;
+            const uint32_t same_a = __match_any_sync(0xFFFFFFFFu, a0);
+            const uint32_t same_b = __match_any_sync(0xFFFFFFFFu, b0);
+            const uint32_t cm = __ballot_sync(0xFFFFFFFFu, lane < want && ((same_a | same_b) & below_lane) != 0u);
+            uint32_t got = cm ? (uint32_t)__ffs(cm) - 1u : want;  // >= 1: lane 0 never clashes
+            uint32_t ua = __reduce_or_sync(0xFFFFFFFFu, lane < got ? 1u << a0 : 0u);  // residues used, mod 8
+            uint32_t ub = __reduce_or_sync(0xFFFFFFFFu, lane < got ? 1u << b0 : 0u);
+            unsigned long long picked = (1ull << got) - 1ull;  // bit p: window position p placed in this group
+            while (got < want) {
+                const uint32_t m0 = __ballot_sync(0xFFFFFFFFu, v0 && !((ua >> a0) & 1u) && !((ub >> b0) & 1u));
+                uint32_t p;
+                if (m0) {
+                    p = (uint32_t)__ffs(m0) - 1u;
+                } else {
+                    const uint32_t m1 = __ballot_sync(0xFFFFFFFFu, v1 && !((ua >> a1) & 1u) && !((ub >> b1) & 1u));
+                    if (!m1) break;
+                    p = 31u + (uint32_t)__ffs(m1);
+                }
+                const uint32_t wp = __shfl_sync(0xFFFFFFFFu, p < 32u ? w0 : w1, p & 31u);
+                ua |= 1u << (wp & 7u);
+                ub |= 1u << ((wp >> 12) & 7u);
+                picked |= 1ull << p;
+                ++got;
             }
-            const uint32_t wp = __shfl_sync(0xFFFFFFFFu, p < 32u ? w0 : w1, p & 31u);
-            ua |= 1u << (wp & 7u);
-            ub |= 1u << ((wp >> 12) & 7u);
-            picked |= 1ull << p;
-            ++got;
+            const unsigned long long valid = len >= 64u ? ~0ull : (1ull << len) - 1ull;
+            for (unsigned long long rest = valid & ~picked; got < want; rest &= rest - 1ull, ++got)
+                picked |= rest & (~rest + 1ull);
+            // the group in window order into slots placed.., the rest compacted
+            const unsigned long long kept = valid & ~picked;
+            __syncwarp();  // every lane has read its window entries
+            if (v0) {
+                const unsigned long long below = (1ull << lane) - 1ull;
+                if ((picked >> lane) & 1ull)
+                    sorder[placed + (uint32_t)__popcll(picked & below)] = (uint16_t)i0;
+                else
+                    win[__popcll(kept & below)] = i0;
+            }
+            if (v1) {
+                const unsigned long long below = (1ull << (lane + 32u)) - 1ull;
+                if ((picked >> (lane + 32u)) & 1ull)
+                    sorder[placed + (uint32_t)__popcll(picked & below)] = (uint16_t)i1;
+                else
+                    win[__popcll(kept & below)] = i1;
+            }
+            __syncwarp();
+            len -= got;
+            placed += got;
         }
-        const unsigned long long valid = len >= 64u ? ~0ull : (1ull << len) - 1ull;
-        for (unsigned long long rest = valid & ~picked; got < want; rest &= rest - 1ull, ++got)
-            picked |= rest & (~rest + 1ull);
-        // the group in window order into slots placed.., the rest compacted
-        const unsigned long long kept = valid & ~picked;
-        __syncwarp();  // every lane has read its window entries
-        if (v0) {
-            const unsigned long long below = (1ull << lane) - 1ull;
-            if ((picked >> lane) & 1ull)
-                sorder[placed + (uint32_t)__popcll(picked & below)] = (uint16_t)i0;
-            else
-                win[__popcll(kept & below)] = i0;
-        }
-        if (v1) {
-            const unsigned long long below = (1ull << (lane + 32u)) - 1ull;
-            if ((picked >> (lane + 32u)) & 1ull)
-                sorder[placed + (uint32_t)__popcll(picked & below)] = (uint16_t)i1;
-            else
-                win[__popcll(kept & below)] = i1;
-        }
-        __syncwarp();
-        len -= got;
-        placed += got;
     }
     __syncthreads();
     for (uint32_t d = tid; d < n; d += kPlaceThreads) {
@@ -859,12 +864,11 @@ cudaError_t launch_bank_place(const BinDesc* bins, uint32_t n_bins, uint32_t max
                               uint32_t* gidx, float* lbar, unsigned long long* scratch, cudaStream_t s) {
     if (n_bins == 0 || max_springs == 0) return cudaSuccess;
     if (max_springs > kMaxBinSprings) return cudaErrorInvalidValue;
+    // the opt-in covers the static windows too: static + dynamic above 48 KB
+    // needs it, so it is set on every launch
     const size_t smem = (size_t)max_springs * (sizeof(uint32_t) + sizeof(uint16_t)) + 4u;
-    if (smem > 48u * 1024u) {
-        cudaError_t e = cudaFuncSetAttribute(bank_place_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)smem);
-        if (e != cudaSuccess) return e;
-    }
+    cudaError_t e = cudaFuncSetAttribute(bank_place_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
     bank_place_kernel<<<n_bins, kPlaceThreads, smem, s>>>(bins, pair, gidx, lbar, scratch);
     return cudaGetLastError();
 }

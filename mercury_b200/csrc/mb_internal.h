@@ -14,6 +14,9 @@ constexpr uint16_t kPadEntry = 0xFFFFu;
 constexpr uint32_t kPadEntry32 = 0xFFFFFFFFu;
 constexpr uint32_t kMaxBinSprings = 32767;  // 15-bit spring index in an entry
 constexpr uint32_t kSliceWidth = 32;  // masses per SELL slice (one warp)
+// springs of a resident bin placed independently for the endpoint loads
+// (a multiple of 8: whole groups of a quarter-warp)
+constexpr uint32_t kPlaceChunk = 1024;
 
 // One bin: a group of whole robots that one CTA simulates together.  Masses
 // and springs of the bin are numbered 0..n-1 in "packed" order; packed

@@ -569,41 +569,46 @@ void build_faces(const mb_batch_desc* b, const std::vector<RobotPack>& packs,
 // masses differ mod 8.  Greedy, in order: each group of 8 slots takes the
 // earliest springs, within a window of the next kWindow unplaced ones, whose
 // a and b are both new mod 8 in the group, then fills any slot left with the
-// earliest unplaced spring.  Returns order[new position] = old position.
+// earliest unplaced spring.  Each chunk of kPlaceChunk springs is placed on
+// its own (the device places the chunks of a bin in parallel).  Returns
+// order[new position] = old position.
 std::vector<uint32_t> bank_order(const std::vector<uint32_t>& words) {
     constexpr uint32_t kWindow = 64;
     const uint32_t n = (uint32_t)words.size();
     std::vector<uint32_t> order;
     order.reserve(n);
-    // the window: the earliest unplaced springs, in order
-    uint32_t win[kWindow], len = 0, next = 0;
-    while (order.size() < n) {
-        while (len < kWindow && next < n) win[len++] = next++;
-        const uint32_t want = std::min<uint32_t>(8, n - (uint32_t)order.size());
-        uint32_t used_a = 0, used_b = 0, got = 0;
-        uint64_t picked = 0;  // bit k: win[k] placed in this group
-        for (uint32_t k = 0; k < len && got < want; ++k) {
-            const uint32_t w = words[win[k]];
-            const uint32_t ba = 1u << (w & 7u), bb = 1u << ((w >> 12) & 7u);
-            if ((used_a & ba) || (used_b & bb)) continue;
-            used_a |= ba;
-            used_b |= bb;
-            picked |= 1ull << k;
-            ++got;
-        }
-        for (uint32_t k = 0; k < len && got < want; ++k)
-            if (!((picked >> k) & 1ull)) {
+    for (uint32_t c0 = 0; c0 < n; c0 += kPlaceChunk) {
+        const uint32_t c1 = std::min(n, c0 + kPlaceChunk);
+        // the window: the earliest unplaced springs of the chunk, in order
+        uint32_t win[kWindow], len = 0, next = c0;
+        while (order.size() < c1) {
+            while (len < kWindow && next < c1) win[len++] = next++;
+            const uint32_t want = std::min<uint32_t>(8, c1 - (uint32_t)order.size());
+            uint32_t used_a = 0, used_b = 0, got = 0;
+            uint64_t picked = 0;  // bit k: win[k] placed in this group
+            for (uint32_t k = 0; k < len && got < want; ++k) {
+                const uint32_t w = words[win[k]];
+                const uint32_t ba = 1u << (w & 7u), bb = 1u << ((w >> 12) & 7u);
+                if ((used_a & ba) || (used_b & bb)) continue;
+                used_a |= ba;
+                used_b |= bb;
                 picked |= 1ull << k;
                 ++got;
             }
-        // the group in window order (= spring order), then the window compacted
-        uint32_t keep = 0;
-        for (uint32_t k = 0; k < len; ++k)
-            if ((picked >> k) & 1ull)
-                order.push_back(win[k]);
-            else
-                win[keep++] = win[k];
-        len = keep;
+            for (uint32_t k = 0; k < len && got < want; ++k)
+                if (!((picked >> k) & 1ull)) {
+                    picked |= 1ull << k;
+                    ++got;
+                }
+            // the group in window order (= spring order), then the window compacted
+            uint32_t keep = 0;
+            for (uint32_t k = 0; k < len; ++k)
+                if ((picked >> k) & 1ull)
+                    order.push_back(win[k]);
+                else
+                    win[keep++] = win[k];
+            len = keep;
+        }
     }
     return order;
 }
