@@ -1666,6 +1666,15 @@ mb_status mb_set_voxel_population(mb_context* ctx, uint32_t n_robots, int sx, in
                                ctx->d_spring_mat.p, ctx->slot_of.p, ctx->spring_pair.p, ctx->spring_lbar.p,
                                ctx->spring_gidx.p, ctx->devo_status.p};
     MB_CUDA(ctx, mb::launch_compact(cp, st));
+    if (!ctx->streamed) {
+        // the compaction keeps the template's placement minus the air
+        // springs, which breaks its groups: the active springs are placed
+        // again for the endpoint loads (the template's counts bound the bins)
+        uint32_t max_springs = 0;
+        for (const mb::BinDesc& d : ctx->h_bins) max_springs = std::max(max_springs, d.n_spring);
+        MB_CUDA(ctx, mb::launch_bank_place(ctx->bins.p, ctx->n_bins, max_springs, ctx->spring_pair.p,
+                                           ctx->spring_gidx.p, ctx->spring_lbar.p, ctx->rows_scratch.p, st));
+    }
     const mb::RebuildParams rp{ctx->bins.p,        ctx->n_bins,          ctx->spring_pair.p,
                                ctx->spring_gidx.p, (uint32_t)ctx->n_spring, ctx->slice_off.p,
                                ctx->slice_width.p, ctx->inc.p,           ctx->inc32.p,
