@@ -951,15 +951,26 @@ void build_part(const mb_batch_desc* b, uint32_t r, const RobotPack& pk, const s
     L.pair.reserve(ns);
     L.lbar.reserve(ns);
     std::vector<uint32_t> row_start(n_own + 1, 0);
-    for (uint32_t ls : sp) {
-        const int64_t g = s0 + ls;
+    std::vector<uint32_t> words(ns);
+    for (uint32_t k = 0; k < ns; ++k) {
+        const int64_t g = s0 + sp[k];
         const uint32_t a = b->pairs[2 * g], c = b->pairs[2 * g + 1];
         const uint32_t la = (uint32_t)local_of[a], lc = (uint32_t)local_of[c];
-        L.spring_gidx.push_back((uint32_t)g | (part_of[a] != p ? 0x80000000u : 0u));
-        L.pair.push_back(la | (lc << 12) | ((uint32_t)slot_of[b->spring_material[g]] << 24));
-        L.lbar.push_back(b->lbar[g]);
+        words[k] = la | (lc << 12) | ((uint32_t)slot_of[b->spring_material[g]] << 24);
         if (part_of[a] == p) row_start[la + 1]++;
         if (part_of[c] == p) row_start[lc + 1]++;
+    }
+    // placed for the endpoint loads as in resident bins (part-local indices:
+    // own masses, then halo; newpos: spring order -> packed position)
+    const std::vector<uint32_t> order = bank_order(words);
+    std::vector<uint32_t> newpos(ns);
+    for (uint32_t i = 0; i < ns; ++i) {
+        const uint32_t k = order[i];
+        const int64_t g = s0 + sp[k];
+        newpos[k] = i;
+        L.spring_gidx.push_back((uint32_t)g | (part_of[b->pairs[2 * g]] != p ? 0x80000000u : 0u));
+        L.pair.push_back(words[k]);
+        L.lbar.push_back(b->lbar[g]);
     }
     for (uint32_t i = 0; i < n_own; ++i) row_start[i + 1] += row_start[i];
     raw_vector<Ent> ents(row_start[n_own]);
@@ -972,12 +983,12 @@ void build_part(const mb_batch_desc* b, uint32_t r, const RobotPack& pk, const s
     for (uint32_t k = ns; k-- > 0;) {
         const int64_t g = s0 + sp[k];
         const uint32_t a = b->pairs[2 * g], c = b->pairs[2 * g + 1];
-        if (part_of[c] == p) ents[fill[(uint32_t)local_of[c]]++] = {a, sp[k], 1u, k, a};
+        if (part_of[c] == p) ents[fill[(uint32_t)local_of[c]]++] = {a, sp[k], 1u, newpos[k], a};
     }
     for (uint32_t k = 0; k < ns; ++k) {
         const int64_t g = s0 + sp[k];
         const uint32_t a = b->pairs[2 * g], c = b->pairs[2 * g + 1];
-        if (part_of[a] == p) ents[fill[(uint32_t)local_of[a]]++] = {c, sp[k], 0u, k, c};
+        if (part_of[a] == p) ents[fill[(uint32_t)local_of[a]]++] = {c, sp[k], 0u, newpos[k], c};
     }
     sort_rows(n_own, row_start, ents);
     L.n_mass = n_own;
