@@ -778,6 +778,9 @@ __global__ void __launch_bounds__(kPlaceThreads) bank_place_kernel(const BinDesc
     uint32_t* win = swin[tid >> 5];
     const uint32_t s0 = bins[blockIdx.x].spring_begin, n = bins[blockIdx.x].n_spring;
     uint16_t* sorder = reinterpret_cast<uint16_t*>(sword + n);  // slot -> upload index (n <= kMaxBinSprings)
+    uint32_t dyn;
+    asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
+    if (n > kMaxBinSprings || (size_t)n * 6u > dyn) return;  // the launch was sized for fewer: left as it is
     for (uint32_t i = tid; i < n; i += kPlaceThreads) {
         sword[i] = pair[s0 + i];
         scratch[s0 + i] = (unsigned long long)gidx[s0 + i] | (unsigned long long)__float_as_uint(lbar[s0 + i]) << 32;

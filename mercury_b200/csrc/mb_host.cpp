@@ -222,6 +222,7 @@ struct mb_context {
         int sx = 0, sy = 0, sz = 0;
         uint32_t h_bits = 0, mass_bits = 0, mode = 0;
         uint32_t n_points = 0, n_springs = 0;  // per robot
+        uint32_t max_bin_springs = 0;          // the template's largest bin (active springs bound)
         mb::DevBuf<float> pos;
         mb::DevBuf<uint16_t> src;
         mb::DevBuf<uint8_t> dir, cells;
@@ -900,6 +901,7 @@ mb_status voxel_setup(mb_context* c, uint32_t R, int sx, int sy, int sz, float h
     for (size_t i = 0; i < word.size(); ++i) word[i] = out.pair[i] & 0xFFFFFFu;
     for (size_t b = 0; b < out.bins.size(); ++b) nsp[b] = out.bins[b].n_spring;
     auto& v = c->vox;
+    v.max_bin_springs = nsp.empty() ? 0u : *std::max_element(nsp.begin(), nsp.end());
     MB_CUDA(c, up(v.word, word.data(), word.size()));
     MB_CUDA(c, up(v.lbar, out.lbar.data(), out.lbar.size()));
     MB_CUDA(c, up(v.gidx, out.spring_gidx.data(), out.spring_gidx.size()));
@@ -1670,9 +1672,7 @@ mb_status mb_set_voxel_population(mb_context* ctx, uint32_t n_robots, int sx, in
         // the compaction keeps the template's placement minus the air
         // springs, which breaks its groups: the active springs are placed
         // again for the endpoint loads (the template's counts bound the bins)
-        uint32_t max_springs = 0;
-        for (const mb::BinDesc& d : ctx->h_bins) max_springs = std::max(max_springs, d.n_spring);
-        MB_CUDA(ctx, mb::launch_bank_place(ctx->bins.p, ctx->n_bins, max_springs, ctx->spring_pair.p,
+        MB_CUDA(ctx, mb::launch_bank_place(ctx->bins.p, ctx->n_bins, v.max_bin_springs, ctx->spring_pair.p,
                                            ctx->spring_gidx.p, ctx->spring_lbar.p, ctx->rows_scratch.p, st));
     }
     const mb::RebuildParams rp{ctx->bins.p,        ctx->n_bins,          ctx->spring_pair.p,
